@@ -1,0 +1,735 @@
+"""CPU oracle for viVlasov1D's implicit midpoint (Picard-over-phi) time step.
+
+TEST INFRASTRUCTURE ONLY.  This module is the checker that the CUDA path is
+compared against; it is imported by ``tests/``, by ``__graft_entry__.smoke()``
+and by the ``cpu_baseline`` leg of ``bench.py`` and by nothing else.  The
+product (``vivlasov1d_b200``) never imports it and has no CPU fallback.
+
+It restates, in numpy/scipy, the reference's algorithm for the configuration
+``method=matrixfree, type=nonlinear, mode=split, timestepping=mp`` with the
+'point' time derivative.  Every function cites the reference file:line it
+follows (paths relative to the viVlasov1D project root).
+
+Array convention: a distribution-function field is an ``(nx, nv)`` float64
+array indexed ``f[i, j]`` (i = x index, j = v index), the same view the
+reference's Cython code works on (``vlasov/toolbox/VIDA.pyx:12-57`` reshapes
+the PETSc vector in Fortran order).  The flat memory layout shared with the
+device code is ``F[j*nx + i]``; :func:`to_flat` / :func:`from_flat` convert.
+
+Parity pins: the bracket, time derivative, residual, JVP, Hamiltonian
+assembly, moments, Poisson operator/RHS/residual, preconditioner eigenvalues
+and band matrices, and the invariants are checked against fixtures produced by
+executing the reference's own loop bodies (``tests/golden/make_golden.py``).
+PETSc's GMRES/CG, FFTW and LAPACK live outside the reference tree: GMRES is a
+restatement of PETSc's documented KSPGMRES defaults (restart 30, classical
+Gram-Schmidt without refinement, Givens least squares, zero initial guess,
+KSPConvergedDefault with divtol 1e5); the FFT is numpy's; the band solves call
+the same LAPACK routines (zgbtrf/zgbtrs) through scipy.
+"""
+from __future__ import annotations
+
+import math
+from dataclasses import dataclass, field
+
+import numpy as np
+from scipy.linalg import lapack
+
+STENCIL = 2  # run/run_base.py:49
+
+# PETSc KSPConvergedReason values (petscksp.h)
+KSP_CONVERGED_ITERATING = 0
+KSP_CONVERGED_RTOL = 2
+KSP_CONVERGED_ATOL = 3
+KSP_DIVERGED_NULL = -2
+KSP_DIVERGED_ITS = -3
+KSP_DIVERGED_DTOL = -4
+KSP_DIVERGED_BREAKDOWN = -5
+KSP_DIVERGED_NANORINF = -9
+
+
+# --------------------------------------------------------------------------
+# layout helpers
+# --------------------------------------------------------------------------
+def to_flat(f):
+    """(nx, nv) view -> (nv, nx) C-contiguous array == F[j*nx + i]."""
+    return np.ascontiguousarray(np.asarray(f).T)
+
+
+def from_flat(F, nx=None, nv=None):
+    """(nv, nx) array (or flat F[j*nx+i] with nx, nv given) -> (nx, nv) view."""
+    F = np.asarray(F)
+    if F.ndim == 1:
+        F = F.reshape(nv, nx)
+    return F.T
+
+
+# --------------------------------------------------------------------------
+# grid  (core/Grid.pyx:14-50, run/run_base.py:118-137, 252-288)
+# --------------------------------------------------------------------------
+class Grid:
+    """Grid spacings, coordinates and inverses.
+
+    x is periodic with ``hx = L/nx`` and ``x_i = 0 + i*hx``; v is bounded with
+    ``hv = (vmax - vmin)/(nv - 1)`` and ``v_j = vmin + j*hv`` -- the
+    coordinates PETSc's DMDASetUniformCoordinates produces for the
+    ``['periodic', 'ghosted']`` DMDA (run/run_base.py:215-220, 252-282).
+    """
+
+    def __init__(self, nx, nv, L, vmax, vmin=None, ht=0.1, nt=1):
+        if vmin is None:  # run/run_base.py:130-131
+            vmin = -vmax
+        self.nx, self.nv, self.nt = int(nx), int(nv), int(nt)
+        self.L, self.vmin, self.vmax = float(L), float(vmin), float(vmax)
+        self.ht = float(ht)
+        self.hx = self.L / self.nx                       # run_base.py:136
+        self.hv = (self.vmax - self.vmin) / (self.nv - 1)  # run_base.py:137
+        self.x = 0.0 + np.arange(self.nx) * self.hx
+        self.v = self.vmin + np.arange(self.nv) * self.hv
+        self.v2 = np.power(self.v, 2)                    # Grid.pyx:30
+        self.stencil = STENCIL
+        self.ht_inv = 1. / self.ht                       # Grid.pyx:40-48
+        self.hx_inv = 1. / self.hx
+        self.hv_inv = 1. / self.hv
+        self.hx2 = self.hx ** 2
+        self.hv2 = self.hv ** 2
+        self.hx2_inv = 1. / self.hx2
+        self.hv2_inv = 1. / self.hv2
+
+    def xLength(self):  # Grid.pyx:130-131
+        return self.x[-1] - self.x[0] + self.hx
+
+
+# --------------------------------------------------------------------------
+# initial data  (toolbox/Toolbox.pyx:175-224, run/run_base.py:409-500, 623-628)
+# --------------------------------------------------------------------------
+def kinetic_hamiltonian_v(grid, mass=1.0):
+    """h0 as a function of v only: ``0.5 * v_j**2 * mass`` (Toolbox.pyx:175-187)."""
+    return 0.5 * grid.v ** 2 * mass
+
+
+def initialise_distribution_function(grid, fn):
+    """``f[i,j] = fn(x_i, v_j)``; zero on the band rows (Toolbox.pyx:190-203)."""
+    X, V = np.meshgrid(grid.x, grid.v, indexing="ij")
+    f = np.asarray(fn(X, V), dtype=np.float64).copy()
+    f[:, :STENCIL] = 0.0
+    f[:, grid.nv - STENCIL:] = 0.0
+    return f
+
+
+def initialise_distribution_nT(grid, n, T):
+    """Maxwellian from density/temperature profiles (Toolbox.pyx:206-224)."""
+    fac = math.sqrt(0.5 / np.pi)
+    n = np.asarray(n, dtype=np.float64)[:, None]
+    T = np.asarray(T, dtype=np.float64)[:, None]
+    v = grid.v[None, :]
+    f = n * fac * np.exp(-0.5 * v ** 2 / T) / np.sqrt(T)
+    f[:, :STENCIL] = 0.0
+    f[:, grid.nv - STENCIL:] = 0.0
+    return f
+
+
+def fourier_filter(f, nfourier):
+    """Keep the first ``nfourier`` packed rFFT coefficients along x
+    (run/run_base.py:467-496, scipy.fftpack real packing)."""
+    if nfourier <= 0:
+        return f
+    from scipy.fftpack import irfft, rfft
+    F = rfft(f, axis=0)
+    F[nfourier:, :] = 0.
+    return irfft(F, axis=0)
+
+
+def normalise(f, grid):
+    """Scale so that ``sum(f)*hv/nx == 1`` (run/run_base.py:623-628)."""
+    nave = f.sum() * grid.hv / grid.nx
+    return f * (1. / nave)
+
+
+# --------------------------------------------------------------------------
+# Hamiltonian assembly  (Toolbox.pyx:38-74, PETScVlasovSolver.pyx:142-157)
+# --------------------------------------------------------------------------
+def potential_to_hamiltonian(phi):
+    """x-profile of h1: ``phi_i - sum(phi)/nx`` (Toolbox.pyx:38-74)."""
+    phi = np.asarray(phi, dtype=np.float64)
+    return phi - phi.sum() / phi.size
+
+
+def have_field(h0v, h1p, h1h, h2p=None, h2h=None):
+    """``Have = H0 + .5 H1p + .5 H1h + .5 H2p + .5 H2h`` in the reference's
+    axpy order (PETScVlasovSolver.pyx:145-149).  h0v depends on v only, the
+    others on x only; the result is the (nx, nv) midpoint Hamiltonian."""
+    nx = np.asarray(h1p).size
+    z = np.zeros(nx)
+    h2p = z if h2p is None else np.asarray(h2p, dtype=np.float64)
+    h2h = z if h2h is None else np.asarray(h2h, dtype=np.float64)
+    H = np.broadcast_to(np.asarray(h0v)[None, :], (nx, np.asarray(h0v).size)).copy()
+    H = H + .5 * np.asarray(h1p)[:, None]
+    H = H + .5 * np.asarray(h1h)[:, None]
+    H = H + .5 * h2p[:, None]
+    H = H + .5 * h2h[:, None]
+    return H
+
+
+# --------------------------------------------------------------------------
+# Arakawa brackets  (solvers/components/PoissonBracket.pyx)
+# --------------------------------------------------------------------------
+def _s(a, di, dj):
+    """``a[ix+di, jx+dj]`` for every x and the interior rows 2 <= j < nv-2,
+    x periodic (the halo the DMDA fills, run_base.py:215-220)."""
+    nv = a.shape[1]
+    return np.roll(a, -di, axis=0)[:, STENCIL + dj: nv - STENCIL + dj]
+
+
+def _j1_terms(x, h):
+    """jpp + jpc + jcp of J1 (PoissonBracket.pyx:100-111 / :360-371)."""
+    jpp = (_s(x, 1, 0) - _s(x, -1, 0)) * (_s(h, 0, 1) - _s(h, 0, -1)) \
+        - (_s(x, 0, 1) - _s(x, 0, -1)) * (_s(h, 1, 0) - _s(h, -1, 0))
+    jpc = _s(x, 1, 0) * (_s(h, 1, 1) - _s(h, 1, -1)) \
+        - _s(x, -1, 0) * (_s(h, -1, 1) - _s(h, -1, -1)) \
+        - _s(x, 0, 1) * (_s(h, 1, 1) - _s(h, -1, 1)) \
+        + _s(x, 0, -1) * (_s(h, 1, -1) - _s(h, -1, -1))
+    jcp = _s(x, 1, 1) * (_s(h, 0, 1) - _s(h, 1, 0)) \
+        - _s(x, -1, -1) * (_s(h, -1, 0) - _s(h, 0, -1)) \
+        - _s(x, -1, 1) * (_s(h, 0, 1) - _s(h, -1, 0)) \
+        + _s(x, 1, -1) * (_s(h, 1, 0) - _s(h, 0, -1))
+    return jpp, jpc, jcp
+
+
+def _j2_terms(x, h):
+    """jcc + jpc + jcp of J2 (PoissonBracket.pyx:221-232 / :373-384)."""
+    jcc = (_s(x, 1, 1) - _s(x, -1, -1)) * (_s(h, -1, 1) - _s(h, 1, -1)) \
+        - (_s(x, -1, 1) - _s(x, 1, -1)) * (_s(h, 1, 1) - _s(h, -1, -1))
+    jpc = _s(x, 2, 0) * (_s(h, 1, 1) - _s(h, 1, -1)) \
+        - _s(x, -2, 0) * (_s(h, -1, 1) - _s(h, -1, -1)) \
+        - _s(x, 0, 2) * (_s(h, 1, 1) - _s(h, -1, 1)) \
+        + _s(x, 0, -2) * (_s(h, 1, -1) - _s(h, -1, -1))
+    jcp = _s(x, 1, 1) * (_s(h, 0, 2) - _s(h, 2, 0)) \
+        - _s(x, -1, -1) * (_s(h, -2, 0) - _s(h, 0, -2)) \
+        - _s(x, -1, 1) * (_s(h, 0, 2) - _s(h, -2, 0)) \
+        + _s(x, 1, -1) * (_s(h, 2, 0) - _s(h, 0, -2))
+    return jcc, jpc, jcp
+
+
+def bracket_add(x, h, y, factor, grid, scheme="arakawaj4"):
+    """``y += factor * [x, h]`` on the interior rows, in place.
+
+    J1: PoissonBracket.pyx:80-113; J2: :200-234; J4 = 2 J1 - J2: :335-389.
+    """
+    nv = grid.nv
+    interior = (slice(None), slice(STENCIL, nv - STENCIL))
+    if scheme == "arakawaj1":
+        jpp, jpc, jcp = _j1_terms(x, h)
+        arakawa_factor = grid.hx_inv * grid.hv_inv / 12.
+        y[interior] += factor * (jpp + jpc + jcp) * arakawa_factor
+    elif scheme == "arakawaj2":
+        jcc, jpc, jcp = _j2_terms(x, h)
+        arakawa_factor = grid.hx_inv * grid.hv_inv / 24.
+        y[interior] += factor * (jcc + jpc + jcp) * arakawa_factor
+    elif scheme == "arakawaj4":
+        f1 = grid.hx_inv * grid.hv_inv / 12.
+        f2 = grid.hx_inv * grid.hv_inv / 24.
+        jpp1, jpc1, jcp1 = _j1_terms(x, h)
+        jcc2, jpc2, jcp2 = _j2_terms(x, h)
+        result_J1 = (jpp1 + jpc1 + jcp1) * f1
+        result_J2 = (jcc2 + jpc2 + jcp2) * f2
+        y[interior] += factor * (2. * result_J1 - result_J2)
+    else:
+        raise ValueError("unknown bracket %r" % scheme)
+    return y
+
+
+def bracket(x, h, grid, scheme="arakawaj4", factor=1.0):
+    y = np.zeros_like(x)
+    return bracket_add(x, h, y, factor, grid, scheme)
+
+
+# --------------------------------------------------------------------------
+# residual and JVP  (solvers/vlasov/PETScNLVlasovMP.pyx:33-58,
+#                    components/TimeDerivative.pyx:56-57)
+# --------------------------------------------------------------------------
+def residual(F, Fh, Have, grid, scheme="arakawaj4"):
+    """``R(F) = (F - Fh)/ht + [ (F+Fh)/2 , Have ]`` (PETScNLVlasovMP.pyx:43-58)."""
+    Fave = 0.5 * Fh + 0.5 * F            # Fave.set(0); axpy(.5,Fh); axpy(.5,F)
+    Fder = F - Fh                        # Fder.set(0); axpy(+1,F); axpy(-1,Fh)
+    Y = grid.ht_inv * Fder               # TimeDerivative.function: Y.axpy(ht_inv, F)
+    bracket_add(Fave, Have, Y, 1.0, grid, scheme)
+    return Y
+
+
+def jvp(X, Have, grid, scheme="arakawaj4"):
+    """``J X = X/ht + 0.5 [X, Have]`` (PETScNLVlasovMP.pyx:33-40)."""
+    Y = grid.ht_inv * X
+    bracket_add(X, Have, Y, 0.5, grid, scheme)
+    return Y
+
+
+# --------------------------------------------------------------------------
+# FFT tensor-product kinetic preconditioner
+#   (preconditioner/TensorProduct.pyx:109-116,
+#    TensorProductKinetic.pyx:345-359,
+#    TensorProductKineticFast.pyx:43-93, 102-224, 248-272)
+# --------------------------------------------------------------------------
+def compute_eigenvalues(n):
+    """TensorProduct.pyx:109-116, including the ifftshift."""
+    eigen = np.empty(n, dtype=np.complex128)
+    for i in range(n):
+        eigen[i] = np.exp(2.j * np.pi * float(i) / n * (n - 1)) \
+            - np.exp(2.j * np.pi * float(i) / n)
+    return np.fft.ifftshift(eigen)
+
+
+def banded_matrix(grid, eigen):
+    """LAPACK band storage (LDAB=4, KL=KU=1) of the v-tridiagonal matrix for
+    one x mode (TensorProductKineticFast.pyx:248-272)."""
+    nv = grid.nv
+    arak_fac_J1 = 0.5 * grid.hx_inv * grid.hv_inv / 12.
+    v = grid.v
+    diagm = eigen * 0.5 * (2. * grid.hv * v - grid.hv2) * arak_fac_J1
+    diag = eigen * 1.0 * (4. * grid.hv * v) * arak_fac_J1 + grid.ht_inv
+    diagp = eigen * 0.5 * (2. * grid.hv * v + grid.hv2) * arak_fac_J1
+    m = np.zeros((4, nv), dtype=np.complex128, order="F")
+    m[1, 1:] = diagp[:-1]
+    m[2, :] = diag[:]
+    m[3, :-1] = diagm[1:]
+    return m
+
+
+class TensorKineticPreconditioner:
+    """``P^-1``: rFFT along x per v row -> banded solve in v per x mode ->
+    normalised irFFT (TensorProductKinetic.pyx:345-359)."""
+
+    def __init__(self, grid):
+        self.grid = grid
+        nxh = grid.nx // 2 + 1
+        self.eigen = compute_eigenvalues(grid.nx)
+        self.lu = []
+        self.piv = []
+        self.raw = []
+        for k in range(nxh):  # TensorProductKineticFast.pyx:81-90
+            m = banded_matrix(grid, self.eigen[k])
+            self.raw.append(m.copy())
+            lu, piv, info = lapack.zgbtrf(m, 1, 1)
+            if info != 0:
+                raise RuntimeError("zgbtrf failed for mode %d (info=%d)" % (k, info))
+            self.lu.append(lu)
+            self.piv.append(piv)
+
+    def pivoted(self):
+        """True when LAPACK's partial pivoting swapped any row."""
+        return any(np.any(p != np.arange(p.size)) for p in self.piv)
+
+    def apply(self, X):
+        """``Y = P^-1 X`` for an (nx, nv) field (TensorProductKineticFast.pyx:102-224)."""
+        rows = to_flat(X)                        # (nv, nx): one row per v (dax layout)
+        spec = np.fft.rfft(rows, axis=1)         # fft(): FFTW r2c per row
+        B = np.ascontiguousarray(spec.T)         # cax -> cay transpose: B[k, j]
+        for k in range(B.shape[0]):             # solve(): zgbtrs per mode
+            x, info = lapack.zgbtrs(self.lu[k], 1, 1, B[k], self.piv[k])
+            if info != 0:
+                raise RuntimeError("zgbtrs failed")
+            B[k] = x
+        rows = np.fft.irfft(B.T, n=self.grid.nx, axis=1)  # ifft(): c2r, normalised 1/nx
+        return from_flat(rows).copy()
+
+
+# --------------------------------------------------------------------------
+# moments  (toolbox/Toolbox.pyx:79-165)
+# --------------------------------------------------------------------------
+def moments(f, grid):
+    """Density, velocity density, energy density and collision factor."""
+    n = f.sum(axis=1) * grid.hv
+    u = (f * grid.v[None, :]).sum(axis=1) * grid.hv
+    e = (f * grid.v2[None, :]).sum(axis=1) * grid.hv
+    with np.errstate(divide="ignore", invalid="ignore"):
+        a = n * n / (n * e - u * u)
+    return n, u, e, a
+
+
+# --------------------------------------------------------------------------
+# Poisson, CFD4  (solvers/poisson/PETScPoissonSolver.pyx:58-74,
+#                 PETScPoissonCFD4.pyx:111-183,
+#                 run/run_nonlinear_matrixfree_split_mp.py:56-80)
+# --------------------------------------------------------------------------
+def poisson_rhs(n, charge):
+    """``b = -(n - mean n) * charge`` (PETScPoissonSolver.pyx:58-74)."""
+    nmean = n.sum() / n.size
+    return -(n - nmean) * charge
+
+
+def poisson_matvec(x, hx2_inv):
+    """CFD4 ``(5,-32,54,-32,5)/(12 hx^2)`` periodic (PETScPoissonCFD4.pyx:146-160)."""
+    r = np.roll
+    return (5. * r(x, 2) - 32. * r(x, 1) + 54. * x - 32. * r(x, -1) + 5. * r(x, -2)) * hx2_inv / 12.
+
+
+def poisson_function(x, n, hx2_inv, charge):
+    """Poisson residual ``A x + (n - mean n) * charge`` (PETScPoissonCFD4.pyx:163-183)."""
+    nmean = n.sum() / n.size
+    return poisson_matvec(x, hx2_inv) + (n - nmean) * charge
+
+
+def poisson_solve(n, grid, charge):
+    """Solve ``A phi = b`` on the mean-free subspace.
+
+    The reference solves the singular periodic system with PETSc CG (rtol
+    1e-13) and the constant null space attached; the oracle uses the exact
+    circulant inverse, whose result is mean-free.  The mean of phi never
+    enters the dynamics (h1 subtracts it, Toolbox.pyx:50-56)."""
+    b = poisson_rhs(n, charge)
+    nx = grid.nx
+    th = 2. * np.pi * np.arange(nx // 2 + 1) / nx
+    sym = (54. - 64. * np.cos(th) + 10. * np.cos(2. * th)) * grid.hx2_inv / 12.
+    bh = np.fft.rfft(b)
+    ph = np.zeros_like(bh)
+    ph[1:] = bh[1:] / sym[1:]
+    return np.fft.irfft(ph, n=nx)
+
+
+# --------------------------------------------------------------------------
+# GMRES, restating PETSc's KSPGMRES with its defaults
+# --------------------------------------------------------------------------
+@dataclass
+class KSPResult:
+    x: np.ndarray
+    its: int
+    reason: int
+    rnorm: float
+    history: list = field(default_factory=list)
+
+
+def gmres(apply_A, b, rtol=1e-5, atol=1e-50, max_it=10000, restart=30,
+          dtol=1e5, haptol=1e-30):
+    """Restarted GMRES as PETSc runs it for ``KSPSetType('gmres')``, ``PC none``,
+    zero initial guess (SNES ksponly, run_nonlinear_matrixfree_split_mp.py:47-53).
+
+    Algorithm (PETSc KSPSolve_GMRES / KSPGMRESCycle /
+    KSPGMRESClassicalGramSchmidtOrthogonalization / KSPGMRESUpdateHessenberg /
+    KSPGMRESBuildSoln / KSPConvergedDefault, as documented by PETSc):
+      * cycle start: r = b - A x (r = b for the zero guess), res = ||r||,
+        v0 = r * (1/res), convergence test with n = its;
+      * Arnoldi step: w = A v_it; h_j = <w, v_j> (one multi-dot); w -= sum h_j v_j
+        (one multi-axpy); tt = ||w||; v_{it+1} = w * (1/tt);
+      * Givens rotation update; res = |g_{it+1}|; its += 1; convergence test;
+      * happy breakdown when tt < min(|tt/g_it|, haptol);
+      * KSPConvergedDefault: at n == 0, rnorm0 = res and
+        ttol = max(rtol*rnorm0, atol); converged if res <= ttol;
+        diverged if res >= dtol*rnorm0; NaN -> diverged;
+      * the solution update is formed by back substitution after each cycle.
+    """
+    b = np.asarray(b, dtype=np.float64).ravel()
+    x = np.zeros_like(b)
+    its = 0
+    reason = KSP_CONVERGED_ITERATING
+    state = {"rnorm0": None, "ttol": None}
+    history = []
+    guess_zero = True
+    res = 0.0
+
+    def converged(n, rnorm):
+        if n == 0:
+            state["rnorm0"] = rnorm
+            state["ttol"] = max(rtol * rnorm, atol)
+        if not np.isfinite(rnorm):
+            return KSP_DIVERGED_NANORINF
+        if rnorm <= state["ttol"]:
+            return KSP_CONVERGED_ATOL if rnorm < atol else KSP_CONVERGED_RTOL
+        if rnorm >= dtol * state["rnorm0"]:
+            return KSP_DIVERGED_DTOL
+        return KSP_CONVERGED_ITERATING
+
+    while reason == KSP_CONVERGED_ITERATING:
+        r = b.copy() if guess_zero else b - apply_A(x)
+        res_norm = float(np.sqrt(np.dot(r, r)))
+        V = [r * (1. / res_norm) if res_norm != 0. else r]
+        hh = np.zeros((restart + 2, restart + 1))
+        grs = np.zeros(restart + 2)
+        cc = np.zeros(restart + 1)
+        ss = np.zeros(restart + 1)
+        grs[0] = res_norm
+        res = res_norm
+        history.append(res)
+        if res == 0.:
+            reason = KSP_CONVERGED_ATOL
+            break
+        reason = converged(its, res)
+        it = 0
+        while reason == KSP_CONVERGED_ITERATING and it < restart and its < max_it:
+            w = apply_A(V[it]).ravel().astype(np.float64)
+            lhh = np.array([np.dot(w, V[j]) for j in range(it + 1)])
+            lhh = -lhh
+            for j in range(it + 1):
+                w = w + lhh[j] * V[j]
+            hh[:it + 1, it] = -lhh
+            tt = float(np.sqrt(np.dot(w, w)))
+            if tt != 0.:
+                w = w * (1. / tt)
+            V.append(w)
+            hh[it + 1, it] = tt
+            hapbnd = abs(tt / grs[it])
+            if hapbnd > haptol:
+                hapbnd = haptol
+            hapend = tt < hapbnd
+            for j in range(1, it + 1):
+                t = hh[j - 1, it]
+                hh[j - 1, it] = cc[j - 1] * t + ss[j - 1] * hh[j, it]
+                hh[j, it] = cc[j - 1] * hh[j, it] - ss[j - 1] * t
+            null = False
+            if not hapend:
+                t = math.sqrt(hh[it, it] * hh[it, it] + hh[it + 1, it] * hh[it + 1, it])
+                if t == 0.:
+                    reason = KSP_DIVERGED_NULL
+                    null = True
+                else:
+                    cc[it] = hh[it, it] / t
+                    ss[it] = hh[it + 1, it] / t
+                    grs[it + 1] = -(ss[it] * grs[it])
+                    grs[it] = cc[it] * grs[it]
+                    hh[it, it] = cc[it] * hh[it, it] + ss[it] * hh[it + 1, it]
+                    res = abs(grs[it + 1])
+            else:
+                res = 0.
+            it += 1
+            its += 1
+            history.append(res)
+            if null:
+                break
+            reason = converged(its, res)
+            if hapend and reason == KSP_CONVERGED_ITERATING:
+                reason = KSP_DIVERGED_BREAKDOWN
+                break
+        # KSPGMRESBuildSoln(it-1)
+        k_last = it - 1
+        if k_last >= 0:
+            if hh[k_last, k_last] == 0.:
+                reason = KSP_DIVERGED_BREAKDOWN
+            else:
+                nrs = np.zeros(k_last + 1)
+                nrs[k_last] = grs[k_last] / hh[k_last, k_last]
+                ok = True
+                for ii in range(1, k_last + 1):
+                    k = k_last - ii
+                    t = grs[k]
+                    for j in range(k + 1, k_last + 1):
+                        t = t - hh[k, j] * nrs[j]
+                    if hh[k, k] == 0.:
+                        reason = KSP_DIVERGED_BREAKDOWN
+                        ok = False
+                        break
+                    nrs[k] = t / hh[k, k]
+                if ok:
+                    temp = np.zeros_like(x)
+                    for j in range(k_last + 1):
+                        temp = temp + nrs[j] * V[j]
+                    x = x + temp
+        if its >= max_it:
+            if reason == KSP_CONVERGED_ITERATING:
+                reason = KSP_DIVERGED_ITS
+            break
+        guess_zero = False
+    return KSPResult(x=x, its=its, reason=reason, rnorm=res, history=history)
+
+
+# --------------------------------------------------------------------------
+# the Vlasov solver  (solvers/vlasov/PETScVlasovSolver.pyx, PETScNLVlasovMP.pyx)
+# --------------------------------------------------------------------------
+class VlasovSolver:
+    """Restates ``PETScVlasovSolver`` for the nonlinear midpoint scheme."""
+
+    def __init__(self, grid, h0v, scheme="arakawaj4", preconditioner="tensor_kinetic"):
+        self.grid = grid
+        self.h0v = np.asarray(h0v, dtype=np.float64)
+        self.scheme = scheme
+        self.pc = TensorKineticPreconditioner(grid) if preconditioner == "tensor_kinetic" else None
+        self.Fh = None
+        self.Have = None
+
+    def update_history(self, F):           # PETScVlasovSolver.pyx:135-140
+        self.Fh = F.copy()
+
+    def update_previous(self, h1p, h1h, h2p=None, h2h=None):  # :142-157
+        self.Have = have_field(self.h0v, h1p, h1h, h2p, h2h)
+
+    def function_solver(self, F):          # PETScNLVlasovMP.pyx:43-58
+        return residual(F, self.Fh, self.Have, self.grid, self.scheme)
+
+    def jacobian_solver(self, F):          # PETScNLVlasovMP.pyx:33-40
+        return jvp(F, self.Have, self.grid, self.scheme)
+
+    def function(self, F):                 # PETScVlasovSolver.pyx:168-174
+        Y = self.function_solver(F)
+        return self.pc.apply(Y) if self.pc is not None else Y
+
+    def jacobian(self, F):                 # PETScVlasovSolver.pyx:160-166
+        Y = self.jacobian_solver(F)
+        return self.pc.apply(Y) if self.pc is not None else Y
+
+    def function_norm(self, F):            # PETScVlasovSolver.pyx:196-198
+        Y = self.function_solver(F)
+        return float(np.sqrt(np.sum(Y * Y)))
+
+
+# --------------------------------------------------------------------------
+# the time loop  (run/run_nonlinear_matrixfree_split_mp.py:111-174,
+#                 run/run_base.py:631-655, 749-763)
+# --------------------------------------------------------------------------
+@dataclass
+class StepReport:
+    picard_its: int = 0
+    gmres_its: list = field(default_factory=list)
+    ksp_reasons: list = field(default_factory=list)
+    residuals: list = field(default_factory=list)
+    reverted: bool = False
+    stop_rule: str = ""
+    aborted: bool = False
+
+
+class Run:
+    """State of one run: f, phi, h1 and moments, current and history."""
+
+    def __init__(self, grid, f0, scheme="arakawaj4", preconditioner="tensor_kinetic",
+                 charge=-1.0, mass=1.0, ksp_rtol=1e-4, ksp_atol=1e-50,
+                 ksp_max_it=1000, snes_atol=1e-10, snes_max_iter=20,
+                 normalise_f=True):
+        self.grid = grid
+        self.charge = charge
+        self.mass = mass
+        self.ksp = dict(rtol=ksp_rtol, atol=ksp_atol, max_it=ksp_max_it)
+        self.snes_atol = snes_atol
+        self.snes_max_iter = snes_max_iter
+        self.h0v = kinetic_hamiltonian_v(grid, mass)
+        self.solver = VlasovSolver(grid, self.h0v, scheme, preconditioner)
+        f = np.asarray(f0, dtype=np.float64)
+        self.fc = normalise(f, grid) if normalise_f else f.copy()
+        self.h2c = np.zeros(grid.nx)
+        self.h2h = np.zeros(grid.nx)
+        self.calculate_moments()
+        self.fh = self.fc.copy()
+        self.h1h = self.h1c.copy()
+        self.reports = []
+
+    def calculate_moments(self):           # run_base.py:640-655
+        self.n, self.u, self.e, self.a = moments(self.fc, self.grid)
+        self.phi = poisson_solve(self.n, self.grid, self.charge)
+        self.h1c = potential_to_hamiltonian(self.phi)
+
+    def calculate_residual(self):          # run_base.py:631-637
+        fnorm = self.solver.function_norm(self.fc)
+        pb = poisson_function(self.phi, self.n, self.grid.hx2_inv, self.charge)
+        return fnorm + float(np.sqrt(np.dot(pb, pb)))
+
+    def make_history(self):                # run_base.py:749-763
+        self.fh = self.fc.copy()
+        self.h1h = self.h1c.copy()
+        self.h2h = self.h2c.copy()
+        self.solver.update_history(self.fc)
+
+    def update_previous(self):
+        self.solver.update_previous(self.h1c, self.h1h, self.h2c, self.h2h)
+
+    def snes_ksponly(self, rep):
+        """One SNES ksponly solve: ``fc <- fc - (P^-1 J)^-1 P^-1 R(fc)``.
+
+        PETSc's SNESSolve_KSPONLY skips the update when the linear solve
+        reports a negative reason (SNESCheckKSPSolve, one allowed failure)."""
+        g = self.grid
+        b = self.solver.function(self.fc)
+
+        def A(vflat):
+            return to_flat(self.solver.jacobian(from_flat(vflat, g.nx, g.nv))).ravel()
+
+        res = gmres(A, to_flat(b).ravel(), **self.ksp)
+        rep.gmres_its.append(res.its)
+        rep.ksp_reasons.append(res.reason)
+        if res.reason >= 0:
+            self.fc = self.fc - from_flat(res.x, g.nx, g.nv)
+
+    def step(self):
+        """One time step (run_nonlinear_matrixfree_split_mp.py:111-174)."""
+        rep = StepReport()
+        self.make_history()
+        self.update_previous()
+        pred_norm = self.calculate_residual()
+        rep.residuals.append(pred_norm)
+        i = 0
+        while True:
+            i += 1
+            fl = self.fc.copy()
+            self.snes_ksponly(rep)
+            self.calculate_moments()
+            self.update_previous()
+            prev_norm = pred_norm
+            pred_norm = self.calculate_residual()
+            rep.residuals.append(pred_norm)
+            rose = pred_norm > prev_norm and i > 1
+            small = pred_norm < self.snes_atol
+            maxed = i >= self.snes_max_iter
+            if rose or small or maxed:
+                rep.stop_rule = "rose" if rose else ("atol" if small else "max_iter")
+                if pred_norm > prev_norm:
+                    self.fc = fl
+                    self.calculate_moments()
+                    rep.reverted = True
+                break
+        rep.picard_its = i
+        if pred_norm > 10.:
+            rep.aborted = True
+        self.reports.append(rep)
+        return rep
+
+
+# --------------------------------------------------------------------------
+# invariants  (core/distribution_function.pyx:130-306, core/hamiltonian.pyx:67-124,
+#              core/potential.pyx:48-59)
+# --------------------------------------------------------------------------
+def invariants(f, phi_or_h1, grid, charge=-1.0, mass=1.0, h2=None):
+    """Every invariant the reference's offline diagnostics compute, for one
+    time level.  ``phi_or_h1`` is the internal potential (x profile); h1 is
+    its mean-free part, as stored in the HDF5 file (Toolbox.pyx:38-74)."""
+    nx, nv = grid.nx, grid.nv
+    hxhv = grid.hx * grid.hv
+    phi = np.asarray(phi_or_h1, dtype=np.float64)
+    h1x = potential_to_hamiltonian(phi)
+    h2x = np.zeros(nx) if h2 is None else np.asarray(h2, dtype=np.float64)
+    fi = f[:, :nv - 1]
+    fp = np.roll(f, -1, axis=0)
+    # distribution_function.pyx:147-157
+    N = (f[:, :nv - 1] + fp[:, :nv - 1] + fp[:, 1:] + f[:, 1:]).sum() * 0.25 * grid.hx * grid.hv
+    out = {"mass": N}
+    for p in (1, 2, 3, 4, 5, 6, 8):   # distribution_function.pyx:186-204
+        out["L%d" % p] = hxhv * (np.abs(fi).sum() if p == 1 else np.power(fi, p).sum())
+    out["Lmin"] = f.min() * hxhv
+    out["Lmax"] = f.max() * hxhv
+    fe = f.copy()                      # distribution_function.pyx:291-306
+    fe[fe <= 0.] = 1e-15
+    out["entropy"] = -grid.hx * grid.hv * (fe[:, :nv - 1] * np.log(fe[:, :nv - 1])).sum()
+    h0 = kinetic_hamiltonian_v(grid, mass)  # hamiltonian.pyx:85-100
+    ekin = (f * h0[None, :]).sum() * grid.hx * grid.hv
+    epot = ((f * h1x[:, None]).sum() + (f * h2x[:, None]).sum()) * grid.hx * grid.hv
+    out["E_kin"] = ekin
+    out["E_pot"] = epot
+    out["energy"] = ekin + 0.5 * epot
+    out["momentum"] = (fi * grid.v[None, :nv - 1]).sum() * mass * grid.hx * grid.hv  # :119-124
+    d = np.roll(phi, -1) - phi          # potential.pyx:54-59
+    out["field_energy"] = 0.5 * charge * (d * d).sum() / grid.hx
+    return out
+
+
+# --------------------------------------------------------------------------
+# named initial conditions used by the workloads
+# --------------------------------------------------------------------------
+def maxwellian(v, T=1.0, vshift=0.0):
+    """toolbox/maxwell.py:22-23 with toolbox/boltzmann.py:20-21."""
+    return math.sqrt(0.5 / np.pi) * np.exp(-0.5 * (v + vshift) ** 2 / T) / np.sqrt(T)
+
+
+def f0_landau(amp=0.01, k=0.5):
+    return lambda x, v: (1. + amp * np.cos(k * x)) * np.exp(-v ** 2 / 2.) / np.sqrt(2. * np.pi)
+
+
+def f0_twostream(amp=0.05, k=0.5):
+    return lambda x, v: v ** 2 * np.exp(-v ** 2 / 2.) / np.sqrt(2. * np.pi) * (1. + amp * np.cos(k * x))
+
+
+def f0_bump_on_tail(amp=0.04, k=0.3):
+    return lambda x, v: (0.9 * np.exp(-v ** 2 / 2.) + 0.2 * np.exp(-(v - 4.5) ** 2 / (2. * 0.25))) \
+        / np.sqrt(2. * np.pi) * (1. + amp * np.cos(k * x))
