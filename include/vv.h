@@ -1,0 +1,235 @@
+/*
+ * vv.h -- C ABI of libvv, a B200 (sm_100a) implementation of viVlasov1D's
+ * implicit variational (midpoint) time step for the 1D1V Vlasov-Poisson
+ * system: Arakawa J1/J2/J4 bracket residual and Jacobian-vector product,
+ * FFT tensor-product kinetic preconditioner, periodic CFD4 Poisson solve,
+ * moments, restarted GMRES and the Picard-over-phi step, and the invariant
+ * diagnostics.
+ *
+ * Conventions
+ *   - Every entry point returns an int status (VV_OK == 0).  No call aborts
+ *     the process and no device wait in the library is unbounded.
+ *   - Field buffers are DEVICE pointers to nx*nv doubles in the reference's
+ *     PETSc natural ordering: F[j*nx + i], x (i, periodic) fastest, v (j,
+ *     bounded) slowest -- the layout of the DMDA ``da1`` global vector
+ *     (vlasov/run/run_base.py:215-220).  x profiles (phi, h1, h2, n, u, e, a)
+ *     are device pointers to nx doubles.
+ *   - Work is enqueued on the stream set with vv_set_stream (default: the
+ *     legacy default stream).  Calls that return a host scalar synchronise
+ *     that stream.
+ *   - The Hamiltonian is never stored as an nx*nv array: h = h0(v) + h1(x)
+ *     (+ h2(x)) is separable, so the solver keeps the 1-D profiles and the
+ *     kernels regenerate h on the fly.
+ *
+ * Every function names the reference interface it replaces (file:line,
+ * relative to the viVlasov1D project root).
+ */
+#ifndef VIVLASOV1D_B200_VV_H
+#define VIVLASOV1D_B200_VV_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ------------------------------------------------------ */
+enum vv_status {
+    VV_OK = 0,
+    VV_ERR_ARG = 1,          /* invalid argument or NULL pointer             */
+    VV_ERR_UNSUPPORTED = 2,  /* configuration not supported by this build    */
+    VV_ERR_CUDA = 3,         /* a CUDA runtime call failed                   */
+    VV_ERR_ALLOC = 4,        /* device allocation failed                     */
+    VV_ERR_DIVERGED = 5,     /* Picard residual above the abort threshold    */
+    VV_ERR_NAN = 6,          /* NaN/Inf met in a norm                        */
+    VV_ERR_TIMEOUT = 7       /* a bounded device wait gave up                */
+};
+
+/* ---- discretisation choices (vlasov/core/config.py:63-126) ------------- */
+enum vv_bracket {            /* solver.poisson_bracket                        */
+    VV_BRACKET_J1 = 1,       /* PoissonBracket.pyx:68-186                      */
+    VV_BRACKET_J2 = 2,       /* PoissonBracket.pyx:188-306                     */
+    VV_BRACKET_J4 = 4        /* PoissonBracket.pyx:309-403 (default)           */
+};
+enum vv_preconditioner {     /* solver.preconditioner_scheme                  */
+    VV_PC_NONE = 0,
+    VV_PC_TENSOR_KINETIC = 1 /* TensorProductKineticFast.pyx                   */
+};
+enum vv_laplace {            /* solver.laplace_operator                       */
+    VV_LAPLACE_CFD4 = 4      /* PETScPoissonCFD4.pyx (default)                 */
+};
+enum vv_order {              /* arithmetic of the bracket kernels             */
+    VV_ORDER_FACTORED = 0,   /* separable-h coefficient form (fast, default)   */
+    VV_ORDER_REFERENCE = 1   /* the reference loop's operation order, no FMA   */
+};
+
+/* ---- grid and run parameters (runspec.cfg [grid], [initial_data]) ------- */
+typedef struct vv_grid {
+    int32_t nx;              /* points in x (periodic)                        */
+    int32_t nv;              /* points in v (bounded), nv >= 5                */
+    double  L;               /* x length; hx = L/nx                           */
+    double  vmin, vmax;      /* hv = (vmax-vmin)/(nv-1)                       */
+    double  ht;              /* time step                                     */
+    double  charge;          /* particle charge (examples use -1)             */
+    double  mass;            /* particle mass                                 */
+    int32_t bracket;         /* enum vv_bracket                               */
+    int32_t preconditioner;  /* enum vv_preconditioner                        */
+    int32_t laplace;         /* enum vv_laplace                               */
+    int32_t order;           /* enum vv_order                                 */
+    int32_t gmres_restart;   /* restart length (PETSc default 30), <= 64      */
+    int32_t reserved;
+} vv_grid;
+
+typedef struct vv_ctx vv_ctx;
+
+/* ---- lifetime ----------------------------------------------------------- */
+/* Allocate a solver for one grid: the GMRES basis, spectra, reduction
+ * scratch and the preconditioner's factorised band matrices.  Replaces the
+ * construction of PETScVlasovSolver (PETScVlasovSolver.pyx:27-104) together
+ * with TensorProductPreconditionerKineticFast (TensorProductKineticFast.pyx:
+ * 25-93: eigenvalues, band matrices, one LU factorisation per x mode). */
+int vv_create(const vv_grid* grid, vv_ctx** out);
+int vv_destroy(vv_ctx* ctx);
+int vv_set_stream(vv_ctx* ctx, void* cuda_stream);
+const char* vv_status_string(int status);
+int vv_version(void);
+/* Velocity grid v_j and the kinetic Hamiltonian profile h0_j = 0.5 v_j^2 m
+ * (Toolbox.pyx:175-187) copied to host arrays of nv doubles. */
+int vv_grid_vectors(vv_ctx* ctx, double* v_host, double* h0_host);
+
+/* ---- PETScVlasovSolver interface ---------------------------------------- */
+/* update_history(F): Fh <- F                   PETScVlasovSolver.pyx:135-140 */
+int vv_update_history(vv_ctx* ctx, const double* F);
+/* update_previous: Have <- H0 + .5 H1p + .5 H1h + .5 H2p + .5 H2h
+ * (PETScVlasovSolver.pyx:142-157).  Arguments are x profiles of h1/h2 at the
+ * current Picard iterate (p) and the previous time level (h); NULL means
+ * zero.  The profiles are copied (a snapshot, as the reference's Have). */
+int vv_update_previous(vv_ctx* ctx, const double* h1p, const double* h1h,
+                       const double* h2p, const double* h2h);
+/* function(F, Y) / function_solver: Y = P^-1 R(F) or R(F) with
+ * R(F) = (F - Fh)/ht + [ (F+Fh)/2, Have ]   PETScVlasovSolver.pyx:168-174,
+ * PETScNLVlasovMP.pyx:43-58 */
+int vv_function(vv_ctx* ctx, const double* F, double* Y, int apply_pc);
+/* jacobian(F, Y) / jacobian_solver: Y = P^-1 J F or J F with
+ * J F = F/ht + 0.5 [F, Have]      PETScVlasovSolver.pyx:160-166, 176-186,
+ * PETScNLVlasovMP.pyx:33-40 (also mult/snes_mult/jacobian_mult) */
+int vv_jacobian(vv_ctx* ctx, const double* F, double* Y, int apply_pc);
+/* function_norm(F, Y): Y = R(F), *norm = ||Y||_2 (host scalar)
+ *                                           PETScVlasovSolver.pyx:196-198 */
+int vv_function_norm(vv_ctx* ctx, const double* F, double* Y, double* norm);
+/* PoissonBracket.function: Y += factor * [X, Have] on rows 2 <= j < nv-2
+ *                                   PoissonBracket.pyx:70-75, 325-330 */
+int vv_bracket(vv_ctx* ctx, const double* X, double* Y, double factor);
+
+/* ---- TensorProductPreconditioner ---------------------------------------- */
+/* tensorProduct(X, Y): Y = P^-1 X     TensorProductKinetic.pyx:345-359,
+ * TensorProductKineticFast.pyx:102-224.  X and Y may alias. */
+int vv_pc_apply(vv_ctx* ctx, const double* X, double* Y);
+
+/* ---- Toolbox ------------------------------------------------------------ */
+/* compute_density / compute_velocity_density / compute_energy_density /
+ * compute_collision_factor (Toolbox.pyx:79-165).  Any output may be NULL. */
+int vv_moments(vv_ctx* ctx, const double* F, double* n, double* u, double* e, double* a);
+/* potential_to_hamiltonian: h1_i = phi_i - sum(phi)/nx   Toolbox.pyx:38-74 */
+int vv_potential_to_hamiltonian(vv_ctx* ctx, const double* phi, double* h1);
+
+/* ---- PETScPoissonSolver (CFD4) ------------------------------------------ */
+/* formRHS: b = -(n - mean n)*charge             PETScPoissonSolver.pyx:58-74 */
+int vv_poisson_rhs(vv_ctx* ctx, const double* n, double* b);
+/* matrix_mult: y = (5,-32,54,-32,5) x / (12 hx^2)  PETScPoissonCFD4.pyx:146-160 */
+int vv_poisson_matvec(vv_ctx* ctx, const double* x, double* y);
+/* function_mult: y = A x + (n - mean n)*charge    PETScPoissonCFD4.pyx:163-183 */
+int vv_poisson_function(vv_ctx* ctx, const double* x, const double* n, double* y);
+/* the KSP solve of A phi = b(n) on the mean-free subspace
+ * (run/run_base.py:658-704, run_nonlinear_matrixfree_split_mp.py:56-80);
+ * exact spectral inverse, phi has zero mean. */
+int vv_poisson_solve(vv_ctx* ctx, const double* n, double* phi);
+
+/* ---- GMRES (PETSc KSPGMRES as configured at
+ *      run_nonlinear_matrixfree_split_mp.py:47-53, run_base.py:189-191) ---- */
+typedef struct vv_ksp_opts {
+    double  rtol;            /* petsc_ksp_rtol  (runspec default 1e-4)        */
+    double  atol;            /* petsc_ksp_atol  (1e-50)                       */
+    double  dtol;            /* divergence tolerance (PETSc default 1e5)      */
+    int32_t max_it;          /* petsc_ksp_max_iter (1000)                     */
+    int32_t restart;         /* 0 -> the context's gmres_restart              */
+} vv_ksp_opts;
+typedef struct vv_ksp_result {
+    int32_t its;             /* KSPGetIterationNumber                         */
+    int32_t reason;          /* KSPConvergedReason (PETSc numbering)          */
+    double  rnorm;           /* last residual estimate                        */
+} vv_ksp_result;
+/* Solve (P^-1 J) x = b with zero initial guess; x and b are device fields. */
+int vv_gmres(vv_ctx* ctx, const double* b, double* x, const vv_ksp_opts* opts,
+             vv_ksp_result* result);
+
+/* ---- the time step (run_nonlinear_matrixfree_split_mp.py:111-174) ------- */
+typedef struct vv_state {    /* caller-owned device buffers                   */
+    double* f;               /* nx*nv current distribution function (fc)    */
+    double* fh;              /* nx*nv previous time level (fh)               */
+    double* phi;             /* nx internal potential, current (pc_int)      */
+    double* phih;            /* nx internal potential, previous (ph_int)     */
+    double* h1c;             /* nx h1 profile, current                       */
+    double* h1h;             /* nx h1 profile, previous                      */
+    double* h2c;             /* nx external h2 profile, current (or NULL)    */
+    double* h2h;             /* nx external h2 profile, previous (or NULL)   */
+    double* n;               /* nx density of f (self.N)                     */
+    double* u;               /* nx velocity density                          */
+    double* e;               /* nx energy density                            */
+    double* a;               /* nx collision factor                          */
+} vv_state;
+typedef struct vv_snes_opts {
+    double  atol;            /* petsc_snes_atol: stop when residual < atol   */
+    int32_t max_iter;        /* petsc_snes_max_iter                           */
+    int32_t reserved;
+    double  abort_residual;  /* abort threshold (reference: 10.)             */
+} vv_snes_opts;
+#define VV_MAX_PICARD 64
+typedef struct vv_step_report {
+    int32_t picard_its;      /* Picard (outer) iterations                    */
+    int32_t gmres_its_total; /* sum of GMRES iterations                      */
+    int32_t reverted;        /* 1 if the last iterate was rejected           */
+    int32_t stop_rule;       /* 1 residual rose, 2 below atol, 3 max_iter    */
+    int32_t ksp_failures;    /* linear solves with a negative reason         */
+    int32_t aborted;         /* 1 if residual > abort threshold              */
+    int32_t gmres_its[VV_MAX_PICARD];
+    int32_t ksp_reason[VV_MAX_PICARD];
+    double  residual[VV_MAX_PICARD + 1]; /* residual before/after each pass  */
+} vv_step_report;
+/* Initial set-up of a run: optionally normalise f so that sum(f)*hv/nx == 1
+ * (run_base.py:623-628), then moments, Poisson and h1 (run_base.py:506). */
+int vv_run_init(vv_ctx* ctx, vv_state* st, int normalise);
+/* calculate_moments: moments of st->f, Poisson, h1c (run_base.py:640-655). */
+int vv_calculate_moments(vv_ctx* ctx, vv_state* st);
+/* calculate_residual: ||R(f)||_2 + ||Poisson residual||_2 (run_base.py:631-637). */
+int vv_calculate_residual(vv_ctx* ctx, vv_state* st, double* residual);
+/* One implicit time step: make_history, update_previous, Picard loop with
+ * one ksponly GMRES solve per pass, revert/stop/abort rules. */
+int vv_step(vv_ctx* ctx, vv_state* st, const vv_snes_opts* snes,
+            const vv_ksp_opts* ksp, vv_step_report* report);
+
+/* ---- invariants (vlasov/core/distribution_function.pyx:130-306,
+ *      hamiltonian.pyx:67-124, potential.pyx:48-59) ---------------------- */
+typedef struct vv_invariant_set {
+    double mass, L1, L2, L3, L4, L5, L6, L8, Lmin, Lmax, entropy;
+    double E_kin, E_pot, energy, momentum, field_energy;
+} vv_invariant_set;
+/* phi: internal potential (nx); h2: external profile or NULL.  Sums are
+ * compensated FP64. */
+int vv_invariants(vv_ctx* ctx, const double* f, const double* phi, const double* h2,
+                  vv_invariant_set* out);
+
+/* ---- timing of the dominant kernel (measurement support) --------------- */
+/* When enabled, the library records CUDA events around every launch of the
+ * Jacobian-vector-product stencil kernel on its stream; vv_timing_read
+ * returns the number of launches and their summed device time (ms). */
+int vv_timing_enable(vv_ctx* ctx, int enable);
+int vv_timing_read(vv_ctx* ctx, int64_t* launches, double* total_ms, int reset);
+/* Number of kernels the library has launched since the last reset. */
+int vv_launch_count(vv_ctx* ctx, int64_t* launches, int reset);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* VIVLASOV1D_B200_VV_H */

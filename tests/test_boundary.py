@@ -1,0 +1,87 @@
+"""The C ABI library loads and exports every symbol include/vv.h declares;
+the host-side configuration reader follows the reference's defaults.  CPU only:
+no compute call is made."""
+import ctypes as C
+import os
+import re
+
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def declared_symbols():
+    txt = open(os.path.join(ROOT, "include", "vv.h")).read()
+    txt = re.sub(r"/\*.*?\*/", "", txt, flags=re.S)
+    return sorted(set(re.findall(r"^\s*(?:int|const char\*)\s+(vv_\w+)\s*\(", txt, flags=re.M)))
+
+
+def test_header_declares_entry_points():
+    syms = declared_symbols()
+    for s in ("vv_create", "vv_destroy", "vv_function", "vv_jacobian", "vv_pc_apply", "vv_gmres",
+              "vv_step", "vv_invariants", "vv_moments", "vv_poisson_solve"):
+        assert s in syms
+
+
+def test_library_exports_every_declared_symbol():
+    from vivlasov1d_b200 import _lib
+    lib = _lib.load()
+    missing = [s for s in declared_symbols() if not hasattr(lib, s)]
+    assert not missing, missing
+    assert set(declared_symbols()) == set(_lib.SIGNATURES), "ctypes signatures out of sync with vv.h"
+    assert lib.vv_version() >= 1
+    assert _lib.status_string(0) == "ok"
+
+
+def test_create_rejects_bad_grid_without_gpu():
+    """Argument checks happen before any device call."""
+    from vivlasov1d_b200 import _lib
+    lib = _lib.load()
+    g = _lib.vv_grid(nx=3, nv=4, L=1.0, vmin=-1.0, vmax=1.0, ht=0.1, charge=-1.0, mass=1.0,
+                     bracket=4, preconditioner=1, laplace=4, order=0, gmres_restart=30)
+    h = C.c_void_p()
+    assert lib.vv_create(C.byref(g), C.byref(h)) == 1  # VV_ERR_ARG
+    g.nx, g.nv = 12, 32
+    assert lib.vv_create(C.byref(g), C.byref(h)) == 2  # VV_ERR_UNSUPPORTED (non power of two)
+
+
+def test_product_does_not_import_oracle():
+    pkg = os.path.join(ROOT, "vivlasov1d_b200")
+    for dirpath, _, files in os.walk(pkg):
+        for fn in files:
+            if fn.endswith(".py"):
+                src = open(os.path.join(dirpath, fn)).read()
+                assert "oracle" not in re.findall(r"^\s*(?:from|import)\s+(\w+)", src, flags=re.M), fn
+
+
+def test_config_reader_defaults_and_reference_cfg():
+    from vivlasov1d_b200.config import Config
+    c = Config()
+    assert c["solver"]["petsc_ksp_rtol"] == 1e-4 and c["solver"]["petsc_snes_max_iter"] == 20
+    assert c.get_poisson_bracket() == "arakawaj4" and c.get_preconditioner() == ""
+    txt = """
+[grid]
+nx = 64
+nv = 128
+ht = 0.1
+L = 12.566370614359172
+vmax = 20.0
+[solver]
+method = 'matrixfree'
+poisson_bracket = 'ArakawaJ1'
+preconditioner_type   = 'tensor'
+preconditioner_scheme   = 'tensor_kinetic'
+petsc_ksp_rtol = 1E-5
+[initial_data]
+charge         = -1.0
+nfourier = 32
+[io]
+hdf5_output = twostream_test.hdf5"
+"""
+    c = Config(text=txt)
+    assert c["grid"]["nx"] == 64 and c["grid"]["vmin"] is None
+    assert c.get_poisson_bracket() == "arakawaj1"
+    assert c.get_preconditioner() == "tensor_kinetic"
+    assert c["solver"]["petsc_ksp_rtol"] == 1e-5
+    assert c["initial_data"]["charge"] == -1.0 and c["initial_data"]["nfourier"] == 32
+    assert c.get_averaging_operator() == "point"

@@ -1,0 +1,139 @@
+"""ctypes binding of libvv.so (include/vv.h).
+
+The library is the product's only compute path: if it is missing or fails to
+load, importing the solver raises -- there is no CPU fallback.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libvv.so")
+
+# ---- constants (vv.h) ----
+VV_OK = 0
+VV_ERR_DIVERGED = 5
+BRACKET = {"arakawaj1": 1, "arakawaj2": 2, "arakawaj4": 4}
+PC_NONE, PC_TENSOR_KINETIC = 0, 1
+LAPLACE = {"cfd4": 4}
+ORDER_FACTORED, ORDER_REFERENCE = 0, 1
+MAX_PICARD = 64
+
+# PETSc KSPConvergedReason names for the reasons the GMRES driver reports
+KSP_REASONS = {2: "CONVERGED_RTOL", 3: "CONVERGED_ATOL", -2: "DIVERGED_NULL", -3: "DIVERGED_ITS",
+               -4: "DIVERGED_DTOL", -5: "DIVERGED_BREAKDOWN", -9: "DIVERGED_NANORINF"}
+
+
+class vv_grid(C.Structure):
+    _fields_ = [("nx", C.c_int32), ("nv", C.c_int32), ("L", C.c_double), ("vmin", C.c_double),
+                ("vmax", C.c_double), ("ht", C.c_double), ("charge", C.c_double), ("mass", C.c_double),
+                ("bracket", C.c_int32), ("preconditioner", C.c_int32), ("laplace", C.c_int32),
+                ("order", C.c_int32), ("gmres_restart", C.c_int32), ("reserved", C.c_int32)]
+
+
+class vv_ksp_opts(C.Structure):
+    _fields_ = [("rtol", C.c_double), ("atol", C.c_double), ("dtol", C.c_double),
+                ("max_it", C.c_int32), ("restart", C.c_int32)]
+
+
+class vv_ksp_result(C.Structure):
+    _fields_ = [("its", C.c_int32), ("reason", C.c_int32), ("rnorm", C.c_double)]
+
+
+class vv_state(C.Structure):
+    _fields_ = [(n, C.c_void_p) for n in
+                ("f", "fh", "phi", "phih", "h1c", "h1h", "h2c", "h2h", "n", "u", "e", "a")]
+
+
+class vv_snes_opts(C.Structure):
+    _fields_ = [("atol", C.c_double), ("max_iter", C.c_int32), ("reserved", C.c_int32),
+                ("abort_residual", C.c_double)]
+
+
+class vv_step_report(C.Structure):
+    _fields_ = [("picard_its", C.c_int32), ("gmres_its_total", C.c_int32), ("reverted", C.c_int32),
+                ("stop_rule", C.c_int32), ("ksp_failures", C.c_int32), ("aborted", C.c_int32),
+                ("gmres_its", C.c_int32 * MAX_PICARD), ("ksp_reason", C.c_int32 * MAX_PICARD),
+                ("residual", C.c_double * (MAX_PICARD + 1))]
+
+
+INVARIANT_NAMES = ("mass", "L1", "L2", "L3", "L4", "L5", "L6", "L8", "Lmin", "Lmax", "entropy",
+                   "E_kin", "E_pot", "energy", "momentum", "field_energy")
+
+
+class vv_invariant_set(C.Structure):
+    _fields_ = [(n, C.c_double) for n in INVARIANT_NAMES]
+
+
+P = C.c_void_p
+I = C.c_int
+D = C.c_double
+
+# name -> (restype, argtypes); every symbol declared in include/vv.h
+SIGNATURES = {
+    "vv_create": (I, [C.POINTER(vv_grid), C.POINTER(P)]),
+    "vv_destroy": (I, [P]),
+    "vv_set_stream": (I, [P, P]),
+    "vv_status_string": (C.c_char_p, [I]),
+    "vv_version": (I, []),
+    "vv_grid_vectors": (I, [P, P, P]),
+    "vv_update_history": (I, [P, P]),
+    "vv_update_previous": (I, [P, P, P, P, P]),
+    "vv_function": (I, [P, P, P, I]),
+    "vv_jacobian": (I, [P, P, P, I]),
+    "vv_function_norm": (I, [P, P, P, C.POINTER(D)]),
+    "vv_bracket": (I, [P, P, P, D]),
+    "vv_pc_apply": (I, [P, P, P]),
+    "vv_moments": (I, [P, P, P, P, P, P]),
+    "vv_potential_to_hamiltonian": (I, [P, P, P]),
+    "vv_poisson_rhs": (I, [P, P, P]),
+    "vv_poisson_matvec": (I, [P, P, P]),
+    "vv_poisson_function": (I, [P, P, P, P]),
+    "vv_poisson_solve": (I, [P, P, P]),
+    "vv_gmres": (I, [P, P, P, C.POINTER(vv_ksp_opts), C.POINTER(vv_ksp_result)]),
+    "vv_run_init": (I, [P, C.POINTER(vv_state), I]),
+    "vv_calculate_moments": (I, [P, C.POINTER(vv_state)]),
+    "vv_calculate_residual": (I, [P, C.POINTER(vv_state), C.POINTER(D)]),
+    "vv_step": (I, [P, C.POINTER(vv_state), C.POINTER(vv_snes_opts), C.POINTER(vv_ksp_opts),
+                    C.POINTER(vv_step_report)]),
+    "vv_invariants": (I, [P, P, P, P, C.POINTER(vv_invariant_set)]),
+    "vv_timing_enable": (I, [P, I]),
+    "vv_timing_read": (I, [P, C.POINTER(C.c_int64), C.POINTER(D), I]),
+    "vv_launch_count": (I, [P, C.POINTER(C.c_int64), I]),
+}
+
+
+class VVError(RuntimeError):
+    def __init__(self, status, what):
+        self.status = status
+        super().__init__("%s failed: %s (status %d)" % (what, status_string(status), status))
+
+
+_lib = None
+
+
+def load():
+    """Load libvv.so (raises OSError if it has not been built)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise OSError("libvv.so not found at %s; run `python -m vivlasov1d_b200.build`" % LIB_PATH)
+        lib = C.CDLL(LIB_PATH)
+        for name, (res, args) in SIGNATURES.items():
+            fn = getattr(lib, name)
+            fn.restype = res
+            fn.argtypes = args
+        _lib = lib
+    return _lib
+
+
+def status_string(status):
+    s = load().vv_status_string(int(status))
+    return s.decode() if s else "?"
+
+
+def check(status, what):
+    if status != VV_OK:
+        raise VVError(status, what)
+    return status

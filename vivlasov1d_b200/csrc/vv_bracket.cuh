@@ -1,0 +1,320 @@
+// Arakawa J1/J2/J4 bracket kernels: residual, Jacobian-vector product and
+// bare bracket, with the time-derivative term fused in.
+//
+// Layout: fields are F[j*nx + i] (x fastest, periodic; v bounded).  A CTA
+// owns a BX x BY tile of outputs and stages the input with a 2-cell halo in
+// shared memory (x wraps periodically; rows outside [0, nv) are never read by
+// interior outputs).  The Hamiltonian is regenerated in the CTA from the 1-D
+// profiles h0(v) and the four x profiles of h1/h2 -- it never touches HBM.
+//
+// Two arithmetic orders:
+//   * REFERENCE -- the exact expression trees of PoissonBracket.pyx:100-113
+//     (J1), :221-234 (J2), :360-389 (J4) and PETScNLVlasovMP.pyx:33-58, with
+//     every operation rounded separately (__dadd_rn/__dmul_rn, no FMA), and
+//     h built in the axpy order of PETScVlasovSolver.pyx:145-149.  Results are
+//     bit-identical to the reference loop.
+//   * FACTORED -- h(x,v) = a(v) + b(x) is separable, so every stencil
+//     coefficient of the bracket (the coefficient form of
+//     PoissonBracket.pyx:168-181 and :290-301) is a sum of a v-difference of a
+//     and an x-difference of b.  The J4 stencil then collapses to 8 input
+//     differences and 6 products per output (~21 FP64 ops instead of ~60).
+#pragma once
+#include "vv_common.cuh"
+
+namespace vv {
+
+enum BracketMode { MODE_JVP = 0, MODE_RESIDUAL = 1, MODE_ADD = 2 };
+
+struct BracketParams {
+    int nx, nv;
+    double ht_inv;   // 1/ht
+    double factor;   // bracket factor (0.5 for the JVP, 1.0 residual)
+    double f1;       // hx_inv*hv_inv/12
+    double f2;       // hx_inv*hv_inv/24
+    const double* h0;   // nv: 0.5 v^2 mass
+    const double* hxp;  // 4*nx: h1p, h1h, h2p, h2h profiles
+};
+
+constexpr int BX = 32;
+constexpr int BY = 16;
+constexpr int TY = 8;             // threads in y; each thread handles BY/TY rows
+constexpr int SX = BX + 4;
+constexpr int SY = BY + 4;
+
+__device__ __forceinline__ int wrapx(int i, int nx) {
+    i %= nx;
+    return i < 0 ? i + nx : i;
+}
+
+// h at (i, j) in the reference's axpy order: (((h0 + .5 h1p) + .5 h1h) + .5 h2p) + .5 h2h
+__device__ __forceinline__ double h_ref(const BracketParams& p, int i, int j) {
+    const int nx = p.nx;
+    double h = p.h0[j];
+    h = __dadd_rn(h, 0.5 * p.hxp[i]);
+    h = __dadd_rn(h, 0.5 * p.hxp[nx + i]);
+    h = __dadd_rn(h, 0.5 * p.hxp[2 * nx + i]);
+    h = __dadd_rn(h, 0.5 * p.hxp[3 * nx + i]);
+    return h;
+}
+
+// x part of h: ((.5 h1p + .5 h1h) + .5 h2p) + .5 h2h
+__device__ __forceinline__ double b_fac(const BracketParams& p, int i) {
+    const int nx = p.nx;
+    double b = 0.5 * p.hxp[i] + 0.5 * p.hxp[nx + i];
+    b += 0.5 * p.hxp[2 * nx + i];
+    b += 0.5 * p.hxp[3 * nx + i];
+    return b;
+}
+
+// Stage input and (reference order only) h into shared memory.
+template <int MODE, bool STAGE_H>
+__device__ __forceinline__ void stage_tile(const double* __restrict__ X, const double* __restrict__ Xh,
+                                           const BracketParams& p, int i0, int j0,
+                                           double (*sx)[SX + 1], double (*sh)[SX + 1]) {
+    const int tid = threadIdx.x + BX * threadIdx.y;
+    for (int s = tid; s < SX * SY; s += BX * TY) {
+        const int ly = s / SX, lx = s - ly * SX;
+        const int gi = wrapx(i0 - 2 + lx, p.nx);
+        const int gj = j0 - 2 + ly;
+        double xv = 0.0, hv = 0.0;
+        if (gj >= 0 && gj < p.nv) {
+            const size_t g = (size_t)gj * p.nx + gi;
+            if (MODE == MODE_RESIDUAL) {
+                // Fave = 0 + .5 Fh + .5 F   (PETScNLVlasovMP.pyx:49-51)
+                xv = __dadd_rn(0.5 * Xh[g], 0.5 * X[g]);
+            } else {
+                xv = X[g];
+            }
+            if (STAGE_H) hv = h_ref(p, gi, gj);
+        }
+        sx[ly][lx] = xv;
+        if (STAGE_H) sh[ly][lx] = hv;
+    }
+}
+
+#define R_ADD(a, b) __dadd_rn((a), (b))
+#define R_SUB(a, b) __dsub_rn((a), (b))
+#define R_MUL(a, b) __dmul_rn((a), (b))
+
+// ---------------------------------------------------------------------------
+// Reference operation order
+// ---------------------------------------------------------------------------
+template <int SCHEME, int MODE>
+__global__ void __launch_bounds__(BX * TY)
+k_bracket_ref(const double* __restrict__ X, const double* __restrict__ Xh,
+              double* __restrict__ Y, BracketParams p, double* __restrict__ sumsq) {
+    __shared__ double sx[SY][SX + 1];
+    __shared__ double sh[SY][SX + 1];
+    __shared__ double sred[BX * TY / 32];
+    const int i0 = blockIdx.x * BX, j0 = blockIdx.y * BY;
+    stage_tile<MODE, true>(X, Xh, p, i0, j0, sx, sh);
+    __syncthreads();
+
+    double acc2 = 0.0;
+    const int lx = threadIdx.x + 2;
+    const int i = i0 + threadIdx.x;
+#pragma unroll
+    for (int r = 0; r < BY / TY; ++r) {
+        const int ly = threadIdx.y + r * TY + 2;
+        const int j = j0 + ly - 2;
+        if (i >= p.nx || j >= p.nv) continue;
+        const size_t g = (size_t)j * p.nx + i;
+#define XS(di, dj) sx[ly + (dj)][lx + (di)]
+#define HS(di, dj) sh[ly + (dj)][lx + (di)]
+        double y;
+        if (MODE == MODE_JVP) {
+            y = R_MUL(p.ht_inv, X[g]);                 // Y.axpy(ht_inv, F)
+        } else if (MODE == MODE_RESIDUAL) {
+            y = R_MUL(p.ht_inv, R_SUB(X[g], Xh[g]));   // Y.axpy(ht_inv, F - Fh)
+        } else {
+            y = Y[g];
+        }
+        if (j >= 2 && j < p.nv - 2) {
+            double s1 = 0.0, s2 = 0.0;
+            if (SCHEME == 1 || SCHEME == 4) {
+                const double jpp = R_SUB(R_MUL(R_SUB(XS(1, 0), XS(-1, 0)), R_SUB(HS(0, 1), HS(0, -1))),
+                                         R_MUL(R_SUB(XS(0, 1), XS(0, -1)), R_SUB(HS(1, 0), HS(-1, 0))));
+                const double jpc = R_ADD(R_SUB(R_SUB(R_MUL(XS(1, 0), R_SUB(HS(1, 1), HS(1, -1))),
+                                                     R_MUL(XS(-1, 0), R_SUB(HS(-1, 1), HS(-1, -1)))),
+                                               R_MUL(XS(0, 1), R_SUB(HS(1, 1), HS(-1, 1)))),
+                                         R_MUL(XS(0, -1), R_SUB(HS(1, -1), HS(-1, -1))));
+                const double jcp = R_ADD(R_SUB(R_SUB(R_MUL(XS(1, 1), R_SUB(HS(0, 1), HS(1, 0))),
+                                                     R_MUL(XS(-1, -1), R_SUB(HS(-1, 0), HS(0, -1)))),
+                                               R_MUL(XS(-1, 1), R_SUB(HS(0, 1), HS(-1, 0)))),
+                                         R_MUL(XS(1, -1), R_SUB(HS(1, 0), HS(0, -1))));
+                s1 = R_ADD(R_ADD(jpp, jpc), jcp);
+            }
+            if (SCHEME == 2 || SCHEME == 4) {
+                const double jcc = R_SUB(R_MUL(R_SUB(XS(1, 1), XS(-1, -1)), R_SUB(HS(-1, 1), HS(1, -1))),
+                                         R_MUL(R_SUB(XS(-1, 1), XS(1, -1)), R_SUB(HS(1, 1), HS(-1, -1))));
+                const double jpc = R_ADD(R_SUB(R_SUB(R_MUL(XS(2, 0), R_SUB(HS(1, 1), HS(1, -1))),
+                                                     R_MUL(XS(-2, 0), R_SUB(HS(-1, 1), HS(-1, -1)))),
+                                               R_MUL(XS(0, 2), R_SUB(HS(1, 1), HS(-1, 1)))),
+                                         R_MUL(XS(0, -2), R_SUB(HS(1, -1), HS(-1, -1))));
+                const double jcp = R_ADD(R_SUB(R_SUB(R_MUL(XS(1, 1), R_SUB(HS(0, 2), HS(2, 0))),
+                                                     R_MUL(XS(-1, -1), R_SUB(HS(-2, 0), HS(0, -2)))),
+                                               R_MUL(XS(-1, 1), R_SUB(HS(0, 2), HS(-2, 0)))),
+                                         R_MUL(XS(1, -1), R_SUB(HS(2, 0), HS(0, -2))));
+                s2 = R_ADD(R_ADD(jcc, jpc), jcp);
+            }
+            double add;
+            if (SCHEME == 1) {
+                add = R_MUL(R_MUL(p.factor, s1), p.f1);      // factor*(..)*arakawa_factor
+            } else if (SCHEME == 2) {
+                add = R_MUL(R_MUL(p.factor, s2), p.f2);
+            } else {
+                const double r1 = R_MUL(s1, p.f1), r2 = R_MUL(s2, p.f2);
+                add = R_MUL(p.factor, R_SUB(R_MUL(2.0, r1), r2));
+            }
+            y = R_ADD(y, add);
+        }
+#undef XS
+#undef HS
+        Y[g] = y;
+        acc2 += y * y;
+    }
+    if (sumsq) {
+        const double t = block_sum(acc2, sred);
+        if (threadIdx.x == 0 && threadIdx.y == 0) sumsq[blockIdx.x + gridDim.x * blockIdx.y] = t;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Factored (separable-h) form
+// ---------------------------------------------------------------------------
+// Per scheme constants of  y/scale = A1*(cA1*d10 + cA2*d20) - B1*(cB1*d01 + cB2*d02)
+//                                    + am*dm + ap*dp + bm*em + bp*ep
+template <int SCHEME> struct Coef;
+template <> struct Coef<1> {
+    static constexpr double cA1 = 2.0, cA2 = 0.0, cB1 = 2.0, cB2 = 0.0;
+    // alpha_m = -Da_m ; alpha_p = -Da_p ; beta_m = Db_m ; beta_p = Db_p
+    VV_DEV static void row(double Dam, double Dap, double A1, double Cm, double Cp, double& am, double& ap) {
+        am = -Dam; ap = -Dap;
+    }
+    VV_DEV static void col(double Dbm, double Dbp, double B1, double Bm, double Bp, double& bm, double& bp) {
+        bm = Dbm; bp = Dbp;
+    }
+};
+template <> struct Coef<2> {
+    static constexpr double cA1 = 0.0, cA2 = 1.0, cB1 = 0.0, cB2 = 1.0;
+    VV_DEV static void row(double Dam, double Dap, double A1, double Cm, double Cp, double& am, double& ap) {
+        am = -Cm - A1; ap = -Cp - A1;
+    }
+    VV_DEV static void col(double Dbm, double Dbp, double B1, double Bm, double Bp, double& bm, double& bp) {
+        bm = Bm + B1; bp = Bp + B1;
+    }
+};
+template <> struct Coef<4> {  // 2*J1 - 0.5*J2 in units of f1 (f2 = f1/2)
+    static constexpr double cA1 = 4.0, cA2 = -0.5, cB1 = 4.0, cB2 = -0.5;
+    VV_DEV static void row(double Dam, double Dap, double A1, double Cm, double Cp, double& am, double& ap) {
+        am = -2.0 * Dam + 0.5 * (Cm + A1);
+        ap = -2.0 * Dap + 0.5 * (Cp + A1);
+    }
+    VV_DEV static void col(double Dbm, double Dbp, double B1, double Bm, double Bp, double& bm, double& bp) {
+        bm = 2.0 * Dbm - 0.5 * (Bm + B1);
+        bp = 2.0 * Dbp - 0.5 * (Bp + B1);
+    }
+};
+
+template <int SCHEME, int MODE, typename T>
+__global__ void __launch_bounds__(BX * TY)
+k_bracket_fac(const T* __restrict__ X, const T* __restrict__ Xh, T* __restrict__ Y,
+              BracketParams p, double* __restrict__ sumsq) {
+    __shared__ T sx[SY][SX + 1];
+    __shared__ double sa[SY];       // a(v) = h0 on the tile rows (with halo)
+    __shared__ double sb[SX];       // b(x) on the tile columns (with halo)
+    __shared__ double srow[BY][3];  // A1, alpha_m, alpha_p (scaled)
+    __shared__ double scol[BX][3];  // B1, beta_m, beta_p (scaled)
+    __shared__ double sred[BX * TY / 32];
+    const int i0 = blockIdx.x * BX, j0 = blockIdx.y * BY;
+    const int tid = threadIdx.x + BX * threadIdx.y;
+    for (int s = tid; s < SX * SY; s += BX * TY) {
+        const int ly = s / SX, lx = s - ly * SX;
+        const int gi = wrapx(i0 - 2 + lx, p.nx);
+        const int gj = j0 - 2 + ly;
+        T xv = T(0);
+        if (gj >= 0 && gj < p.nv) {
+            const size_t g = (size_t)gj * p.nx + gi;
+            if (MODE == MODE_RESIDUAL) xv = T(0.5) * Xh[g] + T(0.5) * X[g];
+            else xv = X[g];
+        }
+        sx[ly][lx] = xv;
+    }
+    if (tid < SY) {
+        const int gj = j0 - 2 + tid;
+        sa[tid] = (gj >= 0 && gj < p.nv) ? p.h0[gj] : 0.0;
+    } else if (tid >= 32 && tid < 32 + SX) {
+        const int l = tid - 32;
+        sb[l] = b_fac(p, wrapx(i0 - 2 + l, p.nx));
+    }
+    __syncthreads();
+    const double scale = (SCHEME == 2) ? p.f2 : p.f1;
+    if (tid < BY) {
+        const int l = tid + 2;
+        const double Dam = sa[l] - sa[l - 1], Dap = sa[l + 1] - sa[l];
+        const double A1 = sa[l + 1] - sa[l - 1];
+        const double Cm = sa[l] - sa[l - 2], Cp = sa[l + 2] - sa[l];
+        double am, ap;
+        Coef<SCHEME>::row(Dam, Dap, A1, Cm, Cp, am, ap);
+        srow[tid][0] = A1; srow[tid][1] = am; srow[tid][2] = ap;
+    } else if (tid >= 32 && tid < 32 + BX) {
+        const int l = tid - 32 + 2;
+        const double Dbm = sb[l] - sb[l - 1], Dbp = sb[l + 1] - sb[l];
+        const double B1 = sb[l + 1] - sb[l - 1];
+        const double Bm = sb[l] - sb[l - 2], Bp = sb[l + 2] - sb[l];
+        double bm, bp;
+        Coef<SCHEME>::col(Dbm, Dbp, B1, Bm, Bp, bm, bp);
+        scol[tid - 32][0] = B1; scol[tid - 32][1] = bm; scol[tid - 32][2] = bp;
+    }
+    __syncthreads();
+
+    const int lx = threadIdx.x + 2;
+    const int i = i0 + threadIdx.x;
+    const T B1 = T(scol[threadIdx.x][0]), bm = T(scol[threadIdx.x][1]), bp = T(scol[threadIdx.x][2]);
+    const T tscale = T(scale * p.factor);
+    double acc2 = 0.0;
+#pragma unroll
+    for (int r = 0; r < BY / TY; ++r) {
+        const int ty = threadIdx.y + r * TY;
+        const int ly = ty + 2;
+        const int j = j0 + ty;
+        if (i >= p.nx || j >= p.nv) continue;
+        const size_t g = (size_t)j * p.nx + i;
+#define XS(di, dj) sx[ly + (dj)][lx + (di)]
+        T y;
+        if (MODE == MODE_JVP) y = T(p.ht_inv) * X[g];
+        else if (MODE == MODE_RESIDUAL) y = T(p.ht_inv) * (X[g] - Xh[g]);
+        else y = Y[g];
+        if (j >= 2 && j < p.nv - 2) {
+            const T A1 = T(srow[ty][0]), am = T(srow[ty][1]), ap = T(srow[ty][2]);
+            const T xm1m1 = XS(-1, -1), xp1m1 = XS(1, -1), xm1p1 = XS(-1, 1), xp1p1 = XS(1, 1);
+            T s = T(0);
+            if (Coef<SCHEME>::cA1 != 0.0 || Coef<SCHEME>::cA2 != 0.0) {
+                T ax = T(0), bx = T(0);
+                if (Coef<SCHEME>::cA1 != 0.0) {
+                    ax = T(Coef<SCHEME>::cA1) * (XS(1, 0) - XS(-1, 0));
+                    bx = T(Coef<SCHEME>::cB1) * (XS(0, 1) - XS(0, -1));
+                }
+                if (Coef<SCHEME>::cA2 != 0.0) {
+                    ax += T(Coef<SCHEME>::cA2) * (XS(2, 0) - XS(-2, 0));
+                    bx += T(Coef<SCHEME>::cB2) * (XS(0, 2) - XS(0, -2));
+                }
+                s = A1 * ax - B1 * bx;
+            }
+            s += am * (xm1m1 - xp1m1);
+            s += ap * (xm1p1 - xp1p1);
+            s += bm * (xm1m1 - xm1p1);
+            s += bp * (xp1m1 - xp1p1);
+            y += tscale * s;
+        }
+#undef XS
+        Y[g] = y;
+        acc2 += (double)y * (double)y;
+    }
+    if (sumsq) {
+        const double t = block_sum(acc2, sred);
+        if (tid == 0) sumsq[blockIdx.x + gridDim.x * blockIdx.y] = t;
+    }
+}
+
+}  // namespace vv

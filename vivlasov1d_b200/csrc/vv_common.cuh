@@ -1,0 +1,64 @@
+// Device helpers shared by the libvv kernels: complex arithmetic on double2,
+// deterministic block reductions and the bounded-wait error flag.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#define VV_DEV __device__ __forceinline__
+
+VV_DEV double2 c_add(double2 a, double2 b) { return make_double2(a.x + b.x, a.y + b.y); }
+VV_DEV double2 c_sub(double2 a, double2 b) { return make_double2(a.x - b.x, a.y - b.y); }
+VV_DEV double2 c_mul(double2 a, double2 b) {
+    return make_double2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+}
+VV_DEV double2 c_conj(double2 a) { return make_double2(a.x, -a.y); }
+VV_DEV double2 c_scale(double2 a, double s) { return make_double2(a.x * s, a.y * s); }
+// multiply by a complex number that is given as (real scalar) * (complex lam)
+VV_DEV double2 c_rmul(double2 lam, double s) { return make_double2(lam.x * s, lam.y * s); }
+
+// Warp sum of a double (all lanes get the result).
+VV_DEV double warp_sum(double v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+VV_DEV double warp_max(double v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
+    return v;
+}
+VV_DEV double warp_min(double v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v = fmin(v, __shfl_xor_sync(0xffffffffu, v, o));
+    return v;
+}
+
+// Block-wide sum; result valid in linear thread 0.  `sh` must hold
+// (threads per block)/32 doubles.  Works for 1-D and 2-D blocks.
+VV_DEV double block_sum(double v, double* sh) {
+    const int tid = threadIdx.x + blockDim.x * threadIdx.y;
+    const int lane = tid & 31, wid = tid >> 5;
+    const int nw = (blockDim.x * blockDim.y + 31) >> 5;
+    v = warp_sum(v);
+    __syncthreads();
+    if (lane == 0) sh[wid] = v;
+    __syncthreads();
+    double r = 0.0;
+    if (wid == 0) {
+        r = (lane < nw) ? sh[lane] : 0.0;
+        r = warp_sum(r);
+    }
+    return r;
+}
+
+// Neumaier compensated accumulator.
+struct KSum {
+    double s, c;
+    VV_DEV void init() { s = 0.0; c = 0.0; }
+    VV_DEV void add(double x) {
+        double t = s + x;
+        if (fabs(s) >= fabs(x)) c += (s - t) + x; else c += (x - t) + s;
+        s = t;
+    }
+    VV_DEV double value() const { return s + c; }
+};

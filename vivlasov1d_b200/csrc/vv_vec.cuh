@@ -1,0 +1,511 @@
+// Vector kernels of the Newton/Picard-GMRES loop: deterministic two-stage
+// reductions, the fused multi-dot / multi-axpy of classical Gram-Schmidt,
+// the GMRES Hessenberg/Givens bookkeeping (one thread; PETSc's KSPGMRES
+// algorithm), moments + Poisson + h1 in one pass pair, and the invariants.
+#pragma once
+#include "vv_common.cuh"
+#include "vv_pc.cuh"
+
+namespace vv {
+
+constexpr int RED_THREADS = 256;
+constexpr int MAX_RESTART = 64;
+constexpr int MDOT_CHUNK = 8;
+
+// ---------------------------------------------------------------------------
+// GMRES state (device resident).  Mirrors the arrays of PETSc's KSP_GMRES:
+// hh (rotated Hessenberg, column-major with ld = restart+2), grs (rotated
+// right-hand side), cc/ss (Givens), plus the KSPConvergedDefault state.
+// ---------------------------------------------------------------------------
+struct GmresState {
+    int it;          // Arnoldi index within the current cycle
+    int its;         // total iterations (ksp->its)
+    int reason;      // KSPConvergedReason
+    int active;      // 1 while the cycle continues
+    int restart, max_it;
+    int cycle_start; // 1 on the first call of a cycle
+    int pad;
+    double rtol, atol, dtol, haptol;
+    double rnorm0, ttol, res;
+    double scale;    // reciprocal norm used by the next normalisation
+    double sumsq;    // reduced sum of squares
+    double hcol[MAX_RESTART + 2];  // <w, v_j> of the current column
+    double grs[MAX_RESTART + 2];
+    double cc[MAX_RESTART + 1], ss[MAX_RESTART + 1];
+    double hh[(MAX_RESTART + 2) * (MAX_RESTART + 1)];
+    double nrs[MAX_RESTART + 1];
+};
+
+// PETSc reasons
+constexpr int R_ITERATING = 0, R_RTOL = 2, R_ATOL = 3, R_NULL = -2, R_ITS = -3, R_DTOL = -4,
+              R_BREAKDOWN = -5, R_NANORINF = -9;
+
+VV_DEV int ksp_converged(GmresState* s, int n, double rnorm) {
+    if (n == 0) {
+        s->rnorm0 = rnorm;
+        s->ttol = fmax(s->rtol * rnorm, s->atol);
+    }
+    if (isnan(rnorm) || isinf(rnorm)) return R_NANORINF;
+    if (rnorm <= s->ttol) return rnorm < s->atol ? R_ATOL : R_RTOL;
+    if (rnorm >= s->dtol * s->rnorm0) return R_DTOL;
+    return R_ITERATING;
+}
+
+// ----- partial sums of squares --------------------------------------------
+template <typename T>
+__global__ void __launch_bounds__(RED_THREADS)
+k_sumsq_partial(const T* __restrict__ x, size_t n, double* __restrict__ part) {
+    __shared__ double sh[RED_THREADS / 32];
+    double acc = 0.0;
+    for (size_t i = blockIdx.x * (size_t)RED_THREADS + threadIdx.x; i < n; i += (size_t)gridDim.x * RED_THREADS) {
+        const double v = (double)x[i];
+        acc += v * v;
+    }
+    const double t = block_sum(acc, sh);
+    if (threadIdx.x == 0) part[blockIdx.x] = t;
+}
+
+template <typename T>
+__global__ void __launch_bounds__(RED_THREADS)
+k_sum_partial(const T* __restrict__ x, size_t n, double* __restrict__ part) {
+    __shared__ double sh[RED_THREADS / 32];
+    double acc = 0.0;
+    for (size_t i = blockIdx.x * (size_t)RED_THREADS + threadIdx.x; i < n; i += (size_t)gridDim.x * RED_THREADS)
+        acc += (double)x[i];
+    const double t = block_sum(acc, sh);
+    if (threadIdx.x == 0) part[blockIdx.x] = t;
+}
+
+// Reduce `np` partials per column (m columns, stride ld) into out[m].
+__global__ void __launch_bounds__(RED_THREADS)
+k_reduce_cols(const double* __restrict__ part, int np, int m, int ld, double* __restrict__ out) {
+    __shared__ double sh[RED_THREADS / 32];
+    for (int q = 0; q < m; ++q) {
+        double acc = 0.0;
+        for (int b = threadIdx.x; b < np; b += RED_THREADS) acc += part[(size_t)q * ld + b];
+        const double t = block_sum(acc, sh);
+        if (threadIdx.x == 0) out[q] = t;
+        __syncthreads();
+    }
+}
+
+// ----- multi-dot: part[q*ld + b] = sum_{block b} w * V_q, q in [q0, q0+CH) -----
+template <typename T>
+__global__ void __launch_bounds__(RED_THREADS)
+k_mdot_partial(const T* __restrict__ w, const T* __restrict__ V, size_t ldv, int q0, int m,
+               size_t n, double* __restrict__ part, int ld) {
+    __shared__ double sh[RED_THREADS / 32];
+    double acc[MDOT_CHUNK];
+#pragma unroll
+    for (int c = 0; c < MDOT_CHUNK; ++c) acc[c] = 0.0;
+    const int cnt = min(MDOT_CHUNK, m - q0);
+    for (size_t i = blockIdx.x * (size_t)RED_THREADS + threadIdx.x; i < n; i += (size_t)gridDim.x * RED_THREADS) {
+        const double wi = (double)w[i];
+#pragma unroll
+        for (int c = 0; c < MDOT_CHUNK; ++c)
+            if (c < cnt) acc[c] += wi * (double)V[(size_t)(q0 + c) * ldv + i];
+    }
+#pragma unroll
+    for (int c = 0; c < MDOT_CHUNK; ++c) {
+        if (c < cnt) {
+            const double t = block_sum(acc[c], sh);
+            if (threadIdx.x == 0) part[(size_t)(q0 + c) * ld + blockIdx.x] = t;
+        }
+    }
+}
+
+// ----- w += sum_q coef[q] * V_q  (coef read from device), plus ||w||^2 partials
+// sign = -1 uses -hcol (Gram-Schmidt), +1 uses nrs (solution update)
+template <typename T>
+__global__ void __launch_bounds__(RED_THREADS)
+k_maxpy(T* __restrict__ w, const T* __restrict__ V, size_t ldv, int m, const double* __restrict__ coef,
+        double sign, size_t n, double* __restrict__ part) {
+    __shared__ double sh[RED_THREADS / 32];
+    __shared__ double cf[MAX_RESTART + 2];
+    for (int q = threadIdx.x; q < m; q += RED_THREADS) cf[q] = sign * coef[q];
+    __syncthreads();
+    double acc = 0.0;
+    for (size_t i = blockIdx.x * (size_t)RED_THREADS + threadIdx.x; i < n; i += (size_t)gridDim.x * RED_THREADS) {
+        double wi = (double)w[i];
+        for (int q = 0; q < m; ++q) wi += cf[q] * (double)V[(size_t)q * ldv + i];
+        w[i] = (T)wi;
+        acc += wi * wi;
+    }
+    if (part) {
+        const double t = block_sum(acc, sh);
+        if (threadIdx.x == 0) part[blockIdx.x] = t;
+    }
+}
+
+// y = s * x, s = *scale (device) ; if scale pointer is null uses sval
+template <typename TI, typename TO>
+__global__ void k_scale(const TI* __restrict__ x, TO* __restrict__ y, size_t n, const double* __restrict__ scale,
+                        double sval) {
+    const double s = scale ? *scale : sval;
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
+        y[i] = (TO)((double)x[i] * s);
+}
+
+// y = a*x + b*y
+template <typename T>
+__global__ void k_axpby(const T* __restrict__ x, T* __restrict__ y, size_t n, double a, double b) {
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
+        y[i] = (T)(a * (double)x[i] + b * (double)y[i]);
+}
+
+// ----- GMRES bookkeeping (single thread) ----------------------------------
+// Cycle start: res = sqrt(sumsq) of the initial residual (KSPGMRESCycle top).
+__global__ void k_gmres_cycle_start(GmresState* s) {
+    if (threadIdx.x != 0) return;
+    const double res = sqrt(s->sumsq);
+    s->it = 0;
+    s->grs[0] = res;
+    s->res = res;
+    s->scale = (res != 0.0) ? 1.0 / res : 1.0;
+    if (res == 0.0) {
+        s->reason = R_ATOL;
+        s->active = 0;
+        return;
+    }
+    s->reason = ksp_converged(s, s->its, res);
+    s->active = (s->reason == R_ITERATING && s->its < s->max_it) ? 1 : 0;
+}
+
+// After w = A v_it, hcol = <w, v_j>, w -= sum hcol_j v_j and sumsq = ||w||^2:
+// the rest of one Arnoldi step (KSPGMRESCycle body + KSPGMRESUpdateHessenberg).
+__global__ void k_gmres_arnoldi(GmresState* s) {
+    if (threadIdx.x != 0 || !s->active) return;
+    const int it = s->it;
+    const int ld = s->restart + 2;
+    double* hh = s->hh;
+#define HH(a, b) hh[(b) * ld + (a)]
+    for (int j = 0; j <= it; ++j) HH(j, it) = s->hcol[j];
+    const double tt = sqrt(s->sumsq);
+    s->scale = (tt != 0.0) ? 1.0 / tt : 1.0;
+    HH(it + 1, it) = tt;
+    double hapbnd = fabs(tt / s->grs[it]);
+    if (hapbnd > s->haptol) hapbnd = s->haptol;
+    const bool hapend = tt < hapbnd;
+    for (int j = 1; j <= it; ++j) {
+        const double t = HH(j - 1, it);
+        HH(j - 1, it) = s->cc[j - 1] * t + s->ss[j - 1] * HH(j, it);
+        HH(j, it) = s->cc[j - 1] * HH(j, it) - s->ss[j - 1] * t;
+    }
+    bool null = false;
+    if (!hapend) {
+        const double t = sqrt(HH(it, it) * HH(it, it) + HH(it + 1, it) * HH(it + 1, it));
+        if (t == 0.0) {
+            s->reason = R_NULL;
+            null = true;
+        } else {
+            s->cc[it] = HH(it, it) / t;
+            s->ss[it] = HH(it + 1, it) / t;
+            s->grs[it + 1] = -(s->ss[it] * s->grs[it]);
+            s->grs[it] = s->cc[it] * s->grs[it];
+            HH(it, it) = s->cc[it] * HH(it, it) + s->ss[it] * HH(it + 1, it);
+            s->res = fabs(s->grs[it + 1]);
+        }
+    } else {
+        s->res = 0.0;
+    }
+#undef HH
+    s->it = it + 1;
+    s->its += 1;
+    if (!null) {
+        s->reason = ksp_converged(s, s->its, s->res);
+        if (hapend && s->reason == R_ITERATING) s->reason = R_BREAKDOWN;
+    }
+    s->active = (s->reason == R_ITERATING && s->it < s->restart && s->its < s->max_it) ? 1 : 0;
+}
+
+// KSPGMRESBuildSoln: back substitution into nrs; sets s->pad = number of
+// coefficients to apply (0 when nothing to add).
+__global__ void k_gmres_backsub(GmresState* s) {
+    if (threadIdx.x != 0) return;
+    const int last = s->it - 1;
+    const int ld = s->restart + 2;
+    const double* hh = s->hh;
+#define HH(a, b) hh[(b) * ld + (a)]
+    s->pad = 0;
+    if (last < 0) return;
+    if (HH(last, last) == 0.0) {
+        s->reason = R_BREAKDOWN;
+        return;
+    }
+    s->nrs[last] = s->grs[last] / HH(last, last);
+    for (int ii = 1; ii <= last; ++ii) {
+        const int k = last - ii;
+        double t = s->grs[k];
+        for (int j = k + 1; j <= last; ++j) t = t - HH(k, j) * s->nrs[j];
+        if (HH(k, k) == 0.0) {
+            s->reason = R_BREAKDOWN;
+            return;
+        }
+        s->nrs[k] = t / HH(k, k);
+    }
+#undef HH
+    s->pad = last + 1;
+    if (s->its >= s->max_it && s->reason == R_ITERATING) s->reason = R_ITS;
+}
+
+// ---------------------------------------------------------------------------
+// moments: partial sums over v segments, then one CTA finishes moments,
+// Poisson (spectral, CFD4 symbol) and h1 = phi - mean(phi).
+// ---------------------------------------------------------------------------
+constexpr int MOM_TX = 32, MOM_TY = 8;
+
+template <typename T>
+__global__ void __launch_bounds__(MOM_TX * MOM_TY)
+k_moments_partial(const T* __restrict__ F, int nx, int nv, int seg, const double* __restrict__ v,
+                  double* __restrict__ part /* [S][3][nx] */) {
+    __shared__ double sh[3][MOM_TY][MOM_TX + 1];
+    const int i = blockIdx.x * MOM_TX + threadIdx.x;
+    const int s = blockIdx.y;
+    const int ja = s * seg, jb = min(nv, ja + seg);
+    double a0 = 0.0, a1 = 0.0, a2 = 0.0;
+    if (i < nx) {
+        for (int j = ja + threadIdx.y; j < jb; j += MOM_TY) {
+            const double f = (double)F[(size_t)j * nx + i];
+            const double vj = v[j];
+            a0 += f;
+            a1 += vj * f;
+            a2 += (vj * vj) * f;
+        }
+    }
+    sh[0][threadIdx.y][threadIdx.x] = a0;
+    sh[1][threadIdx.y][threadIdx.x] = a1;
+    sh[2][threadIdx.y][threadIdx.x] = a2;
+    __syncthreads();
+    if (threadIdx.y < 3 && i < nx) {
+        double t = 0.0;
+        for (int y = 0; y < MOM_TY; ++y) t += sh[threadIdx.y][y][threadIdx.x];
+        part[((size_t)s * 3 + threadIdx.y) * nx + i] = t;
+    }
+}
+
+struct PoissonParams {
+    int nx, M, logM, S;   // S = number of moment partials
+    double hv, charge, hx2_inv, hx, inv_nx;
+    const double2* tw;       // nx/2 twiddles
+    const double* sym_inv;   // M+1 entries: 1/symbol_k (0 for k = 0)
+};
+
+constexpr int POIS_THREADS = 1024;
+
+// Single CTA.  Inputs: moment partials (or n directly when part == nullptr).
+// Outputs (each optional): n, u, e, a, phi, h1; scal[0] = ||Poisson residual||_2,
+// scal[1] = sum(phi).
+__global__ void __launch_bounds__(POIS_THREADS)
+k_moments_poisson(const double* __restrict__ part, const double* __restrict__ n_in,
+                  double* __restrict__ n, double* __restrict__ u, double* __restrict__ e,
+                  double* __restrict__ a, double* __restrict__ phi, double* __restrict__ h1,
+                  double* __restrict__ scal, PoissonParams p) {
+    extern __shared__ double2 psm[];
+    double2* buf = psm;                               // M complex
+    double* nn = reinterpret_cast<double*>(psm + p.M);  // nx
+    double* ph = nn + p.nx;                           // nx
+    __shared__ double red[POIS_THREADS / 32];
+    const int nx = p.nx, M = p.M;
+    // 1. moments
+    for (int i = threadIdx.x; i < nx; i += blockDim.x) {
+        double s0, s1 = 0.0, s2 = 0.0;
+        if (part) {
+            s0 = 0.0;
+            for (int s = 0; s < p.S; ++s) {
+                s0 += part[((size_t)s * 3 + 0) * nx + i];
+                s1 += part[((size_t)s * 3 + 1) * nx + i];
+                s2 += part[((size_t)s * 3 + 2) * nx + i];
+            }
+            s0 *= p.hv; s1 *= p.hv; s2 *= p.hv;
+            if (n) n[i] = s0;
+            if (u) u[i] = s1;
+            if (e) e[i] = s2;
+            if (a) a[i] = s0 * s0 / (s0 * s2 - s1 * s1);   // Toolbox.pyx:164-165
+        } else {
+            s0 = n_in[i];
+        }
+        nn[i] = s0;
+    }
+    __syncthreads();
+    if (!phi && !h1 && !scal) return;
+    // 2. rhs b = -(n - mean n)*charge
+    double t = 0.0;
+    for (int i = threadIdx.x; i < nx; i += blockDim.x) t += nn[i];
+    t = block_sum(t, red);
+    __shared__ double nmean_s;
+    if (threadIdx.x == 0) nmean_s = t * p.inv_nx;
+    __syncthreads();
+    const double nmean = nmean_s;
+    // 3. FFT of b (real, via M-point complex), divide by the symbol, inverse
+    for (int m = threadIdx.x; m < M; m += blockDim.x) {
+        const double b0 = -(nn[2 * m] - nmean) * p.charge;
+        const double b1 = -(nn[2 * m + 1] - nmean) * p.charge;
+        buf[bitrev(m, p.logM)] = make_double2(b0, b1);
+    }
+    __syncthreads();
+    smem_fft<-1>(buf, 1, M, p.tw);
+    // split into X_k (k = 0..M), divide, rebuild Z for the inverse in place:
+    // every thread handles the pair (k, M-k) so the in-place update is safe.
+    double2* X2 = reinterpret_cast<double2*>(ph);  // reuse ph storage: needs (M+1) complex = nx+2 doubles
+    for (int k = threadIdx.x; k <= M; k += blockDim.x) {
+        const double2 zk = buf[k == M ? 0 : k];
+        const double2 zc = c_conj(buf[k == 0 ? 0 : M - k]);
+        const double2 E = c_scale(c_add(zk, zc), 0.5);
+        const double2 D = c_sub(zk, zc);
+        const double2 O = make_double2(0.5 * D.y, -0.5 * D.x);
+        const double2 w = (k < M) ? p.tw[k] : make_double2(-1.0, 0.0);
+        double2 Xk = c_add(E, c_mul(w, O));
+        Xk = c_scale(Xk, p.sym_inv[k]);
+        if (k == 0 || k == M) Xk.y = 0.0;
+        X2[k] = Xk;
+    }
+    __syncthreads();
+    for (int k = threadIdx.x; k < M; k += blockDim.x) {
+        const double2 xk = X2[k];
+        const double2 xc = c_conj(X2[M - k]);
+        const double2 E = c_scale(c_add(xk, xc), 0.5);
+        double2 w = p.tw[k];
+        w.y = -w.y;
+        const double2 O = c_mul(w, c_scale(c_sub(xk, xc), 0.5));
+        buf[bitrev(k, p.logM)] = make_double2(E.x - O.y, E.y + O.x);
+    }
+    __syncthreads();
+    smem_fft<+1>(buf, 1, M, p.tw);
+    const double sc = 1.0 / (double)M;
+    double* phs = reinterpret_cast<double*>(X2);  // overwrite: phi in smem
+    __syncthreads();
+    for (int m = threadIdx.x; m < M; m += blockDim.x) {
+        phs[2 * m] = buf[m].x * sc;
+        phs[2 * m + 1] = buf[m].y * sc;
+    }
+    __syncthreads();
+    // 4. mean of phi, h1 and Poisson residual A phi + (n - nmean) charge
+    t = 0.0;
+    for (int i = threadIdx.x; i < nx; i += blockDim.x) t += phs[i];
+    t = block_sum(t, red);
+    __shared__ double phimean_s, phisum_s;
+    if (threadIdx.x == 0) { phisum_s = t; phimean_s = t * p.inv_nx; }
+    __syncthreads();
+    double r2 = 0.0;
+    for (int i = threadIdx.x; i < nx; i += blockDim.x) {
+        const double pc = phs[i];
+        if (phi) phi[i] = pc;
+        if (h1) h1[i] = pc - phimean_s;
+        const int im2 = (i - 2 + 2 * nx) % nx, im1 = (i - 1 + nx) % nx;
+        const int ip1 = (i + 1) % nx, ip2 = (i + 2) % nx;
+        const double Ax = (5. * phs[im2] - 32. * phs[im1] + 54. * pc - 32. * phs[ip1] + 5. * phs[ip2]) * p.hx2_inv / 12.;
+        const double r = Ax + (nn[i] - nmean) * p.charge;
+        r2 += r * r;
+    }
+    r2 = block_sum(r2, red);
+    if (threadIdx.x == 0 && scal) {
+        scal[0] = sqrt(r2);
+        scal[1] = phisum_s;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// invariants (distribution_function.pyx:130-306, hamiltonian.pyx:67-124,
+// potential.pyx:48-59), compensated FP64 sums
+// ---------------------------------------------------------------------------
+constexpr int INV_SUMS = 13;   // mass, L1..L6, L8, S, Ekin, Ep1, Ep2, P
+constexpr int INV_NPART = INV_SUMS + 2;  // + min, max
+
+// one CTA: h1 = phi - mean(phi) into h1out, field energy into fe[0]
+__global__ void k_xprofile(const double* __restrict__ phi, int nx, double charge, double hx,
+                           double* __restrict__ h1out, double* __restrict__ fe) {
+    __shared__ double red[32];
+    __shared__ double mean_s;
+    double t = 0.0;
+    for (int i = threadIdx.x; i < nx; i += blockDim.x) t += phi[i];
+    t = block_sum(t, red);
+    if (threadIdx.x == 0) mean_s = t / nx;
+    __syncthreads();
+    double w = 0.0;
+    for (int i = threadIdx.x; i < nx; i += blockDim.x) {
+        h1out[i] = phi[i] - mean_s;
+        const double d = phi[(i + 1) % nx] - phi[i];
+        w += d * d;
+    }
+    w = block_sum(w, red);
+    if (threadIdx.x == 0) fe[0] = 0.5 * charge * w / hx;
+}
+
+__global__ void __launch_bounds__(RED_THREADS)
+k_invariants_partial(const double* __restrict__ f, int nx, int nv, const double* __restrict__ v,
+                     const double* __restrict__ h0, const double* __restrict__ h1,
+                     const double* __restrict__ h2, double* __restrict__ part) {
+    __shared__ double sh[RED_THREADS / 32];
+    KSum acc[INV_SUMS];
+#pragma unroll
+    for (int q = 0; q < INV_SUMS; ++q) acc[q].init();
+    double fmn = INFINITY, fmx = -INFINITY;
+    const size_t n = (size_t)nx * nv;
+    for (size_t idx = blockIdx.x * (size_t)RED_THREADS + threadIdx.x; idx < n;
+         idx += (size_t)gridDim.x * RED_THREADS) {
+        const int j = (int)(idx / nx), i = (int)(idx - (size_t)j * nx);
+        const double fv = f[idx];
+        fmn = fmin(fmn, fv);
+        fmx = fmax(fmx, fv);
+        acc[9].add(fv * h0[j]);
+        acc[10].add(fv * h1[i]);
+        if (h2) acc[11].add(fv * h2[i]);
+        if (j < nv - 1) {
+            const int ip = (i + 1 == nx) ? 0 : i + 1;
+            const double s4 = ((fv + f[(size_t)j * nx + ip]) + f[(size_t)(j + 1) * nx + ip]) + f[(size_t)(j + 1) * nx + i];
+            acc[0].add(s4);
+            const double f2 = fv * fv, f3 = f2 * fv, f4 = f2 * f2;
+            acc[1].add(fabs(fv));
+            acc[2].add(f2);
+            acc[3].add(f3);
+            acc[4].add(f4);
+            acc[5].add(f4 * fv);
+            acc[6].add(f3 * f3);
+            acc[7].add(f4 * f4);
+            const double fe = fv <= 0.0 ? 1e-15 : fv;
+            acc[8].add(fe * log(fe));
+            acc[12].add(fv * v[j]);
+        }
+    }
+    for (int q = 0; q < INV_SUMS; ++q) {
+        const double t = block_sum(acc[q].value(), sh);
+        if (threadIdx.x == 0) part[(size_t)q * gridDim.x + blockIdx.x] = t;
+        __syncthreads();
+    }
+    {
+        double m = warp_min(fmn);
+        __shared__ double shm[RED_THREADS / 32], shx[RED_THREADS / 32];
+        double x = warp_max(fmx);
+        if ((threadIdx.x & 31) == 0) { shm[threadIdx.x >> 5] = m; shx[threadIdx.x >> 5] = x; }
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            for (int w = 1; w < RED_THREADS / 32; ++w) { m = fmin(m, shm[w]); x = fmax(x, shx[w]); }
+            part[(size_t)INV_SUMS * gridDim.x + blockIdx.x] = m;
+            part[(size_t)(INV_SUMS + 1) * gridDim.x + blockIdx.x] = x;
+        }
+    }
+}
+
+// one CTA: out[q] for the 13 sums (compensated over partials), min, max
+__global__ void __launch_bounds__(RED_THREADS)
+k_invariants_final(const double* __restrict__ part, int np, double* __restrict__ out) {
+    __shared__ double sh[RED_THREADS / 32];
+    for (int q = 0; q < INV_SUMS; ++q) {
+        KSum a; a.init();
+        for (int b = threadIdx.x; b < np; b += RED_THREADS) a.add(part[(size_t)q * np + b]);
+        const double t = block_sum(a.value(), sh);
+        if (threadIdx.x == 0) out[q] = t;
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        double m = INFINITY, x = -INFINITY;
+        for (int b = 0; b < np; ++b) {
+            m = fmin(m, part[(size_t)INV_SUMS * np + b]);
+            x = fmax(x, part[(size_t)(INV_SUMS + 1) * np + b]);
+        }
+        out[INV_SUMS] = m;
+        out[INV_SUMS + 1] = x;
+    }
+}
+
+}  // namespace vv
