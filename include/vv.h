@@ -226,8 +226,15 @@ int vv_invariants(vv_ctx* ctx, const double* f, const double* phi, const double*
  * returns the number of launches and their summed device time (ms). */
 int vv_timing_enable(vv_ctx* ctx, int enable);
 int vv_timing_read(vv_ctx* ctx, int64_t* launches, double* total_ms, int reset);
-/* Number of kernels the library has launched since the last reset. */
+/* Number of kernels the library has launched since the last reset
+ * (kernels executed inside the time-step graph included). */
 int vv_launch_count(vv_ctx* ctx, int64_t* launches, int reset);
+/* Device time of one kernel on the context's own buffers: `reps` launches
+ * are captured back to back in a CUDA graph and timed with CUDA events on the
+ * context's stream.  which: 0 Jacobian-vector product (input: GMRES basis
+ * vector 0, output: work field), 1 residual, 2 preconditioner apply (its
+ * three kernels).  *avg_ms = time per launch (per apply for which == 2). */
+int vv_time_kernel(vv_ctx* ctx, int which, int reps, double* avg_ms);
 
 #ifdef __cplusplus
 }

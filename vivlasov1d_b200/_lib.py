@@ -101,6 +101,7 @@ SIGNATURES = {
     "vv_timing_enable": (I, [P, I]),
     "vv_timing_read": (I, [P, C.POINTER(C.c_int64), C.POINTER(D), I]),
     "vv_launch_count": (I, [P, C.POINTER(C.c_int64), I]),
+    "vv_time_kernel": (I, [P, I, I, C.POINTER(D)]),
 }
 
 

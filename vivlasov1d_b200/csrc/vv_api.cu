@@ -14,6 +14,7 @@
 #include "vv_vec.cuh"
 
 #include <algorithm>
+#include <cstdlib>
 #include <cmath>
 #include <complex>
 #include <cstddef>
@@ -28,29 +29,40 @@ struct vv_ctx {
     int nx, nv, M, logM, nmodes, restart;
     size_t ncell;
     double hx, hv, ht_inv, hx_inv, hv_inv, hx2_inv, f1, f2;
-    cudaStream_t st;
+    cudaStream_t st;      // the caller's stream
     int device;
     // device buffers
     double *v, *h0, *hxp, *Fh, *tmp, *bvec, *delta, *fl, *V, *part, *scal, *xscratch, *mom_part;
     double2 *spec, *tw, *lambda, *dinv;
     double *alpha, *gamma, *sym_inv;
-    vv::GmresState* gm;
+    vv::DevState* ds;
     // pinned host staging
     double* hpin;
     int* hstat;
+    vv::DevState* hds;    // pinned copy of the device state (report read-back)
     // launch configuration
     int npart, npart_max;
     int mom_S, mom_seg;
     int pcR;
     size_t smem_rfft, smem_irfft, smem_tri, smem_pois;
+    bool tri_stage;
     bool pivot_differs;
-    // timing of the JVP stencil kernel
+    // timing of the JVP stencil kernel (host-driven path)
     bool timing;
     std::vector<cudaEvent_t> ev;
     size_t ev_used;
     int64_t t_launches;
     double t_ms;
     int64_t launches;
+    // graph of one time step
+    bool use_graph;
+    cudaStream_t cs[4];
+    cudaGraph_t step_graph;
+    cudaGraphExec_t step_exec;
+    vv_state step_key;         // state pointers the graph was captured with
+    unsigned long long hnd[5]; // h_gm_outer, h_gm_inner, h_gm_first, h_pic, h_revert
+    // kernels per region of the step graph (for launch accounting)
+    int nk_top, nk_pic, nk_cycle, nk_restart, nk_arnoldi, nk_revert;
 };
 
 namespace {
@@ -116,6 +128,8 @@ vv::BracketParams bparams(const vv_ctx* c, double factor) {
     p.f2 = c->f2;
     p.h0 = c->h0;
     p.hxp = c->hxp;
+    p.xidx = nullptr;
+    p.xstride = 0;
     return p;
 }
 
@@ -127,6 +141,9 @@ vv::PcParams pcparams(const vv_ctx* c) {
     p.logM = c->logM;
     p.R = c->pcR;
     p.tw = c->tw;
+    p.yidx = nullptr;
+    p.yoff = 0;
+    p.ystride = 0;
     return p;
 }
 
@@ -154,11 +171,21 @@ int drain_timing(vv_ctx* c) {
 }
 
 // ---- bracket launches -------------------------------------------------------
+bool aligned16(const void* p) { return p == nullptr || ((uintptr_t)p & 15u) == 0; }
+
+bool wide_ok(const vv_ctx* c, const void* X, const void* Xh, const void* Y) {
+    return c->nx % vv::WX == 0 && aligned16(X) && aligned16(Xh) && aligned16(Y);
+}
+
+// X may be a GMRES basis base pointer with xidx -> the vector index in the state
 template <int SCHEME, int MODE>
-int launch_bracket_s(vv_ctx* c, const double* X, const double* Xh, double* Y, double factor, double* sumsq) {
+int launch_bracket_s(vv_ctx* c, const double* X, const double* Xh, double* Y, double factor, double* sumsq,
+                     const int* xidx) {
     dim3 grid((c->nx + vv::BX - 1) / vv::BX, (c->nv + vv::BY - 1) / vv::BY);
     dim3 block(vv::BX, vv::TY);
     vv::BracketParams p = bparams(c, factor);
+    p.xidx = xidx;
+    p.xstride = xidx ? c->ncell : 0;
     const bool timed = c->timing && MODE == vv::MODE_JVP;
     cudaEvent_t e0 = nullptr, e1 = nullptr;
     if (timed) {
@@ -167,40 +194,41 @@ int launch_bracket_s(vv_ctx* c, const double* X, const double* Xh, double* Y, do
         e1 = next_event(c);
         if (e0) cudaEventRecord(e0, c->st);
     }
-    if (c->g.order == VV_ORDER_REFERENCE)
+    if (c->g.order == VV_ORDER_REFERENCE) {
         vv::k_bracket_ref<SCHEME, MODE><<<grid, block, 0, c->st>>>(X, Xh, Y, p, sumsq);
-    else
+    } else if (wide_ok(c, X, Xh, Y)) {
+        dim3 gw(c->nx / vv::WX, (c->nv + vv::WY - 1) / vv::WY);
+        vv::k_bracket_wide<SCHEME, MODE, double><<<gw, vv::WTHREADS, 0, c->st>>>(X, Xh, Y, p, sumsq);
+    } else {
         vv::k_bracket_fac<SCHEME, MODE, double><<<grid, block, 0, c->st>>>(X, Xh, Y, p, sumsq);
+    }
     CKL(c);
     if (timed && e1) cudaEventRecord(e1, c->st);
     return VV_OK;
 }
 
 template <int MODE>
-int launch_bracket(vv_ctx* c, const double* X, const double* Xh, double* Y, double factor, double* sumsq) {
+int launch_bracket(vv_ctx* c, const double* X, const double* Xh, double* Y, double factor, double* sumsq,
+                   const int* xidx = nullptr) {
     switch (c->g.bracket) {
-        case VV_BRACKET_J1: return launch_bracket_s<1, MODE>(c, X, Xh, Y, factor, sumsq);
-        case VV_BRACKET_J2: return launch_bracket_s<2, MODE>(c, X, Xh, Y, factor, sumsq);
-        default: return launch_bracket_s<4, MODE>(c, X, Xh, Y, factor, sumsq);
+        case VV_BRACKET_J1: return launch_bracket_s<1, MODE>(c, X, Xh, Y, factor, sumsq, xidx);
+        case VV_BRACKET_J2: return launch_bracket_s<2, MODE>(c, X, Xh, Y, factor, sumsq, xidx);
+        default: return launch_bracket_s<4, MODE>(c, X, Xh, Y, factor, sumsq, xidx);
     }
 }
 
-int bracket_tiles(const vv_ctx* c) {
+// number of per-CTA partials a bracket launch writes for these operands
+int bracket_tiles(const vv_ctx* c, const void* X = nullptr, const void* Xh = nullptr, const void* Y = nullptr) {
+    if (c->g.order != VV_ORDER_REFERENCE && wide_ok(c, X, Xh, Y))
+        return (c->nx / vv::WX) * ((c->nv + vv::WY - 1) / vv::WY);
     return ((c->nx + vv::BX - 1) / vv::BX) * ((c->nv + vv::BY - 1) / vv::BY);
 }
 
 // ---- reductions ---------------------------------------------------------------
-// reduce np partials (1 column) into dst (device)
 int reduce_to(vv_ctx* c, const double* part, int np, double* dst) {
     vv::k_reduce_cols<<<1, vv::RED_THREADS, 0, c->st>>>(part, np, 1, np, dst);
     CKL(c);
     return VV_OK;
-}
-
-int sumsq_to(vv_ctx* c, const double* x, double* dst) {
-    vv::k_sumsq_partial<double><<<c->npart, vv::RED_THREADS, 0, c->st>>>(x, c->ncell, c->part);
-    CKL(c);
-    return reduce_to(c, c->part, c->npart, dst);
 }
 
 int read_scalar(vv_ctx* c, const double* dsrc, double* out) {
@@ -211,7 +239,8 @@ int read_scalar(vv_ctx* c, const double* dsrc, double* out) {
 }
 
 // ---- preconditioner ---------------------------------------------------------
-int pc_apply(vv_ctx* c, const double* X, double* Y) {
+// Y may be a GMRES basis base pointer with yidx -> the vector index (+yoff)
+int pc_apply(vv_ctx* c, const double* X, double* Y, const int* yidx = nullptr, int yoff = 0) {
     vv::PcParams p = pcparams(c);
     const unsigned rows = (unsigned)((c->nv + c->pcR - 1) / c->pcR);
     vv::k_rfft_rows<double><<<rows, 256, c->smem_rfft, c->st>>>(X, c->spec, p);
@@ -223,8 +252,14 @@ int pc_apply(vv_ctx* c, const double* X, double* Y) {
     t.alpha = c->alpha;
     t.gamma = c->gamma;
     t.dinv = c->dinv;
-    vv::k_tridiag_modes<<<c->nmodes, vv::TRI_THREADS, c->smem_tri, c->st>>>(c->spec, t);
+    if (c->tri_stage)
+        vv::k_tridiag_modes<true><<<c->nmodes, vv::TRI_THREADS, c->smem_tri, c->st>>>(c->spec, t);
+    else
+        vv::k_tridiag_modes<false><<<c->nmodes, vv::TRI_THREADS, c->smem_tri, c->st>>>(c->spec, t);
     CKL(c);
+    p.yidx = yidx;
+    p.yoff = yoff;
+    p.ystride = yidx ? c->ncell : 0;
     vv::k_irfft_rows<double><<<rows, 256, c->smem_irfft, c->st>>>(c->spec, Y, p);
     CKL(c);
     return VV_OK;
@@ -237,6 +272,23 @@ int apply_operator(vv_ctx* c, const double* X, double* Y) {
         return pc_apply(c, c->tmp, Y);
     }
     return launch_bracket<vv::MODE_JVP>(c, X, nullptr, Y, 0.5, nullptr);
+}
+
+__global__ void k_copy_to_slot(const double* __restrict__ src, double* __restrict__ V, const int* __restrict__ idx,
+                               size_t n) {
+    double* dst = V + (size_t)(*idx + 1) * n;
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
+        dst[i] = src[i];
+}
+
+// Arnoldi operator V[it] -> V[it+1], it read from the device state
+int apply_operator_state(vv_ctx* c) {
+    const int* itp = &c->ds->it;
+    TRY(launch_bracket<vv::MODE_JVP>(c, c->V, nullptr, c->tmp, 0.5, nullptr, itp));
+    if (c->g.preconditioner == VV_PC_TENSOR_KINETIC) return pc_apply(c, c->tmp, c->V, itp, 1);
+    k_copy_to_slot<<<grid1d(c->ncell, 256), 256, 0, c->st>>>(c->tmp, c->V, itp, c->ncell);
+    CKL(c);
+    return VV_OK;
 }
 
 // ---- moments / Poisson ------------------------------------------------------
@@ -305,100 +357,7 @@ int poisson_apply(vv_ctx* c, const double* x, const double* n, double* y, int mo
     return VV_OK;
 }
 
-// ---- GMRES driver ---------------------------------------------------------
-struct GmHead {
-    int it, its, reason, active;
-};
-
-int read_head(vv_ctx* c, GmHead* h) {
-    CK(cudaMemcpyAsync(c->hstat, c->gm, sizeof(GmHead), cudaMemcpyDeviceToHost, c->st));
-    CK(cudaStreamSynchronize(c->st));
-    std::memcpy(h, c->hstat, sizeof(GmHead));
-    return VV_OK;
-}
-
-int gmres(vv_ctx* c, const double* b, double* x, const vv_ksp_opts* o, vv_ksp_result* res) {
-    const int restart = (o->restart > 0) ? o->restart : c->restart;
-    if (restart > c->restart || restart < 1) return VV_ERR_ARG;
-    const size_t n = c->ncell;
-    double* V = c->V;
-    vv::GmresState hs;
-    std::memset(&hs, 0, offsetof(vv::GmresState, hcol));
-    hs.restart = restart;
-    hs.max_it = o->max_it;
-    hs.rtol = o->rtol;
-    hs.atol = o->atol;
-    hs.dtol = (o->dtol > 0.0) ? o->dtol : 1e5;
-    hs.haptol = 1e-30;
-    std::memcpy(c->hpin, &hs, offsetof(vv::GmresState, hcol));
-    CK(cudaMemcpyAsync(c->gm, c->hpin, offsetof(vv::GmresState, hcol), cudaMemcpyHostToDevice, c->st));
-    CK(cudaMemsetAsync(x, 0, n * sizeof(double), c->st));
-    const unsigned eg = grid1d(n, 256);
-    bool guess_zero = true;
-    GmHead h{};
-    for (;;) {
-        // r = b - A x  (KSPInitialResidual) into V0
-        if (guess_zero) {
-            CK(cudaMemcpyAsync(V, b, n * sizeof(double), cudaMemcpyDeviceToDevice, c->st));
-        } else {
-            TRY(apply_operator(c, x, V));
-            vv::k_axpby<double><<<eg, 256, 0, c->st>>>(b, V, n, 1.0, -1.0);
-            CKL(c);
-        }
-        TRY(sumsq_to(c, V, &c->gm->sumsq));
-        vv::k_gmres_cycle_start<<<1, 32, 0, c->st>>>(c->gm);
-        CKL(c);
-        vv::k_scale<double, double><<<eg, 256, 0, c->st>>>(V, V, n, &c->gm->scale, 1.0);
-        CKL(c);
-        TRY(read_head(c, &h));
-        int it = 0;
-        while (h.active) {
-            double* w = V + (size_t)(it + 1) * n;
-            TRY(apply_operator(c, V + (size_t)it * n, w));
-            // classical Gram-Schmidt: hcol = <w, v_j>, w -= sum hcol_j v_j
-            const int m = it + 1;
-            for (int q0 = 0; q0 < m; q0 += vv::MDOT_CHUNK) {
-                vv::k_mdot_partial<double><<<c->npart, vv::RED_THREADS, 0, c->st>>>(w, V, n, q0, m, n, c->part,
-                                                                                    c->npart_max);
-                CKL(c);
-            }
-            vv::k_reduce_cols<<<1, vv::RED_THREADS, 0, c->st>>>(c->part, c->npart, m, c->npart_max, c->gm->hcol);
-            CKL(c);
-            double* part2 = c->part + (size_t)(vv::MAX_RESTART + 1) * c->npart_max;
-            vv::k_maxpy<double><<<c->npart, vv::RED_THREADS, 0, c->st>>>(w, V, n, m, c->gm->hcol, -1.0, n, part2);
-            CKL(c);
-            TRY(reduce_to(c, part2, c->npart, &c->gm->sumsq));
-            vv::k_gmres_arnoldi<<<1, 32, 0, c->st>>>(c->gm);
-            CKL(c);
-            vv::k_scale<double, double><<<eg, 256, 0, c->st>>>(w, w, n, &c->gm->scale, 1.0);
-            CKL(c);
-            TRY(read_head(c, &h));
-            it = h.it;
-        }
-        vv::k_gmres_backsub<<<1, 32, 0, c->st>>>(c->gm);
-        CKL(c);
-        // number of coefficients to apply is in gm->pad
-        int pad = 0;
-        CK(cudaMemcpyAsync(c->hstat, &c->gm->pad, sizeof(int), cudaMemcpyDeviceToHost, c->st));
-        CK(cudaStreamSynchronize(c->st));
-        pad = c->hstat[0];
-        if (pad > 0) {
-            vv::k_maxpy<double><<<c->npart, vv::RED_THREADS, 0, c->st>>>(x, V, n, pad, c->gm->nrs, 1.0, n, nullptr);
-            CKL(c);
-        }
-        TRY(read_head(c, &h));
-        if (h.reason != 0) break;
-        guess_zero = false;
-    }
-    double rn = 0.0;
-    TRY(read_scalar(c, &c->gm->res, &rn));
-    res->its = h.its;
-    res->reason = h.reason;
-    res->rnorm = rn;
-    return VV_OK;
-}
-
-// ---- step helpers -----------------------------------------------------------
+// ---- small copies -----------------------------------------------------------
 int copy_d(vv_ctx* c, double* dst, const double* src, size_t count) {
     if (!dst || !src || dst == src) return VV_OK;
     CK(cudaMemcpyAsync(dst, src, count * sizeof(double), cudaMemcpyDeviceToDevice, c->st));
@@ -418,8 +377,178 @@ int set_hxp(vv_ctx* c, const double* h1p, const double* h1h, const double* h2p, 
     return VV_OK;
 }
 
+// ---- GMRES: kernel sequences shared by the host-driven and graph paths ------
+// state header written by the host before a solve / step (the option fields)
+int upload_options(vv_ctx* c, const vv_ksp_opts* o, const vv_snes_opts* so) {
+    vv::DevState* h = c->hds;
+    h->restart = (o->restart > 0) ? o->restart : c->restart;
+    h->max_it = o->max_it;
+    h->rtol = o->rtol;
+    h->atol = o->atol;
+    h->dtol = (o->dtol > 0.0) ? o->dtol : 1e5;
+    h->haptol = 1e-30;
+    if (so) {
+        h->snes_atol = so->atol;
+        h->pic_max_iter = so->max_iter;
+        h->abort_residual = so->abort_residual;
+    }
+    h->h_gm_outer = c->hnd[0];
+    h->h_gm_inner = c->hnd[1];
+    h->h_gm_first = c->hnd[2];
+    h->h_pic = c->hnd[3];
+    h->h_revert = c->hnd[4];
+    h->cnt[0] = h->cnt[1] = h->cnt[2] = h->cnt[3] = 0u;
+    // one copy of the header (everything before the report arrays)
+    CK(cudaMemcpyAsync(c->ds, h, offsetof(vv::DevState, gmres_its), cudaMemcpyHostToDevice, c->st));
+    return VV_OK;
+}
+
+int gm_init(vv_ctx* c, double* x) {
+    vv::k_gm_init<double><<<grid1d(c->ncell, 256), 256, 0, c->st>>>(c->ds, x, c->ncell);
+    CKL(c);
+    return VV_OK;
+}
+
+// V0 = b (first cycle) or b - A x (restart)
+int gm_cycle_head(vv_ctx* c, const double* b, const double* x, bool first) {
+    if (first) return copy_d(c, c->V, b, c->ncell);
+    TRY(apply_operator(c, x, c->V));
+    vv::k_axpby<double><<<grid1d(c->ncell, 256), 256, 0, c->st>>>(b, c->V, c->ncell, 1.0, -1.0);
+    CKL(c);
+    return VV_OK;
+}
+
+int gm_cycle_start(vv_ctx* c) {
+    vv::k_gm_cycle<double><<<c->npart, vv::RED_THREADS, 0, c->st>>>(c->ds, c->V, c->ncell, c->part);
+    CKL(c);
+    vv::k_gm_scale<double><<<grid1d(c->ncell, 256), 256, 0, c->st>>>(c->ds, c->V, c->ncell, c->ncell);
+    CKL(c);
+    return VV_OK;
+}
+
+int gm_arnoldi(vv_ctx* c) {
+    TRY(apply_operator_state(c));
+    vv::k_gm_mdot<double><<<c->npart, vv::RED_THREADS, 0, c->st>>>(c->ds, c->V, c->ncell, c->ncell, c->part,
+                                                                   c->npart_max);
+    CKL(c);
+    vv::k_gm_maxpy<double><<<c->npart, vv::RED_THREADS, 0, c->st>>>(c->ds, c->V, c->ncell, c->ncell, c->part);
+    CKL(c);
+    vv::k_gm_scale<double><<<grid1d(c->ncell, 256), 256, 0, c->st>>>(c->ds, c->V, c->ncell, c->ncell);
+    CKL(c);
+    return VV_OK;
+}
+
+int gm_finish(vv_ctx* c, double* x) {
+    vv::k_gm_finish<double><<<c->npart, vv::RED_THREADS, 0, c->st>>>(c->ds, c->V, c->ncell, x, c->ncell);
+    CKL(c);
+    return VV_OK;
+}
+
+struct GmHead {
+    int it, its, reason, active;
+};
+
+int read_head(vv_ctx* c, GmHead* h) {
+    CK(cudaMemcpyAsync(c->hstat, c->ds, sizeof(GmHead), cudaMemcpyDeviceToHost, c->st));
+    CK(cudaStreamSynchronize(c->st));
+    std::memcpy(h, c->hstat, sizeof(GmHead));
+    return VV_OK;
+}
+
+// Host-driven GMRES: the same kernels, with the host reading the 16-byte
+// status block after every Arnoldi step.
+int gmres_host(vv_ctx* c, const double* b, double* x, vv_ksp_result* res) {
+    TRY(gm_init(c, x));
+    bool first = true;
+    GmHead h{};
+    for (;;) {
+        TRY(gm_cycle_head(c, b, x, first));
+        TRY(gm_cycle_start(c));
+        TRY(read_head(c, &h));
+        while (h.active) {
+            TRY(gm_arnoldi(c));
+            TRY(read_head(c, &h));
+        }
+        TRY(gm_finish(c, x));
+        TRY(read_head(c, &h));
+        if (h.reason != 0) break;
+        first = false;
+    }
+    if (res) {
+        double rn = 0.0;
+        TRY(read_scalar(c, &c->ds->res, &rn));
+        res->its = h.its;
+        res->reason = h.reason;
+        res->rnorm = rn;
+    }
+    return VV_OK;
+}
+
+// ---- graph capture helpers ----------------------------------------------------
+// Add a conditional node at the current position of the capture on `cs`;
+// its handle is created on the top-level graph `owner` (handles may serve
+// conditional nodes of child graphs) with a default applied at every launch.
+int add_conditional(cudaGraph_t owner, cudaStream_t cs, cudaGraphConditionalNodeType type, unsigned size,
+                    unsigned defval, unsigned long long* handle_out, cudaGraph_t* bodies) {
+    cudaStreamCaptureStatus status;
+    const cudaGraphNode_t* deps = nullptr;
+    size_t nd = 0;
+    cudaGraph_t g = nullptr;
+    CK(cudaStreamGetCaptureInfo(cs, &status, nullptr, &g, &deps, &nd));
+    if (status != cudaStreamCaptureStatusActive) return VV_ERR_CUDA;
+    cudaGraphConditionalHandle h;
+    CK(cudaGraphConditionalHandleCreate(&h, owner, defval, cudaGraphCondAssignDefault));
+    cudaGraphNodeParams prm = {cudaGraphNodeTypeConditional};
+    prm.conditional.handle = h;
+    prm.conditional.type = type;
+    prm.conditional.size = size;
+    cudaGraphNode_t node;
+    CK(cudaGraphAddNode(&node, g, deps, nd, &prm));
+    for (unsigned k = 0; k < size; ++k) bodies[k] = prm.conditional.phGraph_out[k];
+    CK(cudaStreamUpdateCaptureDependencies(cs, &node, 1, cudaStreamSetCaptureDependencies));
+    *handle_out = (unsigned long long)h;
+    return VV_OK;
+}
+
+// Capture `fn` into `body` on capture stream `s`, with c->st pointing at it.
+template <typename F>
+int capture_body(vv_ctx* c, cudaStream_t s, cudaGraph_t body, int* nkernels, F fn) {
+    const cudaStream_t saved = c->st;
+    const int64_t l0 = c->launches;
+    CK(cudaStreamBeginCaptureToGraph(s, body, nullptr, nullptr, 0, cudaStreamCaptureModeRelaxed));
+    c->st = s;
+    int r = fn();
+    c->st = saved;
+    cudaGraph_t out = nullptr;
+    cudaError_t e = cudaStreamEndCapture(s, &out);
+    if (r != VV_OK) return r;
+    if (e != cudaSuccess) return fail_cuda(e, "cudaStreamEndCapture");
+    if (nkernels) *nkernels = (int)(c->launches - l0);
+    return VV_OK;
+}
+
+// GMRES solve b -> x into the graph being captured on cs[level]
+int capture_gmres(vv_ctx* c, int level, const double* b, double* x) {
+    TRY(gm_init(c, x));
+    cudaGraph_t outer[1];
+    TRY(add_conditional(c->step_graph, c->cs[level], cudaGraphCondTypeWhile, 1, 1, &c->hnd[0], outer));
+    const int l1 = level + 1;
+    return capture_body(c, c->cs[l1], outer[0], &c->nk_cycle, [&]() -> int {
+        cudaGraph_t br[2];
+        TRY(add_conditional(c->step_graph, c->cs[l1], cudaGraphCondTypeIf, 2, 1, &c->hnd[2], br));
+        TRY(capture_body(c, c->cs[l1 + 1], br[0], nullptr, [&]() { return gm_cycle_head(c, b, x, true); }));
+        TRY(capture_body(c, c->cs[l1 + 1], br[1], &c->nk_restart, [&]() { return gm_cycle_head(c, b, x, false); }));
+        TRY(gm_cycle_start(c));
+        cudaGraph_t inner[1];
+        TRY(add_conditional(c->step_graph, c->cs[l1], cudaGraphCondTypeWhile, 1, 0, &c->hnd[1], inner));
+        TRY(capture_body(c, c->cs[l1 + 1], inner[0], &c->nk_arnoldi, [&]() { return gm_arnoldi(c); }));
+        return gm_finish(c, x);
+    });
+}
+
+// ---- residual / moments helpers of the step ---------------------------------
 int residual_norm(vv_ctx* c, const double* F, double* Y, double* out) {
-    const int tiles = bracket_tiles(c);
+    const int tiles = bracket_tiles(c, F, c->Fh, Y);
     TRY(launch_bracket<vv::MODE_RESIDUAL>(c, F, c->Fh, Y, 1.0, c->part));
     TRY(reduce_to(c, c->part, tiles, c->scal + 2));
     double s2 = 0.0;
@@ -440,6 +569,115 @@ int calc_residual(vv_ctx* c, vv_state* st, double* out) {
 
 int calc_moments(vv_ctx* c, vv_state* st) {
     return moments_poisson(c, st->f, st->n, st->u, st->e, st->a, st->phi, st->h1c, c->scal);
+}
+
+// residual of f into tmp + tile partials, Poisson residual into ds->pnorm2,
+// then the Picard decision kernel (phase 0: initial residual)
+int step_residual(vv_ctx* c, vv_state* st, int phase) {
+    const int tiles = bracket_tiles(c, st->f, c->Fh, c->tmp);
+    TRY(launch_bracket<vv::MODE_RESIDUAL>(c, st->f, c->Fh, c->tmp, 1.0, c->part));
+    TRY(poisson_apply(c, st->phi, st->n, nullptr, 2, &c->ds->pnorm2));
+    vv::k_pic_residual<<<1, 32, 0, c->st>>>(c->ds, c->part, tiles, phase);
+    CKL(c);
+    return VV_OK;
+}
+
+// make_history + update_previous + initial residual
+int step_prologue(vv_ctx* c, vv_state* st) {
+    const size_t n = c->ncell;
+    const int nx = c->nx;
+    TRY(copy_d(c, st->fh, st->f, n));
+    TRY(copy_d(c, st->h1h, st->h1c, nx));
+    if (st->h2c && st->h2h) TRY(copy_d(c, st->h2h, st->h2c, nx));
+    if (st->phih) TRY(copy_d(c, st->phih, st->phi, nx));
+    TRY(copy_d(c, c->Fh, st->f, n));
+    TRY(set_hxp(c, st->h1c, st->h1h, st->h2c, st->h2h));
+    return step_residual(c, st, 0);
+}
+
+// the preconditioned right-hand side of the ksponly solve: b = P^-1 R(f),
+// with R(f) left in tmp by the last residual evaluation (same Fh and Have)
+int step_rhs(vv_ctx* c, vv_state* st) {
+    TRY(copy_d(c, c->fl, st->f, c->ncell));
+    if (c->g.preconditioner == VV_PC_TENSOR_KINETIC) return pc_apply(c, c->tmp, c->bvec);
+    return copy_d(c, c->bvec, c->tmp, c->ncell);
+}
+
+int step_after_solve(vv_ctx* c, vv_state* st) {
+    vv::k_pic_apply<double><<<grid1d(c->ncell, 256), 256, 0, c->st>>>(c->ds, c->delta, st->f, c->ncell);
+    CKL(c);
+    TRY(calc_moments(c, st));
+    TRY(copy_d(c, c->hxp, st->h1c, c->nx));   // update_previous: H1p <- h1c
+    return step_residual(c, st, 1);
+}
+
+int step_revert(vv_ctx* c, vv_state* st) {
+    TRY(copy_d(c, st->f, c->fl, c->ncell));
+    return calc_moments(c, st);
+}
+
+bool same_state(const vv_state& a, const vv_state& b) { return std::memcmp(&a, &b, sizeof a) == 0; }
+
+void destroy_graph(vv_ctx* c) {
+    if (c->step_exec) cudaGraphExecDestroy(c->step_exec);
+    if (c->step_graph) cudaGraphDestroy(c->step_graph);
+    c->step_exec = nullptr;
+    c->step_graph = nullptr;
+}
+
+// Build the graph of one time step for the buffers in `st`.
+int build_step_graph(vv_ctx* c, vv_state* st) {
+    destroy_graph(c);
+    const int64_t launches0 = c->launches;
+    for (int k = 0; k < 4; ++k)
+        if (!c->cs[k]) CK(cudaStreamCreateWithFlags(&c->cs[k], cudaStreamNonBlocking));
+    CK(cudaGraphCreate(&c->step_graph, 0));
+    int r = capture_body(c, c->cs[0], c->step_graph, &c->nk_top, [&]() -> int {
+        TRY(step_prologue(c, st));
+        cudaGraph_t pic[1];
+        TRY(add_conditional(c->step_graph, c->cs[0], cudaGraphCondTypeWhile, 1, 0, &c->hnd[3], pic));
+        TRY(capture_body(c, c->cs[1], pic[0], &c->nk_pic, [&]() -> int {
+            TRY(step_rhs(c, st));
+            TRY(capture_gmres(c, 1, c->bvec, c->delta));
+            return step_after_solve(c, st);
+        }));
+        cudaGraph_t rev[1];
+        TRY(add_conditional(c->step_graph, c->cs[0], cudaGraphCondTypeIf, 1, 0, &c->hnd[4], rev));
+        return capture_body(c, c->cs[1], rev[0], &c->nk_revert, [&]() { return step_revert(c, st); });
+    });
+    if (r != VV_OK) {
+        destroy_graph(c);
+        return r;
+    }
+    c->launches = launches0;   // captured, not executed
+    cudaError_t e = cudaGraphInstantiate(&c->step_exec, c->step_graph, 0);
+    if (e != cudaSuccess) {
+        destroy_graph(c);
+        return fail_cuda(e, "cudaGraphInstantiate");
+    }
+    c->step_key = *st;
+    return VV_OK;
+}
+
+// Host-driven time step with the same kernel sequence.
+int step_host(vv_ctx* c, vv_state* st) {
+    TRY(step_prologue(c, st));
+    for (;;) {
+        TRY(step_rhs(c, st));
+        TRY(gmres_host(c, c->bvec, c->delta, nullptr));
+        TRY(step_after_solve(c, st));
+        int act = 0;
+        CK(cudaMemcpyAsync(c->hstat, &c->ds->pic_active, sizeof(int), cudaMemcpyDeviceToHost, c->st));
+        CK(cudaStreamSynchronize(c->st));
+        act = c->hstat[0];
+        if (!act) break;
+    }
+    int rev = 0;
+    CK(cudaMemcpyAsync(c->hstat, &c->ds->pic_revert, sizeof(int), cudaMemcpyDeviceToHost, c->st));
+    CK(cudaStreamSynchronize(c->st));
+    rev = c->hstat[0];
+    if (rev) TRY(step_revert(c, st));
+    return VV_OK;
 }
 
 }  // namespace
@@ -492,6 +730,10 @@ int vv_create(const vv_grid* grid, vv_ctx** out) {
     c->ncell = (size_t)g.nx * g.nv;
     c->st = 0;
     cudaGetDevice(&c->device);
+    {
+        const char* e = getenv("VV_GRAPH");
+        c->use_graph = !(e && e[0] == '0');
+    }
     // grid (run_base.py:133-137, Grid.pyx:40-48)
     c->hx = g.L / g.nx;
     c->hv = (g.vmax - g.vmin) / (g.nv - 1);
@@ -511,15 +753,18 @@ int vv_create(const vv_grid* grid, vv_ctx** out) {
     }
     c->mom_seg = 64;
     c->mom_S = (nv + c->mom_seg - 1) / c->mom_seg;
-    c->pcR = std::max(1, 4096 / nx);
-    if (c->pcR > 64) c->pcR = 64;
-    c->smem_rfft = (size_t)c->pcR * M * sizeof(double2);
-    c->smem_irfft = (size_t)c->pcR * (2 * M + 1) * sizeof(double2);
-    c->smem_tri = (size_t)nv * sizeof(double2);
+    // rows per CTA of the x-FFT kernels: enough CTAs for two waves on 148 SMs,
+    // >= 4 consecutive v rows per transposed write when nv allows
+    c->pcR = std::max(1, std::min(8, nv / 256));
+    while (c->pcR > 1 && (size_t)(M + c->pcR * (2 * M + 1)) * sizeof(double2) > 200 * 1024) c->pcR /= 2;
+    c->smem_rfft = (size_t)(M + c->pcR * M) * sizeof(double2);
+    c->smem_irfft = (size_t)(M + c->pcR * M + c->pcR * (M + 1)) * sizeof(double2);
+    c->tri_stage = (size_t)nv * 48 <= 200 * 1024;
+    c->smem_tri = c->tri_stage ? (size_t)nv * 48 : (size_t)nv * sizeof(double2);
     c->smem_pois = (size_t)M * sizeof(double2) + (size_t)nx * sizeof(double) + (size_t)(nx + 2) * sizeof(double);
 
     int s = VV_OK;
-    const int tiles = bracket_tiles(c);
+    const int tiles = ((nx + vv::BX - 1) / vv::BX) * ((nv + vv::BY - 1) / vv::BY);  // the largest grid
     const size_t part_count = std::max({(size_t)(vv::MAX_RESTART + 2) * c->npart_max, (size_t)tiles,
                                         (size_t)vv::INV_NPART * c->npart_max});
     if ((s = dalloc(&c->v, nv)) || (s = dalloc(&c->h0, nv)) || (s = dalloc(&c->hxp, 4 * (size_t)nx)) ||
@@ -529,11 +774,12 @@ int vv_create(const vv_grid* grid, vv_ctx** out) {
         (s = dalloc(&c->mom_part, (size_t)c->mom_S * 3 * nx)) || (s = dalloc(&c->spec, (size_t)nm * nv)) ||
         (s = dalloc(&c->tw, (size_t)std::max(1, nx / 2))) || (s = dalloc(&c->lambda, nm)) ||
         (s = dalloc(&c->dinv, (size_t)nm * nv)) || (s = dalloc(&c->alpha, nv)) || (s = dalloc(&c->gamma, nv)) ||
-        (s = dalloc(&c->sym_inv, nm)) || (s = dalloc(&c->gm, 1))) {
+        (s = dalloc(&c->sym_inv, nm)) || (s = dalloc(&c->ds, 1))) {
         vv_destroy(c);
         return s;
     }
-    if (cudaMallocHost((void**)&c->hpin, sizeof(vv::GmresState) + 256) != cudaSuccess ||
+    if (cudaMallocHost((void**)&c->hpin, 4096) != cudaSuccess ||
+        cudaMallocHost((void**)&c->hds, sizeof(vv::DevState)) != cudaSuccess ||
         cudaMallocHost((void**)&c->hstat, 64) != cudaSuccess) {
         vv_destroy(c);
         return VV_ERR_ALLOC;
@@ -614,7 +860,8 @@ int vv_create(const vv_grid* grid, vv_ctx** out) {
         cudaMemcpy(c->dinv, dinv.data(), dinv.size() * sizeof(double2), cudaMemcpyHostToDevice) != cudaSuccess ||
         cudaMemcpy(c->sym_inv, sym.data(), nm * sizeof(double), cudaMemcpyHostToDevice) != cudaSuccess ||
         cudaMemset(c->hxp, 0, 4 * (size_t)nx * sizeof(double)) != cudaSuccess ||
-        cudaMemset(c->Fh, 0, n * sizeof(double)) != cudaSuccess) {
+        cudaMemset(c->Fh, 0, n * sizeof(double)) != cudaSuccess ||
+        cudaMemset(c->ds, 0, sizeof(vv::DevState)) != cudaSuccess) {
         vv_destroy(c);
         return fail_cuda(cudaGetLastError(), "vv_create upload");
     }
@@ -623,7 +870,9 @@ int vv_create(const vv_grid* grid, vv_ctx** out) {
                              (int)c->smem_rfft) != cudaSuccess ||
         cudaFuncSetAttribute(vv::k_irfft_rows<double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              (int)c->smem_irfft) != cudaSuccess ||
-        cudaFuncSetAttribute(vv::k_tridiag_modes, cudaFuncAttributeMaxDynamicSharedMemorySize,
+        cudaFuncSetAttribute(vv::k_tridiag_modes<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)c->smem_tri) != cudaSuccess ||
+        cudaFuncSetAttribute(vv::k_tridiag_modes<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              (int)c->smem_tri) != cudaSuccess ||
         cudaFuncSetAttribute(vv::k_moments_poisson, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              (int)c->smem_pois) != cudaSuccess) {
@@ -638,7 +887,11 @@ int vv_destroy(vv_ctx* c) {
     if (!c) return VV_OK;
     void* bufs[] = {c->v, c->h0, c->hxp, c->Fh, c->tmp, c->bvec, c->delta, c->fl, c->V, c->part, c->scal,
                     c->xscratch, c->mom_part, c->spec, c->tw, c->lambda, c->dinv, c->alpha, c->gamma,
-                    c->sym_inv, c->gm};
+                    c->sym_inv, c->ds};
+    destroy_graph(c);
+    for (int k = 0; k < 4; ++k)
+        if (c->cs[k]) cudaStreamDestroy(c->cs[k]);
+    if (c->hds) cudaFreeHost(c->hds);
     for (void* p : bufs)
         if (p) cudaFree(p);
     if (c->hpin) cudaFreeHost(c->hpin);
@@ -740,7 +993,15 @@ int vv_poisson_solve(vv_ctx* c, const double* n, double* phi) {
 
 int vv_gmres(vv_ctx* c, const double* b, double* x, const vv_ksp_opts* o, vv_ksp_result* r) {
     if (!c || !b || !x || !o || !r) return VV_ERR_ARG;
-    return gmres(c, b, x, o, r);
+    const int restart = (o->restart > 0) ? o->restart : c->restart;
+    if (restart > c->restart || restart < 1 || o->max_it < 0) return VV_ERR_ARG;
+    const unsigned long long saved[5] = {c->hnd[0], c->hnd[1], c->hnd[2], c->hnd[3], c->hnd[4]};
+    for (auto& h : c->hnd) h = 0;   // host-driven: no conditional handles
+    int s = upload_options(c, o, nullptr);
+    for (int k = 0; k < 5; ++k) c->hnd[k] = saved[k];
+    TRY(s);
+    // b may alias nothing inside the context; run on the caller's buffers
+    return gmres_host(c, b, x, r);
 }
 
 int vv_calculate_moments(vv_ctx* c, vv_state* st) {
@@ -775,61 +1036,46 @@ int vv_run_init(vv_ctx* c, vv_state* st, int normalise) {
 int vv_step(vv_ctx* c, vv_state* st, const vv_snes_opts* so, const vv_ksp_opts* ko, vv_step_report* rep) {
     if (!c || !st || !so || !ko || !rep || !st->f || !st->fh || !st->phi || !st->h1c || !st->h1h || !st->n)
         return VV_ERR_ARG;
+    const int restart = (ko->restart > 0) ? ko->restart : c->restart;
+    if (restart > c->restart || restart < 1 || ko->max_it < 0 || so->max_iter < 1) return VV_ERR_ARG;
     std::memset(rep, 0, sizeof(*rep));
-    const size_t n = c->ncell;
-    const int nx = c->nx;
-    // make_history (run_base.py:749-763) + update_history (PETScVlasovSolver.pyx:135-140)
-    TRY(copy_d(c, st->fh, st->f, n));
-    TRY(copy_d(c, st->h1h, st->h1c, nx));
-    if (st->h2c && st->h2h) TRY(copy_d(c, st->h2h, st->h2c, nx));
-    if (st->phih) TRY(copy_d(c, st->phih, st->phi, nx));
-    TRY(copy_d(c, c->Fh, st->f, n));
-    // update_previous
-    TRY(set_hxp(c, st->h1c, st->h1h, st->h2c, st->h2h));
-    double pred = 0.0;
-    TRY(calc_residual(c, st, &pred));
-    rep->residual[0] = pred;
-    int i = 0;
-    for (;;) {
-        ++i;
-        TRY(copy_d(c, c->fl, st->f, n));
-        // snes ksponly: b = P^-1 R(f); GMRES; f -= delta unless the solve failed.
-        // calc_residual left R(f) -- evaluated with the same Fh and Have -- in tmp.
-        if (c->g.preconditioner == VV_PC_TENSOR_KINETIC) TRY(pc_apply(c, c->tmp, c->bvec));
-        else TRY(copy_d(c, c->bvec, c->tmp, n));
-        vv_ksp_result kr{};
-        TRY(gmres(c, c->bvec, c->delta, ko, &kr));
-        if (i - 1 < VV_MAX_PICARD) {
-            rep->gmres_its[i - 1] = kr.its;
-            rep->ksp_reason[i - 1] = kr.reason;
-        }
-        rep->gmres_its_total += kr.its;
-        if (kr.reason >= 0) {
-            vv::k_axpby<double><<<grid1d(n, 256), 256, 0, c->st>>>(c->delta, st->f, n, -1.0, 1.0);
-            CKL(c);
-        } else {
-            rep->ksp_failures++;
-        }
-        TRY(calc_moments(c, st));
-        TRY(set_hxp(c, st->h1c, st->h1h, st->h2c, st->h2h));
-        const double prev = pred;
-        TRY(calc_residual(c, st, &pred));
-        if (i < VV_MAX_PICARD + 1) rep->residual[i] = pred;
-        const bool rose = pred > prev && i > 1;
-        const bool small = pred < so->atol;
-        const bool maxed = i >= so->max_iter || i >= VV_MAX_PICARD;
-        if (rose || small || maxed) {
-            rep->stop_rule = rose ? 1 : (small ? 2 : 3);
-            if (pred > prev) {
-                TRY(copy_d(c, st->f, c->fl, n));
-                TRY(calc_moments(c, st));
-                rep->reverted = 1;
-            }
-            break;
-        }
+    if (c->use_graph) {
+        if (!c->step_exec || !same_state(c->step_key, *st)) TRY(build_step_graph(c, st));
+        TRY(upload_options(c, ko, so));
+        CK(cudaGraphLaunch(c->step_exec, c->st));
+    } else {
+        const unsigned long long saved[5] = {c->hnd[0], c->hnd[1], c->hnd[2], c->hnd[3], c->hnd[4]};
+        for (auto& h : c->hnd) h = 0;
+        int s = upload_options(c, ko, so);
+        for (int k = 0; k < 5; ++k) c->hnd[k] = saved[k];
+        TRY(s);
+        TRY(step_host(c, st));
     }
-    rep->picard_its = i;
+    // report
+    CK(cudaMemcpyAsync(c->hds, c->ds, sizeof(vv::DevState), cudaMemcpyDeviceToHost, c->st));
     CK(cudaStreamSynchronize(c->st));
+    const vv::DevState& d = *c->hds;
+    rep->picard_its = d.pic_i;
+    rep->gmres_its_total = d.gmres_total;
+    rep->reverted = d.pic_revert;
+    rep->stop_rule = d.pic_stop_rule;
+    rep->ksp_failures = d.ksp_failures;
+    const int np = std::min(d.pic_i, VV_MAX_PICARD);
+    for (int k = 0; k < np; ++k) {
+        rep->gmres_its[k] = d.gmres_its[k];
+        rep->ksp_reason[k] = d.ksp_reason[k];
+    }
+    for (int k = 0; k <= np; ++k) rep->residual[k] = d.residual[k];
+    if (c->use_graph) {
+        // kernels executed by the graph: top level + per Picard pass + per GMRES cycle/iteration
+        int64_t nk = c->nk_top - c->nk_pic - c->nk_revert;   // counted once at capture; re-add per execution
+        nk = (c->nk_top > 0) ? nk : 0;
+        const int64_t cycles = d.ncycles;
+        c->launches += nk + (int64_t)np * (c->nk_pic - c->nk_cycle) + cycles * (c->nk_cycle - c->nk_arnoldi - c->nk_restart)
+                       + (cycles - np) * c->nk_restart + (int64_t)d.gmres_total * c->nk_arnoldi
+                       + (d.pic_revert ? c->nk_revert : 0);
+    }
+    const double pred = d.pred;
     if (std::isnan(pred)) return VV_ERR_NAN;
     if (pred > so->abort_residual) {
         rep->aborted = 1;
@@ -886,6 +1132,52 @@ int vv_timing_read(vv_ctx* c, int64_t* launches, double* total_ms, int reset) {
         c->t_launches = 0;
         c->t_ms = 0.0;
     }
+    return VV_OK;
+}
+
+int vv_time_kernel(vv_ctx* c, int which, int reps, double* avg_ms) {
+    if (!c || !avg_ms || reps < 1 || reps > 100000 || which < 0 || which > 2) return VV_ERR_ARG;
+    for (int k = 0; k < 4; ++k)
+        if (!c->cs[k]) CK(cudaStreamCreateWithFlags(&c->cs[k], cudaStreamNonBlocking));
+    const cudaStream_t saved = c->st;
+    const int64_t l0 = c->launches;
+    cudaGraph_t g = nullptr;
+    CK(cudaStreamSynchronize(saved));
+    CK(cudaStreamBeginCapture(c->cs[0], cudaStreamCaptureModeRelaxed));
+    c->st = c->cs[0];
+    int r = VV_OK;
+    for (int k = 0; k < reps && r == VV_OK; ++k) {
+        if (which == 0) r = launch_bracket<vv::MODE_JVP>(c, c->V, nullptr, c->tmp, 0.5, nullptr);
+        else if (which == 1) r = launch_bracket<vv::MODE_RESIDUAL>(c, c->V, c->Fh, c->tmp, 1.0, nullptr);
+        else r = pc_apply(c, c->V, c->tmp);
+    }
+    c->st = saved;
+    cudaError_t e = cudaStreamEndCapture(c->cs[0], &g);
+    c->launches = l0;
+    if (r != VV_OK) {
+        if (g) cudaGraphDestroy(g);
+        return r;
+    }
+    if (e != cudaSuccess) return fail_cuda(e, "cudaStreamEndCapture");
+    cudaGraphExec_t ex = nullptr;
+    e = cudaGraphInstantiate(&ex, g, 0);
+    cudaGraphDestroy(g);
+    if (e != cudaSuccess) return fail_cuda(e, "cudaGraphInstantiate");
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    cudaGraphLaunch(ex, c->st);                    // warm-up
+    cudaEventRecord(e0, c->st);
+    cudaGraphLaunch(ex, c->st);
+    cudaEventRecord(e1, c->st);
+    e = cudaEventSynchronize(e1);
+    float ms = 0.f;
+    if (e == cudaSuccess) e = cudaEventElapsedTime(&ms, e0, e1);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    cudaGraphExecDestroy(ex);
+    if (e != cudaSuccess) return fail_cuda(e, "vv_time_kernel");
+    *avg_ms = (double)ms / reps;
     return VV_OK;
 }
 

@@ -33,6 +33,8 @@ struct BracketParams {
     double f2;       // hx_inv*hv_inv/24
     const double* h0;   // nv: 0.5 v^2 mass
     const double* hxp;  // 4*nx: h1p, h1h, h2p, h2h profiles
+    const int* xidx;    // optional: input is X + (*xidx) * xstride (GMRES basis vector)
+    size_t xstride;
 };
 
 constexpr int BX = 32;
@@ -103,6 +105,7 @@ template <int SCHEME, int MODE>
 __global__ void __launch_bounds__(BX * TY)
 k_bracket_ref(const double* __restrict__ X, const double* __restrict__ Xh,
               double* __restrict__ Y, BracketParams p, double* __restrict__ sumsq) {
+    if (p.xidx) X += (size_t)(*p.xidx) * p.xstride;
     __shared__ double sx[SY][SX + 1];
     __shared__ double sh[SY][SX + 1];
     __shared__ double sred[BX * TY / 32];
@@ -220,6 +223,7 @@ template <int SCHEME, int MODE, typename T>
 __global__ void __launch_bounds__(BX * TY)
 k_bracket_fac(const T* __restrict__ X, const T* __restrict__ Xh, T* __restrict__ Y,
               BracketParams p, double* __restrict__ sumsq) {
+    if (p.xidx) X += (size_t)(*p.xidx) * p.xstride;
     __shared__ T sx[SY][SX + 1];
     __shared__ double sa[SY];       // a(v) = h0 on the tile rows (with halo)
     __shared__ double sb[SX];       // b(x) on the tile columns (with halo)
@@ -308,6 +312,149 @@ k_bracket_fac(const T* __restrict__ X, const T* __restrict__ Xh, T* __restrict__
             y += tscale * s;
         }
 #undef XS
+        Y[g] = y;
+        acc2 += (double)y * (double)y;
+    }
+    if (sumsq) {
+        const double t = block_sum(acc2, sred);
+        if (tid == 0) sumsq[blockIdx.x + gridDim.x * blockIdx.y] = t;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Factored form, wide tiles: 64 (x) x 32 (v) outputs per CTA, 256 threads,
+// each thread one column and 8 consecutive rows (register window along v,
+// 6 shared-memory loads per output).  Staging uses 16-byte loads; the
+// periodic wrap is one conditional add/subtract.  Requires nx % 64 == 0 and
+// 16-byte aligned fields (checked by the launcher; otherwise k_bracket_fac).
+// ---------------------------------------------------------------------------
+constexpr int WX = 64;
+constexpr int WY = 32;
+constexpr int WR = 8;                 // rows per thread
+constexpr int WSX = WX + 4;           // 68
+constexpr int WSY = WY + 4;           // 36
+constexpr int WTHREADS = WX * (WY / WR);  // 256
+
+template <typename T> struct Vec2;
+template <> struct Vec2<double> { using type = double2; };
+template <> struct Vec2<float> { using type = float2; };
+
+template <int SCHEME, int MODE, typename T>
+__global__ void __launch_bounds__(WTHREADS)
+k_bracket_wide(const T* __restrict__ X, const T* __restrict__ Xh, T* __restrict__ Y,
+               BracketParams p, double* __restrict__ sumsq) {
+    if (p.xidx) X += (size_t)(*p.xidx) * p.xstride;
+    using V2 = typename Vec2<T>::type;
+    __shared__ __align__(16) T sx[WSY][WSX];
+    __shared__ double sa[WSY];
+    __shared__ double sb[WSX];
+    __shared__ double srow[WY][3];
+    __shared__ double scol[WX][3];
+    __shared__ double sred[WTHREADS / 32];
+    const int tid = threadIdx.x;
+    const int i0 = blockIdx.x * WX, j0 = blockIdx.y * WY;
+    const int nx = p.nx, nv = p.nv;
+    // ---- stage the input tile (x pairs) ----
+    constexpr int NP = WSX / 2;   // 34 pairs per row
+    for (int q = tid; q < NP * WSY; q += WTHREADS) {
+        const int ly = q / NP, px = q - ly * NP;
+        int gi = i0 - 2 + 2 * px;
+        if (gi < 0) gi += nx;
+        else if (gi >= nx) gi -= nx;
+        const int gj = j0 - 2 + ly;
+        V2 v;
+        v.x = T(0); v.y = T(0);
+        if (gj >= 0 && gj < nv) {
+            const size_t g = (size_t)gj * nx + gi;
+            const V2 a = *reinterpret_cast<const V2*>(X + g);
+            if (MODE == MODE_RESIDUAL) {
+                const V2 b = *reinterpret_cast<const V2*>(Xh + g);
+                v.x = T(0.5) * b.x + T(0.5) * a.x;
+                v.y = T(0.5) * b.y + T(0.5) * a.y;
+            } else {
+                v = a;
+            }
+        }
+        *reinterpret_cast<V2*>(&sx[ly][2 * px]) = v;
+    }
+    if (tid < WSY) {
+        const int gj = j0 - 2 + tid;
+        sa[tid] = (gj >= 0 && gj < nv) ? p.h0[gj] : 0.0;
+    } else if (tid >= 64 && tid < 64 + WSX) {
+        const int l = tid - 64;
+        int gi = i0 - 2 + l;
+        if (gi < 0) gi += nx;
+        else if (gi >= nx) gi -= nx;
+        sb[l] = b_fac(p, gi);
+    }
+    __syncthreads();
+    if (tid < WY) {
+        const int l = tid + 2;
+        double am, ap;
+        Coef<SCHEME>::row(sa[l] - sa[l - 1], sa[l + 1] - sa[l], sa[l + 1] - sa[l - 1], sa[l] - sa[l - 2],
+                          sa[l + 2] - sa[l], am, ap);
+        srow[tid][0] = sa[l + 1] - sa[l - 1];
+        srow[tid][1] = am;
+        srow[tid][2] = ap;
+    } else if (tid >= 64 && tid < 64 + WX) {
+        const int c = tid - 64, l = c + 2;
+        double bm, bp;
+        Coef<SCHEME>::col(sb[l] - sb[l - 1], sb[l + 1] - sb[l], sb[l + 1] - sb[l - 1], sb[l] - sb[l - 2],
+                          sb[l + 2] - sb[l], bm, bp);
+        scol[c][0] = sb[l + 1] - sb[l - 1];
+        scol[c][1] = bm;
+        scol[c][2] = bp;
+    }
+    __syncthreads();
+    // ---- compute: column tx, rows ty*8 .. ty*8+7 ----
+    const int tx = tid & (WX - 1), ty = tid / WX;
+    const int lx = tx + 2;
+    const int r0 = ty * WR;            // tile row of the first output
+    const int i = i0 + tx;
+    T c0[WR + 4], cm1[WR + 2], cp1[WR + 2], cm2[WR], cp2[WR];
+#pragma unroll
+    for (int k = 0; k < WR + 4; ++k) c0[k] = sx[r0 + k][lx];
+#pragma unroll
+    for (int k = 0; k < WR + 2; ++k) { cm1[k] = sx[r0 + 1 + k][lx - 1]; cp1[k] = sx[r0 + 1 + k][lx + 1]; }
+#pragma unroll
+    for (int k = 0; k < WR; ++k) { cm2[k] = sx[r0 + 2 + k][lx - 2]; cp2[k] = sx[r0 + 2 + k][lx + 2]; }
+    const T B1 = T(scol[tx][0]), bm = T(scol[tx][1]), bp = T(scol[tx][2]);
+    const T tscale = T(((SCHEME == 2) ? p.f2 : p.f1) * p.factor);
+    const T htinv = T(p.ht_inv);
+    double acc2 = 0.0;
+#pragma unroll
+    for (int q = 0; q < WR; ++q) {
+        const int j = j0 + r0 + q;
+        if (j >= nv) break;
+        const size_t g = (size_t)j * nx + i;
+        const T xc = c0[q + 2];
+        T y;
+        if (MODE == MODE_JVP) y = htinv * xc;
+        else if (MODE == MODE_RESIDUAL) y = htinv * (X[g] - Xh[g]);
+        else y = Y[g];
+        if (j >= 2 && j < nv - 2) {
+            const T A1 = T(srow[r0 + q][0]), am = T(srow[r0 + q][1]), ap = T(srow[r0 + q][2]);
+            // neighbours: (di, dj)
+            const T xm1m1 = cm1[q], xm1p1 = cm1[q + 2], xp1m1 = cp1[q], xp1p1 = cp1[q + 2];
+            T s = T(0);
+            if (Coef<SCHEME>::cA1 != 0.0 || Coef<SCHEME>::cA2 != 0.0) {
+                T ax = T(0), bx = T(0);
+                if (Coef<SCHEME>::cA1 != 0.0) {
+                    ax = T(Coef<SCHEME>::cA1) * (cp1[q + 1] - cm1[q + 1]);
+                    bx = T(Coef<SCHEME>::cB1) * (c0[q + 3] - c0[q + 1]);
+                }
+                if (Coef<SCHEME>::cA2 != 0.0) {
+                    ax += T(Coef<SCHEME>::cA2) * (cp2[q] - cm2[q]);
+                    bx += T(Coef<SCHEME>::cB2) * (c0[q + 4] - c0[q]);
+                }
+                s = A1 * ax - B1 * bx;
+            }
+            s += am * (xm1m1 - xp1m1);
+            s += ap * (xm1p1 - xp1p1);
+            s += bm * (xm1m1 - xm1p1);
+            s += bp * (xp1m1 - xp1p1);
+            y += tscale * s;
+        }
         Y[g] = y;
         acc2 += (double)y * (double)y;
     }

@@ -13,34 +13,49 @@ constexpr int MAX_RESTART = 64;
 constexpr int MDOT_CHUNK = 8;
 
 // ---------------------------------------------------------------------------
-// GMRES state (device resident).  Mirrors the arrays of PETSc's KSP_GMRES:
-// hh (rotated Hessenberg, column-major with ld = restart+2), grs (rotated
-// right-hand side), cc/ss (Givens), plus the KSPConvergedDefault state.
+// Device-resident solver state: GMRES (PETSc KSP_GMRES arrays: hh = rotated
+// Hessenberg, column-major with ld = restart+2; grs = rotated right-hand side;
+// cc/ss = Givens; KSPConvergedDefault state) and the Picard loop of the time
+// step, plus the step report.  Every loop decision is taken here, so a whole
+// time step can run as one CUDA graph with conditional nodes; when a
+// conditional handle is 0 the kernels run outside a graph (host-driven).
 // ---------------------------------------------------------------------------
-struct GmresState {
-    int it;          // Arnoldi index within the current cycle
-    int its;         // total iterations (ksp->its)
-    int reason;      // KSPConvergedReason
-    int active;      // 1 while the cycle continues
-    int restart, max_it;
-    int cycle_start; // 1 on the first call of a cycle
-    int pad;
+constexpr int MAX_PICARD_DEV = 64;
+
+struct DevState {
+    // GMRES control
+    int it, its, reason, active;
+    int restart, max_it, first, pad;
+    unsigned int cnt[4];   // last-CTA counters: 0 cycle sumsq, 1 mdot, 2 maxpy, 3 spare
     double rtol, atol, dtol, haptol;
-    double rnorm0, ttol, res;
-    double scale;    // reciprocal norm used by the next normalisation
-    double sumsq;    // reduced sum of squares
-    double hcol[MAX_RESTART + 2];  // <w, v_j> of the current column
+    double rnorm0, ttol, res, scale, sumsq;
+    // Picard control
+    int pic_i, pic_stop, pic_revert, pic_stop_rule;
+    int pic_max_iter, ksp_failures, gmres_total, pic_active;
+    int ncycles, pad2;
+    double snes_atol, abort_residual, pred, prev, pnorm2;
+    // conditional handles (0 outside a graph)
+    unsigned long long h_gm_outer, h_gm_inner, h_gm_first, h_pic, h_revert;
+    // report
+    int gmres_its[MAX_PICARD_DEV];
+    int ksp_reason[MAX_PICARD_DEV];
+    double residual[MAX_PICARD_DEV + 1];
+    // GMRES arrays
+    double hcol[MAX_RESTART + 2];
     double grs[MAX_RESTART + 2];
     double cc[MAX_RESTART + 1], ss[MAX_RESTART + 1];
     double hh[(MAX_RESTART + 2) * (MAX_RESTART + 1)];
-    double nrs[MAX_RESTART + 1];
 };
 
 // PETSc reasons
 constexpr int R_ITERATING = 0, R_RTOL = 2, R_ATOL = 3, R_NULL = -2, R_ITS = -3, R_DTOL = -4,
               R_BREAKDOWN = -5, R_NANORINF = -9;
 
-VV_DEV int ksp_converged(GmresState* s, int n, double rnorm) {
+VV_DEV void set_cond(unsigned long long h, unsigned int v) {
+    if (h) cudaGraphSetConditional((cudaGraphConditionalHandle)h, v);
+}
+
+VV_DEV int ksp_converged(DevState* s, int n, double rnorm) {
     if (n == 0) {
         s->rnorm0 = rnorm;
         s->ttol = fmax(s->rtol * rnorm, s->atol);
@@ -51,7 +66,31 @@ VV_DEV int ksp_converged(GmresState* s, int n, double rnorm) {
     return R_ITERATING;
 }
 
-// ----- partial sums of squares --------------------------------------------
+// Last-CTA election (threadfence reduction): true in every thread of the
+// block that finishes last; that block also resets the counter.  No waiting.
+__device__ __forceinline__ bool last_block(unsigned int* counter) {
+    __shared__ bool am_last;
+    __threadfence();
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        const unsigned int t = atomicAdd(counter, 1u);
+        am_last = (t == gridDim.x - 1);
+        if (am_last) *counter = 0u;
+    }
+    __syncthreads();
+    if (am_last) __threadfence();
+    return am_last;
+}
+
+// deterministic sum of part[0..np) by one warp
+__device__ __forceinline__ double warp_reduce_parts(const double* part, int np) {
+    const int lane = threadIdx.x & 31;
+    double a = 0.0;
+    for (int b = lane; b < np; b += 32) a += __ldcg(part + b);
+    return warp_sum(a);
+}
+
+// ----- partial sums of squares / sums --------------------------------------
 template <typename T>
 __global__ void __launch_bounds__(RED_THREADS)
 k_sumsq_partial(const T* __restrict__ x, size_t n, double* __restrict__ part) {
@@ -79,61 +118,10 @@ k_sum_partial(const T* __restrict__ x, size_t n, double* __restrict__ part) {
 // Reduce `np` partials per column (m columns, stride ld) into out[m].
 __global__ void __launch_bounds__(RED_THREADS)
 k_reduce_cols(const double* __restrict__ part, int np, int m, int ld, double* __restrict__ out) {
-    __shared__ double sh[RED_THREADS / 32];
-    for (int q = 0; q < m; ++q) {
-        double acc = 0.0;
-        for (int b = threadIdx.x; b < np; b += RED_THREADS) acc += part[(size_t)q * ld + b];
-        const double t = block_sum(acc, sh);
-        if (threadIdx.x == 0) out[q] = t;
-        __syncthreads();
-    }
-}
-
-// ----- multi-dot: part[q*ld + b] = sum_{block b} w * V_q, q in [q0, q0+CH) -----
-template <typename T>
-__global__ void __launch_bounds__(RED_THREADS)
-k_mdot_partial(const T* __restrict__ w, const T* __restrict__ V, size_t ldv, int q0, int m,
-               size_t n, double* __restrict__ part, int ld) {
-    __shared__ double sh[RED_THREADS / 32];
-    double acc[MDOT_CHUNK];
-#pragma unroll
-    for (int c = 0; c < MDOT_CHUNK; ++c) acc[c] = 0.0;
-    const int cnt = min(MDOT_CHUNK, m - q0);
-    for (size_t i = blockIdx.x * (size_t)RED_THREADS + threadIdx.x; i < n; i += (size_t)gridDim.x * RED_THREADS) {
-        const double wi = (double)w[i];
-#pragma unroll
-        for (int c = 0; c < MDOT_CHUNK; ++c)
-            if (c < cnt) acc[c] += wi * (double)V[(size_t)(q0 + c) * ldv + i];
-    }
-#pragma unroll
-    for (int c = 0; c < MDOT_CHUNK; ++c) {
-        if (c < cnt) {
-            const double t = block_sum(acc[c], sh);
-            if (threadIdx.x == 0) part[(size_t)(q0 + c) * ld + blockIdx.x] = t;
-        }
-    }
-}
-
-// ----- w += sum_q coef[q] * V_q  (coef read from device), plus ||w||^2 partials
-// sign = -1 uses -hcol (Gram-Schmidt), +1 uses nrs (solution update)
-template <typename T>
-__global__ void __launch_bounds__(RED_THREADS)
-k_maxpy(T* __restrict__ w, const T* __restrict__ V, size_t ldv, int m, const double* __restrict__ coef,
-        double sign, size_t n, double* __restrict__ part) {
-    __shared__ double sh[RED_THREADS / 32];
-    __shared__ double cf[MAX_RESTART + 2];
-    for (int q = threadIdx.x; q < m; q += RED_THREADS) cf[q] = sign * coef[q];
-    __syncthreads();
-    double acc = 0.0;
-    for (size_t i = blockIdx.x * (size_t)RED_THREADS + threadIdx.x; i < n; i += (size_t)gridDim.x * RED_THREADS) {
-        double wi = (double)w[i];
-        for (int q = 0; q < m; ++q) wi += cf[q] * (double)V[(size_t)q * ldv + i];
-        w[i] = (T)wi;
-        acc += wi * wi;
-    }
-    if (part) {
-        const double t = block_sum(acc, sh);
-        if (threadIdx.x == 0) part[blockIdx.x] = t;
+    const int w = threadIdx.x >> 5;
+    for (int q = w; q < m; q += RED_THREADS / 32) {
+        const double t = warp_reduce_parts(part + (size_t)q * ld, np);
+        if ((threadIdx.x & 31) == 0) out[q] = t;
     }
 }
 
@@ -153,11 +141,41 @@ __global__ void k_axpby(const T* __restrict__ x, T* __restrict__ y, size_t n, do
         y[i] = (T)(a * (double)x[i] + b * (double)y[i]);
 }
 
-// ----- GMRES bookkeeping (single thread) ----------------------------------
-// Cycle start: res = sqrt(sumsq) of the initial residual (KSPGMRESCycle top).
-__global__ void k_gmres_cycle_start(GmresState* s) {
+// ----- GMRES kernels (state driven) ----------------------------------------
+// Start of a solve: x = 0; its = 0; first cycle.
+template <typename T>
+__global__ void k_gm_init(DevState* s, T* __restrict__ x, size_t n) {
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
+        x[i] = T(0);
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        s->its = 0;
+        s->reason = R_ITERATING;
+        s->first = 1;
+        s->active = 0;
+        s->it = 0;
+        set_cond(s->h_gm_first, 1u);
+    }
+}
+
+// Cycle start (KSPGMRESCycle top): ||V0||^2 partials; the last CTA computes
+// res, the convergence test with n = its, the scale 1/res and `active`.
+template <typename T>
+__global__ void __launch_bounds__(RED_THREADS)
+k_gm_cycle(DevState* s, const T* __restrict__ V0, size_t n, double* __restrict__ part) {
+    __shared__ double sh[RED_THREADS / 32];
+    double acc = 0.0;
+    for (size_t i = blockIdx.x * (size_t)RED_THREADS + threadIdx.x; i < n; i += (size_t)gridDim.x * RED_THREADS) {
+        const double v = (double)V0[i];
+        acc += v * v;
+    }
+    const double t = block_sum(acc, sh);
+    if (threadIdx.x == 0) part[blockIdx.x] = t;
+    if (!last_block(&s->cnt[0])) return;
+    if (threadIdx.x >= 32) return;
+    const double ss2 = warp_reduce_parts(part, gridDim.x);
     if (threadIdx.x != 0) return;
-    const double res = sqrt(s->sumsq);
+    const double res = sqrt(ss2);
+    s->ncycles += 1;
     s->it = 0;
     s->grs[0] = res;
     s->res = res;
@@ -165,22 +183,65 @@ __global__ void k_gmres_cycle_start(GmresState* s) {
     if (res == 0.0) {
         s->reason = R_ATOL;
         s->active = 0;
-        return;
+    } else {
+        s->reason = ksp_converged(s, s->its, res);
+        s->active = (s->reason == R_ITERATING && s->its < s->max_it) ? 1 : 0;
     }
-    s->reason = ksp_converged(s, s->its, res);
-    s->active = (s->reason == R_ITERATING && s->its < s->max_it) ? 1 : 0;
+    set_cond(s->h_gm_inner, (unsigned)s->active);
 }
 
-// After w = A v_it, hcol = <w, v_j>, w -= sum hcol_j v_j and sumsq = ||w||^2:
-// the rest of one Arnoldi step (KSPGMRESCycle body + KSPGMRESUpdateHessenberg).
-__global__ void k_gmres_arnoldi(GmresState* s) {
-    if (threadIdx.x != 0 || !s->active) return;
+// V[idx] *= scale, idx = s->it (the vector just produced)
+template <typename T>
+__global__ void k_gm_scale(DevState* s, T* __restrict__ V, size_t ldv, size_t n) {
+    T* v = V + (size_t)s->it * ldv;
+    const double sc = s->scale;
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
+        v[i] = (T)((double)v[i] * sc);
+}
+
+// hcol_q = <w, V_q>, q = 0..it, w = V[it+1]  (one multi-dot, last CTA reduces)
+template <typename T>
+__global__ void __launch_bounds__(RED_THREADS)
+k_gm_mdot(DevState* s, const T* __restrict__ V, size_t ldv, size_t n, double* __restrict__ part, int ld) {
+    __shared__ double sh[RED_THREADS / 32];
+    const int it = s->it;
+    const int m = it + 1;
+    const T* w = V + (size_t)(it + 1) * ldv;
+    for (int q0 = 0; q0 < m; q0 += MDOT_CHUNK) {
+        double acc[MDOT_CHUNK];
+#pragma unroll
+        for (int c = 0; c < MDOT_CHUNK; ++c) acc[c] = 0.0;
+        const int cnt = min(MDOT_CHUNK, m - q0);
+        for (size_t i = blockIdx.x * (size_t)RED_THREADS + threadIdx.x; i < n;
+             i += (size_t)gridDim.x * RED_THREADS) {
+            const double wi = (double)w[i];
+#pragma unroll
+            for (int c = 0; c < MDOT_CHUNK; ++c)
+                if (c < cnt) acc[c] += wi * (double)V[(size_t)(q0 + c) * ldv + i];
+        }
+#pragma unroll
+        for (int c = 0; c < MDOT_CHUNK; ++c) {
+            if (c < cnt) {
+                const double t = block_sum(acc[c], sh);
+                if (threadIdx.x == 0) part[(size_t)(q0 + c) * ld + blockIdx.x] = t;
+            }
+        }
+    }
+    if (!last_block(&s->cnt[1])) return;
+    const int wid = threadIdx.x >> 5;
+    for (int q = wid; q < m; q += RED_THREADS / 32) {
+        const double t = warp_reduce_parts(part + (size_t)q * ld, gridDim.x);
+        if ((threadIdx.x & 31) == 0) s->hcol[q] = t;
+    }
+}
+
+// Arnoldi bookkeeping after tt = ||w|| (KSPGMRESCycle + UpdateHessenberg)
+VV_DEV void gm_arnoldi(DevState* s, double tt) {
     const int it = s->it;
     const int ld = s->restart + 2;
     double* hh = s->hh;
 #define HH(a, b) hh[(b) * ld + (a)]
     for (int j = 0; j <= it; ++j) HH(j, it) = s->hcol[j];
-    const double tt = sqrt(s->sumsq);
     s->scale = (tt != 0.0) ? 1.0 / tt : 1.0;
     HH(it + 1, it) = tt;
     double hapbnd = fabs(tt / s->grs[it]);
@@ -216,36 +277,148 @@ __global__ void k_gmres_arnoldi(GmresState* s) {
         if (hapend && s->reason == R_ITERATING) s->reason = R_BREAKDOWN;
     }
     s->active = (s->reason == R_ITERATING && s->it < s->restart && s->its < s->max_it) ? 1 : 0;
+    set_cond(s->h_gm_inner, (unsigned)s->active);
 }
 
-// KSPGMRESBuildSoln: back substitution into nrs; sets s->pad = number of
-// coefficients to apply (0 when nothing to add).
-__global__ void k_gmres_backsub(GmresState* s) {
-    if (threadIdx.x != 0) return;
-    const int last = s->it - 1;
-    const int ld = s->restart + 2;
-    const double* hh = s->hh;
+// w += sum_q (-hcol_q) V_q and ||w||^2 (classical Gram-Schmidt update,
+// VecMAXPY with lhh = -<w,v>); the last CTA finishes the Arnoldi step.
+template <typename T>
+__global__ void __launch_bounds__(RED_THREADS)
+k_gm_maxpy(DevState* s, T* __restrict__ V, size_t ldv, size_t n, double* __restrict__ part) {
+    __shared__ double sh[RED_THREADS / 32];
+    __shared__ double cf[MAX_RESTART + 2];
+    const int it = s->it;
+    const int m = it + 1;
+    T* w = V + (size_t)(it + 1) * ldv;
+    for (int q = threadIdx.x; q < m; q += RED_THREADS) cf[q] = -s->hcol[q];
+    __syncthreads();
+    double acc = 0.0;
+    for (size_t i = blockIdx.x * (size_t)RED_THREADS + threadIdx.x; i < n; i += (size_t)gridDim.x * RED_THREADS) {
+        double wi = (double)w[i];
+        for (int q = 0; q < m; ++q) wi += cf[q] * (double)V[(size_t)q * ldv + i];
+        w[i] = (T)wi;
+        acc += wi * wi;
+    }
+    const double t = block_sum(acc, sh);
+    if (threadIdx.x == 0) part[blockIdx.x] = t;
+    if (!last_block(&s->cnt[2])) return;
+    if (threadIdx.x >= 32) return;
+    const double ss2 = warp_reduce_parts(part, gridDim.x);
+    if (threadIdx.x == 0) gm_arnoldi(s, sqrt(ss2));
+}
+
+// KSPGMRESBuildSoln: every CTA solves the small triangular system (thread 0,
+// into shared memory) and updates its share of x += sum nrs_q V_q; CTA 0
+// records the outcome and decides whether another cycle follows.
+template <typename T>
+__global__ void __launch_bounds__(RED_THREADS)
+k_gm_finish(DevState* s, const T* __restrict__ V, size_t ldv, T* __restrict__ x, size_t n) {
+    __shared__ double nrs[MAX_RESTART + 1];
+    __shared__ int npad, breakdown;
+    if (threadIdx.x == 0) {
+        const int last = s->it - 1;
+        const int ld = s->restart + 2;
+        const double* hh = s->hh;
 #define HH(a, b) hh[(b) * ld + (a)]
-    s->pad = 0;
-    if (last < 0) return;
-    if (HH(last, last) == 0.0) {
-        s->reason = R_BREAKDOWN;
+        npad = 0;
+        breakdown = 0;
+        if (last >= 0) {
+            if (HH(last, last) == 0.0) {
+                breakdown = 1;
+            } else {
+                nrs[last] = s->grs[last] / HH(last, last);
+                for (int ii = 1; ii <= last && !breakdown; ++ii) {
+                    const int k = last - ii;
+                    double t = s->grs[k];
+                    for (int j = k + 1; j <= last; ++j) t = t - HH(k, j) * nrs[j];
+                    if (HH(k, k) == 0.0) breakdown = 1;
+                    else nrs[k] = t / HH(k, k);
+                }
+                if (!breakdown) npad = last + 1;
+            }
+        }
+#undef HH
+    }
+    __syncthreads();
+    const int m = npad;
+    if (m > 0) {
+        for (size_t i = blockIdx.x * (size_t)RED_THREADS + threadIdx.x; i < n;
+             i += (size_t)gridDim.x * RED_THREADS) {
+            double xi = (double)x[i];
+            for (int q = 0; q < m; ++q) xi += nrs[q] * (double)V[(size_t)q * ldv + i];
+            x[i] = (T)xi;
+        }
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        if (breakdown) s->reason = R_BREAKDOWN;
+        if (s->its >= s->max_it && s->reason == R_ITERATING) s->reason = R_ITS;
+        s->first = 0;
+        s->pad = m;
+        set_cond(s->h_gm_outer, s->reason == R_ITERATING ? 1u : 0u);
+        set_cond(s->h_gm_first, 0u);
+    }
+}
+
+// ----- Picard-loop kernels -------------------------------------------------
+// f -= delta unless the linear solve failed (SNES ksponly skips the update
+// when the KSP reason is negative); record the solve in the report.
+template <typename T>
+__global__ void k_pic_apply(DevState* s, const T* __restrict__ delta, T* __restrict__ f, size_t n) {
+    const bool ok = s->reason >= 0;
+    if (ok) {
+        for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
+            f[i] = f[i] - delta[i];
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        const int k = s->pic_i;
+        if (k < MAX_PICARD_DEV) {
+            s->gmres_its[k] = s->its;
+            s->ksp_reason[k] = s->reason;
+        }
+        s->gmres_total += s->its;
+        if (!ok) s->ksp_failures += 1;
+    }
+}
+
+// Residual of the current iterate: ||R(f)|| from the bracket kernel's tile
+// partials plus ||Poisson residual|| (s->pnorm2), then the stop rules of
+// run_nonlinear_matrixfree_split_mp.py:158-163.  phase 0: the initial residual.
+__global__ void k_pic_residual(DevState* s, const double* __restrict__ part, int np, int phase) {
+    if (threadIdx.x >= 32) return;
+    const double f2 = warp_reduce_parts(part, np);
+    if (threadIdx.x != 0) return;
+    const double pred = sqrt(f2) + sqrt(s->pnorm2);
+    if (phase == 0) {
+        s->pred = pred;
+        s->residual[0] = pred;
+        s->pic_i = 0;
+        s->pic_stop = 0;
+        s->pic_revert = 0;
+        s->pic_stop_rule = 0;
+        s->gmres_total = 0;
+        s->ksp_failures = 0;
+        s->ncycles = 0;
+        s->pic_active = 1;
+        set_cond(s->h_pic, 1u);
+        set_cond(s->h_revert, 0u);
         return;
     }
-    s->nrs[last] = s->grs[last] / HH(last, last);
-    for (int ii = 1; ii <= last; ++ii) {
-        const int k = last - ii;
-        double t = s->grs[k];
-        for (int j = k + 1; j <= last; ++j) t = t - HH(k, j) * s->nrs[j];
-        if (HH(k, k) == 0.0) {
-            s->reason = R_BREAKDOWN;
-            return;
-        }
-        s->nrs[k] = t / HH(k, k);
+    const int i = s->pic_i + 1;
+    s->pic_i = i;
+    s->prev = s->pred;
+    s->pred = pred;
+    if (i <= MAX_PICARD_DEV) s->residual[i] = pred;
+    const bool rose = pred > s->prev && i > 1;
+    const bool small = pred < s->snes_atol;
+    const bool maxed = i >= s->pic_max_iter || i >= MAX_PICARD_DEV;
+    if (rose || small || maxed) {
+        s->pic_stop_rule = rose ? 1 : (small ? 2 : 3);
+        s->pic_revert = pred > s->prev ? 1 : 0;
+        s->pic_stop = 1;
+        s->pic_active = 0;
     }
-#undef HH
-    s->pad = last + 1;
-    if (s->its >= s->max_it && s->reason == R_ITERATING) s->reason = R_ITS;
+    set_cond(s->h_pic, s->pic_active ? 1u : 0u);
+    set_cond(s->h_revert, (unsigned)s->pic_revert);
 }
 
 // ---------------------------------------------------------------------------

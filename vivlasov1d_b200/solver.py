@@ -173,6 +173,13 @@ class Context:
         self.call("vv_timing_read", C.byref(n), C.byref(ms), int(reset))
         return n.value, ms.value
 
+    def time_kernel(self, which, reps=50):
+        """Per-launch device time (s) of kernel `which` (0 JVP, 1 residual,
+        2 preconditioner apply) on the context's own buffers."""
+        ms = C.c_double()
+        self.call("vv_time_kernel", int(which), int(reps), C.byref(ms))
+        return ms.value / 1e3
+
     def launch_count(self, reset=False):
         n = C.c_int64()
         self.call("vv_launch_count", C.byref(n), int(reset))
