@@ -154,6 +154,7 @@ __global__ void k_gm_init(DevState* s, T* __restrict__ x, size_t n) {
         s->active = 0;
         s->it = 0;
         set_cond(s->h_gm_first, 1u);
+        set_cond(s->h_gm_outer, 1u);
     }
 }
 
