@@ -209,6 +209,23 @@ int vv_calculate_residual(vv_ctx* ctx, vv_state* st, double* residual);
 int vv_step(vv_ctx* ctx, vv_state* st, const vv_snes_opts* snes,
             const vv_ksp_opts* ksp, vv_step_report* report);
 
+/* ---- batched sweep: many independent runs in one graph launch ---------- */
+/* The reference runs one instance per process; a parameter sweep is many
+ * processes.  A batch advances `n` independent runs (each its own context
+ * and state, grids of any size) by one time step with ONE CUDA graph launch:
+ * the graph has one branch per instance, and every branch carries its own
+ * device-side Picard and GMRES loops, so each instance stops on its own
+ * convergence test while the others continue.  Contexts and states stay
+ * owned by the caller and must outlive the batch. */
+typedef struct vv_batch vv_batch;
+int vv_batch_create(int n, vv_ctx* const* ctxs, const vv_state* states, vv_batch** out);
+int vv_batch_destroy(vv_batch* batch);
+int vv_batch_set_stream(vv_batch* batch, void* cuda_stream);
+/* reports and statuses: arrays of n (statuses may be NULL); returns the
+ * first non-OK instance status, VV_OK if all instances stepped. */
+int vv_batch_step(vv_batch* batch, const vv_snes_opts* snes, const vv_ksp_opts* ksp,
+                  vv_step_report* reports, int* statuses);
+
 /* ---- invariants (vlasov/core/distribution_function.pyx:130-306,
  *      hamiltonian.pyx:67-124, potential.pyx:48-59) ---------------------- */
 typedef struct vv_invariant_set {

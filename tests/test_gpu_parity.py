@@ -350,3 +350,35 @@ def test_graph_step_equals_host_driven_step():
         assert torch.equal(run_g.fc, run_h.fc)
         assert torch.equal(run_g.pc_int, run_h.pc_int)
     assert run_g.ctx.launch_count() > 0
+
+
+def _small_run(nx, nv, f0fn, L, ht, vmax=10.0):
+    from vivlasov1d_b200.run import Run
+    cfg = {"grid": {"nx": nx, "nv": nv, "L": L, "vmin": -vmax, "vmax": vmax, "ht": ht, "nt": 1},
+           "solver": {"method": "matrixfree", "poisson_bracket": "ArakawaJ4", "preconditioner_type": "tensor",
+                      "preconditioner_scheme": "tensor_kinetic", "petsc_ksp_rtol": 1e-6,
+                      "petsc_snes_atol": 1e-11},
+           "initial_data": {"charge": -1.0}}
+    og = vo.Grid(nx, nv, L, vmax, -vmax, ht=ht)
+    f0 = vo.initialise_distribution_function(og, f0fn)
+    return Run(cfg, f0=torch.from_numpy(vo.to_flat(f0)))
+
+
+def test_batch_step_equals_single_steps():
+    """A batch of uneven instances (one graph launch per step) gives the
+    same bits and reports as stepping each instance alone."""
+    from vivlasov1d_b200.batch import Batch
+    specs = [(64, 128, vo.f0_landau(0.1, 0.5), 4 * np.pi, 0.1),
+             (128, 256, vo.f0_twostream(0.05, 0.5), 4 * np.pi, 0.1),
+             (64, 512, vo.f0_bump_on_tail(0.04, 0.3), 2 * np.pi / 0.3, 0.1)]
+    batch_runs = [_small_run(*s) for s in specs]
+    single_runs = [_small_run(*s) for s in specs]
+    batch = Batch(batch_runs)
+    for _ in range(3):
+        rb = batch.step()
+        for i, r in enumerate(single_runs):
+            rs = r.step()
+            rbi = dict(rb[i])
+            rbi.pop("status")
+            assert rbi == rs, i
+            assert torch.equal(batch_runs[i].fc, r.fc), i

@@ -102,6 +102,11 @@ SIGNATURES = {
     "vv_timing_read": (I, [P, C.POINTER(C.c_int64), C.POINTER(D), I]),
     "vv_launch_count": (I, [P, C.POINTER(C.c_int64), I]),
     "vv_time_kernel": (I, [P, I, I, C.POINTER(D)]),
+    "vv_batch_create": (I, [I, C.POINTER(P), C.POINTER(vv_state), C.POINTER(P)]),
+    "vv_batch_destroy": (I, [P]),
+    "vv_batch_set_stream": (I, [P, P]),
+    "vv_batch_step": (I, [P, C.POINTER(vv_snes_opts), C.POINTER(vv_ksp_opts), C.POINTER(vv_step_report),
+                          C.POINTER(C.c_int)]),
 }
 
 

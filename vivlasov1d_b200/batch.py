@@ -1,0 +1,64 @@
+"""Batched sweep: many independent runs advanced by one CUDA graph launch.
+
+The reference runs one instance per process (a parameter sweep is many
+``run.py`` invocations).  ``Batch`` takes several ``Run`` objects -- any mix
+of grid sizes, initial conditions and parameters, each with its own libvv
+context -- and advances all of them by one implicit time step per
+``step()`` call with a single graph launch (``vv_batch_step``).  Each
+instance keeps its own device-side Picard and GMRES loops and stops on its
+own convergence tests.
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import torch
+
+from . import _lib
+from .run import report_dict
+
+
+class Batch:
+    def __init__(self, runs, ksp=None, snes=None):
+        if not runs:
+            raise ValueError("empty batch")
+        ctxs = [r.ctx for r in runs]
+        if len({id(c) for c in ctxs}) != len(ctxs):
+            raise ValueError("every run of a batch needs its own context (its own Grid)")
+        self.runs = list(runs)
+        self.lib = _lib.load()
+        n = len(runs)
+        arr_ctx = (C.c_void_p * n)(*[c.sync_stream().value for c in ctxs])
+        arr_st = (_lib.vv_state * n)(*[r._st for r in runs])
+        h = C.c_void_p()
+        _lib.check(self.lib.vv_batch_create(n, arr_ctx, arr_st, C.byref(h)), "vv_batch_create")
+        self.h = h
+        self.n = n
+        self.ksp = ksp if ksp is not None else runs[0].ksp
+        self.snes = snes if snes is not None else runs[0].snes
+        self._reports = (_lib.vv_step_report * n)()
+        self._status = (C.c_int * n)()
+        self._stream = None
+
+    def __del__(self):
+        if getattr(self, "h", None) is not None and self.h.value:
+            try:
+                self.lib.vv_batch_destroy(self.h)
+            except Exception:
+                pass
+            self.h = None
+
+    def step(self):
+        """Advance every instance by one time step; returns per-instance reports."""
+        s = torch.cuda.current_stream().cuda_stream
+        if s != self._stream:
+            _lib.check(self.lib.vv_batch_set_stream(self.h, C.c_void_p(s)), "vv_batch_set_stream")
+            self._stream = s
+        st = self.lib.vv_batch_step(self.h, C.byref(self.snes), C.byref(self.ksp), self._reports, self._status)
+        reps = [report_dict(self._reports[i]) for i in range(self.n)]
+        for i, r in enumerate(self.runs):
+            r.itime += 1
+            reps[i]["status"] = self._status[i]
+        if st not in (_lib.VV_OK, _lib.VV_ERR_DIVERGED):
+            _lib.check(st, "vv_batch_step")
+        return reps

@@ -14,6 +14,7 @@
 #include "vv_vec.cuh"
 
 #include <algorithm>
+#include <array>
 #include <cstdlib>
 #include <cmath>
 #include <complex>
@@ -61,6 +62,12 @@ struct vv_ctx {
     cudaGraphExec_t step_exec;
     vv_state step_key;         // state pointers the graph was captured with
     unsigned long long hnd[5]; // h_gm_outer, h_gm_inner, h_gm_first, h_pic, h_revert
+    cudaGraph_t cap_owner;     // top-level graph of the capture in progress
+    bool opts_valid;           // last uploaded options still in the device state
+    vv_ksp_opts last_ksp;
+    vv_snes_opts last_snes;
+    unsigned long long last_hnd[5];
+    unsigned long long step_hnd[5];  // handles of this context's own step graph
     // kernels per region of the step graph (for launch accounting)
     int nk_top, nk_pic, nk_cycle, nk_restart, nk_arnoldi, nk_revert;
 };
@@ -243,7 +250,7 @@ int read_scalar(vv_ctx* c, const double* dsrc, double* out) {
 int pc_apply(vv_ctx* c, const double* X, double* Y, const int* yidx = nullptr, int yoff = 0) {
     vv::PcParams p = pcparams(c);
     const unsigned rows = (unsigned)((c->nv + c->pcR - 1) / c->pcR);
-    vv::k_rfft_rows<double><<<rows, 256, c->smem_rfft, c->st>>>(X, c->spec, p);
+    vv::k_rfft_rows<double, double><<<rows, 32 * c->pcR, c->smem_rfft, c->st>>>(X, c->spec, p);
     CKL(c);
     vv::TriParams t;
     t.nv = c->nv;
@@ -253,14 +260,14 @@ int pc_apply(vv_ctx* c, const double* X, double* Y, const int* yidx = nullptr, i
     t.gamma = c->gamma;
     t.dinv = c->dinv;
     if (c->tri_stage)
-        vv::k_tridiag_modes<true><<<c->nmodes, vv::TRI_THREADS, c->smem_tri, c->st>>>(c->spec, t);
+        vv::k_tridiag_modes<double, true><<<c->nmodes, vv::TRI_THREADS, c->smem_tri, c->st>>>(c->spec, t);
     else
-        vv::k_tridiag_modes<false><<<c->nmodes, vv::TRI_THREADS, c->smem_tri, c->st>>>(c->spec, t);
+        vv::k_tridiag_modes<double, false><<<c->nmodes, vv::TRI_THREADS, c->smem_tri, c->st>>>(c->spec, t);
     CKL(c);
     p.yidx = yidx;
     p.yoff = yoff;
     p.ystride = yidx ? c->ncell : 0;
-    vv::k_irfft_rows<double><<<rows, 256, c->smem_irfft, c->st>>>(c->spec, Y, p);
+    vv::k_irfft_rows<double, double><<<rows, 32 * c->pcR, c->smem_irfft, c->st>>>(c->spec, Y, p);
     CKL(c);
     return VV_OK;
 }
@@ -380,6 +387,13 @@ int set_hxp(vv_ctx* c, const double* h1p, const double* h1h, const double* h2p, 
 // ---- GMRES: kernel sequences shared by the host-driven and graph paths ------
 // state header written by the host before a solve / step (the option fields)
 int upload_options(vv_ctx* c, const vv_ksp_opts* o, const vv_snes_opts* so) {
+    if (c->opts_valid && so && std::memcmp(&c->last_ksp, o, sizeof *o) == 0 &&
+        std::memcmp(&c->last_snes, so, sizeof *so) == 0 && std::memcmp(c->last_hnd, c->hnd, sizeof c->hnd) == 0)
+        return VV_OK;
+    c->opts_valid = so != nullptr;
+    c->last_ksp = *o;
+    if (so) c->last_snes = *so;
+    std::memcpy(c->last_hnd, c->hnd, sizeof c->hnd);
     vv::DevState* h = c->hds;
     h->restart = (o->restart > 0) ? o->restart : c->restart;
     h->max_it = o->max_it;
@@ -531,16 +545,16 @@ int capture_body(vv_ctx* c, cudaStream_t s, cudaGraph_t body, int* nkernels, F f
 int capture_gmres(vv_ctx* c, int level, const double* b, double* x) {
     TRY(gm_init(c, x));
     cudaGraph_t outer[1];
-    TRY(add_conditional(c->step_graph, c->cs[level], cudaGraphCondTypeWhile, 1, 1, &c->hnd[0], outer));
+    TRY(add_conditional(c->cap_owner, c->st, cudaGraphCondTypeWhile, 1, 1, &c->hnd[0], outer));
     const int l1 = level + 1;
     return capture_body(c, c->cs[l1], outer[0], &c->nk_cycle, [&]() -> int {
         cudaGraph_t br[2];
-        TRY(add_conditional(c->step_graph, c->cs[l1], cudaGraphCondTypeIf, 2, 1, &c->hnd[2], br));
+        TRY(add_conditional(c->cap_owner, c->cs[l1], cudaGraphCondTypeIf, 2, 1, &c->hnd[2], br));
         TRY(capture_body(c, c->cs[l1 + 1], br[0], nullptr, [&]() { return gm_cycle_head(c, b, x, true); }));
         TRY(capture_body(c, c->cs[l1 + 1], br[1], &c->nk_restart, [&]() { return gm_cycle_head(c, b, x, false); }));
         TRY(gm_cycle_start(c));
         cudaGraph_t inner[1];
-        TRY(add_conditional(c->step_graph, c->cs[l1], cudaGraphCondTypeWhile, 1, 0, &c->hnd[1], inner));
+        TRY(add_conditional(c->cap_owner, c->cs[l1], cudaGraphCondTypeWhile, 1, 0, &c->hnd[1], inner));
         TRY(capture_body(c, c->cs[l1 + 1], inner[0], &c->nk_arnoldi, [&]() { return gm_arnoldi(c); }));
         return gm_finish(c, x);
     });
@@ -625,37 +639,86 @@ void destroy_graph(vv_ctx* c) {
     c->step_graph = nullptr;
 }
 
+// Capture one time step of context c into the graph being captured on c->st
+// (the top-level stream of this instance); conditional handles are created
+// on `owner`, the top-level graph.  Body graphs are captured on c->cs[1..3].
+int capture_step(vv_ctx* c, vv_state* st, cudaGraph_t owner) {
+    for (int k = 1; k < 4; ++k)
+        if (!c->cs[k]) CK(cudaStreamCreateWithFlags(&c->cs[k], cudaStreamNonBlocking));
+    c->cap_owner = owner;
+    const int64_t l0 = c->launches;
+    TRY(step_prologue(c, st));
+    cudaGraph_t pic[1];
+    TRY(add_conditional(owner, c->st, cudaGraphCondTypeWhile, 1, 0, &c->hnd[3], pic));
+    TRY(capture_body(c, c->cs[1], pic[0], &c->nk_pic, [&]() -> int {
+        TRY(step_rhs(c, st));
+        TRY(capture_gmres(c, 1, c->bvec, c->delta));
+        return step_after_solve(c, st);
+    }));
+    cudaGraph_t rev[1];
+    TRY(add_conditional(owner, c->st, cudaGraphCondTypeIf, 1, 0, &c->hnd[4], rev));
+    TRY(capture_body(c, c->cs[1], rev[0], &c->nk_revert, [&]() { return step_revert(c, st); }));
+    c->nk_top = (int)(c->launches - l0);
+    c->launches = l0;   // captured, not executed
+    c->step_key = *st;
+    return VV_OK;
+}
+
 // Build the graph of one time step for the buffers in `st`.
 int build_step_graph(vv_ctx* c, vv_state* st) {
     destroy_graph(c);
-    const int64_t launches0 = c->launches;
-    for (int k = 0; k < 4; ++k)
-        if (!c->cs[k]) CK(cudaStreamCreateWithFlags(&c->cs[k], cudaStreamNonBlocking));
+    if (!c->cs[0]) CK(cudaStreamCreateWithFlags(&c->cs[0], cudaStreamNonBlocking));
     CK(cudaGraphCreate(&c->step_graph, 0));
-    int r = capture_body(c, c->cs[0], c->step_graph, &c->nk_top, [&]() -> int {
-        TRY(step_prologue(c, st));
-        cudaGraph_t pic[1];
-        TRY(add_conditional(c->step_graph, c->cs[0], cudaGraphCondTypeWhile, 1, 0, &c->hnd[3], pic));
-        TRY(capture_body(c, c->cs[1], pic[0], &c->nk_pic, [&]() -> int {
-            TRY(step_rhs(c, st));
-            TRY(capture_gmres(c, 1, c->bvec, c->delta));
-            return step_after_solve(c, st);
-        }));
-        cudaGraph_t rev[1];
-        TRY(add_conditional(c->step_graph, c->cs[0], cudaGraphCondTypeIf, 1, 0, &c->hnd[4], rev));
-        return capture_body(c, c->cs[1], rev[0], &c->nk_revert, [&]() { return step_revert(c, st); });
-    });
+    const cudaStream_t saved = c->st;
+    CK(cudaStreamBeginCaptureToGraph(c->cs[0], c->step_graph, nullptr, nullptr, 0, cudaStreamCaptureModeRelaxed));
+    c->st = c->cs[0];
+    int r = capture_step(c, st, c->step_graph);
+    c->st = saved;
+    cudaGraph_t out = nullptr;
+    cudaError_t e = cudaStreamEndCapture(c->cs[0], &out);
+    if (r == VV_OK && e != cudaSuccess) r = fail_cuda(e, "cudaStreamEndCapture");
     if (r != VV_OK) {
         destroy_graph(c);
         return r;
     }
-    c->launches = launches0;   // captured, not executed
-    cudaError_t e = cudaGraphInstantiate(&c->step_exec, c->step_graph, 0);
+    e = cudaGraphInstantiate(&c->step_exec, c->step_graph, 0);
     if (e != cudaSuccess) {
         destroy_graph(c);
         return fail_cuda(e, "cudaGraphInstantiate");
     }
-    c->step_key = *st;
+    std::memcpy(c->step_hnd, c->hnd, sizeof c->hnd);
+    return VV_OK;
+}
+
+// Read the step report of context c from its pinned state copy.
+int fill_report(vv_ctx* c, const vv::DevState& d, int restart, vv_step_report* rep, double abort_residual) {
+    std::memset(rep, 0, sizeof(*rep));
+    rep->picard_its = d.pic_i;
+    rep->gmres_its_total = d.gmres_total;
+    rep->reverted = d.pic_revert;
+    rep->stop_rule = d.pic_stop_rule;
+    rep->ksp_failures = d.ksp_failures;
+    const int np = std::min(d.pic_i, VV_MAX_PICARD);
+    for (int k = 0; k < np; ++k) {
+        rep->gmres_its[k] = d.gmres_its[k];
+        rep->ksp_reason[k] = d.ksp_reason[k];
+    }
+    for (int k = 0; k <= np; ++k) rep->residual[k] = d.residual[k];
+    (void)restart;
+    if (c->use_graph) {
+        // kernels the graph executed: top level once, the Picard body per pass,
+        // the GMRES cycle body per cycle (+ restart branch), the Arnoldi body per iteration
+        const int64_t top = c->nk_top - c->nk_pic - c->nk_revert;
+        const int64_t cycles = d.ncycles;
+        c->launches += top + (int64_t)np * (c->nk_pic - c->nk_cycle) +
+                       cycles * (c->nk_cycle - c->nk_arnoldi - c->nk_restart) + (cycles - np) * c->nk_restart +
+                       (int64_t)d.gmres_total * c->nk_arnoldi + (d.pic_revert ? c->nk_revert : 0);
+    }
+    if (std::isnan(d.pred)) return VV_ERR_NAN;
+    if (d.pred > abort_residual) {
+        rep->aborted = 1;
+        return VV_ERR_DIVERGED;
+    }
     return VV_OK;
 }
 
@@ -753,14 +816,18 @@ int vv_create(const vv_grid* grid, vv_ctx** out) {
     }
     c->mom_seg = 64;
     c->mom_S = (nv + c->mom_seg - 1) / c->mom_seg;
-    // rows per CTA of the x-FFT kernels: enough CTAs for two waves on 148 SMs,
-    // >= 4 consecutive v rows per transposed write when nv allows
-    c->pcR = std::max(1, std::min(8, nv / 256));
-    while (c->pcR > 1 && (size_t)(M + c->pcR * (2 * M + 1)) * sizeof(double2) > 200 * 1024) c->pcR /= 2;
-    c->smem_rfft = (size_t)(M + c->pcR * M) * sizeof(double2);
-    c->smem_irfft = (size_t)(M + c->pcR * M + c->pcR * (M + 1)) * sizeof(double2);
-    c->tri_stage = (size_t)nv * 48 <= 200 * 1024;
-    c->smem_tri = c->tri_stage ? (size_t)nv * 48 : (size_t)nv * sizeof(double2);
+    // rows (warps) per CTA of the x-FFT kernels: 4 consecutive v rows per
+    // transposed 64-byte write, fewer when shared memory would exceed 200 KB
+    c->pcR = 4;
+    while (c->pcR > 1 && (size_t)(M + 2 * c->pcR * (M + 1)) * sizeof(double2) > 200 * 1024) c->pcR /= 2;
+    c->smem_rfft = (size_t)(M + c->pcR * (M + 1)) * sizeof(double2);
+    c->smem_irfft = (size_t)(M + 2 * c->pcR * (M + 1)) * sizeof(double2);
+    {
+        const int ch = (nv + vv::TRI_THREADS - 1) / vv::TRI_THREADS;
+        const size_t np = (size_t)nv + (nv + ch - 1) / ch;
+        c->tri_stage = np * 48 <= 200 * 1024;
+        c->smem_tri = c->tri_stage ? np * 48 : np * sizeof(double2);
+    }
     c->smem_pois = (size_t)M * sizeof(double2) + (size_t)nx * sizeof(double) + (size_t)(nx + 2) * sizeof(double);
 
     int s = VV_OK;
@@ -866,13 +933,13 @@ int vv_create(const vv_grid* grid, vv_ctx** out) {
         return fail_cuda(cudaGetLastError(), "vv_create upload");
     }
     // dynamic shared memory limits
-    if (cudaFuncSetAttribute(vv::k_rfft_rows<double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    if (cudaFuncSetAttribute(vv::k_rfft_rows<double, double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              (int)c->smem_rfft) != cudaSuccess ||
-        cudaFuncSetAttribute(vv::k_irfft_rows<double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+        cudaFuncSetAttribute(vv::k_irfft_rows<double, double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              (int)c->smem_irfft) != cudaSuccess ||
-        cudaFuncSetAttribute(vv::k_tridiag_modes<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+        cudaFuncSetAttribute(vv::k_tridiag_modes<double, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              (int)c->smem_tri) != cudaSuccess ||
-        cudaFuncSetAttribute(vv::k_tridiag_modes<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+        cudaFuncSetAttribute(vv::k_tridiag_modes<double, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              (int)c->smem_tri) != cudaSuccess ||
         cudaFuncSetAttribute(vv::k_moments_poisson, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              (int)c->smem_pois) != cudaSuccess) {
@@ -997,7 +1064,9 @@ int vv_gmres(vv_ctx* c, const double* b, double* x, const vv_ksp_opts* o, vv_ksp
     if (restart > c->restart || restart < 1 || o->max_it < 0) return VV_ERR_ARG;
     const unsigned long long saved[5] = {c->hnd[0], c->hnd[1], c->hnd[2], c->hnd[3], c->hnd[4]};
     for (auto& h : c->hnd) h = 0;   // host-driven: no conditional handles
+    c->opts_valid = false;
     int s = upload_options(c, o, nullptr);
+    c->opts_valid = false;
     for (int k = 0; k < 5; ++k) c->hnd[k] = saved[k];
     TRY(s);
     // b may alias nothing inside the context; run on the caller's buffers
@@ -1041,6 +1110,7 @@ int vv_step(vv_ctx* c, vv_state* st, const vv_snes_opts* so, const vv_ksp_opts* 
     std::memset(rep, 0, sizeof(*rep));
     if (c->use_graph) {
         if (!c->step_exec || !same_state(c->step_key, *st)) TRY(build_step_graph(c, st));
+        std::memcpy(c->hnd, c->step_hnd, sizeof c->hnd);
         TRY(upload_options(c, ko, so));
         CK(cudaGraphLaunch(c->step_exec, c->st));
     } else {
@@ -1052,36 +1122,9 @@ int vv_step(vv_ctx* c, vv_state* st, const vv_snes_opts* so, const vv_ksp_opts* 
         TRY(step_host(c, st));
     }
     // report
-    CK(cudaMemcpyAsync(c->hds, c->ds, sizeof(vv::DevState), cudaMemcpyDeviceToHost, c->st));
+    CK(cudaMemcpyAsync(c->hds, c->ds, offsetof(vv::DevState, hcol), cudaMemcpyDeviceToHost, c->st));
     CK(cudaStreamSynchronize(c->st));
-    const vv::DevState& d = *c->hds;
-    rep->picard_its = d.pic_i;
-    rep->gmres_its_total = d.gmres_total;
-    rep->reverted = d.pic_revert;
-    rep->stop_rule = d.pic_stop_rule;
-    rep->ksp_failures = d.ksp_failures;
-    const int np = std::min(d.pic_i, VV_MAX_PICARD);
-    for (int k = 0; k < np; ++k) {
-        rep->gmres_its[k] = d.gmres_its[k];
-        rep->ksp_reason[k] = d.ksp_reason[k];
-    }
-    for (int k = 0; k <= np; ++k) rep->residual[k] = d.residual[k];
-    if (c->use_graph) {
-        // kernels executed by the graph: top level + per Picard pass + per GMRES cycle/iteration
-        int64_t nk = c->nk_top - c->nk_pic - c->nk_revert;   // counted once at capture; re-add per execution
-        nk = (c->nk_top > 0) ? nk : 0;
-        const int64_t cycles = d.ncycles;
-        c->launches += nk + (int64_t)np * (c->nk_pic - c->nk_cycle) + cycles * (c->nk_cycle - c->nk_arnoldi - c->nk_restart)
-                       + (cycles - np) * c->nk_restart + (int64_t)d.gmres_total * c->nk_arnoldi
-                       + (d.pic_revert ? c->nk_revert : 0);
-    }
-    const double pred = d.pred;
-    if (std::isnan(pred)) return VV_ERR_NAN;
-    if (pred > so->abort_residual) {
-        rep->aborted = 1;
-        return VV_ERR_DIVERGED;
-    }
-    return VV_OK;
+    return fill_report(c, *c->hds, restart, rep, so->abort_residual);
 }
 
 int vv_invariants(vv_ctx* c, const double* f, const double* phi, const double* h2, vv_invariant_set* out) {
@@ -1186,6 +1229,130 @@ int vv_launch_count(vv_ctx* c, int64_t* launches, int reset) {
     if (launches) *launches = c->launches;
     if (reset) c->launches = 0;
     return VV_OK;
+}
+
+
+// ---- batched sweep ---------------------------------------------------------
+}  // extern "C"
+
+struct vv_batch {
+    int n;
+    std::vector<vv_ctx*> ctx;
+    std::vector<vv_state> st;
+    cudaStream_t origin;
+    std::vector<cudaStream_t> br;
+    std::vector<cudaEvent_t> ev;
+    cudaGraph_t g;
+    cudaGraphExec_t ex;
+    cudaStream_t user;
+    vv::DevState* hbuf;   // pinned, n states (header + report part)
+    std::vector<std::array<unsigned long long, 5>> hnd;   // each instance's handles in this graph
+};
+
+extern "C" {
+
+int vv_batch_destroy(vv_batch* b) {
+    if (!b) return VV_OK;
+    if (b->ex) cudaGraphExecDestroy(b->ex);
+    if (b->g) cudaGraphDestroy(b->g);
+    for (auto s : b->br) if (s) cudaStreamDestroy(s);
+    for (auto e : b->ev) if (e) cudaEventDestroy(e);
+    if (b->origin) cudaStreamDestroy(b->origin);
+    if (b->hbuf) cudaFreeHost(b->hbuf);
+    delete b;
+    return VV_OK;
+}
+
+int vv_batch_create(int n, vv_ctx* const* ctxs, const vv_state* states, vv_batch** out) {
+    if (n < 1 || !ctxs || !states || !out) return VV_ERR_ARG;
+    *out = nullptr;
+    for (int i = 0; i < n; ++i) {
+        const vv_state& s = states[i];
+        if (!ctxs[i] || !s.f || !s.fh || !s.phi || !s.h1c || !s.h1h || !s.n) return VV_ERR_ARG;
+        for (int j = 0; j < i; ++j)
+            if (ctxs[j] == ctxs[i]) return VV_ERR_ARG;   // one context per instance
+    }
+    vv_batch* b = new vv_batch();
+    b->n = n;
+    b->ctx.assign(ctxs, ctxs + n);
+    b->st.assign(states, states + n);
+    b->br.assign(n, nullptr);
+    b->ev.assign(n + 1, nullptr);
+    b->user = 0;
+    int r = VV_OK;
+    auto fail = [&](int code) { vv_batch_destroy(b); return code; };
+    if (cudaMallocHost((void**)&b->hbuf, sizeof(vv::DevState) * (size_t)n) != cudaSuccess) return fail(VV_ERR_ALLOC);
+    if (cudaStreamCreateWithFlags(&b->origin, cudaStreamNonBlocking) != cudaSuccess) return fail(VV_ERR_CUDA);
+    for (int i = 0; i < n; ++i)
+        if (cudaStreamCreateWithFlags(&b->br[i], cudaStreamNonBlocking) != cudaSuccess) return fail(VV_ERR_CUDA);
+    for (int i = 0; i <= n; ++i)
+        if (cudaEventCreateWithFlags(&b->ev[i], cudaEventDisableTiming) != cudaSuccess) return fail(VV_ERR_CUDA);
+    if (cudaGraphCreate(&b->g, 0) != cudaSuccess) return fail(VV_ERR_CUDA);
+    if (cudaStreamBeginCaptureToGraph(b->origin, b->g, nullptr, nullptr, 0, cudaStreamCaptureModeRelaxed) !=
+        cudaSuccess)
+        return fail(VV_ERR_CUDA);
+    cudaEventRecord(b->ev[n], b->origin);   // fork point
+    for (int i = 0; i < n && r == VV_OK; ++i) {
+        vv_ctx* c = b->ctx[i];
+        cudaStreamWaitEvent(b->br[i], b->ev[n], 0);
+        const cudaStream_t saved = c->st;
+        c->st = b->br[i];
+        r = capture_step(c, &b->st[i], b->g);
+        c->st = saved;
+        if (r == VV_OK) {
+            cudaEventRecord(b->ev[i], b->br[i]);
+            std::array<unsigned long long, 5> h;
+            std::memcpy(h.data(), c->hnd, sizeof c->hnd);
+            b->hnd.push_back(h);
+        }
+    }
+    if (r == VV_OK)
+        for (int i = 0; i < n; ++i) cudaStreamWaitEvent(b->origin, b->ev[i], 0);   // join
+    cudaGraph_t outg = nullptr;
+    cudaError_t e = cudaStreamEndCapture(b->origin, &outg);
+    if (r != VV_OK) return fail(r);
+    if (e != cudaSuccess) return fail(fail_cuda(e, "batch capture"));
+    e = cudaGraphInstantiate(&b->ex, b->g, 0);
+    if (e != cudaSuccess) return fail(fail_cuda(e, "batch instantiate"));
+    for (int i = 0; i < n; ++i) b->ctx[i]->use_graph = true;
+    *out = b;
+    return VV_OK;
+}
+
+int vv_batch_set_stream(vv_batch* b, void* stream) {
+    if (!b) return VV_ERR_ARG;
+    b->user = (cudaStream_t)stream;
+    return VV_OK;
+}
+
+int vv_batch_step(vv_batch* b, const vv_snes_opts* so, const vv_ksp_opts* ko, vv_step_report* reports,
+                  int* statuses) {
+    if (!b || !so || !ko || !reports) return VV_ERR_ARG;
+    const size_t hdr = offsetof(vv::DevState, hcol);
+    for (int i = 0; i < b->n; ++i) {
+        vv_ctx* c = b->ctx[i];
+        const int restart = (ko->restart > 0) ? ko->restart : c->restart;
+        if (restart > c->restart || restart < 1) return VV_ERR_ARG;
+        const cudaStream_t saved = c->st;
+        c->st = b->user;
+        std::memcpy(c->hnd, b->hnd[i].data(), sizeof c->hnd);
+        int r = upload_options(c, ko, so);
+        c->st = saved;
+        TRY(r);
+    }
+    CK(cudaGraphLaunch(b->ex, b->user));
+    for (int i = 0; i < b->n; ++i)
+        CK(cudaMemcpyAsync(&b->hbuf[i], b->ctx[i]->ds, hdr, cudaMemcpyDeviceToHost, b->user));
+    CK(cudaStreamSynchronize(b->user));
+    int first_bad = VV_OK;
+    for (int i = 0; i < b->n; ++i) {
+        vv_ctx* c = b->ctx[i];
+        const int restart = (ko->restart > 0) ? ko->restart : c->restart;
+        const int s = fill_report(c, b->hbuf[i], restart, &reports[i], so->abort_residual);
+        if (statuses) statuses[i] = s;
+        if (s != VV_OK && first_bad == VV_OK) first_bad = s;
+    }
+    return first_bad;
 }
 
 }  // extern "C"

@@ -340,7 +340,7 @@ template <> struct Vec2<double> { using type = double2; };
 template <> struct Vec2<float> { using type = float2; };
 
 template <int SCHEME, int MODE, typename T>
-__global__ void __launch_bounds__(WTHREADS)
+__global__ void __launch_bounds__(WTHREADS, 4)
 k_bracket_wide(const T* __restrict__ X, const T* __restrict__ Xh, T* __restrict__ Y,
                BracketParams p, double* __restrict__ sumsq) {
     if (p.xidx) X += (size_t)(*p.xidx) * p.xstride;
@@ -406,57 +406,58 @@ k_bracket_wide(const T* __restrict__ X, const T* __restrict__ Xh, T* __restrict_
         scol[c][2] = bp;
     }
     __syncthreads();
-    // ---- compute: column tx, rows ty*8 .. ty*8+7 ----
+    // ---- compute: column tx, rows ty*8 .. ty*8+7, rolling register window ----
     const int tx = tid & (WX - 1), ty = tid / WX;
     const int lx = tx + 2;
     const int r0 = ty * WR;            // tile row of the first output
     const int i = i0 + tx;
-    T c0[WR + 4], cm1[WR + 2], cp1[WR + 2], cm2[WR], cp2[WR];
-#pragma unroll
-    for (int k = 0; k < WR + 4; ++k) c0[k] = sx[r0 + k][lx];
-#pragma unroll
-    for (int k = 0; k < WR + 2; ++k) { cm1[k] = sx[r0 + 1 + k][lx - 1]; cp1[k] = sx[r0 + 1 + k][lx + 1]; }
-#pragma unroll
-    for (int k = 0; k < WR; ++k) { cm2[k] = sx[r0 + 2 + k][lx - 2]; cp2[k] = sx[r0 + 2 + k][lx + 2]; }
     const T B1 = T(scol[tx][0]), bm = T(scol[tx][1]), bp = T(scol[tx][2]);
     const T tscale = T(((SCHEME == 2) ? p.f2 : p.f1) * p.factor);
     const T htinv = T(p.ht_inv);
+    // window: column i rows j-2..j+2, columns i+-1 rows j-1..j+1
+    T w0 = sx[r0][lx], w1 = sx[r0 + 1][lx], w2 = sx[r0 + 2][lx], w3 = sx[r0 + 3][lx];
+    T m0 = sx[r0 + 1][lx - 1], m1 = sx[r0 + 2][lx - 1];
+    T q0 = sx[r0 + 1][lx + 1], q1 = sx[r0 + 2][lx + 1];
     double acc2 = 0.0;
 #pragma unroll
     for (int q = 0; q < WR; ++q) {
+        const T w4 = sx[r0 + q + 4][lx];
+        const T m2 = sx[r0 + q + 3][lx - 1];
+        const T q2 = sx[r0 + q + 3][lx + 1];
         const int j = j0 + r0 + q;
-        if (j >= nv) break;
-        const size_t g = (size_t)j * nx + i;
-        const T xc = c0[q + 2];
-        T y;
-        if (MODE == MODE_JVP) y = htinv * xc;
-        else if (MODE == MODE_RESIDUAL) y = htinv * (X[g] - Xh[g]);
-        else y = Y[g];
-        if (j >= 2 && j < nv - 2) {
-            const T A1 = T(srow[r0 + q][0]), am = T(srow[r0 + q][1]), ap = T(srow[r0 + q][2]);
-            // neighbours: (di, dj)
-            const T xm1m1 = cm1[q], xm1p1 = cm1[q + 2], xp1m1 = cp1[q], xp1p1 = cp1[q + 2];
-            T s = T(0);
-            if (Coef<SCHEME>::cA1 != 0.0 || Coef<SCHEME>::cA2 != 0.0) {
-                T ax = T(0), bx = T(0);
-                if (Coef<SCHEME>::cA1 != 0.0) {
-                    ax = T(Coef<SCHEME>::cA1) * (cp1[q + 1] - cm1[q + 1]);
-                    bx = T(Coef<SCHEME>::cB1) * (c0[q + 3] - c0[q + 1]);
+        if (j < nv) {
+            const size_t g = (size_t)j * nx + i;
+            T y;
+            if (MODE == MODE_JVP) y = htinv * w2;
+            else if (MODE == MODE_RESIDUAL) y = htinv * (X[g] - Xh[g]);
+            else y = Y[g];
+            if (j >= 2 && j < nv - 2) {
+                const T A1 = T(srow[r0 + q][0]), am = T(srow[r0 + q][1]), ap = T(srow[r0 + q][2]);
+                T s = T(0);
+                if (Coef<SCHEME>::cA1 != 0.0 || Coef<SCHEME>::cA2 != 0.0) {
+                    T ax = T(0), bx = T(0);
+                    if (Coef<SCHEME>::cA1 != 0.0) {
+                        ax = T(Coef<SCHEME>::cA1) * (q1 - m1);
+                        bx = T(Coef<SCHEME>::cB1) * (w3 - w1);
+                    }
+                    if (Coef<SCHEME>::cA2 != 0.0) {
+                        ax += T(Coef<SCHEME>::cA2) * (sx[r0 + q + 2][lx + 2] - sx[r0 + q + 2][lx - 2]);
+                        bx += T(Coef<SCHEME>::cB2) * (w4 - w0);
+                    }
+                    s = A1 * ax - B1 * bx;
                 }
-                if (Coef<SCHEME>::cA2 != 0.0) {
-                    ax += T(Coef<SCHEME>::cA2) * (cp2[q] - cm2[q]);
-                    bx += T(Coef<SCHEME>::cB2) * (c0[q + 4] - c0[q]);
-                }
-                s = A1 * ax - B1 * bx;
+                s += am * (m0 - q0);     // (x(-1,-1) - x(+1,-1))
+                s += ap * (m2 - q2);     // (x(-1,+1) - x(+1,+1))
+                s += bm * (m0 - m2);     // (x(-1,-1) - x(-1,+1))
+                s += bp * (q0 - q2);     // (x(+1,-1) - x(+1,+1))
+                y += tscale * s;
             }
-            s += am * (xm1m1 - xp1m1);
-            s += ap * (xm1p1 - xp1p1);
-            s += bm * (xm1m1 - xm1p1);
-            s += bp * (xp1m1 - xp1p1);
-            y += tscale * s;
+            Y[g] = y;
+            acc2 += (double)y * (double)y;
         }
-        Y[g] = y;
-        acc2 += (double)y * (double)y;
+        w0 = w1; w1 = w2; w2 = w3; w3 = w4;
+        m0 = m1; m1 = m2;
+        q0 = q1; q1 = q2;
     }
     if (sumsq) {
         const double t = block_sum(acc2, sred);

@@ -16,6 +16,24 @@ VV_DEV double2 c_scale(double2 a, double s) { return make_double2(a.x * s, a.y *
 // multiply by a complex number that is given as (real scalar) * (complex lam)
 VV_DEV double2 c_rmul(double2 lam, double s) { return make_double2(lam.x * s, lam.y * s); }
 
+// float2 counterparts (single-precision complex)
+VV_DEV float2 c_add(float2 a, float2 b) { return make_float2(a.x + b.x, a.y + b.y); }
+VV_DEV float2 c_sub(float2 a, float2 b) { return make_float2(a.x - b.x, a.y - b.y); }
+VV_DEV float2 c_mul(float2 a, float2 b) {
+    return make_float2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+}
+VV_DEV float2 c_conj(float2 a) { return make_float2(a.x, -a.y); }
+VV_DEV float2 c_scale(float2 a, float s) { return make_float2(a.x * s, a.y * s); }
+VV_DEV float2 c_rmul(float2 lam, float s) { return make_float2(lam.x * s, lam.y * s); }
+
+// complex type of a real type
+template <typename R> struct Cplx;
+template <> struct Cplx<double> { using type = double2; };
+template <> struct Cplx<float> { using type = float2; };
+template <typename C> VV_DEV C c_make(double x, double y);
+template <> VV_DEV double2 c_make<double2>(double x, double y) { return make_double2(x, y); }
+template <> VV_DEV float2 c_make<float2>(double x, double y) { return make_float2((float)x, (float)y); }
+
 // Warp sum of a double (all lanes get the result).
 VV_DEV double warp_sum(double v) {
 #pragma unroll

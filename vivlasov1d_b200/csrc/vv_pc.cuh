@@ -24,28 +24,54 @@ struct PcParams {
     int nx, nv;
     int M;                 // nx/2: complex FFT length
     int logM;
-    int R;                 // rows per CTA in the row kernels
-    const double2* tw;     // tw[k] = exp(-2 pi i k / nx), k < nx/2
+    int R;                 // rows (warps) per CTA in the row kernels
+    const void* tw;        // tw[k] = exp(-2 pi i k / nx), k < nx/2 (double2 or float2)
     const int* yidx;       // optional: output is Y + (*yidx + yoff) * ystride
     int yoff;
     size_t ystride;
 };
 
-// In-place radix-2 DIT FFT of R rows of length M stored bit-reversed in smem.
-// `stw` is the twiddle table exp(-2 pi i k / (2M)), k < M, in shared memory.
-// sign = -1 forward, +1 inverse (unnormalised).
+__device__ __forceinline__ int bitrev(int m, int logM) {
+    return logM == 0 ? 0 : (int)(__brev((unsigned)m) >> (32 - logM));
+}
+
+// In-place radix-2 DIT FFT of one row of length M (bit-reversed input) by
+// one warp; `stw` holds exp(-2 pi i k /(2M)), k < M, in shared memory.
+// SIGN = -1 forward, +1 inverse (unnormalised).  Only __syncwarp between
+// stages: the warps of a CTA transform their rows independently.
+template <int SIGN, typename C>
+__device__ __forceinline__ void warp_fft(C* buf, int M, int logM, const C* stw) {
+    const int lane = threadIdx.x & 31;
+    const int nb = M >> 1;
+    for (int lh = 0; lh < logM; ++lh) {
+        const int half = 1 << lh;
+        const int tshift = logM - lh;          // twiddle index = pos * (M/half)
+        for (int b = lane; b < nb; b += 32) {
+            const int grp = b >> lh;
+            const int pos = b & (half - 1);
+            const int i0 = (grp << (lh + 1)) + pos;
+            const int i1 = i0 + half;
+            C w = stw[pos << tshift];
+            if (SIGN > 0) w.y = -w.y;
+            const C a = buf[i0];
+            const C t = c_mul(w, buf[i1]);
+            buf[i0] = c_add(a, t);
+            buf[i1] = c_sub(a, t);
+        }
+        __syncwarp();
+    }
+}
+
+// Block-wide in-place radix-2 DIT FFT of one row of length M (bit-reversed
+// input), used by the single-CTA Poisson solve.  stw as in warp_fft.
 template <int SIGN>
-__device__ __forceinline__ void smem_fft(double2* buf, int R, int M, const double2* stw) {
-    const int nthr = blockDim.x;
-    const int nb = R * (M >> 1);
+__device__ __forceinline__ void block_fft(double2* buf, int M, const double2* stw) {
     for (int half = 1; half < M; half <<= 1) {
-        const int tstride = M / half;  // W_M^(pos*M/(2 half)) = stw[pos*M/half]
-        for (int b = threadIdx.x; b < nb; b += nthr) {
-            const int row = b / (M >> 1);
-            const int bb = b - row * (M >> 1);
-            const int grp = bb / half;
-            const int pos = bb - grp * half;
-            const int i0 = row * M + grp * 2 * half + pos;
+        const int tstride = M / half;
+        for (int b = threadIdx.x; b < (M >> 1); b += blockDim.x) {
+            const int grp = b / half;
+            const int pos = b - grp * half;
+            const int i0 = grp * 2 * half + pos;
             const int i1 = i0 + half;
             double2 w = stw[pos * tstride];
             if (SIGN > 0) w.y = -w.y;
@@ -58,92 +84,116 @@ __device__ __forceinline__ void smem_fft(double2* buf, int R, int M, const doubl
     }
 }
 
-__device__ __forceinline__ int bitrev(int m, int logM) {
-    return logM == 0 ? 0 : (int)(__brev((unsigned)m) >> (32 - logM));
-}
-
-__device__ __forceinline__ void load_twiddles(double2* stw, const double2* __restrict__ tw, int M) {
+// Real FFT along x of R consecutive v rows (one warp per row), half
+// spectrum written transposed: spec[k*nv + j], k = 0..M.
+// dynamic smem: [M twiddles][R rows x (M+1) complex]
+template <typename TI, typename R>
+__global__ void k_rfft_rows(const TI* __restrict__ X, typename Cplx<R>::type* __restrict__ spec, PcParams p) {
+    using C = typename Cplx<R>::type;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    C* stw = reinterpret_cast<C*>(smem_raw);
+    const int M = p.M, LD = M + 1;
+    C* rows = stw + M;
+    const C* tw = reinterpret_cast<const C*>(p.tw);
     for (int k = threadIdx.x; k < M; k += blockDim.x) stw[k] = tw[k];
-}
-
-// rows j0 .. j0+R-1 of X -> spec[k*nv + j] for k = 0..M
-// dynamic smem: [M twiddles][R*M buffer]
-template <typename T>
-__global__ void k_rfft_rows(const T* __restrict__ X, double2* __restrict__ spec, PcParams p) {
-    extern __shared__ double2 smem[];
-    const int M = p.M;
-    double2* stw = smem;
-    double2* buf = smem + M;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int j0 = blockIdx.x * p.R;
-    const int nrow = min(p.R, p.nv - j0);
-    load_twiddles(stw, p.tw, M);
-    for (int idx = threadIdx.x; idx < p.R * M; idx += blockDim.x) {
-        const int r = idx / M, m = idx - r * M;
-        double2 z = make_double2(0.0, 0.0);
-        if (r < nrow) {
-            const T* row = X + (size_t)(j0 + r) * p.nx;
-            z = make_double2((double)row[2 * m], (double)row[2 * m + 1]);
+    const int j = j0 + warp;
+    C* buf = rows + warp * LD;
+    __syncthreads();
+    if (warp < p.R && j < p.nv) {
+        const TI* row = X + (size_t)j * p.nx;
+        for (int m = lane; m < M; m += 32)
+            buf[bitrev(m, p.logM)] = c_make<C>((double)row[2 * m], (double)row[2 * m + 1]);
+        __syncwarp();
+        warp_fft<-1>(buf, M, p.logM, stw);
+        // split: X_k = E_k + W_N^k O_k,  E = (Z_k + conj Z_{M-k})/2,  O = -i/2 (Z_k - conj Z_{M-k})
+        // computed for the pair (k, M-k) by one lane so the update is in place
+        for (int k = lane; k <= M / 2; k += 32) {
+            const int kc = M - k;
+            const C zk = buf[k == M ? 0 : k];
+            const C zc = buf[k == 0 ? 0 : kc];
+            C out_k, out_c;
+            {
+                const C zcc = c_conj(zc);
+                const C E = c_scale(c_add(zk, zcc), (R)0.5);
+                const C D = c_sub(zk, zcc);
+                const C O = c_make<C>(0.5 * D.y, -0.5 * D.x);
+                out_k = c_add(E, c_mul(stw[k], O));
+            }
+            {
+                const C zkc = c_conj(zk);   // pair element kc: Z_kc and conj Z_{M-kc} = conj Z_k
+                const C E = c_scale(c_add(zc, zkc), (R)0.5);
+                const C D = c_sub(zc, zkc);
+                const C O = c_make<C>(0.5 * D.y, -0.5 * D.x);
+                const C w = (kc < M) ? stw[kc] : c_make<C>(-1.0, 0.0);
+                out_c = c_add(E, c_mul(w, O));
+            }
+            if (k == 0) {           // k = 0 and k = M share Z_0
+                buf[0] = out_k;
+                buf[M] = out_c;
+            } else if (k == kc) {
+                buf[k] = out_k;
+            } else {
+                buf[k] = out_k;
+                buf[kc] = out_c;
+            }
         }
-        buf[r * M + bitrev(m, p.logM)] = z;
     }
     __syncthreads();
-    smem_fft<-1>(buf, p.R, M, stw);
-    // split: X_k = E_k + W_N^k O_k,  E = (Z_k + conj Z_{M-k})/2,  O = -i/2 (Z_k - conj Z_{M-k})
+    // transposed, coalesced write: R consecutive j per mode k
+    const int nrow = min(p.R, p.nv - j0);
     for (int idx = threadIdx.x; idx < (M + 1) * p.R; idx += blockDim.x) {
         const int k = idx / p.R, r = idx - k * p.R;
-        if (r >= nrow) continue;
-        const double2 zk = buf[r * M + (k == M ? 0 : k)];
-        const double2 zc = c_conj(buf[r * M + (k == 0 ? 0 : M - k)]);
-        const double2 E = c_scale(c_add(zk, zc), 0.5);
-        const double2 D = c_sub(zk, zc);
-        const double2 O = make_double2(0.5 * D.y, -0.5 * D.x);  // -i/2 * D
-        const double2 w = (k < M) ? stw[k] : make_double2(-1.0, 0.0);   // W_N^M = -1
-        spec[(size_t)k * p.nv + j0 + r] = c_add(E, c_mul(w, O));
+        if (r < nrow) spec[(size_t)k * p.nv + j0 + r] = rows[r * LD + k];
     }
 }
 
-// spec[k*nv + j] (k = 0..M) -> rows of Y, scaled by 1/nx
-// dynamic smem: [M twiddles][R*M buffer][R*(M+1) spectrum]
-template <typename T>
-__global__ void k_irfft_rows(const double2* __restrict__ spec, T* __restrict__ Y, PcParams p) {
+// spec[k*nv + j] (k = 0..M) -> rows of Y (one warp per row), scaled by 1/nx
+// dynamic smem: [M twiddles][R rows x (M+1) spectrum][R rows x (M+1) work]
+template <typename R, typename TO>
+__global__ void k_irfft_rows(const typename Cplx<R>::type* __restrict__ spec, TO* __restrict__ Y, PcParams p) {
+    using C = typename Cplx<R>::type;
     if (p.yidx) Y += (size_t)(*p.yidx + p.yoff) * p.ystride;
-    extern __shared__ double2 smem[];
-    const int M = p.M;
-    double2* stw = smem;
-    double2* buf = smem + M;
-    double2* xs = buf + p.R * M;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    C* stw = reinterpret_cast<C*>(smem_raw);
+    const int M = p.M, LD = M + 1;
+    C* xs = stw + M;
+    C* work = xs + p.R * LD;
+    const C* tw = reinterpret_cast<const C*>(p.tw);
+    for (int k = threadIdx.x; k < M; k += blockDim.x) stw[k] = tw[k];
     const int j0 = blockIdx.x * p.R;
     const int nrow = min(p.R, p.nv - j0);
-    load_twiddles(stw, p.tw, M);
     for (int idx = threadIdx.x; idx < (M + 1) * p.R; idx += blockDim.x) {
         const int k = idx / p.R, r = idx - k * p.R;
-        double2 v = make_double2(0.0, 0.0);
+        C v = c_make<C>(0.0, 0.0);
         if (r < nrow) v = spec[(size_t)k * p.nv + j0 + r];
-        if (k == 0 || k == M) v.y = 0.0;   // c2r ignores these imaginary parts
-        xs[r * (M + 1) + k] = v;
+        if (k == 0 || k == M) v.y = 0;   // c2r ignores these imaginary parts
+        xs[r * LD + k] = v;
     }
     __syncthreads();
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    if (warp >= nrow) return;
+    const C* xr = xs + warp * LD;
+    C* buf = work + warp * LD;
     // Z_k = (X_k + conj X_{M-k})/2 + i W_N^{-k} (X_k - conj X_{M-k})/2
-    for (int idx = threadIdx.x; idx < p.R * M; idx += blockDim.x) {
-        const int r = idx / M, k = idx - r * M;
-        const double2 xk = xs[r * (M + 1) + k];
-        const double2 xc = c_conj(xs[r * (M + 1) + (M - k)]);
-        const double2 E = c_scale(c_add(xk, xc), 0.5);
-        double2 w = stw[k];
-        w.y = -w.y;                            // W_N^{-k}
-        const double2 O = c_mul(w, c_scale(c_sub(xk, xc), 0.5));
-        buf[r * M + bitrev(k, p.logM)] = make_double2(E.x - O.y, E.y + O.x);  // E + i O
+    for (int k = lane; k < M; k += 32) {
+        const C xk = xr[k];
+        const C xc = c_conj(xr[M - k]);
+        const C E = c_scale(c_add(xk, xc), (R)0.5);
+        C w = stw[k];
+        w.y = -w.y;
+        const C O = c_mul(w, c_scale(c_sub(xk, xc), (R)0.5));
+        buf[bitrev(k, p.logM)] = c_make<C>(E.x - O.y, E.y + O.x);
     }
-    __syncthreads();
-    smem_fft<+1>(buf, p.R, M, stw);
-    const double s = 1.0 / (double)M;   // (1/M) IDFT_M gives the 1/nx-normalised irfft
-    for (int idx = threadIdx.x; idx < p.R * M; idx += blockDim.x) {
-        const int r = idx / M, m = idx - r * M;
-        if (r >= nrow) continue;
-        const double2 z = buf[r * M + m];
-        T* row = Y + (size_t)(j0 + r) * p.nx;
-        row[2 * m] = (T)(z.x * s);
-        row[2 * m + 1] = (T)(z.y * s);
+    __syncwarp();
+    warp_fft<+1>(buf, M, p.logM, stw);
+    const R s = (R)(1.0 / (double)M);   // (1/M) IDFT_M gives the 1/nx-normalised irfft
+    TO* row = Y + (size_t)(j0 + warp) * p.nx;
+    for (int m = lane; m < M; m += 32) {
+        const C z = buf[m];
+        row[2 * m] = (TO)(z.x * s);
+        row[2 * m + 1] = (TO)(z.y * s);
     }
 }
 
@@ -152,35 +202,34 @@ __global__ void k_irfft_rows(const double2* __restrict__ spec, T* __restrict__ Y
 // ---------------------------------------------------------------------------
 struct TriParams {
     int nv, nmodes;
-    const double2* lambda;  // per mode eigenvalue lambda_k (shifted, TensorProduct.pyx:109-116)
-    const double* alpha;    // nv: sub-diagonal  A[r,r-1] = lambda * alpha[r]
-    const double* gamma;    // nv: super-diagonal A[r,r+1] = lambda * gamma[r]
-    const double2* dinv;    // nmodes*nv: 1 / U[r,r] of the LU factors
+    const void* lambda;  // per mode eigenvalue lambda_k (shifted, TensorProduct.pyx:109-116), complex R
+    const void* alpha;   // nv (R): sub-diagonal  A[r,r-1] = lambda * alpha[r]
+    const void* gamma;   // nv (R): super-diagonal A[r,r+1] = lambda * gamma[r]
+    const void* dinv;    // nmodes*nv (complex R): 1 / U[r,r] of the LU factors
 };
 
 constexpr int TRI_THREADS = 256;
 
 // affine map x -> P x + Q on complex numbers; combine(first, second) = second o first
-struct Aff { double2 P, Q; };
-VV_DEV Aff aff_combine(const Aff& first, const Aff& second) {
-    Aff r;
+template <typename C> struct Aff { C P, Q; };
+template <typename C>
+VV_DEV Aff<C> aff_combine(const Aff<C>& first, const Aff<C>& second) {
+    Aff<C> r;
     r.P = c_mul(second.P, first.P);
     r.Q = c_add(c_mul(second.P, first.Q), second.Q);
     return r;
 }
-VV_DEV Aff shfl_aff(const Aff& a, int d, bool up) {
-    Aff r;
-    if (up) {
-        r.P.x = __shfl_up_sync(0xffffffffu, a.P.x, d);
-        r.P.y = __shfl_up_sync(0xffffffffu, a.P.y, d);
-        r.Q.x = __shfl_up_sync(0xffffffffu, a.Q.x, d);
-        r.Q.y = __shfl_up_sync(0xffffffffu, a.Q.y, d);
-    } else {
-        r.P.x = __shfl_down_sync(0xffffffffu, a.P.x, d);
-        r.P.y = __shfl_down_sync(0xffffffffu, a.P.y, d);
-        r.Q.x = __shfl_down_sync(0xffffffffu, a.Q.x, d);
-        r.Q.y = __shfl_down_sync(0xffffffffu, a.Q.y, d);
-    }
+template <typename T>
+VV_DEV T shfl_dir(T v, int d, bool up) {
+    return up ? __shfl_up_sync(0xffffffffu, v, d) : __shfl_down_sync(0xffffffffu, v, d);
+}
+template <typename C>
+VV_DEV Aff<C> shfl_aff(const Aff<C>& a, int d, bool up) {
+    Aff<C> r;
+    r.P.x = shfl_dir(a.P.x, d, up);
+    r.P.y = shfl_dir(a.P.y, d, up);
+    r.Q.x = shfl_dir(a.Q.x, d, up);
+    r.Q.y = shfl_dir(a.Q.y, d, up);
     return r;
 }
 
@@ -188,102 +237,116 @@ VV_DEV Aff shfl_aff(const Aff& a, int d, bool up) {
 // (pos = tid for the forward sweep, nthreads-1-tid for the backward sweep;
 // both keep warps intact).  Returns the image of 0 under the composition of
 // all earlier chunks.
-__device__ double2 block_scan_aff(Aff a, bool forward, Aff* sh) {
+template <typename C>
+__device__ C block_scan_aff(Aff<C> a, bool forward, Aff<C>* sh) {
     const int pos = forward ? (int)threadIdx.x : TRI_THREADS - 1 - (int)threadIdx.x;
     const int lane = pos & 31, wid = pos >> 5;
-    Aff inc = a;
+    Aff<C> inc = a;
 #pragma unroll
     for (int d = 1; d < 32; d <<= 1) {
-        const Aff o = shfl_aff(inc, d, forward);   // the lane d earlier in pos order
+        const Aff<C> o = shfl_aff(inc, d, forward);   // the lane d earlier in pos order
         if (lane >= d) inc = aff_combine(o, inc);
     }
     if (lane == 31) sh[wid] = inc;
     __syncthreads();
-    Aff pre;
-    pre.P = make_double2(1.0, 0.0);
-    pre.Q = make_double2(0.0, 0.0);
+    Aff<C> pre;
+    pre.P = c_make<C>(1.0, 0.0);
+    pre.Q = c_make<C>(0.0, 0.0);
     for (int w = 0; w < wid; ++w) pre = aff_combine(pre, sh[w]);
-    const Aff prev = shfl_aff(inc, 1, forward);
-    Aff ex = pre;
+    const Aff<C> prev = shfl_aff(inc, 1, forward);
+    Aff<C> ex = pre;
     if (lane > 0) ex = aff_combine(pre, prev);
     __syncthreads();
     return ex.Q;
 }
 
-// One CTA per x mode.  STAGE: the mode's LU reciprocals and the alpha/gamma
-// tables are staged in shared memory (nv <= 4096); otherwise read from L2.
-// dynamic smem: [nv rhs][nv dinv][nv alpha][nv gamma] (the last three only if STAGE)
-template <bool STAGE>
+// One CTA per x mode; each thread owns a chunk of C consecutive rows.  The
+// right-hand side, LU reciprocals and the alpha/gamma tables are staged in
+// shared memory with one pad slot per chunk (conflict-free chunk-strided
+// access).  dynamic smem: 3 arrays of nv + nv/C complex/real slots.
+template <typename R, bool STAGE>
 __global__ void __launch_bounds__(TRI_THREADS)
-k_tridiag_modes(double2* __restrict__ spec, TriParams p) {
-    extern __shared__ double2 sm[];
-    __shared__ Aff shw[TRI_THREADS / 32];
+k_tridiag_modes(typename Cplx<R>::type* __restrict__ spec, TriParams p) {
+    using C = typename Cplx<R>::type;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    __shared__ Aff<C> shw[TRI_THREADS / 32];
     const int k = blockIdx.x;
     const int nv = p.nv;
-    double2* b = sm;
-    double2* line = spec + (size_t)k * nv;
-    const double2* dinv_g = p.dinv + (size_t)k * nv;
-    const double2* dinv = STAGE ? sm + nv : dinv_g;
-    const double* alpha = STAGE ? reinterpret_cast<const double*>(sm + 2 * nv) : p.alpha;
-    const double* gamma = STAGE ? reinterpret_cast<const double*>(sm + 2 * nv) + nv : p.gamma;
-    const double2 lam = p.lambda[k];
+    const int CH = (nv + TRI_THREADS - 1) / TRI_THREADS;   // rows per thread
+    const int NP = nv + (nv + CH - 1) / CH;               // padded length
+    C* b = reinterpret_cast<C*>(smem_raw);
+    C* di = b + NP;
+    R* al = reinterpret_cast<R*>(di + NP);
+    R* ga = al + NP;
+    C* line = spec + (size_t)k * nv;
+    const C* dinv_g = reinterpret_cast<const C*>(p.dinv) + (size_t)k * nv;
+    const R* alpha_g = reinterpret_cast<const R*>(p.alpha);
+    const R* gamma_g = reinterpret_cast<const R*>(p.gamma);
+    const C lam = reinterpret_cast<const C*>(p.lambda)[k];
     for (int r = threadIdx.x; r < nv; r += TRI_THREADS) {
-        b[r] = line[r];
+        const int q = r + r / CH;
+        b[q] = line[r];
         if (STAGE) {
-            sm[nv + r] = dinv_g[r];
-            reinterpret_cast<double*>(sm + 2 * nv)[r] = p.alpha[r];
-            reinterpret_cast<double*>(sm + 2 * nv)[nv + r] = p.gamma[r];
+            di[q] = dinv_g[r];
+            al[q] = alpha_g[r];
+            ga[q] = gamma_g[r];
         }
     }
     __syncthreads();
-    const int C = (nv + TRI_THREADS - 1) / TRI_THREADS;
-    const int r0 = threadIdx.x * C;
-    const int r1 = min(r0 + C, nv);
+    // accessors: row r at padded index q (tables staged or read through L1/L2)
+    auto DI = [&](int r, int q) -> C { return STAGE ? di[q] : dinv_g[r]; };
+    auto AL = [&](int r, int q) -> R { return STAGE ? al[q] : alpha_g[r]; };
+    auto GA = [&](int r, int q) -> R { return STAGE ? ga[q] : gamma_g[r]; };
+    const int r0 = threadIdx.x * CH;
+    const int r1 = min(r0 + CH, nv);
+    const int q0 = threadIdx.x * (CH + 1);       // padded index of r0
     // forward: y_r = b_r - l_r y_{r-1},  l_r = lambda alpha_r / U_{r-1}
-    Aff a;
-    a.P = make_double2(1.0, 0.0);
-    a.Q = make_double2(0.0, 0.0);
-    for (int r = r0; r < r1; ++r) {
-        Aff m;
-        if (r == 0) m.P = make_double2(0.0, 0.0);
+    Aff<C> a;
+    a.P = c_make<C>(1.0, 0.0);
+    a.Q = c_make<C>(0.0, 0.0);
+    for (int r = r0, q = q0; r < r1; ++r, ++q) {
+        Aff<C> m;
+        if (r == 0) m.P = c_make<C>(0.0, 0.0);
         else {
-            const double2 l = c_mul(c_rmul(lam, alpha[r]), dinv[r - 1]);
-            m.P = make_double2(-l.x, -l.y);
+            const C dprev = DI(r - 1, (r == r0) ? q - 2 : q - 1);   // r0-1 sits before the pad slot
+            const C l = c_mul(c_rmul(lam, AL(r, q)), dprev);
+            m.P = c_make<C>(-l.x, -l.y);
         }
-        m.Q = b[r];
+        m.Q = b[q];
         a = aff_combine(a, m);
     }
-    double2 y = block_scan_aff(a, true, shw);
-    for (int r = r0; r < r1; ++r) {
-        if (r == 0) y = b[0];
+    C y = block_scan_aff<C>(a, true, shw);
+    for (int r = r0, q = q0; r < r1; ++r, ++q) {
+        if (r == 0) y = b[q];
         else {
-            const double2 l = c_mul(c_rmul(lam, alpha[r]), dinv[r - 1]);
-            y = c_sub(b[r], c_mul(l, y));
+            const C dprev = DI(r - 1, (r == r0) ? q - 2 : q - 1);
+            const C l = c_mul(c_rmul(lam, AL(r, q)), dprev);
+            y = c_sub(b[q], c_mul(l, y));
         }
-        b[r] = y;
+        b[q] = y;
     }
     __syncthreads();
     // backward: x_r = U_r^-1 (y_r - c_r x_{r+1})  ==  mu_r + nu_r x_{r+1}
-    a.P = make_double2(1.0, 0.0);
-    a.Q = make_double2(0.0, 0.0);
-    for (int r = r1 - 1; r >= r0; --r) {
-        Aff m;
-        const double2 di = dinv[r];
-        m.Q = c_mul(di, b[r]);
-        if (r == nv - 1) m.P = make_double2(0.0, 0.0);
+    a.P = c_make<C>(1.0, 0.0);
+    a.Q = c_make<C>(0.0, 0.0);
+    for (int r = r1 - 1, q = q0 + (r1 - 1 - r0); r >= r0; --r, --q) {
+        Aff<C> m;
+        const C d = DI(r, q);
+        m.Q = c_mul(d, b[q]);
+        if (r == nv - 1) m.P = c_make<C>(0.0, 0.0);
         else {
-            const double2 nu = c_mul(di, c_rmul(lam, gamma[r]));
-            m.P = make_double2(-nu.x, -nu.y);
+            const C nu = c_mul(d, c_rmul(lam, GA(r, q)));
+            m.P = c_make<C>(-nu.x, -nu.y);
         }
         a = aff_combine(a, m);
     }
-    double2 x = block_scan_aff(a, false, shw);
-    for (int r = r1 - 1; r >= r0; --r) {
-        const double2 di = dinv[r];
-        if (r == nv - 1) x = c_mul(di, b[r]);
+    C x = block_scan_aff<C>(a, false, shw);
+    for (int r = r1 - 1, q = q0 + (r1 - 1 - r0); r >= r0; --r, --q) {
+        const C d = DI(r, q);
+        if (r == nv - 1) x = c_mul(d, b[q]);
         else {
-            const double2 c = c_rmul(lam, gamma[r]);
-            x = c_mul(di, c_sub(b[r], c_mul(c, x)));
+            const C cc = c_rmul(lam, GA(r, q));
+            x = c_mul(d, c_sub(b[q], c_mul(cc, x)));
         }
         line[r] = x;
     }

@@ -517,7 +517,7 @@ k_moments_poisson(const double* __restrict__ part, const double* __restrict__ n_
         buf[bitrev(m, p.logM)] = make_double2(b0, b1);
     }
     __syncthreads();
-    smem_fft<-1>(buf, 1, M, p.tw);
+    block_fft<-1>(buf, M, p.tw);
     // split into X_k (k = 0..M), divide, rebuild Z for the inverse in place:
     // every thread handles the pair (k, M-k) so the in-place update is safe.
     double2* X2 = reinterpret_cast<double2*>(ph);  // reuse ph storage: needs (M+1) complex = nx+2 doubles
@@ -544,7 +544,7 @@ k_moments_poisson(const double* __restrict__ part, const double* __restrict__ n_
         buf[bitrev(k, p.logM)] = make_double2(E.x - O.y, E.y + O.x);
     }
     __syncthreads();
-    smem_fft<+1>(buf, 1, M, p.tw);
+    block_fft<+1>(buf, M, p.tw);
     const double sc = 1.0 / (double)M;
     double* phs = reinterpret_cast<double*>(X2);  // overwrite: phi in smem
     __syncthreads();
