@@ -63,6 +63,13 @@ enum vv_order {              /* arithmetic of the bracket kernels             */
     VV_ORDER_FACTORED = 0,   /* separable-h coefficient form (fast, default)   */
     VV_ORDER_REFERENCE = 1   /* the reference loop's operation order, no FMA   */
 };
+enum vv_precision {          /* arithmetic of the linear (GMRES) solve        */
+    VV_PRECISION_FP64 = 0,   /* everything in FP64, as the reference           */
+    VV_PRECISION_MIXED = 1   /* GMRES basis, JVP and preconditioner in FP32;
+                                residual, Picard decisions, moments, Poisson
+                                and invariants in FP64 (the Picard loop refines
+                                the FP32 linear solves to the FP64 residual)   */
+};
 
 /* ---- grid and run parameters (runspec.cfg [grid], [initial_data]) ------- */
 typedef struct vv_grid {
@@ -78,7 +85,7 @@ typedef struct vv_grid {
     int32_t laplace;         /* enum vv_laplace                               */
     int32_t order;           /* enum vv_order                                 */
     int32_t gmres_restart;   /* restart length (PETSc default 30), <= 64      */
-    int32_t reserved;
+    int32_t precision;       /* enum vv_precision                             */
 } vv_grid;
 
 typedef struct vv_ctx vv_ctx;

@@ -18,6 +18,7 @@ BRACKET = {"arakawaj1": 1, "arakawaj2": 2, "arakawaj4": 4}
 PC_NONE, PC_TENSOR_KINETIC = 0, 1
 LAPLACE = {"cfd4": 4}
 ORDER_FACTORED, ORDER_REFERENCE = 0, 1
+PRECISION = {"fp64": 0, "mixed": 1}
 MAX_PICARD = 64
 
 # PETSc KSPConvergedReason names for the reasons the GMRES driver reports
@@ -29,7 +30,7 @@ class vv_grid(C.Structure):
     _fields_ = [("nx", C.c_int32), ("nv", C.c_int32), ("L", C.c_double), ("vmin", C.c_double),
                 ("vmax", C.c_double), ("ht", C.c_double), ("charge", C.c_double), ("mass", C.c_double),
                 ("bracket", C.c_int32), ("preconditioner", C.c_int32), ("laplace", C.c_int32),
-                ("order", C.c_int32), ("gmres_restart", C.c_int32), ("reserved", C.c_int32)]
+                ("order", C.c_int32), ("gmres_restart", C.c_int32), ("precision", C.c_int32)]
 
 
 class vv_ksp_opts(C.Structure):

@@ -21,6 +21,7 @@
 #include <cstddef>
 #include <cstdio>
 #include <cstring>
+#include <type_traits>
 #include <vector>
 
 using cd = std::complex<double>;
@@ -37,6 +38,12 @@ struct vv_ctx {
     double2 *spec, *tw, *lambda, *dinv;
     double *alpha, *gamma, *sym_inv;
     vv::DevState* ds;
+    // single-precision operands of the mixed mode (GMRES basis, JVP, preconditioner)
+    bool mixed;
+    float *V32, *tmp32, *bvec32, *delta32, *alpha32, *gamma32;
+    float2 *spec32, *tw32, *lambda32, *dinv32;
+    size_t smem_rfft32, smem_irfft32, smem_tri32;
+    bool tri_stage32;
     // pinned host staging
     double* hpin;
     int* hstat;
@@ -92,9 +99,9 @@ int fail_cuda(cudaError_t e, const char* what) {
         cudaError_t e_ = cudaGetLastError();                       \
         if (e_ != cudaSuccess) return fail_cuda(e_, "kernel launch"); \
     } while (0)
-#define TRY(x)                    \
-    do {                          \
-        int s_ = (x);             \
+#define TRY(...)                    \
+    do {                            \
+        int s_ = (__VA_ARGS__);     \
         if (s_ != VV_OK) return s_; \
     } while (0)
 
@@ -185,9 +192,8 @@ bool wide_ok(const vv_ctx* c, const void* X, const void* Xh, const void* Y) {
 }
 
 // X may be a GMRES basis base pointer with xidx -> the vector index in the state
-template <int SCHEME, int MODE>
-int launch_bracket_s(vv_ctx* c, const double* X, const double* Xh, double* Y, double factor, double* sumsq,
-                     const int* xidx) {
+template <int SCHEME, int MODE, typename T>
+int launch_bracket_s(vv_ctx* c, const T* X, const T* Xh, T* Y, double factor, double* sumsq, const int* xidx) {
     dim3 grid((c->nx + vv::BX - 1) / vv::BX, (c->nv + vv::BY - 1) / vv::BY);
     dim3 block(vv::BX, vv::TY);
     vv::BracketParams p = bparams(c, factor);
@@ -201,26 +207,33 @@ int launch_bracket_s(vv_ctx* c, const double* X, const double* Xh, double* Y, do
         e1 = next_event(c);
         if (e0) cudaEventRecord(e0, c->st);
     }
-    if (c->g.order == VV_ORDER_REFERENCE) {
-        vv::k_bracket_ref<SCHEME, MODE><<<grid, block, 0, c->st>>>(X, Xh, Y, p, sumsq);
-    } else if (wide_ok(c, X, Xh, Y)) {
-        dim3 gw(c->nx / vv::WX, (c->nv + vv::WY - 1) / vv::WY);
-        vv::k_bracket_wide<SCHEME, MODE, double><<<gw, vv::WTHREADS, 0, c->st>>>(X, Xh, Y, p, sumsq);
-    } else {
-        vv::k_bracket_fac<SCHEME, MODE, double><<<grid, block, 0, c->st>>>(X, Xh, Y, p, sumsq);
+    bool done = false;
+    if constexpr (std::is_same<T, double>::value) {
+        if (c->g.order == VV_ORDER_REFERENCE) {
+            vv::k_bracket_ref<SCHEME, MODE><<<grid, block, 0, c->st>>>(X, Xh, Y, p, sumsq);
+            done = true;
+        }
+    }
+    if (!done) {
+        if (wide_ok(c, X, Xh, Y)) {
+            dim3 gw(c->nx / vv::WX, (c->nv + vv::WY - 1) / vv::WY);
+            vv::k_bracket_wide<SCHEME, MODE, T><<<gw, vv::WTHREADS, 0, c->st>>>(X, Xh, Y, p, sumsq);
+        } else {
+            vv::k_bracket_fac<SCHEME, MODE, T><<<grid, block, 0, c->st>>>(X, Xh, Y, p, sumsq);
+        }
     }
     CKL(c);
     if (timed && e1) cudaEventRecord(e1, c->st);
     return VV_OK;
 }
 
-template <int MODE>
-int launch_bracket(vv_ctx* c, const double* X, const double* Xh, double* Y, double factor, double* sumsq,
+template <int MODE, typename T>
+int launch_bracket(vv_ctx* c, const T* X, const T* Xh, T* Y, double factor, double* sumsq,
                    const int* xidx = nullptr) {
     switch (c->g.bracket) {
-        case VV_BRACKET_J1: return launch_bracket_s<1, MODE>(c, X, Xh, Y, factor, sumsq, xidx);
-        case VV_BRACKET_J2: return launch_bracket_s<2, MODE>(c, X, Xh, Y, factor, sumsq, xidx);
-        default: return launch_bracket_s<4, MODE>(c, X, Xh, Y, factor, sumsq, xidx);
+        case VV_BRACKET_J1: return launch_bracket_s<1, MODE, T>(c, X, Xh, Y, factor, sumsq, xidx);
+        case VV_BRACKET_J2: return launch_bracket_s<2, MODE, T>(c, X, Xh, Y, factor, sumsq, xidx);
+        default: return launch_bracket_s<4, MODE, T>(c, X, Xh, Y, factor, sumsq, xidx);
     }
 }
 
@@ -246,54 +259,90 @@ int read_scalar(vv_ctx* c, const double* dsrc, double* out) {
 }
 
 // ---- preconditioner ---------------------------------------------------------
-// Y may be a GMRES basis base pointer with yidx -> the vector index (+yoff)
-int pc_apply(vv_ctx* c, const double* X, double* Y, const int* yidx = nullptr, int yoff = 0) {
+// P^-1 with input type TI, arithmetic R (double: FP64 tables and spectrum,
+// float: the mixed mode's FP32 copies) and output type TO.  Y may be a GMRES
+// basis base pointer with yidx -> the vector index (+yoff).
+template <typename TI, typename R, typename TO>
+int pc_apply_t(vv_ctx* c, const TI* X, TO* Y, const int* yidx = nullptr, int yoff = 0) {
+    constexpr bool D = std::is_same<R, double>::value;
+    using C2 = typename Cplx<R>::type;
     vv::PcParams p = pcparams(c);
+    C2* spec = D ? reinterpret_cast<C2*>(c->spec) : reinterpret_cast<C2*>(c->spec32);
+    p.tw = D ? (const void*)c->tw : (const void*)c->tw32;
+    const size_t sm_f = D ? c->smem_rfft : c->smem_rfft32;
+    const size_t sm_i = D ? c->smem_irfft : c->smem_irfft32;
+    const size_t sm_t = D ? c->smem_tri : c->smem_tri32;
+    const bool stage = D ? c->tri_stage : c->tri_stage32;
     const unsigned rows = (unsigned)((c->nv + c->pcR - 1) / c->pcR);
-    vv::k_rfft_rows<double, double><<<rows, 32 * c->pcR, c->smem_rfft, c->st>>>(X, c->spec, p);
+    vv::k_rfft_rows<TI, R><<<rows, 32 * c->pcR, sm_f, c->st>>>(X, spec, p);
     CKL(c);
     vv::TriParams t;
     t.nv = c->nv;
     t.nmodes = c->nmodes;
-    t.lambda = c->lambda;
-    t.alpha = c->alpha;
-    t.gamma = c->gamma;
-    t.dinv = c->dinv;
-    if (c->tri_stage)
-        vv::k_tridiag_modes<double, true><<<c->nmodes, vv::TRI_THREADS, c->smem_tri, c->st>>>(c->spec, t);
+    t.lambda = D ? (const void*)c->lambda : (const void*)c->lambda32;
+    t.alpha = D ? (const void*)c->alpha : (const void*)c->alpha32;
+    t.gamma = D ? (const void*)c->gamma : (const void*)c->gamma32;
+    t.dinv = D ? (const void*)c->dinv : (const void*)c->dinv32;
+    if (stage)
+        vv::k_tridiag_modes<R, true><<<c->nmodes, vv::TRI_THREADS, sm_t, c->st>>>(spec, t);
     else
-        vv::k_tridiag_modes<double, false><<<c->nmodes, vv::TRI_THREADS, c->smem_tri, c->st>>>(c->spec, t);
+        vv::k_tridiag_modes<R, false><<<c->nmodes, vv::TRI_THREADS, sm_t, c->st>>>(spec, t);
     CKL(c);
     p.yidx = yidx;
     p.yoff = yoff;
     p.ystride = yidx ? c->ncell : 0;
-    vv::k_irfft_rows<double, double><<<rows, 32 * c->pcR, c->smem_irfft, c->st>>>(c->spec, Y, p);
+    vv::k_irfft_rows<R, TO><<<rows, 32 * c->pcR, sm_i, c->st>>>(spec, Y, p);
     CKL(c);
     return VV_OK;
 }
 
-// Y = P^-1 J X (or J X)
-int apply_operator(vv_ctx* c, const double* X, double* Y) {
-    if (c->g.preconditioner == VV_PC_TENSOR_KINETIC) {
-        TRY(launch_bracket<vv::MODE_JVP>(c, X, nullptr, c->tmp, 0.5, nullptr));
-        return pc_apply(c, c->tmp, Y);
-    }
-    return launch_bracket<vv::MODE_JVP>(c, X, nullptr, Y, 0.5, nullptr);
+int pc_apply(vv_ctx* c, const double* X, double* Y, const int* yidx = nullptr, int yoff = 0) {
+    return pc_apply_t<double, double, double>(c, X, Y, yidx, yoff);
 }
 
-__global__ void k_copy_to_slot(const double* __restrict__ src, double* __restrict__ V, const int* __restrict__ idx,
+// buffers of the GMRES solve in precision T
+template <typename T> struct Buf;
+template <> struct Buf<double> {
+    static double* V(vv_ctx* c) { return c->V; }
+    static double* tmp(vv_ctx* c) { return c->tmp; }
+    static double* b(vv_ctx* c) { return c->bvec; }
+    static double* x(vv_ctx* c) { return c->delta; }
+};
+template <> struct Buf<float> {
+    static float* V(vv_ctx* c) { return c->V32; }
+    static float* tmp(vv_ctx* c) { return c->tmp32; }
+    static float* b(vv_ctx* c) { return c->bvec32; }
+    static float* x(vv_ctx* c) { return c->delta32; }
+};
+
+// Y = P^-1 J X (or J X) in precision T
+template <typename T>
+int apply_operator_t(vv_ctx* c, const T* X, T* Y) {
+    if (c->g.preconditioner == VV_PC_TENSOR_KINETIC) {
+        TRY(launch_bracket<vv::MODE_JVP, T>(c, X, nullptr, Buf<T>::tmp(c), 0.5, nullptr));
+        return pc_apply_t<T, T, T>(c, Buf<T>::tmp(c), Y);
+    }
+    return launch_bracket<vv::MODE_JVP, T>(c, X, nullptr, Y, 0.5, nullptr);
+}
+
+int apply_operator(vv_ctx* c, const double* X, double* Y) { return apply_operator_t<double>(c, X, Y); }
+
+template <typename T>
+__global__ void k_copy_to_slot(const T* __restrict__ src, T* __restrict__ V, const int* __restrict__ idx,
                                size_t n) {
-    double* dst = V + (size_t)(*idx + 1) * n;
+    T* dst = V + (size_t)(*idx + 1) * n;
     for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
         dst[i] = src[i];
 }
 
 // Arnoldi operator V[it] -> V[it+1], it read from the device state
+template <typename T>
 int apply_operator_state(vv_ctx* c) {
     const int* itp = &c->ds->it;
-    TRY(launch_bracket<vv::MODE_JVP>(c, c->V, nullptr, c->tmp, 0.5, nullptr, itp));
-    if (c->g.preconditioner == VV_PC_TENSOR_KINETIC) return pc_apply(c, c->tmp, c->V, itp, 1);
-    k_copy_to_slot<<<grid1d(c->ncell, 256), 256, 0, c->st>>>(c->tmp, c->V, itp, c->ncell);
+    T* V = Buf<T>::V(c);
+    TRY(launch_bracket<vv::MODE_JVP, T>(c, V, nullptr, Buf<T>::tmp(c), 0.5, nullptr, itp));
+    if (c->g.preconditioner == VV_PC_TENSOR_KINETIC) return pc_apply_t<T, T, T>(c, Buf<T>::tmp(c), V, itp, 1);
+    k_copy_to_slot<T><<<grid1d(c->ncell, 256), 256, 0, c->st>>>(Buf<T>::tmp(c), V, itp, c->ncell);
     CKL(c);
     return VV_OK;
 }
@@ -417,43 +466,57 @@ int upload_options(vv_ctx* c, const vv_ksp_opts* o, const vv_snes_opts* so) {
     return VV_OK;
 }
 
-int gm_init(vv_ctx* c, double* x) {
-    vv::k_gm_init<double><<<grid1d(c->ncell, 256), 256, 0, c->st>>>(c->ds, x, c->ncell);
+template <typename T>
+int gm_init(vv_ctx* c, T* x) {
+    vv::k_gm_init<T><<<grid1d(c->ncell, 256), 256, 0, c->st>>>(c->ds, x, c->ncell);
     CKL(c);
+    return VV_OK;
+}
+
+template <typename T>
+int copy_t(vv_ctx* c, T* dst, const T* src, size_t count) {
+    if (!dst || !src || dst == src) return VV_OK;
+    CK(cudaMemcpyAsync(dst, src, count * sizeof(T), cudaMemcpyDeviceToDevice, c->st));
     return VV_OK;
 }
 
 // V0 = b (first cycle) or b - A x (restart)
-int gm_cycle_head(vv_ctx* c, const double* b, const double* x, bool first) {
-    if (first) return copy_d(c, c->V, b, c->ncell);
-    TRY(apply_operator(c, x, c->V));
-    vv::k_axpby<double><<<grid1d(c->ncell, 256), 256, 0, c->st>>>(b, c->V, c->ncell, 1.0, -1.0);
+template <typename T>
+int gm_cycle_head(vv_ctx* c, const T* b, const T* x, bool first) {
+    T* V = Buf<T>::V(c);
+    if (first) return copy_t<T>(c, V, b, c->ncell);
+    TRY(apply_operator_t<T>(c, x, V));
+    vv::k_axpby<T><<<grid1d(c->ncell, 256), 256, 0, c->st>>>(b, V, c->ncell, 1.0, -1.0);
     CKL(c);
     return VV_OK;
 }
 
+template <typename T>
 int gm_cycle_start(vv_ctx* c) {
-    vv::k_gm_cycle<double><<<c->npart, vv::RED_THREADS, 0, c->st>>>(c->ds, c->V, c->ncell, c->part);
+    T* V = Buf<T>::V(c);
+    vv::k_gm_cycle<T><<<c->npart, vv::RED_THREADS, 0, c->st>>>(c->ds, V, c->ncell, c->part);
     CKL(c);
-    vv::k_gm_scale<double><<<grid1d(c->ncell, 256), 256, 0, c->st>>>(c->ds, c->V, c->ncell, c->ncell);
+    vv::k_gm_scale<T><<<grid1d(c->ncell, 256), 256, 0, c->st>>>(c->ds, V, c->ncell, c->ncell);
     CKL(c);
     return VV_OK;
 }
 
+template <typename T>
 int gm_arnoldi(vv_ctx* c) {
-    TRY(apply_operator_state(c));
-    vv::k_gm_mdot<double><<<c->npart, vv::RED_THREADS, 0, c->st>>>(c->ds, c->V, c->ncell, c->ncell, c->part,
-                                                                   c->npart_max);
+    T* V = Buf<T>::V(c);
+    TRY(apply_operator_state<T>(c));
+    vv::k_gm_mdot<T><<<c->npart, vv::RED_THREADS, 0, c->st>>>(c->ds, V, c->ncell, c->ncell, c->part, c->npart_max);
     CKL(c);
-    vv::k_gm_maxpy<double><<<c->npart, vv::RED_THREADS, 0, c->st>>>(c->ds, c->V, c->ncell, c->ncell, c->part);
+    vv::k_gm_maxpy<T><<<c->npart, vv::RED_THREADS, 0, c->st>>>(c->ds, V, c->ncell, c->ncell, c->part);
     CKL(c);
-    vv::k_gm_scale<double><<<grid1d(c->ncell, 256), 256, 0, c->st>>>(c->ds, c->V, c->ncell, c->ncell);
+    vv::k_gm_scale<T><<<grid1d(c->ncell, 256), 256, 0, c->st>>>(c->ds, V, c->ncell, c->ncell);
     CKL(c);
     return VV_OK;
 }
 
-int gm_finish(vv_ctx* c, double* x) {
-    vv::k_gm_finish<double><<<c->npart, vv::RED_THREADS, 0, c->st>>>(c->ds, c->V, c->ncell, x, c->ncell);
+template <typename T>
+int gm_finish(vv_ctx* c, T* x) {
+    vv::k_gm_finish<T><<<c->npart, vv::RED_THREADS, 0, c->st>>>(c->ds, Buf<T>::V(c), c->ncell, x, c->ncell);
     CKL(c);
     return VV_OK;
 }
@@ -471,19 +534,20 @@ int read_head(vv_ctx* c, GmHead* h) {
 
 // Host-driven GMRES: the same kernels, with the host reading the 16-byte
 // status block after every Arnoldi step.
-int gmres_host(vv_ctx* c, const double* b, double* x, vv_ksp_result* res) {
-    TRY(gm_init(c, x));
+template <typename T>
+int gmres_host(vv_ctx* c, const T* b, T* x, vv_ksp_result* res) {
+    TRY(gm_init<T>(c, x));
     bool first = true;
     GmHead h{};
     for (;;) {
-        TRY(gm_cycle_head(c, b, x, first));
-        TRY(gm_cycle_start(c));
+        TRY(gm_cycle_head<T>(c, b, x, first));
+        TRY(gm_cycle_start<T>(c));
         TRY(read_head(c, &h));
         while (h.active) {
-            TRY(gm_arnoldi(c));
+            TRY(gm_arnoldi<T>(c));
             TRY(read_head(c, &h));
         }
-        TRY(gm_finish(c, x));
+        TRY(gm_finish<T>(c, x));
         TRY(read_head(c, &h));
         if (h.reason != 0) break;
         first = false;
@@ -504,6 +568,11 @@ int gmres_host(vv_ctx* c, const double* b, double* x, vv_ksp_result* res) {
 // conditional nodes of child graphs) with a default applied at every launch.
 int add_conditional(cudaGraph_t owner, cudaStream_t cs, cudaGraphConditionalNodeType type, unsigned size,
                     unsigned defval, unsigned long long* handle_out, cudaGraph_t* bodies) {
+    static const bool dbg = getenv("VV_DEBUG") != nullptr;
+    if (dbg) {
+        fprintf(stderr, "[vv] add_conditional type=%d size=%u\n", (int)type, size);
+        fflush(stderr);
+    }
     cudaStreamCaptureStatus status;
     const cudaGraphNode_t* deps = nullptr;
     size_t nd = 0;
@@ -541,29 +610,31 @@ int capture_body(vv_ctx* c, cudaStream_t s, cudaGraph_t body, int* nkernels, F f
     return VV_OK;
 }
 
-// GMRES solve b -> x into the graph being captured on cs[level]
-int capture_gmres(vv_ctx* c, int level, const double* b, double* x) {
-    TRY(gm_init(c, x));
+// GMRES solve b -> x into the graph being captured on c->st (level = depth of c->st)
+template <typename T>
+int capture_gmres(vv_ctx* c, int level, const T* b, T* x) {
+    TRY(gm_init<T>(c, x));
     cudaGraph_t outer[1];
     TRY(add_conditional(c->cap_owner, c->st, cudaGraphCondTypeWhile, 1, 1, &c->hnd[0], outer));
     const int l1 = level + 1;
     return capture_body(c, c->cs[l1], outer[0], &c->nk_cycle, [&]() -> int {
         cudaGraph_t br[2];
         TRY(add_conditional(c->cap_owner, c->cs[l1], cudaGraphCondTypeIf, 2, 1, &c->hnd[2], br));
-        TRY(capture_body(c, c->cs[l1 + 1], br[0], nullptr, [&]() { return gm_cycle_head(c, b, x, true); }));
-        TRY(capture_body(c, c->cs[l1 + 1], br[1], &c->nk_restart, [&]() { return gm_cycle_head(c, b, x, false); }));
-        TRY(gm_cycle_start(c));
+        TRY(capture_body(c, c->cs[l1 + 1], br[0], nullptr, [&]() { return gm_cycle_head<T>(c, b, x, true); }));
+        TRY(capture_body(c, c->cs[l1 + 1], br[1], &c->nk_restart,
+                         [&]() { return gm_cycle_head<T>(c, b, x, false); }));
+        TRY(gm_cycle_start<T>(c));
         cudaGraph_t inner[1];
         TRY(add_conditional(c->cap_owner, c->cs[l1], cudaGraphCondTypeWhile, 1, 0, &c->hnd[1], inner));
-        TRY(capture_body(c, c->cs[l1 + 1], inner[0], &c->nk_arnoldi, [&]() { return gm_arnoldi(c); }));
-        return gm_finish(c, x);
+        TRY(capture_body(c, c->cs[l1 + 1], inner[0], &c->nk_arnoldi, [&]() { return gm_arnoldi<T>(c); }));
+        return gm_finish<T>(c, x);
     });
 }
 
 // ---- residual / moments helpers of the step ---------------------------------
 int residual_norm(vv_ctx* c, const double* F, double* Y, double* out) {
     const int tiles = bracket_tiles(c, F, c->Fh, Y);
-    TRY(launch_bracket<vv::MODE_RESIDUAL>(c, F, c->Fh, Y, 1.0, c->part));
+    TRY(launch_bracket<vv::MODE_RESIDUAL, double>(c, F, c->Fh, Y, 1.0, c->part));
     TRY(reduce_to(c, c->part, tiles, c->scal + 2));
     double s2 = 0.0;
     TRY(read_scalar(c, c->scal + 2, &s2));
@@ -589,7 +660,7 @@ int calc_moments(vv_ctx* c, vv_state* st) {
 // then the Picard decision kernel (phase 0: initial residual)
 int step_residual(vv_ctx* c, vv_state* st, int phase) {
     const int tiles = bracket_tiles(c, st->f, c->Fh, c->tmp);
-    TRY(launch_bracket<vv::MODE_RESIDUAL>(c, st->f, c->Fh, c->tmp, 1.0, c->part));
+    TRY(launch_bracket<vv::MODE_RESIDUAL, double>(c, st->f, c->Fh, c->tmp, 1.0, c->part));
     TRY(poisson_apply(c, st->phi, st->n, nullptr, 2, &c->ds->pnorm2));
     vv::k_pic_residual<<<1, 32, 0, c->st>>>(c->ds, c->part, tiles, phase);
     CKL(c);
@@ -613,12 +684,21 @@ int step_prologue(vv_ctx* c, vv_state* st) {
 // with R(f) left in tmp by the last residual evaluation (same Fh and Have)
 int step_rhs(vv_ctx* c, vv_state* st) {
     TRY(copy_d(c, c->fl, st->f, c->ncell));
+    if (c->mixed) {   // FP64 residual -> FP32 right-hand side
+        if (c->g.preconditioner == VV_PC_TENSOR_KINETIC) return pc_apply_t<double, float, float>(c, c->tmp, c->bvec32);
+        vv::k_scale<double, float><<<grid1d(c->ncell, 256), 256, 0, c->st>>>(c->tmp, c->bvec32, c->ncell, nullptr, 1.0);
+        CKL(c);
+        return VV_OK;
+    }
     if (c->g.preconditioner == VV_PC_TENSOR_KINETIC) return pc_apply(c, c->tmp, c->bvec);
     return copy_d(c, c->bvec, c->tmp, c->ncell);
 }
 
 int step_after_solve(vv_ctx* c, vv_state* st) {
-    vv::k_pic_apply<double><<<grid1d(c->ncell, 256), 256, 0, c->st>>>(c->ds, c->delta, st->f, c->ncell);
+    if (c->mixed)
+        vv::k_pic_apply<float, double><<<grid1d(c->ncell, 256), 256, 0, c->st>>>(c->ds, c->delta32, st->f, c->ncell);
+    else
+        vv::k_pic_apply<double, double><<<grid1d(c->ncell, 256), 256, 0, c->st>>>(c->ds, c->delta, st->f, c->ncell);
     CKL(c);
     TRY(calc_moments(c, st));
     TRY(copy_d(c, c->hxp, st->h1c, c->nx));   // update_previous: H1p <- h1c
@@ -652,7 +732,8 @@ int capture_step(vv_ctx* c, vv_state* st, cudaGraph_t owner) {
     TRY(add_conditional(owner, c->st, cudaGraphCondTypeWhile, 1, 0, &c->hnd[3], pic));
     TRY(capture_body(c, c->cs[1], pic[0], &c->nk_pic, [&]() -> int {
         TRY(step_rhs(c, st));
-        TRY(capture_gmres(c, 1, c->bvec, c->delta));
+        if (c->mixed) TRY(capture_gmres<float>(c, 1, c->bvec32, c->delta32));
+        else TRY(capture_gmres<double>(c, 1, c->bvec, c->delta));
         return step_after_solve(c, st);
     }));
     cudaGraph_t rev[1];
@@ -727,7 +808,8 @@ int step_host(vv_ctx* c, vv_state* st) {
     TRY(step_prologue(c, st));
     for (;;) {
         TRY(step_rhs(c, st));
-        TRY(gmres_host(c, c->bvec, c->delta, nullptr));
+        if (c->mixed) TRY(gmres_host<float>(c, c->bvec32, c->delta32, nullptr));
+        else TRY(gmres_host<double>(c, c->bvec, c->delta, nullptr));
         TRY(step_after_solve(c, st));
         int act = 0;
         CK(cudaMemcpyAsync(c->hstat, &c->ds->pic_active, sizeof(int), cudaMemcpyDeviceToHost, c->st));
@@ -780,6 +862,7 @@ int vv_create(const vv_grid* grid, vv_ctx** out) {
     if (g.laplace != VV_LAPLACE_CFD4) return VV_ERR_UNSUPPORTED;
     const int restart = g.gmres_restart > 0 ? g.gmres_restart : 30;
     if (restart > vv::MAX_RESTART) return VV_ERR_ARG;
+    if (g.precision != VV_PRECISION_FP64 && g.precision != VV_PRECISION_MIXED) return VV_ERR_ARG;
 
     vv_ctx* c = new vv_ctx();
     c->g = g;
@@ -790,6 +873,7 @@ int vv_create(const vv_grid* grid, vv_ctx** out) {
     c->logM = ilog2(c->M);
     c->nmodes = c->M + 1;
     c->restart = restart;
+    c->mixed = g.precision == VV_PRECISION_MIXED;
     c->ncell = (size_t)g.nx * g.nv;
     c->st = 0;
     cudaGetDevice(&c->device);
@@ -827,7 +911,11 @@ int vv_create(const vv_grid* grid, vv_ctx** out) {
         const size_t np = (size_t)nv + (nv + ch - 1) / ch;
         c->tri_stage = np * 48 <= 200 * 1024;
         c->smem_tri = c->tri_stage ? np * 48 : np * sizeof(double2);
+        c->tri_stage32 = np * 24 <= 200 * 1024;
+        c->smem_tri32 = c->tri_stage32 ? np * 24 : np * sizeof(float2);
     }
+    c->smem_rfft32 = (size_t)(M + c->pcR * (M + 1)) * sizeof(float2);
+    c->smem_irfft32 = (size_t)(M + 2 * c->pcR * (M + 1)) * sizeof(float2);
     c->smem_pois = (size_t)M * sizeof(double2) + (size_t)nx * sizeof(double) + (size_t)(nx + 2) * sizeof(double);
 
     int s = VV_OK;
@@ -836,12 +924,21 @@ int vv_create(const vv_grid* grid, vv_ctx** out) {
                                         (size_t)vv::INV_NPART * c->npart_max});
     if ((s = dalloc(&c->v, nv)) || (s = dalloc(&c->h0, nv)) || (s = dalloc(&c->hxp, 4 * (size_t)nx)) ||
         (s = dalloc(&c->Fh, n)) || (s = dalloc(&c->tmp, n)) || (s = dalloc(&c->bvec, n)) ||
-        (s = dalloc(&c->delta, n)) || (s = dalloc(&c->fl, n)) || (s = dalloc(&c->V, (size_t)(restart + 1) * n)) ||
+        (s = dalloc(&c->delta, n)) || (s = dalloc(&c->fl, n)) ||
+        (s = dalloc(&c->V, (size_t)(c->mixed ? 1 : restart + 1) * n)) ||
         (s = dalloc(&c->part, part_count)) || (s = dalloc(&c->scal, 64)) || (s = dalloc(&c->xscratch, 2 * (size_t)nx)) ||
         (s = dalloc(&c->mom_part, (size_t)c->mom_S * 3 * nx)) || (s = dalloc(&c->spec, (size_t)nm * nv)) ||
         (s = dalloc(&c->tw, (size_t)std::max(1, nx / 2))) || (s = dalloc(&c->lambda, nm)) ||
         (s = dalloc(&c->dinv, (size_t)nm * nv)) || (s = dalloc(&c->alpha, nv)) || (s = dalloc(&c->gamma, nv)) ||
         (s = dalloc(&c->sym_inv, nm)) || (s = dalloc(&c->ds, 1))) {
+        vv_destroy(c);
+        return s;
+    }
+    if (c->mixed &&
+        ((s = dalloc(&c->V32, (size_t)(restart + 1) * n)) || (s = dalloc(&c->tmp32, n)) || (s = dalloc(&c->bvec32, n)) ||
+         (s = dalloc(&c->delta32, n)) || (s = dalloc(&c->alpha32, nv)) || (s = dalloc(&c->gamma32, nv)) ||
+         (s = dalloc(&c->spec32, (size_t)nm * nv)) || (s = dalloc(&c->tw32, (size_t)std::max(1, nx / 2))) ||
+         (s = dalloc(&c->lambda32, nm)) || (s = dalloc(&c->dinv32, (size_t)nm * nv)))) {
         vv_destroy(c);
         return s;
     }
@@ -932,6 +1029,35 @@ int vv_create(const vv_grid* grid, vv_ctx** out) {
         vv_destroy(c);
         return fail_cuda(cudaGetLastError(), "vv_create upload");
     }
+    if (c->mixed) {
+        std::vector<float> a32(alpha.begin(), alpha.end()), g32(gamma.begin(), gamma.end());
+        std::vector<float2> tw32(tw.size()), lam32(nm), dinv32(dinv.size());
+        for (size_t k = 0; k < tw.size(); ++k) tw32[k] = make_float2((float)tw[k].x, (float)tw[k].y);
+        for (int k = 0; k < nm; ++k) lam32[k] = make_float2((float)lam2[k].x, (float)lam2[k].y);
+        for (size_t k = 0; k < dinv.size(); ++k) dinv32[k] = make_float2((float)dinv[k].x, (float)dinv[k].y);
+        if (cudaMemcpy(c->alpha32, a32.data(), nv * sizeof(float), cudaMemcpyHostToDevice) != cudaSuccess ||
+            cudaMemcpy(c->gamma32, g32.data(), nv * sizeof(float), cudaMemcpyHostToDevice) != cudaSuccess ||
+            cudaMemcpy(c->tw32, tw32.data(), tw32.size() * sizeof(float2), cudaMemcpyHostToDevice) != cudaSuccess ||
+            cudaMemcpy(c->lambda32, lam32.data(), nm * sizeof(float2), cudaMemcpyHostToDevice) != cudaSuccess ||
+            cudaMemcpy(c->dinv32, dinv32.data(), dinv32.size() * sizeof(float2), cudaMemcpyHostToDevice) !=
+                cudaSuccess) {
+            vv_destroy(c);
+            return fail_cuda(cudaGetLastError(), "vv_create upload (fp32)");
+        }
+        if (cudaFuncSetAttribute(vv::k_rfft_rows<double, float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)c->smem_rfft32) != cudaSuccess ||
+            cudaFuncSetAttribute(vv::k_rfft_rows<float, float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)c->smem_rfft32) != cudaSuccess ||
+            cudaFuncSetAttribute(vv::k_irfft_rows<float, float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)c->smem_irfft32) != cudaSuccess ||
+            cudaFuncSetAttribute(vv::k_tridiag_modes<float, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)c->smem_tri32) != cudaSuccess ||
+            cudaFuncSetAttribute(vv::k_tridiag_modes<float, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)c->smem_tri32) != cudaSuccess) {
+            vv_destroy(c);
+            return fail_cuda(cudaGetLastError(), "cudaFuncSetAttribute (fp32)");
+        }
+    }
     // dynamic shared memory limits
     if (cudaFuncSetAttribute(vv::k_rfft_rows<double, double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              (int)c->smem_rfft) != cudaSuccess ||
@@ -954,7 +1080,8 @@ int vv_destroy(vv_ctx* c) {
     if (!c) return VV_OK;
     void* bufs[] = {c->v, c->h0, c->hxp, c->Fh, c->tmp, c->bvec, c->delta, c->fl, c->V, c->part, c->scal,
                     c->xscratch, c->mom_part, c->spec, c->tw, c->lambda, c->dinv, c->alpha, c->gamma,
-                    c->sym_inv, c->ds};
+                    c->sym_inv, c->ds, c->V32, c->tmp32, c->bvec32, c->delta32, c->alpha32, c->gamma32,
+                    c->spec32, c->tw32, c->lambda32, c->dinv32};
     destroy_graph(c);
     for (int k = 0; k < 4; ++k)
         if (c->cs[k]) cudaStreamDestroy(c->cs[k]);
@@ -994,7 +1121,7 @@ int vv_update_previous(vv_ctx* c, const double* h1p, const double* h1h, const do
 int vv_function(vv_ctx* c, const double* F, double* Y, int apply_pc) {
     if (!c || !F || !Y) return VV_ERR_ARG;
     const bool pc = apply_pc && c->g.preconditioner == VV_PC_TENSOR_KINETIC;
-    TRY(launch_bracket<vv::MODE_RESIDUAL>(c, F, c->Fh, pc ? c->tmp : Y, 1.0, nullptr));
+    TRY(launch_bracket<vv::MODE_RESIDUAL, double>(c, F, c->Fh, pc ? c->tmp : Y, 1.0, nullptr));
     if (pc) TRY(pc_apply(c, c->tmp, Y));
     return VV_OK;
 }
@@ -1002,7 +1129,7 @@ int vv_function(vv_ctx* c, const double* F, double* Y, int apply_pc) {
 int vv_jacobian(vv_ctx* c, const double* F, double* Y, int apply_pc) {
     if (!c || !F || !Y) return VV_ERR_ARG;
     const bool pc = apply_pc && c->g.preconditioner == VV_PC_TENSOR_KINETIC;
-    TRY(launch_bracket<vv::MODE_JVP>(c, F, nullptr, pc ? c->tmp : Y, 0.5, nullptr));
+    TRY(launch_bracket<vv::MODE_JVP, double>(c, F, nullptr, pc ? c->tmp : Y, 0.5, nullptr));
     if (pc) TRY(pc_apply(c, c->tmp, Y));
     return VV_OK;
 }
@@ -1014,7 +1141,7 @@ int vv_function_norm(vv_ctx* c, const double* F, double* Y, double* norm) {
 
 int vv_bracket(vv_ctx* c, const double* X, double* Y, double factor) {
     if (!c || !X || !Y) return VV_ERR_ARG;
-    return launch_bracket<vv::MODE_ADD>(c, X, nullptr, Y, factor, nullptr);
+    return launch_bracket<vv::MODE_ADD, double>(c, X, nullptr, Y, factor, nullptr);
 }
 
 int vv_pc_apply(vv_ctx* c, const double* X, double* Y) {
@@ -1069,8 +1196,14 @@ int vv_gmres(vv_ctx* c, const double* b, double* x, const vv_ksp_opts* o, vv_ksp
     c->opts_valid = false;
     for (int k = 0; k < 5; ++k) c->hnd[k] = saved[k];
     TRY(s);
-    // b may alias nothing inside the context; run on the caller's buffers
-    return gmres_host(c, b, x, r);
+    if (!c->mixed) return gmres_host<double>(c, b, x, r);
+    // mixed: FP32 solve of the FP64 system, converted at the boundary
+    vv::k_scale<double, float><<<grid1d(c->ncell, 256), 256, 0, c->st>>>(b, c->bvec32, c->ncell, nullptr, 1.0);
+    CKL(c);
+    TRY(gmres_host<float>(c, c->bvec32, c->delta32, r));
+    vv::k_scale<float, double><<<grid1d(c->ncell, 256), 256, 0, c->st>>>(c->delta32, x, c->ncell, nullptr, 1.0);
+    CKL(c);
+    return VV_OK;
 }
 
 int vv_calculate_moments(vv_ctx* c, vv_state* st) {
@@ -1190,9 +1323,15 @@ int vv_time_kernel(vv_ctx* c, int which, int reps, double* avg_ms) {
     c->st = c->cs[0];
     int r = VV_OK;
     for (int k = 0; k < reps && r == VV_OK; ++k) {
-        if (which == 0) r = launch_bracket<vv::MODE_JVP>(c, c->V, nullptr, c->tmp, 0.5, nullptr);
-        else if (which == 1) r = launch_bracket<vv::MODE_RESIDUAL>(c, c->V, c->Fh, c->tmp, 1.0, nullptr);
-        else r = pc_apply(c, c->V, c->tmp);
+        if (which == 0) {
+            if (c->mixed) r = launch_bracket<vv::MODE_JVP, float>(c, c->V32, nullptr, c->tmp32, 0.5, nullptr);
+            else r = launch_bracket<vv::MODE_JVP, double>(c, c->V, nullptr, c->tmp, 0.5, nullptr);
+        } else if (which == 1) {
+            r = launch_bracket<vv::MODE_RESIDUAL, double>(c, c->V, c->Fh, c->tmp, 1.0, nullptr);
+        } else {
+            if (c->mixed) r = pc_apply_t<float, float, float>(c, c->V32, c->tmp32);
+            else r = pc_apply(c, c->V, c->tmp);
+        }
     }
     c->st = saved;
     cudaError_t e = cudaStreamEndCapture(c->cs[0], &g);
@@ -1265,6 +1404,15 @@ int vv_batch_destroy(vv_batch* b) {
 
 int vv_batch_create(int n, vv_ctx* const* ctxs, const vv_state* states, vv_batch** out) {
     if (n < 1 || !ctxs || !states || !out) return VV_ERR_ARG;
+    const bool dbg = getenv("VV_DEBUG") != nullptr;
+#define BTRACE(...)                         \
+    do {                                    \
+        if (dbg) {                          \
+            fprintf(stderr, "[vv_batch] " __VA_ARGS__); \
+            fflush(stderr);                 \
+        }                                   \
+    } while (0)
+    BTRACE("create n=%d\n", n);
     *out = nullptr;
     for (int i = 0; i < n; ++i) {
         const vv_state& s = states[i];
@@ -1287,6 +1435,7 @@ int vv_batch_create(int n, vv_ctx* const* ctxs, const vv_state* states, vv_batch
         if (cudaStreamCreateWithFlags(&b->br[i], cudaStreamNonBlocking) != cudaSuccess) return fail(VV_ERR_CUDA);
     for (int i = 0; i <= n; ++i)
         if (cudaEventCreateWithFlags(&b->ev[i], cudaEventDisableTiming) != cudaSuccess) return fail(VV_ERR_CUDA);
+    BTRACE("streams/events ok\n");
     if (cudaGraphCreate(&b->g, 0) != cudaSuccess) return fail(VV_ERR_CUDA);
     if (cudaStreamBeginCaptureToGraph(b->origin, b->g, nullptr, nullptr, 0, cudaStreamCaptureModeRelaxed) !=
         cudaSuccess)
@@ -1294,11 +1443,14 @@ int vv_batch_create(int n, vv_ctx* const* ctxs, const vv_state* states, vv_batch
     cudaEventRecord(b->ev[n], b->origin);   // fork point
     for (int i = 0; i < n && r == VV_OK; ++i) {
         vv_ctx* c = b->ctx[i];
-        cudaStreamWaitEvent(b->br[i], b->ev[n], 0);
+        BTRACE("capture instance %d (nx=%d nv=%d)\n", i, c->nx, c->nv);
+        cudaError_t we = cudaStreamWaitEvent(b->br[i], b->ev[n], 0);
+        BTRACE("  wait event -> %s\n", cudaGetErrorString(we));
         const cudaStream_t saved = c->st;
         c->st = b->br[i];
         r = capture_step(c, &b->st[i], b->g);
         c->st = saved;
+        BTRACE("  capture_step -> %d (%s)\n", r, g_err);
         if (r == VV_OK) {
             cudaEventRecord(b->ev[i], b->br[i]);
             std::array<unsigned long long, 5> h;
@@ -1309,10 +1461,13 @@ int vv_batch_create(int n, vv_ctx* const* ctxs, const vv_state* states, vv_batch
     if (r == VV_OK)
         for (int i = 0; i < n; ++i) cudaStreamWaitEvent(b->origin, b->ev[i], 0);   // join
     cudaGraph_t outg = nullptr;
+    BTRACE("end capture\n");
     cudaError_t e = cudaStreamEndCapture(b->origin, &outg);
+    BTRACE("  -> %s\n", cudaGetErrorString(e));
     if (r != VV_OK) return fail(r);
     if (e != cudaSuccess) return fail(fail_cuda(e, "batch capture"));
     e = cudaGraphInstantiate(&b->ex, b->g, 0);
+    BTRACE("instantiate -> %s\n", cudaGetErrorString(e));
     if (e != cudaSuccess) return fail(fail_cuda(e, "batch instantiate"));
     for (int i = 0; i < n; ++i) b->ctx[i]->use_graph = true;
     *out = b;

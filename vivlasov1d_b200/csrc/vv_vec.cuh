@@ -363,12 +363,12 @@ k_gm_finish(DevState* s, const T* __restrict__ V, size_t ldv, T* __restrict__ x,
 // ----- Picard-loop kernels -------------------------------------------------
 // f -= delta unless the linear solve failed (SNES ksponly skips the update
 // when the KSP reason is negative); record the solve in the report.
-template <typename T>
-__global__ void k_pic_apply(DevState* s, const T* __restrict__ delta, T* __restrict__ f, size_t n) {
+template <typename TF, typename TD>
+__global__ void k_pic_apply(DevState* s, const TF* __restrict__ delta, TD* __restrict__ f, size_t n) {
     const bool ok = s->reason >= 0;
     if (ok) {
         for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
-            f[i] = f[i] - delta[i];
+            f[i] = f[i] - (TD)delta[i];
     }
     if (blockIdx.x == 0 && threadIdx.x == 0) {
         const int k = s->pic_i;

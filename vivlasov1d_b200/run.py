@@ -30,7 +30,7 @@ from .solver import Grid, Toolbox, STENCIL
 class Run:
     """State and driver of one run (run_base.py:35-566 + the runscript)."""
 
-    def __init__(self, cfg, f0=None, device=None, order="factored", restart=30, normalise=True):
+    def __init__(self, cfg, f0=None, device=None, order="factored", restart=30, normalise=True, precision="fp64"):
         if not isinstance(cfg, Config):
             cfg = Config(cfg) if isinstance(cfg, str) else Config(overrides=cfg)
         self.cfg = cfg
@@ -48,7 +48,8 @@ class Run:
         self.mass = idata["mass"]
         self.ctx = self.grid.context(bracket=cfg.get_poisson_bracket(),
                                      preconditioner=cfg.get_preconditioner() or None,
-                                     charge=self.charge, mass=self.mass, order=order, restart=restart)
+                                     charge=self.charge, mass=self.mass, order=order, restart=restart,
+                                     precision=precision)
         g = self.grid
         fld, xv = g.field, g.xvec
         self.fc, self.fh = fld(), fld()
@@ -171,8 +172,9 @@ def main(argv=None):
     ap.add_argument("-c", "--config", required=True)
     ap.add_argument("--steps", type=int, default=None)
     ap.add_argument("--invariants", action="store_true")
+    ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
     args = ap.parse_args(argv)
-    run = Run(args.config)
+    run = Run(args.config, precision=args.precision)
     t0 = time.time()
 
     def log(r):

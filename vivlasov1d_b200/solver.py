@@ -80,8 +80,8 @@ class Grid:
         return torch.zeros(self.nx, dtype=torch.float64, device=self.device)
 
     def context(self, bracket="arakawaj4", preconditioner="tensor_kinetic", charge=-1.0, mass=1.0,
-                order="factored", restart=30):
-        key = (bracket, preconditioner, float(charge), float(mass), order, int(restart))
+                order="factored", restart=30, precision="fp64"):
+        key = (bracket, preconditioner, float(charge), float(mass), order, int(restart), precision)
         ctx = self._contexts.get(key)
         if ctx is None:
             ctx = Context(self, *key)
@@ -94,7 +94,7 @@ class Context:
     """Owner of one ``vv_ctx`` (device work buffers, preconditioner factors)."""
 
     def __init__(self, grid, bracket="arakawaj4", preconditioner="tensor_kinetic", charge=-1.0,
-                 mass=1.0, order="factored", restart=30):
+                 mass=1.0, order="factored", restart=30, precision="fp64"):
         lib = _lib.load()
         if not torch.cuda.is_available():
             raise RuntimeError("vivlasov1d_b200 needs a CUDA device; no CPU fallback exists")
@@ -116,6 +116,10 @@ class Context:
         g.laplace = _lib.LAPLACE["cfd4"]
         g.order = _lib.ORDER_REFERENCE if order == "reference" else _lib.ORDER_FACTORED
         g.gmres_restart = int(restart)
+        if precision not in _lib.PRECISION:
+            raise ValueError("precision must be one of %s" % list(_lib.PRECISION))
+        g.precision = _lib.PRECISION[precision]
+        self.precision = precision
         self.charge, self.mass = float(charge), float(mass)
         self.bracket, self.preconditioner_type, self.order = bracket, preconditioner, order
         self.has_pc = g.preconditioner == _lib.PC_TENSOR_KINETIC
