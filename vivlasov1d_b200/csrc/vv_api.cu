@@ -44,6 +44,10 @@ struct vv_ctx {
     float2 *spec32, *tw32, *lambda32, *dinv32;
     size_t smem_rfft32, smem_irfft32, smem_tri32;
     bool tri_stage32;
+    // kernel variants (picked by the autotuner at vv_create)
+    int fft_kind;      // 0: shared-memory radix-2 per warp, 1: four-step register/shuffle FFT
+    int tri_kind;      // 0: one CTA per mode (block scan), 1: one warp per mode
+    int narrow_bracket;  // 1: 32x16 tiles instead of 64x32
     // pinned host staging
     double* hpin;
     int* hstat;
@@ -188,7 +192,7 @@ int drain_timing(vv_ctx* c) {
 bool aligned16(const void* p) { return p == nullptr || ((uintptr_t)p & 15u) == 0; }
 
 bool wide_ok(const vv_ctx* c, const void* X, const void* Xh, const void* Y) {
-    return c->nx % vv::WX == 0 && aligned16(X) && aligned16(Xh) && aligned16(Y);
+    return !c->narrow_bracket && c->nx % vv::WX == 0 && aligned16(X) && aligned16(Xh) && aligned16(Y);
 }
 
 // X may be a GMRES basis base pointer with xidx -> the vector index in the state
@@ -262,6 +266,97 @@ int read_scalar(vv_ctx* c, const double* dsrc, double* out) {
 // P^-1 with input type TI, arithmetic R (double: FP64 tables and spectrum,
 // float: the mixed mode's FP32 copies) and output type TO.  Y may be a GMRES
 // basis base pointer with yidx -> the vector index (+yoff).
+// shared memory of the FFT kernels for a variant (bytes)
+size_t fft_smem(int kind, int M, int R, size_t csz, bool inverse) {
+    if (kind == 1) {
+        const int E = M / 32;
+        return (size_t)(M + R * (M + 1) + R * 32 * (E + 1)) * csz;
+    }
+    return inverse ? (size_t)(M + 2 * R * (M + 1)) * csz : (size_t)(M + R * (M + 1)) * csz;
+}
+
+bool four_step_ok(int M) { return M >= 32 && M <= 512; }
+
+template <typename TI, typename R>
+int launch_rfft(vv_ctx* c, const TI* X, typename Cplx<R>::type* spec, const vv::PcParams& p, unsigned rows) {
+    const size_t csz = sizeof(typename Cplx<R>::type);
+    const int M = c->M;
+    if (c->fft_kind == 1 && four_step_ok(M)) {
+        const size_t sm = fft_smem(1, M, c->pcR, csz, false);
+        switch (M / 32) {
+            case 1: vv::k_rfft4<TI, R, 1><<<rows, 32 * c->pcR, sm, c->st>>>(X, spec, p); break;
+            case 2: vv::k_rfft4<TI, R, 2><<<rows, 32 * c->pcR, sm, c->st>>>(X, spec, p); break;
+            case 4: vv::k_rfft4<TI, R, 4><<<rows, 32 * c->pcR, sm, c->st>>>(X, spec, p); break;
+            case 8: vv::k_rfft4<TI, R, 8><<<rows, 32 * c->pcR, sm, c->st>>>(X, spec, p); break;
+            default: vv::k_rfft4<TI, R, 16><<<rows, 32 * c->pcR, sm, c->st>>>(X, spec, p); break;
+        }
+    } else {
+        vv::k_rfft_rows<TI, R><<<rows, 32 * c->pcR, fft_smem(0, M, c->pcR, csz, false), c->st>>>(X, spec, p);
+    }
+    CKL(c);
+    return VV_OK;
+}
+
+template <typename R, typename TO>
+int launch_irfft(vv_ctx* c, const typename Cplx<R>::type* spec, TO* Y, const vv::PcParams& p, unsigned rows) {
+    const size_t csz = sizeof(typename Cplx<R>::type);
+    const int M = c->M;
+    if (c->fft_kind == 1 && four_step_ok(M)) {
+        const size_t sm = fft_smem(1, M, c->pcR, csz, true);
+        switch (M / 32) {
+            case 1: vv::k_irfft4<R, TO, 1><<<rows, 32 * c->pcR, sm, c->st>>>(spec, Y, p); break;
+            case 2: vv::k_irfft4<R, TO, 2><<<rows, 32 * c->pcR, sm, c->st>>>(spec, Y, p); break;
+            case 4: vv::k_irfft4<R, TO, 4><<<rows, 32 * c->pcR, sm, c->st>>>(spec, Y, p); break;
+            case 8: vv::k_irfft4<R, TO, 8><<<rows, 32 * c->pcR, sm, c->st>>>(spec, Y, p); break;
+            default: vv::k_irfft4<R, TO, 16><<<rows, 32 * c->pcR, sm, c->st>>>(spec, Y, p); break;
+        }
+    } else {
+        vv::k_irfft_rows<R, TO><<<rows, 32 * c->pcR, fft_smem(0, M, c->pcR, csz, true), c->st>>>(spec, Y, p);
+    }
+    CKL(c);
+    return VV_OK;
+}
+
+// Raise the dynamic shared memory limit of every FFT variant of one precision.
+template <typename R>
+int fft_attributes(vv_ctx* c) {
+    const size_t csz = sizeof(typename Cplx<R>::type);
+    const int M = c->M;
+    const int big = 200 * 1024;
+    auto set = [&](const void* f, size_t bytes) {
+        return cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)std::min<size_t>(bytes, big));
+    };
+    size_t s0 = 0, s1 = 0;
+    for (int rr = 1; rr <= 8; rr *= 2) {
+        s0 = std::max(s0, fft_smem(0, M, rr, csz, true));
+        if (four_step_ok(M)) s1 = std::max(s1, fft_smem(1, M, rr, csz, true));
+    }
+    cudaError_t e = cudaSuccess;
+    auto acc = [&](cudaError_t x) { if (e == cudaSuccess) e = x; };
+    acc(set((const void*)vv::k_rfft_rows<double, R>, s0));
+    acc(set((const void*)vv::k_irfft_rows<R, R>, s0));
+    if (std::is_same<R, double>::value == false) acc(set((const void*)vv::k_rfft_rows<float, R>, s0));
+    if (four_step_ok(M)) {
+#define VV_SET4(E)                                                            \
+    acc(set((const void*)vv::k_rfft4<double, R, E>, s1));                     \
+    acc(set((const void*)vv::k_irfft4<R, R, E>, s1));                          \
+    if (!std::is_same<R, double>::value) acc(set((const void*)vv::k_rfft4<float, R, E>, s1));
+        switch (M / 32) {
+            case 1: VV_SET4(1) break;
+            case 2: VV_SET4(2) break;
+            case 4: VV_SET4(4) break;
+            case 8: VV_SET4(8) break;
+            default: VV_SET4(16) break;
+        }
+#undef VV_SET4
+    }
+    if (e != cudaSuccess) return fail_cuda(e, "fft attributes");
+    return VV_OK;
+}
+
+// P^-1 with input type TI, arithmetic R (double: FP64 tables and spectrum,
+// float: the mixed mode's FP32 copies) and output type TO.  Y may be a GMRES
+// basis base pointer with yidx -> the vector index (+yoff).
 template <typename TI, typename R, typename TO>
 int pc_apply_t(vv_ctx* c, const TI* X, TO* Y, const int* yidx = nullptr, int yoff = 0) {
     constexpr bool D = std::is_same<R, double>::value;
@@ -269,13 +364,10 @@ int pc_apply_t(vv_ctx* c, const TI* X, TO* Y, const int* yidx = nullptr, int yof
     vv::PcParams p = pcparams(c);
     C2* spec = D ? reinterpret_cast<C2*>(c->spec) : reinterpret_cast<C2*>(c->spec32);
     p.tw = D ? (const void*)c->tw : (const void*)c->tw32;
-    const size_t sm_f = D ? c->smem_rfft : c->smem_rfft32;
-    const size_t sm_i = D ? c->smem_irfft : c->smem_irfft32;
     const size_t sm_t = D ? c->smem_tri : c->smem_tri32;
     const bool stage = D ? c->tri_stage : c->tri_stage32;
     const unsigned rows = (unsigned)((c->nv + c->pcR - 1) / c->pcR);
-    vv::k_rfft_rows<TI, R><<<rows, 32 * c->pcR, sm_f, c->st>>>(X, spec, p);
-    CKL(c);
+    TRY(launch_rfft<TI, R>(c, X, spec, p, rows));
     vv::TriParams t;
     t.nv = c->nv;
     t.nmodes = c->nmodes;
@@ -283,7 +375,10 @@ int pc_apply_t(vv_ctx* c, const TI* X, TO* Y, const int* yidx = nullptr, int yof
     t.alpha = D ? (const void*)c->alpha : (const void*)c->alpha32;
     t.gamma = D ? (const void*)c->gamma : (const void*)c->gamma32;
     t.dinv = D ? (const void*)c->dinv : (const void*)c->dinv32;
-    if (stage)
+    if (c->tri_kind == 1)
+        vv::k_tridiag_warp<R><<<(c->nmodes + vv::TRIW_WARPS - 1) / vv::TRIW_WARPS, 32 * vv::TRIW_WARPS, 0, c->st>>>(
+            spec, t);
+    else if (stage)
         vv::k_tridiag_modes<R, true><<<c->nmodes, vv::TRI_THREADS, sm_t, c->st>>>(spec, t);
     else
         vv::k_tridiag_modes<R, false><<<c->nmodes, vv::TRI_THREADS, sm_t, c->st>>>(spec, t);
@@ -291,9 +386,7 @@ int pc_apply_t(vv_ctx* c, const TI* X, TO* Y, const int* yidx = nullptr, int yof
     p.yidx = yidx;
     p.yoff = yoff;
     p.ystride = yidx ? c->ncell : 0;
-    vv::k_irfft_rows<R, TO><<<rows, 32 * c->pcR, sm_i, c->st>>>(spec, Y, p);
-    CKL(c);
-    return VV_OK;
+    return launch_irfft<R, TO>(c, spec, Y, p, rows);
 }
 
 int pc_apply(vv_ctx* c, const double* X, double* Y, const int* yidx = nullptr, int yoff = 0) {
@@ -712,6 +805,103 @@ int step_revert(vv_ctx* c, vv_state* st) {
 
 bool same_state(const vv_state& a, const vv_state& b) { return std::memcmp(&a, &b, sizeof a) == 0; }
 
+// ---- autotuner ---------------------------------------------------------------
+// Times the candidate kernel variants of one grid shape on the context's own
+// scratch buffers (CUDA events, a few launches each) and keeps the fastest:
+// FFT kind x rows per CTA x tridiagonal kind for the preconditioner in the
+// GMRES precision, and the bracket tile shape.  Results are cached per
+// (nx, nv, precision) for the life of the process.
+struct TuneResult {
+    int fft_kind, pcR, tri_kind, narrow;
+};
+
+std::vector<std::pair<std::array<int, 3>, TuneResult>>& tune_cache() {
+    static std::vector<std::pair<std::array<int, 3>, TuneResult>> cache;
+    return cache;
+}
+
+template <typename F>
+int time_it(vv_ctx* c, F fn, int reps, float* ms) {
+    cudaEvent_t e0, e1;
+    CK(cudaEventCreate(&e0));
+    CK(cudaEventCreate(&e1));
+    int r = VV_OK;
+    for (int k = 0; k < 2 && r == VV_OK; ++k) r = fn();
+    cudaEventRecord(e0, c->st);
+    for (int k = 0; k < reps && r == VV_OK; ++k) r = fn();
+    cudaEventRecord(e1, c->st);
+    cudaError_t e = cudaEventSynchronize(e1);
+    if (e == cudaSuccess) e = cudaEventElapsedTime(ms, e0, e1);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (r != VV_OK) return r;
+    if (e != cudaSuccess) return fail_cuda(e, "autotune timing");
+    return VV_OK;
+}
+
+int autotune(vv_ctx* c) {
+    const std::array<int, 3> key = {c->nx, c->nv, c->mixed ? 1 : 0};
+    for (auto& kv : tune_cache())
+        if (kv.first == key) {
+            c->fft_kind = kv.second.fft_kind;
+            c->pcR = kv.second.pcR;
+            c->tri_kind = kv.second.tri_kind;
+            c->narrow_bracket = kv.second.narrow;
+            return VV_OK;
+        }
+    const size_t n = c->ncell;
+    CK(cudaMemsetAsync(c->tmp, 0, n * sizeof(double), c->st));
+    if (c->mixed) CK(cudaMemsetAsync(c->tmp32, 0, n * sizeof(float), c->st));
+    TuneResult best{c->fft_kind, c->pcR, c->tri_kind, 0};
+    float best_ms = 1e30f;
+    const size_t csz = c->mixed ? sizeof(float2) : sizeof(double2);
+    for (int kind = 0; kind <= 1; ++kind) {
+        if (kind == 1 && !four_step_ok(c->M)) continue;
+        for (int R = 1; R <= 8; R *= 2) {
+            if (fft_smem(kind, c->M, R, csz, true) > 200 * 1024) continue;
+            for (int tk = 0; tk <= 1; ++tk) {
+                c->fft_kind = kind;
+                c->pcR = R;
+                c->tri_kind = tk;
+                float ms = 0.f;
+                int r = c->mixed ? time_it(c, [&]() { return pc_apply_t<float, float, float>(c, c->tmp32, c->bvec32); },
+                                           5, &ms)
+                                 : time_it(c, [&]() { return pc_apply(c, c->tmp, c->bvec); }, 5, &ms);
+                TRY(r);
+                if (ms < best_ms) {
+                    best_ms = ms;
+                    best = {kind, R, tk, 0};
+                }
+            }
+        }
+    }
+    c->fft_kind = best.fft_kind;
+    c->pcR = best.pcR;
+    c->tri_kind = best.tri_kind;
+    if (c->nx % vv::WX == 0) {
+        float t_wide = 0.f, t_narrow = 0.f;
+        for (int nb = 0; nb <= 1; ++nb) {
+            c->narrow_bracket = nb;
+            float ms = 0.f;
+            int r = c->mixed ? time_it(c, [&]() {
+                                   return launch_bracket<vv::MODE_JVP, float>(c, c->tmp32, nullptr, c->bvec32, 0.5,
+                                                                              nullptr);
+                               }, 10, &ms)
+                             : time_it(c, [&]() {
+                                   return launch_bracket<vv::MODE_JVP, double>(c, c->tmp, nullptr, c->bvec, 0.5,
+                                                                               nullptr);
+                               }, 10, &ms);
+            TRY(r);
+            (nb ? t_narrow : t_wide) = ms;
+        }
+        best.narrow = t_narrow < t_wide ? 1 : 0;
+    }
+    c->narrow_bracket = best.narrow;
+    c->launches = 0;
+    tune_cache().push_back({key, best});
+    return VV_OK;
+}
+
 void destroy_graph(vv_ctx* c) {
     if (c->step_exec) cudaGraphExecDestroy(c->step_exec);
     if (c->step_graph) cudaGraphDestroy(c->step_graph);
@@ -1044,13 +1234,7 @@ int vv_create(const vv_grid* grid, vv_ctx** out) {
             vv_destroy(c);
             return fail_cuda(cudaGetLastError(), "vv_create upload (fp32)");
         }
-        if (cudaFuncSetAttribute(vv::k_rfft_rows<double, float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 (int)c->smem_rfft32) != cudaSuccess ||
-            cudaFuncSetAttribute(vv::k_rfft_rows<float, float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 (int)c->smem_rfft32) != cudaSuccess ||
-            cudaFuncSetAttribute(vv::k_irfft_rows<float, float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 (int)c->smem_irfft32) != cudaSuccess ||
-            cudaFuncSetAttribute(vv::k_tridiag_modes<float, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+        if (cudaFuncSetAttribute(vv::k_tridiag_modes<float, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  (int)c->smem_tri32) != cudaSuccess ||
             cudaFuncSetAttribute(vv::k_tridiag_modes<float, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  (int)c->smem_tri32) != cudaSuccess) {
@@ -1059,11 +1243,11 @@ int vv_create(const vv_grid* grid, vv_ctx** out) {
         }
     }
     // dynamic shared memory limits
-    if (cudaFuncSetAttribute(vv::k_rfft_rows<double, double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             (int)c->smem_rfft) != cudaSuccess ||
-        cudaFuncSetAttribute(vv::k_irfft_rows<double, double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             (int)c->smem_irfft) != cudaSuccess ||
-        cudaFuncSetAttribute(vv::k_tridiag_modes<double, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    if ((s = fft_attributes<double>(c)) != VV_OK || (c->mixed && (s = fft_attributes<float>(c)) != VV_OK)) {
+        vv_destroy(c);
+        return s;
+    }
+    if (cudaFuncSetAttribute(vv::k_tridiag_modes<double, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              (int)c->smem_tri) != cudaSuccess ||
         cudaFuncSetAttribute(vv::k_tridiag_modes<double, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              (int)c->smem_tri) != cudaSuccess ||
@@ -1071,6 +1255,18 @@ int vv_create(const vv_grid* grid, vv_ctx** out) {
                              (int)c->smem_pois) != cudaSuccess) {
         vv_destroy(c);
         return fail_cuda(cudaGetLastError(), "cudaFuncSetAttribute");
+    }
+    c->fft_kind = four_step_ok(c->M) ? 1 : 0;
+    c->tri_kind = c->nmodes >= 64 ? 1 : 0;
+    c->narrow_bracket = 0;
+    {
+        const char* e = getenv("VV_AUTOTUNE");
+        if (!(e && e[0] == '0')) {
+            if ((s = autotune(c)) != VV_OK) {
+                vv_destroy(c);
+                return s;
+            }
+        }
     }
     *out = c;
     return VV_OK;

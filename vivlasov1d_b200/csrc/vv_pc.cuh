@@ -198,6 +198,189 @@ __global__ void k_irfft_rows(const typename Cplx<R>::type* __restrict__ spec, TO
 }
 
 // ---------------------------------------------------------------------------
+// Four-step FFT by one warp, M = 32 E (E = 1..32): lane l holds z[l + 32 m2];
+// an E-point DFT in registers, the twiddle W_M^{l k2}, then a 32-point DIF
+// across lanes with xor shuffles.  Lane l ends with X[k2 + E bitrev5(l)].
+// No shared memory and no barrier inside the transform.
+// ---------------------------------------------------------------------------
+__host__ __device__ constexpr int crev(int j, int bits) {
+    return bits == 0 ? 0 : (((j & 1) << (bits - 1)) | crev(j >> 1, bits - 1));
+}
+__host__ __device__ constexpr int clog2(int n) { return n <= 1 ? 0 : 1 + clog2(n >> 1); }
+
+template <int E, int SIGN, typename C>
+__device__ __forceinline__ void reg_fft(C (&a)[E], const C* stw) {
+    constexpr int B = clog2(E);
+    C t[E];
+#pragma unroll
+    for (int j = 0; j < E; ++j) t[crev(j, B)] = a[j];
+#pragma unroll
+    for (int h = 1; h < E; h <<= 1) {
+#pragma unroll
+        for (int g = 0; g < E; g += 2 * h) {
+#pragma unroll
+            for (int pos = 0; pos < h; ++pos) {
+                C w = stw[32 * pos * (E / (2 * h))];     // W_E^{pos E/(2h)} = W_M^{32 pos E/(2h)}
+                if (SIGN > 0) w.y = -w.y;
+                const C u = t[g + pos];
+                const C v = c_mul(w, t[g + pos + h]);
+                t[g + pos] = c_add(u, v);
+                t[g + pos + h] = c_sub(u, v);
+            }
+        }
+    }
+#pragma unroll
+    for (int j = 0; j < E; ++j) a[j] = t[j];
+}
+
+template <int E, int SIGN, typename C>
+__device__ __forceinline__ void warp_fft4(C (&a)[E], const C* stw) {
+    const int lane = threadIdx.x & 31;
+    reg_fft<E, SIGN>(a, stw);
+#pragma unroll
+    for (int k2 = 1; k2 < E; ++k2) {                 // W_M^{lane k2}
+        C w = stw[lane * k2];
+        if (SIGN > 0) w.y = -w.y;
+        a[k2] = c_mul(a[k2], w);
+    }
+    if (SIGN < 0) {
+        // lane 0's twiddles are 1; nothing to do
+    }
+#pragma unroll
+    for (int span = 16; span >= 1; span >>= 1) {
+        const bool upper = (lane & span) != 0;
+        const int i = lane & (span - 1);
+        C w = stw[(i * (16 / span)) * E];              // W_32^{i 16/span}
+        if (SIGN > 0) w.y = -w.y;
+#pragma unroll
+        for (int k2 = 0; k2 < E; ++k2) {
+            const C mine = a[k2];
+            C other;
+            other.x = __shfl_xor_sync(0xffffffffu, mine.x, span);
+            other.y = __shfl_xor_sync(0xffffffffu, mine.y, span);
+            a[k2] = upper ? c_mul(c_sub(other, mine), w) : c_add(mine, other);
+        }
+    }
+}
+
+// index in a warp's padded buffer of the value lane l holds as a[k2]
+template <int E>
+__device__ __forceinline__ int zslot(int lane, int k2) { return lane * (E + 1) + k2; }
+// ... and of transform output k (k = k2 + E k1 lives in lane bitrev5(k1))
+template <int E>
+__device__ __forceinline__ int zslot_of(int k) {
+    return (int)(__brev((unsigned)(k / E)) >> 27) * (E + 1) + (k % E);
+}
+
+// Real FFT along x (nx = 2M = 64 E) of RW rows per CTA, one warp per row,
+// half spectrum written transposed: spec[k*nv + j].
+// dynamic smem: [M twiddles][RW x (M+1) half spectra][RW x 32(E+1) transform slots]
+template <typename TI, typename R, int E>
+__global__ void k_rfft4(const TI* __restrict__ X, typename Cplx<R>::type* __restrict__ spec, PcParams p) {
+    using C = typename Cplx<R>::type;
+    constexpr int M = 32 * E, LD = M + 1, ZS = 32 * (E + 1);
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    C* stw = reinterpret_cast<C*>(smem_raw);
+    C* rows = stw + M;
+    C* zb = rows + p.R * LD;
+    const C* tw = reinterpret_cast<const C*>(p.tw);
+    for (int k = threadIdx.x; k < M; k += blockDim.x) stw[k] = tw[k];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int j0 = blockIdx.x * p.R;
+    const int j = j0 + warp;
+    __syncthreads();
+    if (warp < p.R && j < p.nv) {
+        const TI* row = X + (size_t)j * p.nx;
+        C a[E];
+#pragma unroll
+        for (int m2 = 0; m2 < E; ++m2) {
+            const int m = lane + 32 * m2;
+            a[m2] = c_make<C>((double)row[2 * m], (double)row[2 * m + 1]);
+        }
+        warp_fft4<E, -1>(a, stw);
+        C* z = zb + warp * ZS;
+#pragma unroll
+        for (int k2 = 0; k2 < E; ++k2) z[zslot<E>(lane, k2)] = a[k2];
+        __syncwarp();
+        C* out = rows + warp * LD;
+        for (int k = lane; k <= M / 2; k += 32) {
+            const int kc = M - k;
+            const C zk = z[zslot_of<E>(k == M ? 0 : k)];
+            const C zc = z[zslot_of<E>(k == 0 ? 0 : kc)];
+            const C zcc = c_conj(zc);
+            C E1 = c_scale(c_add(zk, zcc), (R)0.5);
+            C D = c_sub(zk, zcc);
+            const C outk = c_add(E1, c_mul(stw[k], c_make<C>(0.5 * D.y, -0.5 * D.x)));
+            const C zkc = c_conj(zk);
+            E1 = c_scale(c_add(zc, zkc), (R)0.5);
+            D = c_sub(zc, zkc);
+            const C w = (kc < M) ? stw[kc] : c_make<C>(-1.0, 0.0);
+            const C outc = c_add(E1, c_mul(w, c_make<C>(0.5 * D.y, -0.5 * D.x)));
+            out[k] = outk;
+            if (kc != k) out[kc] = outc;
+        }
+    }
+    __syncthreads();
+    const int nrow = min(p.R, p.nv - j0);
+    for (int idx = threadIdx.x; idx < (M + 1) * p.R; idx += blockDim.x) {
+        const int k = idx / p.R, r = idx - k * p.R;
+        if (r < nrow) spec[(size_t)k * p.nv + j0 + r] = rows[r * LD + k];
+    }
+}
+
+// spec[k*nv + j] -> RW rows of Y (one warp per row), normalised by 1/nx
+// dynamic smem: [M twiddles][RW x (M+1) half spectra][RW x 32(E+1) transform slots]
+template <typename R, typename TO, int E>
+__global__ void k_irfft4(const typename Cplx<R>::type* __restrict__ spec, TO* __restrict__ Y, PcParams p) {
+    using C = typename Cplx<R>::type;
+    constexpr int M = 32 * E, LD = M + 1, ZS = 32 * (E + 1);
+    if (p.yidx) Y += (size_t)(*p.yidx + p.yoff) * p.ystride;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    C* stw = reinterpret_cast<C*>(smem_raw);
+    C* rows = stw + M;
+    C* zb = rows + p.R * LD;
+    const C* tw = reinterpret_cast<const C*>(p.tw);
+    for (int k = threadIdx.x; k < M; k += blockDim.x) stw[k] = tw[k];
+    const int j0 = blockIdx.x * p.R;
+    const int nrow = min(p.R, p.nv - j0);
+    for (int idx = threadIdx.x; idx < (M + 1) * p.R; idx += blockDim.x) {
+        const int k = idx / p.R, r = idx - k * p.R;
+        C v = c_make<C>(0.0, 0.0);
+        if (r < nrow) v = spec[(size_t)k * p.nv + j0 + r];
+        if (k == 0 || k == M) v.y = 0;   // c2r ignores these imaginary parts
+        rows[r * LD + k] = v;
+    }
+    __syncthreads();
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    if (warp >= nrow) return;
+    const C* xr = rows + warp * LD;
+    C a[E];
+#pragma unroll
+    for (int m2 = 0; m2 < E; ++m2) {
+        const int k = lane + 32 * m2;
+        const C xk = xr[k];
+        const C xc = c_conj(xr[M - k]);
+        const C E1 = c_scale(c_add(xk, xc), (R)0.5);
+        C w = stw[k];
+        w.y = -w.y;
+        const C O = c_mul(w, c_scale(c_sub(xk, xc), (R)0.5));
+        a[m2] = c_make<C>(E1.x - O.y, E1.y + O.x);      // Z_k = E + i O
+    }
+    warp_fft4<E, +1>(a, stw);
+    C* z = zb + warp * ZS;
+#pragma unroll
+    for (int k2 = 0; k2 < E; ++k2) z[zslot<E>(lane, k2)] = a[k2];
+    __syncwarp();
+    const R s = (R)(1.0 / (double)M);
+    TO* row = Y + (size_t)(j0 + warp) * p.nx;
+    for (int m = lane; m < M; m += 32) {
+        const C v = z[zslot_of<E>(m)];
+        row[2 * m] = (TO)(v.x * s);
+        row[2 * m + 1] = (TO)(v.y * s);
+    }
+}
+
+// ---------------------------------------------------------------------------
 // tridiagonal solves, one CTA per x mode
 // ---------------------------------------------------------------------------
 struct TriParams {
@@ -348,6 +531,94 @@ k_tridiag_modes(typename Cplx<R>::type* __restrict__ spec, TriParams p) {
             const C cc = c_rmul(lam, GA(r, q));
             x = c_mul(d, c_sub(b[q], c_mul(cc, x)));
         }
+        line[r] = x;
+    }
+}
+
+
+// Warp-scan of affine maps (no shared memory): returns the image of 0 under
+// the composition of the maps of all earlier lanes in `forward` order.
+template <typename C>
+__device__ __forceinline__ C warp_scan_aff(Aff<C> a, bool forward) {
+    const int lane = threadIdx.x & 31;
+    const int pos = forward ? lane : 31 - lane;
+    Aff<C> inc = a;
+#pragma unroll
+    for (int d = 1; d < 32; d <<= 1) {
+        const Aff<C> o = shfl_aff(inc, d, forward);
+        if (pos >= d) inc = aff_combine(o, inc);
+    }
+    const Aff<C> prev = shfl_aff(inc, 1, forward);
+    return pos > 0 ? prev.Q : c_make<C>(0.0, 0.0);
+}
+
+// One warp per x mode (8 modes per CTA): lane l owns rows
+// [l*CH, (l+1)*CH) of the mode's v line; the LU reciprocals and the
+// alpha/gamma tables are read through L1 in the lane's own contiguous chunk.
+// No shared memory, no block barrier.
+constexpr int TRIW_WARPS = 8;
+
+template <typename R>
+__global__ void __launch_bounds__(32 * TRIW_WARPS)
+k_tridiag_warp(typename Cplx<R>::type* __restrict__ spec, TriParams p) {
+    using C = typename Cplx<R>::type;
+    const int k = blockIdx.x * TRIW_WARPS + (threadIdx.x >> 5);
+    if (k >= p.nmodes) return;
+    const int lane = threadIdx.x & 31;
+    const int nv = p.nv;
+    const int CH = (nv + 31) / 32;
+    const int r0 = lane * CH;
+    const int r1 = min(r0 + CH, nv);
+    C* line = spec + (size_t)k * nv;
+    const C* di = reinterpret_cast<const C*>(p.dinv) + (size_t)k * nv;
+    const R* al = reinterpret_cast<const R*>(p.alpha);
+    const R* ga = reinterpret_cast<const R*>(p.gamma);
+    const C lam = reinterpret_cast<const C*>(p.lambda)[k];
+    // forward: y_r = b_r - l_r y_{r-1},  l_r = lambda alpha_r / U_{r-1}
+    Aff<C> a;
+    a.P = c_make<C>(1.0, 0.0);
+    a.Q = c_make<C>(0.0, 0.0);
+    for (int r = r0; r < r1; ++r) {
+        Aff<C> m;
+        if (r == 0) m.P = c_make<C>(0.0, 0.0);
+        else {
+            const C l = c_mul(c_rmul(lam, al[r]), di[r - 1]);
+            m.P = c_make<C>(-l.x, -l.y);
+        }
+        m.Q = line[r];
+        a = aff_combine(a, m);
+    }
+    C y = warp_scan_aff<C>(a, true);
+    for (int r = r0; r < r1; ++r) {
+        const C b = line[r];
+        if (r == 0) y = b;
+        else {
+            const C l = c_mul(c_rmul(lam, al[r]), di[r - 1]);
+            y = c_sub(b, c_mul(l, y));
+        }
+        line[r] = y;
+    }
+    __syncwarp();
+    // backward: x_r = U_r^-1 (y_r - c_r x_{r+1})  ==  mu_r + nu_r x_{r+1}
+    a.P = c_make<C>(1.0, 0.0);
+    a.Q = c_make<C>(0.0, 0.0);
+    for (int r = r1 - 1; r >= r0; --r) {
+        Aff<C> m;
+        const C d = di[r];
+        m.Q = c_mul(d, line[r]);
+        if (r == nv - 1) m.P = c_make<C>(0.0, 0.0);
+        else {
+            const C nu = c_mul(d, c_rmul(lam, ga[r]));
+            m.P = c_make<C>(-nu.x, -nu.y);
+        }
+        a = aff_combine(a, m);
+    }
+    C x = warp_scan_aff<C>(a, false);
+    for (int r = r1 - 1; r >= r0; --r) {
+        const C d = di[r];
+        const C yv = line[r];
+        if (r == nv - 1) x = c_mul(d, yv);
+        else x = c_mul(d, c_sub(yv, c_mul(c_rmul(lam, ga[r]), x)));
         line[r] = x;
     }
 }
