@@ -21,6 +21,7 @@
 #include <cstddef>
 #include <cstdio>
 #include <cstring>
+#include <mutex>
 #include <type_traits>
 #include <vector>
 
@@ -90,6 +91,12 @@ thread_local char g_err[256];
 int fail_cuda(cudaError_t e, const char* what) {
     snprintf(g_err, sizeof g_err, "%s: %s", what, cudaGetErrorString(e));
     return VV_ERR_CUDA;
+}
+
+template <typename... A>
+int fail(int status, const char* fmt, A... args) {
+    snprintf(g_err, sizeof g_err, fmt, args...);
+    return status;
 }
 
 #define CK(call)                                             \
@@ -263,9 +270,6 @@ int read_scalar(vv_ctx* c, const double* dsrc, double* out) {
 }
 
 // ---- preconditioner ---------------------------------------------------------
-// P^-1 with input type TI, arithmetic R (double: FP64 tables and spectrum,
-// float: the mixed mode's FP32 copies) and output type TO.  Y may be a GMRES
-// basis base pointer with yidx -> the vector index (+yoff).
 // shared memory of the FFT kernels for a variant (bytes)
 size_t fft_smem(int kind, int M, int R, size_t csz, bool inverse) {
     if (kind == 1) {
@@ -317,40 +321,57 @@ int launch_irfft(vv_ctx* c, const typename Cplx<R>::type* spec, TO* Y, const vv:
     return VV_OK;
 }
 
-// Raise the dynamic shared memory limit of every FFT variant of one precision.
+// Dynamic shared memory limits are attributes of a kernel FUNCTION, shared
+// by every context of the process on a device: a per-context value would let
+// a later, smaller context lower the limit an earlier, larger one launches
+// with.  They are raised once per device to the opt-in maximum less each
+// kernel's static shared memory instead; each context then only checks that
+// its own sizes fit under the smallest of those limits.
+void smem_set(const void* f, int optin, int& lowest, cudaError_t& e) {
+    cudaFuncAttributes fa;
+    cudaError_t x = cudaFuncGetAttributes(&fa, f);
+    const int limit = optin - (int)fa.sharedSizeBytes;
+    if (x == cudaSuccess) x = cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, limit);
+    if (e == cudaSuccess) e = x;
+    lowest = std::min(lowest, limit);
+}
+
 template <typename R>
-int fft_attributes(vv_ctx* c) {
-    const size_t csz = sizeof(typename Cplx<R>::type);
-    const int M = c->M;
-    const int big = 200 * 1024;
-    auto set = [&](const void* f, size_t bytes) {
-        return cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)std::min<size_t>(bytes, big));
-    };
-    size_t s0 = 0, s1 = 0;
-    for (int rr = 1; rr <= 8; rr *= 2) {
-        s0 = std::max(s0, fft_smem(0, M, rr, csz, true));
-        if (four_step_ok(M)) s1 = std::max(s1, fft_smem(1, M, rr, csz, true));
-    }
-    cudaError_t e = cudaSuccess;
-    auto acc = [&](cudaError_t x) { if (e == cudaSuccess) e = x; };
-    acc(set((const void*)vv::k_rfft_rows<double, R>, s0));
-    acc(set((const void*)vv::k_irfft_rows<R, R>, s0));
-    if (std::is_same<R, double>::value == false) acc(set((const void*)vv::k_rfft_rows<float, R>, s0));
-    if (four_step_ok(M)) {
-#define VV_SET4(E)                                                            \
-    acc(set((const void*)vv::k_rfft4<double, R, E>, s1));                     \
-    acc(set((const void*)vv::k_irfft4<R, R, E>, s1));                          \
-    if (!std::is_same<R, double>::value) acc(set((const void*)vv::k_rfft4<float, R, E>, s1));
-        switch (M / 32) {
-            case 1: VV_SET4(1) break;
-            case 2: VV_SET4(2) break;
-            case 4: VV_SET4(4) break;
-            case 8: VV_SET4(8) break;
-            default: VV_SET4(16) break;
-        }
+void smem_attributes(int optin, int& lowest, cudaError_t& e) {
+    auto set = [&](const void* f) { smem_set(f, optin, lowest, e); };
+    set((const void*)vv::k_rfft_rows<double, R>);
+    set((const void*)vv::k_rfft_rows<float, R>);
+    set((const void*)vv::k_irfft_rows<R, R>);
+#define VV_SET4(E)                                   \
+    set((const void*)vv::k_rfft4<double, R, E>);     \
+    set((const void*)vv::k_rfft4<float, R, E>);      \
+    set((const void*)vv::k_irfft4<R, R, E>);
+    VV_SET4(1) VV_SET4(2) VV_SET4(4) VV_SET4(8) VV_SET4(16)
 #undef VV_SET4
+    set((const void*)vv::k_tridiag_modes<R, true>);
+    set((const void*)vv::k_tridiag_modes<R, false>);
+}
+
+int raise_smem_limits(int* limit_out) {
+    static std::mutex mu;
+    static int limit_of[64] = {};
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return fail_cuda(e, "cudaGetDevice");
+    if (dev < 0 || dev >= 64) return fail(VV_ERR_ARG, "device ordinal %d out of range", dev);
+    std::lock_guard<std::mutex> lock(mu);
+    if (limit_of[dev] == 0) {
+        int optin = 0;
+        if ((e = cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev)) != cudaSuccess)
+            return fail_cuda(e, "cudaDeviceGetAttribute (shared memory opt-in)");
+        int lowest = optin;
+        smem_attributes<double>(optin, lowest, e);
+        smem_attributes<float>(optin, lowest, e);
+        smem_set((const void*)vv::k_moments_poisson, optin, lowest, e);
+        if (e != cudaSuccess) return fail_cuda(e, "cudaFuncSetAttribute (dynamic shared memory)");
+        limit_of[dev] = lowest;
     }
-    if (e != cudaSuccess) return fail_cuda(e, "fft attributes");
+    *limit_out = limit_of[dev];
     return VV_OK;
 }
 
@@ -854,7 +875,9 @@ int autotune(vv_ctx* c) {
     if (c->mixed) CK(cudaMemsetAsync(c->tmp32, 0, n * sizeof(float), c->st));
     TuneResult best{c->fft_kind, c->pcR, c->tri_kind, 0};
     float best_ms = 1e30f;
-    const size_t csz = c->mixed ? sizeof(float2) : sizeof(double2);
+    // FP64 complex size also in the mixed mode: the FP64 entry points
+    // (vv_pc_apply) share the tuned rows-per-CTA
+    const size_t csz = sizeof(double2);
     for (int kind = 0; kind <= 1; ++kind) {
         if (kind == 1 && !four_step_ok(c->M)) continue;
         for (int R = 1; R <= 8; R *= 2) {
@@ -1234,27 +1257,21 @@ int vv_create(const vv_grid* grid, vv_ctx** out) {
             vv_destroy(c);
             return fail_cuda(cudaGetLastError(), "vv_create upload (fp32)");
         }
-        if (cudaFuncSetAttribute(vv::k_tridiag_modes<float, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 (int)c->smem_tri32) != cudaSuccess ||
-            cudaFuncSetAttribute(vv::k_tridiag_modes<float, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 (int)c->smem_tri32) != cudaSuccess) {
+    }
+    // dynamic shared memory limits (process-wide, raised once per device)
+    {
+        int limit = 0;
+        if ((s = raise_smem_limits(&limit)) != VV_OK) {
             vv_destroy(c);
-            return fail_cuda(cudaGetLastError(), "cudaFuncSetAttribute (fp32)");
+            return s;
         }
-    }
-    // dynamic shared memory limits
-    if ((s = fft_attributes<double>(c)) != VV_OK || (c->mixed && (s = fft_attributes<float>(c)) != VV_OK)) {
-        vv_destroy(c);
-        return s;
-    }
-    if (cudaFuncSetAttribute(vv::k_tridiag_modes<double, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             (int)c->smem_tri) != cudaSuccess ||
-        cudaFuncSetAttribute(vv::k_tridiag_modes<double, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             (int)c->smem_tri) != cudaSuccess ||
-        cudaFuncSetAttribute(vv::k_moments_poisson, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             (int)c->smem_pois) != cudaSuccess) {
-        vv_destroy(c);
-        return fail_cuda(cudaGetLastError(), "cudaFuncSetAttribute");
+        const size_t need = std::max({c->smem_tri, c->mixed ? c->smem_tri32 : (size_t)0, c->smem_pois,
+                                      fft_smem(0, M, c->pcR, sizeof(double2), true)});
+        if (need > (size_t)limit) {
+            vv_destroy(c);
+            return fail(VV_ERR_ARG, "grid %d x %d needs %zu bytes of shared memory per block (limit %d)", nx, nv,
+                        need, limit);
+        }
     }
     c->fft_kind = four_step_ok(c->M) ? 1 : 0;
     c->tri_kind = c->nmodes >= 64 ? 1 : 0;
@@ -1588,11 +1605,24 @@ extern "C" {
 
 int vv_batch_destroy(vv_batch* b) {
     if (!b) return VV_OK;
+    // a failed capture can leave a branch stream capturing: end that first,
+    // and release the streams before the graph they were capturing into
+    auto end_open_capture = [](cudaStream_t s) {
+        cudaStreamCaptureStatus st = cudaStreamCaptureStatusNone;
+        if (s && cudaStreamIsCapturing(s, &st) == cudaSuccess && st != cudaStreamCaptureStatusNone) {
+            cudaGraph_t junk = nullptr;
+            cudaStreamEndCapture(s, &junk);
+            if (junk) cudaGraphDestroy(junk);
+        }
+    };
+    for (auto s : b->br) end_open_capture(s);
+    end_open_capture(b->origin);
+    cudaGetLastError();
+    for (auto s : b->br) if (s) cudaStreamDestroy(s);
+    if (b->origin) cudaStreamDestroy(b->origin);
+    for (auto e : b->ev) if (e) cudaEventDestroy(e);
     if (b->ex) cudaGraphExecDestroy(b->ex);
     if (b->g) cudaGraphDestroy(b->g);
-    for (auto s : b->br) if (s) cudaStreamDestroy(s);
-    for (auto e : b->ev) if (e) cudaEventDestroy(e);
-    if (b->origin) cudaStreamDestroy(b->origin);
     if (b->hbuf) cudaFreeHost(b->hbuf);
     delete b;
     return VV_OK;
@@ -1648,14 +1678,18 @@ int vv_batch_create(int n, vv_ctx* const* ctxs, const vv_state* states, vv_batch
         c->st = saved;
         BTRACE("  capture_step -> %d (%s)\n", r, g_err);
         if (r == VV_OK) {
-            cudaEventRecord(b->ev[i], b->br[i]);
             std::array<unsigned long long, 5> h;
             std::memcpy(h.data(), c->hnd, sizeof c->hnd);
             b->hnd.push_back(h);
         }
     }
-    if (r == VV_OK)
-        for (int i = 0; i < n; ++i) cudaStreamWaitEvent(b->origin, b->ev[i], 0);   // join
+    // join every forked branch, also after a failure (an unjoined branch
+    // would stay in the capture)
+    for (int i = 0; i < n; ++i) {
+        cudaStreamCaptureStatus cst = cudaStreamCaptureStatusNone;
+        if (cudaStreamIsCapturing(b->br[i], &cst) != cudaSuccess || cst != cudaStreamCaptureStatusActive) continue;
+        if (cudaEventRecord(b->ev[i], b->br[i]) == cudaSuccess) cudaStreamWaitEvent(b->origin, b->ev[i], 0);
+    }
     cudaGraph_t outg = nullptr;
     BTRACE("end capture\n");
     cudaError_t e = cudaStreamEndCapture(b->origin, &outg);

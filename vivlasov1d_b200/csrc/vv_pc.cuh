@@ -208,6 +208,17 @@ __host__ __device__ constexpr int crev(int j, int bits) {
 }
 __host__ __device__ constexpr int clog2(int n) { return n <= 1 ? 0 : 1 + clog2(n >> 1); }
 
+// W_M^q (SIGN < 0) or its conjugate from the staged table stw[k] = W_N^k,
+// k < M, N = 2M: W_M^q = W_N^{2q}, and W_N^{k+M} = -W_N^k.
+template <int M, int SIGN, typename C>
+__device__ __forceinline__ C tw_half(const C* stw, int q) {
+    const int idx = 2 * q;
+    C w = idx < M ? stw[idx] : stw[idx - M];
+    if (idx >= M) { w.x = -w.x; w.y = -w.y; }
+    if (SIGN > 0) w.y = -w.y;
+    return w;
+}
+
 template <int E, int SIGN, typename C>
 __device__ __forceinline__ void reg_fft(C (&a)[E], const C* stw) {
     constexpr int B = clog2(E);
@@ -220,8 +231,7 @@ __device__ __forceinline__ void reg_fft(C (&a)[E], const C* stw) {
         for (int g = 0; g < E; g += 2 * h) {
 #pragma unroll
             for (int pos = 0; pos < h; ++pos) {
-                C w = stw[32 * pos * (E / (2 * h))];     // W_E^{pos E/(2h)} = W_M^{32 pos E/(2h)}
-                if (SIGN > 0) w.y = -w.y;
+                const C w = tw_half<32 * E, SIGN>(stw, 32 * pos * (E / (2 * h)));  // W_E^{pos E/(2h)}
                 const C u = t[g + pos];
                 const C v = c_mul(w, t[g + pos + h]);
                 t[g + pos] = c_add(u, v);
@@ -239,19 +249,13 @@ __device__ __forceinline__ void warp_fft4(C (&a)[E], const C* stw) {
     reg_fft<E, SIGN>(a, stw);
 #pragma unroll
     for (int k2 = 1; k2 < E; ++k2) {                 // W_M^{lane k2}
-        C w = stw[lane * k2];
-        if (SIGN > 0) w.y = -w.y;
-        a[k2] = c_mul(a[k2], w);
-    }
-    if (SIGN < 0) {
-        // lane 0's twiddles are 1; nothing to do
+        a[k2] = c_mul(a[k2], tw_half<32 * E, SIGN>(stw, lane * k2));
     }
 #pragma unroll
     for (int span = 16; span >= 1; span >>= 1) {
         const bool upper = (lane & span) != 0;
         const int i = lane & (span - 1);
-        C w = stw[(i * (16 / span)) * E];              // W_32^{i 16/span}
-        if (SIGN > 0) w.y = -w.y;
+        const C w = tw_half<32 * E, SIGN>(stw, (i * (16 / span)) * E);  // W_32^{i 16/span}
 #pragma unroll
         for (int k2 = 0; k2 < E; ++k2) {
             const C mine = a[k2];
