@@ -260,6 +260,37 @@ int vv_launch_count(vv_ctx* ctx, int64_t* launches, int reset);
  * three kernels).  *avg_ms = time per launch (per apply for which == 2). */
 int vv_time_kernel(vv_ctx* ctx, int which, int reps, double* avg_ms);
 
+/* ---- invariants without a context or an allocation ----------------------
+ * No counterpart in the reference: there the invariants are computed on the
+ * host (distribution_function.pyx:130-306, hamiltonian.pyx:67-124,
+ * potential.pyx:48-59).  Same results as vv_invariants (same sums, same
+ * compensated FP64 order) for fields already on the device, but without a
+ * vv_ctx: vv_create allocates the whole solver (GMRES basis, spectra,
+ * preconditioner factors, scratch) and tunes it, which a diagnostics caller
+ * cannot always afford -- a hook between the steps of a running solve, where
+ * cudaMalloc/cudaFree would synchronise the device; a process whose device
+ * memory a caching allocator already holds; analysis code with fields but no
+ * solver.  This call performs no device allocation: its scratch is one fixed
+ * array in the library's device memory (about 198 KiB per device).
+ *   grid:   nx, nv, L, vmin, vmax, charge and mass are read (ht and the
+ *           solver fields are not); f: nx*nv doubles, phi: nx doubles,
+ *           h2: nx doubles or NULL; all device pointers.
+ *   stream: the CUDA stream of the kernels (NULL: the legacy default
+ *           stream); the call returns after synchronising it.
+ * Limits and rules:
+ *   nx > VV_NOALLOC_MAX_NX returns VV_ERR_UNSUPPORTED before any device
+ *   work (the array holds the x profile of phi).
+ *   The array is shared by all callers on a device: calls whose kernels can
+ *   overlap in time (two host threads, or two unordered streams) race on it
+ *   and must be serialised by the caller.
+ *   The first call on each device does a one-time set-up (it looks up the
+ *   array's device address, which may load the library's device code); make
+ *   that first call before any stream capture begins on that device.
+ *   Nothing in the array has to start at zero. */
+#define VV_NOALLOC_MAX_NX 16384
+int vv_invariants_noalloc(const vv_grid* grid, const double* f, const double* phi,
+                          const double* h2, void* cuda_stream, vv_invariant_set* out);
+
 #ifdef __cplusplus
 }
 #endif

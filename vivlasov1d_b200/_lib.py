@@ -13,7 +13,10 @@ LIB_PATH = os.path.join(HERE, "libvv.so")
 
 # ---- constants (vv.h) ----
 VV_OK = 0
+VV_ERR_ARG = 1
+VV_ERR_UNSUPPORTED = 2
 VV_ERR_DIVERGED = 5
+NOALLOC_MAX_NX = 16384      # VV_NOALLOC_MAX_NX: largest nx of vv_invariants_noalloc
 BRACKET = {"arakawaj1": 1, "arakawaj2": 2, "arakawaj4": 4}
 PC_NONE, PC_TENSOR_KINETIC = 0, 1
 LAPLACE = {"cfd4": 4}
@@ -99,6 +102,7 @@ SIGNATURES = {
     "vv_step": (I, [P, C.POINTER(vv_state), C.POINTER(vv_snes_opts), C.POINTER(vv_ksp_opts),
                     C.POINTER(vv_step_report)]),
     "vv_invariants": (I, [P, P, P, P, C.POINTER(vv_invariant_set)]),
+    "vv_invariants_noalloc": (I, [C.POINTER(vv_grid), P, P, P, P, C.POINTER(vv_invariant_set)]),
     "vv_timing_enable": (I, [P, I]),
     "vv_timing_read": (I, [P, C.POINTER(C.c_int64), C.POINTER(D), I]),
     "vv_launch_count": (I, [P, C.POINTER(C.c_int64), I]),

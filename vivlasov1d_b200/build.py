@@ -17,7 +17,7 @@ CSRC = os.path.join(HERE, "csrc")
 INCLUDE = os.path.join(ROOT, "include")
 LIB = os.path.join(HERE, "libvv.so")
 
-SOURCES = ["vv_api.cu"]
+SOURCES = ["vv_api.cu", "vv_noalloc.cu"]
 HEADERS = ["vv_common.cuh", "vv_bracket.cuh", "vv_pc.cuh", "vv_vec.cuh"]
 
 NVCC_FLAGS = [
