@@ -216,14 +216,22 @@ int vv_calculate_residual(vv_ctx* ctx, vv_state* st, double* residual);
 int vv_step(vv_ctx* ctx, vv_state* st, const vv_snes_opts* snes,
             const vv_ksp_opts* ksp, vv_step_report* report);
 
-/* ---- batched sweep: many independent runs in one graph launch ---------- */
+/* ---- batched sweep: many independent runs in lockstep -------------------- */
 /* The reference runs one instance per process; a parameter sweep is many
  * processes.  A batch advances `n` independent runs (each its own context
- * and state, grids of any size) by one time step with ONE CUDA graph launch:
- * the graph has one branch per instance, and every branch carries its own
- * device-side Picard and GMRES loops, so each instance stops on its own
- * convergence test while the others continue.  Contexts and states stay
- * owned by the caller and must outlive the batch. */
+ * and state, grids of different sizes) by one time step.  Every kernel of
+ * the step is launched once for the whole table (each block serves one
+ * instance), and the Picard and GMRES loops run in lockstep: each instance
+ * keeps its own convergence tests and iteration counts, and an instance that
+ * has converged is masked out of the later passes while the others
+ * continue.  The step is one CUDA graph (batch-level conditional loops)
+ * unless VV_GRAPH=0 at context creation, which drives the same kernels from
+ * the host.  All instances must share the precision, bracket scheme and the
+ * tensor_kinetic preconditioner, use the factored order and have nx a
+ * multiple of 64; otherwise vv_batch_create returns VV_ERR_UNSUPPORTED.
+ * Results equal each instance's own vv_step to rounding (the batch uses the
+ * radix-2 x-FFT and 64 x 32 stencil tiles for every instance).  Contexts and
+ * states stay owned by the caller and must outlive the batch. */
 typedef struct vv_batch vv_batch;
 int vv_batch_create(int n, vv_ctx* const* ctxs, const vv_state* states, vv_batch** out);
 int vv_batch_destroy(vv_batch* batch);
@@ -232,6 +240,8 @@ int vv_batch_set_stream(vv_batch* batch, void* cuda_stream);
  * first non-OK instance status, VV_OK if all instances stepped. */
 int vv_batch_step(vv_batch* batch, const vv_snes_opts* snes, const vv_ksp_opts* ksp,
                   vv_step_report* reports, int* statuses);
+/* Number of kernels the batch has launched (graph nodes executed included). */
+int vv_batch_launch_count(vv_batch* batch, int64_t* launches, int reset);
 
 /* ---- invariants (vlasov/core/distribution_function.pyx:130-306,
  *      hamiltonian.pyx:67-124, potential.pyx:48-59) ---------------------- */

@@ -364,24 +364,89 @@ def _small_run(nx, nv, f0fn, L, ht, vmax=10.0):
     return Run(cfg, f0=torch.from_numpy(vo.to_flat(f0)))
 
 
+def _assert_batch_matches(rb, rs, fb, fs, i, ftol):
+    """Lockstep batch vs the instance's own step: same Picard passes and stop
+    rule, GMRES counts within one (rounding near the relative tolerance),
+    f within `ftol` relative (max norm)."""
+    assert rb["picard_its"] == rs["picard_its"], (i, rb, rs)
+    assert rb["stop_rule"] == rs["stop_rule"], (i, rb, rs)
+    assert rb["ksp_failures"] == rs["ksp_failures"] == 0, (i, rb, rs)
+    assert all(abs(a - b) <= 1 for a, b in zip(rb["gmres_its"], rs["gmres_its"])), (i, rb, rs)
+    d = (fb - fs).abs().max().item() / fs.abs().max().item()
+    assert d <= ftol, (i, d)
+
+
+BATCH_SPECS = [(64, 128, vo.f0_landau(0.1, 0.5), 4 * np.pi, 0.1),
+               (128, 256, vo.f0_twostream(0.05, 0.5), 4 * np.pi, 0.1),
+               (64, 512, vo.f0_bump_on_tail(0.04, 0.3), 2 * np.pi / 0.3, 0.1)]
+
+
 def test_batch_step_equals_single_steps():
-    """A batch of uneven instances (one graph launch per step) gives the
-    same bits and reports as stepping each instance alone."""
+    """A lockstep batch of uneven instances (every kernel launched once for
+    the table, per-instance masks) follows each instance's own time step:
+    same Picard passes, GMRES counts within one, f to 1e-10."""
     from vivlasov1d_b200.batch import Batch
-    specs = [(64, 128, vo.f0_landau(0.1, 0.5), 4 * np.pi, 0.1),
-             (128, 256, vo.f0_twostream(0.05, 0.5), 4 * np.pi, 0.1),
-             (64, 512, vo.f0_bump_on_tail(0.04, 0.3), 2 * np.pi / 0.3, 0.1)]
-    batch_runs = [_small_run(*s) for s in specs]
-    single_runs = [_small_run(*s) for s in specs]
+    batch_runs = [_small_run(*s) for s in BATCH_SPECS]
+    single_runs = [_small_run(*s) for s in BATCH_SPECS]
     batch = Batch(batch_runs)
     for _ in range(3):
         rb = batch.step()
         for i, r in enumerate(single_runs):
             rs = r.step()
-            rbi = dict(rb[i])
-            rbi.pop("status")
-            assert rbi == rs, i
-            assert torch.equal(batch_runs[i].fc, r.fc), i
+            assert rb[i]["status"] == 0
+            _assert_batch_matches(rb[i], rs, batch_runs[i].fc, r.fc, i, 1e-10)
+    assert batch.launch_count() > 0
+
+
+def test_batch_graph_equals_host_driven(monkeypatch):
+    """The batch graph (conditional loops folded over the instance masks)
+    and the host-driven loop over the same kernels give identical bits."""
+    from vivlasov1d_b200.batch import Batch
+    graph_runs = [_small_run(*s) for s in BATCH_SPECS]
+    monkeypatch.setenv("VV_GRAPH", "0")
+    host_runs = [_small_run(*s) for s in BATCH_SPECS]
+    monkeypatch.delenv("VV_GRAPH")
+    bg, bh = Batch(graph_runs), Batch(host_runs)
+    for _ in range(2):
+        rg, rh = bg.step(), bh.step()
+        for i in range(len(BATCH_SPECS)):
+            assert rg[i] == rh[i], i
+            assert torch.equal(graph_runs[i].fc, host_runs[i].fc), i
+
+
+def test_batch_sweep_instances_match_single_steps():
+    """Twelve instances of the seeded sweep (Landau, two-stream and
+    bump-on-tail; nx 64..256, nv 128..1024) in one batch, FP64, against
+    each instance stepped alone."""
+    from vivlasov1d_b200 import workloads as W
+    from vivlasov1d_b200.batch import Batch
+    specs = W.sweep_specs(12)
+    br = W.sweep_runs(specs=specs)
+    sr = W.sweep_runs(specs=specs)
+    batch = Batch(br)
+    for _ in range(2):
+        rb = batch.step()
+        for i, r in enumerate(sr):
+            _assert_batch_matches(rb[i], r.step(), br[i].fc, r.fc, i, 1e-9)
+
+
+def test_batch_mixed_precision_field_energy():
+    """Batched mixed precision against FP64 single steps: field energy to
+    1e-9 relative after three steps for every instance."""
+    from vivlasov1d_b200 import workloads as W
+    from vivlasov1d_b200.batch import Batch
+    specs = W.sweep_specs(8)
+    mixed = W.sweep_runs(specs=specs, precision="mixed")
+    plain = W.sweep_runs(specs=specs)
+    batch = Batch(mixed)
+    for _ in range(3):
+        rb = batch.step()
+        assert all(r["status"] == 0 and r["ksp_failures"] == 0 for r in rb)
+        for r in plain:
+            r.step()
+    fm, fp = W.field_energies(mixed), W.field_energies(plain)
+    rel = np.abs(fm - fp) / np.abs(fp)
+    assert rel.max() <= 1e-9, rel
 
 
 def test_mixed_precision_matches_fp64():

@@ -112,6 +112,7 @@ SIGNATURES = {
     "vv_batch_set_stream": (I, [P, P]),
     "vv_batch_step": (I, [P, C.POINTER(vv_snes_opts), C.POINTER(vv_ksp_opts), C.POINTER(vv_step_report),
                           C.POINTER(C.c_int)]),
+    "vv_batch_launch_count": (I, [P, C.POINTER(C.c_int64), I]),
 }
 
 

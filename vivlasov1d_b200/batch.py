@@ -1,12 +1,13 @@
-"""Batched sweep: many independent runs advanced by one CUDA graph launch.
+"""Batched sweep: many independent runs advanced in lockstep.
 
 The reference runs one instance per process (a parameter sweep is many
 ``run.py`` invocations).  ``Batch`` takes several ``Run`` objects -- any mix
 of grid sizes, initial conditions and parameters, each with its own libvv
 context -- and advances all of them by one implicit time step per
-``step()`` call with a single graph launch (``vv_batch_step``).  Each
-instance keeps its own device-side Picard and GMRES loops and stops on its
-own convergence tests.
+``step()`` call (``vv_batch_step``): one CUDA graph in which every kernel
+serves the whole instance table.  Each instance keeps its own Picard and
+GMRES state and convergence tests; converged instances are masked out of
+later passes while the others continue.
 """
 from __future__ import annotations
 
@@ -47,6 +48,12 @@ class Batch:
             except Exception:
                 pass
             self.h = None
+
+    def launch_count(self, reset=False):
+        """Kernels the batch has launched so far (graph nodes executed included)."""
+        n = C.c_int64()
+        _lib.check(self.lib.vv_batch_launch_count(self.h, C.byref(n), int(bool(reset))), "vv_batch_launch_count")
+        return n.value
 
     def step(self):
         """Advance every instance by one time step; returns per-instance reports."""

@@ -12,6 +12,7 @@
 #include "vv_bracket.cuh"
 #include "vv_pc.cuh"
 #include "vv_vec.cuh"
+#include "vv_batch.cuh"
 
 #include <algorithm>
 #include <array>
@@ -368,6 +369,14 @@ int raise_smem_limits(int* limit_out) {
         smem_attributes<double>(optin, lowest, e);
         smem_attributes<float>(optin, lowest, e);
         smem_set((const void*)vv::k_moments_poisson, optin, lowest, e);
+        smem_set((const void*)vv::k_b_moments_poisson, optin, lowest, e);
+        smem_set((const void*)vv::k_b_rfft<double, double>, optin, lowest, e);
+        smem_set((const void*)vv::k_b_rfft<double, float>, optin, lowest, e);
+        smem_set((const void*)vv::k_b_rfft<float, float>, optin, lowest, e);
+        smem_set((const void*)vv::k_b_irfft<double, double>, optin, lowest, e);
+        smem_set((const void*)vv::k_b_irfft<float, float>, optin, lowest, e);
+        smem_set((const void*)vv::k_b_tridiag<double>, optin, lowest, e);
+        smem_set((const void*)vv::k_b_tridiag<float>, optin, lowest, e);
         if (e != cudaSuccess) return fail_cuda(e, "cudaFuncSetAttribute (dynamic shared memory)");
         limit_of[dev] = lowest;
     }
@@ -490,35 +499,10 @@ int moments_poisson(vv_ctx* c, const double* F, double* n, double* u, double* e,
     return VV_OK;
 }
 
-// Poisson apply: mode 0 rhs, 1 matvec, 2 function; optional ||y||^2 -> sumsq
 __global__ void k_poisson_apply(const double* __restrict__ x, const double* __restrict__ n,
                                 double* __restrict__ y, int nx, double hx2_inv, double charge, int mode,
                                 double* __restrict__ sumsq) {
-    __shared__ double red[32];
-    __shared__ double nmean_s;
-    double t = 0.0;
-    if (mode != 1) {
-        for (int i = threadIdx.x; i < nx; i += blockDim.x) t += n[i];
-        t = block_sum(t, red);
-        if (threadIdx.x == 0) nmean_s = t / nx;
-        __syncthreads();
-    }
-    double r2 = 0.0;
-    for (int i = threadIdx.x; i < nx; i += blockDim.x) {
-        double r;
-        if (mode == 0) {
-            r = -(n[i] - nmean_s) * charge;
-        } else {
-            const int im2 = (i - 2 + 2 * nx) % nx, im1 = (i - 1 + nx) % nx;
-            const int ip1 = (i + 1) % nx, ip2 = (i + 2) % nx;
-            r = (5. * x[im2] - 32. * x[im1] + 54. * x[i] - 32. * x[ip1] + 5. * x[ip2]) * hx2_inv / 12.;
-            if (mode == 2) r = r + (n[i] - nmean_s) * charge;
-        }
-        if (y) y[i] = r;
-        r2 += r * r;
-    }
-    r2 = block_sum(r2, red);
-    if (threadIdx.x == 0 && sumsq) sumsq[0] = r2;
+    vv::poisson_apply_cta(x, n, y, nx, hx2_inv, charge, mode, sumsq);
 }
 
 int poisson_apply(vv_ctx* c, const double* x, const double* n, double* y, int mode, double* sumsq) {
@@ -677,9 +661,10 @@ int gmres_host(vv_ctx* c, const T* b, T* x, vv_ksp_result* res) {
 }
 
 // ---- graph capture helpers ----------------------------------------------------
-// Add a conditional node at the current position of the capture on `cs`;
-// its handle is created on the top-level graph `owner` (handles may serve
-// conditional nodes of child graphs) with a default applied at every launch.
+// Add a conditional node at the current position of the capture on `cs`.
+// *handle_out: a handle created earlier on `owner`, or 0 to create one on the
+// top-level graph `owner` (handles may serve conditional nodes of child
+// graphs) with a default applied at every launch.
 int add_conditional(cudaGraph_t owner, cudaStream_t cs, cudaGraphConditionalNodeType type, unsigned size,
                     unsigned defval, unsigned long long* handle_out, cudaGraph_t* bodies) {
     static const bool dbg = getenv("VV_DEBUG") != nullptr;
@@ -693,8 +678,8 @@ int add_conditional(cudaGraph_t owner, cudaStream_t cs, cudaGraphConditionalNode
     cudaGraph_t g = nullptr;
     CK(cudaStreamGetCaptureInfo(cs, &status, nullptr, &g, &deps, &nd));
     if (status != cudaStreamCaptureStatusActive) return VV_ERR_CUDA;
-    cudaGraphConditionalHandle h;
-    CK(cudaGraphConditionalHandleCreate(&h, owner, defval, cudaGraphCondAssignDefault));
+    cudaGraphConditionalHandle h = (cudaGraphConditionalHandle)*handle_out;   // an existing handle, or a new one
+    if (!h) CK(cudaGraphConditionalHandleCreate(&h, owner, defval, cudaGraphCondAssignDefault));
     cudaGraphNodeParams prm = {cudaGraphNodeTypeConditional};
     prm.conditional.handle = h;
     prm.conditional.type = type;
@@ -938,6 +923,7 @@ void destroy_graph(vv_ctx* c) {
 int capture_step(vv_ctx* c, vv_state* st, cudaGraph_t owner) {
     for (int k = 1; k < 4; ++k)
         if (!c->cs[k]) CK(cudaStreamCreateWithFlags(&c->cs[k], cudaStreamNonBlocking));
+    for (auto& h : c->hnd) h = 0;   // new handles on `owner`
     c->cap_owner = owner;
     const int64_t l0 = c->launches;
     TRY(step_prologue(c, st));
@@ -985,7 +971,8 @@ int build_step_graph(vv_ctx* c, vv_state* st) {
 }
 
 // Read the step report of context c from its pinned state copy.
-int fill_report(vv_ctx* c, const vv::DevState& d, int restart, vv_step_report* rep, double abort_residual) {
+int fill_report(vv_ctx* c, const vv::DevState& d, int restart, vv_step_report* rep, double abort_residual,
+                bool count_launches = true) {
     std::memset(rep, 0, sizeof(*rep));
     rep->picard_its = d.pic_i;
     rep->gmres_its_total = d.gmres_total;
@@ -999,7 +986,7 @@ int fill_report(vv_ctx* c, const vv::DevState& d, int restart, vv_step_report* r
     }
     for (int k = 0; k <= np; ++k) rep->residual[k] = d.residual[k];
     (void)restart;
-    if (c->use_graph) {
+    if (c->use_graph && count_launches) {
         // kernels the graph executed: top level once, the Picard body per pass,
         // the GMRES cycle body per cycle (+ restart branch), the Arnoldi body per iteration
         const int64_t top = c->nk_top - c->nk_pic - c->nk_revert;
@@ -1584,61 +1571,399 @@ int vv_launch_count(vv_ctx* c, int64_t* launches, int reset) {
 }
 
 
-// ---- batched sweep ---------------------------------------------------------
+// ---- batched sweep: lockstep over an instance table --------------------------
 }  // extern "C"
 
+// One graph (or host-driven loop) advances every instance of the batch by one
+// time step.  Each kernel launch covers all instances with a persistent grid
+// that walks the work list of the current mask; the Picard/GMRES loops run in
+// lockstep, and the batch loop conditions are the OR of the instance flags
+// (k_b_ctrl, which also rebuilds the work lists).
 struct vv_batch {
     int n;
     std::vector<vv_ctx*> ctx;
-    std::vector<vv_state> st;
-    cudaStream_t origin;
-    std::vector<cudaStream_t> br;
-    std::vector<cudaEvent_t> ev;
+    std::vector<vv_state> states;
+    bool mixed;
+    int scheme;
+    int R;                       // FFT rows per CTA
+    int tri_warp;                // tridiagonal solves: 1 one warp per mode, 0 one CTA per mode
+    double* wpart;               // device: per-warp partial sums of every instance
+    vv::BInst* tab;              // device instance table
+    int* lists;                  // device work lists (vv::NLIST of them)
+    size_t list_words;
+    int tot[vv::NFAM];           // work items per family over all instances
+    size_t smem_rfft, smem_irfft, smem_tri, smem_pois;
+    unsigned int* counts;        // device: passes per control op
+    int* flag;                   // device: last control result
+    int* hflag;                  // pinned
+    unsigned int* hcounts;       // pinned
+    unsigned int* gather;        // device: n state headers
+    unsigned int* hgather;       // pinned
+    int words;                   // 32-bit words of a state header
+    int nsm;                     // multiprocessors
+    cudaStream_t st;             // stream of the kernels (the capture stream during capture)
+    cudaStream_t user;
+    cudaStream_t cs[4];
     cudaGraph_t g;
     cudaGraphExec_t ex;
-    cudaStream_t user;
-    vv::DevState* hbuf;   // pinned, n states (header + report part)
-    std::vector<std::array<unsigned long long, 5>> hnd;   // each instance's handles in this graph
+    unsigned long long hnd[4];   // batch handles: pic, outer, inner, revert (index = BH_*)
+    bool use_graph;
+    int64_t launches;
+    int nk_prologue, nk_pic_head, nk_cycle_head, nk_arnoldi, nk_cycle_tail, nk_pic_tail, nk_revert_ctrl, nk_revert;
 };
+
+namespace {
+
+enum { BH_PIC = 0, BH_OUTER = 1, BH_INNER = 2, BH_REVERT = 3 };
+
+// Persistent launch of a batch kernel over family `fam`: as many blocks as fit
+// on the GPU at once (never more than the family's work items).
+template <typename... KA, typename... A>
+int blaunch(vv_batch* b, void (*k)(KA...), int fam, dim3 threads, size_t smem, A... args) {
+    int per_sm = 0;
+    cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, (int)(threads.x * threads.y * threads.z),
+                                                                  smem);
+    if (e != cudaSuccess) return fail_cuda(e, "batch occupancy");
+    const long cap = (long)std::max(1, per_sm) * b->nsm;
+    const unsigned grid = (unsigned)std::max<long>(1, std::min<long>(cap, b->tot[fam]));
+    k<<<grid, threads, smem, b->st>>>(args...);
+    b->launches++;
+    e = cudaGetLastError();
+    return e == cudaSuccess ? VV_OK : fail_cuda(e, "batch kernel launch");
+}
+
+const int* blist(const vv_batch* b, int l) { return b->lists + (size_t)l * b->list_words; }
+
+int b_ctrl(vv_batch* b, int op, int h) {
+    vv::k_b_ctrl<<<1, vv::CTRL_THREADS, 0, b->st>>>(b->tab, b->n, op, (b->use_graph && h >= 0) ? b->hnd[h] : 0ull,
+                                                     b->flag, b->counts, b->lists);
+    b->launches++;
+    const cudaError_t e = cudaGetLastError();
+    return e == cudaSuccess ? VV_OK : fail_cuda(e, "batch control launch");
+}
+
+int b_flag(vv_batch* b, int* out) {
+    CK(cudaMemcpyAsync(b->hflag, b->flag, sizeof(int), cudaMemcpyDeviceToHost, b->st));
+    CK(cudaStreamSynchronize(b->st));
+    *out = *b->hflag;
+    return VV_OK;
+}
+
+// P^-1 of every instance in list l: input FP64 tmp (right-hand side) or the
+// GMRES-precision scratch; output b, V0 or V[it+1]
+template <typename T>
+int b_pc(vv_batch* b, int l, bool from_tmp64, int dst) {
+    const vv::BInst* tab = b->tab;
+    const int* L = blist(b, l);
+    const dim3 rt(32 * b->R);
+    if (from_tmp64) TRY(blaunch(b, vv::k_b_rfft<double, T>, vv::F_ROWS, rt, b->smem_rfft, tab, L, b->n, 1));
+    else TRY(blaunch(b, vv::k_b_rfft<T, T>, vv::F_ROWS, rt, b->smem_rfft, tab, L, b->n, 0));
+    if (b->tri_warp) TRY(blaunch(b, vv::k_b_tridiag_w<T>, vv::F_MODES, 32 * vv::TRIW_WARPS, 0, tab, L, b->n));
+    else TRY(blaunch(b, vv::k_b_tridiag<T>, vv::F_MODES, vv::TRI_THREADS, b->smem_tri, tab, L, b->n));
+    return blaunch(b, vv::k_b_irfft<T, T>, vv::F_ROWS, rt, b->smem_irfft, tab, L, b->n, dst);
+}
+
+template <int S, typename T>
+int b_residual(vv_batch* b, int l, int phase) {
+    const vv::BInst* tab = b->tab;
+    const int* L = blist(b, l);
+    TRY(blaunch(b, vv::k_b_poisson, vv::F_INST, 1024, 0, tab, L, b->n));
+    TRY(blaunch(b, vv::k_b_bracket<S, vv::BS_RESIDUAL, T>, vv::F_TILE, vv::WTHREADS, 0, tab, L, b->n));
+    TRY(blaunch(b, vv::k_b_pic_residual, vv::F_INST, 32, 0, tab, L, b->n, phase));
+    return b_ctrl(b, vv::BC_PIC, BH_PIC);
+}
+
+template <int S, typename T>
+int b_prologue(vv_batch* b) {
+    TRY(blaunch(b, vv::k_b_prologue, vv::F_VEC, vv::RED_THREADS, 0, (const vv::BInst*)b->tab, blist(b, vv::L_ALL), b->n));
+    return b_residual<S, T>(b, vv::L_ALL, 0);
+}
+
+template <int S, typename T>
+int b_pic_head(vv_batch* b) {
+    TRY(b_pc<T>(b, vv::L_PIC, true, vv::BD_B));
+    TRY(blaunch(b, vv::k_b_gm_init<T>, vv::F_VEC, vv::RED_THREADS, 0, (const vv::BInst*)b->tab, blist(b, vv::L_PIC), b->n));
+    return b_ctrl(b, vv::BC_GM_START, BH_OUTER);
+}
+
+template <int S, typename T>
+int b_cycle_head(vv_batch* b) {
+    const vv::BInst* tab = b->tab;
+    const int* G = blist(b, vv::L_GM);
+    TRY(blaunch(b, vv::k_b_bracket<S, vv::BS_X, T>, vv::F_TILE, vv::WTHREADS, 0, tab, blist(b, vv::L_GMR), b->n));
+    TRY(b_pc<T>(b, vv::L_GMR, false, vv::BD_V0));
+    TRY(blaunch(b, vv::k_b_gm_head<T>, vv::F_VEC, vv::RED_THREADS, 0, tab, G, b->n));
+    TRY(blaunch(b, vv::k_b_gm_cycle_p<T>, vv::F_VEC, vv::RED_THREADS, 0, tab, G, b->n));
+    TRY(blaunch(b, vv::k_b_gm_cycle_f, vv::F_INST, 32, 0, tab, G, b->n));
+    TRY(blaunch(b, vv::k_b_gm_scale<T>, vv::F_VEC, vv::RED_THREADS, 0, tab, G, b->n));
+    return b_ctrl(b, vv::BC_INNER, BH_INNER);
+}
+
+template <int S, typename T>
+int b_arnoldi(vv_batch* b) {
+    const vv::BInst* tab = b->tab;
+    const int* A = blist(b, vv::L_INNER);
+    TRY(blaunch(b, vv::k_b_bracket<S, vv::BS_VIT, T>, vv::F_TILE, vv::WTHREADS, 0, tab, A, b->n));
+    TRY(b_pc<T>(b, vv::L_INNER, false, vv::BD_VNEXT));
+    TRY(blaunch(b, vv::k_b_gm_mdot_p<T>, vv::F_VEC, vv::RED_THREADS, 0, tab, A, b->n));
+    TRY(blaunch(b, vv::k_b_gm_mdot_f, vv::F_INST, vv::RED_THREADS, 0, tab, A, b->n));
+    TRY(blaunch(b, vv::k_b_gm_maxpy_p<T>, vv::F_VEC, vv::RED_THREADS, 0, tab, A, b->n));
+    TRY(blaunch(b, vv::k_b_gm_maxpy_f, vv::F_INST, 32, 0, tab, A, b->n));
+    TRY(blaunch(b, vv::k_b_gm_scale<T>, vv::F_VEC, vv::RED_THREADS, 0, tab, A, b->n));
+    return b_ctrl(b, vv::BC_INNER, BH_INNER);
+}
+
+template <int S, typename T>
+int b_cycle_tail(vv_batch* b) {
+    const int* G = blist(b, vv::L_GM);
+    TRY(blaunch(b, vv::k_b_gm_solve, vv::F_INST, 32, 0, (const vv::BInst*)b->tab, G, b->n));
+    TRY(blaunch(b, vv::k_b_gm_update<T>, vv::F_VEC, vv::RED_THREADS, 0, (const vv::BInst*)b->tab, G, b->n));
+    return b_ctrl(b, vv::BC_GM_FINISH, BH_OUTER);
+}
+
+int b_moments(vv_batch* b, int l) {
+    const int* L = blist(b, l);
+    TRY(blaunch(b, vv::k_b_moments_partial, vv::F_MOM, dim3(vv::MOM_TX, vv::MOM_TY), 0, (const vv::BInst*)b->tab, L, b->n));
+    return blaunch(b, vv::k_b_moments_poisson, vv::F_INST, vv::POIS_THREADS, b->smem_pois, (const vv::BInst*)b->tab, L,
+                   b->n);
+}
+
+template <int S, typename T>
+int b_pic_tail(vv_batch* b) {
+    TRY(blaunch(b, vv::k_b_pic_apply<T>, vv::F_VEC, vv::RED_THREADS, 0, (const vv::BInst*)b->tab, blist(b, vv::L_PIC), b->n));
+    TRY(b_moments(b, vv::L_PIC));
+    return b_residual<S, T>(b, vv::L_PIC, 1);
+}
+
+int b_revert_ctrl(vv_batch* b) { return b_ctrl(b, vv::BC_REVERT, BH_REVERT); }
+
+int b_revert(vv_batch* b) {
+    TRY(blaunch(b, vv::k_b_revert, vv::F_VEC, vv::RED_THREADS, 0, (const vv::BInst*)b->tab, blist(b, vv::L_REVERT), b->n));
+    return b_moments(b, vv::L_REVERT);
+}
+
+// host-driven step (the same kernels; the host reads each loop flag)
+template <int S, typename T>
+int b_step_host(vv_batch* b) {
+    int f = 0;
+    TRY(b_prologue<S, T>(b));
+    TRY(b_flag(b, &f));
+    while (f) {
+        TRY(b_pic_head<S, T>(b));
+        int outer = 0;
+        TRY(b_flag(b, &outer));
+        while (outer) {
+            TRY(b_cycle_head<S, T>(b));
+            int inner = 0;
+            TRY(b_flag(b, &inner));
+            while (inner) {
+                TRY(b_arnoldi<S, T>(b));
+                TRY(b_flag(b, &inner));
+            }
+            TRY(b_cycle_tail<S, T>(b));
+            TRY(b_flag(b, &outer));
+        }
+        TRY(b_pic_tail<S, T>(b));
+        TRY(b_flag(b, &f));
+    }
+    TRY(b_revert_ctrl(b));
+    TRY(b_flag(b, &f));
+    if (f) TRY(b_revert(b));
+    return VV_OK;
+}
+
+// body capture on a batch capture stream
+template <typename F>
+int b_body(vv_batch* b, int level, cudaGraph_t body, F fn) {
+    const cudaStream_t saved = b->st;
+    CK(cudaStreamBeginCaptureToGraph(b->cs[level], body, nullptr, nullptr, 0, cudaStreamCaptureModeRelaxed));
+    b->st = b->cs[level];
+    const int r = fn();
+    b->st = saved;
+    cudaGraph_t out = nullptr;
+    const cudaError_t e = cudaStreamEndCapture(b->cs[level], &out);
+    if (r != VV_OK) return r;
+    if (e != cudaSuccess) return fail_cuda(e, "cudaStreamEndCapture (batch)");
+    return VV_OK;
+}
+
+template <int S, typename T>
+int b_capture(vv_batch* b) {
+    // the loop handles exist before the control kernels that set them are captured
+    for (auto& h : b->hnd) {
+        cudaGraphConditionalHandle ch;
+        CK(cudaGraphConditionalHandleCreate(&ch, b->g, 0, cudaGraphCondAssignDefault));
+        h = (unsigned long long)ch;
+    }
+    // kernels per sequence (for the launch count of graph steps)
+    const int64_t l0 = b->launches;
+    TRY(b_prologue<S, T>(b));
+    b->nk_prologue = (int)(b->launches - l0);
+    cudaGraph_t pic[1];
+    TRY(add_conditional(b->g, b->st, cudaGraphCondTypeWhile, 1, 0, &b->hnd[BH_PIC], pic));
+    TRY(b_body(b, 1, pic[0], [&]() -> int {
+        int64_t m = b->launches;
+        TRY(b_pic_head<S, T>(b));
+        b->nk_pic_head = (int)(b->launches - m);
+        cudaGraph_t outer[1];
+        TRY(add_conditional(b->g, b->st, cudaGraphCondTypeWhile, 1, 0, &b->hnd[BH_OUTER], outer));
+        TRY(b_body(b, 2, outer[0], [&]() -> int {
+            int64_t q = b->launches;
+            TRY(b_cycle_head<S, T>(b));
+            b->nk_cycle_head = (int)(b->launches - q);
+            cudaGraph_t inner[1];
+            TRY(add_conditional(b->g, b->st, cudaGraphCondTypeWhile, 1, 0, &b->hnd[BH_INNER], inner));
+            TRY(b_body(b, 3, inner[0], [&]() -> int {
+                const int64_t w = b->launches;
+                TRY(b_arnoldi<S, T>(b));
+                b->nk_arnoldi = (int)(b->launches - w);
+                return VV_OK;
+            }));
+            q = b->launches;
+            TRY(b_cycle_tail<S, T>(b));
+            b->nk_cycle_tail = (int)(b->launches - q);
+            return VV_OK;
+        }));
+        m = b->launches;
+        TRY(b_pic_tail<S, T>(b));
+        b->nk_pic_tail = (int)(b->launches - m);
+        return VV_OK;
+    }));
+    int64_t m = b->launches;
+    TRY(b_revert_ctrl(b));
+    b->nk_revert_ctrl = (int)(b->launches - m);
+    cudaGraph_t rev[1];
+    TRY(add_conditional(b->g, b->st, cudaGraphCondTypeIf, 1, 0, &b->hnd[BH_REVERT], rev));
+    TRY(b_body(b, 1, rev[0], [&]() -> int {
+        const int64_t w = b->launches;
+        TRY(b_revert(b));
+        b->nk_revert = (int)(b->launches - w);
+        return VV_OK;
+    }));
+    b->launches = l0;   // captured, not executed
+    return VV_OK;
+}
+
+template <typename T>
+int b_dispatch_capture(vv_batch* b) {
+    switch (b->scheme) {
+        case VV_BRACKET_J1: return b_capture<1, T>(b);
+        case VV_BRACKET_J2: return b_capture<2, T>(b);
+        default: return b_capture<4, T>(b);
+    }
+}
+
+template <typename T>
+int b_dispatch_host(vv_batch* b) {
+    switch (b->scheme) {
+        case VV_BRACKET_J1: return b_step_host<1, T>(b);
+        case VV_BRACKET_J2: return b_step_host<2, T>(b);
+        default: return b_step_host<4, T>(b);
+    }
+}
+
+// Launch shape of the preconditioner kernels: rows per CTA of the x-FFTs and
+// the tridiagonal variant (work items per instance and shared memory).
+void b_shape(vv_batch* b, std::vector<vv::BInst>& tab, int R, int tri_warp) {
+    b->R = R;
+    b->tri_warp = tri_warp;
+    const size_t csz = b->mixed ? sizeof(float2) : sizeof(double2);
+    for (int f = 0; f < vv::NFAM; ++f) b->tot[f] = 0;
+    b->smem_rfft = b->smem_irfft = 0;
+    for (int i = 0; i < b->n; ++i) {
+        vv::BInst& I = tab[i];
+        const vv_ctx* c = b->ctx[i];
+        I.pp.R = R;
+        I.cnt[vv::F_ROWS] = (c->nv + R - 1) / R;
+        I.cnt[vv::F_MODES] = tri_warp ? (c->nmodes + vv::TRIW_WARPS - 1) / vv::TRIW_WARPS : c->nmodes;
+        for (int f = 0; f < vv::NFAM; ++f) b->tot[f] += I.cnt[f];
+        b->smem_rfft = std::max(b->smem_rfft, fft_smem(0, c->M, R, csz, false));
+        b->smem_irfft = std::max(b->smem_irfft, fft_smem(0, c->M, R, csz, true));
+    }
+}
+
+// upload the table in its current shape and rebuild the list of all instances
+int b_apply_shape(vv_batch* b, const std::vector<vv::BInst>& tab) {
+    CK(cudaMemcpyAsync(b->tab, tab.data(), tab.size() * sizeof(vv::BInst), cudaMemcpyHostToDevice, b->st));
+    TRY(b_ctrl(b, vv::BC_ALL, -1));
+    CK(cudaStreamSynchronize(b->st));
+    return VV_OK;
+}
+
+// Batch autotuner: times the whole-table preconditioner (the step's largest
+// share) for FFT rows per CTA x tridiagonal variant and keeps the fastest.
+template <typename T>
+int b_autotune(vv_batch* b, std::vector<vv::BInst>& tab) {
+    for (int i = 0; i < b->n; ++i) {
+        const vv_ctx* c = b->ctx[i];
+        CK(cudaMemsetAsync(b->mixed ? (void*)c->tmp32 : (void*)c->tmp, 0, c->ncell * sizeof(T), b->st));
+    }
+    cudaEvent_t e0, e1;
+    CK(cudaEventCreate(&e0));
+    CK(cudaEventCreate(&e1));
+    float best = 1e30f;
+    int bR = b->R, bW = b->tri_warp, r = VV_OK;
+    for (int tw = 0; tw <= 1 && r == VV_OK; ++tw) {
+        for (int R = 2; R <= 8 && r == VV_OK; R *= 2) {
+            b_shape(b, tab, R, tw);
+            if ((r = b_apply_shape(b, tab)) != VV_OK) break;
+            for (int k = 0; k < 2 && r == VV_OK; ++k) r = b_pc<T>(b, vv::L_ALL, false, vv::BD_B);
+            cudaEventRecord(e0, b->st);
+            for (int k = 0; k < 5 && r == VV_OK; ++k) r = b_pc<T>(b, vv::L_ALL, false, vv::BD_B);
+            cudaEventRecord(e1, b->st);
+            float ms = 0.f;
+            if (r == VV_OK && cudaEventSynchronize(e1) == cudaSuccess && cudaEventElapsedTime(&ms, e0, e1) == cudaSuccess &&
+                ms < best) {
+                best = ms;
+                bR = R;
+                bW = tw;
+            }
+        }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    TRY(r);
+    b_shape(b, tab, bR, bW);
+    return b_apply_shape(b, tab);
+}
+
+template <typename X>
+int upload_vec(X** dst, const std::vector<X>& v) {
+    if (cudaMalloc((void**)dst, std::max<size_t>(1, v.size()) * sizeof(X)) != cudaSuccess) return VV_ERR_ALLOC;
+    if (!v.empty() && cudaMemcpy(*dst, v.data(), v.size() * sizeof(X), cudaMemcpyHostToDevice) != cudaSuccess)
+        return fail_cuda(cudaGetLastError(), "batch table upload");
+    return VV_OK;
+}
+
+}  // namespace
 
 extern "C" {
 
 int vv_batch_destroy(vv_batch* b) {
     if (!b) return VV_OK;
-    // a failed capture can leave a branch stream capturing: end that first,
-    // and release the streams before the graph they were capturing into
-    auto end_open_capture = [](cudaStream_t s) {
-        cudaStreamCaptureStatus st = cudaStreamCaptureStatusNone;
-        if (s && cudaStreamIsCapturing(s, &st) == cudaSuccess && st != cudaStreamCaptureStatusNone) {
+    for (auto s : b->cs) {
+        cudaStreamCaptureStatus cst = cudaStreamCaptureStatusNone;
+        if (s && cudaStreamIsCapturing(s, &cst) == cudaSuccess && cst != cudaStreamCaptureStatusNone) {
             cudaGraph_t junk = nullptr;
             cudaStreamEndCapture(s, &junk);
             if (junk) cudaGraphDestroy(junk);
         }
-    };
-    for (auto s : b->br) end_open_capture(s);
-    end_open_capture(b->origin);
+    }
     cudaGetLastError();
-    for (auto s : b->br) if (s) cudaStreamDestroy(s);
-    if (b->origin) cudaStreamDestroy(b->origin);
-    for (auto e : b->ev) if (e) cudaEventDestroy(e);
+    for (auto s : b->cs) if (s) cudaStreamDestroy(s);
     if (b->ex) cudaGraphExecDestroy(b->ex);
     if (b->g) cudaGraphDestroy(b->g);
-    if (b->hbuf) cudaFreeHost(b->hbuf);
+    for (void* p : {(void*)b->tab, (void*)b->lists, (void*)b->counts, (void*)b->flag, (void*)b->gather, (void*)b->wpart})
+        if (p) cudaFree(p);
+    if (b->hflag) cudaFreeHost(b->hflag);
+    if (b->hcounts) cudaFreeHost(b->hcounts);
+    if (b->hgather) cudaFreeHost(b->hgather);
     delete b;
     return VV_OK;
 }
 
 int vv_batch_create(int n, vv_ctx* const* ctxs, const vv_state* states, vv_batch** out) {
     if (n < 1 || !ctxs || !states || !out) return VV_ERR_ARG;
-    const bool dbg = getenv("VV_DEBUG") != nullptr;
-#define BTRACE(...)                         \
-    do {                                    \
-        if (dbg) {                          \
-            fprintf(stderr, "[vv_batch] " __VA_ARGS__); \
-            fflush(stderr);                 \
-        }                                   \
-    } while (0)
-    BTRACE("create n=%d\n", n);
     *out = nullptr;
     for (int i = 0; i < n; ++i) {
         const vv_state& s = states[i];
@@ -1646,60 +1971,144 @@ int vv_batch_create(int n, vv_ctx* const* ctxs, const vv_state* states, vv_batch
         for (int j = 0; j < i; ++j)
             if (ctxs[j] == ctxs[i]) return VV_ERR_ARG;   // one context per instance
     }
-    vv_batch* b = new vv_batch();
+    const vv_ctx* c0 = ctxs[0];
+    for (int i = 0; i < n; ++i) {
+        const vv_ctx* c = ctxs[i];
+        // one scheme, precision and preconditioner for the table; the wide
+        // 64 x 32 stencil tiles (nx a multiple of 64); the factored order
+        if (c->mixed != c0->mixed || c->g.bracket != c0->g.bracket ||
+            c->g.preconditioner != VV_PC_TENSOR_KINETIC || c->g.order == VV_ORDER_REFERENCE ||
+            c->nx % vv::WX != 0 || c->device != c0->device)
+            return VV_ERR_UNSUPPORTED;
+    }
+    vv_batch* b = new vv_batch();   // value-initialised: pointers and counts start at zero
     b->n = n;
     b->ctx.assign(ctxs, ctxs + n);
-    b->st.assign(states, states + n);
-    b->br.assign(n, nullptr);
-    b->ev.assign(n + 1, nullptr);
-    b->user = 0;
+    b->states.assign(states, states + n);
+    b->mixed = c0->mixed;
+    b->scheme = c0->g.bracket;
+    b->R = 4;
+    b->use_graph = c0->use_graph;
+    auto fail_b = [&](int code) { vv_batch_destroy(b); return code; };
+    if (cudaDeviceGetAttribute(&b->nsm, cudaDevAttrMultiProcessorCount, c0->device) != cudaSuccess)
+        return fail_b(fail_cuda(cudaGetLastError(), "multiprocessor count"));
+    std::vector<vv::BInst> tab(n);
+    for (int i = 0; i < n; ++i) {
+        vv_ctx* c = ctxs[i];
+        const vv_state& s = states[i];
+        vv::BInst& I = tab[i];
+        std::memset(&I, 0, sizeof I);
+        I.ds = c->ds;
+        I.nx = c->nx;
+        I.nv = c->nv;
+        I.ncell = c->ncell;
+        I.tiles_x = c->nx / vv::WX;
+        // vector kernels: 2048 cells per block item (eight warp items of 256)
+        I.vblk = (int)std::max<size_t>(1, std::min<size_t>((c->ncell + 2047) / 2048, (size_t)c->npart_max));
+        I.mom_seg = c->mom_seg;
+        I.mom_bx = (c->nx + vv::MOM_TX - 1) / vv::MOM_TX;
+        I.mom_S = c->mom_S;
+        I.cnt[vv::F_TILE] = I.tiles_x * ((c->nv + vv::WY - 1) / vv::WY);
+        I.cnt[vv::F_VEC] = I.vblk;
+        I.cnt[vv::F_MOM] = I.mom_bx * c->mom_S;
+        I.cnt[vv::F_INST] = 1;
+        I.bp = bparams(c, 0.5);
+        I.pp = pcparams(c);
+        I.pp.R = b->R;
+        I.pp.tw = b->mixed ? (const void*)c->tw32 : (const void*)c->tw;
+        I.tp.nv = c->nv;
+        I.tp.nmodes = c->nmodes;
+        I.tp.lambda = b->mixed ? (const void*)c->lambda32 : (const void*)c->lambda;
+        I.tp.alpha = b->mixed ? (const void*)c->alpha32 : (const void*)c->alpha;
+        I.tp.gamma = b->mixed ? (const void*)c->gamma32 : (const void*)c->gamma;
+        I.tp.dinv = b->mixed ? (const void*)c->dinv32 : (const void*)c->dinv;
+        I.po = pparams(c);
+        I.f = s.f; I.fh = s.fh; I.phi = s.phi; I.phih = s.phih;
+        I.h1c = s.h1c; I.h1h = s.h1h; I.h2c = s.h2c; I.h2h = s.h2h;
+        I.n = s.n; I.u = s.u; I.e = s.e; I.a = s.a;
+        I.Fh = c->Fh; I.tmp = c->tmp; I.fl = c->fl; I.part = c->part; I.mom_part = c->mom_part;
+        I.hxp = c->hxp; I.v = c->v; I.scal = c->scal;
+        if (b->mixed) {
+            I.V = c->V32; I.tmpT = c->tmp32; I.bT = c->bvec32; I.xT = c->delta32; I.specT = c->spec32;
+        } else {
+            I.V = c->V; I.tmpT = c->tmp; I.bT = c->bvec; I.xT = c->delta; I.specT = c->spec;
+        }
+        {
+            const int ch = (c->nv + vv::TRI_THREADS - 1) / vv::TRI_THREADS;
+            const size_t np = (size_t)c->nv + (c->nv + ch - 1) / ch;
+            b->smem_tri = std::max(b->smem_tri, np * (b->mixed ? 24 : 48));
+        }
+        b->smem_pois = std::max(b->smem_pois, c->smem_pois);
+    }
+    b_shape(b, tab, 8, 0);   // the largest shared-memory shape, for the limit check
+    {
+        int limit = 0;
+        int r = raise_smem_limits(&limit);
+        if (r != VV_OK) return fail_b(r);
+        if (std::max({b->smem_rfft, b->smem_irfft, b->smem_tri, b->smem_pois}) > (size_t)limit)
+            return fail_b(VV_ERR_UNSUPPORTED);
+    }
+    // per-warp partials: (restart + 2) columns of 8 vblk per instance
+    {
+        size_t words = 0;
+        std::vector<size_t> off(n);
+        for (int i = 0; i < n; ++i) {
+            off[i] = words;
+            words += (size_t)(ctxs[i]->restart + 2) * 8 * tab[i].vblk;
+        }
+        if (cudaMalloc((void**)&b->wpart, words * sizeof(double)) != cudaSuccess) return fail_b(VV_ERR_ALLOC);
+        for (int i = 0; i < n; ++i) tab[i].wpart = b->wpart + off[i];
+    }
     int r = VV_OK;
-    auto fail = [&](int code) { vv_batch_destroy(b); return code; };
-    if (cudaMallocHost((void**)&b->hbuf, sizeof(vv::DevState) * (size_t)n) != cudaSuccess) return fail(VV_ERR_ALLOC);
-    if (cudaStreamCreateWithFlags(&b->origin, cudaStreamNonBlocking) != cudaSuccess) return fail(VV_ERR_CUDA);
-    for (int i = 0; i < n; ++i)
-        if (cudaStreamCreateWithFlags(&b->br[i], cudaStreamNonBlocking) != cudaSuccess) return fail(VV_ERR_CUDA);
-    for (int i = 0; i <= n; ++i)
-        if (cudaEventCreateWithFlags(&b->ev[i], cudaEventDisableTiming) != cudaSuccess) return fail(VV_ERR_CUDA);
-    BTRACE("streams/events ok\n");
-    if (cudaGraphCreate(&b->g, 0) != cudaSuccess) return fail(VV_ERR_CUDA);
-    if (cudaStreamBeginCaptureToGraph(b->origin, b->g, nullptr, nullptr, 0, cudaStreamCaptureModeRelaxed) !=
-        cudaSuccess)
-        return fail(VV_ERR_CUDA);
-    cudaEventRecord(b->ev[n], b->origin);   // fork point
-    for (int i = 0; i < n && r == VV_OK; ++i) {
-        vv_ctx* c = b->ctx[i];
-        BTRACE("capture instance %d (nx=%d nv=%d)\n", i, c->nx, c->nv);
-        cudaError_t we = cudaStreamWaitEvent(b->br[i], b->ev[n], 0);
-        BTRACE("  wait event -> %s\n", cudaGetErrorString(we));
-        const cudaStream_t saved = c->st;
-        c->st = b->br[i];
-        r = capture_step(c, &b->st[i], b->g);
-        c->st = saved;
-        BTRACE("  capture_step -> %d (%s)\n", r, g_err);
-        if (r == VV_OK) {
-            std::array<unsigned long long, 5> h;
-            std::memcpy(h.data(), c->hnd, sizeof c->hnd);
-            b->hnd.push_back(h);
+    if ((r = upload_vec(&b->tab, tab))) return fail_b(r);
+    b->list_words = vv::blist_words(n);
+    b->words = (int)(offsetof(vv::DevState, hcol) / sizeof(unsigned int));
+    if (cudaMalloc((void**)&b->lists, (size_t)vv::NLIST * b->list_words * sizeof(int)) != cudaSuccess ||
+        cudaMalloc((void**)&b->counts, 8 * sizeof(unsigned int)) != cudaSuccess ||
+        cudaMalloc((void**)&b->flag, sizeof(int)) != cudaSuccess ||
+        cudaMalloc((void**)&b->gather, (size_t)n * b->words * sizeof(unsigned int)) != cudaSuccess)
+        return fail_b(VV_ERR_ALLOC);
+    if (cudaMallocHost((void**)&b->hflag, sizeof(int)) != cudaSuccess ||
+        cudaMallocHost((void**)&b->hcounts, 8 * sizeof(unsigned int)) != cudaSuccess ||
+        cudaMallocHost((void**)&b->hgather, (size_t)n * b->words * sizeof(unsigned int)) != cudaSuccess)
+        return fail_b(VV_ERR_ALLOC);
+    for (auto& s : b->cs)
+        if (cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking) != cudaSuccess) return fail_b(VV_ERR_CUDA);
+    b->user = 0;
+    b->st = b->cs[0];
+    // empty lists, then the list of every instance
+    if (cudaMemsetAsync(b->lists, 0, (size_t)vv::NLIST * b->list_words * sizeof(int), b->st) != cudaSuccess)
+        return fail_b(fail_cuda(cudaGetLastError(), "batch lists"));
+    b_shape(b, tab, 4, 0);
+    if ((r = b_apply_shape(b, tab)) != VV_OK) return fail_b(r);
+    {
+        const char* at = getenv("VV_AUTOTUNE");
+        if (!(at && at[0] == '0')) {
+            r = b->mixed ? b_autotune<float>(b, tab) : b_autotune<double>(b, tab);
+            if (r != VV_OK) return fail_b(r);
         }
     }
-    // join every forked branch, also after a failure (an unjoined branch
-    // would stay in the capture)
-    for (int i = 0; i < n; ++i) {
-        cudaStreamCaptureStatus cst = cudaStreamCaptureStatusNone;
-        if (cudaStreamIsCapturing(b->br[i], &cst) != cudaSuccess || cst != cudaStreamCaptureStatusActive) continue;
-        if (cudaEventRecord(b->ev[i], b->br[i]) == cudaSuccess) cudaStreamWaitEvent(b->origin, b->ev[i], 0);
+    b->launches = 0;
+    if (b->use_graph) {
+        if (cudaGraphCreate(&b->g, 0) != cudaSuccess) return fail_b(VV_ERR_CUDA);
+        if (cudaStreamBeginCaptureToGraph(b->cs[0], b->g, nullptr, nullptr, 0, cudaStreamCaptureModeRelaxed) !=
+            cudaSuccess)
+            return fail_b(VV_ERR_CUDA);
+        r = b->mixed ? b_dispatch_capture<float>(b) : b_dispatch_capture<double>(b);
+        cudaGraph_t outg = nullptr;
+        const cudaError_t e = cudaStreamEndCapture(b->cs[0], &outg);
+        if (r != VV_OK) return fail_b(r);
+        if (e != cudaSuccess) return fail_b(fail_cuda(e, "batch capture"));
+        cudaGraphInstantiateParams ip = {};
+        const cudaError_t ie = cudaGraphInstantiateWithParams(&b->ex, b->g, &ip);
+        if (ie != cudaSuccess) {
+            cudaGraphNodeType t = cudaGraphNodeTypeEmpty;
+            if (ip.errNode_out) cudaGraphNodeGetType(ip.errNode_out, &t);
+            char what[128];
+            snprintf(what, sizeof what, "batch instantiate (result %d, node type %d)", (int)ip.result_out, (int)t);
+            return fail_b(fail_cuda(ie, what));
+        }
     }
-    cudaGraph_t outg = nullptr;
-    BTRACE("end capture\n");
-    cudaError_t e = cudaStreamEndCapture(b->origin, &outg);
-    BTRACE("  -> %s\n", cudaGetErrorString(e));
-    if (r != VV_OK) return fail(r);
-    if (e != cudaSuccess) return fail(fail_cuda(e, "batch capture"));
-    e = cudaGraphInstantiate(&b->ex, b->g, 0);
-    BTRACE("instantiate -> %s\n", cudaGetErrorString(e));
-    if (e != cudaSuccess) return fail(fail_cuda(e, "batch instantiate"));
-    for (int i = 0; i < n; ++i) b->ctx[i]->use_graph = true;
     *out = b;
     return VV_OK;
 }
@@ -1713,31 +2122,62 @@ int vv_batch_set_stream(vv_batch* b, void* stream) {
 int vv_batch_step(vv_batch* b, const vv_snes_opts* so, const vv_ksp_opts* ko, vv_step_report* reports,
                   int* statuses) {
     if (!b || !so || !ko || !reports) return VV_ERR_ARG;
-    const size_t hdr = offsetof(vv::DevState, hcol);
     for (int i = 0; i < b->n; ++i) {
         vv_ctx* c = b->ctx[i];
         const int restart = (ko->restart > 0) ? ko->restart : c->restart;
-        if (restart > c->restart || restart < 1) return VV_ERR_ARG;
+        if (restart > c->restart || restart < 1 || ko->max_it < 0 || so->max_iter < 1) return VV_ERR_ARG;
+        // the instance's own graph handles stay out of the batch graph
+        for (auto& h : c->hnd) h = 0;
         const cudaStream_t saved = c->st;
         c->st = b->user;
-        std::memcpy(c->hnd, b->hnd[i].data(), sizeof c->hnd);
-        int r = upload_options(c, ko, so);
+        const int r = upload_options(c, ko, so);
         c->st = saved;
         TRY(r);
     }
-    CK(cudaGraphLaunch(b->ex, b->user));
-    for (int i = 0; i < b->n; ++i)
-        CK(cudaMemcpyAsync(&b->hbuf[i], b->ctx[i]->ds, hdr, cudaMemcpyDeviceToHost, b->user));
+    b->st = b->user;
+    const int64_t l0 = b->launches;
+    CK(cudaMemsetAsync(b->counts, 0, 8 * sizeof(unsigned int), b->user));
+    if (b->use_graph) {
+        CK(cudaGraphLaunch(b->ex, b->user));
+    } else {
+        const int r = b->mixed ? b_dispatch_host<float>(b) : b_dispatch_host<double>(b);
+        b->st = b->cs[0];
+        TRY(r);
+    }
+    b->st = b->user;
+    vv::k_b_gather_states<<<b->n, 128, 0, b->user>>>(b->tab, b->words, b->gather);
+    b->launches++;
+    CK(cudaGetLastError());
+    CK(cudaMemcpyAsync(b->hgather, b->gather, (size_t)b->n * b->words * sizeof(unsigned int), cudaMemcpyDeviceToHost,
+                       b->user));
+    CK(cudaMemcpyAsync(b->hcounts, b->counts, 8 * sizeof(unsigned int), cudaMemcpyDeviceToHost, b->user));
     CK(cudaStreamSynchronize(b->user));
+    b->st = b->cs[0];
+    if (b->use_graph) {
+        const unsigned* k = b->hcounts;
+        b->launches = l0 + 1 + b->nk_prologue + b->nk_revert_ctrl +
+                      (int64_t)k[vv::BC_PIC] * (b->nk_pic_head + b->nk_pic_tail) +
+                      (int64_t)(k[vv::BC_GM_START] + k[vv::BC_GM_FINISH]) * (b->nk_cycle_head + b->nk_cycle_tail) +
+                      (int64_t)k[vv::BC_INNER] * b->nk_arnoldi + (int64_t)k[vv::BC_REVERT] * b->nk_revert;
+    }
     int first_bad = VV_OK;
+    vv::DevState d;
     for (int i = 0; i < b->n; ++i) {
         vv_ctx* c = b->ctx[i];
+        std::memcpy(&d, b->hgather + (size_t)i * b->words, (size_t)b->words * sizeof(unsigned int));
         const int restart = (ko->restart > 0) ? ko->restart : c->restart;
-        const int s = fill_report(c, b->hbuf[i], restart, &reports[i], so->abort_residual);
+        const int s = fill_report(c, d, restart, &reports[i], so->abort_residual, false);
         if (statuses) statuses[i] = s;
         if (s != VV_OK && first_bad == VV_OK) first_bad = s;
     }
     return first_bad;
+}
+
+int vv_batch_launch_count(vv_batch* b, int64_t* launches, int reset) {
+    if (!b) return VV_ERR_ARG;
+    if (launches) *launches = b->launches;
+    if (reset) b->launches = 0;
+    return VV_OK;
 }
 
 }  // extern "C"

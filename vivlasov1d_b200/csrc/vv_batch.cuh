@@ -1,0 +1,515 @@
+// Lockstep batch kernels: one launch serves every instance of a batch.
+//
+// A batch is a table of independent runs (any mix of grid sizes and initial
+// data).  Each kernel of the time step is launched once for the whole table
+// with a persistent grid (sized to fill the GPU once): its blocks loop over
+// the work items of the instances that are active in the current pass --
+// every item is (instance, local block), and runs the same body as the
+// single-grid kernel does for that block.  Every instance keeps its own
+// Picard and GMRES state (DevState).  The one-block control kernel k_b_ctrl
+// applies the state transitions of the loop masks, folds them into the loop
+// conditions of the batch graph and rebuilds the compacted work lists:
+// for each mask, the active instances and, per kernel family, the prefix
+// sums of their block counts.  Instances that converge early thus cost
+// nothing in the passes the others still need.
+#pragma once
+#include "vv_bracket.cuh"
+#include "vv_pc.cuh"
+#include "vv_vec.cuh"
+
+namespace vv {
+
+// kernel families (work items per instance)
+enum BFam { F_TILE = 0, F_ROWS = 1, F_MODES = 2, F_VEC = 3, F_MOM = 4, F_INST = 5, NFAM = 6 };
+// work lists (one per mask)
+enum BList { L_ALL = 0, L_PIC = 1, L_GM = 2, L_GMR = 3, L_INNER = 4, L_REVERT = 5, NLIST = 6 };
+
+// per-instance description read by the batched kernels (device-resident)
+struct BInst {
+    DevState* ds;
+    int cnt[NFAM];               // work items per family
+    int nx, nv, tiles_x, vblk;   // wide-stencil tiles along x; blocks of the vector kernels
+    int mom_seg, mom_bx, mom_S;  // moments: v rows per segment, x blocks, segments
+    size_t ncell;
+    BracketParams bp;            // factor and xidx are set per launch
+    PcParams pp;                 // FFT parameters in the GMRES precision (R = rows per CTA of the batch)
+    TriParams tp;
+    PoissonParams po;
+    // run state (FP64, vv_state)
+    double *f, *fh, *phi, *phih, *h1c, *h1h, *h2c, *h2h, *n, *u, *e, *a;
+    // context work buffers (FP64)
+    double *Fh, *tmp, *fl, *part, *mom_part, *hxp, *v, *scal;
+    // GMRES buffers in the GMRES precision: basis, operator scratch, rhs, solution, spectrum
+    void *V, *tmpT, *bT, *xT, *specT;
+    // per-warp partial sums of the GMRES reductions: (restart + 2) columns of 8 * vblk
+    double* wpart;
+};
+
+// layout of one work list: [nact][total per family][ids: n][prefix per family: n+1]
+__host__ __device__ constexpr size_t blist_words(int n) { return 1 + NFAM + (size_t)n + (size_t)NFAM * (n + 1); }
+
+// active instances whose list a block stages in shared memory for the search
+constexpr int BLIST_SMEM = 512;
+
+// Loop of a persistent block over the work items of family F in list L:
+// body(instance, local block).  Block-uniform; a barrier separates items.
+// Lists of up to BLIST_SMEM instances are searched in shared memory.
+template <int F, typename Body>
+VV_DEV void for_work(const BInst* __restrict__ tab, const int* __restrict__ L, int n, Body body) {
+    __shared__ int s_pre[BLIST_SMEM + 1];
+    __shared__ int s_ids[BLIST_SMEM];
+    const int nact = L[0];
+    const int total = L[1 + F];
+    if ((int)blockIdx.x >= total) return;
+    const int* ids = L + 1 + NFAM;
+    const int* pre = ids + n + (size_t)F * (n + 1);
+    const bool staged = nact <= BLIST_SMEM;
+    if (staged) {
+        for (int i = threadIdx.x; i <= nact; i += blockDim.x) s_pre[i] = pre[i];
+        for (int i = threadIdx.x; i < nact; i += blockDim.x) s_ids[i] = ids[i];
+        __syncthreads();
+        pre = s_pre;
+        ids = s_ids;
+    }
+    for (int w = blockIdx.x; w < total; w += gridDim.x) {
+        int lo = 0, hi = nact - 1;   // the last p with pre[p] <= w
+        while (lo < hi) {
+            const int mid = (lo + hi + 1) >> 1;
+            if (pre[mid] <= w) lo = mid;
+            else hi = mid - 1;
+        }
+        body(tab[ids[lo]], w - pre[lo]);
+        __syncthreads();
+    }
+}
+
+// ---- stencil ----------------------------------------------------------------
+enum BSrc { BS_RESIDUAL = 0, BS_X = 1, BS_VIT = 2 };
+
+// RESIDUAL: tmp = R(f) (FP64) with tile partials; BS_X: tmpT = J x;
+// BS_VIT: tmpT = J V[it] (the Arnoldi input)
+template <int SCHEME, int SRC, typename T>
+__global__ void __launch_bounds__(WTHREADS, 4) k_b_bracket(const BInst* __restrict__ tab, const int* __restrict__ L, int n) {
+    for_work<F_TILE>(tab, L, n, [&](const BInst& I, int local) {
+        BracketParams p = I.bp;
+        p.xidx = nullptr;
+        const int bx = local % I.tiles_x, by = local / I.tiles_x;
+        if (SRC == BS_RESIDUAL) {
+            p.factor = 1.0;
+            bracket_wide_tile<SCHEME, MODE_RESIDUAL, double>(I.f, I.Fh, I.tmp, p, I.part, bx, by, I.tiles_x);
+        } else {
+            p.factor = 0.5;
+            const T* X = (SRC == BS_X) ? (const T*)I.xT : (const T*)I.V + (size_t)I.ds->it * I.ncell;
+            bracket_wide_tile<SCHEME, MODE_JVP, T>(X, nullptr, (T*)I.tmpT, p, nullptr, bx, by, I.tiles_x);
+        }
+    });
+}
+
+// ---- preconditioner ---------------------------------------------------------
+// rFFT rows: input FP64 tmp (right-hand side) or the GMRES-precision scratch
+template <typename TI, typename R>
+__global__ void k_b_rfft(const BInst* __restrict__ tab, const int* __restrict__ L, int n, int from_tmp64) {
+    for_work<F_ROWS>(tab, L, n, [&](const BInst& I, int local) {
+        const TI* X = from_tmp64 ? (const TI*)I.tmp : (const TI*)I.tmpT;
+        rfft_rows_block<TI, R>(X, (typename Cplx<R>::type*)I.specT, I.pp, local);
+    });
+}
+
+// tridiagonal solves: one CTA per mode, or one warp per mode (an item is
+// TRIW_WARPS modes); the batch autotuner picks the variant
+template <typename R>
+__global__ void __launch_bounds__(TRI_THREADS) k_b_tridiag(const BInst* __restrict__ tab, const int* __restrict__ L, int n) {
+    for_work<F_MODES>(tab, L, n, [&](const BInst& I, int local) {
+        tridiag_mode<R, true>((typename Cplx<R>::type*)I.specT, I.tp, local);
+    });
+}
+
+template <typename R>
+__global__ void __launch_bounds__(32 * TRIW_WARPS) k_b_tridiag_w(const BInst* __restrict__ tab, const int* __restrict__ L,
+                                                                int n) {
+    for_work<F_MODES>(tab, L, n, [&](const BInst& I, int local) {
+        const int k = local * TRIW_WARPS + (threadIdx.x >> 5);
+        if (k < I.tp.nmodes) tridiag_warp_mode<R>((typename Cplx<R>::type*)I.specT, I.tp, k);
+    });
+}
+
+enum BDst { BD_B = 0, BD_V0 = 1, BD_VNEXT = 2 };
+
+template <typename R, typename TO>
+__global__ void k_b_irfft(const BInst* __restrict__ tab, const int* __restrict__ L, int n, int dst) {
+    for_work<F_ROWS>(tab, L, n, [&](const BInst& I, int local) {
+        TO* Y = (TO*)I.bT;
+        if (dst == BD_V0) Y = (TO*)I.V;
+        else if (dst == BD_VNEXT) Y = (TO*)I.V + (size_t)(I.ds->it + 1) * I.ncell;
+        irfft_rows_block<R, TO>((const typename Cplx<R>::type*)I.specT, Y, I.pp, local);
+    });
+}
+
+// ---- step prologue: make_history + update_previous (run_base.py:749-763) ----
+__global__ void k_b_prologue(const BInst* __restrict__ tab, const int* __restrict__ L, int n) {
+    for_work<F_VEC>(tab, L, n, [&](const BInst& I, int bid) {
+        const int nb = I.vblk;
+        for (size_t i = bid * (size_t)blockDim.x + threadIdx.x; i < I.ncell; i += (size_t)nb * blockDim.x) {
+            const double fv = I.f[i];
+            I.fh[i] = fv;
+            I.Fh[i] = fv;
+        }
+        const int nx = I.nx;
+        const bool h2both = I.h2c && I.h2h;
+        for (int i = bid * blockDim.x + threadIdx.x; i < nx; i += nb * blockDim.x) {
+            const double h1 = I.h1c[i];
+            I.h1h[i] = h1;
+            if (h2both) I.h2h[i] = I.h2c[i];
+            if (I.phih) I.phih[i] = I.phi[i];
+            I.hxp[i] = h1;
+            I.hxp[nx + i] = h1;
+            I.hxp[2 * nx + i] = I.h2c ? I.h2c[i] : 0.0;
+            I.hxp[3 * nx + i] = I.h2h ? I.h2h[i] : 0.0;
+        }
+    });
+}
+
+// ---- Poisson residual of the current moments (and H1p <- h1c) -------------
+__global__ void __launch_bounds__(1024) k_b_poisson(const BInst* __restrict__ tab, const int* __restrict__ L, int n) {
+    for_work<F_INST>(tab, L, n, [&](const BInst& I, int) {
+        for (int i = threadIdx.x; i < I.nx; i += blockDim.x) I.hxp[i] = I.h1c[i];
+        poisson_apply_cta(I.phi, I.n, nullptr, I.nx, I.po.hx2_inv, I.po.charge, 2, &I.ds->pnorm2);
+    });
+}
+
+__global__ void k_b_pic_residual(const BInst* __restrict__ tab, const int* __restrict__ L, int n, int phase) {
+    for_work<F_INST>(tab, L, n, [&](const BInst& I, int) {
+        pic_residual_warp(I.ds, I.part, I.cnt[F_TILE], phase);
+    });
+}
+
+// ---- moments + Poisson + h1 -------------------------------------------------
+__global__ void __launch_bounds__(MOM_TX * MOM_TY)
+k_b_moments_partial(const BInst* __restrict__ tab, const int* __restrict__ L, int n) {
+    for_work<F_MOM>(tab, L, n, [&](const BInst& I, int local) {
+        const int bx = local % I.mom_bx, s = local / I.mom_bx;
+        moments_partial_block<double>(I.f, I.nx, I.nv, I.mom_seg, I.v, I.mom_part, bx, s);
+    });
+}
+
+__global__ void __launch_bounds__(POIS_THREADS) k_b_moments_poisson(const BInst* __restrict__ tab, const int* __restrict__ L,
+                                                                   int n) {
+    for_work<F_INST>(tab, L, n, [&](const BInst& I, int) {
+        moments_poisson_cta(I.mom_part, nullptr, I.n, I.u, I.e, I.a, I.phi, I.h1c, I.scal, I.po);
+    });
+}
+
+// ---- Picard pass ------------------------------------------------------------
+// start of the linear solve: x = 0, GMRES state reset; fl <- f (the iterate
+// a rejected pass reverts to)
+template <typename T>
+__global__ void k_b_gm_init(const BInst* __restrict__ tab, const int* __restrict__ L, int n) {
+    for_work<F_VEC>(tab, L, n, [&](const BInst& I, int bid) {
+        gm_init_block<T>(I.ds, (T*)I.xT, I.ncell, bid, I.vblk);
+        for (size_t i = bid * (size_t)blockDim.x + threadIdx.x; i < I.ncell; i += (size_t)I.vblk * blockDim.x)
+            I.fl[i] = I.f[i];
+    });
+}
+
+template <typename T>
+__global__ void k_b_pic_apply(const BInst* __restrict__ tab, const int* __restrict__ L, int n) {
+    for_work<F_VEC>(tab, L, n, [&](const BInst& I, int bid) {
+        pic_apply_block<T, double>(I.ds, (const T*)I.xT, I.f, I.ncell, bid, I.vblk);
+    });
+}
+
+__global__ void k_b_revert(const BInst* __restrict__ tab, const int* __restrict__ L, int n) {
+    for_work<F_VEC>(tab, L, n, [&](const BInst& I, int bid) {
+        for (size_t i = bid * (size_t)blockDim.x + threadIdx.x; i < I.ncell; i += (size_t)I.vblk * blockDim.x)
+            I.f[i] = I.fl[i];
+    });
+}
+
+// ---- GMRES ------------------------------------------------------------------
+// The batch reductions work on warp items: block item `bid` of an instance is
+// eight warp items wi = 8 bid + warp, and warp item wi covers the cells
+// i = 32 wi + lane + 32 nwi s (nwi = 8 vblk warp items, s = 0, 1, ...).  Each
+// warp writes its own partial sum (no barrier, no atomic); a one-block
+// finalize kernel per instance reduces them in a fixed order.
+VV_DEV int wi_count(const BInst& I) { return 8 * I.vblk; }
+
+// cycle head: V0 = b (first cycle) or b - P^-1 J x (restart, P^-1 J x in V0)
+template <typename T>
+__global__ void k_b_gm_head(const BInst* __restrict__ tab, const int* __restrict__ L, int n) {
+    for_work<F_VEC>(tab, L, n, [&](const BInst& I, int bid) {
+        const T* b = (const T*)I.bT;
+        T* v = (T*)I.V;
+        const bool first = I.ds->first != 0;
+        for (size_t i = bid * (size_t)blockDim.x + threadIdx.x; i < I.ncell; i += (size_t)I.vblk * blockDim.x)
+            v[i] = first ? b[i] : (T)(1.0 * (double)b[i] + (-1.0) * (double)v[i]);
+    });
+}
+
+// ||V0||^2 per warp item
+template <typename T>
+__global__ void __launch_bounds__(RED_THREADS) k_b_gm_cycle_p(const BInst* __restrict__ tab, const int* __restrict__ L, int n) {
+    for_work<F_VEC>(tab, L, n, [&](const BInst& I, int bid) {
+        const int lane = threadIdx.x & 31, nwi = wi_count(I), wi = bid * 8 + (threadIdx.x >> 5);
+        const T* V0 = (const T*)I.V;
+        double acc = 0.0;
+        for (size_t i = (size_t)wi * 32 + lane; i < I.ncell; i += (size_t)nwi * 32) {
+            const double v = (double)V0[i];
+            acc += v * v;
+        }
+        acc = warp_sum(acc);
+        if (lane == 0) I.wpart[wi] = acc;
+    });
+}
+
+// cycle start: res, convergence test, scale, `active`
+__global__ void k_b_gm_cycle_f(const BInst* __restrict__ tab, const int* __restrict__ L, int n) {
+    for_work<F_INST>(tab, L, n, [&](const BInst& I, int) {
+        if (threadIdx.x >= 32) return;
+        const double ss2 = warp_reduce_parts(I.wpart, wi_count(I));
+        if (threadIdx.x == 0) gm_cycle_state(I.ds, ss2);
+    });
+}
+
+template <typename T>
+__global__ void k_b_gm_scale(const BInst* __restrict__ tab, const int* __restrict__ L, int n) {
+    for_work<F_VEC>(tab, L, n, [&](const BInst& I, int bid) {
+        gm_scale_block<T>(I.ds, (T*)I.V, I.ncell, I.ncell, bid, I.vblk);
+    });
+}
+
+// <w, V_q>, q = 0..it, w = V[it+1], per warp item (column q of the partials)
+template <typename T>
+__global__ void __launch_bounds__(RED_THREADS) k_b_gm_mdot_p(const BInst* __restrict__ tab, const int* __restrict__ L, int n) {
+    for_work<F_VEC>(tab, L, n, [&](const BInst& I, int bid) {
+        const int lane = threadIdx.x & 31, nwi = wi_count(I), wi = bid * 8 + (threadIdx.x >> 5);
+        const int it = I.ds->it, m = it + 1;
+        const size_t nc = I.ncell;
+        const T* V = (const T*)I.V;
+        const T* w = V + (size_t)(it + 1) * nc;
+        for (int q0 = 0; q0 < m; q0 += MDOT_CHUNK) {
+            double acc[MDOT_CHUNK];
+#pragma unroll
+            for (int c = 0; c < MDOT_CHUNK; ++c) acc[c] = 0.0;
+            const int cnt = min(MDOT_CHUNK, m - q0);
+            for (size_t i = (size_t)wi * 32 + lane; i < nc; i += (size_t)nwi * 32) {
+                const double wv = (double)w[i];
+#pragma unroll
+                for (int c = 0; c < MDOT_CHUNK; ++c)
+                    if (c < cnt) acc[c] += wv * (double)V[(size_t)(q0 + c) * nc + i];
+            }
+#pragma unroll
+            for (int c = 0; c < MDOT_CHUNK; ++c) {
+                if (c < cnt) {
+                    const double t = warp_sum(acc[c]);
+                    if (lane == 0) I.wpart[(size_t)(q0 + c) * nwi + wi] = t;
+                }
+            }
+        }
+    });
+}
+
+// hcol_q from the partials (one warp per column)
+__global__ void __launch_bounds__(RED_THREADS) k_b_gm_mdot_f(const BInst* __restrict__ tab, const int* __restrict__ L, int n) {
+    for_work<F_INST>(tab, L, n, [&](const BInst& I, int) {
+        DevState* s = I.ds;
+        const int m = s->it + 1, nwi = wi_count(I);
+        for (int q = threadIdx.x >> 5; q < m; q += RED_THREADS / 32) {
+            const double t = warp_reduce_parts(I.wpart + (size_t)q * nwi, nwi);
+            if ((threadIdx.x & 31) == 0) s->hcol[q] = t;
+        }
+    });
+}
+
+// w += sum_q (-hcol_q) V_q and ||w||^2 per warp item
+template <typename T>
+__global__ void __launch_bounds__(RED_THREADS) k_b_gm_maxpy_p(const BInst* __restrict__ tab, const int* __restrict__ L, int n) {
+    __shared__ double cf[MAX_RESTART + 2];
+    for_work<F_VEC>(tab, L, n, [&](const BInst& I, int bid) {
+        const DevState* s = I.ds;
+        const int m = s->it + 1;
+        for (int q = threadIdx.x; q < m; q += blockDim.x) cf[q] = -s->hcol[q];
+        __syncthreads();
+        const int lane = threadIdx.x & 31, nwi = wi_count(I), wi = bid * 8 + (threadIdx.x >> 5);
+        const size_t nc = I.ncell;
+        T* V = (T*)I.V;
+        T* w = V + (size_t)m * nc;
+        double acc = 0.0;
+        for (size_t i = (size_t)wi * 32 + lane; i < nc; i += (size_t)nwi * 32) {
+            double wv = (double)w[i];
+            for (int q = 0; q < m; ++q) wv += cf[q] * (double)V[(size_t)q * nc + i];
+            w[i] = (T)wv;
+            acc += wv * wv;
+        }
+        acc = warp_sum(acc);
+        if (lane == 0) I.wpart[wi] = acc;
+    });
+}
+
+// ||w|| and the Arnoldi bookkeeping (Hessenberg column, Givens, test)
+__global__ void k_b_gm_maxpy_f(const BInst* __restrict__ tab, const int* __restrict__ L, int n) {
+    for_work<F_INST>(tab, L, n, [&](const BInst& I, int) {
+        if (threadIdx.x >= 32) return;
+        const double ss2 = warp_reduce_parts(I.wpart, wi_count(I));
+        if (threadIdx.x == 0) gm_arnoldi(I.ds, sqrt(ss2));
+    });
+}
+
+// end of a cycle: triangular solve once per instance (coefficients into
+// hcol, their count into pad), then the solution update x += sum nrs_q V_q
+__global__ void k_b_gm_solve(const BInst* __restrict__ tab, const int* __restrict__ L, int n) {
+    for_work<F_INST>(tab, L, n, [&](const BInst& I, int) {
+        if (threadIdx.x != 0) return;
+        DevState* s = I.ds;
+        int npad = 0, breakdown = 0;
+        gm_backsolve(s, s->hcol, &npad, &breakdown);
+        gm_finish_state(s, npad, breakdown);
+    });
+}
+
+template <typename T>
+__global__ void __launch_bounds__(RED_THREADS) k_b_gm_update(const BInst* __restrict__ tab, const int* __restrict__ L, int n) {
+    __shared__ double nrs[MAX_RESTART + 1];
+    for_work<F_VEC>(tab, L, n, [&](const BInst& I, int bid) {
+        const DevState* s = I.ds;
+        const int m = s->pad;
+        for (int q = threadIdx.x; q < m; q += blockDim.x) nrs[q] = s->hcol[q];
+        __syncthreads();
+        if (m <= 0) return;
+        const T* V = (const T*)I.V;
+        T* x = (T*)I.xT;
+        for (size_t i = bid * (size_t)RED_THREADS + threadIdx.x; i < I.ncell; i += (size_t)I.vblk * RED_THREADS) {
+            double xi = (double)x[i];
+            for (int q = 0; q < m; ++q) xi += nrs[q] * (double)V[(size_t)q * I.ncell + i];
+            x[i] = (T)xi;
+        }
+    });
+}
+
+// ---- control ----------------------------------------------------------------
+// One block.  Applies the mask transitions of `op` to every instance,
+// rebuilds the work lists of the masks it changed, and folds the result into
+// the batch loop condition: handle (0 outside a graph) and *flag (read by
+// the host-driven loop).  counts[op] counts the passes.
+enum BCtrl { BC_PIC = 0, BC_GM_START = 1, BC_INNER = 2, BC_GM_FINISH = 3, BC_REVERT = 4, BC_ALL = 5 };
+
+constexpr int CTRL_THREADS = 1024;
+
+// in-block exclusive scan of one int per thread (CTRL_THREADS threads); returns the block total
+__device__ __forceinline__ int ctrl_scan(int v, int& excl, int* sh) {
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    int inc = v;
+#pragma unroll
+    for (int d = 1; d < 32; d <<= 1) {
+        const int o = __shfl_up_sync(0xffffffffu, inc, d);
+        if (lane >= d) inc += o;
+    }
+    if (lane == 31) sh[wid] = inc;
+    __syncthreads();
+    if (wid == 0) {
+        int s = (lane < CTRL_THREADS / 32) ? sh[lane] : 0;
+#pragma unroll
+        for (int d = 1; d < 32; d <<= 1) {
+            const int o = __shfl_up_sync(0xffffffffu, s, d);
+            if (lane >= d) s += o;
+        }
+        sh[lane] = s;   // inclusive warp totals
+    }
+    __syncthreads();
+    excl = inc - v + (wid > 0 ? sh[wid - 1] : 0);
+    const int total = sh[CTRL_THREADS / 32 - 1];
+    __syncthreads();
+    return total;
+}
+
+// rebuild list `l` from the per-instance membership test `in(q)`
+template <typename In>
+__device__ void ctrl_build(const BInst* __restrict__ tab, int n, int* __restrict__ lists, int l, In in, int* sh) {
+    int* L = lists + (size_t)l * blist_words(n);
+    int* ids = L + 1 + NFAM;
+    int* pre = ids + n;
+    __shared__ int base_id, base_f[NFAM];
+    if (threadIdx.x == 0) {
+        base_id = 0;
+        for (int f = 0; f < NFAM; ++f) base_f[f] = 0;
+    }
+    __syncthreads();
+    for (int q0 = 0; q0 < n; q0 += CTRL_THREADS) {
+        const int q = q0 + threadIdx.x;
+        const int on = (q < n && in(q)) ? 1 : 0;
+        int pos = 0;
+        const int cnt_on = ctrl_scan(on, pos, sh);
+        if (on) ids[base_id + pos] = q;
+        for (int f = 0; f < NFAM; ++f) {
+            const int c = on ? tab[q].cnt[f] : 0;
+            int ex = 0;
+            const int tot = ctrl_scan(c, ex, sh);
+            if (on) pre[(size_t)f * (n + 1) + base_id + pos] = base_f[f] + ex;
+            __syncthreads();
+            if (threadIdx.x == 0) base_f[f] += tot;
+            __syncthreads();
+        }
+        if (threadIdx.x == 0) base_id += cnt_on;
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        L[0] = base_id;
+        for (int f = 0; f < NFAM; ++f) {
+            L[1 + f] = base_f[f];
+            pre[(size_t)f * (n + 1) + base_id] = base_f[f];
+        }
+    }
+    __syncthreads();
+}
+
+__global__ void __launch_bounds__(CTRL_THREADS)
+k_b_ctrl(const BInst* __restrict__ tab, int n, int op, unsigned long long handle, int* __restrict__ flag,
+         unsigned int* __restrict__ counts, int* __restrict__ lists) {
+    __shared__ int sh[CTRL_THREADS / 32];
+    // mask transitions (each instance by one thread)
+    for (int q = threadIdx.x; q < n; q += CTRL_THREADS) {
+        DevState* s = tab[q].ds;
+        if (op == BC_GM_START) s->gm_outer = s->pic_active != 0 ? 1 : 0;
+        else if (op == BC_GM_FINISH && s->gm_outer) s->gm_outer = s->reason == R_ITERATING ? 1 : 0;
+    }
+    __syncthreads();
+    int l = L_PIC;
+    switch (op) {
+        case BC_ALL: l = L_ALL; ctrl_build(tab, n, lists, L_ALL, [&](int) { return true; }, sh); break;
+        case BC_PIC: ctrl_build(tab, n, lists, L_PIC, [&](int q) { return tab[q].ds->pic_active != 0; }, sh); break;
+        case BC_GM_START:
+        case BC_GM_FINISH:
+            l = L_GM;
+            ctrl_build(tab, n, lists, L_GM, [&](int q) { return tab[q].ds->gm_outer != 0; }, sh);
+            ctrl_build(tab, n, lists, L_GMR, [&](int q) {
+                const DevState* s = tab[q].ds;
+                return s->gm_outer != 0 && s->first == 0;
+            }, sh);
+            break;
+        case BC_INNER:
+            l = L_INNER;
+            ctrl_build(tab, n, lists, L_INNER, [&](int q) {
+                const DevState* s = tab[q].ds;
+                return s->gm_outer != 0 && s->active != 0;
+            }, sh);
+            break;
+        default:
+            l = L_REVERT;
+            ctrl_build(tab, n, lists, L_REVERT, [&](int q) { return tab[q].ds->pic_revert != 0; }, sh);
+            break;
+    }
+    if (threadIdx.x == 0) {
+        const int any = lists[(size_t)l * blist_words(n)] > 0 ? 1 : 0;
+        set_cond(handle, any ? 1u : 0u);
+        if (flag) *flag = any;
+        if (any && counts) counts[op] += 1u;
+    }
+}
+
+// copy the first `words` 32-bit words of every instance's state into out[n][words]
+__global__ void k_b_gather_states(const BInst* __restrict__ tab, int words, unsigned int* __restrict__ out) {
+    const unsigned int* src = reinterpret_cast<const unsigned int*>(tab[blockIdx.x].ds);
+    unsigned int* dst = out + (size_t)blockIdx.x * words;
+    for (int w = threadIdx.x; w < words; w += blockDim.x) dst[w] = src[w];
+}
+
+}  // namespace vv

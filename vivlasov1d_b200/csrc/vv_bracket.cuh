@@ -339,11 +339,13 @@ template <typename T> struct Vec2;
 template <> struct Vec2<double> { using type = double2; };
 template <> struct Vec2<float> { using type = float2; };
 
+// One 64 x 32 output tile (bx, by) of the bracket; the tile grid is tiles_x
+// wide (the per-tile sum of squares goes to sumsq[bx + tiles_x by]).  Shared
+// by the single-grid kernel below and the batched kernels.
 template <int SCHEME, int MODE, typename T>
-__global__ void __launch_bounds__(WTHREADS, 4)
-k_bracket_wide(const T* __restrict__ X, const T* __restrict__ Xh, T* __restrict__ Y,
-               BracketParams p, double* __restrict__ sumsq) {
-    if (p.xidx) X += (size_t)(*p.xidx) * p.xstride;
+__device__ __forceinline__ void bracket_wide_tile(const T* __restrict__ X, const T* __restrict__ Xh,
+                                                  T* __restrict__ Y, const BracketParams& p,
+                                                  double* __restrict__ sumsq, int bx, int by, int tiles_x) {
     using V2 = typename Vec2<T>::type;
     __shared__ __align__(16) T sx[WSY][WSX];
     __shared__ double sa[WSY];
@@ -352,7 +354,7 @@ k_bracket_wide(const T* __restrict__ X, const T* __restrict__ Xh, T* __restrict_
     __shared__ double scol[WX][3];
     __shared__ double sred[WTHREADS / 32];
     const int tid = threadIdx.x;
-    const int i0 = blockIdx.x * WX, j0 = blockIdx.y * WY;
+    const int i0 = bx * WX, j0 = by * WY;
     const int nx = p.nx, nv = p.nv;
     // ---- stage the input tile (x pairs) ----
     constexpr int NP = WSX / 2;   // 34 pairs per row
@@ -461,8 +463,16 @@ k_bracket_wide(const T* __restrict__ X, const T* __restrict__ Xh, T* __restrict_
     }
     if (sumsq) {
         const double t = block_sum(acc2, sred);
-        if (tid == 0) sumsq[blockIdx.x + gridDim.x * blockIdx.y] = t;
+        if (tid == 0) sumsq[bx + tiles_x * by] = t;
     }
+}
+
+template <int SCHEME, int MODE, typename T>
+__global__ void __launch_bounds__(WTHREADS, 4)
+k_bracket_wide(const T* __restrict__ X, const T* __restrict__ Xh, T* __restrict__ Y,
+               BracketParams p, double* __restrict__ sumsq) {
+    if (p.xidx) X += (size_t)(*p.xidx) * p.xstride;
+    bracket_wide_tile<SCHEME, MODE, T>(X, Xh, Y, p, sumsq, blockIdx.x, blockIdx.y, gridDim.x);
 }
 
 }  // namespace vv

@@ -88,7 +88,8 @@ __device__ __forceinline__ void block_fft(double2* buf, int M, const double2* st
 // spectrum written transposed: spec[k*nv + j], k = 0..M.
 // dynamic smem: [M twiddles][R rows x (M+1) complex]
 template <typename TI, typename R>
-__global__ void k_rfft_rows(const TI* __restrict__ X, typename Cplx<R>::type* __restrict__ spec, PcParams p) {
+__device__ __forceinline__ void rfft_rows_block(const TI* __restrict__ X, typename Cplx<R>::type* __restrict__ spec,
+                                                const PcParams& p, int bid) {
     using C = typename Cplx<R>::type;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     C* stw = reinterpret_cast<C*>(smem_raw);
@@ -97,7 +98,7 @@ __global__ void k_rfft_rows(const TI* __restrict__ X, typename Cplx<R>::type* __
     const C* tw = reinterpret_cast<const C*>(p.tw);
     for (int k = threadIdx.x; k < M; k += blockDim.x) stw[k] = tw[k];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int j0 = blockIdx.x * p.R;
+    const int j0 = bid * p.R;
     const int j = j0 + warp;
     C* buf = rows + warp * LD;
     __syncthreads();
@@ -149,12 +150,17 @@ __global__ void k_rfft_rows(const TI* __restrict__ X, typename Cplx<R>::type* __
     }
 }
 
+template <typename TI, typename R>
+__global__ void k_rfft_rows(const TI* __restrict__ X, typename Cplx<R>::type* __restrict__ spec, PcParams p) {
+    rfft_rows_block<TI, R>(X, spec, p, blockIdx.x);
+}
+
 // spec[k*nv + j] (k = 0..M) -> rows of Y (one warp per row), scaled by 1/nx
 // dynamic smem: [M twiddles][R rows x (M+1) spectrum][R rows x (M+1) work]
 template <typename R, typename TO>
-__global__ void k_irfft_rows(const typename Cplx<R>::type* __restrict__ spec, TO* __restrict__ Y, PcParams p) {
+__device__ __forceinline__ void irfft_rows_block(const typename Cplx<R>::type* __restrict__ spec,
+                                                 TO* __restrict__ Y, const PcParams& p, int bid) {
     using C = typename Cplx<R>::type;
-    if (p.yidx) Y += (size_t)(*p.yidx + p.yoff) * p.ystride;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     C* stw = reinterpret_cast<C*>(smem_raw);
     const int M = p.M, LD = M + 1;
@@ -162,7 +168,7 @@ __global__ void k_irfft_rows(const typename Cplx<R>::type* __restrict__ spec, TO
     C* work = xs + p.R * LD;
     const C* tw = reinterpret_cast<const C*>(p.tw);
     for (int k = threadIdx.x; k < M; k += blockDim.x) stw[k] = tw[k];
-    const int j0 = blockIdx.x * p.R;
+    const int j0 = bid * p.R;
     const int nrow = min(p.R, p.nv - j0);
     for (int idx = threadIdx.x; idx < (M + 1) * p.R; idx += blockDim.x) {
         const int k = idx / p.R, r = idx - k * p.R;
@@ -195,6 +201,12 @@ __global__ void k_irfft_rows(const typename Cplx<R>::type* __restrict__ spec, TO
         row[2 * m] = (TO)(z.x * s);
         row[2 * m + 1] = (TO)(z.y * s);
     }
+}
+
+template <typename R, typename TO>
+__global__ void k_irfft_rows(const typename Cplx<R>::type* __restrict__ spec, TO* __restrict__ Y, PcParams p) {
+    if (p.yidx) Y += (size_t)(*p.yidx + p.yoff) * p.ystride;
+    irfft_rows_block<R, TO>(spec, Y, p, blockIdx.x);
 }
 
 // ---------------------------------------------------------------------------
@@ -452,12 +464,10 @@ __device__ C block_scan_aff(Aff<C> a, bool forward, Aff<C>* sh) {
 // shared memory with one pad slot per chunk (conflict-free chunk-strided
 // access).  dynamic smem: 3 arrays of nv + nv/C complex/real slots.
 template <typename R, bool STAGE>
-__global__ void __launch_bounds__(TRI_THREADS)
-k_tridiag_modes(typename Cplx<R>::type* __restrict__ spec, TriParams p) {
+__device__ __forceinline__ void tridiag_mode(typename Cplx<R>::type* __restrict__ spec, const TriParams& p, int k) {
     using C = typename Cplx<R>::type;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     __shared__ Aff<C> shw[TRI_THREADS / 32];
-    const int k = blockIdx.x;
     const int nv = p.nv;
     const int CH = (nv + TRI_THREADS - 1) / TRI_THREADS;   // rows per thread
     const int NP = nv + (nv + CH - 1) / CH;               // padded length
@@ -539,6 +549,11 @@ k_tridiag_modes(typename Cplx<R>::type* __restrict__ spec, TriParams p) {
     }
 }
 
+template <typename R, bool STAGE>
+__global__ void __launch_bounds__(TRI_THREADS)
+k_tridiag_modes(typename Cplx<R>::type* __restrict__ spec, TriParams p) {
+    tridiag_mode<R, STAGE>(spec, p, blockIdx.x);
+}
 
 // Warp-scan of affine maps (no shared memory): returns the image of 0 under
 // the composition of the maps of all earlier lanes in `forward` order.
@@ -562,12 +577,11 @@ __device__ __forceinline__ C warp_scan_aff(Aff<C> a, bool forward) {
 // No shared memory, no block barrier.
 constexpr int TRIW_WARPS = 8;
 
+// mode k of the spectrum by the calling warp
 template <typename R>
-__global__ void __launch_bounds__(32 * TRIW_WARPS)
-k_tridiag_warp(typename Cplx<R>::type* __restrict__ spec, TriParams p) {
+__device__ __forceinline__ void tridiag_warp_mode(typename Cplx<R>::type* __restrict__ spec, const TriParams& p,
+                                                  int k) {
     using C = typename Cplx<R>::type;
-    const int k = blockIdx.x * TRIW_WARPS + (threadIdx.x >> 5);
-    if (k >= p.nmodes) return;
     const int lane = threadIdx.x & 31;
     const int nv = p.nv;
     const int CH = (nv + 31) / 32;
@@ -625,6 +639,14 @@ k_tridiag_warp(typename Cplx<R>::type* __restrict__ spec, TriParams p) {
         else x = c_mul(d, c_sub(yv, c_mul(c_rmul(lam, ga[r]), x)));
         line[r] = x;
     }
+}
+
+template <typename R>
+__global__ void __launch_bounds__(32 * TRIW_WARPS)
+k_tridiag_warp(typename Cplx<R>::type* __restrict__ spec, TriParams p) {
+    const int k = blockIdx.x * TRIW_WARPS + (threadIdx.x >> 5);
+    if (k >= p.nmodes) return;
+    tridiag_warp_mode<R>(spec, p, k);
 }
 
 }  // namespace vv

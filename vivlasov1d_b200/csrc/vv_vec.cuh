@@ -32,7 +32,7 @@ struct DevState {
     // Picard control
     int pic_i, pic_stop, pic_revert, pic_stop_rule;
     int pic_max_iter, ksp_failures, gmres_total, pic_active;
-    int ncycles, pad2;
+    int ncycles, gm_outer;   // gm_outer: in a GMRES solve (lockstep batch mask)
     double snes_atol, abort_residual, pred, prev, pnorm2;
     // conditional handles (0 outside a graph)
     unsigned long long h_gm_outer, h_gm_inner, h_gm_first, h_pic, h_revert;
@@ -68,19 +68,20 @@ VV_DEV int ksp_converged(DevState* s, int n, double rnorm) {
 
 // Last-CTA election (threadfence reduction): true in every thread of the
 // block that finishes last; that block also resets the counter.  No waiting.
-__device__ __forceinline__ bool last_block(unsigned int* counter) {
+__device__ __forceinline__ bool last_block(unsigned int* counter, unsigned int nblk) {
     __shared__ bool am_last;
     __threadfence();
     __syncthreads();
     if (threadIdx.x == 0) {
         const unsigned int t = atomicAdd(counter, 1u);
-        am_last = (t == gridDim.x - 1);
+        am_last = (t == nblk - 1);
         if (am_last) *counter = 0u;
     }
     __syncthreads();
     if (am_last) __threadfence();
     return am_last;
 }
+__device__ __forceinline__ bool last_block(unsigned int* counter) { return last_block(counter, gridDim.x); }
 
 // deterministic sum of part[0..np) by one warp
 __device__ __forceinline__ double warp_reduce_parts(const double* part, int np) {
@@ -144,10 +145,10 @@ __global__ void k_axpby(const T* __restrict__ x, T* __restrict__ y, size_t n, do
 // ----- GMRES kernels (state driven) ----------------------------------------
 // Start of a solve: x = 0; its = 0; first cycle.
 template <typename T>
-__global__ void k_gm_init(DevState* s, T* __restrict__ x, size_t n) {
-    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
+__device__ __forceinline__ void gm_init_block(DevState* s, T* __restrict__ x, size_t n, int bid, int nblk) {
+    for (size_t i = bid * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)nblk * blockDim.x)
         x[i] = T(0);
-    if (blockIdx.x == 0 && threadIdx.x == 0) {
+    if (bid == 0 && threadIdx.x == 0) {
         s->its = 0;
         s->reason = R_ITERATING;
         s->first = 1;
@@ -157,24 +158,13 @@ __global__ void k_gm_init(DevState* s, T* __restrict__ x, size_t n) {
         set_cond(s->h_gm_outer, 1u);
     }
 }
-
-// Cycle start (KSPGMRESCycle top): ||V0||^2 partials; the last CTA computes
-// res, the convergence test with n = its, the scale 1/res and `active`.
 template <typename T>
-__global__ void __launch_bounds__(RED_THREADS)
-k_gm_cycle(DevState* s, const T* __restrict__ V0, size_t n, double* __restrict__ part) {
-    __shared__ double sh[RED_THREADS / 32];
-    double acc = 0.0;
-    for (size_t i = blockIdx.x * (size_t)RED_THREADS + threadIdx.x; i < n; i += (size_t)gridDim.x * RED_THREADS) {
-        const double v = (double)V0[i];
-        acc += v * v;
-    }
-    const double t = block_sum(acc, sh);
-    if (threadIdx.x == 0) part[blockIdx.x] = t;
-    if (!last_block(&s->cnt[0])) return;
-    if (threadIdx.x >= 32) return;
-    const double ss2 = warp_reduce_parts(part, gridDim.x);
-    if (threadIdx.x != 0) return;
+__global__ void k_gm_init(DevState* s, T* __restrict__ x, size_t n) {
+    gm_init_block<T>(s, x, n, blockIdx.x, gridDim.x);
+}
+
+// state update of a cycle start from ||V0||^2 (one thread)
+VV_DEV void gm_cycle_state(DevState* s, double ss2) {
     const double res = sqrt(ss2);
     s->ncycles += 1;
     s->it = 0;
@@ -191,20 +181,51 @@ k_gm_cycle(DevState* s, const T* __restrict__ V0, size_t n, double* __restrict__
     set_cond(s->h_gm_inner, (unsigned)s->active);
 }
 
+// Cycle start (KSPGMRESCycle top): ||V0||^2 partials; the last CTA computes
+// res, the convergence test with n = its, the scale 1/res and `active`.
+template <typename T>
+__device__ __forceinline__ void gm_cycle_block(DevState* s, const T* __restrict__ V0, size_t n,
+                                               double* __restrict__ part, int bid, int nblk) {
+    __shared__ double sh[RED_THREADS / 32];
+    double acc = 0.0;
+    for (size_t i = bid * (size_t)RED_THREADS + threadIdx.x; i < n; i += (size_t)nblk * RED_THREADS) {
+        const double v = (double)V0[i];
+        acc += v * v;
+    }
+    const double t = block_sum(acc, sh);
+    if (threadIdx.x == 0) part[bid] = t;
+    if (!last_block(&s->cnt[0], nblk)) return;
+    if (threadIdx.x >= 32) return;
+    const double ss2 = warp_reduce_parts(part, nblk);
+    if (threadIdx.x != 0) return;
+    gm_cycle_state(s, ss2);
+}
+template <typename T>
+__global__ void __launch_bounds__(RED_THREADS)
+k_gm_cycle(DevState* s, const T* __restrict__ V0, size_t n, double* __restrict__ part) {
+    gm_cycle_block<T>(s, V0, n, part, blockIdx.x, gridDim.x);
+}
+
 // V[idx] *= scale, idx = s->it (the vector just produced)
 template <typename T>
-__global__ void k_gm_scale(DevState* s, T* __restrict__ V, size_t ldv, size_t n) {
+__device__ __forceinline__ void gm_scale_block(const DevState* s, T* __restrict__ V, size_t ldv, size_t n, int bid,
+                                               int nblk) {
     T* v = V + (size_t)s->it * ldv;
     const double sc = s->scale;
-    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
+    for (size_t i = bid * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)nblk * blockDim.x)
         v[i] = (T)((double)v[i] * sc);
+}
+template <typename T>
+__global__ void k_gm_scale(DevState* s, T* __restrict__ V, size_t ldv, size_t n) {
+    gm_scale_block<T>(s, V, ldv, n, blockIdx.x, gridDim.x);
 }
 
 // hcol_q = <w, V_q>, q = 0..it, w = V[it+1]  (one multi-dot, last CTA reduces)
 template <typename T>
-__global__ void __launch_bounds__(RED_THREADS)
-k_gm_mdot(DevState* s, const T* __restrict__ V, size_t ldv, size_t n, double* __restrict__ part, int ld) {
-    __shared__ double sh[RED_THREADS / 32];
+__device__ __forceinline__ void gm_mdot_block(DevState* s, const T* __restrict__ V, size_t ldv, size_t n,
+                                              double* __restrict__ part, int ld, int bid, int nblk) {
+    static_assert(MDOT_CHUNK <= RED_THREADS / 32, "one warp per dot of a chunk");
+    __shared__ double shc[MDOT_CHUNK][RED_THREADS / 32];
     const int it = s->it;
     const int m = it + 1;
     const T* w = V + (size_t)(it + 1) * ldv;
@@ -213,27 +234,41 @@ k_gm_mdot(DevState* s, const T* __restrict__ V, size_t ldv, size_t n, double* __
 #pragma unroll
         for (int c = 0; c < MDOT_CHUNK; ++c) acc[c] = 0.0;
         const int cnt = min(MDOT_CHUNK, m - q0);
-        for (size_t i = blockIdx.x * (size_t)RED_THREADS + threadIdx.x; i < n;
-             i += (size_t)gridDim.x * RED_THREADS) {
+        for (size_t i = bid * (size_t)RED_THREADS + threadIdx.x; i < n; i += (size_t)nblk * RED_THREADS) {
             const double wi = (double)w[i];
 #pragma unroll
             for (int c = 0; c < MDOT_CHUNK; ++c)
                 if (c < cnt) acc[c] += wi * (double)V[(size_t)(q0 + c) * ldv + i];
         }
+        // block sums of the chunk's dots: warp sums, one barrier, then warp c
+        // adds the warp sums of dot c (the order of block_sum)
+        const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
 #pragma unroll
         for (int c = 0; c < MDOT_CHUNK; ++c) {
             if (c < cnt) {
-                const double t = block_sum(acc[c], sh);
-                if (threadIdx.x == 0) part[(size_t)(q0 + c) * ld + blockIdx.x] = t;
+                const double t = warp_sum(acc[c]);
+                if (lane == 0) shc[c][wid] = t;
             }
         }
+        __syncthreads();
+        if (wid < cnt) {
+            double r = (lane < RED_THREADS / 32) ? shc[wid][lane] : 0.0;
+            r = warp_sum(r);
+            if (lane == 0) part[(size_t)(q0 + wid) * ld + bid] = r;
+        }
+        __syncthreads();
     }
-    if (!last_block(&s->cnt[1])) return;
+    if (!last_block(&s->cnt[1], nblk)) return;
     const int wid = threadIdx.x >> 5;
     for (int q = wid; q < m; q += RED_THREADS / 32) {
-        const double t = warp_reduce_parts(part + (size_t)q * ld, gridDim.x);
+        const double t = warp_reduce_parts(part + (size_t)q * ld, nblk);
         if ((threadIdx.x & 31) == 0) s->hcol[q] = t;
     }
+}
+template <typename T>
+__global__ void __launch_bounds__(RED_THREADS)
+k_gm_mdot(DevState* s, const T* __restrict__ V, size_t ldv, size_t n, double* __restrict__ part, int ld) {
+    gm_mdot_block<T>(s, V, ldv, n, part, ld, blockIdx.x, gridDim.x);
 }
 
 // Arnoldi bookkeeping after tt = ||w|| (KSPGMRESCycle + UpdateHessenberg)
@@ -284,8 +319,8 @@ VV_DEV void gm_arnoldi(DevState* s, double tt) {
 // w += sum_q (-hcol_q) V_q and ||w||^2 (classical Gram-Schmidt update,
 // VecMAXPY with lhh = -<w,v>); the last CTA finishes the Arnoldi step.
 template <typename T>
-__global__ void __launch_bounds__(RED_THREADS)
-k_gm_maxpy(DevState* s, T* __restrict__ V, size_t ldv, size_t n, double* __restrict__ part) {
+__device__ __forceinline__ void gm_maxpy_block(DevState* s, T* __restrict__ V, size_t ldv, size_t n,
+                                               double* __restrict__ part, int bid, int nblk) {
     __shared__ double sh[RED_THREADS / 32];
     __shared__ double cf[MAX_RESTART + 2];
     const int it = s->it;
@@ -294,83 +329,101 @@ k_gm_maxpy(DevState* s, T* __restrict__ V, size_t ldv, size_t n, double* __restr
     for (int q = threadIdx.x; q < m; q += RED_THREADS) cf[q] = -s->hcol[q];
     __syncthreads();
     double acc = 0.0;
-    for (size_t i = blockIdx.x * (size_t)RED_THREADS + threadIdx.x; i < n; i += (size_t)gridDim.x * RED_THREADS) {
+    for (size_t i = bid * (size_t)RED_THREADS + threadIdx.x; i < n; i += (size_t)nblk * RED_THREADS) {
         double wi = (double)w[i];
         for (int q = 0; q < m; ++q) wi += cf[q] * (double)V[(size_t)q * ldv + i];
         w[i] = (T)wi;
         acc += wi * wi;
     }
     const double t = block_sum(acc, sh);
-    if (threadIdx.x == 0) part[blockIdx.x] = t;
-    if (!last_block(&s->cnt[2])) return;
+    if (threadIdx.x == 0) part[bid] = t;
+    if (!last_block(&s->cnt[2], nblk)) return;
     if (threadIdx.x >= 32) return;
-    const double ss2 = warp_reduce_parts(part, gridDim.x);
+    const double ss2 = warp_reduce_parts(part, nblk);
     if (threadIdx.x == 0) gm_arnoldi(s, sqrt(ss2));
+}
+template <typename T>
+__global__ void __launch_bounds__(RED_THREADS)
+k_gm_maxpy(DevState* s, T* __restrict__ V, size_t ldv, size_t n, double* __restrict__ part) {
+    gm_maxpy_block<T>(s, V, ldv, n, part, blockIdx.x, gridDim.x);
 }
 
 // KSPGMRESBuildSoln: every CTA solves the small triangular system (thread 0,
 // into shared memory) and updates its share of x += sum nrs_q V_q; CTA 0
 // records the outcome and decides whether another cycle follows.
+// KSPGMRESBuildSoln's triangular solve (one thread): nrs[0..npad) from the
+// rotated Hessenberg and right-hand side; npad = 0 on breakdown or no step.
+VV_DEV void gm_backsolve(const DevState* s, double* nrs, int* npad_out, int* breakdown_out) {
+    const int last = s->it - 1;
+    const int ld = s->restart + 2;
+    const double* hh = s->hh;
+#define HH(a, b) hh[(b) * ld + (a)]
+    int npad = 0, breakdown = 0;
+    if (last >= 0) {
+        if (HH(last, last) == 0.0) {
+            breakdown = 1;
+        } else {
+            nrs[last] = s->grs[last] / HH(last, last);
+            for (int ii = 1; ii <= last && !breakdown; ++ii) {
+                const int k = last - ii;
+                double t = s->grs[k];
+                for (int j = k + 1; j <= last; ++j) t = t - HH(k, j) * nrs[j];
+                if (HH(k, k) == 0.0) breakdown = 1;
+                else nrs[k] = t / HH(k, k);
+            }
+            if (!breakdown) npad = last + 1;
+        }
+    }
+#undef HH
+    *npad_out = npad;
+    *breakdown_out = breakdown;
+}
+
+// outcome of a cycle after the solution update (one thread)
+VV_DEV void gm_finish_state(DevState* s, int npad, int breakdown) {
+    if (breakdown) s->reason = R_BREAKDOWN;
+    if (s->its >= s->max_it && s->reason == R_ITERATING) s->reason = R_ITS;
+    s->first = 0;
+    s->pad = npad;
+    set_cond(s->h_gm_outer, s->reason == R_ITERATING ? 1u : 0u);
+    set_cond(s->h_gm_first, 0u);
+}
+
 template <typename T>
-__global__ void __launch_bounds__(RED_THREADS)
-k_gm_finish(DevState* s, const T* __restrict__ V, size_t ldv, T* __restrict__ x, size_t n) {
+__device__ __forceinline__ void gm_finish_block(DevState* s, const T* __restrict__ V, size_t ldv, T* __restrict__ x,
+                                                size_t n, int bid, int nblk) {
     __shared__ double nrs[MAX_RESTART + 1];
     __shared__ int npad, breakdown;
-    if (threadIdx.x == 0) {
-        const int last = s->it - 1;
-        const int ld = s->restart + 2;
-        const double* hh = s->hh;
-#define HH(a, b) hh[(b) * ld + (a)]
-        npad = 0;
-        breakdown = 0;
-        if (last >= 0) {
-            if (HH(last, last) == 0.0) {
-                breakdown = 1;
-            } else {
-                nrs[last] = s->grs[last] / HH(last, last);
-                for (int ii = 1; ii <= last && !breakdown; ++ii) {
-                    const int k = last - ii;
-                    double t = s->grs[k];
-                    for (int j = k + 1; j <= last; ++j) t = t - HH(k, j) * nrs[j];
-                    if (HH(k, k) == 0.0) breakdown = 1;
-                    else nrs[k] = t / HH(k, k);
-                }
-                if (!breakdown) npad = last + 1;
-            }
-        }
-#undef HH
-    }
+    if (threadIdx.x == 0) gm_backsolve(s, nrs, &npad, &breakdown);
     __syncthreads();
     const int m = npad;
     if (m > 0) {
-        for (size_t i = blockIdx.x * (size_t)RED_THREADS + threadIdx.x; i < n;
-             i += (size_t)gridDim.x * RED_THREADS) {
+        for (size_t i = bid * (size_t)RED_THREADS + threadIdx.x; i < n; i += (size_t)nblk * RED_THREADS) {
             double xi = (double)x[i];
             for (int q = 0; q < m; ++q) xi += nrs[q] * (double)V[(size_t)q * ldv + i];
             x[i] = (T)xi;
         }
     }
-    if (blockIdx.x == 0 && threadIdx.x == 0) {
-        if (breakdown) s->reason = R_BREAKDOWN;
-        if (s->its >= s->max_it && s->reason == R_ITERATING) s->reason = R_ITS;
-        s->first = 0;
-        s->pad = m;
-        set_cond(s->h_gm_outer, s->reason == R_ITERATING ? 1u : 0u);
-        set_cond(s->h_gm_first, 0u);
-    }
+    if (bid == 0 && threadIdx.x == 0) gm_finish_state(s, m, breakdown);
+}
+template <typename T>
+__global__ void __launch_bounds__(RED_THREADS)
+k_gm_finish(DevState* s, const T* __restrict__ V, size_t ldv, T* __restrict__ x, size_t n) {
+    gm_finish_block<T>(s, V, ldv, x, n, blockIdx.x, gridDim.x);
 }
 
 // ----- Picard-loop kernels -------------------------------------------------
 // f -= delta unless the linear solve failed (SNES ksponly skips the update
 // when the KSP reason is negative); record the solve in the report.
 template <typename TF, typename TD>
-__global__ void k_pic_apply(DevState* s, const TF* __restrict__ delta, TD* __restrict__ f, size_t n) {
+__device__ __forceinline__ void pic_apply_block(DevState* s, const TF* __restrict__ delta, TD* __restrict__ f,
+                                                size_t n, int bid, int nblk) {
     const bool ok = s->reason >= 0;
     if (ok) {
-        for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
+        for (size_t i = bid * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)nblk * blockDim.x)
             f[i] = f[i] - (TD)delta[i];
     }
-    if (blockIdx.x == 0 && threadIdx.x == 0) {
+    if (bid == 0 && threadIdx.x == 0) {
         const int k = s->pic_i;
         if (k < MAX_PICARD_DEV) {
             s->gmres_its[k] = s->its;
@@ -380,11 +433,15 @@ __global__ void k_pic_apply(DevState* s, const TF* __restrict__ delta, TD* __res
         if (!ok) s->ksp_failures += 1;
     }
 }
+template <typename TF, typename TD>
+__global__ void k_pic_apply(DevState* s, const TF* __restrict__ delta, TD* __restrict__ f, size_t n) {
+    pic_apply_block<TF, TD>(s, delta, f, n, blockIdx.x, gridDim.x);
+}
 
 // Residual of the current iterate: ||R(f)|| from the bracket kernel's tile
 // partials plus ||Poisson residual|| (s->pnorm2), then the stop rules of
 // run_nonlinear_matrixfree_split_mp.py:158-163.  phase 0: the initial residual.
-__global__ void k_pic_residual(DevState* s, const double* __restrict__ part, int np, int phase) {
+__device__ __forceinline__ void pic_residual_warp(DevState* s, const double* __restrict__ part, int np, int phase) {
     if (threadIdx.x >= 32) return;
     const double f2 = warp_reduce_parts(part, np);
     if (threadIdx.x != 0) return;
@@ -421,6 +478,9 @@ __global__ void k_pic_residual(DevState* s, const double* __restrict__ part, int
     set_cond(s->h_pic, s->pic_active ? 1u : 0u);
     set_cond(s->h_revert, (unsigned)s->pic_revert);
 }
+__global__ void k_pic_residual(DevState* s, const double* __restrict__ part, int np, int phase) {
+    pic_residual_warp(s, part, np, phase);
+}
 
 // ---------------------------------------------------------------------------
 // moments: partial sums over v segments, then one CTA finishes moments,
@@ -429,12 +489,11 @@ __global__ void k_pic_residual(DevState* s, const double* __restrict__ part, int
 constexpr int MOM_TX = 32, MOM_TY = 8;
 
 template <typename T>
-__global__ void __launch_bounds__(MOM_TX * MOM_TY)
-k_moments_partial(const T* __restrict__ F, int nx, int nv, int seg, const double* __restrict__ v,
-                  double* __restrict__ part /* [S][3][nx] */) {
+__device__ __forceinline__ void moments_partial_block(const T* __restrict__ F, int nx, int nv, int seg,
+                                                      const double* __restrict__ v,
+                                                      double* __restrict__ part /* [S][3][nx] */, int bx, int s) {
     __shared__ double sh[3][MOM_TY][MOM_TX + 1];
-    const int i = blockIdx.x * MOM_TX + threadIdx.x;
-    const int s = blockIdx.y;
+    const int i = bx * MOM_TX + threadIdx.x;
     const int ja = s * seg, jb = min(nv, ja + seg);
     double a0 = 0.0, a1 = 0.0, a2 = 0.0;
     if (i < nx) {
@@ -456,6 +515,12 @@ k_moments_partial(const T* __restrict__ F, int nx, int nv, int seg, const double
         part[((size_t)s * 3 + threadIdx.y) * nx + i] = t;
     }
 }
+template <typename T>
+__global__ void __launch_bounds__(MOM_TX * MOM_TY)
+k_moments_partial(const T* __restrict__ F, int nx, int nv, int seg, const double* __restrict__ v,
+                  double* __restrict__ part /* [S][3][nx] */) {
+    moments_partial_block<T>(F, nx, nv, seg, v, part, blockIdx.x, blockIdx.y);
+}
 
 struct PoissonParams {
     int nx, M, logM, S;   // S = number of moment partials
@@ -469,11 +534,11 @@ constexpr int POIS_THREADS = 1024;
 // Single CTA.  Inputs: moment partials (or n directly when part == nullptr).
 // Outputs (each optional): n, u, e, a, phi, h1; scal[0] = ||Poisson residual||_2,
 // scal[1] = sum(phi).
-__global__ void __launch_bounds__(POIS_THREADS)
-k_moments_poisson(const double* __restrict__ part, const double* __restrict__ n_in,
-                  double* __restrict__ n, double* __restrict__ u, double* __restrict__ e,
-                  double* __restrict__ a, double* __restrict__ phi, double* __restrict__ h1,
-                  double* __restrict__ scal, PoissonParams p) {
+__device__ __forceinline__ void moments_poisson_cta(const double* __restrict__ part, const double* __restrict__ n_in,
+                                                    double* __restrict__ n, double* __restrict__ u,
+                                                    double* __restrict__ e, double* __restrict__ a,
+                                                    double* __restrict__ phi, double* __restrict__ h1,
+                                                    double* __restrict__ scal, const PoissonParams& p) {
     extern __shared__ double2 psm[];
     double2* buf = psm;                               // M complex
     double* nn = reinterpret_cast<double*>(psm + p.M);  // nx
@@ -576,6 +641,46 @@ k_moments_poisson(const double* __restrict__ part, const double* __restrict__ n_
         scal[0] = sqrt(r2);
         scal[1] = phisum_s;
     }
+}
+__global__ void __launch_bounds__(POIS_THREADS)
+k_moments_poisson(const double* __restrict__ part, const double* __restrict__ n_in,
+                  double* __restrict__ n, double* __restrict__ u, double* __restrict__ e,
+                  double* __restrict__ a, double* __restrict__ phi, double* __restrict__ h1,
+                  double* __restrict__ scal, PoissonParams p) {
+    moments_poisson_cta(part, n_in, n, u, e, a, phi, h1, scal, p);
+}
+
+// Poisson apply (one CTA): mode 0 rhs b = -(n - mean n) charge, 1 matvec
+// (CFD4 stencil), 2 function (matvec + (n - mean n) charge); optional
+// ||y||^2 -> sumsq (PETScPoissonSolver.pyx:58-74, PETScPoissonCFD4.pyx:64-101)
+__device__ __forceinline__ void poisson_apply_cta(const double* __restrict__ x, const double* __restrict__ n,
+                                                  double* __restrict__ y, int nx, double hx2_inv, double charge,
+                                                  int mode, double* __restrict__ sumsq) {
+    __shared__ double red[32];
+    __shared__ double nmean_s;
+    double t = 0.0;
+    if (mode != 1) {
+        for (int i = threadIdx.x; i < nx; i += blockDim.x) t += n[i];
+        t = block_sum(t, red);
+        if (threadIdx.x == 0) nmean_s = t / nx;
+        __syncthreads();
+    }
+    double r2 = 0.0;
+    for (int i = threadIdx.x; i < nx; i += blockDim.x) {
+        double r;
+        if (mode == 0) {
+            r = -(n[i] - nmean_s) * charge;
+        } else {
+            const int im2 = (i - 2 + 2 * nx) % nx, im1 = (i - 1 + nx) % nx;
+            const int ip1 = (i + 1) % nx, ip2 = (i + 2) % nx;
+            r = (5. * x[im2] - 32. * x[im1] + 54. * x[i] - 32. * x[ip1] + 5. * x[ip2]) * hx2_inv / 12.;
+            if (mode == 2) r = r + (n[i] - nmean_s) * charge;
+        }
+        if (y) y[i] = r;
+        r2 += r * r;
+    }
+    r2 = block_sum(r2, red);
+    if (threadIdx.x == 0 && sumsq) sumsq[0] = r2;
 }
 
 // ---------------------------------------------------------------------------
