@@ -1,26 +1,32 @@
-"""Benchmark: implicit time steps of the 1D1V Vlasov-Poisson midpoint scheme.
+"""Benchmark: batched mixed-precision implicit steps of a seeded parameter sweep
+against the plain FP64 step, on one B200.
 
-Workload (the single-instance FP64 configuration): nonlinear two-stream
-f0 = v^2 exp(-v^2/2)/sqrt(2 pi) (1 + 0.05 cos(0.5 x)), x in [0, 4 pi) with
-nx = 512, v in [-8, 8] with nv = 1024, dt = 0.05, Arakawa J4, FFT
-tensor-product kinetic preconditioner, GMRES(30) with ksp_rtol 1e-4,
-Picard tolerance 1e-10 (runspec defaults).  A "step" is one implicit time
-step (Picard loop with one GMRES solve per pass).  The metric is
-Gcell-steps/s = nx*nv*steps / seconds.
+Workload (the metric's configuration): 256 independent runs drawn from the
+seed 20261203 -- Landau, two-stream and bump-on-tail initial data, k ~ U[0.3,
+0.6], amplitude log-uniform in [1e-3, 0.5], nx in {64, 128, 256}, nv in
+{128, 256, 512, 1024}, v in [-10, 10], L = 2 pi / k, dt = 0.1, Arakawa J4,
+FFT tensor-product kinetic preconditioner, GMRES(30) with ksp_rtol 1e-4,
+Picard tolerance 1e-10 (about 17.5 M cells in all).  A "step" advances every
+instance by one implicit time step.  Gcell-steps/s = sum(nx nv) * steps / s.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
 
-value : device time of K steps (CUDA events on the solver's stream, L2
-        flushed between steps outside the timed intervals), state resident
-        in HBM.
-e2e   : the same steps through the public API with the distribution
-        function copied host->device (pinned) before and device->host after
-        every step.
+value       : batched + mixed precision -- every kernel launched once for the
+              instance table, lockstep Picard/GMRES loops with per-instance
+              masks, one CUDA graph per step; FP32 GMRES basis, Jacobian and
+              preconditioner, FP64 residual, Picard loop, moments, Poisson and
+              invariants.  Device time of K steps (CUDA events), state
+              resident in HBM (the working set is far larger than L2).
+plain_fp64  : the same instances in FP64, each advanced by its own vv_step
+              one after another -- how the reference runs a sweep.
+field_energy: after W+K steps, |E_mixed - E_fp64| / |E_fp64| per instance.
+e2e         : the batched mixed step through Batch.step with every
+              instance's f copied host->device (pinned) before and
+              device->host after each step.
 --impl reference : the CPU restatement of the reference algorithm (the C
-        port under oracle/, all host threads) on the same workload, a
-        bounded number of steps.
-Multi-GPU: independent replicas, one per rank (scaling "weak"); the time is
-the max over ranks.
+              port under oracle/, all host threads) on the same instances.
+Multi-GPU: independent replicas, one sweep per rank with its own seed
+(scaling "weak"); the time is the max over ranks.
 """
 from __future__ import annotations
 
@@ -31,7 +37,6 @@ import statistics
 import subprocess
 import sys
 import tempfile
-import threading
 import time
 
 import numpy as np
@@ -39,38 +44,11 @@ import numpy as np
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
-NX, NV = 512, 1024
-L = 4 * np.pi
-VMIN, VMAX = -8.0, 8.0
-HT = 0.05
-KSP_RTOL, SNES_ATOL = 1e-4, 1e-10
 METRIC = "Gcell-steps/s"
-WORKLOAD = "two-stream 512x1024 FP64, J4, dt=0.05, GMRES(30)+tensor_kinetic PC"
-JVP_BYTES_PER_CELL = 16      # read X, write Y (FP64); h regenerated from 1-D profiles
-
-
-def f0_twostream(x, v):
-    return v ** 2 * np.exp(-v ** 2 / 2.) / np.sqrt(2. * np.pi) * (1. + 0.05 * np.cos(0.5 * x))
-
-
-def config_dict():
-    return {"grid": {"nx": NX, "nv": NV, "L": L, "vmin": VMIN, "vmax": VMAX, "ht": HT, "nt": 1},
-            "solver": {"method": "matrixfree", "poisson_bracket": "ArakawaJ4", "preconditioner_type": "tensor",
-                       "preconditioner_scheme": "tensor_kinetic", "petsc_ksp_rtol": KSP_RTOL,
-                       "petsc_snes_atol": SNES_ATOL},
-            "initial_data": {"charge": -1.0}}
-
-
-def initial_field():
-    hx = L / NX
-    hv = (VMAX - VMIN) / (NV - 1)
-    x = np.arange(NX) * hx
-    v = VMIN + np.arange(NV) * hv
-    X, V = np.meshgrid(x, v, indexing="xy")
-    f = f0_twostream(X, V)
-    f[:2, :] = 0.
-    f[NV - 2:, :] = 0.
-    return np.ascontiguousarray(f)
+N_INSTANCES = 256
+WORKLOAD = ("sweep: 256 seeded instances (Landau/two-stream/bump-on-tail, nx 64-256, nv 128-1024), "
+            "J4, dt=0.1, GMRES(30)+tensor_kinetic, batched + mixed precision vs plain FP64")
+MDOT_IT = 4   # Arnoldi index of the roofline launch of the multi-dot
 
 
 def measured_peaks():
@@ -83,11 +61,11 @@ def measured_peaks():
 
 
 def profiled_traffic():
-    """DRAM bytes per JVP launch from the committed ncu summary (or None)."""
-    p = os.path.join(ROOT, "profiles", "jvp_traffic.json")
+    """DRAM bytes per whole-table multi-dot launch from the committed ncu summary (or None)."""
+    p = os.path.join(ROOT, "profiles", "batch_mdot_traffic.json")
     if os.path.exists(p):
         with open(p) as fh:
-            return json.load(fh).get("bytes_per_launch_full_size")
+            return json.load(fh).get("bytes_per_launch")
     return None
 
 
@@ -141,25 +119,41 @@ class ClockSampler:
                 "samples": len(sm)}
 
 
-def flush_l2(buf):
-    buf.add_(1.0)   # 256 MB write, larger than the 126 MB L2
+def specs_for(rank):
+    from vivlasov1d_b200 import workloads as W
+    return W.sweep_specs(N_INSTANCES, seed=W.SWEEP_SEED + rank)
+
+
+def time_steps(fn, k, stream):
+    import torch
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    out = [fn() for _ in range(k)]
+    e1.record(stream)
+    e1.synchronize()
+    return e0.elapsed_time(e1) / 1e3, out
 
 
 def run_gpu(args, rank, world):
     import torch
-    import ctypes as C
-    from vivlasov1d_b200.run import Run
-    from vivlasov1d_b200 import _lib
+    from vivlasov1d_b200 import workloads as W
+    from vivlasov1d_b200.batch import Batch
 
     dev = torch.device("cuda", int(os.environ.get("LOCAL_RANK", 0)))
     torch.cuda.set_device(dev)
-    f0 = torch.from_numpy(initial_field())
-    run = Run(config_dict(), f0=f0, device=dev)
-    ctx = run.ctx
     stream = torch.cuda.current_stream(dev)
-    flush = torch.zeros(32 * 1024 * 1024, dtype=torch.float64, device=dev)
+    specs = specs_for(rank)
+    cells = sum(s["nx"] * s["nv"] for s in specs)
+    mixed = W.sweep_runs(specs=specs, device=dev, precision="mixed")
+    plain = W.sweep_runs(specs=specs, device=dev, precision="fp64")
+    batch = Batch(mixed)
+    # ---- warm-up (both arms advance W steps from the same initial state) ----
     for _ in range(args.warmup):
-        run.step()
+        batch.step()
+        for r in plain:
+            r.step()
     torch.cuda.synchronize()
     if world > 1:
         import torch.distributed as dist
@@ -167,126 +161,124 @@ def run_gpu(args, rank, world):
     sampler = ClockSampler(dev.index) if rank == 0 else None
     if sampler:
         sampler.start()
-    # ---- value: resident state ----
-    launches0 = ctx.launch_count()
-    picard = gmres = 0
-    total_ms = 0.0
-    for _ in range(args.steps):
-        flush_l2(flush)
-        e0 = torch.cuda.Event(enable_timing=True)
-        e1 = torch.cuda.Event(enable_timing=True)
-        torch.cuda.synchronize()
-        e0.record(stream)
-        r = run.step()
-        e1.record(stream)
-        e1.synchronize()
-        total_ms += e0.elapsed_time(e1)
-        picard += r["picard_its"]
-        gmres += sum(r["gmres_its"])
-    launches = ctx.launch_count() - launches0
-    # dominant-kernel timing on the workload's own buffers (the last GMRES
-    # basis vector 0 and the solver's Hamiltonian), CUDA events on the
-    # solver's stream, 200 back-to-back launches in one graph
-    jvp_s = ctx.time_kernel(0, reps=200)
-    pc_s = ctx.time_kernel(2, reps=50)
-    # ---- e2e: host buffers through the public API ----
-    host = torch.empty((NV, NX), dtype=torch.float64).pin_memory()
-    host.copy_(run.fc.cpu())
-    e2e_ms = 0.0
-    for _ in range(args.steps):
-        flush_l2(flush)
-        e0 = torch.cuda.Event(enable_timing=True)
-        e1 = torch.cuda.Event(enable_timing=True)
-        torch.cuda.synchronize()
-        e0.record(stream)
-        run.fc.copy_(host, non_blocking=True)
-        run.calculate_moments()
-        run.step()
-        host.copy_(run.fc, non_blocking=True)
-        e1.record(stream)
-        e1.synchronize()
-        e2e_ms += e0.elapsed_time(e1)
+    # the state the timed steps start from (the e2e steps repeat them)
+    snapshot = [r.fc.clone() for r in mixed]
+    # ---- value: batched + mixed, resident state ----
+    batch.launch_count(reset=True)
+    t_value, reps = time_steps(batch.step, args.steps, stream)
+    launches = batch.launch_count()
     clocks = sampler.stop() if sampler else None
-    t_value = total_ms / 1e3
-    t_e2e = e2e_ms / 1e3
+    picard = sum(r["picard_its"] for rep in reps for r in rep) / (args.steps * len(specs))
+    gmres = sum(sum(r["gmres_its"]) for rep in reps for r in rep) / (args.steps * len(specs))
+    # ---- plain FP64, one instance after the other ----
+    t_plain, _ = time_steps(lambda: [r.step() for r in plain], args.steps, stream)
+    fe_m, fe_p = W.field_energies(mixed), W.field_energies(plain)
+    fe_rel = np.abs(fe_m - fe_p) / np.abs(fe_p)
+    # ---- roofline kernels on the whole table (between steps) ----
+    mdot_s = batch.time_kernel(0, it=MDOT_IT, reps=20)
+    pc_s = batch.time_kernel(1, it=MDOT_IT, reps=10)
+    jvp_s = batch.time_kernel(2, it=MDOT_IT, reps=20)
+    # ---- e2e: host buffers through the public API, the same K steps again ----
+    hosts = [torch.empty_like(r.fc, device="cpu").pin_memory() for r in mixed]
+    for h, snap, r in zip(hosts, snapshot, mixed):
+        h.copy_(snap)
+        r.fc.copy_(snap)
+        r.calculate_moments()
+    del snapshot
+
+    def e2e_step():
+        for h, r in zip(hosts, mixed):
+            r.fc.copy_(h, non_blocking=True)
+        out = batch.step()
+        for h, r in zip(hosts, mixed):
+            h.copy_(r.fc, non_blocking=True)
+        return out
+
+    t_e2e, _ = time_steps(e2e_step, args.steps, stream)
     if world > 1:
         import torch.distributed as dist
-        t = torch.tensor([t_value, t_e2e], dtype=torch.float64, device=dev)
+        t = torch.tensor([t_value, t_plain, t_e2e], dtype=torch.float64, device=dev)
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        t_value, t_e2e = float(t[0]), float(t[1])
-    inv = run.invariants()
-    return dict(t_value=t_value, t_e2e=t_e2e, picard=picard, gmres=gmres, launches=launches,
-                jvp_s=jvp_s, pc_s=pc_s, clocks=clocks, invariants=inv)
+        t_value, t_plain, t_e2e = (float(x) for x in t)
+    return dict(cells=cells, t_value=t_value, t_plain=t_plain, t_e2e=t_e2e, launches=launches, clocks=clocks,
+                picard=picard, gmres=gmres, fe_rel=fe_rel, mdot_s=mdot_s, pc_s=pc_s, jvp_s=jvp_s)
 
 
-def cpu_baseline_sample(seconds=20.0):
-    """Time the oracle port on the host, bounded to about `seconds`."""
-    try:
-        from oracle.c import CPort
-        port = CPort(NX, NV, L, VMIN, VMAX, HT, ksp_rtol=KSP_RTOL, snes_atol=SNES_ATOL)
-        port.set_f(initial_field())
-        t0 = time.perf_counter()
-        steps = 0
-        while True:
-            port.step()
-            steps += 1
-            if time.perf_counter() - t0 > seconds or steps >= 50:
-                break
-        dt = time.perf_counter() - t0
-        return {"value": NX * NV * steps / dt / 1e9, "unit": METRIC, "cores": port.threads,
-                "kind": "port", "sample": "%d steps of the workload from t=0 (C port, OpenMP)" % steps}
-    except ImportError:
-        pass
-    from oracle import vlasov_oracle as vo
-    g = vo.Grid(NX, NV, L, VMAX, VMIN, ht=HT)
-    f0 = vo.from_flat(initial_field()).copy()
+def port_runs(specs):
+    """C-port instances of the sweep (FP64, all host threads)."""
+    from oracle.c import CPort
+    from vivlasov1d_b200 import workloads as W
+    runs = []
+    for s in specs:
+        p = CPort(s["nx"], s["nv"], s["L"], -10.0, 10.0, 0.1, ksp_rtol=1e-4, snes_atol=1e-10)
+        hx, hv = s["L"] / s["nx"], 20.0 / (s["nv"] - 1)
+        x = np.arange(s["nx"]) * hx
+        v = -10.0 + np.arange(s["nv"]) * hv
+        X, V = np.meshgrid(x, v, indexing="xy")
+        f = W.FAMILIES[s["family"]](s["amp"], s["k"])(X, V)
+        f[:2, :] = 0.
+        f[s["nv"] - 2:, :] = 0.
+        p.set_f(f)
+        runs.append(p)
+    return runs
+
+
+def cpu_baseline_sample(specs, seconds=15.0):
+    """The C port on the host: whole sweep steps (every instance once) until
+    about `seconds` have passed, at least one."""
+    runs = port_runs(specs)
+    cells = sum(s["nx"] * s["nv"] for s in specs)
     t0 = time.perf_counter()
-    orun = vo.Run(g, f0, ksp_rtol=KSP_RTOL, snes_atol=SNES_ATOL)
     steps = 0
     while True:
-        orun.step()
+        for p in runs:
+            p.step()
         steps += 1
         if time.perf_counter() - t0 > seconds:
             break
     dt = time.perf_counter() - t0
-    return {"value": NX * NV * steps / dt / 1e9, "unit": METRIC, "cores": 1, "kind": "port",
-            "sample": "%d steps of the workload from t=0 (numpy oracle, incl. set-up)" % steps}
+    return {"value": cells * steps / dt / 1e9, "unit": METRIC, "cores": runs[0].threads, "kind": "port",
+            "sample": "%d step(s) of all %d sweep instances from t=0 (C port of the oracle, OpenMP)"
+                      % (steps, len(specs))}
 
 
 def reference_arm(steps, warmup, budget=240.0):
-    """W warm-up + K timed steps of the C port on all host threads; stops
-    early (and says so) if the timed steps would exceed `budget` seconds."""
-    from oracle.c import CPort
-    port = CPort(NX, NV, L, VMIN, VMAX, HT, ksp_rtol=KSP_RTOL, snes_atol=SNES_ATOL)
-    port.set_f(initial_field())
+    """W warm-up + K timed sweep steps of the C port on all host threads;
+    stops early (and says so) if the timed steps would exceed `budget` s."""
+    specs = specs_for(0)
+    runs = port_runs(specs)
+    cells = sum(s["nx"] * s["nv"] for s in specs)
     for _ in range(warmup):
-        port.step()
+        for p in runs:
+            p.step()
     t0 = time.perf_counter()
     done = 0
     for _ in range(steps):
-        port.step()
+        for p in runs:
+            p.step()
         done += 1
         if time.perf_counter() - t0 > budget:
             break
     dt = time.perf_counter() - t0
-    return {"value": NX * NV * done / dt / 1e9, "cores": port.threads, "kind": "port",
-            "sample": "%d timed steps after %d warm-up steps (C port of the oracle, OpenMP)" % (done, warmup)}
+    return {"value": cells * done / dt / 1e9, "cores": runs[0].threads, "kind": "port",
+            "sample": "%d timed sweep steps (all %d instances) after %d warm-up steps (C port of the oracle, "
+                      "OpenMP)" % (done, len(specs), warmup)}
 
 
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()
     rank = int(os.environ.get("RANK", 0))
     world = int(os.environ.get("WORLD_SIZE", 1))
-    config = {"workload": WORKLOAD, "nx": NX, "nv": NV, "dt": HT, "bracket": "arakawaj4",
-              "preconditioner": "tensor_kinetic", "ksp_rtol": KSP_RTOL, "snes_atol": SNES_ATOL,
-              "instances_per_gpu": 1, "parallelism": "replicas x%d" % args.gpus,
-              "l2": "flushed between timed steps (256 MB write)"}
+    config = {"workload": WORKLOAD, "instances": N_INSTANCES, "seed": 20261203, "precision": "mixed",
+              "mixed_inner_rtol": 1e-2, "ksp_rtol": 1e-4, "snes_atol": 1e-10, "dt": 0.1,
+              "bracket": "arakawaj4", "preconditioner": "tensor_kinetic", "parallelism": "replicas x%d" % args.gpus,
+              "l2": "working set far larger than L2 (17.5 M cells x ~40 fields); no flush"}
 
     if args.impl == "reference":
         if rank != 0:
@@ -295,7 +287,7 @@ def main():
         line = {"impl": "reference", "metric": METRIC, "value": cb["value"], "unit": METRIC,
                 "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
                 "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-                "data": "synthetic (analytic initial condition)", "config": config,
+                "data": "synthetic (seeded analytic initial data)", "config": config,
                 "cpu_baseline": {"value": cb["value"], "unit": METRIC, "cores": cb["cores"], "kind": cb["kind"],
                                  "sample": cb["sample"]},
                 "e2e": {"value": cb["value"], "unit": METRIC, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
@@ -315,29 +307,35 @@ def main():
         dist.destroy_process_group()
     if rank != 0:
         return
-    cells = NX * NV
+    cells = res["cells"]
     value = cells * args.steps * world / res["t_value"] / 1e9
+    plain = cells * args.steps * world / res["t_plain"] / 1e9
     e2e = cells * args.steps * world / res["t_e2e"] / 1e9
     peak, peak_kind = measured_peaks()
-    avg_s = res["jvp_s"]
-    achieved = JVP_BYTES_PER_CELL * cells / avg_s / 1e9
-    roofline = {"kernel": "k_bracket_wide<4,JVP> (Jacobian-vector product stencil)", "bound": "hbm",
-                "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                "peak_kind": peak_kind, "traffic": profiled_traffic(),
-                "algorithmic_bytes_per_launch": JVP_BYTES_PER_CELL * cells,
-                "avg_launch_us": avg_s * 1e6,
-                "note": "4 MiB operands are L2-resident at this size; see DESIGN.md for the HBM-resident figure",
-                "pc_apply_us": res["pc_s"] * 1e6}
+    mdot_bytes = cells * (MDOT_IT + 2) * 4      # w and V_0..V_it read in FP32
+    achieved = mdot_bytes / res["mdot_s"] / 1e9
+    roofline = {"kernel": "k_b_gm_mdot_p<float> (Gram-Schmidt multi-dot, whole table, Arnoldi index %d)" % MDOT_IT,
+                "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                "peak_kind": peak_kind, "traffic": profiled_traffic(), "algorithmic_bytes_per_launch": mdot_bytes,
+                "avg_launch_us": res["mdot_s"] * 1e6,
+                "others": {"preconditioner_3_kernels_us": res["pc_s"] * 1e6,
+                           "preconditioner_achieved_GBps": cells * 24 / res["pc_s"] / 1e9,
+                           "jacobian_stencil_us": res["jvp_s"] * 1e6,
+                           "jacobian_achieved_GBps": cells * 8 / res["jvp_s"] / 1e9}}
+    fe = res["fe_rel"]
     line = {"metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": res["t_value"] * 1e3 / args.steps, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-            "data": "synthetic (analytic two-stream initial condition)", "config": config,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32 inner / f64 outer (mixed)",
+            "data": "synthetic (seeded analytic initial data)", "config": config,
+            "plain_fp64": {"value": plain, "unit": METRIC, "ms_per_step": res["t_plain"] * 1e3 / args.steps,
+                           "ratio_batched_mixed": value / plain},
+            "field_energy_rel_err": {"max": float(fe.max()), "median": float(np.median(fe)),
+                                     "vs": "plain FP64 GPU step (pinned to the oracle by the tests)"},
             "e2e": {"value": e2e, "unit": METRIC, "h2d_bytes_per_step": cells * 8, "d2h_bytes_per_step": cells * 8},
             "gpu_launches": res["launches"], "roofline": roofline, "clocks": res["clocks"],
-            "iterations": {"picard_per_step": res["picard"] / args.steps, "gmres_per_step": res["gmres"] / args.steps},
-            "field_energy_end": res["invariants"]["field_energy"]}
+            "iterations": {"picard_per_step_mean": res["picard"], "gmres_per_step_mean": res["gmres"]}}
     if not args.no_cpu_baseline:
-        line["cpu_baseline"] = cpu_baseline_sample(seconds=20.0)
+        line["cpu_baseline"] = cpu_baseline_sample(specs_for(0), seconds=15.0)
     print(json.dumps(line))
 
 

@@ -86,6 +86,15 @@ typedef struct vv_grid {
     int32_t order;           /* enum vv_order                                 */
     int32_t gmres_restart;   /* restart length (PETSc default 30), <= 64      */
     int32_t precision;       /* enum vv_precision                             */
+    double  mixed_rtol;      /* VV_PRECISION_MIXED only: relative tolerance of
+                                the FP32 linear solves inside vv_step and the
+                                batch step (<= 0: 1e-2; never below the KSP
+                                rtol).  The FP64 Picard residual refines the
+                                solution to the same fixed point, as in
+                                mixed-precision iterative refinement; FP32
+                                Krylov vectors cannot reduce a residual near
+                                the FP64 round-off floor by 1e-4 cheaply.
+                                vv_gmres always uses the rtol it is given.    */
 } vv_grid;
 
 typedef struct vv_ctx vv_ctx;
@@ -242,6 +251,14 @@ int vv_batch_step(vv_batch* batch, const vv_snes_opts* snes, const vv_ksp_opts* 
                   vv_step_report* reports, int* statuses);
 /* Number of kernels the batch has launched (graph nodes executed included). */
 int vv_batch_launch_count(vv_batch* batch, int64_t* launches, int reset);
+/* Device time of one whole-table launch of a batch kernel with every instance
+ * active: `reps` launches are captured in a CUDA graph and timed with CUDA
+ * events.  which: 0 Gram-Schmidt multi-dot (w and V_0..V_it read), 1
+ * preconditioner (its three kernels), 2 Jacobian-vector-product stencil,
+ * 3 Gram-Schmidt multi-axpy (w updated).  it: the Arnoldi index set in every
+ * instance first (it + 1 <= each context's restart).  Between steps only:
+ * the GMRES scratch of every instance is overwritten. */
+int vv_batch_time_kernel(vv_batch* batch, int which, int it, int reps, double* avg_ms);
 
 /* ---- invariants (vlasov/core/distribution_function.pyx:130-306,
  *      hamiltonian.pyx:67-124, potential.pyx:48-59) ---------------------- */

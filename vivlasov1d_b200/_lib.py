@@ -33,7 +33,8 @@ class vv_grid(C.Structure):
     _fields_ = [("nx", C.c_int32), ("nv", C.c_int32), ("L", C.c_double), ("vmin", C.c_double),
                 ("vmax", C.c_double), ("ht", C.c_double), ("charge", C.c_double), ("mass", C.c_double),
                 ("bracket", C.c_int32), ("preconditioner", C.c_int32), ("laplace", C.c_int32),
-                ("order", C.c_int32), ("gmres_restart", C.c_int32), ("precision", C.c_int32)]
+                ("order", C.c_int32), ("gmres_restart", C.c_int32), ("precision", C.c_int32),
+                ("mixed_rtol", C.c_double)]
 
 
 class vv_ksp_opts(C.Structure):
@@ -113,6 +114,7 @@ SIGNATURES = {
     "vv_batch_step": (I, [P, C.POINTER(vv_snes_opts), C.POINTER(vv_ksp_opts), C.POINTER(vv_step_report),
                           C.POINTER(C.c_int)]),
     "vv_batch_launch_count": (I, [P, C.POINTER(C.c_int64), I]),
+    "vv_batch_time_kernel": (I, [P, I, I, I, C.POINTER(D)]),
 }
 
 

@@ -55,6 +55,14 @@ class Batch:
         _lib.check(self.lib.vv_batch_launch_count(self.h, C.byref(n), int(bool(reset))), "vv_batch_launch_count")
         return n.value
 
+    def time_kernel(self, which, it=4, reps=20):
+        """Seconds per whole-table launch of one batch kernel (0 multi-dot,
+        1 preconditioner, 2 Jacobian stencil, 3 multi-axpy); between steps."""
+        ms = C.c_double()
+        _lib.check(self.lib.vv_batch_time_kernel(self.h, int(which), int(it), int(reps), C.byref(ms)),
+                   "vv_batch_time_kernel")
+        return ms.value / 1e3
+
     def step(self):
         """Advance every instance by one time step; returns per-instance reports."""
         s = torch.cuda.current_stream().cuda_stream

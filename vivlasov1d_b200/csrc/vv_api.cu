@@ -375,8 +375,10 @@ int raise_smem_limits(int* limit_out) {
         smem_set((const void*)vv::k_b_rfft<float, float>, optin, lowest, e);
         smem_set((const void*)vv::k_b_irfft<double, double>, optin, lowest, e);
         smem_set((const void*)vv::k_b_irfft<float, float>, optin, lowest, e);
-        smem_set((const void*)vv::k_b_tridiag<double>, optin, lowest, e);
-        smem_set((const void*)vv::k_b_tridiag<float>, optin, lowest, e);
+        smem_set((const void*)vv::k_b_tridiag<double, true>, optin, lowest, e);
+        smem_set((const void*)vv::k_b_tridiag<float, true>, optin, lowest, e);
+        smem_set((const void*)vv::k_b_tridiag<double, false>, optin, lowest, e);
+        smem_set((const void*)vv::k_b_tridiag<float, false>, optin, lowest, e);
         if (e != cudaSuccess) return fail_cuda(e, "cudaFuncSetAttribute (dynamic shared memory)");
         limit_of[dev] = lowest;
     }
@@ -545,6 +547,7 @@ int upload_options(vv_ctx* c, const vv_ksp_opts* o, const vv_snes_opts* so) {
     h->restart = (o->restart > 0) ? o->restart : c->restart;
     h->max_it = o->max_it;
     h->rtol = o->rtol;
+    if (so && c->mixed) h->rtol = std::max(o->rtol, c->g.mixed_rtol > 0.0 ? c->g.mixed_rtol : 1e-2);
     h->atol = o->atol;
     h->dtol = (o->dtol > 0.0) ? o->dtol : 1e5;
     h->haptol = 1e-30;
@@ -1586,13 +1589,15 @@ struct vv_batch {
     bool mixed;
     int scheme;
     int R;                       // FFT rows per CTA
-    int tri_warp;                // tridiagonal solves: 1 one warp per mode, 0 one CTA per mode
+    int tri_kind;                // tridiagonal solves: 0 CTA per mode (tables staged), 1 warp per mode,
+                                 // 2 CTA per mode (tables through L1)
+    size_t smem_tri_stage, smem_tri_plain;
     double* wpart;               // device: per-warp partial sums of every instance
     vv::BInst* tab;              // device instance table
     int* lists;                  // device work lists (vv::NLIST of them)
     size_t list_words;
     int tot[vv::NFAM];           // work items per family over all instances
-    size_t smem_rfft, smem_irfft, smem_tri, smem_pois;
+    size_t smem_rfft, smem_irfft, smem_pois;
     unsigned int* counts;        // device: passes per control op
     int* flag;                   // device: last control result
     int* hflag;                  // pinned
@@ -1658,8 +1663,9 @@ int b_pc(vv_batch* b, int l, bool from_tmp64, int dst) {
     const dim3 rt(32 * b->R);
     if (from_tmp64) TRY(blaunch(b, vv::k_b_rfft<double, T>, vv::F_ROWS, rt, b->smem_rfft, tab, L, b->n, 1));
     else TRY(blaunch(b, vv::k_b_rfft<T, T>, vv::F_ROWS, rt, b->smem_rfft, tab, L, b->n, 0));
-    if (b->tri_warp) TRY(blaunch(b, vv::k_b_tridiag_w<T>, vv::F_MODES, 32 * vv::TRIW_WARPS, 0, tab, L, b->n));
-    else TRY(blaunch(b, vv::k_b_tridiag<T>, vv::F_MODES, vv::TRI_THREADS, b->smem_tri, tab, L, b->n));
+    if (b->tri_kind == 1) TRY(blaunch(b, vv::k_b_tridiag_w<T>, vv::F_MODES, 32 * vv::TRIW_WARPS, 0, tab, L, b->n));
+    else if (b->tri_kind == 2) TRY(blaunch(b, vv::k_b_tridiag<T, false>, vv::F_MODES, vv::TRI_THREADS, b->smem_tri_plain, tab, L, b->n));
+    else TRY(blaunch(b, vv::k_b_tridiag<T, true>, vv::F_MODES, vv::TRI_THREADS, b->smem_tri_stage, tab, L, b->n));
     return blaunch(b, vv::k_b_irfft<T, T>, vv::F_ROWS, rt, b->smem_irfft, tab, L, b->n, dst);
 }
 
@@ -1864,9 +1870,10 @@ int b_dispatch_host(vv_batch* b) {
 
 // Launch shape of the preconditioner kernels: rows per CTA of the x-FFTs and
 // the tridiagonal variant (work items per instance and shared memory).
-void b_shape(vv_batch* b, std::vector<vv::BInst>& tab, int R, int tri_warp) {
+void b_shape(vv_batch* b, std::vector<vv::BInst>& tab, int R, int tri_kind) {
     b->R = R;
-    b->tri_warp = tri_warp;
+    b->tri_kind = tri_kind;
+    const bool tri_warp = tri_kind == 1;
     const size_t csz = b->mixed ? sizeof(float2) : sizeof(double2);
     for (int f = 0; f < vv::NFAM; ++f) b->tot[f] = 0;
     b->smem_rfft = b->smem_irfft = 0;
@@ -1902,8 +1909,8 @@ int b_autotune(vv_batch* b, std::vector<vv::BInst>& tab) {
     CK(cudaEventCreate(&e0));
     CK(cudaEventCreate(&e1));
     float best = 1e30f;
-    int bR = b->R, bW = b->tri_warp, r = VV_OK;
-    for (int tw = 0; tw <= 1 && r == VV_OK; ++tw) {
+    int bR = b->R, bW = b->tri_kind, r = VV_OK;
+    for (int tw = 0; tw <= 2 && r == VV_OK; ++tw) {
         for (int R = 2; R <= 8 && r == VV_OK; R *= 2) {
             b_shape(b, tab, R, tw);
             if ((r = b_apply_shape(b, tab)) != VV_OK) break;
@@ -2036,7 +2043,8 @@ int vv_batch_create(int n, vv_ctx* const* ctxs, const vv_state* states, vv_batch
         {
             const int ch = (c->nv + vv::TRI_THREADS - 1) / vv::TRI_THREADS;
             const size_t np = (size_t)c->nv + (c->nv + ch - 1) / ch;
-            b->smem_tri = std::max(b->smem_tri, np * (b->mixed ? 24 : 48));
+            b->smem_tri_stage = std::max(b->smem_tri_stage, np * (b->mixed ? 24 : 48));
+            b->smem_tri_plain = std::max(b->smem_tri_plain, np * (b->mixed ? sizeof(float2) : sizeof(double2)));
         }
         b->smem_pois = std::max(b->smem_pois, c->smem_pois);
     }
@@ -2045,7 +2053,7 @@ int vv_batch_create(int n, vv_ctx* const* ctxs, const vv_state* states, vv_batch
         int limit = 0;
         int r = raise_smem_limits(&limit);
         if (r != VV_OK) return fail_b(r);
-        if (std::max({b->smem_rfft, b->smem_irfft, b->smem_tri, b->smem_pois}) > (size_t)limit)
+        if (std::max({b->smem_rfft, b->smem_irfft, b->smem_tri_stage, b->smem_pois}) > (size_t)limit)
             return fail_b(VV_ERR_UNSUPPORTED);
     }
     // per-warp partials: (restart + 2) columns of 8 vblk per instance
@@ -2171,6 +2179,70 @@ int vv_batch_step(vv_batch* b, const vv_snes_opts* so, const vv_ksp_opts* ko, vv
         if (s != VV_OK && first_bad == VV_OK) first_bad = s;
     }
     return first_bad;
+}
+
+int vv_batch_time_kernel(vv_batch* b, int which, int it, int reps, double* avg_ms) {
+    if (!b || !avg_ms || reps < 1 || which < 0 || which > 3 || it < 0) return VV_ERR_ARG;
+    for (int i = 0; i < b->n; ++i)
+        if (it + 1 >= b->ctx[i]->restart + 1) return VV_ERR_ARG;   // V[it+1] must exist
+    const int64_t l0 = b->launches;
+    b->st = b->cs[0];
+    vv::k_b_set_it<<<1, 256, 0, b->st>>>(b->tab, b->n, it);
+    CK(cudaGetLastError());
+    const vv::BInst* tab = b->tab;
+    const int* L = blist(b, vv::L_ALL);
+    auto one = [&]() -> int {
+        switch (which) {
+            case 0:
+                return b->mixed ? blaunch(b, vv::k_b_gm_mdot_p<float>, vv::F_VEC, vv::RED_THREADS, 0, tab, L, b->n)
+                                : blaunch(b, vv::k_b_gm_mdot_p<double>, vv::F_VEC, vv::RED_THREADS, 0, tab, L, b->n);
+            case 1: return b->mixed ? b_pc<float>(b, vv::L_ALL, false, vv::BD_B) : b_pc<double>(b, vv::L_ALL, false, vv::BD_B);
+            case 2:
+                switch (b->scheme) {
+                    case VV_BRACKET_J1:
+                        return b->mixed ? blaunch(b, vv::k_b_bracket<1, vv::BS_X, float>, vv::F_TILE, vv::WTHREADS, 0, tab, L, b->n)
+                                        : blaunch(b, vv::k_b_bracket<1, vv::BS_X, double>, vv::F_TILE, vv::WTHREADS, 0, tab, L, b->n);
+                    case VV_BRACKET_J2:
+                        return b->mixed ? blaunch(b, vv::k_b_bracket<2, vv::BS_X, float>, vv::F_TILE, vv::WTHREADS, 0, tab, L, b->n)
+                                        : blaunch(b, vv::k_b_bracket<2, vv::BS_X, double>, vv::F_TILE, vv::WTHREADS, 0, tab, L, b->n);
+                    default:
+                        return b->mixed ? blaunch(b, vv::k_b_bracket<4, vv::BS_X, float>, vv::F_TILE, vv::WTHREADS, 0, tab, L, b->n)
+                                        : blaunch(b, vv::k_b_bracket<4, vv::BS_X, double>, vv::F_TILE, vv::WTHREADS, 0, tab, L, b->n);
+                }
+            default:
+                return b->mixed ? blaunch(b, vv::k_b_gm_maxpy_p<float>, vv::F_VEC, vv::RED_THREADS, 0, tab, L, b->n)
+                                : blaunch(b, vv::k_b_gm_maxpy_p<double>, vv::F_VEC, vv::RED_THREADS, 0, tab, L, b->n);
+        }
+    };
+    cudaGraph_t g = nullptr;
+    cudaGraphExec_t ex = nullptr;
+    CK(cudaStreamBeginCapture(b->st, cudaStreamCaptureModeRelaxed));
+    int r = VV_OK;
+    for (int k = 0; k < reps && r == VV_OK; ++k) r = one();
+    cudaError_t e = cudaStreamEndCapture(b->st, &g);
+    if (r == VV_OK && e != cudaSuccess) r = fail_cuda(e, "vv_batch_time_kernel capture");
+    if (r == VV_OK && (e = cudaGraphInstantiate(&ex, g, 0)) != cudaSuccess) r = fail_cuda(e, "vv_batch_time_kernel instantiate");
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    float ms = 0.f;
+    if (r == VV_OK) {
+        cudaEventCreate(&e0);
+        cudaEventCreate(&e1);
+        e = cudaGraphLaunch(ex, b->st);   // warm-up
+        if (e == cudaSuccess) e = cudaEventRecord(e0, b->st);
+        if (e == cudaSuccess) e = cudaGraphLaunch(ex, b->st);
+        if (e == cudaSuccess) e = cudaEventRecord(e1, b->st);
+        if (e == cudaSuccess) e = cudaEventSynchronize(e1);
+        if (e == cudaSuccess) e = cudaEventElapsedTime(&ms, e0, e1);
+        if (e != cudaSuccess) r = fail_cuda(e, "vv_batch_time_kernel");
+    }
+    if (e0) cudaEventDestroy(e0);
+    if (e1) cudaEventDestroy(e1);
+    if (ex) cudaGraphExecDestroy(ex);
+    if (g) cudaGraphDestroy(g);
+    b->launches = l0;
+    TRY(r);
+    *avg_ms = (double)ms / reps;
+    return VV_OK;
 }
 
 int vv_batch_launch_count(vv_batch* b, int64_t* launches, int reset) {

@@ -115,12 +115,13 @@ __global__ void k_b_rfft(const BInst* __restrict__ tab, const int* __restrict__ 
     });
 }
 
-// tridiagonal solves: one CTA per mode, or one warp per mode (an item is
-// TRIW_WARPS modes); the batch autotuner picks the variant
-template <typename R>
+// tridiagonal solves: one CTA per mode (tables staged in shared memory or
+// read through L1), or one warp per mode (an item is TRIW_WARPS modes); the
+// batch autotuner picks the variant
+template <typename R, bool STAGE>
 __global__ void __launch_bounds__(TRI_THREADS) k_b_tridiag(const BInst* __restrict__ tab, const int* __restrict__ L, int n) {
     for_work<F_MODES>(tab, L, n, [&](const BInst& I, int local) {
-        tridiag_mode<R, true>((typename Cplx<R>::type*)I.specT, I.tp, local);
+        tridiag_mode<R, STAGE>((typename Cplx<R>::type*)I.specT, I.tp, local);
     });
 }
 
@@ -227,11 +228,32 @@ __global__ void k_b_revert(const BInst* __restrict__ tab, const int* __restrict_
 
 // ---- GMRES ------------------------------------------------------------------
 // The batch reductions work on warp items: block item `bid` of an instance is
-// eight warp items wi = 8 bid + warp, and warp item wi covers the cells
-// i = 32 wi + lane + 32 nwi s (nwi = 8 vblk warp items, s = 0, 1, ...).  Each
-// warp writes its own partial sum (no barrier, no atomic); a one-block
-// finalize kernel per instance reduces them in a fixed order.
+// eight warp items wi = 8 bid + warp, and warp item wi covers the contiguous
+// cells [256 (wi + nwi s), 256 (wi + nwi s) + 256) (nwi = 8 vblk warp items,
+// s = 0, 1, ...), read with 16-byte vector loads: lane l holds vectors
+// l + 32 t, t < WV.  Each warp writes its own partial sum (no barrier, no
+// atomic); a one-block finalize kernel per instance reduces them in a fixed
+// order.
 VV_DEV int wi_count(const BInst& I) { return 8 * I.vblk; }
+
+constexpr int WCELLS = 256;   // cells of a warp item
+template <typename T> struct Vec16;
+template <> struct Vec16<float> { using type = float4; static constexpr int n = 4; };
+template <> struct Vec16<double> { using type = double2; static constexpr int n = 2; };
+template <typename T> VV_DEV constexpr int vec_n() { return Vec16<T>::n; }
+// elements of a 16-byte vector as double
+VV_DEV void vload(const float* p, double (&o)[4]) {
+    const float4 v = *reinterpret_cast<const float4*>(p);
+    o[0] = v.x; o[1] = v.y; o[2] = v.z; o[3] = v.w;
+}
+VV_DEV void vload(const double* p, double (&o)[2]) {
+    const double2 v = *reinterpret_cast<const double2*>(p);
+    o[0] = v.x; o[1] = v.y;
+}
+VV_DEV void vstore(float* p, const double (&o)[4]) {
+    *reinterpret_cast<float4*>(p) = make_float4((float)o[0], (float)o[1], (float)o[2], (float)o[3]);
+}
+VV_DEV void vstore(double* p, const double (&o)[2]) { *reinterpret_cast<double2*>(p) = make_double2(o[0], o[1]); }
 
 // cycle head: V0 = b (first cycle) or b - P^-1 J x (restart, P^-1 J x in V0)
 template <typename T>
@@ -248,13 +270,22 @@ __global__ void k_b_gm_head(const BInst* __restrict__ tab, const int* __restrict
 // ||V0||^2 per warp item
 template <typename T>
 __global__ void __launch_bounds__(RED_THREADS) k_b_gm_cycle_p(const BInst* __restrict__ tab, const int* __restrict__ L, int n) {
+    constexpr int VN = vec_n<T>(), WV = WCELLS / (32 * VN);
     for_work<F_VEC>(tab, L, n, [&](const BInst& I, int bid) {
         const int lane = threadIdx.x & 31, nwi = wi_count(I), wi = bid * 8 + (threadIdx.x >> 5);
         const T* V0 = (const T*)I.V;
         double acc = 0.0;
-        for (size_t i = (size_t)wi * 32 + lane; i < I.ncell; i += (size_t)nwi * 32) {
-            const double v = (double)V0[i];
-            acc += v * v;
+        for (size_t base = (size_t)wi * WCELLS; base < I.ncell; base += (size_t)nwi * WCELLS) {
+#pragma unroll
+            for (int t = 0; t < WV; ++t) {
+                const size_t i = base + (size_t)(lane + 32 * t) * VN;
+                if (i < I.ncell) {
+                    double v[VN];
+                    vload(V0 + i, v);
+#pragma unroll
+                    for (int e = 0; e < VN; ++e) acc += v[e] * v[e];
+                }
+            }
         }
         acc = warp_sum(acc);
         if (lane == 0) I.wpart[wi] = acc;
@@ -279,7 +310,8 @@ __global__ void k_b_gm_scale(const BInst* __restrict__ tab, const int* __restric
 
 // <w, V_q>, q = 0..it, w = V[it+1], per warp item (column q of the partials)
 template <typename T>
-__global__ void __launch_bounds__(RED_THREADS) k_b_gm_mdot_p(const BInst* __restrict__ tab, const int* __restrict__ L, int n) {
+__global__ void __launch_bounds__(RED_THREADS, 4) k_b_gm_mdot_p(const BInst* __restrict__ tab, const int* __restrict__ L, int n) {
+    constexpr int VN = vec_n<T>(), WV = WCELLS / (32 * VN);
     for_work<F_VEC>(tab, L, n, [&](const BInst& I, int bid) {
         const int lane = threadIdx.x & 31, nwi = wi_count(I), wi = bid * 8 + (threadIdx.x >> 5);
         const int it = I.ds->it, m = it + 1;
@@ -291,11 +323,30 @@ __global__ void __launch_bounds__(RED_THREADS) k_b_gm_mdot_p(const BInst* __rest
 #pragma unroll
             for (int c = 0; c < MDOT_CHUNK; ++c) acc[c] = 0.0;
             const int cnt = min(MDOT_CHUNK, m - q0);
-            for (size_t i = (size_t)wi * 32 + lane; i < nc; i += (size_t)nwi * 32) {
-                const double wv = (double)w[i];
+            for (size_t base = (size_t)wi * WCELLS; base < nc; base += (size_t)nwi * WCELLS) {
+                double wv[WV][VN];
 #pragma unroll
-                for (int c = 0; c < MDOT_CHUNK; ++c)
-                    if (c < cnt) acc[c] += wv * (double)V[(size_t)(q0 + c) * nc + i];
+                for (int t = 0; t < WV; ++t) {
+                    const size_t i = base + (size_t)(lane + 32 * t) * VN;
+                    if (i < nc) vload(w + i, wv[t]);
+                    else for (int e = 0; e < VN; ++e) wv[t][e] = 0.0;
+                }
+#pragma unroll
+                for (int c = 0; c < MDOT_CHUNK; ++c) {
+                    if (c < cnt) {
+                        const T* vq = V + (size_t)(q0 + c) * nc;
+#pragma unroll
+                        for (int t = 0; t < WV; ++t) {
+                            const size_t i = base + (size_t)(lane + 32 * t) * VN;
+                            if (i < nc) {
+                                double v[VN];
+                                vload(vq + i, v);
+#pragma unroll
+                                for (int e = 0; e < VN; ++e) acc[c] += wv[t][e] * v[e];
+                            }
+                        }
+                    }
+                }
             }
 #pragma unroll
             for (int c = 0; c < MDOT_CHUNK; ++c) {
@@ -322,7 +373,8 @@ __global__ void __launch_bounds__(RED_THREADS) k_b_gm_mdot_f(const BInst* __rest
 
 // w += sum_q (-hcol_q) V_q and ||w||^2 per warp item
 template <typename T>
-__global__ void __launch_bounds__(RED_THREADS) k_b_gm_maxpy_p(const BInst* __restrict__ tab, const int* __restrict__ L, int n) {
+__global__ void __launch_bounds__(RED_THREADS, 4) k_b_gm_maxpy_p(const BInst* __restrict__ tab, const int* __restrict__ L, int n) {
+    constexpr int VN = vec_n<T>(), WV = WCELLS / (32 * VN);
     __shared__ double cf[MAX_RESTART + 2];
     for_work<F_VEC>(tab, L, n, [&](const BInst& I, int bid) {
         const DevState* s = I.ds;
@@ -334,11 +386,36 @@ __global__ void __launch_bounds__(RED_THREADS) k_b_gm_maxpy_p(const BInst* __res
         T* V = (T*)I.V;
         T* w = V + (size_t)m * nc;
         double acc = 0.0;
-        for (size_t i = (size_t)wi * 32 + lane; i < nc; i += (size_t)nwi * 32) {
-            double wv = (double)w[i];
-            for (int q = 0; q < m; ++q) wv += cf[q] * (double)V[(size_t)q * nc + i];
-            w[i] = (T)wv;
-            acc += wv * wv;
+        for (size_t base = (size_t)wi * WCELLS; base < nc; base += (size_t)nwi * WCELLS) {
+            double wv[WV][VN];
+#pragma unroll
+            for (int t = 0; t < WV; ++t) {
+                const size_t i = base + (size_t)(lane + 32 * t) * VN;
+                if (i < nc) vload(w + i, wv[t]);
+            }
+            for (int q = 0; q < m; ++q) {
+                const T* vq = V + (size_t)q * nc;
+                const double c = cf[q];
+#pragma unroll
+                for (int t = 0; t < WV; ++t) {
+                    const size_t i = base + (size_t)(lane + 32 * t) * VN;
+                    if (i < nc) {
+                        double v[VN];
+                        vload(vq + i, v);
+#pragma unroll
+                        for (int e = 0; e < VN; ++e) wv[t][e] += c * v[e];
+                    }
+                }
+            }
+#pragma unroll
+            for (int t = 0; t < WV; ++t) {
+                const size_t i = base + (size_t)(lane + 32 * t) * VN;
+                if (i < nc) {
+                    vstore(w + i, wv[t]);
+#pragma unroll
+                    for (int e = 0; e < VN; ++e) acc += wv[t][e] * wv[t][e];
+                }
+            }
         }
         acc = warp_sum(acc);
         if (lane == 0) I.wpart[wi] = acc;
@@ -503,6 +580,11 @@ k_b_ctrl(const BInst* __restrict__ tab, int n, int op, unsigned long long handle
         if (flag) *flag = any;
         if (any && counts) counts[op] += 1u;
     }
+}
+
+// set the Arnoldi index of every instance (kernel timing)
+__global__ void k_b_set_it(const BInst* __restrict__ tab, int n, int it) {
+    for (int q = threadIdx.x; q < n; q += blockDim.x) tab[q].ds->it = it;
 }
 
 // copy the first `words` 32-bit words of every instance's state into out[n][words]

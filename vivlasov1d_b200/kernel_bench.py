@@ -1,6 +1,7 @@
 """Per-kernel timing at a chosen grid size (CUDA events on the launching stream).
 
     python -m vivlasov1d_b200.kernel_bench --nx 4096 --nv 8192 [--reps 20] [--order factored]
+    python -m vivlasov1d_b200.kernel_bench --sweep 256 [--precision mixed] [--kernels mdot,pc,jvp,maxpy]
 
 Times, in isolation (graph-captured back-to-back launches, CUDA events) and
 on inputs larger than L2 when the grid is large:
@@ -9,6 +10,9 @@ the residual stencil (24 B/cell: read F, Fh, write Y), the tensor-product
 preconditioner (48 B/cell over its three kernels) and the moments pass
 (8 B/cell).  Prints one JSON line per kernel with the achieved algorithmic
 bandwidth.  The GMRES basis is not allocated beyond two vectors.
+With --sweep N: the whole-table batch kernels of the seeded N-instance sweep
+(multi-dot and multi-axpy at Arnoldi index --it, preconditioner, Jacobian
+stencil), algorithmic bytes per cell in the batch precision.
 """
 from __future__ import annotations
 
@@ -44,7 +48,13 @@ def main(argv=None):
     ap.add_argument("--reps", type=int, default=20)
     ap.add_argument("--order", default="factored", choices=["factored", "reference"])
     ap.add_argument("--kernels", default="jvp,residual,pc,moments")
+    ap.add_argument("--sweep", type=int, default=0,
+                    help="time the whole-table batch kernels of an N-instance seeded sweep instead")
+    ap.add_argument("--precision", default="mixed", choices=["fp64", "mixed"])
+    ap.add_argument("--it", type=int, default=4, help="Arnoldi index of the sweep multi-dot/multi-axpy launches")
     args = ap.parse_args(argv)
+    if args.sweep:
+        return sweep_main(args)
     nx, nv = args.nx, args.nv
     g = Grid(nx, nv, 12.566370614359172, 8.0, ht=0.05)
     ctx = g.context(order=args.order, restart=1)
@@ -83,6 +93,27 @@ def main(argv=None):
                           "median_us": med * 1e6, "mean_us": avg * 1e6,
                           "achieved_GBps": bpc * cells / med / 1e9,
                           "cells_per_s": cells / med}))
+
+
+def sweep_main(args):
+    """Whole-table launches of the batch kernels (every instance active),
+    no time step run before them: the first launch of each kernel is timed."""
+    from . import workloads as W
+    from .batch import Batch
+    specs = W.sweep_specs(args.sweep)
+    cells = sum(s["nx"] * s["nv"] for s in specs)
+    batch = Batch(W.sweep_runs(specs=specs, precision=args.precision))
+    word = 4 if args.precision == "mixed" else 8
+    kinds = {"mdot": (0, (args.it + 2) * word), "pc": (1, 6 * word), "jvp": (2, 2 * word),
+             "maxpy": (3, (args.it + 3) * word)}
+    for name in args.kernels.split(","):
+        if name not in kinds:
+            continue
+        which, bpc = kinds[name]
+        t = batch.time_kernel(which, it=args.it, reps=args.reps)
+        print(json.dumps({"kernel": "batch " + name, "instances": args.sweep, "cells": cells,
+                          "precision": args.precision, "it": args.it, "bytes_per_cell": bpc,
+                          "avg_us": t * 1e6, "achieved_GBps": bpc * cells / t / 1e9}))
 
 
 if __name__ == "__main__":

@@ -80,8 +80,8 @@ class Grid:
         return torch.zeros(self.nx, dtype=torch.float64, device=self.device)
 
     def context(self, bracket="arakawaj4", preconditioner="tensor_kinetic", charge=-1.0, mass=1.0,
-                order="factored", restart=30, precision="fp64"):
-        key = (bracket, preconditioner, float(charge), float(mass), order, int(restart), precision)
+                order="factored", restart=30, precision="fp64", mixed_rtol=0.0):
+        key = (bracket, preconditioner, float(charge), float(mass), order, int(restart), precision, float(mixed_rtol))
         ctx = self._contexts.get(key)
         if ctx is None:
             ctx = Context(self, *key)
@@ -94,7 +94,7 @@ class Context:
     """Owner of one ``vv_ctx`` (device work buffers, preconditioner factors)."""
 
     def __init__(self, grid, bracket="arakawaj4", preconditioner="tensor_kinetic", charge=-1.0,
-                 mass=1.0, order="factored", restart=30, precision="fp64"):
+                 mass=1.0, order="factored", restart=30, precision="fp64", mixed_rtol=0.0):
         lib = _lib.load()
         if not torch.cuda.is_available():
             raise RuntimeError("vivlasov1d_b200 needs a CUDA device; no CPU fallback exists")
@@ -119,6 +119,7 @@ class Context:
         if precision not in _lib.PRECISION:
             raise ValueError("precision must be one of %s" % list(_lib.PRECISION))
         g.precision = _lib.PRECISION[precision]
+        g.mixed_rtol = float(mixed_rtol)   # mixed precision: FP32 inner-solve tolerance (0: library default)
         self.precision = precision
         self.charge, self.mass = float(charge), float(mass)
         self.bracket, self.preconditioner_type, self.order = bracket, preconditioner, order
