@@ -1919,8 +1919,10 @@ int b_autotune(vv_batch* b, std::vector<vv::BInst>& tab) {
             for (int k = 0; k < 5 && r == VV_OK; ++k) r = b_pc<T>(b, vv::L_ALL, false, vv::BD_B);
             cudaEventRecord(e1, b->st);
             float ms = 0.f;
-            if (r == VV_OK && cudaEventSynchronize(e1) == cudaSuccess && cudaEventElapsedTime(&ms, e0, e1) == cudaSuccess &&
-                ms < best) {
+            const bool timed = r == VV_OK && cudaEventSynchronize(e1) == cudaSuccess &&
+                               cudaEventElapsedTime(&ms, e0, e1) == cudaSuccess;
+            if (timed && getenv("VV_DEBUG")) fprintf(stderr, "[vv_batch] tune R=%d tri=%d: %.1f us\n", R, tw, ms * 200.f);
+            if (timed && ms < best) {
                 best = ms;
                 bR = R;
                 bW = tw;

@@ -52,6 +52,8 @@ def main(argv=None):
                     help="time the whole-table batch kernels of an N-instance seeded sweep instead")
     ap.add_argument("--precision", default="mixed", choices=["fp64", "mixed"])
     ap.add_argument("--it", type=int, default=4, help="Arnoldi index of the sweep multi-dot/multi-axpy launches")
+    ap.add_argument("--sweep-steps", type=int, default=0,
+                    help="with --sweep: run this many batched time steps (after one warm-up step) instead")
     args = ap.parse_args(argv)
     if args.sweep:
         return sweep_main(args)
@@ -103,6 +105,20 @@ def sweep_main(args):
     specs = W.sweep_specs(args.sweep)
     cells = sum(s["nx"] * s["nv"] for s in specs)
     batch = Batch(W.sweep_runs(specs=specs, precision=args.precision))
+    if args.sweep_steps:
+        batch.step()
+        for k in range(args.sweep_steps):
+            torch.cuda.synchronize()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            reps = batch.step()
+            e1.record()
+            e1.synchronize()
+            print(json.dumps({"sweep_step": k + 1, "instances": args.sweep, "cells": cells, "precision": args.precision,
+                              "ms": e0.elapsed_time(e1), "launches": batch.launch_count(reset=True),
+                              "picard_max": max(r["picard_its"] for r in reps),
+                              "gmres_max": max(sum(r["gmres_its"]) for r in reps)}))
+        return
     word = 4 if args.precision == "mixed" else 8
     kinds = {"mdot": (0, (args.it + 2) * word), "pc": (1, 6 * word), "jvp": (2, 2 * word),
              "maxpy": (3, (args.it + 3) * word)}
