@@ -260,6 +260,26 @@ int vv_batch_launch_count(vv_batch* batch, int64_t* launches, int reset);
  * the GMRES scratch of every instance is overwritten. */
 int vv_batch_time_kernel(vv_batch* batch, int which, int it, int reps, double* avg_ms);
 
+/* ---- discrete adjoint of the converged step (no counterpart in the
+ *      reference; built from its discrete operators) ---------------------
+ * For a converged step f -> F (F = f^{n+1}, f = f^n, with the external
+ * profiles h2p/h2h or NULL) and the gradient gF of a loss with respect to F,
+ * writes the gradient with respect to f: gf = -gF + (2/ht) lambda with
+ * A^T lambda = gF, A the coupled Jacobian of the step's residual (the
+ * Jacobian-vector product of PETScNLVlasovMP.pyx:33-40 plus the f-phi
+ * coupling through the moments and the Poisson solve,
+ * solvers/full/PETScNLArakawaJ4.pyx:26-110).  The transpose system is solved
+ * by GMRES preconditioned with the transposed kinetic preconditioner, to the
+ * tolerances in opts; result reports its iterations.  FP64 contexts only
+ * (VV_ERR_UNSUPPORTED for mixed).  The first call allocates the adjoint's
+ * buffers (24 fields). */
+int vv_step_adjoint(vv_ctx* ctx, const double* F, const double* f, const double* h2p,
+                    const double* h2h, const double* gF, double* gf, const vv_ksp_opts* opts,
+                    vv_ksp_result* result);
+/* Gradient of the field energy 1/2 charge sum_i (phi_{i+1} - phi_i)^2 / hx
+ * (potential.pyx:48-59) with respect to f. */
+int vv_field_energy_grad(vv_ctx* ctx, const double* f, double* grad);
+
 /* ---- invariants (vlasov/core/distribution_function.pyx:130-306,
  *      hamiltonian.pyx:67-124, potential.pyx:48-59) ---------------------- */
 typedef struct vv_invariant_set {

@@ -103,6 +103,8 @@ SIGNATURES = {
     "vv_step": (I, [P, C.POINTER(vv_state), C.POINTER(vv_snes_opts), C.POINTER(vv_ksp_opts),
                     C.POINTER(vv_step_report)]),
     "vv_invariants": (I, [P, P, P, P, C.POINTER(vv_invariant_set)]),
+    "vv_step_adjoint": (I, [P, P, P, P, P, P, P, C.POINTER(vv_ksp_opts), C.POINTER(vv_ksp_result)]),
+    "vv_field_energy_grad": (I, [P, P, P]),
     "vv_invariants_noalloc": (I, [C.POINTER(vv_grid), P, P, P, P, C.POINTER(vv_invariant_set)]),
     "vv_timing_enable": (I, [P, I]),
     "vv_timing_read": (I, [P, C.POINTER(C.c_int64), C.POINTER(D), I]),

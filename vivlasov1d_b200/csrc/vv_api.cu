@@ -13,6 +13,7 @@
 #include "vv_pc.cuh"
 #include "vv_vec.cuh"
 #include "vv_batch.cuh"
+#include "vv_adjoint.cuh"
 
 #include <algorithm>
 #include <array>
@@ -83,6 +84,10 @@ struct vv_ctx {
     unsigned long long step_hnd[5];  // handles of this context's own step graph
     // kernels per region of the step graph (for launch accounting)
     int nk_top, nk_pic, nk_cycle, nk_restart, nk_arnoldi, nk_revert;
+    // discrete adjoint (allocated at the first adjoint call): GMRES operator
+    // switch, coefficient planes of J_H^T and J_Fbar^T, Poisson-chain scratch
+    bool adj;
+    double *adj_cH, *adj_cF, *adj_zpart, *adj_zbuf, *adj_q, *adj_hprof, *adj_h1a, *adj_h1b;
 };
 
 namespace {
@@ -370,6 +375,8 @@ int raise_smem_limits(int* limit_out) {
         smem_attributes<float>(optin, lowest, e);
         smem_set((const void*)vv::k_moments_poisson, optin, lowest, e);
         smem_set((const void*)vv::k_b_moments_poisson, optin, lowest, e);
+        smem_set((const void*)vv::k_adj_poisson, optin, lowest, e);
+        smem_set((const void*)vv::k_tridiag_modes_adjT, optin, lowest, e);
         smem_set((const void*)vv::k_b_rfft<double, double>, optin, lowest, e);
         smem_set((const void*)vv::k_b_rfft<double, float>, optin, lowest, e);
         smem_set((const void*)vv::k_b_rfft<float, float>, optin, lowest, e);
@@ -440,9 +447,73 @@ template <> struct Buf<float> {
     static float* x(vv_ctx* c) { return c->delta32; }
 };
 
+// ---- discrete adjoint: A^T and P^-T (FP64) ----------------------------------
+vv::PoissonParams pparams(const vv_ctx* c);
+int copy_d(vv_ctx* c, double* dst, const double* src, size_t count);
+
+vv::AdjParams adjparams(const vv_ctx* c) {
+    vv::AdjParams p;
+    p.nx = c->nx;
+    p.nv = c->nv;
+    p.ncell = c->ncell;
+    p.ht_inv = c->ht_inv;
+    p.f1 = c->f1;
+    p.f2 = c->f2;
+    p.hv = c->hv;
+    return p;
+}
+
+// Y = A^T X (X may be a basis base pointer with xidx)
+int adj_apply(vv_ctx* c, const double* X, const int* xidx, double* Y) {
+    const vv::AdjParams p = adjparams(c);
+    dim3 grid((c->nx + vv::ADJ_TX - 1) / vv::ADJ_TX, c->mom_S);
+    vv::k_adj_apply<<<grid, dim3(vv::ADJ_TX, vv::ADJ_TY), 0, c->st>>>(p, c->adj_cH, c->adj_cF, X, xidx, Y, c->mom_seg,
+                                                                      c->adj_zpart);
+    CKL(c);
+    vv::k_adj_poisson<<<1, vv::POIS_THREADS, c->smem_pois, c->st>>>(c->adj_zpart, c->mom_S, c->adj_zbuf, c->adj_q,
+                                                                    pparams(c));
+    CKL(c);
+    vv::k_adj_bcast<<<grid1d(c->ncell, 256), 256, 0, c->st>>>(p, c->adj_q, Y);
+    CKL(c);
+    return VV_OK;
+}
+
+// Y = P^-T X: the same FFT pair, conjugate-transposed mode solves
+int pcT_apply(vv_ctx* c, const double* X, double* Y, const int* yidx = nullptr, int yoff = 0) {
+    if (c->g.preconditioner != VV_PC_TENSOR_KINETIC) {
+        if (yidx) return VV_ERR_UNSUPPORTED;
+        return copy_d(c, Y, X, c->ncell);
+    }
+    vv::PcParams p = pcparams(c);
+    p.tw = c->tw;
+    const unsigned rows = (unsigned)((c->nv + c->pcR - 1) / c->pcR);
+    TRY(launch_rfft<double, double>(c, X, c->spec, p, rows));
+    vv::TriParams t;
+    t.nv = c->nv;
+    t.nmodes = c->nmodes;
+    t.lambda = c->lambda;
+    t.alpha = c->alpha;
+    t.gamma = c->gamma;
+    t.dinv = c->dinv;
+    const int ch = (c->nv + vv::TRI_THREADS - 1) / vv::TRI_THREADS;
+    const size_t sm = ((size_t)c->nv + (c->nv + ch - 1) / ch) * sizeof(double2);
+    vv::k_tridiag_modes_adjT<<<c->nmodes, vv::TRI_THREADS, sm, c->st>>>(c->spec, t);
+    CKL(c);
+    p.yidx = yidx;
+    p.yoff = yoff;
+    p.ystride = yidx ? c->ncell : 0;
+    return launch_irfft<double, double>(c, c->spec, Y, p, rows);
+}
+
 // Y = P^-1 J X (or J X) in precision T
 template <typename T>
 int apply_operator_t(vv_ctx* c, const T* X, T* Y) {
+    if constexpr (std::is_same<T, double>::value) {
+        if (c->adj) {   // the adjoint solve: P^-T A^T
+            TRY(adj_apply(c, X, nullptr, c->tmp));
+            return pcT_apply(c, c->tmp, Y);
+        }
+    }
     if (c->g.preconditioner == VV_PC_TENSOR_KINETIC) {
         TRY(launch_bracket<vv::MODE_JVP, T>(c, X, nullptr, Buf<T>::tmp(c), 0.5, nullptr));
         return pc_apply_t<T, T, T>(c, Buf<T>::tmp(c), Y);
@@ -465,6 +536,15 @@ template <typename T>
 int apply_operator_state(vv_ctx* c) {
     const int* itp = &c->ds->it;
     T* V = Buf<T>::V(c);
+    if constexpr (std::is_same<T, double>::value) {
+        if (c->adj) {   // the adjoint solve: V[it+1] = P^-T A^T V[it]
+            TRY(adj_apply(c, V, itp, c->tmp));
+            if (c->g.preconditioner == VV_PC_TENSOR_KINETIC) return pcT_apply(c, c->tmp, V, itp, 1);
+            k_copy_to_slot<double><<<grid1d(c->ncell, 256), 256, 0, c->st>>>(c->tmp, V, itp, c->ncell);
+            CKL(c);
+            return VV_OK;
+        }
+    }
     TRY(launch_bracket<vv::MODE_JVP, T>(c, V, nullptr, Buf<T>::tmp(c), 0.5, nullptr, itp));
     if (c->g.preconditioner == VV_PC_TENSOR_KINETIC) return pc_apply_t<T, T, T>(c, Buf<T>::tmp(c), V, itp, 1);
     k_copy_to_slot<T><<<grid1d(c->ncell, 256), 256, 0, c->st>>>(Buf<T>::tmp(c), V, itp, c->ncell);
@@ -1284,7 +1364,8 @@ int vv_destroy(vv_ctx* c) {
     void* bufs[] = {c->v, c->h0, c->hxp, c->Fh, c->tmp, c->bvec, c->delta, c->fl, c->V, c->part, c->scal,
                     c->xscratch, c->mom_part, c->spec, c->tw, c->lambda, c->dinv, c->alpha, c->gamma,
                     c->sym_inv, c->ds, c->V32, c->tmp32, c->bvec32, c->delta32, c->alpha32, c->gamma32,
-                    c->spec32, c->tw32, c->lambda32, c->dinv32};
+                    c->spec32, c->tw32, c->lambda32, c->dinv32, c->adj_cH, c->adj_cF, c->adj_zpart,
+                    c->adj_zbuf, c->adj_q, c->adj_hprof, c->adj_h1a, c->adj_h1b};
     destroy_graph(c);
     for (int k = 0; k < 4; ++k)
         if (c->cs[k]) cudaStreamDestroy(c->cs[k]);
@@ -1405,6 +1486,86 @@ int vv_gmres(vv_ctx* c, const double* b, double* x, const vv_ksp_opts* o, vv_ksp
     CKL(c);
     TRY(gmres_host<float>(c, c->bvec32, c->delta32, r));
     vv::k_scale<float, double><<<grid1d(c->ncell, 256), 256, 0, c->st>>>(c->delta32, x, c->ncell, nullptr, 1.0);
+    CKL(c);
+    return VV_OK;
+}
+
+}  // extern "C"
+
+namespace {
+
+int adj_buffers(vv_ctx* c) {
+    if (c->adj_cH) return VV_OK;
+    int s = VV_OK;
+    const size_t nx = c->nx;
+    if ((s = dalloc(&c->adj_cH, (size_t)vv::ADJ_NOFF * c->ncell)) || (s = dalloc(&c->adj_cF, (size_t)vv::ADJ_NOFF * c->ncell)) ||
+        (s = dalloc(&c->adj_zpart, (size_t)c->mom_S * nx)) || (s = dalloc(&c->adj_zbuf, nx)) ||
+        (s = dalloc(&c->adj_q, nx)) || (s = dalloc(&c->adj_hprof, nx)) || (s = dalloc(&c->adj_h1a, nx)) ||
+        (s = dalloc(&c->adj_h1b, nx)))
+        return s;
+    return VV_OK;
+}
+
+template <int S>
+int adj_coefs(vv_ctx* c, const double* F, const double* f) {
+    const vv::AdjParams p = adjparams(c);
+    const dim3 grid((c->nx + 255) / 256, c->nv);
+    vv::k_adj_coef<S, 0><<<grid, 256, 0, c->st>>>(p, c->h0, c->adj_hprof, nullptr, nullptr, c->adj_cH);
+    CKL(c);
+    vv::k_adj_coef<S, 1><<<grid, 256, 0, c->st>>>(p, nullptr, nullptr, F, f, c->adj_cF);
+    CKL(c);
+    return VV_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int vv_step_adjoint(vv_ctx* c, const double* F, const double* f, const double* h2p, const double* h2h,
+                    const double* gF, double* gf, const vv_ksp_opts* o, vv_ksp_result* r) {
+    if (!c || !F || !f || !gF || !gf || !o || !r) return VV_ERR_ARG;
+    if (c->mixed) return VV_ERR_UNSUPPORTED;
+    const int restart = (o->restart > 0) ? o->restart : c->restart;
+    if (restart > c->restart || restart < 1 || o->max_it < 0) return VV_ERR_ARG;
+    TRY(adj_buffers(c));
+    // H = h0 + (h1(F) + h1(f) + h2p + h2h)/2 and Fbar = (F + f)/2 as coefficient planes
+    TRY(moments_poisson(c, F, nullptr, nullptr, nullptr, nullptr, nullptr, c->adj_h1a, nullptr));
+    TRY(moments_poisson(c, f, nullptr, nullptr, nullptr, nullptr, nullptr, c->adj_h1b, nullptr));
+    vv::k_adj_hprof<<<1, 256, 0, c->st>>>(c->nx, c->adj_h1a, c->adj_h1b, h2p, h2h, c->adj_hprof);
+    CKL(c);
+    switch (c->g.bracket) {
+        case VV_BRACKET_J1: TRY(adj_coefs<1>(c, F, f)); break;
+        case VV_BRACKET_J2: TRY(adj_coefs<2>(c, F, f)); break;
+        default: TRY(adj_coefs<4>(c, F, f)); break;
+    }
+    // left-preconditioned transpose system  P^-T A^T lambda = P^-T gF
+    TRY(pcT_apply(c, gF, c->bvec));
+    const unsigned long long saved[5] = {c->hnd[0], c->hnd[1], c->hnd[2], c->hnd[3], c->hnd[4]};
+    for (auto& h : c->hnd) h = 0;
+    c->opts_valid = false;
+    int s = upload_options(c, o, nullptr);
+    c->opts_valid = false;
+    for (int k = 0; k < 5; ++k) c->hnd[k] = saved[k];
+    TRY(s);
+    c->adj = true;
+    s = gmres_host<double>(c, c->bvec, c->delta, r);
+    c->adj = false;
+    TRY(s);
+    vv::k_adj_pull<<<grid1d(c->ncell, 256), 256, 0, c->st>>>(adjparams(c), gF, c->delta, gf);
+    CKL(c);
+    return VV_OK;
+}
+
+int vv_field_energy_grad(vv_ctx* c, const double* f, double* g) {
+    if (!c || !f || !g) return VV_ERR_ARG;
+    TRY(adj_buffers(c));
+    // phi of f, then dW/dphi, then the transpose of the moments -> Poisson chain
+    TRY(moments_poisson(c, f, nullptr, nullptr, nullptr, nullptr, c->adj_h1a, nullptr, nullptr));
+    vv::k_adj_fe_gphi<<<1, 1024, 0, c->st>>>(c->nx, c->g.charge, c->hx, c->adj_h1a, c->adj_zpart);
+    CKL(c);
+    vv::k_adj_poisson<<<1, vv::POIS_THREADS, c->smem_pois, c->st>>>(c->adj_zpart, 1, c->adj_zbuf, c->adj_q, pparams(c));
+    CKL(c);
+    vv::k_adj_fill<<<grid1d(c->ncell, 256), 256, 0, c->st>>>(adjparams(c), c->adj_q, g);
     CKL(c);
     return VV_OK;
 }
