@@ -124,6 +124,18 @@ def specs_for(rank):
     return W.sweep_specs(N_INSTANCES, seed=W.SWEEP_SEED + rank)
 
 
+def reduce_over_ranks(maxes, sums, device):
+    """Max over ranks of the times and sum over ranks of the work (one
+    all-reduce each; every rank calls it the same way)."""
+    import torch
+    import torch.distributed as dist
+    tm = torch.tensor(maxes, dtype=torch.float64, device=device)
+    ts = torch.tensor(sums, dtype=torch.float64, device=device)
+    dist.all_reduce(tm, op=dist.ReduceOp.MAX)
+    dist.all_reduce(ts, op=dist.ReduceOp.SUM)
+    return [float(x) for x in tm], [float(x) for x in ts]
+
+
 def time_steps(fn, k, stream):
     import torch
     torch.cuda.synchronize()
@@ -195,12 +207,10 @@ def run_gpu(args, rank, world):
         return out
 
     t_e2e, _ = time_steps(e2e_step, args.steps, stream)
+    total_cells = cells
     if world > 1:
-        import torch.distributed as dist
-        t = torch.tensor([t_value, t_plain, t_e2e], dtype=torch.float64, device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        t_value, t_plain, t_e2e = (float(x) for x in t)
-    return dict(cells=cells, t_value=t_value, t_plain=t_plain, t_e2e=t_e2e, launches=launches, clocks=clocks,
+        (t_value, t_plain, t_e2e), (total_cells,) = reduce_over_ranks([t_value, t_plain, t_e2e], [cells], dev)
+    return dict(cells=cells, total_cells=total_cells, t_value=t_value, t_plain=t_plain, t_e2e=t_e2e, launches=launches, clocks=clocks,
                 picard=picard, gmres=gmres, fe_rel=fe_rel, mdot_s=mdot_s, pc_s=pc_s, jvp_s=jvp_s)
 
 
@@ -307,10 +317,11 @@ def main():
         dist.destroy_process_group()
     if rank != 0:
         return
-    cells = res["cells"]
-    value = cells * args.steps * world / res["t_value"] / 1e9
-    plain = cells * args.steps * world / res["t_plain"] / 1e9
-    e2e = cells * args.steps * world / res["t_e2e"] / 1e9
+    cells = res["cells"]                      # this rank's sweep (for the per-launch roofline)
+    work = res["total_cells"] * args.steps    # every rank's cells, every timed step
+    value = work / res["t_value"] / 1e9
+    plain = work / res["t_plain"] / 1e9
+    e2e = work / res["t_e2e"] / 1e9
     peak, peak_kind = measured_peaks()
     mdot_bytes = cells * (MDOT_IT + 2) * 4      # w and V_0..V_it read in FP32
     achieved = mdot_bytes / res["mdot_s"] / 1e9
