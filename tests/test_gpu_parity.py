@@ -472,3 +472,36 @@ def test_mixed_precision_matches_fp64():
     for k in ("mass", "L2", "energy", "entropy"):
         assert abs(i32[k] - i64[k]) <= 1e-10 * abs(i64[k]), k
     assert rel(host(r32.fc), host(r64.fc)) < 1e-9
+
+
+@pytest.mark.parametrize("march", [128, 256])
+def test_marching_jvp_equals_tiled_jvp(monkeypatch, march):
+    """The marching Jacobian stencil (cp.async ring, one thread per column)
+    gives the same bits as the 64 x 32 tile kernel: FP64 through vv_jacobian
+    and FP32 inside a mixed time step."""
+    from vivlasov1d_b200 import Grid
+    import ctypes as C
+    nx, nv = 256, 512
+    rng = np.random.default_rng(41)
+    x = rng.standard_normal((nx, nv))
+    h1 = 0.1 * rng.standard_normal(nx)
+    outs = []
+    monkeypatch.setenv("VV_AUTOTUNE", "0")
+    for m in (0, march):
+        monkeypatch.setenv("VV_MARCH", str(m))
+        g = Grid(nx, nv, 4 * np.pi, 8.0, ht=0.05)
+        ctx = g.context(preconditioner=None)
+        X, P, Y = dev(x), xdev(h1), g.field()
+        ctx.call("vv_update_previous", ctx.xprof(P), ctx.xprof(P), None, None)
+        ctx.call("vv_jacobian", ctx.field(X), ctx.field(Y), 0)
+        outs.append(Y.clone())
+    assert torch.equal(outs[0], outs[1])
+    runs = []
+    for m in (0, march):
+        monkeypatch.setenv("VV_MARCH", str(m))
+        r = _small_run(256, 256, vo.f0_twostream(0.05, 0.5), 4 * np.pi, 0.1)
+        from vivlasov1d_b200.run import Run
+        r2 = Run(r.cfg, f0=r.fc.clone(), precision="mixed", normalise=False)
+        r2.step()
+        runs.append(r2.fc.clone())
+    assert torch.equal(runs[0], runs[1])

@@ -51,6 +51,7 @@ struct vv_ctx {
     int fft_kind;      // 0: shared-memory radix-2 per warp, 1: four-step register/shuffle FFT
     int tri_kind;      // 0: one CTA per mode (block scan), 1: one warp per mode
     int narrow_bracket;  // 1: 32x16 tiles instead of 64x32
+    int march;           // Jacobian stencil: 0 tiles, 128 or 256 the strip width of the marching kernel
     // pinned host staging
     double* hpin;
     int* hstat;
@@ -208,6 +209,24 @@ bool wide_ok(const vv_ctx* c, const void* X, const void* Xh, const void* Y) {
     return !c->narrow_bracket && c->nx % vv::WX == 0 && aligned16(X) && aligned16(Xh) && aligned16(Y);
 }
 
+// the marching Jacobian stencil: about two waves of CTAs, segments of whole chunks
+template <int SCHEME, typename T, int MW>
+int launch_march(vv_ctx* c, const T* X, T* Y, const vv::BracketParams& p) {
+    const size_t smem = vv::MarchRow<T, MW>::smem_bytes();
+    constexpr int CH = vv::MarchShape<T>::CH;
+    int per_sm = 0, nsm = 148;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, vv::k_bracket_march<SCHEME, T, MW>, MW, smem);
+    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, c->device);
+    const int strips = c->nx / MW;
+    const long target = 2L * nsm * std::max(1, per_sm);
+    const int nseg = (int)std::max<long>(1, (target + strips - 1) / strips);
+    int seg = (c->nv + nseg - 1) / nseg;
+    seg = std::max(CH, (seg + CH - 1) / CH * CH);
+    const dim3 grid(strips, (c->nv + seg - 1) / seg);
+    vv::k_bracket_march<SCHEME, T, MW><<<grid, MW, smem, c->st>>>(X, Y, p, seg);
+    return VV_OK;
+}
+
 // X may be a GMRES basis base pointer with xidx -> the vector index in the state
 template <int SCHEME, int MODE, typename T>
 int launch_bracket_s(vv_ctx* c, const T* X, const T* Xh, T* Y, double factor, double* sumsq, const int* xidx) {
@@ -230,6 +249,11 @@ int launch_bracket_s(vv_ctx* c, const T* X, const T* Xh, T* Y, double factor, do
             vv::k_bracket_ref<SCHEME, MODE><<<grid, block, 0, c->st>>>(X, Xh, Y, p, sumsq);
             done = true;
         }
+    }
+    if (!done && MODE == vv::MODE_JVP && c->march && c->g.order != VV_ORDER_REFERENCE && c->nx % c->march == 0 &&
+        aligned16(X) && aligned16(Y)) {
+        TRY(c->march == 256 ? launch_march<SCHEME, T, 256>(c, X, Y, p) : launch_march<SCHEME, T, 128>(c, X, Y, p));
+        done = true;
     }
     if (!done) {
         if (wide_ok(c, X, Xh, Y)) {
@@ -376,6 +400,13 @@ int raise_smem_limits(int* limit_out) {
         smem_set((const void*)vv::k_moments_poisson, optin, lowest, e);
         smem_set((const void*)vv::k_b_moments_poisson, optin, lowest, e);
         smem_set((const void*)vv::k_adj_poisson, optin, lowest, e);
+#define VV_SET_MARCH(S)                                                              \
+    smem_set((const void*)vv::k_bracket_march<S, double, 128>, optin, lowest, e);     \
+    smem_set((const void*)vv::k_bracket_march<S, double, 256>, optin, lowest, e);     \
+    smem_set((const void*)vv::k_bracket_march<S, float, 128>, optin, lowest, e);      \
+    smem_set((const void*)vv::k_bracket_march<S, float, 256>, optin, lowest, e);
+        VV_SET_MARCH(1) VV_SET_MARCH(2) VV_SET_MARCH(4)
+#undef VV_SET_MARCH
         smem_set((const void*)vv::k_tridiag_modes_adjT, optin, lowest, e);
         smem_set((const void*)vv::k_b_rfft<double, double>, optin, lowest, e);
         smem_set((const void*)vv::k_b_rfft<double, float>, optin, lowest, e);
@@ -901,7 +932,7 @@ bool same_state(const vv_state& a, const vv_state& b) { return std::memcmp(&a, &
 // GMRES precision, and the bracket tile shape.  Results are cached per
 // (nx, nv, precision) for the life of the process.
 struct TuneResult {
-    int fft_kind, pcR, tri_kind, narrow;
+    int fft_kind, pcR, tri_kind, narrow, march;
 };
 
 std::vector<std::pair<std::array<int, 3>, TuneResult>>& tune_cache() {
@@ -936,12 +967,13 @@ int autotune(vv_ctx* c) {
             c->pcR = kv.second.pcR;
             c->tri_kind = kv.second.tri_kind;
             c->narrow_bracket = kv.second.narrow;
+            c->march = kv.second.march;
             return VV_OK;
         }
     const size_t n = c->ncell;
     CK(cudaMemsetAsync(c->tmp, 0, n * sizeof(double), c->st));
     if (c->mixed) CK(cudaMemsetAsync(c->tmp32, 0, n * sizeof(float), c->st));
-    TuneResult best{c->fft_kind, c->pcR, c->tri_kind, 0};
+    TuneResult best{c->fft_kind, c->pcR, c->tri_kind, 0, 0};
     float best_ms = 1e30f;
     // FP64 complex size also in the mixed mode: the FP64 entry points
     // (vv_pc_apply) share the tuned rows-per-CTA
@@ -961,7 +993,7 @@ int autotune(vv_ctx* c) {
                 TRY(r);
                 if (ms < best_ms) {
                     best_ms = ms;
-                    best = {kind, R, tk, 0};
+                    best = {kind, R, tk, 0, 0};
                 }
             }
         }
@@ -988,6 +1020,29 @@ int autotune(vv_ctx* c) {
         best.narrow = t_narrow < t_wide ? 1 : 0;
     }
     c->narrow_bracket = best.narrow;
+    // the Jacobian stencil: tiles (the choice above) or the marching kernel
+    {
+        float t_best = 1e30f;
+        for (int mw : {0, 128, 256}) {
+            if (mw && (c->nx % mw != 0 || c->g.order == VV_ORDER_REFERENCE)) continue;
+            c->march = mw;
+            float ms = 0.f;
+            int r = c->mixed ? time_it(c, [&]() {
+                                   return launch_bracket<vv::MODE_JVP, float>(c, c->tmp32, nullptr, c->bvec32, 0.5,
+                                                                              nullptr);
+                               }, 10, &ms)
+                             : time_it(c, [&]() {
+                                   return launch_bracket<vv::MODE_JVP, double>(c, c->tmp, nullptr, c->bvec, 0.5,
+                                                                               nullptr);
+                               }, 10, &ms);
+            TRY(r);
+            if (ms < t_best) {
+                t_best = ms;
+                best.march = mw;
+            }
+        }
+    }
+    c->march = best.march;
     c->launches = 0;
     tune_cache().push_back({key, best});
     return VV_OK;
@@ -1346,6 +1401,11 @@ int vv_create(const vv_grid* grid, vv_ctx** out) {
     c->fft_kind = four_step_ok(c->M) ? 1 : 0;
     c->tri_kind = c->nmodes >= 64 ? 1 : 0;
     c->narrow_bracket = 0;
+    c->march = 0;
+    {
+        const char* e = getenv("VV_MARCH");   // fixed strip width (tests, profiling); the autotuner may override
+        if (e) c->march = atoi(e);
+    }
     {
         const char* e = getenv("VV_AUTOTUNE");
         if (!(e && e[0] == '0')) {

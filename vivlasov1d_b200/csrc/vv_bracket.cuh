@@ -467,6 +467,185 @@ __device__ __forceinline__ void bracket_wide_tile(const T* __restrict__ X, const
     }
 }
 
+// ---------------------------------------------------------------------------
+// Marching Jacobian-vector product: a CTA owns a strip of MW columns (one
+// thread per column) and a segment of rows, and walks down v through a ring
+// of NR rows in shared memory (a power of two) that cp.async fills three
+// chunks of CH rows ahead of the compute.  Each thread keeps its column's five-row
+// window and its column's x-coefficients in registers; the v-coefficients of
+// a chunk's rows are formed once per CTA.  A row costs 5 shared loads per
+// output; the x halo is 4 of MW + 4 columns and the v halo 4 rows per segment.
+// ---------------------------------------------------------------------------
+// rows per chunk and ring rows (a power of two >= 2 chunks + 4 halo rows)
+template <typename T> struct MarchShape;
+template <> struct MarchShape<double> { static constexpr int CH = 8, NR = 32; };
+template <> struct MarchShape<float> { static constexpr int CH = 16, NR = 64; };
+
+VV_DEV void cp_async_16(void* smem, const void* gmem, int src_bytes) {
+    const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(s), "l"(gmem), "r"(src_bytes));
+}
+VV_DEV void cp_async_8(void* smem, const void* gmem, int src_bytes) {
+    const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(s), "l"(gmem), "r"(src_bytes));
+}
+VV_DEV void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::); }
+VV_DEV void cp_async_wait2() { asm volatile("cp.async.wait_group 2;\n" ::); }
+
+// ring row layout: [pad][2 left halo][MW columns][2 right halo][pad]; the
+// main columns start at LP elements (16 bytes), every row is 16-byte aligned
+template <typename T, int MW>
+struct MarchRow {
+    static constexpr int LP = 16 / (int)sizeof(T);
+    static constexpr int RS = MW + 2 * LP;
+    static constexpr size_t smem_bytes() {
+        return (size_t)MarchShape<T>::NR * RS * sizeof(T) + (size_t)MarchShape<T>::CH * 3 * sizeof(double);
+    }
+};
+
+// rows [ra, rb] of the strip starting at column x0 into their ring slots
+template <typename T, int MW>
+VV_DEV void march_load(const T* __restrict__ X, T* ring, int nx, int nv, int x0, int ra, int rb) {
+    using RW = MarchRow<T, MW>;
+    constexpr int NR = MarchShape<T>::NR;
+    constexpr int NMAIN = MW * (int)sizeof(T) / 16;     // 16-byte chunks of the main columns
+    constexpr int NCH = NMAIN + 2;
+    constexpr int EPC = 16 / (int)sizeof(T);             // elements per 16-byte chunk
+    const int nrow = rb - ra + 1;
+    const int xl = x0 == 0 ? nx - 2 : x0 - 2;           // periodic halo columns
+    const int xr = x0 + MW == nx ? 0 : x0 + MW;
+    for (int idx = threadIdx.x; idx < nrow * NCH; idx += blockDim.x) {
+        const int rr = idx / NCH, c = idx - rr * NCH;
+        const int r = ra + rr;
+        T* row = ring + ((r + NR) & (NR - 1)) * RW::RS;
+        const bool in = r >= 0 && r < nv;
+        const T* src = X + (size_t)(in ? r : 0) * nx;
+        if (c < NMAIN) {
+            cp_async_16(row + RW::LP + c * EPC, src + x0 + c * EPC, in ? 16 : 0);
+        } else {
+            const int gx = c == NMAIN ? xl : xr;
+            T* dst = c == NMAIN ? row + RW::LP - 2 : row + RW::LP + MW;
+            if (sizeof(T) == 8) cp_async_16(dst, src + gx, in ? 16 : 0);
+            else cp_async_8(dst, src + gx, in ? 8 : 0);
+        }
+    }
+}
+
+template <int SCHEME, typename T, int MW>
+__global__ void __launch_bounds__(MW)
+k_bracket_march(const T* __restrict__ X, T* __restrict__ Y, BracketParams p, int seg) {
+    using RW = MarchRow<T, MW>;
+    constexpr int CH = MarchShape<T>::CH, NR = MarchShape<T>::NR;
+    static_assert(NR >= 3 * CH + 4 && (NR & (NR - 1)) == 0, "ring of three chunks and the halo, a power of two");
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    T* ring = reinterpret_cast<T*>(smem_raw);
+    double* rc = reinterpret_cast<double*>(smem_raw + (size_t)NR * RW::RS * sizeof(T));   // [CH][3] row coefficients
+    if (p.xidx) X += (size_t)(*p.xidx) * p.xstride;
+    const int nx = p.nx, nv = p.nv;
+    const int tx = threadIdx.x;
+    const int x0 = blockIdx.x * MW;
+    const int i = x0 + tx;
+    const int j_start = blockIdx.y * seg;
+    const int j_end = min(nv, j_start + seg);
+    if (j_start >= j_end) return;
+    // column coefficients (fixed for the thread)
+    double b[5];
+#pragma unroll
+    for (int d = 0; d < 5; ++d) {
+        int gi = i - 2 + d;
+        gi = gi < 0 ? gi + nx : (gi >= nx ? gi - nx : gi);
+        b[d] = b_fac(p, gi);
+    }
+    double bm_d, bp_d;
+    Coef<SCHEME>::col(b[2] - b[1], b[3] - b[2], b[3] - b[1], b[2] - b[0], b[4] - b[2], bm_d, bp_d);
+    const T B1 = T(b[3] - b[1]), bm = T(bm_d), bp = T(bp_d);
+    const T tscale = T(((SCHEME == 2) ? p.f2 : p.f1) * p.factor);
+    const T htinv = T(p.ht_inv);
+    auto hv0 = [&](int j) -> double { return (j >= 0 && j < nv) ? p.h0[j] : 0.0; };
+    // prologue: the first chunk with its halo, then the next two chunks (three
+    // copy groups in flight; the compute of a chunk waits for its own group)
+    march_load<T, MW>(X, ring, nx, nv, x0, j_start - 2, min(j_start + CH + 1, j_end + 1));
+    cp_async_commit();
+    for (int k = 1; k <= 2; ++k) {
+        const int ra = j_start + k * CH + 2, rb = min(j_start + (k + 1) * CH + 1, j_end + 1);
+        if (ra <= rb) march_load<T, MW>(X, ring, nx, nv, x0, ra, rb);
+        cp_async_commit();
+    }
+    const int lx = RW::LP + tx;
+    auto rowp = [&](int r) -> const T* { return ring + ((r + NR) & (NR - 1)) * RW::RS + lx; };
+    T w0, w1, w2, w3, m0, m1, q0, q1;
+    bool primed = false;
+    for (int jc = j_start; jc < j_end; jc += CH) {
+        const int jn = min(jc + CH, j_end);
+        // the chunk's row coefficients (A1, am, ap), once per CTA
+        if (tx < jn - jc) {
+            const int j = jc + tx;
+            const double a0 = hv0(j - 2), a1 = hv0(j - 1), a2 = hv0(j), a3 = hv0(j + 1), a4 = hv0(j + 2);
+            double am_d, ap_d;
+            Coef<SCHEME>::row(a2 - a1, a3 - a2, a3 - a1, a2 - a0, a4 - a2, am_d, ap_d);
+            rc[3 * tx] = a3 - a1;
+            rc[3 * tx + 1] = am_d;
+            rc[3 * tx + 2] = ap_d;
+        }
+        cp_async_wait2();
+        __syncthreads();
+        if (!primed) {
+            w0 = rowp(jc - 2)[0]; w1 = rowp(jc - 1)[0]; w2 = rowp(jc)[0]; w3 = rowp(jc + 1)[0];
+            m0 = rowp(jc - 1)[-1]; m1 = rowp(jc)[-1];
+            q0 = rowp(jc - 1)[1]; q1 = rowp(jc)[1];
+            primed = true;
+        }
+        T* yout = Y + (size_t)jc * nx + i;
+        // one output row; the window shifts by renaming when the loop is unrolled
+        auto row_out = [&](int j, T* yo) {
+            const T* r2 = rowp(j + 2);
+            const T* r1 = rowp(j + 1);
+            const T w4 = r2[0];
+            const T m2 = r1[-1];
+            const T q2 = r1[1];
+            T y = htinv * w2;
+            if (j >= 2 && j < nv - 2) {
+                const double* cj = rc + 3 * (j - jc);
+                const T A1 = T(cj[0]), am = T(cj[1]), ap = T(cj[2]);
+                T s = T(0);
+                if (Coef<SCHEME>::cA1 != 0.0 || Coef<SCHEME>::cA2 != 0.0) {
+                    T ax = T(0), bx = T(0);
+                    if (Coef<SCHEME>::cA1 != 0.0) {
+                        ax = T(Coef<SCHEME>::cA1) * (q1 - m1);
+                        bx = T(Coef<SCHEME>::cB1) * (w3 - w1);
+                    }
+                    if (Coef<SCHEME>::cA2 != 0.0) {
+                        const T* r0 = rowp(j);
+                        ax += T(Coef<SCHEME>::cA2) * (r0[2] - r0[-2]);
+                        bx += T(Coef<SCHEME>::cB2) * (w4 - w0);
+                    }
+                    s = A1 * ax - B1 * bx;
+                }
+                s += am * (m0 - q0);
+                s += ap * (m2 - q2);
+                s += bm * (m0 - m2);
+                s += bp * (q0 - q2);
+                y += tscale * s;
+            }
+            *yo = y;
+            w0 = w1; w1 = w2; w2 = w3; w3 = w4;
+            m0 = m1; m1 = m2;
+            q0 = q1; q1 = q2;
+        };
+        if (jn - jc == CH) {
+#pragma unroll
+            for (int k = 0; k < CH; ++k) row_out(jc + k, yout + (size_t)k * nx);
+        } else {
+            for (int j = jc; j < jn; ++j, yout += nx) row_out(j, yout);
+        }
+        __syncthreads();
+        // the third chunk ahead into the slots this chunk no longer needs
+        const int ra = jc + 3 * CH + 2, rb = min(jc + 4 * CH + 1, j_end + 1);
+        if (ra <= rb) march_load<T, MW>(X, ring, nx, nv, x0, ra, rb);
+        cp_async_commit();
+    }
+}
+
 template <int SCHEME, int MODE, typename T>
 __global__ void __launch_bounds__(WTHREADS, 4)
 k_bracket_wide(const T* __restrict__ X, const T* __restrict__ Xh, T* __restrict__ Y,
