@@ -381,13 +381,17 @@ BATCH_SPECS = [(64, 128, vo.f0_landau(0.1, 0.5), 4 * np.pi, 0.1),
                (64, 512, vo.f0_bump_on_tail(0.04, 0.3), 2 * np.pi / 0.3, 0.1)]
 
 
-def test_batch_step_equals_single_steps():
+@pytest.mark.parametrize("shape", [None, "2,1,0", "8,2,1", "4,0,1"])
+def test_batch_step_equals_single_steps(monkeypatch, shape):
     """A lockstep batch of uneven instances (every kernel launched once for
     the table, per-instance masks) follows each instance's own time step:
-    same Picard passes, GMRES counts within one, f to 1e-10."""
+    same Picard passes, GMRES counts within one, f to 1e-10.  Autotuned, and
+    with fixed shapes "FFT rows per CTA, tridiagonal kind, four-step FFT"."""
     from vivlasov1d_b200.batch import Batch
     batch_runs = [_small_run(*s) for s in BATCH_SPECS]
     single_runs = [_small_run(*s) for s in BATCH_SPECS]
+    if shape:
+        monkeypatch.setenv("VV_BATCH_SHAPE", shape)
     batch = Batch(batch_runs)
     for _ in range(3):
         rb = batch.step()
@@ -398,10 +402,13 @@ def test_batch_step_equals_single_steps():
     assert batch.launch_count() > 0
 
 
-def test_batch_graph_equals_host_driven(monkeypatch):
+@pytest.mark.parametrize("shape", ["4,0,0", "4,1,1"])
+def test_batch_graph_equals_host_driven(monkeypatch, shape):
     """The batch graph (conditional loops folded over the instance masks)
-    and the host-driven loop over the same kernels give identical bits."""
+    and the host-driven loop over the same kernels (one fixed shape) give
+    identical bits."""
     from vivlasov1d_b200.batch import Batch
+    monkeypatch.setenv("VV_BATCH_SHAPE", shape)
     graph_runs = [_small_run(*s) for s in BATCH_SPECS]
     monkeypatch.setenv("VV_GRAPH", "0")
     host_runs = [_small_run(*s) for s in BATCH_SPECS]

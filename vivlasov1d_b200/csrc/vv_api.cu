@@ -408,11 +408,15 @@ int raise_smem_limits(int* limit_out) {
         VV_SET_MARCH(1) VV_SET_MARCH(2) VV_SET_MARCH(4)
 #undef VV_SET_MARCH
         smem_set((const void*)vv::k_tridiag_modes_adjT, optin, lowest, e);
-        smem_set((const void*)vv::k_b_rfft<double, double>, optin, lowest, e);
-        smem_set((const void*)vv::k_b_rfft<double, float>, optin, lowest, e);
-        smem_set((const void*)vv::k_b_rfft<float, float>, optin, lowest, e);
-        smem_set((const void*)vv::k_b_irfft<double, double>, optin, lowest, e);
-        smem_set((const void*)vv::k_b_irfft<float, float>, optin, lowest, e);
+#define VV_SET_BFFT(FS)                                                         \
+    smem_set((const void*)vv::k_b_rfft<double, double, FS>, optin, lowest, e);  \
+    smem_set((const void*)vv::k_b_rfft<double, float, FS>, optin, lowest, e);   \
+    smem_set((const void*)vv::k_b_rfft<float, float, FS>, optin, lowest, e);    \
+    smem_set((const void*)vv::k_b_irfft<double, double, FS>, optin, lowest, e); \
+    smem_set((const void*)vv::k_b_irfft<float, float, FS>, optin, lowest, e);
+        VV_SET_BFFT(true)
+        VV_SET_BFFT(false)
+#undef VV_SET_BFFT
         smem_set((const void*)vv::k_b_tridiag<double, true>, optin, lowest, e);
         smem_set((const void*)vv::k_b_tridiag<float, true>, optin, lowest, e);
         smem_set((const void*)vv::k_b_tridiag<double, false>, optin, lowest, e);
@@ -1810,6 +1814,7 @@ struct vv_batch {
     bool mixed;
     int scheme;
     int R;                       // FFT rows per CTA
+    int fft4;                    // x-FFTs: 1 four-step register/shuffle, 0 radix-2
     int tri_kind;                // tridiagonal solves: 0 CTA per mode (tables staged), 1 warp per mode,
                                  // 2 CTA per mode (tables through L1)
     size_t smem_tri_stage, smem_tri_plain;
@@ -1882,12 +1887,18 @@ int b_pc(vv_batch* b, int l, bool from_tmp64, int dst) {
     const vv::BInst* tab = b->tab;
     const int* L = blist(b, l);
     const dim3 rt(32 * b->R);
-    if (from_tmp64) TRY(blaunch(b, vv::k_b_rfft<double, T>, vv::F_ROWS, rt, b->smem_rfft, tab, L, b->n, 1));
-    else TRY(blaunch(b, vv::k_b_rfft<T, T>, vv::F_ROWS, rt, b->smem_rfft, tab, L, b->n, 0));
+    if (b->fft4) {
+        if (from_tmp64) TRY(blaunch(b, vv::k_b_rfft<double, T, true>, vv::F_ROWS, rt, b->smem_rfft, tab, L, b->n, 1));
+        else TRY(blaunch(b, vv::k_b_rfft<T, T, true>, vv::F_ROWS, rt, b->smem_rfft, tab, L, b->n, 0));
+    } else {
+        if (from_tmp64) TRY(blaunch(b, vv::k_b_rfft<double, T, false>, vv::F_ROWS, rt, b->smem_rfft, tab, L, b->n, 1));
+        else TRY(blaunch(b, vv::k_b_rfft<T, T, false>, vv::F_ROWS, rt, b->smem_rfft, tab, L, b->n, 0));
+    }
     if (b->tri_kind == 1) TRY(blaunch(b, vv::k_b_tridiag_w<T>, vv::F_MODES, 32 * vv::TRIW_WARPS, 0, tab, L, b->n));
     else if (b->tri_kind == 2) TRY(blaunch(b, vv::k_b_tridiag<T, false>, vv::F_MODES, vv::TRI_THREADS, b->smem_tri_plain, tab, L, b->n));
     else TRY(blaunch(b, vv::k_b_tridiag<T, true>, vv::F_MODES, vv::TRI_THREADS, b->smem_tri_stage, tab, L, b->n));
-    return blaunch(b, vv::k_b_irfft<T, T>, vv::F_ROWS, rt, b->smem_irfft, tab, L, b->n, dst);
+    if (b->fft4) return blaunch(b, vv::k_b_irfft<T, T, true>, vv::F_ROWS, rt, b->smem_irfft, tab, L, b->n, dst);
+    return blaunch(b, vv::k_b_irfft<T, T, false>, vv::F_ROWS, rt, b->smem_irfft, tab, L, b->n, dst);
 }
 
 template <int S, typename T>
@@ -2089,11 +2100,13 @@ int b_dispatch_host(vv_batch* b) {
     }
 }
 
-// Launch shape of the preconditioner kernels: rows per CTA of the x-FFTs and
-// the tridiagonal variant (work items per instance and shared memory).
-void b_shape(vv_batch* b, std::vector<vv::BInst>& tab, int R, int tri_kind) {
+// Launch shape of the preconditioner kernels: rows per CTA of the x-FFTs,
+// the tridiagonal variant and the FFT kind (work items per instance and
+// shared memory).
+void b_shape(vv_batch* b, std::vector<vv::BInst>& tab, int R, int tri_kind, int fft4) {
     b->R = R;
     b->tri_kind = tri_kind;
+    b->fft4 = fft4;
     const bool tri_warp = tri_kind == 1;
     const size_t csz = b->mixed ? sizeof(float2) : sizeof(double2);
     for (int f = 0; f < vv::NFAM; ++f) b->tot[f] = 0;
@@ -2107,6 +2120,10 @@ void b_shape(vv_batch* b, std::vector<vv::BInst>& tab, int R, int tri_kind) {
         for (int f = 0; f < vv::NFAM; ++f) b->tot[f] += I.cnt[f];
         b->smem_rfft = std::max(b->smem_rfft, fft_smem(0, c->M, R, csz, false));
         b->smem_irfft = std::max(b->smem_irfft, fft_smem(0, c->M, R, csz, true));
+        if (fft4 && c->M >= 32 && c->M <= 128) {   // the lengths k_b_rfft/k_b_irfft run four-step
+            b->smem_rfft = std::max(b->smem_rfft, fft_smem(1, c->M, R, csz, false));
+            b->smem_irfft = std::max(b->smem_irfft, fft_smem(1, c->M, R, csz, true));
+        }
     }
 }
 
@@ -2119,7 +2136,8 @@ int b_apply_shape(vv_batch* b, const std::vector<vv::BInst>& tab) {
 }
 
 // Batch autotuner: times the whole-table preconditioner (the step's largest
-// share) for FFT rows per CTA x tridiagonal variant and keeps the fastest.
+// share) for FFT kind x FFT rows per CTA x tridiagonal variant and keeps the
+// fastest.
 template <typename T>
 int b_autotune(vv_batch* b, std::vector<vv::BInst>& tab) {
     for (int i = 0; i < b->n; ++i) {
@@ -2130,10 +2148,11 @@ int b_autotune(vv_batch* b, std::vector<vv::BInst>& tab) {
     CK(cudaEventCreate(&e0));
     CK(cudaEventCreate(&e1));
     float best = 1e30f;
-    int bR = b->R, bW = b->tri_kind, r = VV_OK;
+    int bR = b->R, bW = b->tri_kind, bF = b->fft4, r = VV_OK;
+    for (int f4 = 0; f4 <= 1 && r == VV_OK; ++f4)
     for (int tw = 0; tw <= 2 && r == VV_OK; ++tw) {
         for (int R = 2; R <= 8 && r == VV_OK; R *= 2) {
-            b_shape(b, tab, R, tw);
+            b_shape(b, tab, R, tw, f4);
             if ((r = b_apply_shape(b, tab)) != VV_OK) break;
             for (int k = 0; k < 2 && r == VV_OK; ++k) r = b_pc<T>(b, vv::L_ALL, false, vv::BD_B);
             cudaEventRecord(e0, b->st);
@@ -2142,18 +2161,20 @@ int b_autotune(vv_batch* b, std::vector<vv::BInst>& tab) {
             float ms = 0.f;
             const bool timed = r == VV_OK && cudaEventSynchronize(e1) == cudaSuccess &&
                                cudaEventElapsedTime(&ms, e0, e1) == cudaSuccess;
-            if (timed && getenv("VV_DEBUG")) fprintf(stderr, "[vv_batch] tune R=%d tri=%d: %.1f us\n", R, tw, ms * 200.f);
+            if (timed && getenv("VV_DEBUG"))
+                fprintf(stderr, "[vv_batch] tune fft4=%d R=%d tri=%d: %.1f us\n", f4, R, tw, ms * 200.f);
             if (timed && ms < best) {
                 best = ms;
                 bR = R;
                 bW = tw;
+                bF = f4;
             }
         }
     }
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
     TRY(r);
-    b_shape(b, tab, bR, bW);
+    b_shape(b, tab, bR, bW, bF);
     return b_apply_shape(b, tab);
 }
 
@@ -2271,7 +2292,7 @@ int vv_batch_create(int n, vv_ctx* const* ctxs, const vv_state* states, vv_batch
         }
         b->smem_pois = std::max(b->smem_pois, c->smem_pois);
     }
-    b_shape(b, tab, 8, 0);   // the largest shared-memory shape, for the limit check
+    b_shape(b, tab, 8, 0, 1);   // the largest shared-memory shape, for the limit check
     {
         int limit = 0;
         int r = raise_smem_limits(&limit);
@@ -2310,11 +2331,19 @@ int vv_batch_create(int n, vv_ctx* const* ctxs, const vv_state* states, vv_batch
     // empty lists, then the list of every instance
     if (cudaMemsetAsync(b->lists, 0, (size_t)vv::NLIST * b->list_words * sizeof(int), b->st) != cudaSuccess)
         return fail_b(fail_cuda(cudaGetLastError(), "batch lists"));
-    b_shape(b, tab, 4, 0);
+    b_shape(b, tab, 4, 0, 0);
     if ((r = b_apply_shape(b, tab)) != VV_OK) return fail_b(r);
     {
+        // VV_BATCH_SHAPE="R,tri,fft4" fixes the shape (tests, profiling); else the autotuner picks it
+        const char* bs = getenv("VV_BATCH_SHAPE");
+        int fR = 0, fT = 0, fF = 0;
+        const bool fixed = bs && sscanf(bs, "%d,%d,%d", &fR, &fT, &fF) == 3 && (fR == 2 || fR == 4 || fR == 8) &&
+                           fT >= 0 && fT <= 2 && (fF == 0 || fF == 1);
         const char* at = getenv("VV_AUTOTUNE");
-        if (!(at && at[0] == '0')) {
+        if (fixed) {
+            b_shape(b, tab, fR, fT, fF);
+            if ((r = b_apply_shape(b, tab)) != VV_OK) return fail_b(r);
+        } else if (!(at && at[0] == '0')) {
             r = b->mixed ? b_autotune<float>(b, tab) : b_autotune<double>(b, tab);
             if (r != VV_OK) return fail_b(r);
         }

@@ -107,11 +107,23 @@ __global__ void __launch_bounds__(WTHREADS, 4) k_b_bracket(const BInst* __restri
 
 // ---- preconditioner ---------------------------------------------------------
 // rFFT rows: input FP64 tmp (right-hand side) or the GMRES-precision scratch
-template <typename TI, typename R>
+// FS: the four-step register/shuffle FFT for rows of 64 to 256 points (a
+// switch on each instance's half length M; longer rows would raise the
+// register count of every instance's blocks), else the radix-2 warp FFT
+template <typename TI, typename R, bool FS>
 __global__ void k_b_rfft(const BInst* __restrict__ tab, const int* __restrict__ L, int n, int from_tmp64) {
     for_work<F_ROWS>(tab, L, n, [&](const BInst& I, int local) {
         const TI* X = from_tmp64 ? (const TI*)I.tmp : (const TI*)I.tmpT;
-        rfft_rows_block<TI, R>(X, (typename Cplx<R>::type*)I.specT, I.pp, local);
+        auto* spec = (typename Cplx<R>::type*)I.specT;
+        if (FS) {
+            switch (I.pp.M) {
+                case 32: rfft4_block<TI, R, 1>(X, spec, I.pp, local); return;
+                case 64: rfft4_block<TI, R, 2>(X, spec, I.pp, local); return;
+                case 128: rfft4_block<TI, R, 4>(X, spec, I.pp, local); return;
+                default: break;
+            }
+        }
+        rfft_rows_block<TI, R>(X, spec, I.pp, local);
     });
 }
 
@@ -136,13 +148,22 @@ __global__ void __launch_bounds__(32 * TRIW_WARPS) k_b_tridiag_w(const BInst* __
 
 enum BDst { BD_B = 0, BD_V0 = 1, BD_VNEXT = 2 };
 
-template <typename R, typename TO>
+template <typename R, typename TO, bool FS>
 __global__ void k_b_irfft(const BInst* __restrict__ tab, const int* __restrict__ L, int n, int dst) {
     for_work<F_ROWS>(tab, L, n, [&](const BInst& I, int local) {
         TO* Y = (TO*)I.bT;
         if (dst == BD_V0) Y = (TO*)I.V;
         else if (dst == BD_VNEXT) Y = (TO*)I.V + (size_t)(I.ds->it + 1) * I.ncell;
-        irfft_rows_block<R, TO>((const typename Cplx<R>::type*)I.specT, Y, I.pp, local);
+        const auto* spec = (const typename Cplx<R>::type*)I.specT;
+        if (FS) {
+            switch (I.pp.M) {
+                case 32: irfft4_block<R, TO, 1>(spec, Y, I.pp, local); return;
+                case 64: irfft4_block<R, TO, 2>(spec, Y, I.pp, local); return;
+                case 128: irfft4_block<R, TO, 4>(spec, Y, I.pp, local); return;
+                default: break;
+            }
+        }
+        irfft_rows_block<R, TO>(spec, Y, I.pp, local);
     });
 }
 

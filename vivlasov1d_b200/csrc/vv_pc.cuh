@@ -215,8 +215,12 @@ __global__ void k_irfft_rows(const typename Cplx<R>::type* __restrict__ spec, TO
 // across lanes with xor shuffles.  Lane l ends with X[k2 + E bitrev5(l)].
 // No shared memory and no barrier inside the transform.
 // ---------------------------------------------------------------------------
+// bit reversal of j over `bits` bits; a loop (not recursion) so that it folds
+// to a constant inside unrolled loops and register arrays stay in registers
 __host__ __device__ constexpr int crev(int j, int bits) {
-    return bits == 0 ? 0 : (((j & 1) << (bits - 1)) | crev(j >> 1, bits - 1));
+    int r = 0;
+    for (int b = 0; b < bits; ++b) r |= ((j >> b) & 1) << (bits - 1 - b);
+    return r;
 }
 __host__ __device__ constexpr int clog2(int n) { return n <= 1 ? 0 : 1 + clog2(n >> 1); }
 
@@ -292,7 +296,8 @@ __device__ __forceinline__ int zslot_of(int k) {
 // half spectrum written transposed: spec[k*nv + j].
 // dynamic smem: [M twiddles][RW x (M+1) half spectra][RW x 32(E+1) transform slots]
 template <typename TI, typename R, int E>
-__global__ void k_rfft4(const TI* __restrict__ X, typename Cplx<R>::type* __restrict__ spec, PcParams p) {
+__device__ __forceinline__ void rfft4_block(const TI* __restrict__ X, typename Cplx<R>::type* __restrict__ spec,
+                                            const PcParams& p, int bid) {
     using C = typename Cplx<R>::type;
     constexpr int M = 32 * E, LD = M + 1, ZS = 32 * (E + 1);
     extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -302,7 +307,7 @@ __global__ void k_rfft4(const TI* __restrict__ X, typename Cplx<R>::type* __rest
     const C* tw = reinterpret_cast<const C*>(p.tw);
     for (int k = threadIdx.x; k < M; k += blockDim.x) stw[k] = tw[k];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int j0 = blockIdx.x * p.R;
+    const int j0 = bid * p.R;
     const int j = j0 + warp;
     __syncthreads();
     if (warp < p.R && j < p.nv) {
@@ -344,20 +349,25 @@ __global__ void k_rfft4(const TI* __restrict__ X, typename Cplx<R>::type* __rest
     }
 }
 
+template <typename TI, typename R, int E>
+__global__ void k_rfft4(const TI* __restrict__ X, typename Cplx<R>::type* __restrict__ spec, PcParams p) {
+    rfft4_block<TI, R, E>(X, spec, p, blockIdx.x);
+}
+
 // spec[k*nv + j] -> RW rows of Y (one warp per row), normalised by 1/nx
 // dynamic smem: [M twiddles][RW x (M+1) half spectra][RW x 32(E+1) transform slots]
 template <typename R, typename TO, int E>
-__global__ void k_irfft4(const typename Cplx<R>::type* __restrict__ spec, TO* __restrict__ Y, PcParams p) {
+__device__ __forceinline__ void irfft4_block(const typename Cplx<R>::type* __restrict__ spec, TO* __restrict__ Y,
+                                             const PcParams& p, int bid) {
     using C = typename Cplx<R>::type;
     constexpr int M = 32 * E, LD = M + 1, ZS = 32 * (E + 1);
-    if (p.yidx) Y += (size_t)(*p.yidx + p.yoff) * p.ystride;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     C* stw = reinterpret_cast<C*>(smem_raw);
     C* rows = stw + M;
     C* zb = rows + p.R * LD;
     const C* tw = reinterpret_cast<const C*>(p.tw);
     for (int k = threadIdx.x; k < M; k += blockDim.x) stw[k] = tw[k];
-    const int j0 = blockIdx.x * p.R;
+    const int j0 = bid * p.R;
     const int nrow = min(p.R, p.nv - j0);
     for (int idx = threadIdx.x; idx < (M + 1) * p.R; idx += blockDim.x) {
         const int k = idx / p.R, r = idx - k * p.R;
@@ -394,6 +404,12 @@ __global__ void k_irfft4(const typename Cplx<R>::type* __restrict__ spec, TO* __
         row[2 * m] = (TO)(v.x * s);
         row[2 * m + 1] = (TO)(v.y * s);
     }
+}
+
+template <typename R, typename TO, int E>
+__global__ void k_irfft4(const typename Cplx<R>::type* __restrict__ spec, TO* __restrict__ Y, PcParams p) {
+    if (p.yidx) Y += (size_t)(*p.yidx + p.yoff) * p.ystride;
+    irfft4_block<R, TO, E>(spec, Y, p, blockIdx.x);
 }
 
 // ---------------------------------------------------------------------------
