@@ -49,7 +49,9 @@ struct vv_ctx {
     bool tri_stage32;
     // kernel variants (picked by the autotuner at vv_create)
     int fft_kind;      // 0: shared-memory radix-2 per warp, 1: four-step register/shuffle FFT
-    int tri_kind;      // 0: one CTA per mode (block scan), 1: one warp per mode
+    int tri_kind;      // 0: one CTA per mode (block scan), 1: one warp per mode (lines staged in shared
+                       // memory when tri_ws_smem fits smem_limit)
+    int smem_limit;    // dynamic shared memory per block on this device
     int narrow_bracket;  // 1: 32x16 tiles instead of 64x32
     int march;           // Jacobian stencil: 0 tiles, 128 or 256 the strip width of the marching kernel
     // pinned host staging
@@ -380,6 +382,18 @@ void smem_attributes(int optin, int& lowest, cudaError_t& e) {
 #undef VV_SET4
     set((const void*)vv::k_tridiag_modes<R, true>);
     set((const void*)vv::k_tridiag_modes<R, false>);
+    set((const void*)vv::k_tridiag_warp_staged<R>);
+    set((const void*)vv::k_b_tridiag_w<R>);
+    set((const void*)vv::k_b_rfftj<double, R>);
+    set((const void*)vv::k_b_rfftj<float, R>);
+    set((const void*)vv::k_b_irfftj<R, R>);
+    set((const void*)vv::k_b_tridiagj<R>);
+    set((const void*)vv::k_b_tridiagjs<R>);
+}
+
+// dynamic shared memory of the staged warp-per-mode tridiagonal solve
+size_t tri_ws_smem(int nv, size_t csz) {
+    return (size_t)vv::TRIW_WARPS * 2 * vv::tri_ws_slots(nv) * csz + 2 * vv::tri_ws_slots(nv) * (csz / 2);
 }
 
 int raise_smem_limits(int* limit_out) {
@@ -449,9 +463,14 @@ int pc_apply_t(vv_ctx* c, const TI* X, TO* Y, const int* yidx = nullptr, int yof
     t.alpha = D ? (const void*)c->alpha : (const void*)c->alpha32;
     t.gamma = D ? (const void*)c->gamma : (const void*)c->gamma32;
     t.dinv = D ? (const void*)c->dinv : (const void*)c->dinv32;
-    if (c->tri_kind == 1)
-        vv::k_tridiag_warp<R><<<(c->nmodes + vv::TRIW_WARPS - 1) / vv::TRIW_WARPS, 32 * vv::TRIW_WARPS, 0, c->st>>>(
-            spec, t);
+    if (c->tri_kind == 1) {
+        const unsigned g = (unsigned)((c->nmodes + vv::TRIW_WARPS - 1) / vv::TRIW_WARPS);
+        const size_t sm = tri_ws_smem(c->nv, sizeof(typename Cplx<R>::type));
+        if (sm <= (size_t)c->smem_limit)
+            vv::k_tridiag_warp_staged<R><<<g, 32 * vv::TRIW_WARPS, sm, c->st>>>(spec, t);
+        else
+            vv::k_tridiag_warp<R><<<g, 32 * vv::TRIW_WARPS, 0, c->st>>>(spec, t);
+    }
     else if (stage)
         vv::k_tridiag_modes<R, true><<<c->nmodes, vv::TRI_THREADS, sm_t, c->st>>>(spec, t);
     else
@@ -1394,6 +1413,7 @@ int vv_create(const vv_grid* grid, vv_ctx** out) {
             vv_destroy(c);
             return s;
         }
+        c->smem_limit = limit;
         const size_t need = std::max({c->smem_tri, c->mixed ? c->smem_tri32 : (size_t)0, c->smem_pois,
                                       fft_smem(0, M, c->pcR, sizeof(double2), true)});
         if (need > (size_t)limit) {
@@ -1815,9 +1835,15 @@ struct vv_batch {
     int scheme;
     int R;                       // FFT rows per CTA
     int fft4;                    // x-FFTs: 1 four-step register/shuffle, 0 radix-2
+    int pcj;                     // 1: preconditioner in the v-major layout (vv_pcj.cuh); fft4/R/tri_kind unused
+    bool pcj_ok;                 // every instance has M in 32..256 (the v-major kernels' lengths)
+    void* dinvJ;                 // device: v-major LU reciprocals of every instance (GMRES precision)
+    size_t smem_fftj;            // dynamic shared memory of the v-major FFT blocks
     int tri_kind;                // tridiagonal solves: 0 CTA per mode (tables staged), 1 warp per mode,
                                  // 2 CTA per mode (tables through L1)
-    size_t smem_tri_stage, smem_tri_plain;
+    size_t smem_tri_stage, smem_tri_plain, smem_tri_warp;
+    int nvmax;                   // largest velocity grid of the table
+    int smem_limit;              // dynamic shared memory per block available to the batch kernels
     double* wpart;               // device: per-warp partial sums of every instance
     vv::BInst* tab;              // device instance table
     int* lists;                  // device work lists (vv::NLIST of them)
@@ -1886,6 +1912,18 @@ template <typename T>
 int b_pc(vv_batch* b, int l, bool from_tmp64, int dst) {
     const vv::BInst* tab = b->tab;
     const int* L = blist(b, l);
+    if (b->pcj) {
+        const dim3 ft(vv::FJ_THREADS);
+        if (from_tmp64) TRY(blaunch(b, vv::k_b_rfftj<double, T>, vv::F_ROWS, ft, b->smem_fftj, tab, L, b->n, 1));
+        else TRY(blaunch(b, vv::k_b_rfftj<T, T>, vv::F_ROWS, ft, b->smem_fftj, tab, L, b->n, 0));
+        if (b->tri_kind == 1)
+            TRY(blaunch(b, vv::k_b_tridiagjs<T>, vv::F_MODES, 32 * vv::TRIW_WARPS, b->smem_tri_warp, tab, L, b->n,
+                        vv::tri_ws_slots(b->nvmax)));
+        else
+            TRY(blaunch(b, vv::k_b_tridiagj<T>, vv::F_MODES, 32,
+                        (size_t)64 * vv::TJ_RING * sizeof(typename Cplx<T>::type), tab, L, b->n));
+        return blaunch(b, vv::k_b_irfftj<T, T>, vv::F_ROWS, ft, b->smem_fftj, tab, L, b->n, dst);
+    }
     const dim3 rt(32 * b->R);
     if (b->fft4) {
         if (from_tmp64) TRY(blaunch(b, vv::k_b_rfft<double, T, true>, vv::F_ROWS, rt, b->smem_rfft, tab, L, b->n, 1));
@@ -1894,7 +1932,9 @@ int b_pc(vv_batch* b, int l, bool from_tmp64, int dst) {
         if (from_tmp64) TRY(blaunch(b, vv::k_b_rfft<double, T, false>, vv::F_ROWS, rt, b->smem_rfft, tab, L, b->n, 1));
         else TRY(blaunch(b, vv::k_b_rfft<T, T, false>, vv::F_ROWS, rt, b->smem_rfft, tab, L, b->n, 0));
     }
-    if (b->tri_kind == 1) TRY(blaunch(b, vv::k_b_tridiag_w<T>, vv::F_MODES, 32 * vv::TRIW_WARPS, 0, tab, L, b->n));
+    if (b->tri_kind == 1)
+        TRY(blaunch(b, vv::k_b_tridiag_w<T>, vv::F_MODES, 32 * vv::TRIW_WARPS, b->smem_tri_warp, tab, L, b->n,
+                    vv::tri_ws_slots(b->nvmax)));
     else if (b->tri_kind == 2) TRY(blaunch(b, vv::k_b_tridiag<T, false>, vv::F_MODES, vv::TRI_THREADS, b->smem_tri_plain, tab, L, b->n));
     else TRY(blaunch(b, vv::k_b_tridiag<T, true>, vv::F_MODES, vv::TRI_THREADS, b->smem_tri_stage, tab, L, b->n));
     if (b->fft4) return blaunch(b, vv::k_b_irfft<T, T, true>, vv::F_ROWS, rt, b->smem_irfft, tab, L, b->n, dst);
@@ -2103,10 +2143,11 @@ int b_dispatch_host(vv_batch* b) {
 // Launch shape of the preconditioner kernels: rows per CTA of the x-FFTs,
 // the tridiagonal variant and the FFT kind (work items per instance and
 // shared memory).
-void b_shape(vv_batch* b, std::vector<vv::BInst>& tab, int R, int tri_kind, int fft4) {
+void b_shape(vv_batch* b, std::vector<vv::BInst>& tab, int R, int tri_kind, int fft4, int pcj = 0) {
     b->R = R;
     b->tri_kind = tri_kind;
     b->fft4 = fft4;
+    b->pcj = pcj && b->pcj_ok;
     const bool tri_warp = tri_kind == 1;
     const size_t csz = b->mixed ? sizeof(float2) : sizeof(double2);
     for (int f = 0; f < vv::NFAM; ++f) b->tot[f] = 0;
@@ -2117,6 +2158,11 @@ void b_shape(vv_batch* b, std::vector<vv::BInst>& tab, int R, int tri_kind, int 
         I.pp.R = R;
         I.cnt[vv::F_ROWS] = (c->nv + R - 1) / R;
         I.cnt[vv::F_MODES] = tri_warp ? (c->nmodes + vv::TRIW_WARPS - 1) / vv::TRIW_WARPS : c->nmodes;
+        if (b->pcj) {
+            const int rb = vv::fj_rows_of(c->M);
+            I.cnt[vv::F_ROWS] = (c->nv + rb - 1) / rb;
+            I.cnt[vv::F_MODES] = tri_warp ? (c->nmodes + vv::TRIW_WARPS - 1) / vv::TRIW_WARPS : (c->nmodes + 31) / 32;
+        }
         for (int f = 0; f < vv::NFAM; ++f) b->tot[f] += I.cnt[f];
         b->smem_rfft = std::max(b->smem_rfft, fft_smem(0, c->M, R, csz, false));
         b->smem_irfft = std::max(b->smem_irfft, fft_smem(0, c->M, R, csz, true));
@@ -2148,11 +2194,13 @@ int b_autotune(vv_batch* b, std::vector<vv::BInst>& tab) {
     CK(cudaEventCreate(&e0));
     CK(cudaEventCreate(&e1));
     float best = 1e30f;
-    int bR = b->R, bW = b->tri_kind, bF = b->fft4, r = VV_OK;
-    for (int f4 = 0; f4 <= 1 && r == VV_OK; ++f4)
-    for (int tw = 0; tw <= 2 && r == VV_OK; ++tw) {
-        for (int R = 2; R <= 8 && r == VV_OK; R *= 2) {
-            b_shape(b, tab, R, tw, f4);
+    int bR = b->R, bW = b->tri_kind, bF = b->fft4, bJ = b->pcj, r = VV_OK;
+    for (int pj = 0; pj <= (b->pcj_ok ? 1 : 0) && r == VV_OK; ++pj)
+    for (int f4 = 0; f4 <= (pj ? 0 : 1) && r == VV_OK; ++f4)
+    for (int tw = 0; tw <= (pj ? 1 : 2) && r == VV_OK; ++tw) {
+        if (tw == 1 && b->smem_tri_warp > (size_t)b->smem_limit) continue;
+        for (int R = 2; R <= (pj ? 2 : 8) && r == VV_OK; R *= 2) {
+            b_shape(b, tab, R, tw, f4, pj);
             if ((r = b_apply_shape(b, tab)) != VV_OK) break;
             for (int k = 0; k < 2 && r == VV_OK; ++k) r = b_pc<T>(b, vv::L_ALL, false, vv::BD_B);
             cudaEventRecord(e0, b->st);
@@ -2162,19 +2210,20 @@ int b_autotune(vv_batch* b, std::vector<vv::BInst>& tab) {
             const bool timed = r == VV_OK && cudaEventSynchronize(e1) == cudaSuccess &&
                                cudaEventElapsedTime(&ms, e0, e1) == cudaSuccess;
             if (timed && getenv("VV_DEBUG"))
-                fprintf(stderr, "[vv_batch] tune fft4=%d R=%d tri=%d: %.1f us\n", f4, R, tw, ms * 200.f);
+                fprintf(stderr, "[vv_batch] tune pcj=%d fft4=%d R=%d tri=%d: %.1f us\n", pj, f4, R, tw, ms * 200.f);
             if (timed && ms < best) {
                 best = ms;
                 bR = R;
                 bW = tw;
                 bF = f4;
+                bJ = pj;
             }
         }
     }
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
     TRY(r);
-    b_shape(b, tab, bR, bW, bF);
+    b_shape(b, tab, bR, bW, bF, bJ);
     return b_apply_shape(b, tab);
 }
 
@@ -2204,7 +2253,8 @@ int vv_batch_destroy(vv_batch* b) {
     for (auto s : b->cs) if (s) cudaStreamDestroy(s);
     if (b->ex) cudaGraphExecDestroy(b->ex);
     if (b->g) cudaGraphDestroy(b->g);
-    for (void* p : {(void*)b->tab, (void*)b->lists, (void*)b->counts, (void*)b->flag, (void*)b->gather, (void*)b->wpart})
+    for (void* p : {(void*)b->tab, (void*)b->lists, (void*)b->counts, (void*)b->flag, (void*)b->gather, (void*)b->wpart,
+                    b->dinvJ})
         if (p) cudaFree(p);
     if (b->hflag) cudaFreeHost(b->hflag);
     if (b->hcounts) cudaFreeHost(b->hcounts);
@@ -2289,6 +2339,8 @@ int vv_batch_create(int n, vv_ctx* const* ctxs, const vv_state* states, vv_batch
             const size_t np = (size_t)c->nv + (c->nv + ch - 1) / ch;
             b->smem_tri_stage = std::max(b->smem_tri_stage, np * (b->mixed ? 24 : 48));
             b->smem_tri_plain = std::max(b->smem_tri_plain, np * (b->mixed ? sizeof(float2) : sizeof(double2)));
+            b->smem_tri_warp = std::max(b->smem_tri_warp, tri_ws_smem(c->nv, b->mixed ? sizeof(float2) : sizeof(double2)));
+            b->nvmax = std::max(b->nvmax, c->nv);
         }
         b->smem_pois = std::max(b->smem_pois, c->smem_pois);
     }
@@ -2297,8 +2349,38 @@ int vv_batch_create(int n, vv_ctx* const* ctxs, const vv_state* states, vv_batch
         int limit = 0;
         int r = raise_smem_limits(&limit);
         if (r != VV_OK) return fail_b(r);
+        b->smem_limit = limit;
         if (std::max({b->smem_rfft, b->smem_irfft, b->smem_tri_stage, b->smem_pois}) > (size_t)limit)
             return fail_b(VV_ERR_UNSUPPORTED);
+    }
+    // the v-major preconditioner layout: lengths, shared memory and the v-major LU tables
+    {
+        const size_t csz = b->mixed ? sizeof(float2) : sizeof(double2);
+        b->pcj_ok = true;
+        size_t words = 0;
+        for (int i = 0; i < n; ++i) {
+            const int slots = vv::fj_slots_of(ctxs[i]->M);
+            if (slots < 0) b->pcj_ok = false;
+            else b->smem_fftj = std::max(b->smem_fftj, (size_t)slots * csz);
+            words += (size_t)ctxs[i]->nmodes * ctxs[i]->nv;
+        }
+        if (b->smem_fftj > (size_t)b->smem_limit) b->pcj_ok = false;
+        if (b->pcj_ok) {
+            if (cudaMalloc(&b->dinvJ, words * csz) != cudaSuccess) return fail_b(VV_ERR_ALLOC);
+            size_t off = 0;
+            for (int i = 0; i < n; ++i) {
+                const vv_ctx* c = ctxs[i];
+                const size_t cnt = (size_t)c->nmodes * c->nv;
+                const unsigned g = (unsigned)((cnt + 255) / 256);
+                char* dst = (char*)b->dinvJ + off * csz;
+                if (b->mixed) vv::k_modes_to_vmajor<float2><<<g, 256>>>(c->dinv32, (float2*)dst, c->nmodes, c->nv);
+                else vv::k_modes_to_vmajor<double2><<<g, 256>>>(c->dinv, (double2*)dst, c->nmodes, c->nv);
+                tab[i].dinvJ = dst;
+                off += cnt;
+            }
+            const cudaError_t e = cudaDeviceSynchronize();
+            if (e != cudaSuccess) return fail_b(fail_cuda(e, "v-major LU tables"));
+        }
     }
     // per-warp partials: (restart + 2) columns of 8 vblk per instance
     {
@@ -2334,14 +2416,16 @@ int vv_batch_create(int n, vv_ctx* const* ctxs, const vv_state* states, vv_batch
     b_shape(b, tab, 4, 0, 0);
     if ((r = b_apply_shape(b, tab)) != VV_OK) return fail_b(r);
     {
-        // VV_BATCH_SHAPE="R,tri,fft4" fixes the shape (tests, profiling); else the autotuner picks it
+        // VV_BATCH_SHAPE="R,tri,fft4[,vmajor]" fixes the shape (tests, profiling); else the autotuner picks it
         const char* bs = getenv("VV_BATCH_SHAPE");
-        int fR = 0, fT = 0, fF = 0;
-        const bool fixed = bs && sscanf(bs, "%d,%d,%d", &fR, &fT, &fF) == 3 && (fR == 2 || fR == 4 || fR == 8) &&
-                           fT >= 0 && fT <= 2 && (fF == 0 || fF == 1);
+        int fR = 0, fT = 0, fF = 0, fJ = 0;
+        const int nf = bs ? sscanf(bs, "%d,%d,%d,%d", &fR, &fT, &fF, &fJ) : 0;
+        const bool fixed = nf >= 3 && (fR == 2 || fR == 4 || fR == 8) && fT >= 0 && fT <= 2 && (fF == 0 || fF == 1) &&
+                           (fJ == 0 || (fJ == 1 && b->pcj_ok)) &&
+                           !(fT == 1 && b->smem_tri_warp > (size_t)b->smem_limit);
         const char* at = getenv("VV_AUTOTUNE");
         if (fixed) {
-            b_shape(b, tab, fR, fT, fF);
+            b_shape(b, tab, fR, fT, fF, fJ);
             if ((r = b_apply_shape(b, tab)) != VV_OK) return fail_b(r);
         } else if (!(at && at[0] == '0')) {
             r = b->mixed ? b_autotune<float>(b, tab) : b_autotune<double>(b, tab);

@@ -15,6 +15,7 @@
 #pragma once
 #include "vv_bracket.cuh"
 #include "vv_pc.cuh"
+#include "vv_pcj.cuh"
 #include "vv_vec.cuh"
 
 namespace vv {
@@ -41,6 +42,8 @@ struct BInst {
     double *Fh, *tmp, *fl, *part, *mom_part, *hxp, *v, *scal;
     // GMRES buffers in the GMRES precision: basis, operator scratch, rhs, solution, spectrum
     void *V, *tmpT, *bT, *xT, *specT;
+    // LU reciprocals of the preconditioner, v-major (dinvJ[j*(M+1) + k]; the v-major layout)
+    const void* dinvJ;
     // per-warp partial sums of the GMRES reductions: (restart + 2) columns of 8 * vblk
     double* wpart;
 };
@@ -137,16 +140,134 @@ __global__ void __launch_bounds__(TRI_THREADS) k_b_tridiag(const BInst* __restri
     });
 }
 
+// warp per mode, lines staged in the warp's shared-memory slice and the
+// instance's alpha/gamma tables in the CTA's (dynamic smem:
+// TRIW_WARPS x 2 x tri_ws_slots(largest nv) complex + 2 x as many real)
 template <typename R>
 __global__ void __launch_bounds__(32 * TRIW_WARPS) k_b_tridiag_w(const BInst* __restrict__ tab, const int* __restrict__ L,
-                                                                int n) {
+                                                                int n, int nsmax) {
+    using C = typename Cplx<R>::type;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
     for_work<F_MODES>(tab, L, n, [&](const BInst& I, int local) {
-        const int k = local * TRIW_WARPS + (threadIdx.x >> 5);
-        if (k < I.tp.nmodes) tridiag_warp_mode<R>((typename Cplx<R>::type*)I.specT, I.tp, k);
+        const int w = threadIdx.x >> 5;
+        const int k = local * TRIW_WARPS + w;
+        const int ns = tri_ws_slots(I.tp.nv);
+        C* sb = reinterpret_cast<C*>(smem_raw) + (size_t)w * 2 * ns;
+        R* sal = reinterpret_cast<R*>(reinterpret_cast<C*>(smem_raw) + (size_t)TRIW_WARPS * 2 * nsmax);
+        R* sga = sal + ns;
+        tri_ws_stage_tables<R>(I.tp, sal, sga);
+        if (k < I.tp.nmodes) tri_ws_stage_line<R>((const C*)I.specT, I.tp, k, sb, sb + ns);
+        cp_async_commit();
+        cp_async_wait0();
+        __syncthreads();
+        if (k < I.tp.nmodes) tridiag_warp_staged<R>((C*)I.specT, I.tp, k, sb, sb + ns, sal, sga);
     });
 }
 
 enum BDst { BD_B = 0, BD_V0 = 1, BD_VNEXT = 2 };
+
+// ---- preconditioner, v-major spectrum layout (vv_pcj.cuh) ---------------------
+// x-FFTs of RB rows per work item (RB set by the instance's M = 32..256)
+template <typename TI, typename R>
+__global__ void __launch_bounds__(FJ_THREADS) k_b_rfftj(const BInst* __restrict__ tab, const int* __restrict__ L, int n,
+                                                        int from_tmp64) {
+    for_work<F_ROWS>(tab, L, n, [&](const BInst& I, int local) {
+        const TI* X = from_tmp64 ? (const TI*)I.tmp : (const TI*)I.tmpT;
+        auto* spec = (typename Cplx<R>::type*)I.specT;
+        switch (I.pp.M) {
+            case 32: rfftj_block<TI, R, 32>(X, spec, I.pp, local); break;
+            case 64: rfftj_block<TI, R, 64>(X, spec, I.pp, local); break;
+            case 128: rfftj_block<TI, R, 128>(X, spec, I.pp, local); break;
+            default: rfftj_block<TI, R, 256>(X, spec, I.pp, local); break;
+        }
+    });
+}
+
+// LU solves: one lane per x mode, 32 modes per work item (dynamic smem:
+// the warp's ring, 64 TJ_RING complex)
+template <typename R>
+__global__ void __launch_bounds__(32) k_b_tridiagj(const BInst* __restrict__ tab, const int* __restrict__ L, int n) {
+    using C = typename Cplx<R>::type;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    for_work<F_MODES>(tab, L, n, [&](const BInst& I, int local) {
+        const int k = local * 32 + (int)threadIdx.x;
+        tridiagj_lane<R>((C*)I.specT, (const C*)I.dinvJ, I.tp, k, reinterpret_cast<C*>(smem_raw));
+    });
+}
+
+template <typename R, typename TO>
+__global__ void __launch_bounds__(FJ_THREADS) k_b_irfftj(const BInst* __restrict__ tab, const int* __restrict__ L, int n,
+                                                         int dst) {
+    for_work<F_ROWS>(tab, L, n, [&](const BInst& I, int local) {
+        TO* Y = (TO*)I.bT;
+        if (dst == BD_V0) Y = (TO*)I.V;
+        else if (dst == BD_VNEXT) Y = (TO*)I.V + (size_t)(I.ds->it + 1) * I.ncell;
+        const auto* spec = (const typename Cplx<R>::type*)I.specT;
+        switch (I.pp.M) {
+            case 32: irfftj_block<R, TO, 32>(spec, Y, I.pp, local); break;
+            case 64: irfftj_block<R, TO, 64>(spec, Y, I.pp, local); break;
+            case 128: irfftj_block<R, TO, 128>(spec, Y, I.pp, local); break;
+            default: irfftj_block<R, TO, 256>(spec, Y, I.pp, local); break;
+        }
+    });
+}
+
+// LU solves on the v-major layout by the staged warp solve: TRIW_WARPS
+// consecutive modes per work item, one warp per mode; the CTA stages the
+// modes' columns together (a row's TRIW_WARPS values are one 32-byte sector
+// in FP32) into the warps' slices and writes the solutions back the same
+// way (dynamic smem as k_b_tridiag_w)
+template <typename R>
+__global__ void __launch_bounds__(32 * TRIW_WARPS) k_b_tridiagjs(const BInst* __restrict__ tab, const int* __restrict__ L,
+                                                                int n, int nsmax) {
+    using C = typename Cplx<R>::type;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    for_work<F_MODES>(tab, L, n, [&](const BInst& I, int local) {
+        const int nv = I.tp.nv, nm = I.tp.nmodes;
+        const int CH = (nv + 31) / 32;
+        const int ns = tri_ws_slots(nv);
+        const int w = threadIdx.x >> 5;
+        const int k0 = local * TRIW_WARPS;
+        C* base = reinterpret_cast<C*>(smem_raw);
+        R* sal = reinterpret_cast<R*>(base + (size_t)TRIW_WARPS * 2 * nsmax);
+        R* sga = sal + ns;
+        C* spec = (C*)I.specT;
+        const C* dj = (const C*)I.dinvJ;
+        tri_ws_stage_tables<R>(I.tp, sal, sga);
+        for (int t = threadIdx.x; t < nv * TRIW_WARPS; t += blockDim.x) {
+            const int j = t / TRIW_WARPS, m = t % TRIW_WARPS;
+            const int k = k0 + m;
+            if (k < nm) {
+                C* sb = base + (size_t)m * 2 * ns;
+                const int q = j + j / CH;
+                cp_async_elem(&sb[q], &spec[(size_t)j * nm + k]);
+                cp_async_elem(&sb[ns + q], &dj[(size_t)j * nm + k]);
+            }
+        }
+        cp_async_commit();
+        cp_async_wait0();
+        __syncthreads();
+        if (k0 + w < nm) {
+            C* sb = base + (size_t)w * 2 * ns;
+            tri_ws_solve<R>(sb, sb + ns, sal, sga, reinterpret_cast<const C*>(I.tp.lambda)[k0 + w], nv);
+        }
+        __syncthreads();
+        for (int t = threadIdx.x; t < nv * TRIW_WARPS; t += blockDim.x) {
+            const int j = t / TRIW_WARPS, m = t % TRIW_WARPS;
+            const int k = k0 + m;
+            if (k < nm) spec[(size_t)j * nm + k] = base[(size_t)m * 2 * ns + j + j / CH];
+        }
+    });
+}
+
+// dst[j*nm + k] = src[k*nv + j]: the v-major copy of a mode-major table
+template <typename C>
+__global__ void k_modes_to_vmajor(const C* __restrict__ src, C* __restrict__ dst, int nm, int nv) {
+    const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= (size_t)nm * nv) return;
+    const int j = (int)(i / nm), k = (int)(i % nm);
+    dst[i] = src[(size_t)k * nv + j];
+}
 
 template <typename R, typename TO, bool FS>
 __global__ void k_b_irfft(const BInst* __restrict__ tab, const int* __restrict__ L, int n, int dst) {

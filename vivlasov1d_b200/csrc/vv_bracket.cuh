@@ -481,16 +481,6 @@ template <typename T> struct MarchShape;
 template <> struct MarchShape<double> { static constexpr int CH = 8, NR = 32; };
 template <> struct MarchShape<float> { static constexpr int CH = 16, NR = 64; };
 
-VV_DEV void cp_async_16(void* smem, const void* gmem, int src_bytes) {
-    const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
-    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(s), "l"(gmem), "r"(src_bytes));
-}
-VV_DEV void cp_async_8(void* smem, const void* gmem, int src_bytes) {
-    const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
-    asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(s), "l"(gmem), "r"(src_bytes));
-}
-VV_DEV void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::); }
-VV_DEV void cp_async_wait2() { asm volatile("cp.async.wait_group 2;\n" ::); }
 
 // ring row layout: [pad][2 left halo][MW columns][2 right halo][pad]; the
 // main columns start at LP elements (16 bytes), every row is 16-byte aligned

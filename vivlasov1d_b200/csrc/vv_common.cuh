@@ -80,3 +80,30 @@ struct KSum {
     }
     VV_DEV double value() const { return s + c; }
 };
+
+// Asynchronous global -> shared copies (cp.async, sm_80+): a zero src_bytes
+// fills the destination with zeros and reads nothing.
+VV_DEV void cp_async_16(void* smem, const void* gmem, int src_bytes) {
+    const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(s), "l"(gmem), "r"(src_bytes));
+}
+VV_DEV void cp_async_8(void* smem, const void* gmem, int src_bytes) {
+    const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(s), "l"(gmem), "r"(src_bytes));
+}
+VV_DEV void cp_async_4(void* smem, const void* gmem) {
+    const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4, 4;\n" ::"r"(s), "l"(gmem));
+}
+// one element of 4, 8 or 16 bytes
+template <typename E>
+VV_DEV void cp_async_elem(E* smem, const E* gmem) {
+    static_assert(sizeof(E) == 4 || sizeof(E) == 8 || sizeof(E) == 16, "cp.async copies 4, 8 or 16 bytes");
+    if (sizeof(E) == 16) cp_async_16(smem, gmem, 16);
+    else if (sizeof(E) == 8) cp_async_8(smem, gmem, 8);
+    else cp_async_4(smem, gmem);
+}
+// the waits clobber memory so that no shared-memory read moves above them
+VV_DEV void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+VV_DEV void cp_async_wait2() { asm volatile("cp.async.wait_group 2;\n" ::: "memory"); }
+VV_DEV void cp_async_wait0() { asm volatile("cp.async.wait_group 0;\n" ::: "memory"); }

@@ -496,15 +496,17 @@ __device__ __forceinline__ void tridiag_mode(typename Cplx<R>::type* __restrict_
     const R* alpha_g = reinterpret_cast<const R*>(p.alpha);
     const R* gamma_g = reinterpret_cast<const R*>(p.gamma);
     const C lam = reinterpret_cast<const C*>(p.lambda)[k];
-    for (int r = threadIdx.x; r < nv; r += TRI_THREADS) {
+    for (int r = threadIdx.x; r < nv; r += TRI_THREADS) {   // every copy in flight at once
         const int q = r + r / CH;
-        b[q] = line[r];
+        cp_async_elem(&b[q], &line[r]);
         if (STAGE) {
-            di[q] = dinv_g[r];
-            al[q] = alpha_g[r];
-            ga[q] = gamma_g[r];
+            cp_async_elem(&di[q], &dinv_g[r]);
+            cp_async_elem(&al[q], &alpha_g[r]);
+            cp_async_elem(&ga[q], &gamma_g[r]);
         }
     }
+    cp_async_commit();
+    cp_async_wait0();
     __syncthreads();
     // accessors: row r at padded index q (tables staged or read through L1/L2)
     auto DI = [&](int r, int q) -> C { return STAGE ? di[q] : dinv_g[r]; };
@@ -591,7 +593,11 @@ __device__ __forceinline__ C warp_scan_aff(Aff<C> a, bool forward) {
 // [l*CH, (l+1)*CH) of the mode's v line; the LU reciprocals and the
 // alpha/gamma tables are read through L1 in the lane's own contiguous chunk.
 // No shared memory, no block barrier.
-constexpr int TRIW_WARPS = 8;
+constexpr int TRIW_WARPS = 4;
+
+// shared-memory slots per warp and array of the staged warp solve: the line
+// padded by one slot per lane chunk (at most 32 pads)
+__host__ __device__ constexpr int tri_ws_slots(int nv) { return nv + 32; }
 
 // mode k of the spectrum by the calling warp
 template <typename R>
@@ -663,6 +669,142 @@ k_tridiag_warp(typename Cplx<R>::type* __restrict__ spec, TriParams p) {
     const int k = blockIdx.x * TRIW_WARPS + (threadIdx.x >> 5);
     if (k >= p.nmodes) return;
     tridiag_warp_mode<R>(spec, p, k);
+}
+
+// One warp per x mode with the mode's line and its LU reciprocals staged in
+// the warp's slice of shared memory (and the alpha/gamma tables in the CTA's,
+// shared by its warps): coalesced cp.async copies of whole lines, then lane l
+// sweeps rows [l*CH, (l+1)*CH) out of shared memory (row r at padded slot
+// r + r/CH; CH + 1 is odd for power-of-two lines, so the lanes'
+// chunk-strided accesses are free of bank conflicts), with the chunks joined
+// by warp scans of affine maps.  Every slice holds tri_ws_slots(nv) slots.
+//
+// tri_ws_stage_tables (all threads of the CTA) and tri_ws_stage_line (the
+// warp of mode k) issue the copies; the caller waits for them
+// (cp_async_wait0 + __syncthreads) before tridiag_warp_staged.
+template <typename R>
+__device__ __forceinline__ void tri_ws_stage_tables(const TriParams& p, R* __restrict__ sal, R* __restrict__ sga) {
+    const int nv = p.nv;
+    const int CH = (nv + 31) / 32;
+    const R* al = reinterpret_cast<const R*>(p.alpha);
+    const R* ga = reinterpret_cast<const R*>(p.gamma);
+    for (int r = threadIdx.x; r < nv; r += blockDim.x) {
+        const int q = r + r / CH;
+        cp_async_elem(&sal[q], &al[r]);
+        cp_async_elem(&sga[q], &ga[r]);
+    }
+}
+template <typename R>
+__device__ __forceinline__ void tri_ws_stage_line(const typename Cplx<R>::type* __restrict__ spec, const TriParams& p,
+                                                  int k, typename Cplx<R>::type* __restrict__ sb,
+                                                  typename Cplx<R>::type* __restrict__ sd) {
+    using C = typename Cplx<R>::type;
+    const int lane = threadIdx.x & 31;
+    const int nv = p.nv;
+    const int CH = (nv + 31) / 32;
+    const C* line = spec + (size_t)k * nv;
+    const C* dg = reinterpret_cast<const C*>(p.dinv) + (size_t)k * nv;
+    for (int r = lane; r < nv; r += 32) {   // every copy in flight at once
+        const int q = r + r / CH;
+        cp_async_elem(&sb[q], &line[r]);
+        cp_async_elem(&sd[q], &dg[r]);
+    }
+}
+// the solve of one mode by the calling warp out of its staged slices (the
+// solution replaces the right-hand side in sb)
+template <typename R>
+__device__ __forceinline__ void tri_ws_solve(typename Cplx<R>::type* __restrict__ sb,
+                                             const typename Cplx<R>::type* __restrict__ sd,
+                                             const R* __restrict__ al, const R* __restrict__ ga,
+                                             typename Cplx<R>::type lam, int nv) {
+    using C = typename Cplx<R>::type;
+    const int lane = threadIdx.x & 31;
+    const int CH = (nv + 31) / 32;
+    const int r0 = lane * CH;
+    const int r1 = min(r0 + CH, nv);
+    const int q0 = lane * (CH + 1);
+    // forward: y_r = b_r - l_r y_{r-1},  l_r = lambda alpha_r / U_{r-1}
+    Aff<C> a;
+    a.P = c_make<C>(1.0, 0.0);
+    a.Q = c_make<C>(0.0, 0.0);
+    for (int r = r0, q = q0; r < r1; ++r, ++q) {
+        Aff<C> m;
+        if (r == 0) m.P = c_make<C>(0.0, 0.0);
+        else {
+            const C dprev = sd[(r == r0) ? q - 2 : q - 1];   // r0-1 sits before the previous chunk's pad slot
+            const C l = c_mul(c_rmul(lam, al[q]), dprev);
+            m.P = c_make<C>(-l.x, -l.y);
+        }
+        m.Q = sb[q];
+        a = aff_combine(a, m);
+    }
+    C y = warp_scan_aff<C>(a, true);
+    for (int r = r0, q = q0; r < r1; ++r, ++q) {
+        const C b = sb[q];
+        if (r == 0) y = b;
+        else {
+            const C dprev = sd[(r == r0) ? q - 2 : q - 1];
+            const C l = c_mul(c_rmul(lam, al[q]), dprev);
+            y = c_sub(b, c_mul(l, y));
+        }
+        sb[q] = y;
+    }
+    // backward: x_r = U_r^-1 (y_r - c_r x_{r+1})  ==  mu_r + nu_r x_{r+1} (each lane reads its own chunk only)
+    a.P = c_make<C>(1.0, 0.0);
+    a.Q = c_make<C>(0.0, 0.0);
+    for (int r = r1 - 1, q = q0 + (r1 - 1 - r0); r >= r0; --r, --q) {
+        Aff<C> m;
+        const C d = sd[q];
+        m.Q = c_mul(d, sb[q]);
+        if (r == nv - 1) m.P = c_make<C>(0.0, 0.0);
+        else {
+            const C nu = c_mul(d, c_rmul(lam, ga[q]));
+            m.P = c_make<C>(-nu.x, -nu.y);
+        }
+        a = aff_combine(a, m);
+    }
+    C x = warp_scan_aff<C>(a, false);
+    for (int r = r1 - 1, q = q0 + (r1 - 1 - r0); r >= r0; --r, --q) {
+        const C d = sd[q];
+        if (r == nv - 1) x = c_mul(d, sb[q]);
+        else x = c_mul(d, c_sub(sb[q], c_mul(c_rmul(lam, ga[q]), x)));
+        sb[q] = x;
+    }
+}
+
+template <typename R>
+__device__ __forceinline__ void tridiag_warp_staged(typename Cplx<R>::type* __restrict__ spec, const TriParams& p,
+                                                    int k, typename Cplx<R>::type* __restrict__ sb,
+                                                    const typename Cplx<R>::type* __restrict__ sd,
+                                                    const R* __restrict__ al, const R* __restrict__ ga) {
+    using C = typename Cplx<R>::type;
+    const int lane = threadIdx.x & 31;
+    const int nv = p.nv;
+    const int CH = (nv + 31) / 32;
+    C* line = spec + (size_t)k * nv;
+    tri_ws_solve<R>(sb, sd, al, ga, reinterpret_cast<const C*>(p.lambda)[k], nv);
+    __syncwarp();
+    for (int r = lane; r < nv; r += 32) line[r] = sb[r + r / CH];
+}
+
+// dynamic smem: TRIW_WARPS x 2 x tri_ws_slots(nv) complex + 2 x tri_ws_slots(nv) real
+template <typename R>
+__global__ void __launch_bounds__(32 * TRIW_WARPS)
+k_tridiag_warp_staged(typename Cplx<R>::type* __restrict__ spec, TriParams p) {
+    using C = typename Cplx<R>::type;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const int w = threadIdx.x >> 5;
+    const int k = blockIdx.x * TRIW_WARPS + w;
+    const int ns = tri_ws_slots(p.nv);
+    C* sb = reinterpret_cast<C*>(smem_raw) + (size_t)w * 2 * ns;
+    R* sal = reinterpret_cast<R*>(reinterpret_cast<C*>(smem_raw) + (size_t)TRIW_WARPS * 2 * ns);
+    R* sga = sal + ns;
+    tri_ws_stage_tables<R>(p, sal, sga);
+    if (k < p.nmodes) tri_ws_stage_line<R>(spec, p, k, sb, sb + ns);
+    cp_async_commit();
+    cp_async_wait0();
+    __syncthreads();
+    if (k < p.nmodes) tridiag_warp_staged<R>(spec, p, k, sb, sb + ns, sal, sga);
 }
 
 }  // namespace vv
