@@ -1973,7 +1973,6 @@ int b_cycle_head(vv_batch* b) {
     TRY(blaunch(b, vv::k_b_gm_head<T>, vv::F_VEC, vv::RED_THREADS, 0, tab, G, b->n));
     TRY(blaunch(b, vv::k_b_gm_cycle_p<T>, vv::F_VEC, vv::RED_THREADS, 0, tab, G, b->n));
     TRY(blaunch(b, vv::k_b_gm_cycle_f, vv::F_INST, 32, 0, tab, G, b->n));
-    TRY(blaunch(b, vv::k_b_gm_scale<T>, vv::F_VEC, vv::RED_THREADS, 0, tab, G, b->n));
     return b_ctrl(b, vv::BC_INNER, BH_INNER);
 }
 
@@ -1987,7 +1986,6 @@ int b_arnoldi(vv_batch* b) {
     TRY(blaunch(b, vv::k_b_gm_mdot_f, vv::F_INST, vv::RED_THREADS, 0, tab, A, b->n));
     TRY(blaunch(b, vv::k_b_gm_maxpy_p<T>, vv::F_VEC, vv::RED_THREADS, 0, tab, A, b->n));
     TRY(blaunch(b, vv::k_b_gm_maxpy_f, vv::F_INST, 32, 0, tab, A, b->n));
-    TRY(blaunch(b, vv::k_b_gm_scale<T>, vv::F_VEC, vv::RED_THREADS, 0, tab, A, b->n));
     return b_ctrl(b, vv::BC_INNER, BH_INNER);
 }
 

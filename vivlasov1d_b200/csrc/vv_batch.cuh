@@ -90,7 +90,8 @@ VV_DEV void for_work(const BInst* __restrict__ tab, const int* __restrict__ L, i
 enum BSrc { BS_RESIDUAL = 0, BS_X = 1, BS_VIT = 2 };
 
 // RESIDUAL: tmp = R(f) (FP64) with tile partials; BS_X: tmpT = J x;
-// BS_VIT: tmpT = J V[it] (the Arnoldi input)
+// BS_VIT: tmpT = J v_it, v_it = vsc[it] V[it] (the Arnoldi input; the
+// operator is linear, so the factor scales its two coefficients)
 template <int SCHEME, int SRC, typename T>
 __global__ void __launch_bounds__(WTHREADS, 4) k_b_bracket(const BInst* __restrict__ tab, const int* __restrict__ L, int n) {
     for_work<F_TILE>(tab, L, n, [&](const BInst& I, int local) {
@@ -102,6 +103,11 @@ __global__ void __launch_bounds__(WTHREADS, 4) k_b_bracket(const BInst* __restri
             bracket_wide_tile<SCHEME, MODE_RESIDUAL, double>(I.f, I.Fh, I.tmp, p, I.part, bx, by, I.tiles_x);
         } else {
             p.factor = 0.5;
+            if (SRC == BS_VIT) {
+                const double sc = I.ds->vsc[I.ds->it];
+                p.factor *= sc;
+                p.ht_inv *= sc;
+            }
             const T* X = (SRC == BS_X) ? (const T*)I.xT : (const T*)I.V + (size_t)I.ds->it * I.ncell;
             bracket_wide_tile<SCHEME, MODE_JVP, T>(X, nullptr, (T*)I.tmpT, p, nullptr, bx, by, I.tiles_x);
         }
@@ -443,12 +449,6 @@ __global__ void k_b_gm_cycle_f(const BInst* __restrict__ tab, const int* __restr
     });
 }
 
-template <typename T>
-__global__ void k_b_gm_scale(const BInst* __restrict__ tab, const int* __restrict__ L, int n) {
-    for_work<F_VEC>(tab, L, n, [&](const BInst& I, int bid) {
-        gm_scale_block<T>(I.ds, (T*)I.V, I.ncell, I.ncell, bid, I.vblk);
-    });
-}
 
 // <w, V_q>, q = 0..it, w = V[it+1], per warp item (column q of the partials)
 template <typename T>
@@ -501,19 +501,21 @@ __global__ void __launch_bounds__(RED_THREADS, 4) k_b_gm_mdot_p(const BInst* __r
     });
 }
 
-// hcol_q from the partials (one warp per column)
+// hcol_q = vsc_q <w, V_q> = <w, v_q> from the partials (one warp per column).
+// A separate kernel: a last-block reduction inside the multi-dot needs a
+// device-scope fence per work item, which waits for the item's stores.
 __global__ void __launch_bounds__(RED_THREADS) k_b_gm_mdot_f(const BInst* __restrict__ tab, const int* __restrict__ L, int n) {
     for_work<F_INST>(tab, L, n, [&](const BInst& I, int) {
         DevState* s = I.ds;
         const int m = s->it + 1, nwi = wi_count(I);
         for (int q = threadIdx.x >> 5; q < m; q += RED_THREADS / 32) {
             const double t = warp_reduce_parts(I.wpart + (size_t)q * nwi, nwi);
-            if ((threadIdx.x & 31) == 0) s->hcol[q] = t;
+            if ((threadIdx.x & 31) == 0) s->hcol[q] = t * s->vsc[q];
         }
     });
 }
 
-// w += sum_q (-hcol_q) V_q and ||w||^2 per warp item
+// w += sum_q (-hcol_q vsc_q) V_q and ||w||^2 per warp item
 template <typename T>
 __global__ void __launch_bounds__(RED_THREADS, 4) k_b_gm_maxpy_p(const BInst* __restrict__ tab, const int* __restrict__ L, int n) {
     constexpr int VN = vec_n<T>(), WV = WCELLS / (32 * VN);
@@ -521,7 +523,7 @@ __global__ void __launch_bounds__(RED_THREADS, 4) k_b_gm_maxpy_p(const BInst* __
     for_work<F_VEC>(tab, L, n, [&](const BInst& I, int bid) {
         const DevState* s = I.ds;
         const int m = s->it + 1;
-        for (int q = threadIdx.x; q < m; q += blockDim.x) cf[q] = -s->hcol[q];
+        for (int q = threadIdx.x; q < m; q += blockDim.x) cf[q] = -s->hcol[q] * s->vsc[q];
         __syncthreads();
         const int lane = threadIdx.x & 31, nwi = wi_count(I), wi = bid * 8 + (threadIdx.x >> 5);
         const size_t nc = I.ncell;
@@ -564,7 +566,8 @@ __global__ void __launch_bounds__(RED_THREADS, 4) k_b_gm_maxpy_p(const BInst* __
     });
 }
 
-// ||w|| and the Arnoldi bookkeeping (Hessenberg column, Givens, test)
+// ||w|| and the Arnoldi bookkeeping (Hessenberg column, Givens, test; vsc of
+// the new vector)
 __global__ void k_b_gm_maxpy_f(const BInst* __restrict__ tab, const int* __restrict__ L, int n) {
     for_work<F_INST>(tab, L, n, [&](const BInst& I, int) {
         if (threadIdx.x >= 32) return;
@@ -591,7 +594,7 @@ __global__ void __launch_bounds__(RED_THREADS) k_b_gm_update(const BInst* __rest
     for_work<F_VEC>(tab, L, n, [&](const BInst& I, int bid) {
         const DevState* s = I.ds;
         const int m = s->pad;
-        for (int q = threadIdx.x; q < m; q += blockDim.x) nrs[q] = s->hcol[q];
+        for (int q = threadIdx.x; q < m; q += blockDim.x) nrs[q] = s->hcol[q] * s->vsc[q];
         __syncthreads();
         if (m <= 0) return;
         const T* V = (const T*)I.V;
@@ -728,6 +731,8 @@ k_b_ctrl(const BInst* __restrict__ tab, int n, int op, unsigned long long handle
 __global__ void k_b_set_it(const BInst* __restrict__ tab, int n, int it) {
     for (int q = threadIdx.x; q < n; q += blockDim.x) tab[q].ds->it = it;
 }
+
+
 
 // copy the first `words` 32-bit words of every instance's state into out[n][words]
 __global__ void k_b_gather_states(const BInst* __restrict__ tab, int words, unsigned int* __restrict__ out) {

@@ -45,6 +45,9 @@ struct DevState {
     double grs[MAX_RESTART + 2];
     double cc[MAX_RESTART + 1], ss[MAX_RESTART + 1];
     double hh[(MAX_RESTART + 2) * (MAX_RESTART + 1)];
+    // 1/||V_q|| of the basis vectors as produced (the lockstep batch keeps V_q
+    // unnormalised and applies these factors where it reads the basis)
+    double vsc[MAX_RESTART + 2];
 };
 
 // PETSc reasons
@@ -171,6 +174,7 @@ VV_DEV void gm_cycle_state(DevState* s, double ss2) {
     s->grs[0] = res;
     s->res = res;
     s->scale = (res != 0.0) ? 1.0 / res : 1.0;
+    s->vsc[0] = s->scale;
     if (res == 0.0) {
         s->reason = R_ATOL;
         s->active = 0;
@@ -279,6 +283,7 @@ VV_DEV void gm_arnoldi(DevState* s, double tt) {
 #define HH(a, b) hh[(b) * ld + (a)]
     for (int j = 0; j <= it; ++j) HH(j, it) = s->hcol[j];
     s->scale = (tt != 0.0) ? 1.0 / tt : 1.0;
+    s->vsc[it + 1] = s->scale;
     HH(it + 1, it) = tt;
     double hapbnd = fabs(tt / s->grs[it]);
     if (hapbnd > s->haptol) hapbnd = s->haptol;
