@@ -566,16 +566,6 @@ __global__ void __launch_bounds__(RED_THREADS, 4) k_b_gm_maxpy_p(const BInst* __
     });
 }
 
-// ||w|| and the Arnoldi bookkeeping (Hessenberg column, Givens, test; vsc of
-// the new vector)
-__global__ void k_b_gm_maxpy_f(const BInst* __restrict__ tab, const int* __restrict__ L, int n) {
-    for_work<F_INST>(tab, L, n, [&](const BInst& I, int) {
-        if (threadIdx.x >= 32) return;
-        const double ss2 = warp_reduce_parts(I.wpart, wi_count(I));
-        if (threadIdx.x == 0) gm_arnoldi(I.ds, sqrt(ss2));
-    });
-}
-
 // end of a cycle: triangular solve once per instance (coefficients into
 // hcol, their count into pad), then the solution update x += sum nrs_q V_q
 __global__ void k_b_gm_solve(const BInst* __restrict__ tab, const int* __restrict__ L, int n) {
@@ -616,77 +606,76 @@ enum BCtrl { BC_PIC = 0, BC_GM_START = 1, BC_INNER = 2, BC_GM_FINISH = 3, BC_REV
 
 constexpr int CTRL_THREADS = 1024;
 
-// in-block exclusive scan of one int per thread (CTRL_THREADS threads); returns the block total
-__device__ __forceinline__ int ctrl_scan(int v, int& excl, int* sh) {
-    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-    int inc = v;
-#pragma unroll
-    for (int d = 1; d < 32; d <<= 1) {
-        const int o = __shfl_up_sync(0xffffffffu, inc, d);
-        if (lane >= d) inc += o;
-    }
-    if (lane == 31) sh[wid] = inc;
-    __syncthreads();
-    if (wid == 0) {
-        int s = (lane < CTRL_THREADS / 32) ? sh[lane] : 0;
-#pragma unroll
-        for (int d = 1; d < 32; d <<= 1) {
-            const int o = __shfl_up_sync(0xffffffffu, s, d);
-            if (lane >= d) s += o;
-        }
-        sh[lane] = s;   // inclusive warp totals
-    }
-    __syncthreads();
-    excl = inc - v + (wid > 0 ? sh[wid - 1] : 0);
-    const int total = sh[CTRL_THREADS / 32 - 1];
-    __syncthreads();
-    return total;
-}
-
-// rebuild list `l` from the per-instance membership test `in(q)`
+// rebuild list `l` from the per-instance membership test `in(q)`: one pass
+// of warp scans over (member, work items per family) and one scan of the
+// warp totals per value (CTRL_THREADS threads)
 template <typename In>
-__device__ void ctrl_build(const BInst* __restrict__ tab, int n, int* __restrict__ lists, int l, In in, int* sh) {
+__device__ void ctrl_build(const BInst* __restrict__ tab, int n, int* __restrict__ lists, int l, In in) {
+    constexpr int NV = NFAM + 1, NW = CTRL_THREADS / 32;
+    static_assert(NV <= NW, "one warp per scanned value");
     int* L = lists + (size_t)l * blist_words(n);
     int* ids = L + 1 + NFAM;
     int* pre = ids + n;
-    __shared__ int base_id, base_f[NFAM];
-    if (threadIdx.x == 0) {
-        base_id = 0;
-        for (int f = 0; f < NFAM; ++f) base_f[f] = 0;
-    }
+    __shared__ int wsum[NV][NW];
+    __shared__ int wtot[NV];
+    __shared__ int carry[NV];
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    if (threadIdx.x < NV) carry[threadIdx.x] = 0;
     __syncthreads();
     for (int q0 = 0; q0 < n; q0 += CTRL_THREADS) {
         const int q = q0 + threadIdx.x;
-        const int on = (q < n && in(q)) ? 1 : 0;
-        int pos = 0;
-        const int cnt_on = ctrl_scan(on, pos, sh);
-        if (on) ids[base_id + pos] = q;
-        for (int f = 0; f < NFAM; ++f) {
-            const int c = on ? tab[q].cnt[f] : 0;
-            int ex = 0;
-            const int tot = ctrl_scan(c, ex, sh);
-            if (on) pre[(size_t)f * (n + 1) + base_id + pos] = base_f[f] + ex;
-            __syncthreads();
-            if (threadIdx.x == 0) base_f[f] += tot;
-            __syncthreads();
+        const bool on = q < n && in(q);
+        int v[NV], inc[NV];
+        v[0] = on ? 1 : 0;
+#pragma unroll
+        for (int f = 0; f < NFAM; ++f) v[1 + f] = on ? tab[q].cnt[f] : 0;
+#pragma unroll
+        for (int k = 0; k < NV; ++k) {
+            inc[k] = v[k];
+#pragma unroll
+            for (int d = 1; d < 32; d <<= 1) {
+                const int o = __shfl_up_sync(0xffffffffu, inc[k], d);
+                if (lane >= d) inc[k] += o;
+            }
+            if (lane == 31) wsum[k][wid] = inc[k];
         }
-        if (threadIdx.x == 0) base_id += cnt_on;
+        __syncthreads();
+        if (wid < NV) {   // warp k: exclusive scan of the warp totals of value k
+            const int x = wsum[wid][lane];
+            int y = x;
+#pragma unroll
+            for (int d = 1; d < 32; d <<= 1) {
+                const int o = __shfl_up_sync(0xffffffffu, y, d);
+                if (lane >= d) y += o;
+            }
+            wsum[wid][lane] = y - x;
+            if (lane == 31) wtot[wid] = y;
+        }
+        __syncthreads();
+        if (on) {
+            const int pos = carry[0] + wsum[0][wid] + inc[0] - 1;
+            ids[pos] = q;
+#pragma unroll
+            for (int f = 0; f < NFAM; ++f)
+                pre[(size_t)f * (n + 1) + pos] = carry[1 + f] + wsum[1 + f][wid] + inc[1 + f] - v[1 + f];
+        }
+        __syncthreads();
+        if (threadIdx.x < NV) carry[threadIdx.x] += wtot[threadIdx.x];
         __syncthreads();
     }
     if (threadIdx.x == 0) {
-        L[0] = base_id;
+        L[0] = carry[0];
         for (int f = 0; f < NFAM; ++f) {
-            L[1 + f] = base_f[f];
-            pre[(size_t)f * (n + 1) + base_id] = base_f[f];
+            L[1 + f] = carry[1 + f];
+            pre[(size_t)f * (n + 1) + carry[0]] = carry[1 + f];
         }
     }
     __syncthreads();
 }
 
-__global__ void __launch_bounds__(CTRL_THREADS)
-k_b_ctrl(const BInst* __restrict__ tab, int n, int op, unsigned long long handle, int* __restrict__ flag,
-         unsigned int* __restrict__ counts, int* __restrict__ lists) {
-    __shared__ int sh[CTRL_THREADS / 32];
+// the control step by one block of CTRL_THREADS threads
+__device__ void ctrl_run(const BInst* __restrict__ tab, int n, int op, unsigned long long handle, int* __restrict__ flag,
+                         unsigned int* __restrict__ counts, int* __restrict__ lists) {
     // mask transitions (each instance by one thread)
     for (int q = threadIdx.x; q < n; q += CTRL_THREADS) {
         DevState* s = tab[q].ds;
@@ -696,27 +685,27 @@ k_b_ctrl(const BInst* __restrict__ tab, int n, int op, unsigned long long handle
     __syncthreads();
     int l = L_PIC;
     switch (op) {
-        case BC_ALL: l = L_ALL; ctrl_build(tab, n, lists, L_ALL, [&](int) { return true; }, sh); break;
-        case BC_PIC: ctrl_build(tab, n, lists, L_PIC, [&](int q) { return tab[q].ds->pic_active != 0; }, sh); break;
+        case BC_ALL: l = L_ALL; ctrl_build(tab, n, lists, L_ALL, [&](int) { return true; }); break;
+        case BC_PIC: ctrl_build(tab, n, lists, L_PIC, [&](int q) { return tab[q].ds->pic_active != 0; }); break;
         case BC_GM_START:
         case BC_GM_FINISH:
             l = L_GM;
-            ctrl_build(tab, n, lists, L_GM, [&](int q) { return tab[q].ds->gm_outer != 0; }, sh);
+            ctrl_build(tab, n, lists, L_GM, [&](int q) { return tab[q].ds->gm_outer != 0; });
             ctrl_build(tab, n, lists, L_GMR, [&](int q) {
                 const DevState* s = tab[q].ds;
                 return s->gm_outer != 0 && s->first == 0;
-            }, sh);
+            });
             break;
         case BC_INNER:
             l = L_INNER;
             ctrl_build(tab, n, lists, L_INNER, [&](int q) {
                 const DevState* s = tab[q].ds;
                 return s->gm_outer != 0 && s->active != 0;
-            }, sh);
+            });
             break;
         default:
             l = L_REVERT;
-            ctrl_build(tab, n, lists, L_REVERT, [&](int q) { return tab[q].ds->pic_revert != 0; }, sh);
+            ctrl_build(tab, n, lists, L_REVERT, [&](int q) { return tab[q].ds->pic_revert != 0; });
             break;
     }
     if (threadIdx.x == 0) {
@@ -725,6 +714,31 @@ k_b_ctrl(const BInst* __restrict__ tab, int n, int op, unsigned long long handle
         if (flag) *flag = any;
         if (any && counts) counts[op] += 1u;
     }
+}
+
+__global__ void __launch_bounds__(CTRL_THREADS)
+k_b_ctrl(const BInst* __restrict__ tab, int n, int op, unsigned long long handle, int* __restrict__ flag,
+         unsigned int* __restrict__ counts, int* __restrict__ lists) {
+    ctrl_run(tab, n, op, handle, flag, counts, lists);
+}
+
+// End of an Arnoldi step: ||w|| and the Arnoldi bookkeeping of every
+// instance of list L (one warp per instance; vsc of the new vector), then the
+// BC_INNER control step by the block that finishes last (`done`: a grid
+// counter, zero on entry and on exit).  The blocks only write instance
+// state before the counter, so the device-scope fence is short.
+__global__ void __launch_bounds__(CTRL_THREADS)
+k_b_arnoldi_ctrl(const BInst* __restrict__ tab, const int* __restrict__ L, int n, unsigned long long handle,
+                 int* __restrict__ flag, unsigned int* __restrict__ counts, int* __restrict__ lists,
+                 unsigned int* __restrict__ done) {
+    for_work<F_INST>(tab, L, n, [&](const BInst& I, int) {
+        if (threadIdx.x < 32) {
+            const double ss2 = warp_reduce_parts(I.wpart, wi_count(I));
+            if (threadIdx.x == 0) gm_arnoldi(I.ds, sqrt(ss2));
+        }
+    });
+    if (!last_block(done, gridDim.x)) return;
+    ctrl_run(tab, n, BC_INNER, handle, flag, counts, lists);
 }
 
 // set the Arnoldi index of every instance (kernel timing)
