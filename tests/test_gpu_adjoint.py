@@ -45,9 +45,11 @@ def dev(a):
     return torch.from_numpy(np.ascontiguousarray(a)).to("cuda")
 
 
-def test_step_adjoint_equals_oracle_adjoint():
+@pytest.mark.parametrize("nx,nv", [(32, 64), (51, 64), (100, 128)])
+def test_step_adjoint_equals_oracle_adjoint(nx, nv):
+    """The GPU step adjoint against the oracle adjoint, power-of-two and
+    other nx (the direct-DFT preconditioner and Poisson kernels)."""
     from vivlasov1d_b200.adjoint import Adjoint
-    nx, nv = 32, 64
     f0 = f_amp(nx, nv, [0.2, 0.05])
     run = run_of(nx, nv, f0)
     f = run.fc.clone()

@@ -48,7 +48,9 @@ struct vv_ctx {
     size_t smem_rfft32, smem_irfft32, smem_tri32;
     bool tri_stage32;
     // kernel variants (picked by the autotuner at vv_create)
-    int fft_kind;      // 0: shared-memory radix-2 per warp, 1: four-step register/shuffle FFT
+    int fft_kind;      // 0: shared-memory radix-2 per warp, 1: four-step register/shuffle FFT,
+                       // 2: direct DFT (the only kind for nx that is not a power of two)
+    bool pow2;         // nx a power of two
     int tri_kind;      // 0: one CTA per mode (block scan), 1: one warp per mode (lines staged in shared
                        // memory when tri_ws_smem fits smem_limit)
     int smem_limit;    // dynamic shared memory per block on this device
@@ -313,11 +315,18 @@ size_t fft_smem(int kind, int M, int R, size_t csz, bool inverse) {
 
 bool four_step_ok(int M) { return M >= 32 && M <= 512; }
 
+// shared memory of the direct-DFT kernels (any nx)
+size_t rdft_smem(int nx, size_t csz) { return (size_t)nx * csz + (size_t)vv::DFT_ROWS * nx * (csz / 2); }
+size_t irdft_smem(int nx, size_t csz) { return (size_t)nx * csz + (size_t)vv::DFT_ROWS * (nx / 2 + 1) * csz; }
+
 template <typename TI, typename R>
 int launch_rfft(vv_ctx* c, const TI* X, typename Cplx<R>::type* spec, const vv::PcParams& p, unsigned rows) {
     const size_t csz = sizeof(typename Cplx<R>::type);
     const int M = c->M;
-    if (c->fft_kind == 1 && four_step_ok(M)) {
+    if (c->fft_kind == 2 || !c->pow2) {
+        const unsigned g = (unsigned)((c->nv + vv::DFT_ROWS - 1) / vv::DFT_ROWS);
+        vv::k_rdft_rows<TI, R><<<g, vv::DFT_THREADS, rdft_smem(c->nx, csz), c->st>>>(X, spec, p);
+    } else if (c->fft_kind == 1 && four_step_ok(M)) {
         const size_t sm = fft_smem(1, M, c->pcR, csz, false);
         switch (M / 32) {
             case 1: vv::k_rfft4<TI, R, 1><<<rows, 32 * c->pcR, sm, c->st>>>(X, spec, p); break;
@@ -337,7 +346,10 @@ template <typename R, typename TO>
 int launch_irfft(vv_ctx* c, const typename Cplx<R>::type* spec, TO* Y, const vv::PcParams& p, unsigned rows) {
     const size_t csz = sizeof(typename Cplx<R>::type);
     const int M = c->M;
-    if (c->fft_kind == 1 && four_step_ok(M)) {
+    if (c->fft_kind == 2 || !c->pow2) {
+        const unsigned g = (unsigned)((c->nv + vv::DFT_ROWS - 1) / vv::DFT_ROWS);
+        vv::k_irdft_rows<R, TO><<<g, vv::DFT_THREADS, irdft_smem(c->nx, csz), c->st>>>(spec, Y, p);
+    } else if (c->fft_kind == 1 && four_step_ok(M)) {
         const size_t sm = fft_smem(1, M, c->pcR, csz, true);
         switch (M / 32) {
             case 1: vv::k_irfft4<R, TO, 1><<<rows, 32 * c->pcR, sm, c->st>>>(spec, Y, p); break;
@@ -382,6 +394,9 @@ void smem_attributes(int optin, int& lowest, cudaError_t& e) {
 #undef VV_SET4
     set((const void*)vv::k_tridiag_modes<R, true>);
     set((const void*)vv::k_tridiag_modes<R, false>);
+    set((const void*)vv::k_rdft_rows<double, R>);
+    set((const void*)vv::k_rdft_rows<float, R>);
+    set((const void*)vv::k_irdft_rows<R, R>);
     set((const void*)vv::k_tridiag_warp_staged<R>);
     set((const void*)vv::k_b_tridiag_w<R>);
     set((const void*)vv::k_b_rfftj<double, R>);
@@ -1001,10 +1016,11 @@ int autotune(vv_ctx* c) {
     // FP64 complex size also in the mixed mode: the FP64 entry points
     // (vv_pc_apply) share the tuned rows-per-CTA
     const size_t csz = sizeof(double2);
-    for (int kind = 0; kind <= 1; ++kind) {
+    for (int kind = c->pow2 ? 0 : 2; kind <= 2; ++kind) {
         if (kind == 1 && !four_step_ok(c->M)) continue;
-        for (int R = 1; R <= 8; R *= 2) {
-            if (fft_smem(kind, c->M, R, csz, true) > 200 * 1024) continue;
+        if (kind == 2 && c->pow2) continue;   // the FFT kernels always beat the O(nx^2) DFT
+        for (int R = 1; R <= (kind == 2 ? 1 : 8); R *= 2) {
+            if (kind < 2 && fft_smem(kind, c->M, R, csz, true) > 200 * 1024) continue;
             for (int tk = 0; tk <= 1; ++tk) {
                 c->fft_kind = kind;
                 c->pcR = R;
@@ -1214,10 +1230,6 @@ int vv_create(const vv_grid* grid, vv_ctx** out) {
     *out = nullptr;
     const vv_grid& g = *grid;
     if (g.nx < 4 || g.nv < 5 || !(g.L > 0.0) || !(g.vmax > g.vmin) || !(g.ht > 0.0)) return VV_ERR_ARG;
-    if (!is_pow2(g.nx)) {
-        snprintf(g_err, sizeof g_err, "nx=%d: the x FFT kernels need a power of two", g.nx);
-        return VV_ERR_UNSUPPORTED;
-    }
     if (g.bracket != VV_BRACKET_J1 && g.bracket != VV_BRACKET_J2 && g.bracket != VV_BRACKET_J4) return VV_ERR_ARG;
     if (g.preconditioner != VV_PC_NONE && g.preconditioner != VV_PC_TENSOR_KINETIC) return VV_ERR_ARG;
     if (g.laplace != VV_LAPLACE_CFD4) return VV_ERR_UNSUPPORTED;
@@ -1231,7 +1243,8 @@ int vv_create(const vv_grid* grid, vv_ctx** out) {
     c->nx = g.nx;
     c->nv = g.nv;
     c->M = g.nx / 2;
-    c->logM = ilog2(c->M);
+    c->pow2 = is_pow2(g.nx);
+    c->logM = c->pow2 ? ilog2(c->M) : -1;   // -1: the Poisson solve takes its direct-DFT branch
     c->nmodes = c->M + 1;
     c->restart = restart;
     c->mixed = g.precision == VV_PRECISION_MIXED;
@@ -1277,7 +1290,9 @@ int vv_create(const vv_grid* grid, vv_ctx** out) {
     }
     c->smem_rfft32 = (size_t)(M + c->pcR * (M + 1)) * sizeof(float2);
     c->smem_irfft32 = (size_t)(M + 2 * c->pcR * (M + 1)) * sizeof(float2);
-    c->smem_pois = (size_t)M * sizeof(double2) + (size_t)nx * sizeof(double) + (size_t)(nx + 2) * sizeof(double);
+    // moments_poisson_cta: M+1 complex, nx (padded to even) and nx + 2 doubles
+    c->smem_pois = (size_t)(M + 1) * sizeof(double2) + (size_t)((nx + 1) & ~1) * sizeof(double) +
+                   (size_t)(nx + 2) * sizeof(double);
 
     int s = VV_OK;
     const int tiles = ((nx + vv::BX - 1) / vv::BX) * ((nv + vv::BY - 1) / vv::BY);  // the largest grid
@@ -1289,7 +1304,7 @@ int vv_create(const vv_grid* grid, vv_ctx** out) {
         (s = dalloc(&c->V, (size_t)(c->mixed ? 1 : restart + 1) * n)) ||
         (s = dalloc(&c->part, part_count)) || (s = dalloc(&c->scal, 64)) || (s = dalloc(&c->xscratch, 2 * (size_t)nx)) ||
         (s = dalloc(&c->mom_part, (size_t)c->mom_S * 3 * nx)) || (s = dalloc(&c->spec, (size_t)nm * nv)) ||
-        (s = dalloc(&c->tw, (size_t)std::max(1, nx / 2))) || (s = dalloc(&c->lambda, nm)) ||
+        (s = dalloc(&c->tw, (size_t)nx)) || (s = dalloc(&c->lambda, nm)) ||
         (s = dalloc(&c->dinv, (size_t)nm * nv)) || (s = dalloc(&c->alpha, nv)) || (s = dalloc(&c->gamma, nv)) ||
         (s = dalloc(&c->sym_inv, nm)) || (s = dalloc(&c->ds, 1))) {
         vv_destroy(c);
@@ -1298,7 +1313,7 @@ int vv_create(const vv_grid* grid, vv_ctx** out) {
     if (c->mixed &&
         ((s = dalloc(&c->V32, (size_t)(restart + 1) * n)) || (s = dalloc(&c->tmp32, n)) || (s = dalloc(&c->bvec32, n)) ||
          (s = dalloc(&c->delta32, n)) || (s = dalloc(&c->alpha32, nv)) || (s = dalloc(&c->gamma32, nv)) ||
-         (s = dalloc(&c->spec32, (size_t)nm * nv)) || (s = dalloc(&c->tw32, (size_t)std::max(1, nx / 2))) ||
+         (s = dalloc(&c->spec32, (size_t)nm * nv)) || (s = dalloc(&c->tw32, (size_t)nx)) ||
          (s = dalloc(&c->lambda32, nm)) || (s = dalloc(&c->dinv32, (size_t)nm * nv)))) {
         vv_destroy(c);
         return s;
@@ -1317,8 +1332,8 @@ int vv_create(const vv_grid* grid, vv_ctx** out) {
         h0_[j] = 0.5 * (hv_[j] * hv_[j]) * g.mass;        // Toolbox.pyx:187
     }
     const long double PI = 3.141592653589793238462643383279502884L;
-    std::vector<double2> tw(std::max(1, nx / 2));
-    for (int k = 0; k < nx / 2; ++k) {
+    std::vector<double2> tw(nx);   // W^k = exp(-2 pi i k / nx), k < nx
+    for (int k = 0; k < nx; ++k) {
         const long double a = 2.0L * PI * (long double)k / (long double)nx;
         tw[k] = make_double2((double)cosl(a), (double)(-sinl(a)));
     }
@@ -1415,14 +1430,15 @@ int vv_create(const vv_grid* grid, vv_ctx** out) {
         }
         c->smem_limit = limit;
         const size_t need = std::max({c->smem_tri, c->mixed ? c->smem_tri32 : (size_t)0, c->smem_pois,
-                                      fft_smem(0, M, c->pcR, sizeof(double2), true)});
+                                      c->pow2 ? fft_smem(0, M, c->pcR, sizeof(double2), true)
+                                              : std::max(rdft_smem(nx, sizeof(double2)), irdft_smem(nx, sizeof(double2)))});
         if (need > (size_t)limit) {
             vv_destroy(c);
             return fail(VV_ERR_ARG, "grid %d x %d needs %zu bytes of shared memory per block (limit %d)", nx, nv,
                         need, limit);
         }
     }
-    c->fft_kind = four_step_ok(c->M) ? 1 : 0;
+    c->fft_kind = !c->pow2 ? 2 : four_step_ok(c->M) ? 1 : 0;
     c->tri_kind = c->nmodes >= 64 ? 1 : 0;
     c->narrow_bracket = 0;
     c->march = 0;
@@ -2278,7 +2294,7 @@ int vv_batch_create(int n, vv_ctx* const* ctxs, const vv_state* states, vv_batch
         // 64 x 32 stencil tiles (nx a multiple of 64); the factored order
         if (c->mixed != c0->mixed || c->g.bracket != c0->g.bracket ||
             c->g.preconditioner != VV_PC_TENSOR_KINETIC || c->g.order == VV_ORDER_REFERENCE ||
-            c->nx % vv::WX != 0 || c->device != c0->device)
+            c->nx % vv::WX != 0 || !c->pow2 || c->device != c0->device)
             return VV_ERR_UNSUPPORTED;
     }
     vv_batch* b = new vv_batch();   // value-initialised: pointers and counts start at zero

@@ -25,7 +25,7 @@ struct PcParams {
     int M;                 // nx/2: complex FFT length
     int logM;
     int R;                 // rows (warps) per CTA in the row kernels
-    const void* tw;        // tw[k] = exp(-2 pi i k / nx), k < nx/2 (double2 or float2)
+    const void* tw;        // tw[k] = exp(-2 pi i k / nx), k < nx (double2 or float2); the FFT kernels read k < nx/2
     const int* yidx;       // optional: output is Y + (*yidx + yoff) * ystride
     int yoff;
     size_t ystride;
@@ -410,6 +410,85 @@ template <typename R, typename TO, int E>
 __global__ void k_irfft4(const typename Cplx<R>::type* __restrict__ spec, TO* __restrict__ Y, PcParams p) {
     if (p.yidx) Y += (size_t)(*p.yidx + p.yoff) * p.ystride;
     irfft4_block<R, TO, E>(spec, Y, p, blockIdx.x);
+}
+
+// ---------------------------------------------------------------------------
+// Direct real DFT along x for any nx (the lengths the FFT kernels do not
+// take: odd and other non-power-of-two grids of the reference's example
+// configurations).  O(nx^2) per row from the nx-entry twiddle table;
+// numpy's rfft / irfft conventions (irfft ignores the imaginary parts of
+// X_0 and, for even nx, X_{nx/2}).  DFT_ROWS rows per CTA.
+// ---------------------------------------------------------------------------
+constexpr int DFT_ROWS = 4, DFT_THREADS = 256;
+
+// X_k = sum_n x_n W^{nk}, k = 0..nx/2, written mode-major spec[k*nv + j].
+// dynamic smem: nx twiddles (complex R) + DFT_ROWS x nx (R)
+template <typename TI, typename R>
+__global__ void __launch_bounds__(DFT_THREADS)
+k_rdft_rows(const TI* __restrict__ X, typename Cplx<R>::type* __restrict__ spec, PcParams p) {
+    using C = typename Cplx<R>::type;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const int N = p.nx, nm = N / 2 + 1;
+    C* stw = reinterpret_cast<C*>(smem_raw);
+    R* xs = reinterpret_cast<R*>(stw + N);
+    const C* tw = reinterpret_cast<const C*>(p.tw);
+    for (int k = threadIdx.x; k < N; k += blockDim.x) stw[k] = tw[k];
+    const int j0 = blockIdx.x * DFT_ROWS;
+    for (int i = threadIdx.x; i < DFT_ROWS * N; i += blockDim.x) {
+        const int r = i / N, n = i - r * N, j = j0 + r;
+        xs[i] = (j < p.nv) ? (R)X[(size_t)j * N + n] : (R)0;
+    }
+    __syncthreads();
+    for (int u = threadIdx.x; u < nm * DFT_ROWS; u += blockDim.x) {
+        const int k = u / DFT_ROWS, r = u - k * DFT_ROWS, j = j0 + r;
+        const R* xr = xs + r * N;
+        R re = 0, im = 0;
+        int idx = 0;
+        for (int n = 0; n < N; ++n) {
+            const C w = stw[idx];
+            re += xr[n] * w.x;
+            im += xr[n] * w.y;
+            idx += k;
+            if (idx >= N) idx -= N;
+        }
+        if (j < p.nv) spec[(size_t)k * p.nv + j] = c_make<C>((double)re, (double)im);
+    }
+}
+
+// x_n = (1/nx) [Re X_0 + 2 sum_{k=1}^{(nx-1)/2} Re(X_k W^{-nk}) + (nx even) Re X_{nx/2} (-1)^n]
+// dynamic smem: nx twiddles + DFT_ROWS x (nx/2 + 1) complex
+template <typename R, typename TO>
+__global__ void __launch_bounds__(DFT_THREADS)
+k_irdft_rows(const typename Cplx<R>::type* __restrict__ spec, TO* __restrict__ Y, PcParams p) {
+    using C = typename Cplx<R>::type;
+    if (p.yidx) Y += (size_t)(*p.yidx + p.yoff) * p.ystride;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const int N = p.nx, nm = N / 2 + 1, K = (N - 1) / 2;
+    C* stw = reinterpret_cast<C*>(smem_raw);
+    C* xs = stw + N;
+    const C* tw = reinterpret_cast<const C*>(p.tw);
+    for (int k = threadIdx.x; k < N; k += blockDim.x) stw[k] = tw[k];
+    const int j0 = blockIdx.x * DFT_ROWS;
+    for (int i = threadIdx.x; i < DFT_ROWS * nm; i += blockDim.x) {
+        const int k = i / DFT_ROWS, r = i - k * DFT_ROWS, j = j0 + r;
+        xs[r * nm + k] = (j < p.nv) ? spec[(size_t)k * p.nv + j] : c_make<C>(0.0, 0.0);
+    }
+    __syncthreads();
+    const R inv = (R)(1.0 / (double)N);
+    for (int u = threadIdx.x; u < DFT_ROWS * N; u += blockDim.x) {
+        const int r = u / N, n = u - r * N, j = j0 + r;
+        const C* xr = xs + r * nm;
+        R s = xr[0].x;
+        int idx = 0;
+        for (int k = 1; k <= K; ++k) {
+            idx += n;
+            if (idx >= N) idx -= N;
+            const C w = stw[idx];   // W^{nk} = (cos, -sin): Re(X e^{+i theta}) = X.x w.x + X.y w.y
+            s += (R)2 * (xr[k].x * w.x + xr[k].y * w.y);
+        }
+        if (!(N & 1)) s += (n & 1) ? -xr[N / 2].x : xr[N / 2].x;
+        if (j < p.nv) Y[(size_t)j * N + n] = (TO)(s * inv);
+    }
 }
 
 // ---------------------------------------------------------------------------

@@ -530,7 +530,7 @@ k_moments_partial(const T* __restrict__ F, int nx, int nv, int seg, const double
 struct PoissonParams {
     int nx, M, logM, S;   // S = number of moment partials
     double hv, charge, hx2_inv, hx, inv_nx;
-    const double2* tw;       // nx/2 twiddles
+    const double2* tw;       // nx twiddles W^k (the FFT reads k < nx/2)
     const double* sym_inv;   // M+1 entries: 1/symbol_k (0 for k = 0)
 };
 
@@ -545,9 +545,9 @@ __device__ __forceinline__ void moments_poisson_cta(const double* __restrict__ p
                                                     double* __restrict__ phi, double* __restrict__ h1,
                                                     double* __restrict__ scal, const PoissonParams& p) {
     extern __shared__ double2 psm[];
-    double2* buf = psm;                               // M complex
-    double* nn = reinterpret_cast<double*>(psm + p.M);  // nx
-    double* ph = nn + p.nx;                           // nx
+    double2* buf = psm;                                   // M + 1 complex
+    double* nn = reinterpret_cast<double*>(psm + p.M + 1);  // nx, padded to an even count
+    double* ph = nn + ((p.nx + 1) & ~1);                  // nx + 2; 16-byte aligned (read as double2)
     __shared__ double red[POIS_THREADS / 32];
     const int nx = p.nx, M = p.M;
     // 1. moments
@@ -580,6 +580,43 @@ __device__ __forceinline__ void moments_poisson_cta(const double* __restrict__ p
     if (threadIdx.x == 0) nmean_s = t * p.inv_nx;
     __syncthreads();
     const double nmean = nmean_s;
+    double* phs;
+    if (p.logM < 0) {
+        // 3'. any nx: direct DFT of b, divide by the symbol, direct inverse
+        //     (numpy's rfft / irfft conventions)
+        double2* X2 = reinterpret_cast<double2*>(ph);   // M+1 complex <= nx + 2 doubles
+        for (int k = threadIdx.x; k <= M; k += blockDim.x) {
+            double re = 0.0, im = 0.0;
+            int idx = 0;
+            for (int m = 0; m < nx; ++m) {
+                const double b = -(nn[m] - nmean) * p.charge;
+                const double2 w = p.tw[idx];
+                re += b * w.x;
+                im += b * w.y;
+                idx += k;
+                if (idx >= nx) idx -= nx;
+            }
+            double2 Xk = make_double2(re * p.sym_inv[k], im * p.sym_inv[k]);
+            if (k == 0 || 2 * k == nx) Xk.y = 0.0;
+            X2[k] = Xk;
+        }
+        __syncthreads();
+        phs = reinterpret_cast<double*>(buf);            // 2M + 2 >= nx doubles
+        const int K = (nx - 1) / 2;
+        for (int m = threadIdx.x; m < nx; m += blockDim.x) {
+            double s = X2[0].x;
+            int idx = 0;
+            for (int k = 1; k <= K; ++k) {
+                idx += m;
+                if (idx >= nx) idx -= nx;
+                const double2 w = p.tw[idx];
+                s += 2.0 * (X2[k].x * w.x + X2[k].y * w.y);
+            }
+            if (!(nx & 1)) s += (m & 1) ? -X2[nx / 2].x : X2[nx / 2].x;
+            phs[m] = s * p.inv_nx;
+        }
+        __syncthreads();
+    } else {
     // 3. FFT of b (real, via M-point complex), divide by the symbol, inverse
     for (int m = threadIdx.x; m < M; m += blockDim.x) {
         const double b0 = -(nn[2 * m] - nmean) * p.charge;
@@ -616,13 +653,14 @@ __device__ __forceinline__ void moments_poisson_cta(const double* __restrict__ p
     __syncthreads();
     block_fft<+1>(buf, M, p.tw);
     const double sc = 1.0 / (double)M;
-    double* phs = reinterpret_cast<double*>(X2);  // overwrite: phi in smem
+    phs = reinterpret_cast<double*>(X2);  // overwrite: phi in smem
     __syncthreads();
     for (int m = threadIdx.x; m < M; m += blockDim.x) {
         phs[2 * m] = buf[m].x * sc;
         phs[2 * m + 1] = buf[m].y * sc;
     }
     __syncthreads();
+    }
     // 4. mean of phi, h1 and Poisson residual A phi + (n - nmean) charge
     t = 0.0;
     for (int i = threadIdx.x; i < nx; i += blockDim.x) t += phs[i];
