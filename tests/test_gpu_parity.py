@@ -386,7 +386,7 @@ BATCH_SPECS = [(64, 128, vo.f0_landau(0.1, 0.5), 4 * np.pi, 0.1),
                (64, 512, vo.f0_bump_on_tail(0.04, 0.3), 2 * np.pi / 0.3, 0.1)]
 
 
-@pytest.mark.parametrize("shape", [None, "2,1,0", "8,2,1", "4,0,1", "2,0,0,1", "2,1,0,1"])
+@pytest.mark.parametrize("shape", [None, "2,1,0", "8,2,1", "4,0,1", "2,0,0,1", "2,1,0,1", "4,0,1,0,1"])
 def test_batch_step_equals_single_steps(monkeypatch, shape):
     """A lockstep batch of uneven instances (every kernel launched once for
     the table, per-instance masks) follows each instance's own time step:
@@ -408,7 +408,7 @@ def test_batch_step_equals_single_steps(monkeypatch, shape):
     assert batch.launch_count() > 0
 
 
-@pytest.mark.parametrize("shape", ["4,0,0", "4,1,1", "2,0,0,1", "2,1,0,1"])
+@pytest.mark.parametrize("shape", ["4,0,0", "4,1,1", "2,0,0,1", "2,1,0,1", "2,1,0,1,1"])
 def test_batch_graph_equals_host_driven(monkeypatch, shape):
     """The batch graph (conditional loops folded over the instance masks)
     and the host-driven loop over the same kernels (one fixed shape) give
@@ -427,6 +427,26 @@ def test_batch_graph_equals_host_driven(monkeypatch, shape):
             assert torch.equal(graph_runs[i].fc, host_runs[i].fc), i
 
 
+def test_batch_marching_stencil_equals_tiles(monkeypatch):
+    """The batch's marching Jacobian stencil and its 64 x 32 tiles evaluate
+    the same expression (the compiler may contract multiply-adds differently
+    in the two kernels): two batches of the same instances, two steps each,
+    same Picard passes, GMRES counts within one, f to 1e-12."""
+    from vivlasov1d_b200.batch import Batch
+    out = []
+    for m in ("0", "1"):
+        monkeypatch.setenv("VV_BATCH_SHAPE", "4,0,1,0," + m)
+        runs = [_small_run(*s) for s in BATCH_SPECS]
+        batch = Batch(runs)
+        reps = [batch.step(), batch.step()]
+        out.append(([r.fc.clone() for r in runs], reps))
+    for a, b in zip(out[0][0], out[1][0]):
+        assert (a - b).abs().max().item() <= 1e-12 * b.abs().max().item()
+    for ra, rb in zip(out[0][1], out[1][1]):
+        for i, (x, y) in enumerate(zip(ra, rb)):
+            _assert_batch_matches(x, y, out[0][0][i], out[1][0][i], i, 1e-12)
+
+
 def test_batch_sweep_instances_match_single_steps():
     """Twelve instances of the seeded sweep (Landau, two-stream and
     bump-on-tail; nx 64..256, nv 128..1024) in one batch, FP64, against
@@ -443,7 +463,7 @@ def test_batch_sweep_instances_match_single_steps():
             _assert_batch_matches(rb[i], r.step(), br[i].fc, r.fc, i, 1e-9)
 
 
-@pytest.mark.parametrize("shape", [None, "4,0,1,0", "2,0,0,1", "2,1,0,1"])
+@pytest.mark.parametrize("shape", [None, "4,0,1,0", "2,0,0,1", "2,1,0,1", "2,1,0,1,1"])
 def test_batch_mixed_precision_field_energy(monkeypatch, shape):
     """Batched mixed precision against FP64 single steps: field energy to
     1e-9 relative after three steps for every instance (autotuned, the

@@ -1852,6 +1852,7 @@ struct vv_batch {
     int R;                       // FFT rows per CTA
     int fft4;                    // x-FFTs: 1 four-step register/shuffle, 0 radix-2
     int pcj;                     // 1: preconditioner in the v-major layout (vv_pcj.cuh); fft4/R/tri_kind unused
+    int march;                   // 1: Jacobian stencil by the marching kernel, 0: 64 x 32 tiles
     bool pcj_ok;                 // every instance has M in 32..256 (the v-major kernels' lengths)
     void* dinvJ;                 // device: v-major LU reciprocals of every instance (GMRES precision)
     size_t smem_fftj;            // dynamic shared memory of the v-major FFT blocks
@@ -1957,6 +1958,25 @@ int b_pc(vv_batch* b, int l, bool from_tmp64, int dst) {
     return blaunch(b, vv::k_b_irfft<T, T, false>, vv::F_ROWS, rt, b->smem_irfft, tab, L, b->n, dst);
 }
 
+// the Jacobian stencil of every instance in list L (tiles or marching strips)
+template <int S, int SRC, typename T>
+int b_jvp(vv_batch* b, const int* L) {
+    if (b->march)
+        return blaunch(b, vv::k_b_bracket_march<S, SRC, T>, vv::F_MARCH, vv::MARCH_BW,
+                       vv::MarchRow<T, vv::MARCH_BW>::smem_bytes(), (const vv::BInst*)b->tab, L, b->n);
+    return blaunch(b, vv::k_b_bracket<S, SRC, T>, vv::F_TILE, vv::WTHREADS, 0, (const vv::BInst*)b->tab, L, b->n);
+}
+
+template <typename T>
+int b_jvp_all(vv_batch* b) {
+    const int* L = blist(b, vv::L_ALL);
+    switch (b->scheme) {
+        case VV_BRACKET_J1: return b_jvp<1, vv::BS_X, T>(b, L);
+        case VV_BRACKET_J2: return b_jvp<2, vv::BS_X, T>(b, L);
+        default: return b_jvp<4, vv::BS_X, T>(b, L);
+    }
+}
+
 template <int S, typename T>
 int b_residual(vv_batch* b, int l, int phase) {
     const vv::BInst* tab = b->tab;
@@ -1984,7 +2004,7 @@ template <int S, typename T>
 int b_cycle_head(vv_batch* b) {
     const vv::BInst* tab = b->tab;
     const int* G = blist(b, vv::L_GM);
-    TRY(blaunch(b, vv::k_b_bracket<S, vv::BS_X, T>, vv::F_TILE, vv::WTHREADS, 0, tab, blist(b, vv::L_GMR), b->n));
+    TRY(b_jvp<S, vv::BS_X, T>(b, blist(b, vv::L_GMR)));
     TRY(b_pc<T>(b, vv::L_GMR, false, vv::BD_V0));
     TRY(blaunch(b, vv::k_b_gm_head<T>, vv::F_VEC, vv::RED_THREADS, 0, tab, G, b->n));
     TRY(blaunch(b, vv::k_b_gm_cycle_p<T>, vv::F_VEC, vv::RED_THREADS, 0, tab, G, b->n));
@@ -1996,7 +2016,7 @@ template <int S, typename T>
 int b_arnoldi(vv_batch* b) {
     const vv::BInst* tab = b->tab;
     const int* A = blist(b, vv::L_INNER);
-    TRY(blaunch(b, vv::k_b_bracket<S, vv::BS_VIT, T>, vv::F_TILE, vv::WTHREADS, 0, tab, A, b->n));
+    TRY(b_jvp<S, vv::BS_VIT, T>(b, A));
     TRY(b_pc<T>(b, vv::L_INNER, false, vv::BD_VNEXT));
     TRY(blaunch(b, vv::k_b_gm_mdot_p<T>, vv::F_VEC, vv::RED_THREADS, 0, tab, A, b->n));
     TRY(blaunch(b, vv::k_b_gm_mdot_f, vv::F_INST, vv::RED_THREADS, 0, tab, A, b->n));
@@ -2239,7 +2259,27 @@ int b_autotune(vv_batch* b, std::vector<vv::BInst>& tab) {
     cudaEventDestroy(e1);
     TRY(r);
     b_shape(b, tab, bR, bW, bF, bJ);
-    return b_apply_shape(b, tab);
+    TRY(b_apply_shape(b, tab));
+    // Jacobian stencil: 64 x 32 tiles or marching strips
+    float tj[2] = {1e30f, 1e30f};
+    CK(cudaEventCreate(&e0));
+    CK(cudaEventCreate(&e1));
+    for (int m = 0; m <= 1 && r == VV_OK; ++m) {
+        b->march = m;
+        for (int k = 0; k < 2 && r == VV_OK; ++k) r = b_jvp_all<T>(b);
+        cudaEventRecord(e0, b->st);
+        for (int k = 0; k < 5 && r == VV_OK; ++k) r = b_jvp_all<T>(b);
+        cudaEventRecord(e1, b->st);
+        float ms = 0.f;
+        if (r == VV_OK && cudaEventSynchronize(e1) == cudaSuccess && cudaEventElapsedTime(&ms, e0, e1) == cudaSuccess)
+            tj[m] = ms;
+        if (getenv("VV_DEBUG")) fprintf(stderr, "[vv_batch] tune march=%d: %.1f us\n", m, ms * 200.f);
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    TRY(r);
+    b->march = tj[1] < tj[0] ? 1 : 0;
+    return VV_OK;
 }
 
 template <typename X>
@@ -2325,6 +2365,7 @@ int vv_batch_create(int n, vv_ctx* const* ctxs, const vv_state* states, vv_batch
         I.mom_bx = (c->nx + vv::MOM_TX - 1) / vv::MOM_TX;
         I.mom_S = c->mom_S;
         I.cnt[vv::F_TILE] = I.tiles_x * ((c->nv + vv::WY - 1) / vv::WY);
+        I.cnt[vv::F_MARCH] = (c->nx / vv::MARCH_BW) * ((c->nv + vv::MARCH_SEG - 1) / vv::MARCH_SEG);
         I.cnt[vv::F_VEC] = I.vblk;
         I.cnt[vv::F_MOM] = I.mom_bx * c->mom_S;
         I.cnt[vv::F_INST] = 1;
@@ -2431,15 +2472,16 @@ int vv_batch_create(int n, vv_ctx* const* ctxs, const vv_state* states, vv_batch
     b_shape(b, tab, 4, 0, 0);
     if ((r = b_apply_shape(b, tab)) != VV_OK) return fail_b(r);
     {
-        // VV_BATCH_SHAPE="R,tri,fft4[,vmajor]" fixes the shape (tests, profiling); else the autotuner picks it
+        // VV_BATCH_SHAPE="R,tri,fft4[,vmajor[,march]]" fixes the shape (tests, profiling); else the autotuner picks it
         const char* bs = getenv("VV_BATCH_SHAPE");
-        int fR = 0, fT = 0, fF = 0, fJ = 0;
-        const int nf = bs ? sscanf(bs, "%d,%d,%d,%d", &fR, &fT, &fF, &fJ) : 0;
+        int fR = 0, fT = 0, fF = 0, fJ = 0, fM = 0;
+        const int nf = bs ? sscanf(bs, "%d,%d,%d,%d,%d", &fR, &fT, &fF, &fJ, &fM) : 0;
         const bool fixed = nf >= 3 && (fR == 2 || fR == 4 || fR == 8) && fT >= 0 && fT <= 2 && (fF == 0 || fF == 1) &&
                            (fJ == 0 || (fJ == 1 && b->pcj_ok)) &&
                            !(fT == 1 && b->smem_tri_warp > (size_t)b->smem_limit);
         const char* at = getenv("VV_AUTOTUNE");
         if (fixed) {
+            b->march = fM != 0;
             b_shape(b, tab, fR, fT, fF, fJ);
             if ((r = b_apply_shape(b, tab)) != VV_OK) return fail_b(r);
         } else if (!(at && at[0] == '0')) {
@@ -2548,18 +2590,7 @@ int vv_batch_time_kernel(vv_batch* b, int which, int it, int reps, double* avg_m
                 return b->mixed ? blaunch(b, vv::k_b_gm_mdot_p<float>, vv::F_VEC, vv::RED_THREADS, 0, tab, L, b->n)
                                 : blaunch(b, vv::k_b_gm_mdot_p<double>, vv::F_VEC, vv::RED_THREADS, 0, tab, L, b->n);
             case 1: return b->mixed ? b_pc<float>(b, vv::L_ALL, false, vv::BD_B) : b_pc<double>(b, vv::L_ALL, false, vv::BD_B);
-            case 2:
-                switch (b->scheme) {
-                    case VV_BRACKET_J1:
-                        return b->mixed ? blaunch(b, vv::k_b_bracket<1, vv::BS_X, float>, vv::F_TILE, vv::WTHREADS, 0, tab, L, b->n)
-                                        : blaunch(b, vv::k_b_bracket<1, vv::BS_X, double>, vv::F_TILE, vv::WTHREADS, 0, tab, L, b->n);
-                    case VV_BRACKET_J2:
-                        return b->mixed ? blaunch(b, vv::k_b_bracket<2, vv::BS_X, float>, vv::F_TILE, vv::WTHREADS, 0, tab, L, b->n)
-                                        : blaunch(b, vv::k_b_bracket<2, vv::BS_X, double>, vv::F_TILE, vv::WTHREADS, 0, tab, L, b->n);
-                    default:
-                        return b->mixed ? blaunch(b, vv::k_b_bracket<4, vv::BS_X, float>, vv::F_TILE, vv::WTHREADS, 0, tab, L, b->n)
-                                        : blaunch(b, vv::k_b_bracket<4, vv::BS_X, double>, vv::F_TILE, vv::WTHREADS, 0, tab, L, b->n);
-                }
+            case 2: return b->mixed ? b_jvp_all<float>(b) : b_jvp_all<double>(b);   // the tuned stencil kernel
             default:
                 return b->mixed ? blaunch(b, vv::k_b_gm_maxpy_p<float>, vv::F_VEC, vv::RED_THREADS, 0, tab, L, b->n)
                                 : blaunch(b, vv::k_b_gm_maxpy_p<double>, vv::F_VEC, vv::RED_THREADS, 0, tab, L, b->n);

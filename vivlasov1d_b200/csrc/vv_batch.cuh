@@ -21,7 +21,11 @@
 namespace vv {
 
 // kernel families (work items per instance)
-enum BFam { F_TILE = 0, F_ROWS = 1, F_MODES = 2, F_VEC = 3, F_MOM = 4, F_INST = 5, NFAM = 6 };
+enum BFam { F_TILE = 0, F_ROWS = 1, F_MODES = 2, F_VEC = 3, F_MOM = 4, F_INST = 5, F_MARCH = 6, NFAM = 7 };
+
+// marching Jacobian stencil of the batch: strips of MARCH_BW columns (every
+// batch nx is a multiple of 64), segments of MARCH_SEG rows
+constexpr int MARCH_BW = 64, MARCH_SEG = 128;
 // work lists (one per mask)
 enum BList { L_ALL = 0, L_PIC = 1, L_GM = 2, L_GMR = 3, L_INNER = 4, L_REVERT = 5, NLIST = 6 };
 
@@ -111,6 +115,26 @@ __global__ void __launch_bounds__(WTHREADS, 4) k_b_bracket(const BInst* __restri
             const T* X = (SRC == BS_X) ? (const T*)I.xT : (const T*)I.V + (size_t)I.ds->it * I.ncell;
             bracket_wide_tile<SCHEME, MODE_JVP, T>(X, nullptr, (T*)I.tmpT, p, nullptr, bx, by, I.tiles_x);
         }
+    });
+}
+
+// The Jacobian stencil by the marching kernel (same arithmetic as the tiles,
+// bit for bit): BS_X: tmpT = J x; BS_VIT: tmpT = J v_it
+template <int SCHEME, int SRC, typename T>
+__global__ void __launch_bounds__(MARCH_BW) k_b_bracket_march(const BInst* __restrict__ tab, const int* __restrict__ L,
+                                                             int n) {
+    for_work<F_MARCH>(tab, L, n, [&](const BInst& I, int local) {
+        BracketParams p = I.bp;
+        p.xidx = nullptr;
+        p.factor = 0.5;
+        if (SRC == BS_VIT) {
+            const double sc = I.ds->vsc[I.ds->it];
+            p.factor *= sc;
+            p.ht_inv *= sc;
+        }
+        const T* X = (SRC == BS_X) ? (const T*)I.xT : (const T*)I.V + (size_t)I.ds->it * I.ncell;
+        const int strips = I.nx / MARCH_BW;
+        bracket_march_item<SCHEME, T, MARCH_BW>(X, (T*)I.tmpT, p, MARCH_SEG, local % strips, local / strips);
     });
 }
 

@@ -521,21 +521,22 @@ VV_DEV void march_load(const T* __restrict__ X, T* ring, int nx, int nv, int x0,
     }
 }
 
+// one (strip, segment) item of the marching stencil by a CTA of MW threads
+// (block-uniform; the ring is idle when it returns)
 template <int SCHEME, typename T, int MW>
-__global__ void __launch_bounds__(MW)
-k_bracket_march(const T* __restrict__ X, T* __restrict__ Y, BracketParams p, int seg) {
+VV_DEV void bracket_march_item(const T* __restrict__ X, T* __restrict__ Y, const BracketParams& p, int seg,
+                               int strip, int segi) {
     using RW = MarchRow<T, MW>;
     constexpr int CH = MarchShape<T>::CH, NR = MarchShape<T>::NR;
     static_assert(NR >= 3 * CH + 4 && (NR & (NR - 1)) == 0, "ring of three chunks and the halo, a power of two");
     extern __shared__ __align__(16) unsigned char smem_raw[];
     T* ring = reinterpret_cast<T*>(smem_raw);
     double* rc = reinterpret_cast<double*>(smem_raw + (size_t)NR * RW::RS * sizeof(T));   // [CH][3] row coefficients
-    if (p.xidx) X += (size_t)(*p.xidx) * p.xstride;
     const int nx = p.nx, nv = p.nv;
     const int tx = threadIdx.x;
-    const int x0 = blockIdx.x * MW;
+    const int x0 = strip * MW;
     const int i = x0 + tx;
-    const int j_start = blockIdx.y * seg;
+    const int j_start = segi * seg;
     const int j_end = min(nv, j_start + seg);
     if (j_start >= j_end) return;
     // column coefficients (fixed for the thread)
@@ -634,6 +635,14 @@ k_bracket_march(const T* __restrict__ X, T* __restrict__ Y, BracketParams p, int
         if (ra <= rb) march_load<T, MW>(X, ring, nx, nv, x0, ra, rb);
         cp_async_commit();
     }
+    cp_async_wait0();
+}
+
+template <int SCHEME, typename T, int MW>
+__global__ void __launch_bounds__(MW)
+k_bracket_march(const T* __restrict__ X, T* __restrict__ Y, BracketParams p, int seg) {
+    if (p.xidx) X += (size_t)(*p.xidx) * p.xstride;
+    bracket_march_item<SCHEME, T, MW>(X, Y, p, seg, blockIdx.x, blockIdx.y);
 }
 
 template <int SCHEME, int MODE, typename T>
