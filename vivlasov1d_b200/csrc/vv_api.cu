@@ -2225,9 +2225,42 @@ int b_autotune(vv_batch* b, std::vector<vv::BInst>& tab) {
         const vv_ctx* c = b->ctx[i];
         CK(cudaMemsetAsync(b->mixed ? (void*)c->tmp32 : (void*)c->tmp, 0, c->ncell * sizeof(T), b->st));
     }
+    // the lockstep tail: a few of the slowest instances run alone for most of
+    // a step's GMRES iterations; the largest NTAIL instances stand in for it
+    constexpr int NTAIL = 4;
+    std::vector<int> member(b->n, 0), order(b->n);
+    for (int i = 0; i < b->n; ++i) order[i] = i;
+    std::stable_sort(order.begin(), order.end(), [&](int a, int c) { return b->ctx[a]->ncell > b->ctx[c]->ncell; });
+    for (int i = 0; i < std::min(NTAIL, b->n); ++i) member[order[i]] = 1;
+    int* dmember = nullptr;
+    CK(cudaMalloc((void**)&dmember, b->n * sizeof(int)));
+    if (cudaMemcpy(dmember, member.data(), b->n * sizeof(int), cudaMemcpyHostToDevice) != cudaSuccess) {
+        cudaFree(dmember);
+        return fail_cuda(cudaGetLastError(), "batch autotune");
+    }
+    auto tail_list = [&]() -> int {
+        vv::k_b_build_subset<<<1, vv::CTRL_THREADS, 0, b->st>>>(b->tab, b->n, b->lists, vv::L_TAIL, dmember);
+        const cudaError_t e = cudaGetLastError();
+        return e == cudaSuccess ? VV_OK : fail_cuda(e, "batch autotune list");
+    };
     cudaEvent_t e0, e1;
     CK(cudaEventCreate(&e0));
     CK(cudaEventCreate(&e1));
+    // mean time of `reps` calls of fn after two untimed ones (1e30 on failure)
+    auto timed = [&](auto fn, int reps, int& r) -> float {
+        for (int k = 0; k < 2 && r == VV_OK; ++k) r = fn();
+        cudaEventRecord(e0, b->st);
+        for (int k = 0; k < reps && r == VV_OK; ++k) r = fn();
+        cudaEventRecord(e1, b->st);
+        float ms = 0.f;
+        if (r != VV_OK || cudaEventSynchronize(e1) != cudaSuccess || cudaEventElapsedTime(&ms, e0, e1) != cudaSuccess)
+            return 1e30f;
+        return ms / reps;
+    };
+    // weights of the lockstep profile of a step of the 256-instance sweep:
+    // about 30 whole-table-equivalent GMRES iterations and 100 iterations in
+    // which only the slowest instances are left
+    constexpr float W_FULL = 30.f, W_TAIL = 100.f;
     float best = 1e30f;
     int bR = b->R, bW = b->tri_kind, bF = b->fft4, bJ = b->pcj, r = VV_OK;
     for (int pj = 0; pj <= (b->pcj_ok ? 1 : 0) && r == VV_OK; ++pj)
@@ -2237,17 +2270,15 @@ int b_autotune(vv_batch* b, std::vector<vv::BInst>& tab) {
         for (int R = 2; R <= (pj ? 2 : 8) && r == VV_OK; R *= 2) {
             b_shape(b, tab, R, tw, f4, pj);
             if ((r = b_apply_shape(b, tab)) != VV_OK) break;
-            for (int k = 0; k < 2 && r == VV_OK; ++k) r = b_pc<T>(b, vv::L_ALL, false, vv::BD_B);
-            cudaEventRecord(e0, b->st);
-            for (int k = 0; k < 5 && r == VV_OK; ++k) r = b_pc<T>(b, vv::L_ALL, false, vv::BD_B);
-            cudaEventRecord(e1, b->st);
-            float ms = 0.f;
-            const bool timed = r == VV_OK && cudaEventSynchronize(e1) == cudaSuccess &&
-                               cudaEventElapsedTime(&ms, e0, e1) == cudaSuccess;
-            if (timed && getenv("VV_DEBUG"))
-                fprintf(stderr, "[vv_batch] tune pcj=%d fft4=%d R=%d tri=%d: %.1f us\n", pj, f4, R, tw, ms * 200.f);
-            if (timed && ms < best) {
-                best = ms;
+            if ((r = tail_list()) != VV_OK) break;
+            const float tf = timed([&]() { return b_pc<T>(b, vv::L_ALL, false, vv::BD_B); }, 5, r);
+            const float tt = timed([&]() { return b_pc<T>(b, vv::L_TAIL, false, vv::BD_B); }, 5, r);
+            const float score = W_FULL * tf + W_TAIL * tt;
+            if (getenv("VV_DEBUG"))
+                fprintf(stderr, "[vv_batch] tune pcj=%d fft4=%d R=%d tri=%d: full %.1f us, tail %.1f us\n", pj, f4, R,
+                        tw, tf * 1e3f, tt * 1e3f);
+            if (r == VV_OK && score < best) {
+                best = score;
                 bR = R;
                 bW = tw;
                 bF = f4;
@@ -2255,30 +2286,32 @@ int b_autotune(vv_batch* b, std::vector<vv::BInst>& tab) {
             }
         }
     }
-    cudaEventDestroy(e0);
-    cudaEventDestroy(e1);
-    TRY(r);
-    b_shape(b, tab, bR, bW, bF, bJ);
-    TRY(b_apply_shape(b, tab));
-    // Jacobian stencil: 64 x 32 tiles or marching strips
-    float tj[2] = {1e30f, 1e30f};
-    CK(cudaEventCreate(&e0));
-    CK(cudaEventCreate(&e1));
+    if (r == VV_OK) {
+        b_shape(b, tab, bR, bW, bF, bJ);
+        r = b_apply_shape(b, tab);
+    }
+    if (r == VV_OK) r = tail_list();
+    // Jacobian stencil: 64 x 32 tiles or marching strips, by the same weights
+    float sj[2] = {1e30f, 1e30f};
     for (int m = 0; m <= 1 && r == VV_OK; ++m) {
         b->march = m;
-        for (int k = 0; k < 2 && r == VV_OK; ++k) r = b_jvp_all<T>(b);
-        cudaEventRecord(e0, b->st);
-        for (int k = 0; k < 5 && r == VV_OK; ++k) r = b_jvp_all<T>(b);
-        cudaEventRecord(e1, b->st);
-        float ms = 0.f;
-        if (r == VV_OK && cudaEventSynchronize(e1) == cudaSuccess && cudaEventElapsedTime(&ms, e0, e1) == cudaSuccess)
-            tj[m] = ms;
-        if (getenv("VV_DEBUG")) fprintf(stderr, "[vv_batch] tune march=%d: %.1f us\n", m, ms * 200.f);
+        const int* LT = blist(b, vv::L_TAIL);
+        const float tf = timed([&]() { return b_jvp_all<T>(b); }, 5, r);
+        const float tt = timed([&]() {
+            switch (b->scheme) {
+                case VV_BRACKET_J1: return b_jvp<1, vv::BS_X, T>(b, LT);
+                case VV_BRACKET_J2: return b_jvp<2, vv::BS_X, T>(b, LT);
+                default: return b_jvp<4, vv::BS_X, T>(b, LT);
+            }
+        }, 5, r);
+        sj[m] = W_FULL * tf + W_TAIL * tt;
+        if (getenv("VV_DEBUG")) fprintf(stderr, "[vv_batch] tune march=%d: full %.1f us, tail %.1f us\n", m, tf * 1e3f, tt * 1e3f);
     }
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
+    cudaFree(dmember);
     TRY(r);
-    b->march = tj[1] < tj[0] ? 1 : 0;
+    b->march = sj[1] < sj[0] ? 1 : 0;
     return VV_OK;
 }
 

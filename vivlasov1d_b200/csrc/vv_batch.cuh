@@ -27,7 +27,8 @@ enum BFam { F_TILE = 0, F_ROWS = 1, F_MODES = 2, F_VEC = 3, F_MOM = 4, F_INST = 
 // batch nx is a multiple of 64), segments of MARCH_SEG rows
 constexpr int MARCH_BW = 64, MARCH_SEG = 128;
 // work lists (one per mask)
-enum BList { L_ALL = 0, L_PIC = 1, L_GM = 2, L_GMR = 3, L_INNER = 4, L_REVERT = 5, NLIST = 6 };
+// L_TAIL: the batch autotuner's stand-in for the lockstep tail (the largest instances)
+enum BList { L_ALL = 0, L_PIC = 1, L_GM = 2, L_GMR = 3, L_INNER = 4, L_REVERT = 5, L_TAIL = 6, NLIST = 7 };
 
 // per-instance description read by the batched kernels (device-resident)
 struct BInst {
@@ -744,6 +745,12 @@ __global__ void __launch_bounds__(CTRL_THREADS)
 k_b_ctrl(const BInst* __restrict__ tab, int n, int op, unsigned long long handle, int* __restrict__ flag,
          unsigned int* __restrict__ counts, int* __restrict__ lists) {
     ctrl_run(tab, n, op, handle, flag, counts, lists);
+}
+
+// list l of the instances q with member[q] != 0 (one block of CTRL_THREADS)
+__global__ void __launch_bounds__(CTRL_THREADS)
+k_b_build_subset(const BInst* __restrict__ tab, int n, int* __restrict__ lists, int l, const int* __restrict__ member) {
+    ctrl_build(tab, n, lists, l, [&](int q) { return member[q] != 0; });
 }
 
 // End of an Arnoldi step: ||w|| and the Arnoldi bookkeeping of every
