@@ -54,7 +54,8 @@ enum vv_bracket {            /* solver.poisson_bracket                        */
 };
 enum vv_preconditioner {     /* solver.preconditioner_scheme                  */
     VV_PC_NONE = 0,
-    VV_PC_TENSOR_KINETIC = 1 /* TensorProductKineticFast.pyx                   */
+    VV_PC_TENSOR_KINETIC = 1,   /* TensorProductKineticFast.pyx                */
+    VV_PC_TENSOR_POTENTIAL = 2  /* TensorProductPotentialFast.pyx              */
 };
 enum vv_laplace {            /* solver.laplace_operator                       */
     VV_LAPLACE_CFD4 = 4      /* PETScPoissonCFD4.pyx (default)                 */
@@ -142,6 +143,12 @@ int vv_bracket(vv_ctx* ctx, const double* X, double* Y, double factor);
 /* tensorProduct(X, Y): Y = P^-1 X     TensorProductKinetic.pyx:345-359,
  * TensorProductKineticFast.pyx:102-224.  X and Y may alias. */
 int vv_pc_apply(vv_ctx* ctx, const double* X, double* Y);
+/* update_matrices() of the potential preconditioner: its x-tridiagonal
+ * matrices are built from phi (nx values; the solver's phi at update_history)
+ * TensorProductPotentialFast.pyx:205-266, PETScVlasovSolver.pyx:135-140.
+ * The time step (vv_step) takes phi at its own make_history.  A no-op for the
+ * other preconditioners. */
+int vv_pc_set_potential(vv_ctx* ctx, const double* phi);
 
 /* ---- Toolbox ------------------------------------------------------------ */
 /* compute_density / compute_velocity_density / compute_energy_density /

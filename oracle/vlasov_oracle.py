@@ -333,6 +333,65 @@ class TensorKineticPreconditioner:
 
 
 # --------------------------------------------------------------------------
+# FFT tensor-product potential preconditioner
+#   (preconditioner/TensorProductPotential.pyx:157-183,
+#    TensorProductPotentialFast.pyx:43-266)
+# --------------------------------------------------------------------------
+def potential_banded_matrix(grid, eigen, phi):
+    """LAPACK band storage (LDAB=4, KL=KU=1) of the x-tridiagonal matrix of
+    one v mode, built from phi with periodic differences and no corner
+    entries (TensorProductPotentialFast.pyx:219-260)."""
+    nx = grid.nx
+    phi = np.asarray(phi, dtype=np.float64)
+    arak_fac_J1 = 0.5 * grid.hx_inv * grid.hv_inv / 12.
+    diagm = np.zeros(nx, dtype=np.complex128)
+    diag = np.ones(nx, dtype=np.complex128)
+    diagp = np.zeros(nx, dtype=np.complex128)
+    for i in range(nx):
+        im = (i - 1) % nx
+        ip = (i + 1) % nx
+        diagm[i] = eigen * 1.0 * (phi[i] - phi[im]) * arak_fac_J1
+        diag[i] = eigen * 2.0 * (phi[ip] - phi[im]) * arak_fac_J1 + grid.ht_inv
+        diagp[i] = eigen * 1.0 * (phi[ip] - phi[i]) * arak_fac_J1
+    m = np.zeros((4, nx), dtype=np.complex128, order="F")
+    m[1, 1:] = diagp[:-1]
+    m[2, :] = diag[:]
+    m[3, :-1] = diagm[1:]
+    return m
+
+
+class TensorPotentialPreconditioner:
+    """``P^-1``: rFFT along v per x column -> banded solve in x per v mode
+    (zgbtrf/zgbtrs, matrices from phi) -> normalised irFFT along v."""
+
+    def __init__(self, grid, phi=None):
+        self.grid = grid
+        self.eigen = compute_eigenvalues(grid.nv)
+        self.update_matrices(np.zeros(grid.nx) if phi is None else phi)
+
+    def update_matrices(self, phi):        # TensorProductPotentialFast.pyx:205-217
+        self.lu, self.piv, self.raw = [], [], []
+        for k in range(self.grid.nv // 2 + 1):
+            m = potential_banded_matrix(self.grid, self.eigen[k], phi)
+            self.raw.append(m.copy())
+            lu, piv, info = lapack.zgbtrf(m, 1, 1)
+            if info != 0:
+                raise RuntimeError("zgbtrf failed for mode %d (info=%d)" % (k, info))
+            self.lu.append(lu)
+            self.piv.append(piv)
+
+    def apply(self, X):
+        """``Y = P^-1 X`` for an (nx, nv) field."""
+        spec = np.fft.rfft(np.asarray(X, dtype=np.float64), axis=1)   # fft(): r2c along v per x
+        for k in range(spec.shape[1]):                                # solve(): zgbtrs per v mode
+            x, info = lapack.zgbtrs(self.lu[k], 1, 1, spec[:, k].copy(), self.piv[k])
+            if info != 0:
+                raise RuntimeError("zgbtrs failed")
+            spec[:, k] = x
+        return np.fft.irfft(spec, n=self.grid.nv, axis=1)            # ifft(): c2r, normalised 1/nv
+
+
+# --------------------------------------------------------------------------
 # moments  (toolbox/Toolbox.pyx:79-165)
 # --------------------------------------------------------------------------
 def moments(f, grid):
@@ -539,12 +598,19 @@ class VlasovSolver:
         self.grid = grid
         self.h0v = np.asarray(h0v, dtype=np.float64)
         self.scheme = scheme
-        self.pc = TensorKineticPreconditioner(grid) if preconditioner == "tensor_kinetic" else None
+        if preconditioner == "tensor_kinetic":
+            self.pc = TensorKineticPreconditioner(grid)
+        elif preconditioner == "tensor_potential":
+            self.pc = TensorPotentialPreconditioner(grid)
+        else:
+            self.pc = None
         self.Fh = None
         self.Have = None
 
-    def update_history(self, F):           # PETScVlasovSolver.pyx:135-140
+    def update_history(self, F, phi=None):  # PETScVlasovSolver.pyx:135-140
         self.Fh = F.copy()
+        if phi is not None and isinstance(self.pc, TensorPotentialPreconditioner):
+            self.pc.update_matrices(phi)   # the solver's phi at make_history
 
     def update_previous(self, h1p, h1h, h2p=None, h2h=None):  # :142-157
         self.Have = have_field(self.h0v, h1p, h1h, h2p, h2h)
@@ -621,7 +687,7 @@ class Run:
         self.fh = self.fc.copy()
         self.h1h = self.h1c.copy()
         self.h2h = self.h2c.copy()
-        self.solver.update_history(self.fc)
+        self.solver.update_history(self.fc, self.phi)
 
     def update_previous(self):
         self.solver.update_previous(self.h1c, self.h1h, self.h2c, self.h2h)

@@ -15,7 +15,8 @@ petsc4py exists in this image, so its extensions cannot be compiled.  Its
   4. calls the reference's methods (PoissonBracket J1/J2/J4, TimeDerivative,
      PETScVlasovSolver function/jacobian/update_previous/function_norm,
      Toolbox moments and initialisers, PETScPoissonCFD4 RHS/matvec/residual,
-     TensorProduct eigenvalues and banded preconditioner matrices, and the
+     TensorProduct eigenvalues and banded preconditioner matrices (kinetic
+     and potential), and the
      DistributionFunction/Hamiltonian/Potential invariant diagnostics) on
      seeded inputs, and writes their outputs to ``golden_<nx>x<nv>.npz``.
 
@@ -213,6 +214,12 @@ class Vec:
         else:
             self.a[np.asarray(idx)] = vals
 
+    def getValues(self, idx):
+        return self.a[np.asarray(list(idx))].copy()
+
+    def destroy(self):
+        pass
+
     def __getitem__(self, k):
         return self.a[k]
 
@@ -294,7 +301,25 @@ class DMDA1:
         l.a[:] = g.a[xi]
 
 
-PETSc = types.SimpleNamespace(InsertMode=InsertMode)
+class _Scatter:
+    """Scatter.toAll for one process: a copy of the whole vector."""
+
+    @staticmethod
+    def toAll(vec):
+        return _Scatter(), vec.copy()
+
+    def begin(self, *args):
+        pass
+
+    def end(self, *args):
+        pass
+
+    def destroy(self):
+        pass
+
+
+PETSc = types.SimpleNamespace(InsertMode=InsertMode, Scatter=_Scatter,
+                              ScatterMode=types.SimpleNamespace(FORWARD="forward"))
 
 
 class Config:
@@ -353,6 +378,10 @@ def reference_namespace():
                                 "formBandedPreconditionerMatrix")
     exec(banded_src, ns)
     ns["formBandedPreconditionerMatrix_fn"] = ns["formBandedPreconditionerMatrix"]
+    pot = dict(ns)
+    exec(extract_method("vlasov/solvers/preconditioner/TensorProductPotentialFast.pyx",
+                        "formBandedPreconditionerMatrix"), pot)
+    ns["formBandedPotential_fn"] = pot["formBandedPreconditionerMatrix"]
     return ns
 
 
@@ -465,6 +494,19 @@ def make_case(ns, nx, nv, L, vmin, vmax, ht, seed):
         ns["formBandedPreconditionerMatrix_fn"](holder, m, eig[k])
         bands[k] = m
     out["bands"] = bands
+    # potential preconditioner (TensorProductPotentialFast.pyx:219-260): v
+    # eigenvalues and x-band matrices built from phi_p
+    eig_v = ns["TensorProductPreconditioner"].compute_eigenvalues(None, nv)
+    out["eigen_v"] = eig_v
+    phiv = Vec(nx)
+    phiv.a[:] = phip
+    holder_p = types.SimpleNamespace(grid=grid, phi=phiv)
+    bands_pot = np.zeros((nv // 2 + 1, 4, nx), dtype=np.complex128)
+    for k in range(nv // 2 + 1):
+        m = np.zeros((4, nx), dtype=np.complex128, order="F")
+        ns["formBandedPotential_fn"](holder_p, m, eig_v[k])
+        bands_pot[k] = m
+    out["bands_pot"] = bands_pot
 
     # initial data (Toolbox.pyx:190-224)
     F0 = da1.createGlobalVec()

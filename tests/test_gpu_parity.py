@@ -588,3 +588,118 @@ def test_any_nx_mixed_precision_field_energy():
         assert r32.step()["ksp_failures"] == 0
     a, b = r32.invariants()["field_energy"], r64.invariants()["field_energy"]
     assert abs(a - b) <= 1e-9 * abs(b)
+
+
+# ---------------------------------------------------------------------------
+# the potential preconditioner (tensor_potential)
+# ---------------------------------------------------------------------------
+@pytest.mark.parametrize("shape", [(16, 32), (64, 256), (128, 128), (15, 24), (100, 201), (33, 50), (256, 2048)])
+def test_potential_preconditioner_matches_oracle(shape):
+    """vv_pc_apply of a tensor_potential context (v FFTs as row transforms of
+    the transposed field, x solves by elimination with partial pivoting)
+    against the oracle (numpy FFTs, LAPACK zgbtrf/zgbtrs) to 1e-12; power-of-
+    two and other nv, matrices from a smooth and a rough phi."""
+    from vivlasov1d_b200 import Grid, TensorProductPreconditioner
+    nx, nv = shape
+    og = vo.Grid(nx, nv, 4 * np.pi, 8.0, ht=0.05)
+    grid = Grid(nx, nv, 4 * np.pi, 8.0, ht=0.05)
+    rng = np.random.default_rng(nx * 7 + nv)
+    xg = np.arange(nx) * og.hx
+    for phi in (0.3 * np.cos(0.5 * xg) + 0.1 * np.sin(1.5 * xg), 0.5 * rng.standard_normal(nx).cumsum()):
+        x = rng.standard_normal((nx, nv))
+        pc = TensorProductPreconditioner.create("tensor_potential", grid=grid, phi=xdev(phi))
+        X, Y = dev(x), grid.field()
+        pc.tensorProduct(X, Y)
+        ref = vo.TensorPotentialPreconditioner(og, phi).apply(x)
+        assert rel(host(Y), ref) < 1e-12
+
+
+def test_potential_preconditioner_golden_bands():
+    """The GPU operator with phi_p of the golden fixtures inverts the
+    reference's own x-band matrices (A assembled from golden bands_pot)."""
+    from vivlasov1d_b200 import TensorProductPreconditioner
+    for path in GOLDEN:
+        g = dict(np.load(path))
+        if int(g["nv"]) % 2:
+            continue
+        grid = ggrid(g)
+        nx, nv = int(g["nx"]), int(g["nv"])
+        rng = np.random.default_rng(5)
+        x = rng.standard_normal((nx, nv))
+        spec = np.fft.rfft(x, axis=1)
+        out = np.empty_like(spec)
+        for k in range(spec.shape[1]):
+            b = g["bands_pot"][k]
+            y = b[2] * spec[:, k]
+            y[:-1] += b[1, 1:] * spec[1:, k]
+            y[1:] += b[3, :-1] * spec[:-1, k]
+            out[:, k] = y
+        Ax = np.fft.irfft(out, n=nv, axis=1)
+        pc = TensorProductPreconditioner.create("tensor_potential", grid=grid, phi=xdev(g["phi_p"]))
+        Y = grid.field()
+        pc.tensorProduct(dev(Ax), Y)
+        assert rel(host(Y), x) < 1e-11, path
+
+
+def _potential_cfg(nx, nv, **solver):
+    cfg = _example_cfg(nx, nv, **solver)
+    cfg["solver"]["preconditioner_scheme"] = "tensor_potential"
+    return cfg
+
+
+@pytest.mark.parametrize("nx,nv", [(64, 256), (50, 101)])
+def test_potential_step_matches_oracle(nx, nv):
+    """One implicit step with the tensor_potential preconditioner (matrices
+    from the phi of make_history, as jeans_weak.cfg runs) against the oracle's
+    step: same Picard count, f to 1e-10."""
+    from vivlasov1d_b200.run import Run
+    og = vo.Grid(nx, nv, 4 * np.pi, 10.0, -10.0, ht=0.1)
+    f0 = vo.initialise_distribution_function(og, vo.f0_landau(0.2))
+    run = Run(_potential_cfg(nx, nv), f0=torch.from_numpy(vo.to_flat(f0)))
+    orun = vo.Run(og, f0, preconditioner="tensor_potential", ksp_rtol=1e-10, snes_atol=1e-12)
+    for _ in range(2):
+        rep = run.step()
+        orep = orun.step()
+        assert rep["picard_its"] == orep.picard_its, (rep, orep.picard_its)
+    assert rel(host(run.fc), orun.fc) < 1e-10
+
+
+def test_potential_mixed_precision_field_energy():
+    """Mixed precision with the potential preconditioner: field energy within
+    1e-9 of the FP64 run after three steps (64 x 256)."""
+    from vivlasov1d_b200.run import Run
+    og = vo.Grid(64, 256, 4 * np.pi, 10.0, -10.0, ht=0.1)
+    f0 = torch.from_numpy(vo.to_flat(vo.initialise_distribution_function(og, vo.f0_landau(0.2))))
+    cfg = _potential_cfg(64, 256, petsc_ksp_rtol=1e-4)
+    r64 = Run(cfg, f0=f0)
+    r32 = Run(cfg, f0=f0, precision="mixed")
+    for _ in range(3):
+        r64.step()
+        assert r32.step()["ksp_failures"] == 0
+    a, b = r32.invariants()["field_energy"], r64.invariants()["field_energy"]
+    assert abs(a - b) <= 1e-9 * abs(b)
+
+
+def test_potential_solver_class_update_history():
+    """The solver-class path: update_history rebuilds the potential
+    preconditioner from the solver's phi, and jacobian() applies it
+    (PETScVlasovSolver.pyx:135-140, 160-166), against the oracle solver."""
+    from vivlasov1d_b200 import Grid, PETScVlasovSolver
+    nx, nv = 32, 64
+    og = vo.Grid(nx, nv, 4 * np.pi, 8.0, ht=0.05)
+    grid = Grid(nx, nv, 4 * np.pi, 8.0, ht=0.05)
+    rng = np.random.default_rng(9)
+    phi = 0.2 * np.cos(0.5 * np.arange(nx) * og.hx)
+    h1 = phi - phi.mean()
+    F = np.abs(rng.standard_normal((nx, nv)))
+    PHI = xdev(phi)
+    s = PETScVlasovSolver({"poisson_bracket": "arakawaj4", "preconditioner": "tensor_potential"}, None, None, grid,
+                          None, xdev(h1), xdev(h1), None, None, PHI)
+    s.update_history(dev(F))
+    s.update_previous(dev(F))
+    Y = grid.field()
+    s.jacobian(dev(F), Y)
+    os_ = vo.VlasovSolver(og, vo.kinetic_hamiltonian_v(og), "arakawaj4", "tensor_potential")
+    os_.update_history(F, phi)
+    os_.update_previous(h1, h1)
+    assert rel(host(Y), os_.jacobian(F)) < 1e-12

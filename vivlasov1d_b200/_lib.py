@@ -18,7 +18,7 @@ VV_ERR_UNSUPPORTED = 2
 VV_ERR_DIVERGED = 5
 NOALLOC_MAX_NX = 16384      # VV_NOALLOC_MAX_NX: largest nx of vv_invariants_noalloc
 BRACKET = {"arakawaj1": 1, "arakawaj2": 2, "arakawaj4": 4}
-PC_NONE, PC_TENSOR_KINETIC = 0, 1
+PC_NONE, PC_TENSOR_KINETIC, PC_TENSOR_POTENTIAL = 0, 1, 2
 LAPLACE = {"cfd4": 4}
 ORDER_FACTORED, ORDER_REFERENCE = 0, 1
 PRECISION = {"fp64": 0, "mixed": 1}
@@ -90,6 +90,7 @@ SIGNATURES = {
     "vv_function_norm": (I, [P, P, P, C.POINTER(D)]),
     "vv_bracket": (I, [P, P, P, D]),
     "vv_pc_apply": (I, [P, P, P]),
+    "vv_pc_set_potential": (I, [P, P]),
     "vv_moments": (I, [P, P, P, P, P, P]),
     "vv_potential_to_hamiltonian": (I, [P, P, P]),
     "vv_poisson_rhs": (I, [P, P, P]),

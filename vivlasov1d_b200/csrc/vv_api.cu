@@ -14,6 +14,7 @@
 #include "vv_vec.cuh"
 #include "vv_batch.cuh"
 #include "vv_adjoint.cuh"
+#include "vv_pcv.cuh"
 
 #include <algorithm>
 #include <array>
@@ -34,6 +35,14 @@ struct vv_ctx {
     int nx, nv, M, logM, nmodes, restart;
     size_t ncell;
     double hx, hv, ht_inv, hx_inv, hv_inv, hx2_inv, f1, f2;
+    // the potential preconditioner (VV_PC_TENSOR_POTENTIAL): v modes, eigenvalues
+    // for n = nv, nv twiddles, transposed field, v spectrum, elimination
+    // scratch (FP32 copies in the mixed mode), rows per CTA of the v FFT, phi
+    int nmv, pvR;
+    double2 *lamv, *twv, *pv_spec, *pv_scr;
+    double *pv_xt, *phipc;
+    float2 *twv32, *pv_spec32, *pv_scr32;
+    float* pv_xt32;
     cudaStream_t st;      // the caller's stream
     int device;
     // device buffers
@@ -461,7 +470,7 @@ int raise_smem_limits(int* limit_out) {
 // float: the mixed mode's FP32 copies) and output type TO.  Y may be a GMRES
 // basis base pointer with yidx -> the vector index (+yoff).
 template <typename TI, typename R, typename TO>
-int pc_apply_t(vv_ctx* c, const TI* X, TO* Y, const int* yidx = nullptr, int yoff = 0) {
+int pck_apply_t(vv_ctx* c, const TI* X, TO* Y, const int* yidx = nullptr, int yoff = 0) {
     constexpr bool D = std::is_same<R, double>::value;
     using C2 = typename Cplx<R>::type;
     vv::PcParams p = pcparams(c);
@@ -495,6 +504,61 @@ int pc_apply_t(vv_ctx* c, const TI* X, TO* Y, const int* yidx = nullptr, int yof
     p.yoff = yoff;
     p.ystride = yidx ? c->ncell : 0;
     return launch_irfft<R, TO>(c, spec, Y, p, rows);
+}
+
+// The potential preconditioner: the v transforms as row transforms of the
+// transposed field (radix-2 FFT for a power-of-two nv, else the direct DFT),
+// the x-tridiagonal systems per v mode by elimination with partial pivoting
+template <typename TI, typename R, typename TO>
+int pcv_apply_t(vv_ctx* c, const TI* X, TO* Y, const int* yidx = nullptr, int yoff = 0) {
+    constexpr bool D = std::is_same<R, double>::value;
+    using C2 = typename Cplx<R>::type;
+    const int nx = c->nx, nv = c->nv;
+    R* xt = D ? reinterpret_cast<R*>(c->pv_xt) : reinterpret_cast<R*>(c->pv_xt32);
+    C2* spec = D ? reinterpret_cast<C2*>(c->pv_spec) : reinterpret_cast<C2*>(c->pv_spec32);
+    C2* scr = D ? reinterpret_cast<C2*>(c->pv_scr) : reinterpret_cast<C2*>(c->pv_scr32);
+    const dim3 tb(32, 8);
+    vv::k_transpose<TI, R><<<dim3((nx + 31) / 32, (nv + 31) / 32), tb, 0, c->st>>>(X, xt, nv, nx, nullptr, 0, 0);
+    CKL(c);
+    vv::PcParams p;
+    p.nx = nv;   // rows of length nv ...
+    p.nv = nx;   // ... one per x point
+    p.M = nv / 2;
+    p.logM = is_pow2(nv) ? ilog2(nv / 2) : -1;
+    p.R = c->pvR;
+    p.tw = D ? (const void*)c->twv : (const void*)c->twv32;
+    p.yidx = nullptr;
+    p.yoff = 0;
+    p.ystride = 0;
+    const size_t csz = sizeof(C2);
+    const bool fft = is_pow2(nv);
+    const unsigned gr = (unsigned)((nx + c->pvR - 1) / c->pvR), gd = (unsigned)((nx + vv::DFT_ROWS - 1) / vv::DFT_ROWS);
+    if (fft) vv::k_rfft_rows<R, R><<<gr, 32 * c->pvR, fft_smem(0, nv / 2, c->pvR, csz, false), c->st>>>(xt, spec, p);
+    else vv::k_rdft_rows<R, R><<<gd, vv::DFT_THREADS, rdft_smem(nv, csz), c->st>>>(xt, spec, p);
+    CKL(c);
+    vv::PotParams q;
+    q.nx = nx;
+    q.nmv = c->nmv;
+    q.arak = 0.5 * c->hx_inv * c->hv_inv / 12.;   // TensorProductPotentialFast.pyx:237
+    q.ht_inv = c->ht_inv;
+    q.phi = c->phipc;
+    q.lam = c->lamv;
+    vv::k_pcv_solve<R><<<(unsigned)((c->nmv + 63) / 64), 64, 0, c->st>>>(spec, scr, q);
+    CKL(c);
+    if (fft) vv::k_irfft_rows<R, R><<<gr, 32 * c->pvR, fft_smem(0, nv / 2, c->pvR, csz, true), c->st>>>(spec, xt, p);
+    else vv::k_irdft_rows<R, R><<<gd, vv::DFT_THREADS, irdft_smem(nv, csz), c->st>>>(spec, xt, p);
+    CKL(c);
+    vv::k_transpose<R, TO><<<dim3((nv + 31) / 32, (nx + 31) / 32), tb, 0, c->st>>>(xt, Y, nx, nv, yidx, yoff,
+                                                                                   yidx ? c->ncell : 0);
+    CKL(c);
+    return VV_OK;
+}
+
+// P^-1 of the context's preconditioner
+template <typename TI, typename R, typename TO>
+int pc_apply_t(vv_ctx* c, const TI* X, TO* Y, const int* yidx = nullptr, int yoff = 0) {
+    if (c->g.preconditioner == VV_PC_TENSOR_POTENTIAL) return pcv_apply_t<TI, R, TO>(c, X, Y, yidx, yoff);
+    return pck_apply_t<TI, R, TO>(c, X, Y, yidx, yoff);
 }
 
 int pc_apply(vv_ctx* c, const double* X, double* Y, const int* yidx = nullptr, int yoff = 0) {
@@ -548,8 +612,11 @@ int adj_apply(vv_ctx* c, const double* X, const int* xidx, double* Y) {
 }
 
 // Y = P^-T X: the same FFT pair, conjugate-transposed mode solves
+// (the kinetic factors for the potential preconditioner too: any fixed P
+// serves the transposed solve, and P^-T of the potential preconditioner is
+// not built)
 int pcT_apply(vv_ctx* c, const double* X, double* Y, const int* yidx = nullptr, int yoff = 0) {
-    if (c->g.preconditioner != VV_PC_TENSOR_KINETIC) {
+    if (c->g.preconditioner == VV_PC_NONE) {
         if (yidx) return VV_ERR_UNSUPPORTED;
         return copy_d(c, Y, X, c->ncell);
     }
@@ -583,7 +650,7 @@ int apply_operator_t(vv_ctx* c, const T* X, T* Y) {
             return pcT_apply(c, c->tmp, Y);
         }
     }
-    if (c->g.preconditioner == VV_PC_TENSOR_KINETIC) {
+    if (c->g.preconditioner != VV_PC_NONE) {
         TRY(launch_bracket<vv::MODE_JVP, T>(c, X, nullptr, Buf<T>::tmp(c), 0.5, nullptr));
         return pc_apply_t<T, T, T>(c, Buf<T>::tmp(c), Y);
     }
@@ -608,14 +675,14 @@ int apply_operator_state(vv_ctx* c) {
     if constexpr (std::is_same<T, double>::value) {
         if (c->adj) {   // the adjoint solve: V[it+1] = P^-T A^T V[it]
             TRY(adj_apply(c, V, itp, c->tmp));
-            if (c->g.preconditioner == VV_PC_TENSOR_KINETIC) return pcT_apply(c, c->tmp, V, itp, 1);
+            if (c->g.preconditioner != VV_PC_NONE) return pcT_apply(c, c->tmp, V, itp, 1);
             k_copy_to_slot<double><<<grid1d(c->ncell, 256), 256, 0, c->st>>>(c->tmp, V, itp, c->ncell);
             CKL(c);
             return VV_OK;
         }
     }
     TRY(launch_bracket<vv::MODE_JVP, T>(c, V, nullptr, Buf<T>::tmp(c), 0.5, nullptr, itp));
-    if (c->g.preconditioner == VV_PC_TENSOR_KINETIC) return pc_apply_t<T, T, T>(c, Buf<T>::tmp(c), V, itp, 1);
+    if (c->g.preconditioner != VV_PC_NONE) return pc_apply_t<T, T, T>(c, Buf<T>::tmp(c), V, itp, 1);
     k_copy_to_slot<T><<<grid1d(c->ncell, 256), 256, 0, c->st>>>(Buf<T>::tmp(c), V, itp, c->ncell);
     CKL(c);
     return VV_OK;
@@ -927,6 +994,8 @@ int step_prologue(vv_ctx* c, vv_state* st) {
     if (st->h2c && st->h2h) TRY(copy_d(c, st->h2h, st->h2c, nx));
     if (st->phih) TRY(copy_d(c, st->phih, st->phi, nx));
     TRY(copy_d(c, c->Fh, st->f, n));
+    // update_history -> update_matrices of the potential preconditioner
+    if (c->g.preconditioner == VV_PC_TENSOR_POTENTIAL) TRY(copy_d(c, c->phipc, st->phi, nx));
     TRY(set_hxp(c, st->h1c, st->h1h, st->h2c, st->h2h));
     return step_residual(c, st, 0);
 }
@@ -936,12 +1005,12 @@ int step_prologue(vv_ctx* c, vv_state* st) {
 int step_rhs(vv_ctx* c, vv_state* st) {
     TRY(copy_d(c, c->fl, st->f, c->ncell));
     if (c->mixed) {   // FP64 residual -> FP32 right-hand side
-        if (c->g.preconditioner == VV_PC_TENSOR_KINETIC) return pc_apply_t<double, float, float>(c, c->tmp, c->bvec32);
+        if (c->g.preconditioner != VV_PC_NONE) return pc_apply_t<double, float, float>(c, c->tmp, c->bvec32);
         vv::k_scale<double, float><<<grid1d(c->ncell, 256), 256, 0, c->st>>>(c->tmp, c->bvec32, c->ncell, nullptr, 1.0);
         CKL(c);
         return VV_OK;
     }
-    if (c->g.preconditioner == VV_PC_TENSOR_KINETIC) return pc_apply(c, c->tmp, c->bvec);
+    if (c->g.preconditioner != VV_PC_NONE) return pc_apply(c, c->tmp, c->bvec);
     return copy_d(c, c->bvec, c->tmp, c->ncell);
 }
 
@@ -1231,7 +1300,9 @@ int vv_create(const vv_grid* grid, vv_ctx** out) {
     const vv_grid& g = *grid;
     if (g.nx < 4 || g.nv < 5 || !(g.L > 0.0) || !(g.vmax > g.vmin) || !(g.ht > 0.0)) return VV_ERR_ARG;
     if (g.bracket != VV_BRACKET_J1 && g.bracket != VV_BRACKET_J2 && g.bracket != VV_BRACKET_J4) return VV_ERR_ARG;
-    if (g.preconditioner != VV_PC_NONE && g.preconditioner != VV_PC_TENSOR_KINETIC) return VV_ERR_ARG;
+    if (g.preconditioner != VV_PC_NONE && g.preconditioner != VV_PC_TENSOR_KINETIC &&
+        g.preconditioner != VV_PC_TENSOR_POTENTIAL)
+        return VV_ERR_ARG;
     if (g.laplace != VV_LAPLACE_CFD4) return VV_ERR_UNSUPPORTED;
     const int restart = g.gmres_restart > 0 ? g.gmres_restart : 30;
     if (restart > vv::MAX_RESTART) return VV_ERR_ARG;
@@ -1421,6 +1492,49 @@ int vv_create(const vv_grid* grid, vv_ctx** out) {
             return fail_cuda(cudaGetLastError(), "vv_create upload (fp32)");
         }
     }
+    // the potential preconditioner: eigenvalues for n = nv (TensorProduct.pyx:109-116
+    // with the ifftshift), nv twiddles, buffers; phi starts at zero until
+    // vv_pc_set_potential or a step's make_history sets it
+    if (g.preconditioner == VV_PC_TENSOR_POTENTIAL) {
+        const int nmv = nv / 2 + 1;
+        c->nmv = nmv;
+        c->pvR = 4;
+        while (c->pvR > 1 && fft_smem(0, nv / 2, c->pvR, sizeof(double2), true) > 200 * 1024) c->pvR /= 2;
+        if ((s = dalloc(&c->lamv, nmv)) || (s = dalloc(&c->twv, (size_t)nv)) || (s = dalloc(&c->pv_xt, n)) ||
+            (s = dalloc(&c->pv_spec, (size_t)nmv * nx)) || (s = dalloc(&c->pv_scr, (size_t)3 * nmv * nx)) ||
+            (s = dalloc(&c->phipc, (size_t)nx)) ||
+            (c->mixed && ((s = dalloc(&c->twv32, (size_t)nv)) || (s = dalloc(&c->pv_xt32, n)) ||
+                          (s = dalloc(&c->pv_spec32, (size_t)nmv * nx)) ||
+                          (s = dalloc(&c->pv_scr32, (size_t)3 * nmv * nx))))) {
+            vv_destroy(c);
+            return s;
+        }
+        std::vector<cd> ev(nv);
+        for (int i = 0; i < nv; ++i) {
+            const double t2 = (twopi * (double)i) / (double)nv;
+            const double t1 = t2 * (double)(nv - 1);
+            ev[i] = cd(std::cos(t1), std::sin(t1)) - cd(std::cos(t2), std::sin(t2));
+        }
+        std::vector<double2> lv(nmv), twvh(nv);
+        std::vector<float2> twv32h(nv);
+        for (int k = 0; k < nmv; ++k) {
+            const cd L = ev[(k + nv / 2) % nv];
+            lv[k] = make_double2(L.real(), L.imag());
+        }
+        for (int k = 0; k < nv; ++k) {
+            const long double a = 2.0L * PI * (long double)k / (long double)nv;
+            twvh[k] = make_double2((double)cosl(a), (double)(-sinl(a)));
+            twv32h[k] = make_float2((float)twvh[k].x, (float)twvh[k].y);
+        }
+        if (cudaMemcpy(c->lamv, lv.data(), nmv * sizeof(double2), cudaMemcpyHostToDevice) != cudaSuccess ||
+            cudaMemcpy(c->twv, twvh.data(), nv * sizeof(double2), cudaMemcpyHostToDevice) != cudaSuccess ||
+            (c->mixed && cudaMemcpy(c->twv32, twv32h.data(), nv * sizeof(float2), cudaMemcpyHostToDevice) !=
+                             cudaSuccess) ||
+            cudaMemset(c->phipc, 0, nx * sizeof(double)) != cudaSuccess) {
+            vv_destroy(c);
+            return fail_cuda(cudaGetLastError(), "vv_create upload (potential preconditioner)");
+        }
+    }
     // dynamic shared memory limits (process-wide, raised once per device)
     {
         int limit = 0;
@@ -1465,7 +1579,8 @@ int vv_destroy(vv_ctx* c) {
                     c->xscratch, c->mom_part, c->spec, c->tw, c->lambda, c->dinv, c->alpha, c->gamma,
                     c->sym_inv, c->ds, c->V32, c->tmp32, c->bvec32, c->delta32, c->alpha32, c->gamma32,
                     c->spec32, c->tw32, c->lambda32, c->dinv32, c->adj_cH, c->adj_cF, c->adj_zpart,
-                    c->adj_zbuf, c->adj_q, c->adj_hprof, c->adj_h1a, c->adj_h1b};
+                    c->adj_zbuf, c->adj_q, c->adj_hprof, c->adj_h1a, c->adj_h1b, c->lamv, c->twv, c->pv_spec,
+                    c->pv_scr, c->pv_xt, c->phipc, c->twv32, c->pv_spec32, c->pv_scr32, c->pv_xt32};
     destroy_graph(c);
     for (int k = 0; k < 4; ++k)
         if (c->cs[k]) cudaStreamDestroy(c->cs[k]);
@@ -1504,7 +1619,7 @@ int vv_update_previous(vv_ctx* c, const double* h1p, const double* h1h, const do
 
 int vv_function(vv_ctx* c, const double* F, double* Y, int apply_pc) {
     if (!c || !F || !Y) return VV_ERR_ARG;
-    const bool pc = apply_pc && c->g.preconditioner == VV_PC_TENSOR_KINETIC;
+    const bool pc = apply_pc && c->g.preconditioner != VV_PC_NONE;
     TRY(launch_bracket<vv::MODE_RESIDUAL, double>(c, F, c->Fh, pc ? c->tmp : Y, 1.0, nullptr));
     if (pc) TRY(pc_apply(c, c->tmp, Y));
     return VV_OK;
@@ -1512,7 +1627,7 @@ int vv_function(vv_ctx* c, const double* F, double* Y, int apply_pc) {
 
 int vv_jacobian(vv_ctx* c, const double* F, double* Y, int apply_pc) {
     if (!c || !F || !Y) return VV_ERR_ARG;
-    const bool pc = apply_pc && c->g.preconditioner == VV_PC_TENSOR_KINETIC;
+    const bool pc = apply_pc && c->g.preconditioner != VV_PC_NONE;
     TRY(launch_bracket<vv::MODE_JVP, double>(c, F, nullptr, pc ? c->tmp : Y, 0.5, nullptr));
     if (pc) TRY(pc_apply(c, c->tmp, Y));
     return VV_OK;
@@ -1530,8 +1645,14 @@ int vv_bracket(vv_ctx* c, const double* X, double* Y, double factor) {
 
 int vv_pc_apply(vv_ctx* c, const double* X, double* Y) {
     if (!c || !X || !Y) return VV_ERR_ARG;
-    if (c->g.preconditioner != VV_PC_TENSOR_KINETIC) return copy_d(c, Y, X, c->ncell);
+    if (c->g.preconditioner == VV_PC_NONE) return copy_d(c, Y, X, c->ncell);
     return pc_apply(c, X, Y);
+}
+
+int vv_pc_set_potential(vv_ctx* c, const double* phi) {
+    if (!c || !phi) return VV_ERR_ARG;
+    if (c->g.preconditioner != VV_PC_TENSOR_POTENTIAL) return VV_OK;
+    return copy_d(c, c->phipc, phi, c->nx);
 }
 
 int vv_moments(vv_ctx* c, const double* F, double* n, double* u, double* e, double* a) {

@@ -109,8 +109,10 @@ class Context:
         g.bracket = _lib.BRACKET[bracket]
         if preconditioner in (None, "", "none"):
             g.preconditioner = _lib.PC_NONE
-        elif preconditioner == "tensor_kinetic":
+        elif preconditioner in ("tensor_kinetic", "tensor_kinetic_scipy"):
             g.preconditioner = _lib.PC_TENSOR_KINETIC
+        elif preconditioner in ("tensor_potential", "tensor_potential_scipy"):
+            g.preconditioner = _lib.PC_TENSOR_POTENTIAL
         else:
             raise NotImplementedError("preconditioner %r is not implemented on this path" % preconditioner)
         g.laplace = _lib.LAPLACE["cfd4"]
@@ -123,7 +125,8 @@ class Context:
         self.precision = precision
         self.charge, self.mass = float(charge), float(mass)
         self.bracket, self.preconditioner_type, self.order = bracket, preconditioner, order
-        self.has_pc = g.preconditioner == _lib.PC_TENSOR_KINETIC
+        self.has_pc = g.preconditioner != _lib.PC_NONE
+        self.pc_kind = g.preconditioner
         h = C.c_void_p()
         with torch.cuda.device(grid.device):
             check(lib.vv_create(C.byref(g), C.byref(h)), "vv_create")
@@ -201,6 +204,10 @@ class TensorProductPreconditioner:
             if context is None:
                 context = grid.context(preconditioner="tensor_kinetic")
             return TensorProductPreconditionerKinetic(context)
+        if type in ("tensor_potential", "tensor_potential_scipy"):
+            if context is None:
+                context = grid.context(preconditioner="tensor_potential")
+            return TensorProductPreconditionerPotential(context, phi)
         if type in (None, "", "none"):
             return None
         raise NotImplementedError("preconditioner %r is not implemented on this path" % type)
@@ -210,7 +217,7 @@ class TensorProductPreconditionerKinetic:
     """``P^-1`` = irFFT_x o (A_k^-1 in v) o rFFT_x (TensorProductKinetic.pyx:345-359)."""
 
     def __init__(self, context):
-        if not context.has_pc:
+        if context.pc_kind != _lib.PC_TENSOR_KINETIC:
             raise ValueError("context was created without the tensor_kinetic preconditioner")
         self.ctx = context
         self.grid = context.grid
@@ -229,6 +236,33 @@ class TensorProductPreconditionerKinetic:
 
     def update_matrices(self):
         """The kinetic matrices do not depend on phi (TensorProductKineticFast.pyx:244-245)."""
+
+
+class TensorProductPreconditionerPotential:
+    """``P^-1`` = irFFT_v o (A_k^-1 in x, from phi) o rFFT_v
+    (TensorProductPotential.pyx:157-183, TensorProductPotentialFast.pyx:43-266).
+
+    ``phi`` is kept by reference (an nx tensor) and read by
+    :meth:`update_matrices`, which the solver calls at ``update_history``."""
+
+    def __init__(self, context, phi=None):
+        if context.pc_kind != _lib.PC_TENSOR_POTENTIAL:
+            raise ValueError("context was created without the tensor_potential preconditioner")
+        self.ctx = context
+        self.grid = context.grid
+        self.phi = phi
+        self.eigen = TensorProductPreconditionerKinetic.compute_eigenvalues(self.grid.nv)
+        if phi is not None:
+            self.update_matrices()
+
+    def tensorProduct(self, X, Y):
+        self.ctx.call("vv_pc_apply", self.ctx.field(X, "X"), self.ctx.field(Y, "Y"))
+
+    def update_matrices(self):
+        """Rebuild the x-tridiagonal systems from the current phi
+        (TensorProductPotentialFast.pyx:205-266)."""
+        if self.phi is not None:
+            self.ctx.call("vv_pc_set_potential", self.ctx.xprof(self.phi, "phi"))
 
 
 # ---------------------------------------------------------------------------
@@ -259,7 +293,7 @@ class PETScVlasovSolver:
                                 order=order, restart=restart)
         self.H0, self.H1p, self.H1h, self.H2p, self.H2h = H0, H1p, H1h, H2p, H2h
         self.phi = phi
-        self.preconditioner = TensorProductPreconditioner.create(pc, grid=grid, context=self.ctx) \
+        self.preconditioner = TensorProductPreconditioner.create(pc, grid=grid, phi=phi, context=self.ctx) \
             if pc else None
         self.Np = self.Up = self.Ep = self.Ap = None
         self.Nh = self.Uh = self.Eh = self.Ah = None
@@ -270,6 +304,8 @@ class PETScVlasovSolver:
 
     def update_history(self, F):                               # :135-140
         self.ctx.call("vv_update_history", self.ctx.field(F, "F"))
+        if self.preconditioner is not None:
+            self.preconditioner.update_matrices()
 
     def update_previous(self, F=None):                         # :142-157
         c = self.ctx
