@@ -58,7 +58,9 @@ enum vv_preconditioner {     /* solver.preconditioner_scheme                  */
     VV_PC_TENSOR_POTENTIAL = 2  /* TensorProductPotentialFast.pyx              */
 };
 enum vv_laplace {            /* solver.laplace_operator                       */
-    VV_LAPLACE_CFD4 = 4      /* PETScPoissonCFD4.pyx (default)                 */
+    VV_LAPLACE_CFD2 = 2,     /* PETScPoissonCFD2.pyx                           */
+    VV_LAPLACE_CFD4 = 4,     /* PETScPoissonCFD4.pyx (default)                 */
+    VV_LAPLACE_SIMPSON = 5   /* PETScPoissonSimpson.pyx                        */
 };
 enum vv_order {              /* arithmetic of the bracket kernels             */
     VV_ORDER_FACTORED = 0,   /* separable-h coefficient form (fast, default)   */

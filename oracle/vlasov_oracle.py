@@ -415,19 +415,35 @@ def poisson_rhs(n, charge):
     return -(n - nmean) * charge
 
 
-def poisson_matvec(x, hx2_inv):
-    """CFD4 ``(5,-32,54,-32,5)/(12 hx^2)`` periodic (PETScPoissonCFD4.pyx:146-160)."""
+# laplace_operator: the periodic 5-point stencil (a0, a1, a2) / den hx^-2 and
+# its Fourier symbol (a0 + 2 a1 cos t + 2 a2 cos 2t) / den hx^-2
+LAPLACE = {
+    "cfd2": (2., -1., 0., 1.),       # PETScPoissonCFD2.pyx:64-101
+    "cfd4": (54., -32., 5., 12.),    # PETScPoissonCFD4.pyx:146-183
+    "simpson": (30., -16., 1., 12.),  # PETScPoissonSimpson.pyx:62-101
+}
+
+
+def poisson_matvec(x, hx2_inv, laplace="cfd4"):
+    """``A x`` of the chosen Laplacian, periodic (the matrix_mult of
+    PETScPoissonCFD4.pyx:146-160, PETScPoissonCFD2.pyx:64-78,
+    PETScPoissonSimpson.pyx:62-76, in their operation order)."""
     r = np.roll
+    if laplace == "cfd2":
+        return (2. * x - r(x, 1) - r(x, -1)) * hx2_inv
+    if laplace == "simpson":
+        return (1. * r(x, 2) - 16. * r(x, 1) + 30. * x - 16. * r(x, -1) + 1. * r(x, -2)) * hx2_inv / 12.
     return (5. * r(x, 2) - 32. * r(x, 1) + 54. * x - 32. * r(x, -1) + 5. * r(x, -2)) * hx2_inv / 12.
 
 
-def poisson_function(x, n, hx2_inv, charge):
-    """Poisson residual ``A x + (n - mean n) * charge`` (PETScPoissonCFD4.pyx:163-183)."""
+def poisson_function(x, n, hx2_inv, charge, laplace="cfd4"):
+    """Poisson residual ``A x + (n - mean n) * charge`` (function_mult of
+    the three operators, e.g. PETScPoissonCFD4.pyx:163-183)."""
     nmean = n.sum() / n.size
-    return poisson_matvec(x, hx2_inv) + (n - nmean) * charge
+    return poisson_matvec(x, hx2_inv, laplace) + (n - nmean) * charge
 
 
-def poisson_solve(n, grid, charge):
+def poisson_solve(n, grid, charge, laplace="cfd4"):
     """Solve ``A phi = b`` on the mean-free subspace.
 
     The reference solves the singular periodic system with PETSc CG (rtol
@@ -437,7 +453,8 @@ def poisson_solve(n, grid, charge):
     b = poisson_rhs(n, charge)
     nx = grid.nx
     th = 2. * np.pi * np.arange(nx // 2 + 1) / nx
-    sym = (54. - 64. * np.cos(th) + 10. * np.cos(2. * th)) * grid.hx2_inv / 12.
+    a0, a1, a2, den = LAPLACE[laplace]
+    sym = (a0 + 2. * a1 * np.cos(th) + 2. * a2 * np.cos(2. * th)) * grid.hx2_inv / den
     bh = np.fft.rfft(b)
     ph = np.zeros_like(bh)
     ph[1:] = bh[1:] / sym[1:]
@@ -655,8 +672,9 @@ class Run:
     def __init__(self, grid, f0, scheme="arakawaj4", preconditioner="tensor_kinetic",
                  charge=-1.0, mass=1.0, ksp_rtol=1e-4, ksp_atol=1e-50,
                  ksp_max_it=1000, snes_atol=1e-10, snes_max_iter=20,
-                 normalise_f=True):
+                 normalise_f=True, laplace="cfd4"):
         self.grid = grid
+        self.laplace = laplace
         self.charge = charge
         self.mass = mass
         self.ksp = dict(rtol=ksp_rtol, atol=ksp_atol, max_it=ksp_max_it)
@@ -675,12 +693,12 @@ class Run:
 
     def calculate_moments(self):           # run_base.py:640-655
         self.n, self.u, self.e, self.a = moments(self.fc, self.grid)
-        self.phi = poisson_solve(self.n, self.grid, self.charge)
+        self.phi = poisson_solve(self.n, self.grid, self.charge, self.laplace)
         self.h1c = potential_to_hamiltonian(self.phi)
 
     def calculate_residual(self):          # run_base.py:631-637
         fnorm = self.solver.function_norm(self.fc)
-        pb = poisson_function(self.phi, self.n, self.grid.hx2_inv, self.charge)
+        pb = poisson_function(self.phi, self.n, self.grid.hx2_inv, self.charge, self.laplace)
         return fnorm + float(np.sqrt(np.dot(pb, pb)))
 
     def make_history(self):                # run_base.py:749-763

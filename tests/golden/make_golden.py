@@ -369,6 +369,11 @@ def reference_namespace():
     ps["PETScPoissonSolverBase"] = ps["PETScPoissonSolverBase"]
     load("vlasov/solvers/poisson/PETScPoissonCFD4.pyx", ps)
     ns["PETScPoissonSolverCFD4"] = ps["PETScPoissonSolver"]
+    for name, fn in (("CFD2", "PETScPoissonCFD2.pyx"), ("Simpson", "PETScPoissonSimpson.pyx")):
+        pv = dict(ns)
+        load("vlasov/solvers/poisson/PETScPoissonSolver.pyx", pv)
+        load("vlasov/solvers/poisson/" + fn, pv)
+        ns["PETScPoissonSolver" + name] = pv["PETScPoissonSolver"]
     ns["boltzmannian_grid"] = None
     ns["maxwellian_grid"] = None
     load("vlasov/core/distribution_function.pyx", ns)
@@ -483,6 +488,13 @@ def make_case(ns, nx, nv, L, vmin, vmax, ht, seed):
     out["poisson_matvec"] = Y.a.copy()
     ps.function_mult(P, N, Y)
     out["poisson_function"] = Y.a.copy()
+    # the other laplace_operator choices (PETScPoissonCFD2.pyx, PETScPoissonSimpson.pyx)
+    for name in ("CFD2", "Simpson"):
+        pso = ns["PETScPoissonSolver" + name](dax, nx, hx, -1.0)
+        pso.matrix_mult(P, Y)
+        out["poisson_matvec_" + name.lower()] = Y.a.copy()
+        pso.function_mult(P, N, Y)
+        out["poisson_function_" + name.lower()] = Y.a.copy()
 
     # preconditioner eigenvalues and band matrices
     eig = ns["TensorProductPreconditioner"].compute_eigenvalues(None, nx)

@@ -41,8 +41,8 @@ def test_create_rejects_bad_grid_without_gpu():
                      bracket=4, preconditioner=1, laplace=4, order=0, gmres_restart=30)
     h = C.c_void_p()
     assert lib.vv_create(C.byref(g), C.byref(h)) == 1  # VV_ERR_ARG
-    g.nx, g.nv, g.laplace = 12, 32, 2
-    assert lib.vv_create(C.byref(g), C.byref(h)) == 2  # VV_ERR_UNSUPPORTED (Laplacian other than CFD4)
+    g.nx, g.nv, g.laplace = 12, 32, 3
+    assert lib.vv_create(C.byref(g), C.byref(h)) == 2  # VV_ERR_UNSUPPORTED (no Laplacian with that code)
 
 
 def test_product_does_not_import_oracle():

@@ -166,3 +166,19 @@ def test_potential_preconditioner_inverts_band_operator(golden):
         out[:, k] = y
     Ax = np.fft.irfft(out, n=g.nv, axis=1)
     assert relerr(pc.apply(Ax), x) < 1e-12
+
+
+@pytest.mark.parametrize("laplace", ["cfd2", "simpson"])
+def test_poisson_operator_variants(golden, laplace):
+    """The CFD2 and Simpson Laplacians (matrix_mult, function_mult) equal the
+    reference's own, and the circulant solve inverts them on the mean-free
+    subspace."""
+    g = _grid(golden)
+    n = golden["n"]
+    assert relerr(vo.poisson_matvec(golden["phi_p"], g.hx2_inv, laplace),
+                  golden["poisson_matvec_" + laplace]) < 1e-13
+    assert relerr(vo.poisson_function(golden["phi_p"], n, g.hx2_inv, -1.0, laplace),
+                  golden["poisson_function_" + laplace]) < 1e-13
+    phi = vo.poisson_solve(n, g, -1.0, laplace)
+    r = vo.poisson_function(phi, n, g.hx2_inv, -1.0, laplace)
+    assert np.max(np.abs(r)) < 1e-12 * max(1.0, np.max(np.abs(golden["poisson_rhs"])))

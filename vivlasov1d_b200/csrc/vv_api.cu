@@ -35,6 +35,7 @@ struct vv_ctx {
     int nx, nv, M, logM, nmodes, restart;
     size_t ncell;
     double hx, hv, ht_inv, hx_inv, hv_inv, hx2_inv, f1, f2;
+    double lap[4];   // the Laplacian: stencil a0, a1, a2 and denominator (x hx^-2)
     // the potential preconditioner (VV_PC_TENSOR_POTENTIAL): v modes, eigenvalues
     // for n = nv, nv twiddles, transposed field, v spectrum, elimination
     // scratch (FP32 copies in the mixed mode), rows per CTA of the v FFT, phi
@@ -702,6 +703,10 @@ vv::PoissonParams pparams(const vv_ctx* c) {
     p.inv_nx = 1.0 / c->nx;
     p.tw = c->tw;
     p.sym_inv = c->sym_inv;
+    p.la0 = c->lap[0];
+    p.la1 = c->lap[1];
+    p.la2 = c->lap[2];
+    p.lden = c->lap[3];
     return p;
 }
 
@@ -719,12 +724,13 @@ int moments_poisson(vv_ctx* c, const double* F, double* n, double* u, double* e,
 
 __global__ void k_poisson_apply(const double* __restrict__ x, const double* __restrict__ n,
                                 double* __restrict__ y, int nx, double hx2_inv, double charge, int mode,
-                                double* __restrict__ sumsq) {
-    vv::poisson_apply_cta(x, n, y, nx, hx2_inv, charge, mode, sumsq);
+                                double* __restrict__ sumsq, double a0, double a1, double a2, double den) {
+    vv::poisson_apply_cta(x, n, y, nx, hx2_inv, charge, mode, sumsq, a0, a1, a2, den);
 }
 
 int poisson_apply(vv_ctx* c, const double* x, const double* n, double* y, int mode, double* sumsq) {
-    k_poisson_apply<<<1, 1024, 0, c->st>>>(x, n, y, c->nx, c->hx2_inv, c->g.charge, mode, sumsq);
+    k_poisson_apply<<<1, 1024, 0, c->st>>>(x, n, y, c->nx, c->hx2_inv, c->g.charge, mode, sumsq, c->lap[0], c->lap[1],
+                                           c->lap[2], c->lap[3]);
     CKL(c);
     return VV_OK;
 }
@@ -1303,7 +1309,8 @@ int vv_create(const vv_grid* grid, vv_ctx** out) {
     if (g.preconditioner != VV_PC_NONE && g.preconditioner != VV_PC_TENSOR_KINETIC &&
         g.preconditioner != VV_PC_TENSOR_POTENTIAL)
         return VV_ERR_ARG;
-    if (g.laplace != VV_LAPLACE_CFD4) return VV_ERR_UNSUPPORTED;
+    if (g.laplace != VV_LAPLACE_CFD4 && g.laplace != VV_LAPLACE_CFD2 && g.laplace != VV_LAPLACE_SIMPSON)
+        return VV_ERR_UNSUPPORTED;
     const int restart = g.gmres_restart > 0 ? g.gmres_restart : 30;
     if (restart > vv::MAX_RESTART) return VV_ERR_ARG;
     if (g.precision != VV_PRECISION_FP64 && g.precision != VV_PRECISION_MIXED) return VV_ERR_ARG;
@@ -1333,6 +1340,11 @@ int vv_create(const vv_grid* grid, vv_ctx** out) {
     c->hx_inv = 1. / c->hx;
     c->hv_inv = 1. / c->hv;
     c->hx2_inv = 1. / (c->hx * c->hx);
+    {   // the Laplacian's stencil (matrix_mult of PETScPoissonCFD2/CFD4/Simpson.pyx)
+        const double cfd2[4] = {2., -1., 0., 1.}, cfd4[4] = {54., -32., 5., 12.}, simp[4] = {30., -16., 1., 12.};
+        const double* l = g.laplace == VV_LAPLACE_CFD2 ? cfd2 : g.laplace == VV_LAPLACE_SIMPSON ? simp : cfd4;
+        for (int k = 0; k < 4; ++k) c->lap[k] = l[k];
+    }
     c->f1 = c->hx_inv * c->hv_inv / 12.;  // PoissonBracket.pyx:344
     c->f2 = c->hx_inv * c->hv_inv / 24.;  // PoissonBracket.pyx:345
 
@@ -1458,7 +1470,9 @@ int vv_create(const vv_grid* grid, vv_ctx** out) {
     std::vector<double> sym(nm);
     for (int k = 0; k < nm; ++k) {
         const long double t = 2.0L * PI * (long double)k / (long double)nx;
-        const long double s_ = (54.0L - 64.0L * cosl(t) + 10.0L * cosl(2.0L * t)) * (long double)c->hx2_inv / 12.0L;
+        const long double s_ = ((long double)c->lap[0] + 2.0L * (long double)c->lap[1] * cosl(t) +
+                                2.0L * (long double)c->lap[2] * cosl(2.0L * t)) *
+                               (long double)c->hx2_inv / (long double)c->lap[3];
         sym[k] = (k == 0) ? 0.0 : (double)(1.0L / s_);
     }
     std::vector<double2> lam_h(lam2);

@@ -347,7 +347,8 @@ __global__ void k_b_prologue(const BInst* __restrict__ tab, const int* __restric
 __global__ void __launch_bounds__(1024) k_b_poisson(const BInst* __restrict__ tab, const int* __restrict__ L, int n) {
     for_work<F_INST>(tab, L, n, [&](const BInst& I, int) {
         for (int i = threadIdx.x; i < I.nx; i += blockDim.x) I.hxp[i] = I.h1c[i];
-        poisson_apply_cta(I.phi, I.n, nullptr, I.nx, I.po.hx2_inv, I.po.charge, 2, &I.ds->pnorm2);
+        poisson_apply_cta(I.phi, I.n, nullptr, I.nx, I.po.hx2_inv, I.po.charge, 2, &I.ds->pnorm2, I.po.la0, I.po.la1,
+                          I.po.la2, I.po.lden);
     });
 }
 

@@ -532,6 +532,8 @@ struct PoissonParams {
     double hv, charge, hx2_inv, hx, inv_nx;
     const double2* tw;       // nx twiddles W^k (the FFT reads k < nx/2)
     const double* sym_inv;   // M+1 entries: 1/symbol_k (0 for k = 0)
+    // the Laplacian: periodic stencil (la2, la1, la0, la1, la2) / lden hx^-2
+    double la0, la1, la2, lden;
 };
 
 constexpr int POIS_THREADS = 1024;
@@ -675,7 +677,8 @@ __device__ __forceinline__ void moments_poisson_cta(const double* __restrict__ p
         if (h1) h1[i] = pc - phimean_s;
         const int im2 = (i - 2 + 2 * nx) % nx, im1 = (i - 1 + nx) % nx;
         const int ip1 = (i + 1) % nx, ip2 = (i + 2) % nx;
-        const double Ax = (5. * phs[im2] - 32. * phs[im1] + 54. * pc - 32. * phs[ip1] + 5. * phs[ip2]) * p.hx2_inv / 12.;
+        const double Ax =
+            (p.la2 * phs[im2] + p.la1 * phs[im1] + p.la0 * pc + p.la1 * phs[ip1] + p.la2 * phs[ip2]) * p.hx2_inv / p.lden;
         const double r = Ax + (nn[i] - nmean) * p.charge;
         r2 += r * r;
     }
@@ -694,11 +697,14 @@ k_moments_poisson(const double* __restrict__ part, const double* __restrict__ n_
 }
 
 // Poisson apply (one CTA): mode 0 rhs b = -(n - mean n) charge, 1 matvec
-// (CFD4 stencil), 2 function (matvec + (n - mean n) charge); optional
-// ||y||^2 -> sumsq (PETScPoissonSolver.pyx:58-74, PETScPoissonCFD4.pyx:64-101)
+// (the stencil (a2, a1, a0, a1, a2) / den hx^-2 of the Laplacian), 2
+// function (matvec + (n - mean n) charge); optional ||y||^2 -> sumsq
+// (PETScPoissonSolver.pyx:58-74, PETScPoissonCFD4.pyx:64-101,
+// PETScPoissonCFD2.pyx:64-101, PETScPoissonSimpson.pyx:62-101)
 __device__ __forceinline__ void poisson_apply_cta(const double* __restrict__ x, const double* __restrict__ n,
                                                   double* __restrict__ y, int nx, double hx2_inv, double charge,
-                                                  int mode, double* __restrict__ sumsq) {
+                                                  int mode, double* __restrict__ sumsq, double a0, double a1,
+                                                  double a2, double den) {
     __shared__ double red[32];
     __shared__ double nmean_s;
     double t = 0.0;
@@ -716,7 +722,7 @@ __device__ __forceinline__ void poisson_apply_cta(const double* __restrict__ x, 
         } else {
             const int im2 = (i - 2 + 2 * nx) % nx, im1 = (i - 1 + nx) % nx;
             const int ip1 = (i + 1) % nx, ip2 = (i + 2) % nx;
-            r = (5. * x[im2] - 32. * x[im1] + 54. * x[i] - 32. * x[ip1] + 5. * x[ip2]) * hx2_inv / 12.;
+            r = (a2 * x[im2] + a1 * x[im1] + a0 * x[i] + a1 * x[ip1] + a2 * x[ip2]) * hx2_inv / den;
             if (mode == 2) r = r + (n[i] - nmean_s) * charge;
         }
         if (y) y[i] = r;

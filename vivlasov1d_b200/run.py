@@ -49,7 +49,7 @@ class Run:
         self.ctx = self.grid.context(bracket=cfg.get_poisson_bracket(),
                                      preconditioner=cfg.get_preconditioner() or None,
                                      charge=self.charge, mass=self.mass, order=order, restart=restart,
-                                     precision=precision)
+                                     precision=precision, laplace=cfg.get_laplace_operator())
         g = self.grid
         fld, xv = g.field, g.xvec
         self.fc, self.fh = fld(), fld()

@@ -80,8 +80,9 @@ class Grid:
         return torch.zeros(self.nx, dtype=torch.float64, device=self.device)
 
     def context(self, bracket="arakawaj4", preconditioner="tensor_kinetic", charge=-1.0, mass=1.0,
-                order="factored", restart=30, precision="fp64", mixed_rtol=0.0):
-        key = (bracket, preconditioner, float(charge), float(mass), order, int(restart), precision, float(mixed_rtol))
+                order="factored", restart=30, precision="fp64", mixed_rtol=0.0, laplace="cfd4"):
+        key = (bracket, preconditioner, float(charge), float(mass), order, int(restart), precision, float(mixed_rtol),
+               laplace.lower())
         ctx = self._contexts.get(key)
         if ctx is None:
             ctx = Context(self, *key)
@@ -94,7 +95,7 @@ class Context:
     """Owner of one ``vv_ctx`` (device work buffers, preconditioner factors)."""
 
     def __init__(self, grid, bracket="arakawaj4", preconditioner="tensor_kinetic", charge=-1.0,
-                 mass=1.0, order="factored", restart=30, precision="fp64", mixed_rtol=0.0):
+                 mass=1.0, order="factored", restart=30, precision="fp64", mixed_rtol=0.0, laplace="cfd4"):
         lib = _lib.load()
         if not torch.cuda.is_available():
             raise RuntimeError("vivlasov1d_b200 needs a CUDA device; no CPU fallback exists")
@@ -115,7 +116,10 @@ class Context:
             g.preconditioner = _lib.PC_TENSOR_POTENTIAL
         else:
             raise NotImplementedError("preconditioner %r is not implemented on this path" % preconditioner)
-        g.laplace = _lib.LAPLACE["cfd4"]
+        if laplace.lower() not in _lib.LAPLACE:
+            raise NotImplementedError("laplace_operator %r is not implemented on this path" % laplace)
+        g.laplace = _lib.LAPLACE[laplace.lower()]
+        self.laplace = laplace.lower()
         g.order = _lib.ORDER_REFERENCE if order == "reference" else _lib.ORDER_FACTORED
         g.gmres_restart = int(restart)
         if precision not in _lib.PRECISION:
@@ -360,9 +364,11 @@ class PETScVlasovSolver:
 
 # ---------------------------------------------------------------------------
 class PETScPoissonSolver:
-    """CFD4 periodic Poisson solver (PETScPoissonCFD4.pyx:18-183)."""
+    """Periodic Poisson solver of the chosen Laplacian: CFD4 (default,
+    PETScPoissonCFD4.pyx:18-183), CFD2 (PETScPoissonCFD2.pyx) or Simpson
+    (PETScPoissonSimpson.pyx)."""
 
-    def __init__(self, dax, nx=None, hx=None, charge=-1.0, grid=None):
+    def __init__(self, dax, nx=None, hx=None, charge=-1.0, grid=None, laplace="cfd4"):
         grid = grid if grid is not None else dax
         self.grid = grid
         self.nx = grid.nx
@@ -370,7 +376,7 @@ class PETScPoissonSolver:
         self.hx2 = grid.hx ** 2
         self.hx2_inv = 1. / self.hx2
         self.charge = charge
-        self.ctx = grid.context(preconditioner=None, charge=charge)
+        self.ctx = grid.context(preconditioner=None, charge=charge, laplace=laplace)
 
     def formRHS(self, N, B):                      # PETScPoissonSolver.pyx:58-74
         c = self.ctx
