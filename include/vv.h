@@ -50,7 +50,8 @@ enum vv_status {
 enum vv_bracket {            /* solver.poisson_bracket                        */
     VV_BRACKET_J1 = 1,       /* PoissonBracket.pyx:68-186                      */
     VV_BRACKET_J2 = 2,       /* PoissonBracket.pyx:188-306                     */
-    VV_BRACKET_J4 = 4        /* PoissonBracket.pyx:309-403 (default)           */
+    VV_BRACKET_J4 = 4,       /* PoissonBracket.pyx:309-403 (default)           */
+    VV_BRACKET_SIMPSON = 5   /* PoissonBracket.pyx:405-492                     */
 };
 enum vv_preconditioner {     /* solver.preconditioner_scheme                  */
     VV_PC_NONE = 0,

@@ -210,6 +210,32 @@ def _j2_terms(x, h):
     return jcc, jpc, jcp
 
 
+def _simpson_terms(x, h, a, b):
+    """One J1-pattern bracket of the Simpson scheme at x spacing a and v
+    spacing b, without its denominator (PoissonBracket.pyx:436-486; the term
+    order of each of the four blocks there)."""
+    s = _s
+    t = (s(x, 0, b) - s(x, 0, -b)) * (s(h, -a, 0) - s(h, a, 0)) \
+        + (s(x, a, 0) - s(x, -a, 0)) * (s(h, 0, b) - s(h, 0, -b)) \
+        + s(x, 0, b) * (s(h, -a, b) - s(h, a, b)) \
+        + s(x, 0, -b) * (s(h, a, -b) - s(h, -a, -b))
+    if a == 1 and b == 1:   # bracket11 lists the -x neighbour first
+        t = t + s(x, -a, 0) * (s(h, -a, -b) - s(h, -a, b)) \
+            + s(x, a, 0) * (s(h, a, b) - s(h, a, -b))
+    else:
+        t = t + s(x, a, 0) * (s(h, a, b) - s(h, a, -b)) \
+            + s(x, -a, 0) * (s(h, -a, -b) - s(h, -a, b))
+    t = t + s(x, a, b) * (s(h, 0, b) - s(h, a, 0)) \
+        + s(x, a, -b) * (s(h, a, 0) - s(h, 0, -b))
+    if a == 2 and b == 1 or a == 2 and b == 2:   # bracket21 / bracket22: (-a, +b) before (-a, -b)
+        t = t + s(x, -a, b) * (s(h, -a, 0) - s(h, 0, b)) \
+            + s(x, -a, -b) * (s(h, 0, -b) - s(h, -a, 0))
+    else:                                        # bracket11 / bracket12: (-a, -b) before (-a, +b)
+        t = t + s(x, -a, -b) * (s(h, 0, -b) - s(h, -a, 0)) \
+            + s(x, -a, b) * (s(h, -a, 0) - s(h, 0, b))
+    return t
+
+
 def bracket_add(x, h, y, factor, grid, scheme="arakawaj4"):
     """``y += factor * [x, h]`` on the interior rows, in place.
 
@@ -233,6 +259,13 @@ def bracket_add(x, h, y, factor, grid, scheme="arakawaj4"):
         result_J1 = (jpp1 + jpc1 + jcp1) * f1
         result_J2 = (jcc2 + jpc2 + jcp2) * f2
         y[interior] += factor * (2. * result_J1 - result_J2)
+    elif scheme == "simpson":   # PoissonBracket.pyx:420-492
+        simpson_factor = factor * grid.hx_inv * grid.hv_inv / 9.
+        b22 = _simpson_terms(x, h, 2, 2) / 48.
+        b12 = _simpson_terms(x, h, 1, 2) / 24.
+        b21 = _simpson_terms(x, h, 2, 1) / 24.
+        b11 = _simpson_terms(x, h, 1, 1) / 12.
+        y[interior] += (25. * b11 - 10. * b12 - 10. * b21 + 4. * b22) * simpson_factor
     else:
         raise ValueError("unknown bracket %r" % scheme)
     return y

@@ -12,7 +12,7 @@ petsc4py exists in this image, so its extensions cannot be compiled.  Its
   3. executes the result against a small numpy-backed stand-in for the PETSc
      objects those methods touch (Vec, DMDA ranges/corners, global-to-local
      halo fill with periodic x and ghosted v, setValues/axpy/norm),
-  4. calls the reference's methods (PoissonBracket J1/J2/J4, TimeDerivative,
+  4. calls the reference's methods (PoissonBracket J1/J2/J4/Simpson, TimeDerivative,
      PETScVlasovSolver function/jacobian/update_previous/function_norm,
      Toolbox moments and initialisers, PETScPoissonCFD4 RHS/matvec/residual,
      TensorProduct eigenvalues and banded preconditioner matrices (kinetic
@@ -448,7 +448,7 @@ def make_case(ns, nx, nv, L, vmin, vmax, ht, seed):
     out["h1p"] = vec_to_2d(H1p, nx, nv)
     out["h1h"] = vec_to_2d(H1h, nx, nv)
 
-    for scheme in ("arakawaj1", "arakawaj2", "arakawaj4"):
+    for scheme in ("arakawaj1", "arakawaj2", "arakawaj4", "simpson"):
         solver = ns["PETScVlasovSolver"](Config(scheme), da1, dax, grid, H0, H1p, H1h, H2, H2, P)
         Fv = to_vec(F)
         solver.update_history(to_vec(Fh))

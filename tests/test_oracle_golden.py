@@ -48,7 +48,7 @@ def test_hamiltonian_assembly_bitexact(golden):
     assert np.array_equal(H, golden["Have"])
 
 
-@pytest.mark.parametrize("scheme", ["arakawaj1", "arakawaj2", "arakawaj4"])
+@pytest.mark.parametrize("scheme", ["arakawaj1", "arakawaj2", "arakawaj4", "simpson"])
 def test_bracket_residual_jvp_bitexact(golden, scheme):
     """Same operation order as the reference loop -> identical bits."""
     g = _grid(golden)

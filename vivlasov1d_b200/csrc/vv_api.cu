@@ -172,6 +172,8 @@ vv::BracketParams bparams(const vv_ctx* c, double factor) {
     p.factor = factor;
     p.f1 = c->f1;
     p.f2 = c->f2;
+    p.hx_inv = c->hx_inv;
+    p.hv_inv = c->hv_inv;
     p.h0 = c->h0;
     p.hxp = c->hxp;
     p.xidx = nullptr;
@@ -282,10 +284,25 @@ int launch_bracket_s(vv_ctx* c, const T* X, const T* Xh, T* Y, double factor, do
     return VV_OK;
 }
 
+// the Simpson bracket: one kernel in the reference's operation order for
+// every order setting and precision (BX x BY tiles)
+template <int MODE, typename T>
+int launch_simpson(vv_ctx* c, const T* X, const T* Xh, T* Y, double factor, double* sumsq, const int* xidx) {
+    dim3 grid((c->nx + vv::BX - 1) / vv::BX, (c->nv + vv::BY - 1) / vv::BY);
+    dim3 block(vv::BX, vv::TY);
+    vv::BracketParams p = bparams(c, factor);
+    p.xidx = xidx;
+    p.xstride = xidx ? c->ncell : 0;
+    vv::k_bracket_simpson<MODE, T><<<grid, block, 0, c->st>>>(X, Xh, Y, p, sumsq);
+    CKL(c);
+    return VV_OK;
+}
+
 template <int MODE, typename T>
 int launch_bracket(vv_ctx* c, const T* X, const T* Xh, T* Y, double factor, double* sumsq,
                    const int* xidx = nullptr) {
     switch (c->g.bracket) {
+        case VV_BRACKET_SIMPSON: return launch_simpson<MODE, T>(c, X, Xh, Y, factor, sumsq, xidx);
         case VV_BRACKET_J1: return launch_bracket_s<1, MODE, T>(c, X, Xh, Y, factor, sumsq, xidx);
         case VV_BRACKET_J2: return launch_bracket_s<2, MODE, T>(c, X, Xh, Y, factor, sumsq, xidx);
         default: return launch_bracket_s<4, MODE, T>(c, X, Xh, Y, factor, sumsq, xidx);
@@ -294,7 +311,7 @@ int launch_bracket(vv_ctx* c, const T* X, const T* Xh, T* Y, double factor, doub
 
 // number of per-CTA partials a bracket launch writes for these operands
 int bracket_tiles(const vv_ctx* c, const void* X = nullptr, const void* Xh = nullptr, const void* Y = nullptr) {
-    if (c->g.order != VV_ORDER_REFERENCE && wide_ok(c, X, Xh, Y))
+    if (c->g.order != VV_ORDER_REFERENCE && c->g.bracket != VV_BRACKET_SIMPSON && wide_ok(c, X, Xh, Y))
         return (c->nx / vv::WX) * ((c->nv + vv::WY - 1) / vv::WY);
     return ((c->nx + vv::BX - 1) / vv::BX) * ((c->nv + vv::BY - 1) / vv::BY);
 }
@@ -1305,7 +1322,9 @@ int vv_create(const vv_grid* grid, vv_ctx** out) {
     *out = nullptr;
     const vv_grid& g = *grid;
     if (g.nx < 4 || g.nv < 5 || !(g.L > 0.0) || !(g.vmax > g.vmin) || !(g.ht > 0.0)) return VV_ERR_ARG;
-    if (g.bracket != VV_BRACKET_J1 && g.bracket != VV_BRACKET_J2 && g.bracket != VV_BRACKET_J4) return VV_ERR_ARG;
+    if (g.bracket != VV_BRACKET_J1 && g.bracket != VV_BRACKET_J2 && g.bracket != VV_BRACKET_J4 &&
+        g.bracket != VV_BRACKET_SIMPSON)
+        return VV_ERR_ARG;
     if (g.preconditioner != VV_PC_NONE && g.preconditioner != VV_PC_TENSOR_KINETIC &&
         g.preconditioner != VV_PC_TENSOR_POTENTIAL)
         return VV_ERR_ARG;
@@ -1760,6 +1779,8 @@ int vv_step_adjoint(vv_ctx* c, const double* F, const double* f, const double* h
                     const double* gF, double* gf, const vv_ksp_opts* o, vv_ksp_result* r) {
     if (!c || !F || !f || !gF || !gf || !o || !r) return VV_ERR_ARG;
     if (c->mixed) return VV_ERR_UNSUPPORTED;
+    if (c->g.bracket == VV_BRACKET_SIMPSON)   // the transposed stencil is built for the Arakawa brackets
+        return fail(VV_ERR_UNSUPPORTED, "vv_step_adjoint: the Simpson bracket has no transposed stencil here");
     const int restart = (o->restart > 0) ? o->restart : c->restart;
     if (restart > c->restart || restart < 1 || o->max_it < 0) return VV_ERR_ARG;
     TRY(adj_buffers(c));
@@ -2502,6 +2523,7 @@ int vv_batch_create(int n, vv_ctx* const* ctxs, const vv_state* states, vv_batch
         // 64 x 32 stencil tiles (nx a multiple of 64); the factored order
         if (c->mixed != c0->mixed || c->g.bracket != c0->g.bracket ||
             c->g.preconditioner != VV_PC_TENSOR_KINETIC || c->g.order == VV_ORDER_REFERENCE ||
+            c->g.bracket == VV_BRACKET_SIMPSON ||
             c->nx % vv::WX != 0 || !c->pow2 || c->device != c0->device)
             return VV_ERR_UNSUPPORTED;
     }

@@ -31,6 +31,7 @@ struct BracketParams {
     double factor;   // bracket factor (0.5 for the JVP, 1.0 residual)
     double f1;       // hx_inv*hv_inv/12
     double f2;       // hx_inv*hv_inv/24
+    double hx_inv, hv_inv;
     const double* h0;   // nv: 0.5 v^2 mass
     const double* hxp;  // 4*nx: h1p, h1h, h2p, h2h profiles
     const int* xidx;    // optional: input is X + (*xidx) * xstride (GMRES basis vector)
@@ -176,6 +177,131 @@ k_bracket_ref(const double* __restrict__ X, const double* __restrict__ Xh,
         Y[g] = y;
         acc2 += y * y;
     }
+    if (sumsq) {
+        const double t = block_sum(acc2, sred);
+        if (threadIdx.x == 0 && threadIdx.y == 0) sumsq[blockIdx.x + gridDim.x * blockIdx.y] = t;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Simpson bracket (PoissonBracket.pyx:405-492): four J1-pattern brackets at
+// x/v spacings (1,1), (1,2), (2,1), (2,2), combined as
+// (25 b11 - 10 b12 - 10 b21 + 4 b22) factor hx^-1 hv^-1 / 9, in the
+// reference's operation order (round-to-nearest adds and multiplies: the
+// FP64 result is the reference's bits); T = float for the mixed-precision
+// Jacobian.
+// ---------------------------------------------------------------------------
+template <typename T> VV_DEV T rn_add(T a, T b);
+template <typename T> VV_DEV T rn_sub(T a, T b);
+template <typename T> VV_DEV T rn_mul(T a, T b);
+template <> VV_DEV double rn_add<double>(double a, double b) { return __dadd_rn(a, b); }
+template <> VV_DEV double rn_sub<double>(double a, double b) { return __dsub_rn(a, b); }
+template <> VV_DEV double rn_mul<double>(double a, double b) { return __dmul_rn(a, b); }
+template <> VV_DEV float rn_add<float>(float a, float b) { return __fadd_rn(a, b); }
+template <> VV_DEV float rn_sub<float>(float a, float b) { return __fsub_rn(a, b); }
+template <> VV_DEV float rn_mul<float>(float a, float b) { return __fmul_rn(a, b); }
+
+template <int MODE, typename T>
+__global__ void __launch_bounds__(BX * TY)
+k_bracket_simpson(const T* __restrict__ X, const T* __restrict__ Xh, T* __restrict__ Y, BracketParams p,
+                  double* __restrict__ sumsq) {
+    if (p.xidx) X += (size_t)(*p.xidx) * p.xstride;
+    __shared__ T sx[SY][SX + 1];
+    __shared__ T sh[SY][SX + 1];
+    __shared__ double sred[BX * TY / 32];
+    const int i0 = blockIdx.x * BX, j0 = blockIdx.y * BY;
+    const int tid = threadIdx.x + BX * threadIdx.y;
+    for (int s = tid; s < SX * SY; s += BX * TY) {
+        const int ly = s / SX, lx = s - ly * SX;
+        const int gi = wrapx(i0 - 2 + lx, p.nx);
+        const int gj = j0 - 2 + ly;
+        T xv = T(0), hv = T(0);
+        if (gj >= 0 && gj < p.nv) {
+            const size_t g = (size_t)gj * p.nx + gi;
+            // Fave = 0 + .5 Fh + .5 F  (PETScNLVlasovMP.pyx:49-51)
+            xv = (MODE == MODE_RESIDUAL) ? rn_add<T>(rn_mul<T>(T(0.5), Xh[g]), rn_mul<T>(T(0.5), X[g])) : X[g];
+            hv = T(h_ref(p, gi, gj));
+        }
+        sx[ly][lx] = xv;
+        sh[ly][lx] = hv;
+    }
+    __syncthreads();
+    const T sfac = T(((p.factor * p.hx_inv) * p.hv_inv) / 9.);   // simpson_factor
+    const T htinv = T(p.ht_inv);
+    double acc2 = 0.0;
+    const int lx = threadIdx.x + 2;
+    const int i = i0 + threadIdx.x;
+#define A_(x, y) rn_add<T>((x), (y))
+#define S_(x, y) rn_sub<T>((x), (y))
+#define M_(x, y) rn_mul<T>((x), (y))
+#pragma unroll
+    for (int r = 0; r < BY / TY; ++r) {
+        const int ly = threadIdx.y + r * TY + 2;
+        const int j = j0 + ly - 2;
+        if (i >= p.nx || j >= p.nv) continue;
+        const size_t g = (size_t)j * p.nx + i;
+#define XS(di, dj) sx[ly + (dj)][lx + (di)]
+#define HS(di, dj) sh[ly + (dj)][lx + (di)]
+        T y;
+        if (MODE == MODE_JVP) y = M_(htinv, X[g]);                       // Y.axpy(ht_inv, F)
+        else if (MODE == MODE_RESIDUAL) y = M_(htinv, S_(X[g], Xh[g]));  // Y.axpy(ht_inv, F - Fh)
+        else y = Y[g];                                                   // bracket only: Y += factor [X, H]
+        if (j >= 2 && j < p.nv - 2) {
+            T t = M_(S_(XS(0, 2), XS(0, -2)), S_(HS(-2, 0), HS(2, 0)));
+            t = A_(t, M_(S_(XS(2, 0), XS(-2, 0)), S_(HS(0, 2), HS(0, -2))));
+            t = A_(t, M_(XS(0, 2), S_(HS(-2, 2), HS(2, 2))));
+            t = A_(t, M_(XS(0, -2), S_(HS(2, -2), HS(-2, -2))));
+            t = A_(t, M_(XS(2, 0), S_(HS(2, 2), HS(2, -2))));
+            t = A_(t, M_(XS(-2, 0), S_(HS(-2, -2), HS(-2, 2))));
+            t = A_(t, M_(XS(2, 2), S_(HS(0, 2), HS(2, 0))));
+            t = A_(t, M_(XS(2, -2), S_(HS(2, 0), HS(0, -2))));
+            t = A_(t, M_(XS(-2, 2), S_(HS(-2, 0), HS(0, 2))));
+            t = A_(t, M_(XS(-2, -2), S_(HS(0, -2), HS(-2, 0))));
+            const T b22 = t / T(48.);
+            t = M_(S_(XS(0, 2), XS(0, -2)), S_(HS(-1, 0), HS(1, 0)));
+            t = A_(t, M_(S_(XS(1, 0), XS(-1, 0)), S_(HS(0, 2), HS(0, -2))));
+            t = A_(t, M_(XS(0, 2), S_(HS(-1, 2), HS(1, 2))));
+            t = A_(t, M_(XS(0, -2), S_(HS(1, -2), HS(-1, -2))));
+            t = A_(t, M_(XS(1, 0), S_(HS(1, 2), HS(1, -2))));
+            t = A_(t, M_(XS(-1, 0), S_(HS(-1, -2), HS(-1, 2))));
+            t = A_(t, M_(XS(1, 2), S_(HS(0, 2), HS(1, 0))));
+            t = A_(t, M_(XS(1, -2), S_(HS(1, 0), HS(0, -2))));
+            t = A_(t, M_(XS(-1, -2), S_(HS(0, -2), HS(-1, 0))));
+            t = A_(t, M_(XS(-1, 2), S_(HS(-1, 0), HS(0, 2))));
+            const T b12 = t / T(24.);
+            t = M_(S_(XS(0, 1), XS(0, -1)), S_(HS(-2, 0), HS(2, 0)));
+            t = A_(t, M_(S_(XS(2, 0), XS(-2, 0)), S_(HS(0, 1), HS(0, -1))));
+            t = A_(t, M_(XS(0, 1), S_(HS(-2, 1), HS(2, 1))));
+            t = A_(t, M_(XS(0, -1), S_(HS(2, -1), HS(-2, -1))));
+            t = A_(t, M_(XS(2, 0), S_(HS(2, 1), HS(2, -1))));
+            t = A_(t, M_(XS(-2, 0), S_(HS(-2, -1), HS(-2, 1))));
+            t = A_(t, M_(XS(2, 1), S_(HS(0, 1), HS(2, 0))));
+            t = A_(t, M_(XS(2, -1), S_(HS(2, 0), HS(0, -1))));
+            t = A_(t, M_(XS(-2, 1), S_(HS(-2, 0), HS(0, 1))));
+            t = A_(t, M_(XS(-2, -1), S_(HS(0, -1), HS(-2, 0))));
+            const T b21 = t / T(24.);
+            t = M_(S_(XS(0, 1), XS(0, -1)), S_(HS(-1, 0), HS(1, 0)));
+            t = A_(t, M_(S_(XS(1, 0), XS(-1, 0)), S_(HS(0, 1), HS(0, -1))));
+            t = A_(t, M_(XS(0, 1), S_(HS(-1, 1), HS(1, 1))));
+            t = A_(t, M_(XS(0, -1), S_(HS(1, -1), HS(-1, -1))));
+            t = A_(t, M_(XS(-1, 0), S_(HS(-1, -1), HS(-1, 1))));
+            t = A_(t, M_(XS(1, 0), S_(HS(1, 1), HS(1, -1))));
+            t = A_(t, M_(XS(1, 1), S_(HS(0, 1), HS(1, 0))));
+            t = A_(t, M_(XS(1, -1), S_(HS(1, 0), HS(0, -1))));
+            t = A_(t, M_(XS(-1, -1), S_(HS(0, -1), HS(-1, 0))));
+            t = A_(t, M_(XS(-1, 1), S_(HS(-1, 0), HS(0, 1))));
+            const T b11 = t / T(12.);
+            const T c = A_(S_(S_(M_(T(25.), b11), M_(T(10.), b12)), M_(T(10.), b21)), M_(T(4.), b22));
+            y = A_(y, M_(c, sfac));
+        }
+#undef XS
+#undef HS
+        Y[g] = y;
+        acc2 += (double)y * (double)y;
+    }
+#undef A_
+#undef S_
+#undef M_
     if (sumsq) {
         const double t = block_sum(acc2, sred);
         if (threadIdx.x == 0 && threadIdx.y == 0) sumsq[blockIdx.x + gridDim.x * blockIdx.y] = t;
