@@ -63,6 +63,15 @@ enum vv_laplace {            /* solver.laplace_operator                       */
     VV_LAPLACE_CFD4 = 4,     /* PETScPoissonCFD4.pyx (default)                 */
     VV_LAPLACE_SIMPSON = 5   /* PETScPoissonSimpson.pyx                        */
 };
+enum vv_averaging {          /* solver.averaging_operator: the time derivative
+                                (TimeDerivative.pyx:36-53; 0 for None/'none') */
+    VV_AVERAGING_POINT = 0,     /* TimeDerivative: Y += F/ht (default)         */
+    VV_AVERAGING_MIDPOINT = 1,  /* TimeDerivativeMidpoint (:84-157), also the
+                                   arakawa_J1 class (:236-237)                 */
+    VV_AVERAGING_ARAKAWA_J2 = 2,/* TimeDerivativeArakawaJ2 (:240-242) = point  */
+    VV_AVERAGING_ARAKAWA_J4 = 4,/* TimeDerivativeArakawaJ4 (:245-321)          */
+    VV_AVERAGING_SIMPSON = 5    /* TimeDerivativeSimpson (:160-233)            */
+};
 enum vv_order {              /* arithmetic of the bracket kernels             */
     VV_ORDER_FACTORED = 0,   /* separable-h coefficient form (fast, default)   */
     VV_ORDER_REFERENCE = 1   /* the reference loop's operation order, no FMA   */
@@ -99,6 +108,12 @@ typedef struct vv_grid {
                                 Krylov vectors cannot reduce a residual near
                                 the FP64 round-off floor by 1e-4 cheaply.
                                 vv_gmres always uses the rtol it is given.    */
+    int32_t averaging;       /* enum vv_averaging (0: point).  The averaged
+                                operators replace F/ht on the rows
+                                2 <= j < nv-2 by a 9- or 13-point stencil of
+                                F times 1/(ht d); they are supported by the
+                                single-instance step, not by vv_batch_create
+                                or vv_step_adjoint (VV_ERR_UNSUPPORTED).      */
 } vv_grid;
 
 typedef struct vv_ctx vv_ctx;

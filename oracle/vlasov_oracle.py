@@ -6,8 +6,9 @@ and by the ``cpu_baseline`` leg of ``bench.py`` and by nothing else.  The
 product (``vivlasov1d_b200``) never imports it and has no CPU fallback.
 
 It restates, in numpy/scipy, the reference's algorithm for the configuration
-``method=matrixfree, type=nonlinear, mode=split, timestepping=mp`` with the
-'point' time derivative.  Every function cites the reference file:line it
+``method=matrixfree, type=nonlinear, mode=split, timestepping=mp`` with every
+time derivative ``TimeDerivative.create`` builds ('point' and the averaging
+stencils).  Every function cites the reference file:line it
 follows (paths relative to the viVlasov1D project root).
 
 Array convention: a distribution-function field is an ``(nx, nv)`` float64
@@ -277,21 +278,85 @@ def bracket(x, h, grid, scheme="arakawaj4", factor=1.0):
 
 
 # --------------------------------------------------------------------------
-# residual and JVP  (solvers/vlasov/PETScNLVlasovMP.pyx:33-58,
-#                    components/TimeDerivative.pyx:56-57)
+# time derivative  (solvers/components/TimeDerivative.pyx)
 # --------------------------------------------------------------------------
-def residual(F, Fh, Have, grid, scheme="arakawaj4"):
-    """``R(F) = (F - Fh)/ht + [ (F+Fh)/2 , Have ]`` (PETScNLVlasovMP.pyx:43-58)."""
+# averaging stencils: divisor and the (di, dj, weight) terms in the order the
+# reference's loop body sums them (x offset di, v offset dj)
+_AVG_POINT, _AVG_MIDPOINT, _AVG_SIMPSON, _AVG_J4 = "point", "midpoint", "simpson", "arakawa_J4"
+_AVERAGING_STENCILS = {
+    _AVG_MIDPOINT: (16., [(-1, -1, 1.), (0, -1, 2.), (1, -1, 1.),       # TimeDerivative.pyx:110-112
+                          (-1, 0, 2.), (0, 0, 4.), (1, 0, 2.),
+                          (-1, 1, 1.), (0, 1, 2.), (1, 1, 1.)]),
+    _AVG_SIMPSON: (36., [(-1, -1, 1.), (0, -1, 4.), (1, -1, 1.),        # :184-186
+                         (-1, 0, 4.), (0, 0, 16.), (1, 0, 4.),
+                         (-1, 1, 1.), (0, 1, 4.), (1, 1, 1.)]),
+    _AVG_J4: (64., [(0, -2, 1.),                                         # :271-275
+                    (-1, -1, 2.), (0, -1, 8.), (1, -1, 2.),
+                    (-2, 0, 1.), (-1, 0, 8.), (0, 0, 20.), (1, 0, 8.), (2, 0, 1.),
+                    (-1, 1, 2.), (0, 1, 8.), (1, 1, 2.),
+                    (0, 2, 1.)]),
+}
+
+
+def averaging_kind(name):
+    """Normalise an averaging-operator name to the class
+    ``TimeDerivative.create`` builds (TimeDerivative.pyx:36-53).
+
+    ``None``/'none'/'point' and 'arakawa_J2' (a plain subclass of the point
+    operator, :240-242) are the point derivative; 'arakawa_J1' is the midpoint
+    stencil (:236-237).  ``config.get_averaging_operator`` lower-cases the
+    runspec value, so the runspec spellings 'ArakawaJ1/J2/J4' reach ``create``
+    as 'arakawaj1' etc., which it does not know (it returns None); they are
+    rejected here with a ValueError instead."""
+    if name is None or name == "" or name.lower() in ("none", "point"):
+        return _AVG_POINT
+    table = {"midpoint": _AVG_MIDPOINT, "simpson": _AVG_SIMPSON, "arakawa_J1": _AVG_MIDPOINT,
+             "arakawa_J2": _AVG_POINT, "arakawa_J4": _AVG_J4}
+    key = name if name in table else name.lower()
+    if key not in table:
+        raise ValueError("unknown averaging operator %r" % name)
+    return table[key]
+
+
+def time_derivative_add(x, y, grid, averaging="point"):
+    """``y += D_t x`` in place (TimeDerivative.function).
+
+    'point' (:56-57) is ``Y.axpy(ht_inv, X)``.  The averaging variants apply
+    their stencil times ``ht_inv / divisor`` on the rows 2 <= j < nv-2 and
+    ``ht_inv * x`` on the two boundary rows at each end (:88-112, :164-188,
+    :249-275), summing the stencil terms left to right."""
+    kind = averaging_kind(averaging)
+    if kind == _AVG_POINT:
+        y += grid.ht_inv * x
+        return y
+    div, terms = _AVERAGING_STENCILS[kind]
+    time_fac = grid.ht_inv / div
+    s = None
+    for di, dj, w in terms:
+        t = w * _s(x, di, dj)
+        s = t if s is None else s + t
+    nv = x.shape[1]
+    y[:, STENCIL:nv - STENCIL] += s * time_fac
+    y[:, :STENCIL] += grid.ht_inv * x[:, :STENCIL]
+    y[:, nv - STENCIL:] += grid.ht_inv * x[:, nv - STENCIL:]
+    return y
+
+
+# --------------------------------------------------------------------------
+# residual and JVP  (solvers/vlasov/PETScNLVlasovMP.pyx:33-58)
+# --------------------------------------------------------------------------
+def residual(F, Fh, Have, grid, scheme="arakawaj4", averaging="point"):
+    """``R(F) = D_t (F - Fh) + [ (F+Fh)/2 , Have ]`` (PETScNLVlasovMP.pyx:43-58)."""
     Fave = 0.5 * Fh + 0.5 * F            # Fave.set(0); axpy(.5,Fh); axpy(.5,F)
     Fder = F - Fh                        # Fder.set(0); axpy(+1,F); axpy(-1,Fh)
-    Y = grid.ht_inv * Fder               # TimeDerivative.function: Y.axpy(ht_inv, F)
+    Y = time_derivative_add(Fder, np.zeros_like(F), grid, averaging)
     bracket_add(Fave, Have, Y, 1.0, grid, scheme)
     return Y
 
 
-def jvp(X, Have, grid, scheme="arakawaj4"):
-    """``J X = X/ht + 0.5 [X, Have]`` (PETScNLVlasovMP.pyx:33-40)."""
-    Y = grid.ht_inv * X
+def jvp(X, Have, grid, scheme="arakawaj4", averaging="point"):
+    """``J X = D_t X + 0.5 [X, Have]`` (PETScNLVlasovMP.pyx:33-40)."""
+    Y = time_derivative_add(X, np.zeros_like(X), grid, averaging)
     bracket_add(X, Have, Y, 0.5, grid, scheme)
     return Y
 
@@ -644,10 +709,11 @@ def gmres(apply_A, b, rtol=1e-5, atol=1e-50, max_it=10000, restart=30,
 class VlasovSolver:
     """Restates ``PETScVlasovSolver`` for the nonlinear midpoint scheme."""
 
-    def __init__(self, grid, h0v, scheme="arakawaj4", preconditioner="tensor_kinetic"):
+    def __init__(self, grid, h0v, scheme="arakawaj4", preconditioner="tensor_kinetic", averaging="point"):
         self.grid = grid
         self.h0v = np.asarray(h0v, dtype=np.float64)
         self.scheme = scheme
+        self.averaging = averaging_kind(averaging)   # PETScVlasovSolver.pyx:99
         if preconditioner == "tensor_kinetic":
             self.pc = TensorKineticPreconditioner(grid)
         elif preconditioner == "tensor_potential":
@@ -666,10 +732,10 @@ class VlasovSolver:
         self.Have = have_field(self.h0v, h1p, h1h, h2p, h2h)
 
     def function_solver(self, F):          # PETScNLVlasovMP.pyx:43-58
-        return residual(F, self.Fh, self.Have, self.grid, self.scheme)
+        return residual(F, self.Fh, self.Have, self.grid, self.scheme, self.averaging)
 
     def jacobian_solver(self, F):          # PETScNLVlasovMP.pyx:33-40
-        return jvp(F, self.Have, self.grid, self.scheme)
+        return jvp(F, self.Have, self.grid, self.scheme, self.averaging)
 
     def function(self, F):                 # PETScVlasovSolver.pyx:168-174
         Y = self.function_solver(F)
@@ -705,7 +771,7 @@ class Run:
     def __init__(self, grid, f0, scheme="arakawaj4", preconditioner="tensor_kinetic",
                  charge=-1.0, mass=1.0, ksp_rtol=1e-4, ksp_atol=1e-50,
                  ksp_max_it=1000, snes_atol=1e-10, snes_max_iter=20,
-                 normalise_f=True, laplace="cfd4"):
+                 normalise_f=True, laplace="cfd4", averaging="point"):
         self.grid = grid
         self.laplace = laplace
         self.charge = charge
@@ -714,7 +780,7 @@ class Run:
         self.snes_atol = snes_atol
         self.snes_max_iter = snes_max_iter
         self.h0v = kinetic_hamiltonian_v(grid, mass)
-        self.solver = VlasovSolver(grid, self.h0v, scheme, preconditioner)
+        self.solver = VlasovSolver(grid, self.h0v, scheme, preconditioner, averaging)
         f = np.asarray(f0, dtype=np.float64)
         self.fc = normalise(f, grid) if normalise_f else f.copy()
         self.h2c = np.zeros(grid.nx)

@@ -323,11 +323,12 @@ PETSc = types.SimpleNamespace(InsertMode=InsertMode, Scatter=_Scatter,
 
 
 class Config:
-    def __init__(self, bracket):
+    def __init__(self, bracket, averaging="point"):
         self.bracket = bracket
+        self.averaging = averaging
 
     def get_averaging_operator(self):
-        return "point"
+        return self.averaging
 
     def get_poisson_bracket(self):
         return self.bracket
@@ -467,6 +468,22 @@ def make_case(ns, nx, nv, L, vmin, vmax, ht, seed):
         Yb = da1.createGlobalVec()
         pb.function(Fv, solver.Have, Yb, 1.0)
         out["bracket_" + scheme] = vec_to_2d(Yb, nx, nv)
+
+    # averaged time derivatives (TimeDerivative.pyx:84-275) under the J4 and
+    # Simpson brackets; 'arakawa_J1' is the midpoint class, 'arakawa_J2' the
+    # point class
+    for avg in ("midpoint", "simpson", "arakawa_J4"):
+        for scheme in ("arakawaj4", "simpson"):
+            solver = ns["PETScVlasovSolver"](Config(scheme, avg), da1, dax, grid, H0, H1p, H1h, H2, H2, P)
+            Fv = to_vec(F)
+            solver.update_history(to_vec(Fh))
+            solver.update_previous(Fv)
+            Y = da1.createGlobalVec()
+            solver.function(Fv, Y)
+            out["residual_%s_avg_%s" % (scheme, avg)] = vec_to_2d(Y, nx, nv)
+            Y2 = da1.createGlobalVec()
+            solver.jacobian(Fv, Y2)
+            out["jvp_%s_avg_%s" % (scheme, avg)] = vec_to_2d(Y2, nx, nv)
 
     # moments (Toolbox.pyx:79-165)
     N, U, E, A = (dax.createGlobalVec() for _ in range(4))

@@ -43,6 +43,25 @@ def test_create_rejects_bad_grid_without_gpu():
     assert lib.vv_create(C.byref(g), C.byref(h)) == 1  # VV_ERR_ARG
     g.nx, g.nv, g.laplace = 12, 32, 3
     assert lib.vv_create(C.byref(g), C.byref(h)) == 2  # VV_ERR_UNSUPPORTED (no Laplacian with that code)
+    g.laplace, g.averaging = 4, 3
+    assert lib.vv_create(C.byref(g), C.byref(h)) == 1  # VV_ERR_ARG (no time derivative with that code)
+
+
+def test_averaging_operator_names():
+    """The time-derivative names TimeDerivative.create knows
+    (TimeDerivative.pyx:36-53) map to the vv_averaging codes; the lower-cased
+    runspec spellings of the Arakawa variants are unknown to create and are
+    rejected."""
+    from vivlasov1d_b200 import _lib
+    assert _lib.averaging_code(None) == _lib.averaging_code("none") == _lib.averaging_code("point") == 0
+    assert _lib.averaging_code("midpoint") == _lib.averaging_code("arakawa_J1") == 1
+    assert _lib.averaging_code("arakawa_J2") == 2
+    assert _lib.averaging_code("arakawa_J4") == 4
+    assert _lib.averaging_code("simpson") == _lib.averaging_code("Simpson") == 5
+    for bad in ("arakawaj1", "arakawaj4", "trapezoid"):
+        with pytest.raises(ValueError):
+            _lib.averaging_code(bad)
+    assert [f[0] for f in _lib.vv_grid._fields_][-1] == "averaging"
 
 
 def test_product_does_not_import_oracle():

@@ -61,6 +61,38 @@ def test_bracket_residual_jvp_bitexact(golden, scheme):
     assert abs(np.sqrt((R * R).sum()) - golden["fnorm_" + scheme]) <= 1e-14 * golden["fnorm_" + scheme]
 
 
+@pytest.mark.parametrize("avg", ["midpoint", "simpson", "arakawa_J4"])
+@pytest.mark.parametrize("scheme", ["arakawaj4", "simpson"])
+def test_averaged_time_derivative_bitexact(golden, scheme, avg):
+    """The averaging stencils of TimeDerivative.pyx in the residual and the
+    JVP, summed in the reference loop's order -> identical bits."""
+    g = _grid(golden)
+    H = golden["Have"]
+    F, Fh = golden["F"], golden["Fh"]
+    key = "%s_avg_%s" % (scheme, avg)
+    assert np.array_equal(vo.residual(F, Fh, H, g, scheme, avg), golden["residual_" + key])
+    assert np.array_equal(vo.jvp(F, H, g, scheme, avg), golden["jvp_" + key])
+    # the averaged derivative differs from the point one on the interior rows only
+    pt = vo.jvp(F, H, g, scheme)
+    d = golden["jvp_" + key] - pt
+    assert np.array_equal(d[:, :2], np.zeros_like(d[:, :2])) and np.array_equal(d[:, -2:], np.zeros_like(d[:, -2:]))
+    assert np.max(np.abs(d[:, 2:-2])) > 0
+
+
+def test_averaging_operator_names():
+    """TimeDerivative.create's names (TimeDerivative.pyx:36-53): the J1 class
+    is the midpoint stencil, the J2 class the point derivative; unknown names
+    (including the lower-cased runspec spellings 'arakawaj1' that create does
+    not know) are rejected."""
+    assert vo.averaging_kind(None) == "point" and vo.averaging_kind("none") == "point"
+    assert vo.averaging_kind("arakawa_J1") == vo.averaging_kind("midpoint") == "midpoint"
+    assert vo.averaging_kind("arakawa_J2") == "point"
+    assert vo.averaging_kind("Simpson") == "simpson"
+    for bad in ("arakawaj1", "arakawaj4", "trapezoid"):
+        with pytest.raises(ValueError):
+            vo.averaging_kind(bad)
+
+
 def test_moments(golden):
     g = _grid(golden)
     n, u, e, a = vo.moments(golden["F_pos"], g)

@@ -20,6 +20,26 @@ NOALLOC_MAX_NX = 16384      # VV_NOALLOC_MAX_NX: largest nx of vv_invariants_noa
 BRACKET = {"arakawaj1": 1, "arakawaj2": 2, "arakawaj4": 4, "simpson": 5}
 PC_NONE, PC_TENSOR_KINETIC, PC_TENSOR_POTENTIAL = 0, 1, 2
 LAPLACE = {"cfd2": 2, "cfd4": 4, "simpson": 5}
+# the time derivative by the names TimeDerivative.create knows (TimeDerivative.pyx:36-53)
+AVERAGING = {"point": 0, "midpoint": 1, "arakawa_J1": 1, "arakawa_J2": 2, "arakawa_J4": 4, "simpson": 5}
+
+
+def averaging_code(name):
+    """vv_averaging code of an averaging-operator name (or of a valid code).
+    None/''/'none' is the point derivative (config.py:110-114).  Names
+    TimeDerivative.create does not know -- among them the lower-cased runspec
+    spellings 'arakawaj1/j2/j4', for which create returns None -- raise
+    ValueError."""
+    if isinstance(name, int) and name in AVERAGING.values():
+        return name
+    if name is None or name == "" or str(name).lower() in ("none", "point"):
+        return 0
+    if name in AVERAGING:
+        return AVERAGING[name]
+    if str(name).lower() in ("midpoint", "simpson"):
+        return AVERAGING[str(name).lower()]
+    raise ValueError("unknown averaging operator %r (TimeDerivative.create knows %s)"
+                     % (name, sorted(AVERAGING)))
 ORDER_FACTORED, ORDER_REFERENCE = 0, 1
 PRECISION = {"fp64": 0, "mixed": 1}
 MAX_PICARD = 64
@@ -34,7 +54,7 @@ class vv_grid(C.Structure):
                 ("vmax", C.c_double), ("ht", C.c_double), ("charge", C.c_double), ("mass", C.c_double),
                 ("bracket", C.c_int32), ("preconditioner", C.c_int32), ("laplace", C.c_int32),
                 ("order", C.c_int32), ("gmres_restart", C.c_int32), ("precision", C.c_int32),
-                ("mixed_rtol", C.c_double)]
+                ("mixed_rtol", C.c_double), ("averaging", C.c_int32)]
 
 
 class vv_ksp_opts(C.Structure):

@@ -36,6 +36,8 @@ struct vv_ctx {
     size_t ncell;
     double hx, hv, ht_inv, hx_inv, hv_inv, hx2_inv, f1, f2;
     double lap[4];   // the Laplacian: stencil a0, a1, a2 and denominator (x hx^-2)
+    int avg;         // the time derivative (vv::AvgKind; arakawa_J2 -> point)
+    double tfac;     // ht_inv / divisor of the averaging stencil
     // the potential preconditioner (VV_PC_TENSOR_POTENTIAL): v modes, eigenvalues
     // for n = nv, nv twiddles, transposed field, v spectrum, elimination
     // scratch (FP32 copies in the mixed mode), rows per CTA of the v FFT, phi
@@ -169,6 +171,7 @@ vv::BracketParams bparams(const vv_ctx* c, double factor) {
     p.nx = c->nx;
     p.nv = c->nv;
     p.ht_inv = c->ht_inv;
+    p.tfac = c->tfac;
     p.factor = factor;
     p.f1 = c->f1;
     p.f2 = c->f2;
@@ -221,8 +224,11 @@ int drain_timing(vv_ctx* c) {
 // ---- bracket launches -------------------------------------------------------
 bool aligned16(const void* p) { return p == nullptr || ((uintptr_t)p & 15u) == 0; }
 
+// the wide tiles; with an averaged time derivative only for the Jacobian
+// (the residual, Xh != null, stages F - Fh in the narrow tiles)
 bool wide_ok(const vv_ctx* c, const void* X, const void* Xh, const void* Y) {
-    return !c->narrow_bracket && c->nx % vv::WX == 0 && aligned16(X) && aligned16(Xh) && aligned16(Y);
+    return !c->narrow_bracket && c->nx % vv::WX == 0 && aligned16(X) && aligned16(Xh) && aligned16(Y) &&
+           !(c->avg != vv::AVG_POINT && Xh != nullptr);
 }
 
 // the marching Jacobian stencil: about two waves of CTAs, segments of whole chunks
@@ -243,9 +249,10 @@ int launch_march(vv_ctx* c, const T* X, T* Y, const vv::BracketParams& p) {
     return VV_OK;
 }
 
-// X may be a GMRES basis base pointer with xidx -> the vector index in the state
-template <int SCHEME, int MODE, typename T>
-int launch_bracket_s(vv_ctx* c, const T* X, const T* Xh, T* Y, double factor, double* sumsq, const int* xidx) {
+// X may be a GMRES basis base pointer with xidx -> the vector index in the state;
+// AVG: the time derivative (vv::AvgKind)
+template <int SCHEME, int MODE, typename T, int AVG>
+int launch_bracket_a(vv_ctx* c, const T* X, const T* Xh, T* Y, double factor, double* sumsq, const int* xidx) {
     dim3 grid((c->nx + vv::BX - 1) / vv::BX, (c->nv + vv::BY - 1) / vv::BY);
     dim3 block(vv::BX, vv::TY);
     vv::BracketParams p = bparams(c, factor);
@@ -262,22 +269,24 @@ int launch_bracket_s(vv_ctx* c, const T* X, const T* Xh, T* Y, double factor, do
     bool done = false;
     if constexpr (std::is_same<T, double>::value) {
         if (c->g.order == VV_ORDER_REFERENCE) {
-            vv::k_bracket_ref<SCHEME, MODE><<<grid, block, 0, c->st>>>(X, Xh, Y, p, sumsq);
+            vv::k_bracket_ref<SCHEME, MODE, AVG><<<grid, block, 0, c->st>>>(X, Xh, Y, p, sumsq);
             done = true;
         }
     }
-    if (!done && MODE == vv::MODE_JVP && c->march && c->g.order != VV_ORDER_REFERENCE && c->nx % c->march == 0 &&
-        aligned16(X) && aligned16(Y)) {
+    if (!done && MODE == vv::MODE_JVP && AVG == vv::AVG_POINT && c->march && c->g.order != VV_ORDER_REFERENCE &&
+        c->nx % c->march == 0 && aligned16(X) && aligned16(Y)) {
         TRY(c->march == 256 ? launch_march<SCHEME, T, 256>(c, X, Y, p) : launch_march<SCHEME, T, 128>(c, X, Y, p));
         done = true;
     }
     if (!done) {
-        if (wide_ok(c, X, Xh, Y)) {
-            dim3 gw(c->nx / vv::WX, (c->nv + vv::WY - 1) / vv::WY);
-            vv::k_bracket_wide<SCHEME, MODE, T><<<gw, vv::WTHREADS, 0, c->st>>>(X, Xh, Y, p, sumsq);
-        } else {
-            vv::k_bracket_fac<SCHEME, MODE, T><<<grid, block, 0, c->st>>>(X, Xh, Y, p, sumsq);
+        if constexpr (AVG == vv::AVG_POINT || MODE == vv::MODE_JVP) {
+            if (wide_ok(c, X, Xh, Y)) {
+                dim3 gw(c->nx / vv::WX, (c->nv + vv::WY - 1) / vv::WY);
+                vv::k_bracket_wide<SCHEME, MODE, T, AVG><<<gw, vv::WTHREADS, 0, c->st>>>(X, Xh, Y, p, sumsq);
+                done = true;
+            }
         }
+        if (!done) vv::k_bracket_fac<SCHEME, MODE, T, AVG><<<grid, block, 0, c->st>>>(X, Xh, Y, p, sumsq);
     }
     CKL(c);
     if (timed && e1) cudaEventRecord(e1, c->st);
@@ -286,27 +295,43 @@ int launch_bracket_s(vv_ctx* c, const T* X, const T* Xh, T* Y, double factor, do
 
 // the Simpson bracket: one kernel in the reference's operation order for
 // every order setting and precision (BX x BY tiles)
-template <int MODE, typename T>
+template <int MODE, typename T, int AVG>
 int launch_simpson(vv_ctx* c, const T* X, const T* Xh, T* Y, double factor, double* sumsq, const int* xidx) {
     dim3 grid((c->nx + vv::BX - 1) / vv::BX, (c->nv + vv::BY - 1) / vv::BY);
     dim3 block(vv::BX, vv::TY);
     vv::BracketParams p = bparams(c, factor);
     p.xidx = xidx;
     p.xstride = xidx ? c->ncell : 0;
-    vv::k_bracket_simpson<MODE, T><<<grid, block, 0, c->st>>>(X, Xh, Y, p, sumsq);
+    vv::k_bracket_simpson<MODE, T, AVG><<<grid, block, 0, c->st>>>(X, Xh, Y, p, sumsq);
     CKL(c);
     return VV_OK;
 }
 
+template <int MODE, typename T, int AVG>
+int launch_bracket_avg(vv_ctx* c, const T* X, const T* Xh, T* Y, double factor, double* sumsq, const int* xidx) {
+    switch (c->g.bracket) {
+        case VV_BRACKET_SIMPSON: return launch_simpson<MODE, T, AVG>(c, X, Xh, Y, factor, sumsq, xidx);
+        case VV_BRACKET_J1: return launch_bracket_a<1, MODE, T, AVG>(c, X, Xh, Y, factor, sumsq, xidx);
+        case VV_BRACKET_J2: return launch_bracket_a<2, MODE, T, AVG>(c, X, Xh, Y, factor, sumsq, xidx);
+        default: return launch_bracket_a<4, MODE, T, AVG>(c, X, Xh, Y, factor, sumsq, xidx);
+    }
+}
+
+// MODE_ADD (the bare bracket) has no time derivative
 template <int MODE, typename T>
 int launch_bracket(vv_ctx* c, const T* X, const T* Xh, T* Y, double factor, double* sumsq,
                    const int* xidx = nullptr) {
-    switch (c->g.bracket) {
-        case VV_BRACKET_SIMPSON: return launch_simpson<MODE, T>(c, X, Xh, Y, factor, sumsq, xidx);
-        case VV_BRACKET_J1: return launch_bracket_s<1, MODE, T>(c, X, Xh, Y, factor, sumsq, xidx);
-        case VV_BRACKET_J2: return launch_bracket_s<2, MODE, T>(c, X, Xh, Y, factor, sumsq, xidx);
-        default: return launch_bracket_s<4, MODE, T>(c, X, Xh, Y, factor, sumsq, xidx);
+    if constexpr (MODE != vv::MODE_ADD) {
+        switch (c->avg) {
+            case vv::AVG_MIDPOINT:
+                return launch_bracket_avg<MODE, T, vv::AVG_MIDPOINT>(c, X, Xh, Y, factor, sumsq, xidx);
+            case vv::AVG_SIMPSON:
+                return launch_bracket_avg<MODE, T, vv::AVG_SIMPSON>(c, X, Xh, Y, factor, sumsq, xidx);
+            case vv::AVG_J4: return launch_bracket_avg<MODE, T, vv::AVG_J4>(c, X, Xh, Y, factor, sumsq, xidx);
+            default: break;
+        }
     }
+    return launch_bracket_avg<MODE, T, vv::AVG_POINT>(c, X, Xh, Y, factor, sumsq, xidx);
 }
 
 // number of per-CTA partials a bracket launch writes for these operands
@@ -1060,13 +1085,13 @@ bool same_state(const vv_state& a, const vv_state& b) { return std::memcmp(&a, &
 // scratch buffers (CUDA events, a few launches each) and keeps the fastest:
 // FFT kind x rows per CTA x tridiagonal kind for the preconditioner in the
 // GMRES precision, and the bracket tile shape.  Results are cached per
-// (nx, nv, precision) for the life of the process.
+// (nx, nv, precision, time derivative) for the life of the process.
 struct TuneResult {
     int fft_kind, pcR, tri_kind, narrow, march;
 };
 
-std::vector<std::pair<std::array<int, 3>, TuneResult>>& tune_cache() {
-    static std::vector<std::pair<std::array<int, 3>, TuneResult>> cache;
+std::vector<std::pair<std::array<int, 4>, TuneResult>>& tune_cache() {
+    static std::vector<std::pair<std::array<int, 4>, TuneResult>> cache;
     return cache;
 }
 
@@ -1090,7 +1115,7 @@ int time_it(vv_ctx* c, F fn, int reps, float* ms) {
 }
 
 int autotune(vv_ctx* c) {
-    const std::array<int, 3> key = {c->nx, c->nv, c->mixed ? 1 : 0};
+    const std::array<int, 4> key = {c->nx, c->nv, c->mixed ? 1 : 0, c->avg};
     for (auto& kv : tune_cache())
         if (kv.first == key) {
             c->fft_kind = kv.second.fft_kind;
@@ -1155,7 +1180,7 @@ int autotune(vv_ctx* c) {
     {
         float t_best = 1e30f;
         for (int mw : {0, 128, 256}) {
-            if (mw && (c->nx % mw != 0 || c->g.order == VV_ORDER_REFERENCE)) continue;
+            if (mw && (c->nx % mw != 0 || c->g.order == VV_ORDER_REFERENCE || c->avg != vv::AVG_POINT)) continue;
             c->march = mw;
             float ms = 0.f;
             int r = c->mixed ? time_it(c, [&]() {
@@ -1330,6 +1355,10 @@ int vv_create(const vv_grid* grid, vv_ctx** out) {
         return VV_ERR_ARG;
     if (g.laplace != VV_LAPLACE_CFD4 && g.laplace != VV_LAPLACE_CFD2 && g.laplace != VV_LAPLACE_SIMPSON)
         return VV_ERR_UNSUPPORTED;
+    if (g.averaging != VV_AVERAGING_POINT && g.averaging != VV_AVERAGING_MIDPOINT &&
+        g.averaging != VV_AVERAGING_ARAKAWA_J2 && g.averaging != VV_AVERAGING_ARAKAWA_J4 &&
+        g.averaging != VV_AVERAGING_SIMPSON)
+        return VV_ERR_ARG;
     const int restart = g.gmres_restart > 0 ? g.gmres_restart : 30;
     if (restart > vv::MAX_RESTART) return VV_ERR_ARG;
     if (g.precision != VV_PRECISION_FP64 && g.precision != VV_PRECISION_MIXED) return VV_ERR_ARG;
@@ -1359,6 +1388,12 @@ int vv_create(const vv_grid* grid, vv_ctx** out) {
     c->hx_inv = 1. / c->hx;
     c->hv_inv = 1. / c->hv;
     c->hx2_inv = 1. / (c->hx * c->hx);
+    // the time derivative (TimeDerivative.pyx:36-53): time_fac = ht_inv / divisor
+    c->avg = g.averaging == VV_AVERAGING_MIDPOINT   ? vv::AVG_MIDPOINT
+             : g.averaging == VV_AVERAGING_SIMPSON  ? vv::AVG_SIMPSON
+             : g.averaging == VV_AVERAGING_ARAKAWA_J4 ? vv::AVG_J4
+                                                      : vv::AVG_POINT;
+    c->tfac = c->ht_inv / vv::avg_divisor(c->avg);
     {   // the Laplacian's stencil (matrix_mult of PETScPoissonCFD2/CFD4/Simpson.pyx)
         const double cfd2[4] = {2., -1., 0., 1.}, cfd4[4] = {54., -32., 5., 12.}, simp[4] = {30., -16., 1., 12.};
         const double* l = g.laplace == VV_LAPLACE_CFD2 ? cfd2 : g.laplace == VV_LAPLACE_SIMPSON ? simp : cfd4;
@@ -1781,6 +1816,8 @@ int vv_step_adjoint(vv_ctx* c, const double* F, const double* f, const double* h
     if (c->mixed) return VV_ERR_UNSUPPORTED;
     if (c->g.bracket == VV_BRACKET_SIMPSON)   // the transposed stencil is built for the Arakawa brackets
         return fail(VV_ERR_UNSUPPORTED, "vv_step_adjoint: the Simpson bracket has no transposed stencil here");
+    if (c->avg != vv::AVG_POINT)   // the transposed operator is built for the point time derivative
+        return fail(VV_ERR_UNSUPPORTED, "vv_step_adjoint: averaged time derivatives have no transposed stencil here");
     const int restart = (o->restart > 0) ? o->restart : c->restart;
     if (restart > c->restart || restart < 1 || o->max_it < 0) return VV_ERR_ARG;
     TRY(adj_buffers(c));
@@ -2520,10 +2557,11 @@ int vv_batch_create(int n, vv_ctx* const* ctxs, const vv_state* states, vv_batch
     for (int i = 0; i < n; ++i) {
         const vv_ctx* c = ctxs[i];
         // one scheme, precision and preconditioner for the table; the wide
-        // 64 x 32 stencil tiles (nx a multiple of 64); the factored order
+        // 64 x 32 stencil tiles (nx a multiple of 64); the factored order;
+        // the point time derivative
         if (c->mixed != c0->mixed || c->g.bracket != c0->g.bracket ||
             c->g.preconditioner != VV_PC_TENSOR_KINETIC || c->g.order == VV_ORDER_REFERENCE ||
-            c->g.bracket == VV_BRACKET_SIMPSON ||
+            c->g.bracket == VV_BRACKET_SIMPSON || c->avg != vv::AVG_POINT ||
             c->nx % vv::WX != 0 || !c->pow2 || c->device != c0->device)
             return VV_ERR_UNSUPPORTED;
     }

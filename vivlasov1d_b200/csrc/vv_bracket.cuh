@@ -28,6 +28,7 @@ enum BracketMode { MODE_JVP = 0, MODE_RESIDUAL = 1, MODE_ADD = 2 };
 struct BracketParams {
     int nx, nv;
     double ht_inv;   // 1/ht
+    double tfac;     // ht_inv / divisor of the averaging stencil (unused for 'point')
     double factor;   // bracket factor (0.5 for the JVP, 1.0 residual)
     double f1;       // hx_inv*hv_inv/12
     double f2;       // hx_inv*hv_inv/24
@@ -37,6 +38,73 @@ struct BracketParams {
     const int* xidx;    // optional: input is X + (*xidx) * xstride (GMRES basis vector)
     size_t xstride;
 };
+
+template <typename T> VV_DEV T rn_add(T a, T b);
+template <typename T> VV_DEV T rn_sub(T a, T b);
+template <typename T> VV_DEV T rn_mul(T a, T b);
+template <> VV_DEV double rn_add<double>(double a, double b) { return __dadd_rn(a, b); }
+template <> VV_DEV double rn_sub<double>(double a, double b) { return __dsub_rn(a, b); }
+template <> VV_DEV double rn_mul<double>(double a, double b) { return __dmul_rn(a, b); }
+template <> VV_DEV float rn_add<float>(float a, float b) { return __fadd_rn(a, b); }
+template <> VV_DEV float rn_sub<float>(float a, float b) { return __fsub_rn(a, b); }
+template <> VV_DEV float rn_mul<float>(float a, float b) { return __fmul_rn(a, b); }
+
+// Averaged time derivative (TimeDerivative.pyx:84-275).  On the rows
+// 2 <= j < nv-2 the averaging operators replace ht_inv * x by
+// (stencil sum of x) * ht_inv / divisor:
+//   AVG 1  midpoint (also the arakawa_J1 class)  1 2 1 / 2 4 2 / 1 2 1, /16
+//   AVG 5  Simpson                               1 4 1 / 4 16 4 / 1 4 1, /36
+//   AVG 4  Arakawa J4: 13 points, (0,+-2) 1, diagonals 2, (+-1,0) and
+//          (0,+-1) 8, (+-2,0) 1, centre 20, /64
+// The terms are added in the order of the reference's loop body (v offset
+// outer, x offset inner).  EXACT rounds every operation separately (the
+// FP64 result is the reference's bits); otherwise the compiler may contract,
+// which changes nothing for AVG 1 and 5 (their weights are powers of two).
+// xs(di, dj) returns the input at x offset di, v offset dj.
+enum AvgKind { AVG_POINT = 0, AVG_MIDPOINT = 1, AVG_J4 = 4, AVG_SIMPSON = 5 };
+
+template <int AVG, bool EXACT, typename T, typename Get>
+VV_DEV T avg_stencil(const Get& xs) {
+    auto add = [](T a, T b) -> T {
+        if constexpr (EXACT) return rn_add<T>(a, b);
+        else return a + b;
+    };
+    auto mul = [](T w, T b) -> T {
+        if constexpr (EXACT) return rn_mul<T>(w, b);
+        else return w * b;
+    };
+    if constexpr (AVG == AVG_J4) {
+        T s = xs(0, -2);
+        s = add(s, mul(T(2), xs(-1, -1)));
+        s = add(s, mul(T(8), xs(0, -1)));
+        s = add(s, mul(T(2), xs(1, -1)));
+        s = add(s, xs(-2, 0));
+        s = add(s, mul(T(8), xs(-1, 0)));
+        s = add(s, mul(T(20), xs(0, 0)));
+        s = add(s, mul(T(8), xs(1, 0)));
+        s = add(s, xs(2, 0));
+        s = add(s, mul(T(2), xs(-1, 1)));
+        s = add(s, mul(T(8), xs(0, 1)));
+        s = add(s, mul(T(2), xs(1, 1)));
+        s = add(s, xs(0, 2));
+        return s;
+    } else {
+        constexpr double e = AVG == AVG_MIDPOINT ? 2.0 : 4.0, c = AVG == AVG_MIDPOINT ? 4.0 : 16.0;
+        T s = xs(-1, -1);
+        s = add(s, mul(T(e), xs(0, -1)));
+        s = add(s, xs(1, -1));
+        s = add(s, mul(T(e), xs(-1, 0)));
+        s = add(s, mul(T(c), xs(0, 0)));
+        s = add(s, mul(T(e), xs(1, 0)));
+        s = add(s, xs(-1, 1));
+        s = add(s, mul(T(e), xs(0, 1)));
+        s = add(s, xs(1, 1));
+        return s;
+    }
+}
+
+// divisor of each averaging stencil
+constexpr double avg_divisor(int avg) { return avg == AVG_J4 ? 64.0 : avg == AVG_SIMPSON ? 36.0 : 16.0; }
 
 constexpr int BX = 32;
 constexpr int BY = 16;
@@ -95,6 +163,25 @@ __device__ __forceinline__ void stage_tile(const double* __restrict__ X, const d
     }
 }
 
+// Stage D = X - Xh (the residual's Fder, PETScNLVlasovMP.pyx:53-55) with the
+// same 2-cell halo, for the averaged time derivative of the residual.
+template <typename T, int LD>
+__device__ __forceinline__ void stage_diff(const T* __restrict__ X, const T* __restrict__ Xh,
+                                           const BracketParams& p, int i0, int j0, T (*sd)[LD],
+                                           int sx_w, int sy_h, int nthreads, int tid) {
+    for (int s = tid; s < sx_w * sy_h; s += nthreads) {
+        const int ly = s / sx_w, lx = s - ly * sx_w;
+        const int gi = wrapx(i0 - 2 + lx, p.nx);
+        const int gj = j0 - 2 + ly;
+        T d = T(0);
+        if (gj >= 0 && gj < p.nv) {
+            const size_t g = (size_t)gj * p.nx + gi;
+            d = rn_sub<T>(X[g], Xh[g]);
+        }
+        sd[ly][lx] = d;
+    }
+}
+
 #define R_ADD(a, b) __dadd_rn((a), (b))
 #define R_SUB(a, b) __dsub_rn((a), (b))
 #define R_MUL(a, b) __dmul_rn((a), (b))
@@ -102,16 +189,19 @@ __device__ __forceinline__ void stage_tile(const double* __restrict__ X, const d
 // ---------------------------------------------------------------------------
 // Reference operation order
 // ---------------------------------------------------------------------------
-template <int SCHEME, int MODE>
+template <int SCHEME, int MODE, int AVG = AVG_POINT>
 __global__ void __launch_bounds__(BX * TY)
 k_bracket_ref(const double* __restrict__ X, const double* __restrict__ Xh,
               double* __restrict__ Y, BracketParams p, double* __restrict__ sumsq) {
+    constexpr bool DIFF = AVG != AVG_POINT && MODE == MODE_RESIDUAL;
     if (p.xidx) X += (size_t)(*p.xidx) * p.xstride;
     __shared__ double sx[SY][SX + 1];
     __shared__ double sh[SY][SX + 1];
+    __shared__ double sd[DIFF ? SY : 1][SX + 1];
     __shared__ double sred[BX * TY / 32];
     const int i0 = blockIdx.x * BX, j0 = blockIdx.y * BY;
     stage_tile<MODE, true>(X, Xh, p, i0, j0, sx, sh);
+    if constexpr (DIFF) stage_diff<double, SX + 1>(X, Xh, p, i0, j0, sd, SX, SY, BX * TY, threadIdx.x + BX * threadIdx.y);
     __syncthreads();
 
     double acc2 = 0.0;
@@ -126,14 +216,20 @@ k_bracket_ref(const double* __restrict__ X, const double* __restrict__ Xh,
 #define XS(di, dj) sx[ly + (dj)][lx + (di)]
 #define HS(di, dj) sh[ly + (dj)][lx + (di)]
         double y;
-        if (MODE == MODE_JVP) {
+        const bool inner = j >= 2 && j < p.nv - 2;
+        if (AVG != AVG_POINT && MODE == MODE_JVP && inner) {
+            y = __dmul_rn(avg_stencil<AVG, true, double>([&](int di, int dj) { return XS(di, dj); }), p.tfac);
+        } else if (DIFF && inner) {
+            y = __dmul_rn(avg_stencil<AVG, true, double>([&](int di, int dj) { return sd[ly + dj][lx + di]; }),
+                          p.tfac);
+        } else if (MODE == MODE_JVP) {
             y = R_MUL(p.ht_inv, X[g]);                 // Y.axpy(ht_inv, F)
         } else if (MODE == MODE_RESIDUAL) {
             y = R_MUL(p.ht_inv, R_SUB(X[g], Xh[g]));   // Y.axpy(ht_inv, F - Fh)
         } else {
             y = Y[g];
         }
-        if (j >= 2 && j < p.nv - 2) {
+        if (inner) {
             double s1 = 0.0, s2 = 0.0;
             if (SCHEME == 1 || SCHEME == 4) {
                 const double jpp = R_SUB(R_MUL(R_SUB(XS(1, 0), XS(-1, 0)), R_SUB(HS(0, 1), HS(0, -1))),
@@ -191,23 +287,16 @@ k_bracket_ref(const double* __restrict__ X, const double* __restrict__ Xh,
 // FP64 result is the reference's bits); T = float for the mixed-precision
 // Jacobian.
 // ---------------------------------------------------------------------------
-template <typename T> VV_DEV T rn_add(T a, T b);
-template <typename T> VV_DEV T rn_sub(T a, T b);
-template <typename T> VV_DEV T rn_mul(T a, T b);
-template <> VV_DEV double rn_add<double>(double a, double b) { return __dadd_rn(a, b); }
-template <> VV_DEV double rn_sub<double>(double a, double b) { return __dsub_rn(a, b); }
-template <> VV_DEV double rn_mul<double>(double a, double b) { return __dmul_rn(a, b); }
-template <> VV_DEV float rn_add<float>(float a, float b) { return __fadd_rn(a, b); }
-template <> VV_DEV float rn_sub<float>(float a, float b) { return __fsub_rn(a, b); }
-template <> VV_DEV float rn_mul<float>(float a, float b) { return __fmul_rn(a, b); }
 
-template <int MODE, typename T>
+template <int MODE, typename T, int AVG = AVG_POINT>
 __global__ void __launch_bounds__(BX * TY)
 k_bracket_simpson(const T* __restrict__ X, const T* __restrict__ Xh, T* __restrict__ Y, BracketParams p,
                   double* __restrict__ sumsq) {
+    constexpr bool DIFF = AVG != AVG_POINT && MODE == MODE_RESIDUAL;
     if (p.xidx) X += (size_t)(*p.xidx) * p.xstride;
     __shared__ T sx[SY][SX + 1];
     __shared__ T sh[SY][SX + 1];
+    __shared__ T sd[DIFF ? SY : 1][SX + 1];
     __shared__ double sred[BX * TY / 32];
     const int i0 = blockIdx.x * BX, j0 = blockIdx.y * BY;
     const int tid = threadIdx.x + BX * threadIdx.y;
@@ -225,6 +314,7 @@ k_bracket_simpson(const T* __restrict__ X, const T* __restrict__ Xh, T* __restri
         sx[ly][lx] = xv;
         sh[ly][lx] = hv;
     }
+    if constexpr (DIFF) stage_diff<T, SX + 1>(X, Xh, p, i0, j0, sd, SX, SY, BX * TY, tid);
     __syncthreads();
     const T sfac = T(((p.factor * p.hx_inv) * p.hv_inv) / 9.);   // simpson_factor
     const T htinv = T(p.ht_inv);
@@ -243,10 +333,16 @@ k_bracket_simpson(const T* __restrict__ X, const T* __restrict__ Xh, T* __restri
 #define XS(di, dj) sx[ly + (dj)][lx + (di)]
 #define HS(di, dj) sh[ly + (dj)][lx + (di)]
         T y;
-        if (MODE == MODE_JVP) y = M_(htinv, X[g]);                       // Y.axpy(ht_inv, F)
+        const bool inner = j >= 2 && j < p.nv - 2;
+        if (AVG != AVG_POINT && MODE == MODE_JVP && inner)
+            y = rn_mul<T>(avg_stencil<AVG, true, T>([&](int di, int dj) { return XS(di, dj); }), T(p.tfac));
+        else if (DIFF && inner)
+            y = rn_mul<T>(avg_stencil<AVG, true, T>([&](int di, int dj) { return sd[ly + dj][lx + di]; }),
+                          T(p.tfac));
+        else if (MODE == MODE_JVP) y = M_(htinv, X[g]);                  // Y.axpy(ht_inv, F)
         else if (MODE == MODE_RESIDUAL) y = M_(htinv, S_(X[g], Xh[g]));  // Y.axpy(ht_inv, F - Fh)
         else y = Y[g];                                                   // bracket only: Y += factor [X, H]
-        if (j >= 2 && j < p.nv - 2) {
+        if (inner) {
             T t = M_(S_(XS(0, 2), XS(0, -2)), S_(HS(-2, 0), HS(2, 0)));
             t = A_(t, M_(S_(XS(2, 0), XS(-2, 0)), S_(HS(0, 2), HS(0, -2))));
             t = A_(t, M_(XS(0, 2), S_(HS(-2, 2), HS(2, 2))));
@@ -345,12 +441,14 @@ template <> struct Coef<4> {  // 2*J1 - 0.5*J2 in units of f1 (f2 = f1/2)
     }
 };
 
-template <int SCHEME, int MODE, typename T>
+template <int SCHEME, int MODE, typename T, int AVG = AVG_POINT>
 __global__ void __launch_bounds__(BX * TY)
 k_bracket_fac(const T* __restrict__ X, const T* __restrict__ Xh, T* __restrict__ Y,
               BracketParams p, double* __restrict__ sumsq) {
+    constexpr bool DIFF = AVG != AVG_POINT && MODE == MODE_RESIDUAL;
     if (p.xidx) X += (size_t)(*p.xidx) * p.xstride;
     __shared__ T sx[SY][SX + 1];
+    __shared__ T sd[DIFF ? SY : 1][SX + 1];
     __shared__ double sa[SY];       // a(v) = h0 on the tile rows (with halo)
     __shared__ double sb[SX];       // b(x) on the tile columns (with halo)
     __shared__ double srow[BY][3];  // A1, alpha_m, alpha_p (scaled)
@@ -370,6 +468,7 @@ k_bracket_fac(const T* __restrict__ X, const T* __restrict__ Xh, T* __restrict__
         }
         sx[ly][lx] = xv;
     }
+    if constexpr (DIFF) stage_diff<T, SX + 1>(X, Xh, p, i0, j0, sd, SX, SY, BX * TY, tid);
     if (tid < SY) {
         const int gj = j0 - 2 + tid;
         sa[tid] = (gj >= 0 && gj < p.nv) ? p.h0[gj] : 0.0;
@@ -412,10 +511,15 @@ k_bracket_fac(const T* __restrict__ X, const T* __restrict__ Xh, T* __restrict__
         const size_t g = (size_t)j * p.nx + i;
 #define XS(di, dj) sx[ly + (dj)][lx + (di)]
         T y;
-        if (MODE == MODE_JVP) y = T(p.ht_inv) * X[g];
+        const bool inner = j >= 2 && j < p.nv - 2;
+        if (AVG != AVG_POINT && MODE == MODE_JVP && inner)
+            y = avg_stencil<AVG, false, T>([&](int di, int dj) { return XS(di, dj); }) * T(p.tfac);
+        else if (DIFF && inner)
+            y = avg_stencil<AVG, false, T>([&](int di, int dj) { return sd[ly + dj][lx + di]; }) * T(p.tfac);
+        else if (MODE == MODE_JVP) y = T(p.ht_inv) * X[g];
         else if (MODE == MODE_RESIDUAL) y = T(p.ht_inv) * (X[g] - Xh[g]);
         else y = Y[g];
-        if (j >= 2 && j < p.nv - 2) {
+        if (inner) {
             const T A1 = T(srow[ty][0]), am = T(srow[ty][1]), ap = T(srow[ty][2]);
             const T xm1m1 = XS(-1, -1), xp1m1 = XS(1, -1), xm1p1 = XS(-1, 1), xp1p1 = XS(1, 1);
             T s = T(0);
@@ -468,10 +572,11 @@ template <> struct Vec2<float> { using type = float2; };
 // One 64 x 32 output tile (bx, by) of the bracket; the tile grid is tiles_x
 // wide (the per-tile sum of squares goes to sumsq[bx + tiles_x by]).  Shared
 // by the single-grid kernel below and the batched kernels.
-template <int SCHEME, int MODE, typename T>
+template <int SCHEME, int MODE, typename T, int AVG = AVG_POINT>
 __device__ __forceinline__ void bracket_wide_tile(const T* __restrict__ X, const T* __restrict__ Xh,
                                                   T* __restrict__ Y, const BracketParams& p,
                                                   double* __restrict__ sumsq, int bx, int by, int tiles_x) {
+    static_assert(AVG == AVG_POINT || MODE == MODE_JVP, "the wide tiles average the Jacobian only");
     using V2 = typename Vec2<T>::type;
     __shared__ __align__(16) T sx[WSY][WSX];
     __shared__ double sa[WSY];
@@ -556,10 +661,19 @@ __device__ __forceinline__ void bracket_wide_tile(const T* __restrict__ X, const
         if (j < nv) {
             const size_t g = (size_t)j * nx + i;
             T y;
-            if (MODE == MODE_JVP) y = htinv * w2;
+            const bool inner = j >= 2 && j < nv - 2;
+            if (AVG != AVG_POINT && inner) {
+                // the window holds every stencil point but (+-2, 0)
+                y = avg_stencil<AVG, false, T>([&](int di, int dj) -> T {
+                        if (di == 0) return dj == -2 ? w0 : dj == -1 ? w1 : dj == 0 ? w2 : dj == 1 ? w3 : w4;
+                        if (di == -1) return dj == -1 ? m0 : dj == 0 ? m1 : m2;
+                        if (di == 1) return dj == -1 ? q0 : dj == 0 ? q1 : q2;
+                        return sx[r0 + q + 2][lx + di];
+                    }) * T(p.tfac);
+            } else if (MODE == MODE_JVP) y = htinv * w2;
             else if (MODE == MODE_RESIDUAL) y = htinv * (X[g] - Xh[g]);
             else y = Y[g];
-            if (j >= 2 && j < nv - 2) {
+            if (inner) {
                 const T A1 = T(srow[r0 + q][0]), am = T(srow[r0 + q][1]), ap = T(srow[r0 + q][2]);
                 T s = T(0);
                 if (Coef<SCHEME>::cA1 != 0.0 || Coef<SCHEME>::cA2 != 0.0) {
@@ -771,12 +885,12 @@ k_bracket_march(const T* __restrict__ X, T* __restrict__ Y, BracketParams p, int
     bracket_march_item<SCHEME, T, MW>(X, Y, p, seg, blockIdx.x, blockIdx.y);
 }
 
-template <int SCHEME, int MODE, typename T>
+template <int SCHEME, int MODE, typename T, int AVG = AVG_POINT>
 __global__ void __launch_bounds__(WTHREADS, 4)
 k_bracket_wide(const T* __restrict__ X, const T* __restrict__ Xh, T* __restrict__ Y,
                BracketParams p, double* __restrict__ sumsq) {
     if (p.xidx) X += (size_t)(*p.xidx) * p.xstride;
-    bracket_wide_tile<SCHEME, MODE, T>(X, Xh, Y, p, sumsq, blockIdx.x, blockIdx.y, gridDim.x);
+    bracket_wide_tile<SCHEME, MODE, T, AVG>(X, Xh, Y, p, sumsq, blockIdx.x, blockIdx.y, gridDim.x);
 }
 
 }  // namespace vv

@@ -49,7 +49,8 @@ class Run:
         self.ctx = self.grid.context(bracket=cfg.get_poisson_bracket(),
                                      preconditioner=cfg.get_preconditioner() or None,
                                      charge=self.charge, mass=self.mass, order=order, restart=restart,
-                                     precision=precision, laplace=cfg.get_laplace_operator())
+                                     precision=precision, laplace=cfg.get_laplace_operator(),
+                                     averaging=cfg.get_averaging_operator())
         g = self.grid
         fld, xv = g.field, g.xvec
         self.fc, self.fh = fld(), fld()

@@ -80,9 +80,9 @@ class Grid:
         return torch.zeros(self.nx, dtype=torch.float64, device=self.device)
 
     def context(self, bracket="arakawaj4", preconditioner="tensor_kinetic", charge=-1.0, mass=1.0,
-                order="factored", restart=30, precision="fp64", mixed_rtol=0.0, laplace="cfd4"):
+                order="factored", restart=30, precision="fp64", mixed_rtol=0.0, laplace="cfd4", averaging="point"):
         key = (bracket, preconditioner, float(charge), float(mass), order, int(restart), precision, float(mixed_rtol),
-               laplace.lower())
+               laplace.lower(), _lib.averaging_code(averaging))
         ctx = self._contexts.get(key)
         if ctx is None:
             ctx = Context(self, *key)
@@ -95,7 +95,8 @@ class Context:
     """Owner of one ``vv_ctx`` (device work buffers, preconditioner factors)."""
 
     def __init__(self, grid, bracket="arakawaj4", preconditioner="tensor_kinetic", charge=-1.0,
-                 mass=1.0, order="factored", restart=30, precision="fp64", mixed_rtol=0.0, laplace="cfd4"):
+                 mass=1.0, order="factored", restart=30, precision="fp64", mixed_rtol=0.0, laplace="cfd4",
+                 averaging="point"):
         lib = _lib.load()
         if not torch.cuda.is_available():
             raise RuntimeError("vivlasov1d_b200 needs a CUDA device; no CPU fallback exists")
@@ -120,6 +121,8 @@ class Context:
             raise NotImplementedError("laplace_operator %r is not implemented on this path" % laplace)
         g.laplace = _lib.LAPLACE[laplace.lower()]
         self.laplace = laplace.lower()
+        g.averaging = _lib.averaging_code(averaging)
+        self.averaging = g.averaging
         g.order = _lib.ORDER_REFERENCE if order == "reference" else _lib.ORDER_FACTORED
         g.gmres_restart = int(restart)
         if precision not in _lib.PRECISION:
@@ -289,12 +292,11 @@ class PETScVlasovSolver:
         cfg = config if config is not None else {}
         bracket = _cfg_get(cfg, "get_poisson_bracket", "poisson_bracket", "arakawaj4")
         pc = _cfg_get(cfg, "get_preconditioner", "preconditioner", "")
+        # TimeDerivative.create(config.get_averaging_operator(), ...) (PETScVlasovSolver.pyx:99)
         avg = _cfg_get(cfg, "get_averaging_operator", "averaging_operator", "point")
-        if avg not in ("point", None, "", "none"):
-            raise NotImplementedError("averaging operator %r is not on this path" % avg)
         mass = 1.0 if H0 is None or isinstance(H0, torch.Tensor) else float(H0)
         self.ctx = grid.context(bracket=bracket, preconditioner=pc or None, charge=charge, mass=mass,
-                                order=order, restart=restart)
+                                order=order, restart=restart, averaging=avg)
         self.H0, self.H1p, self.H1h, self.H2p, self.H2h = H0, H1p, H1h, H2p, H2h
         self.phi = phi
         self.preconditioner = TensorProductPreconditioner.create(pc, grid=grid, phi=phi, context=self.ctx) \
