@@ -58,10 +58,15 @@ enum vv_preconditioner {     /* solver.preconditioner_scheme                  */
     VV_PC_TENSOR_KINETIC = 1,   /* TensorProductKineticFast.pyx                */
     VV_PC_TENSOR_POTENTIAL = 2  /* TensorProductPotentialFast.pyx              */
 };
-enum vv_laplace {            /* solver.laplace_operator                       */
+enum vv_laplace {            /* solver.laplace_operator (run_base.py:93-94
+                                imports PETScPoisson<laplace_operator>)       */
     VV_LAPLACE_CFD2 = 2,     /* PETScPoissonCFD2.pyx                           */
     VV_LAPLACE_CFD4 = 4,     /* PETScPoissonCFD4.pyx (default)                 */
-    VV_LAPLACE_SIMPSON = 5   /* PETScPoissonSimpson.pyx                        */
+    VV_LAPLACE_SIMPSON = 5,  /* PETScPoissonSimpson.pyx                        */
+    VV_LAPLACE_CFD2_AVE = 12,   /* PETScPoissonCFD2Ave.pyx: the CFD2 Laplacian,
+                                   density averaged (1 2 1)/4 in the RHS       */
+    VV_LAPLACE_SIMPSON_AVE = 15 /* PETScPoissonSimpsonAve.pyx: the Simpson
+                                   Laplacian, density (1 8 18 8 1)/36          */
 };
 enum vv_averaging {          /* solver.averaging_operator: the time derivative
                                 (TimeDerivative.pyx:36-53; 0 for None/'none') */

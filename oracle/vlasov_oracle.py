@@ -507,19 +507,39 @@ def moments(f, grid):
 #                 PETScPoissonCFD4.pyx:111-183,
 #                 run/run_nonlinear_matrixfree_split_mp.py:56-80)
 # --------------------------------------------------------------------------
-def poisson_rhs(n, charge):
-    """``b = -(n - mean n) * charge`` (PETScPoissonSolver.pyx:58-74)."""
+def rhs_density(n, laplace="cfd4"):
+    """The density the right-hand side uses: n itself, or the periodic
+    average of the Ave operators in their operation order
+    (PETScPoissonCFD2Ave.pyx:64-80: 0.25 (n[i-1] + 2 n[i] + n[i+1]);
+    PETScPoissonSimpsonAve.pyx:64-80: (n[i-2] + 8 n[i-1] + 18 n[i]
+    + 8 n[i+1] + n[i+2]) / 36)."""
+    r = np.roll
+    if laplace == "cfd2ave":
+        return 0.25 * (r(n, 1) + 2. * n + r(n, -1))
+    if laplace == "simpsonave":
+        return (r(n, 2) + 8. * r(n, 1) + 18. * n + 8. * r(n, -1) + r(n, -2)) / 36.
+    return n
+
+
+def poisson_rhs(n, charge, laplace="cfd4"):
+    """``b = -(n~ - mean n) * charge`` (PETScPoissonSolver.pyx:58-74; n~ the
+    Ave operators' averaged density, :func:`rhs_density`)."""
     nmean = n.sum() / n.size
-    return -(n - nmean) * charge
+    return -(rhs_density(n, laplace) - nmean) * charge
 
 
 # laplace_operator: the periodic 5-point stencil (a0, a1, a2) / den hx^-2 and
-# its Fourier symbol (a0 + 2 a1 cos t + 2 a2 cos 2t) / den hx^-2
+# its Fourier symbol (a0 + 2 a1 cos t + 2 a2 cos 2t) / den hx^-2; the Ave
+# operators keep CFD2's / Simpson's stencil and average the density in the
+# right-hand side with the symbol RHS_AVERAGE (r0 + 2 r1 cos t + 2 r2 cos 2t)/rden
 LAPLACE = {
     "cfd2": (2., -1., 0., 1.),       # PETScPoissonCFD2.pyx:64-101
     "cfd4": (54., -32., 5., 12.),    # PETScPoissonCFD4.pyx:146-183
     "simpson": (30., -16., 1., 12.),  # PETScPoissonSimpson.pyx:62-101
+    "cfd2ave": (2., -1., 0., 1.),    # PETScPoissonCFD2Ave.pyx:83-115
+    "simpsonave": (30., -16., 1., 12.),  # PETScPoissonSimpsonAve.pyx:83-120
 }
+RHS_AVERAGE = {"cfd2ave": (2., 1., 0., 4.), "simpsonave": (18., 8., 1., 36.)}
 
 
 def poisson_matvec(x, hx2_inv, laplace="cfd4"):
@@ -527,18 +547,18 @@ def poisson_matvec(x, hx2_inv, laplace="cfd4"):
     PETScPoissonCFD4.pyx:146-160, PETScPoissonCFD2.pyx:64-78,
     PETScPoissonSimpson.pyx:62-76, in their operation order)."""
     r = np.roll
-    if laplace == "cfd2":
+    if laplace in ("cfd2", "cfd2ave"):
         return (2. * x - r(x, 1) - r(x, -1)) * hx2_inv
-    if laplace == "simpson":
+    if laplace in ("simpson", "simpsonave"):
         return (1. * r(x, 2) - 16. * r(x, 1) + 30. * x - 16. * r(x, -1) + 1. * r(x, -2)) * hx2_inv / 12.
     return (5. * r(x, 2) - 32. * r(x, 1) + 54. * x - 32. * r(x, -1) + 5. * r(x, -2)) * hx2_inv / 12.
 
 
 def poisson_function(x, n, hx2_inv, charge, laplace="cfd4"):
-    """Poisson residual ``A x + (n - mean n) * charge`` (function_mult of
-    the three operators, e.g. PETScPoissonCFD4.pyx:163-183)."""
+    """Poisson residual ``A x + (n~ - mean n) * charge`` (function_mult of
+    the operators, e.g. PETScPoissonCFD4.pyx:163-183)."""
     nmean = n.sum() / n.size
-    return poisson_matvec(x, hx2_inv, laplace) + (n - nmean) * charge
+    return poisson_matvec(x, hx2_inv, laplace) + (rhs_density(n, laplace) - nmean) * charge
 
 
 def poisson_solve(n, grid, charge, laplace="cfd4"):
@@ -548,7 +568,7 @@ def poisson_solve(n, grid, charge, laplace="cfd4"):
     1e-13) and the constant null space attached; the oracle uses the exact
     circulant inverse, whose result is mean-free.  The mean of phi never
     enters the dynamics (h1 subtracts it, Toolbox.pyx:50-56)."""
-    b = poisson_rhs(n, charge)
+    b = poisson_rhs(n, charge, laplace)
     nx = grid.nx
     th = 2. * np.pi * np.arange(nx // 2 + 1) / nx
     a0, a1, a2, den = LAPLACE[laplace]

@@ -370,7 +370,8 @@ def reference_namespace():
     ps["PETScPoissonSolverBase"] = ps["PETScPoissonSolverBase"]
     load("vlasov/solvers/poisson/PETScPoissonCFD4.pyx", ps)
     ns["PETScPoissonSolverCFD4"] = ps["PETScPoissonSolver"]
-    for name, fn in (("CFD2", "PETScPoissonCFD2.pyx"), ("Simpson", "PETScPoissonSimpson.pyx")):
+    for name, fn in (("CFD2", "PETScPoissonCFD2.pyx"), ("Simpson", "PETScPoissonSimpson.pyx"),
+                     ("CFD2Ave", "PETScPoissonCFD2Ave.pyx"), ("SimpsonAve", "PETScPoissonSimpsonAve.pyx")):
         pv = dict(ns)
         load("vlasov/solvers/poisson/PETScPoissonSolver.pyx", pv)
         load("vlasov/solvers/poisson/" + fn, pv)
@@ -505,13 +506,17 @@ def make_case(ns, nx, nv, L, vmin, vmax, ht, seed):
     out["poisson_matvec"] = Y.a.copy()
     ps.function_mult(P, N, Y)
     out["poisson_function"] = Y.a.copy()
-    # the other laplace_operator choices (PETScPoissonCFD2.pyx, PETScPoissonSimpson.pyx)
-    for name in ("CFD2", "Simpson"):
+    # the other laplace_operator choices (PETScPoissonCFD2.pyx, PETScPoissonSimpson.pyx and
+    # the density-averaging PETScPoissonCFD2Ave.pyx, PETScPoissonSimpsonAve.pyx)
+    for name in ("CFD2", "Simpson", "CFD2Ave", "SimpsonAve"):
         pso = ns["PETScPoissonSolver" + name](dax, nx, hx, -1.0)
         pso.matrix_mult(P, Y)
         out["poisson_matvec_" + name.lower()] = Y.a.copy()
         pso.function_mult(P, N, Y)
         out["poisson_function_" + name.lower()] = Y.a.copy()
+        if name.endswith("Ave"):
+            pso.formRHS(N, B)
+            out["poisson_rhs_" + name.lower()] = B.a.copy()
 
     # preconditioner eigenvalues and band matrices
     eig = ns["TensorProductPreconditioner"].compute_eigenvalues(None, nx)

@@ -709,15 +709,19 @@ def test_potential_solver_class_update_history():
 # laplace_operator: CFD2 and Simpson
 # ---------------------------------------------------------------------------
 @pytest.mark.parametrize("path", GOLDEN, ids=[os.path.basename(p) for p in GOLDEN])
-@pytest.mark.parametrize("laplace", ["cfd2", "simpson"])
+@pytest.mark.parametrize("laplace", ["cfd2", "simpson", "cfd2ave", "simpsonave"])
 def test_poisson_variants_golden(path, laplace):
-    """matrix_mult / function_mult of the CFD2 and Simpson Laplacians against
-    the reference's own vectors, and the solve against the oracle's."""
+    """matrix_mult / function_mult (and formRHS of the density-averaging Ave
+    operators) of the CFD2 and Simpson Laplacians against the reference's own
+    vectors, and the solve against the oracle's."""
     from vivlasov1d_b200 import PETScPoissonSolver
     g = dict(np.load(path))
     grid = ggrid(g)
     ps = PETScPoissonSolver(grid, charge=-1.0, laplace=laplace)
     B = grid.xvec()
+    if laplace.endswith("ave"):
+        ps.formRHS(xdev(g["n"]), B)
+        assert rel(B.cpu().numpy(), g["poisson_rhs_" + laplace]) < 1e-13
     P = xdev(g["phi_p"])
     ps.matrix_mult(P, B)
     assert rel(B.cpu().numpy(), g["poisson_matvec_" + laplace]) < 1e-13
@@ -728,7 +732,7 @@ def test_poisson_variants_golden(path, laplace):
     assert rel(phi.cpu().numpy(), vo.poisson_solve(g["n"], ogrid(g), -1.0, laplace)) < 1e-12
 
 
-@pytest.mark.parametrize("laplace", ["CFD2", "Simpson"])
+@pytest.mark.parametrize("laplace", ["CFD2", "Simpson", "CFD2Ave", "SimpsonAve"])
 def test_laplace_variant_step_matches_oracle(laplace):
     """Two implicit steps with laplace_operator = CFD2 / Simpson (moments,
     Poisson solve and the Poisson part of the Picard residual) against the

@@ -200,13 +200,16 @@ def test_potential_preconditioner_inverts_band_operator(golden):
     assert relerr(pc.apply(Ax), x) < 1e-12
 
 
-@pytest.mark.parametrize("laplace", ["cfd2", "simpson"])
+@pytest.mark.parametrize("laplace", ["cfd2", "simpson", "cfd2ave", "simpsonave"])
 def test_poisson_operator_variants(golden, laplace):
-    """The CFD2 and Simpson Laplacians (matrix_mult, function_mult) equal the
-    reference's own, and the circulant solve inverts them on the mean-free
-    subspace."""
+    """The CFD2 and Simpson Laplacians and their density-averaging Ave
+    variants (matrix_mult, function_mult, and formRHS of the Ave classes)
+    equal the reference's own, and the circulant solve inverts them on the
+    mean-free subspace."""
     g = _grid(golden)
     n = golden["n"]
+    if laplace.endswith("ave"):
+        assert relerr(vo.poisson_rhs(n, -1.0, laplace), golden["poisson_rhs_" + laplace]) < 1e-14
     assert relerr(vo.poisson_matvec(golden["phi_p"], g.hx2_inv, laplace),
                   golden["poisson_matvec_" + laplace]) < 1e-13
     assert relerr(vo.poisson_function(golden["phi_p"], n, g.hx2_inv, -1.0, laplace),

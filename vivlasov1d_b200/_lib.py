@@ -19,7 +19,7 @@ VV_ERR_DIVERGED = 5
 NOALLOC_MAX_NX = 16384      # VV_NOALLOC_MAX_NX: largest nx of vv_invariants_noalloc
 BRACKET = {"arakawaj1": 1, "arakawaj2": 2, "arakawaj4": 4, "simpson": 5}
 PC_NONE, PC_TENSOR_KINETIC, PC_TENSOR_POTENTIAL = 0, 1, 2
-LAPLACE = {"cfd2": 2, "cfd4": 4, "simpson": 5}
+LAPLACE = {"cfd2": 2, "cfd4": 4, "simpson": 5, "cfd2ave": 12, "simpsonave": 15}
 # the time derivative by the names TimeDerivative.create knows (TimeDerivative.pyx:36-53)
 AVERAGING = {"point": 0, "midpoint": 1, "arakawa_J1": 1, "arakawa_J2": 2, "arakawa_J4": 4, "simpson": 5}
 

@@ -36,6 +36,7 @@ struct vv_ctx {
     size_t ncell;
     double hx, hv, ht_inv, hx_inv, hv_inv, hx2_inv, f1, f2;
     double lap[4];   // the Laplacian: stencil a0, a1, a2 and denominator (x hx^-2)
+    double ravg[4];  // the right-hand side's density average: r0, r1, r2, denominator
     int avg;         // the time derivative (vv::AvgKind; arakawa_J2 -> point)
     double tfac;     // ht_inv / divisor of the averaging stencil
     // the potential preconditioner (VV_PC_TENSOR_POTENTIAL): v modes, eigenvalues
@@ -749,6 +750,11 @@ vv::PoissonParams pparams(const vv_ctx* c) {
     p.la1 = c->lap[1];
     p.la2 = c->lap[2];
     p.lden = c->lap[3];
+    p.ravg = c->ravg[3] != 1.0 ? 1 : 0;
+    p.ra0 = c->ravg[0];
+    p.ra1 = c->ravg[1];
+    p.ra2 = c->ravg[2];
+    p.rden = c->ravg[3];
     return p;
 }
 
@@ -765,14 +771,13 @@ int moments_poisson(vv_ctx* c, const double* F, double* n, double* u, double* e,
 }
 
 __global__ void k_poisson_apply(const double* __restrict__ x, const double* __restrict__ n,
-                                double* __restrict__ y, int nx, double hx2_inv, double charge, int mode,
-                                double* __restrict__ sumsq, double a0, double a1, double a2, double den) {
-    vv::poisson_apply_cta(x, n, y, nx, hx2_inv, charge, mode, sumsq, a0, a1, a2, den);
+                                double* __restrict__ y, int mode, double* __restrict__ sumsq, vv::PoissonParams p) {
+    vv::poisson_apply_cta(x, n, y, p.nx, p.hx2_inv, p.charge, mode, sumsq, p.la0, p.la1, p.la2, p.lden, p.ravg, p.ra0,
+                          p.ra1, p.ra2, p.rden);
 }
 
 int poisson_apply(vv_ctx* c, const double* x, const double* n, double* y, int mode, double* sumsq) {
-    k_poisson_apply<<<1, 1024, 0, c->st>>>(x, n, y, c->nx, c->hx2_inv, c->g.charge, mode, sumsq, c->lap[0], c->lap[1],
-                                           c->lap[2], c->lap[3]);
+    k_poisson_apply<<<1, 1024, 0, c->st>>>(x, n, y, mode, sumsq, pparams(c));
     CKL(c);
     return VV_OK;
 }
@@ -1353,7 +1358,8 @@ int vv_create(const vv_grid* grid, vv_ctx** out) {
     if (g.preconditioner != VV_PC_NONE && g.preconditioner != VV_PC_TENSOR_KINETIC &&
         g.preconditioner != VV_PC_TENSOR_POTENTIAL)
         return VV_ERR_ARG;
-    if (g.laplace != VV_LAPLACE_CFD4 && g.laplace != VV_LAPLACE_CFD2 && g.laplace != VV_LAPLACE_SIMPSON)
+    if (g.laplace != VV_LAPLACE_CFD4 && g.laplace != VV_LAPLACE_CFD2 && g.laplace != VV_LAPLACE_SIMPSON &&
+        g.laplace != VV_LAPLACE_CFD2_AVE && g.laplace != VV_LAPLACE_SIMPSON_AVE)
         return VV_ERR_UNSUPPORTED;
     if (g.averaging != VV_AVERAGING_POINT && g.averaging != VV_AVERAGING_MIDPOINT &&
         g.averaging != VV_AVERAGING_ARAKAWA_J2 && g.averaging != VV_AVERAGING_ARAKAWA_J4 &&
@@ -1394,10 +1400,18 @@ int vv_create(const vv_grid* grid, vv_ctx** out) {
              : g.averaging == VV_AVERAGING_ARAKAWA_J4 ? vv::AVG_J4
                                                       : vv::AVG_POINT;
     c->tfac = c->ht_inv / vv::avg_divisor(c->avg);
-    {   // the Laplacian's stencil (matrix_mult of PETScPoissonCFD2/CFD4/Simpson.pyx)
+    {   // the Laplacian's stencil (matrix_mult of PETScPoissonCFD2/CFD4/Simpson.pyx; the Ave classes
+        // keep CFD2's / Simpson's) and the density average of their formRHS (PETScPoissonCFD2Ave.pyx:
+        // 0.25 (n_{i-1} + 2 n_i + n_{i+1}); PETScPoissonSimpsonAve.pyx: (n_{i-2} + 8 n_{i-1} + 18 n_i
+        // + 8 n_{i+1} + n_{i+2}) / 36)
         const double cfd2[4] = {2., -1., 0., 1.}, cfd4[4] = {54., -32., 5., 12.}, simp[4] = {30., -16., 1., 12.};
-        const double* l = g.laplace == VV_LAPLACE_CFD2 ? cfd2 : g.laplace == VV_LAPLACE_SIMPSON ? simp : cfd4;
+        const bool c2 = g.laplace == VV_LAPLACE_CFD2 || g.laplace == VV_LAPLACE_CFD2_AVE;
+        const bool sp = g.laplace == VV_LAPLACE_SIMPSON || g.laplace == VV_LAPLACE_SIMPSON_AVE;
+        const double* l = c2 ? cfd2 : sp ? simp : cfd4;
         for (int k = 0; k < 4; ++k) c->lap[k] = l[k];
+        const double none[4] = {1., 0., 0., 1.}, a2[4] = {2., 1., 0., 4.}, as[4] = {18., 8., 1., 36.};
+        const double* r = g.laplace == VV_LAPLACE_CFD2_AVE ? a2 : g.laplace == VV_LAPLACE_SIMPSON_AVE ? as : none;
+        for (int k = 0; k < 4; ++k) c->ravg[k] = r[k];
     }
     c->f1 = c->hx_inv * c->hv_inv / 12.;  // PoissonBracket.pyx:344
     c->f2 = c->hx_inv * c->hv_inv / 24.;  // PoissonBracket.pyx:345
@@ -1520,14 +1534,18 @@ int vv_create(const vv_grid* grid, vv_ctx** out) {
         }
     }
     c->pivot_differs = piv;
-    // CFD4 symbol (PETScPoissonCFD4.pyx:130-134): (54 - 64 cos t + 10 cos 2t)/(12 hx^2)
+    // the Laplacian's symbol (e.g. CFD4, PETScPoissonCFD4.pyx:130-134: (54 - 64 cos t + 10 cos 2t)/(12 hx^2))
+    // and, for the Ave operators, the symbol of the density average in the numerator
     std::vector<double> sym(nm);
     for (int k = 0; k < nm; ++k) {
         const long double t = 2.0L * PI * (long double)k / (long double)nx;
         const long double s_ = ((long double)c->lap[0] + 2.0L * (long double)c->lap[1] * cosl(t) +
                                 2.0L * (long double)c->lap[2] * cosl(2.0L * t)) *
                                (long double)c->hx2_inv / (long double)c->lap[3];
-        sym[k] = (k == 0) ? 0.0 : (double)(1.0L / s_);
+        const long double a_ = ((long double)c->ravg[0] + 2.0L * (long double)c->ravg[1] * cosl(t) +
+                                2.0L * (long double)c->ravg[2] * cosl(2.0L * t)) /
+                               (long double)c->ravg[3];
+        sym[k] = (k == 0) ? 0.0 : (double)(a_ / s_);
     }
     std::vector<double2> lam_h(lam2);
     if (cudaMemcpy(c->v, hv_.data(), nv * sizeof(double), cudaMemcpyHostToDevice) != cudaSuccess ||

@@ -91,6 +91,41 @@ VV_DEV void for_work(const BInst* __restrict__ tab, const int* __restrict__ L, i
     }
 }
 
+// Warp-granular loop over the same work: block item b of an instance is the
+// eight warp items 8 b .. 8 b + 7, and every warp walks the list's warp items
+// on its own (body(instance, local warp item), warp-uniform), with no barrier
+// between items, so the warps of an SM overlap one item's header loads with
+// another's data.  For bodies that use no shared memory per item; the block
+// must have 8 warps.
+template <int F, typename Body>
+VV_DEV void for_warp_work(const BInst* __restrict__ tab, const int* __restrict__ L, int n, Body body) {
+    __shared__ int s_pre[BLIST_SMEM + 1];
+    __shared__ int s_ids[BLIST_SMEM];
+    const int nact = L[0];
+    const int total = L[1 + F];
+    if ((int)blockIdx.x >= total) return;
+    const int* ids = L + 1 + NFAM;
+    const int* pre = ids + n + (size_t)F * (n + 1);
+    if (nact <= BLIST_SMEM) {
+        for (int i = threadIdx.x; i <= nact; i += blockDim.x) s_pre[i] = pre[i];
+        for (int i = threadIdx.x; i < nact; i += blockDim.x) s_ids[i] = ids[i];
+        __syncthreads();
+        pre = s_pre;
+        ids = s_ids;
+    }
+    const int nw = gridDim.x * 8, wtotal = 8 * total;
+    for (int w = blockIdx.x * 8 + (threadIdx.x >> 5); w < wtotal; w += nw) {
+        const int bw = w >> 3;
+        int lo = 0, hi = nact - 1;   // the last p with pre[p] <= bw
+        while (lo < hi) {
+            const int mid = (lo + hi + 1) >> 1;
+            if (pre[mid] <= bw) lo = mid;
+            else hi = mid - 1;
+        }
+        body(tab[ids[lo]], w - 8 * pre[lo]);
+    }
+}
+
 // ---- stencil ----------------------------------------------------------------
 enum BSrc { BS_RESIDUAL = 0, BS_X = 1, BS_VIT = 2 };
 
@@ -348,7 +383,7 @@ __global__ void __launch_bounds__(1024) k_b_poisson(const BInst* __restrict__ ta
     for_work<F_INST>(tab, L, n, [&](const BInst& I, int) {
         for (int i = threadIdx.x; i < I.nx; i += blockDim.x) I.hxp[i] = I.h1c[i];
         poisson_apply_cta(I.phi, I.n, nullptr, I.nx, I.po.hx2_inv, I.po.charge, 2, &I.ds->pnorm2, I.po.la0, I.po.la1,
-                          I.po.la2, I.po.lden);
+                          I.po.la2, I.po.lden, I.po.ravg, I.po.ra0, I.po.ra1, I.po.ra2, I.po.rden);
     });
 }
 
@@ -479,9 +514,10 @@ __global__ void k_b_gm_cycle_f(const BInst* __restrict__ tab, const int* __restr
 // <w, V_q>, q = 0..it, w = V[it+1], per warp item (column q of the partials)
 template <typename T>
 __global__ void __launch_bounds__(RED_THREADS, 4) k_b_gm_mdot_p(const BInst* __restrict__ tab, const int* __restrict__ L, int n) {
+    static_assert(RED_THREADS == 256, "eight warp items per block item");
     constexpr int VN = vec_n<T>(), WV = WCELLS / (32 * VN);
-    for_work<F_VEC>(tab, L, n, [&](const BInst& I, int bid) {
-        const int lane = threadIdx.x & 31, nwi = wi_count(I), wi = bid * 8 + (threadIdx.x >> 5);
+    for_warp_work<F_VEC>(tab, L, n, [&](const BInst& I, int wi) {
+        const int lane = threadIdx.x & 31, nwi = wi_count(I);
         const int it = I.ds->it, m = it + 1;
         const size_t nc = I.ncell;
         const T* V = (const T*)I.V;

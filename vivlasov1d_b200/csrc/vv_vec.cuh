@@ -531,10 +531,26 @@ struct PoissonParams {
     int nx, M, logM, S;   // S = number of moment partials
     double hv, charge, hx2_inv, hx, inv_nx;
     const double2* tw;       // nx twiddles W^k (the FFT reads k < nx/2)
-    const double* sym_inv;   // M+1 entries: 1/symbol_k (0 for k = 0)
+    const double* sym_inv;   // M+1 entries: (density-average symbol / Laplacian symbol)_k, 0 for k = 0
     // the Laplacian: periodic stencil (la2, la1, la0, la1, la2) / lden hx^-2
     double la0, la1, la2, lden;
+    // the density in the right-hand side: (ra2, ra1, ra0, ra1, ra2) / rden
+    // (PETScPoissonCFD2Ave/SimpsonAve.pyx; ravg = 0: n itself); the spectral
+    // solve folds its symbol into sym_inv
+    int ravg;
+    double ra0, ra1, ra2, rden;
 };
+
+// the right-hand side's density at i: n_i, or its periodic 5-point average
+// in the reference's order ((((r2 n_{i-2} + r1 n_{i-1}) + r0 n_i) + r1 n_{i+1})
+// + r2 n_{i+2}) / rden
+__device__ __forceinline__ double rhs_density(const double* __restrict__ n, int i, int nx, int ravg, double r0,
+                                              double r1, double r2, double rden) {
+    if (!ravg) return n[i];
+    const int im2 = (i - 2 + 2 * nx) % nx, im1 = (i - 1 + nx) % nx;
+    const int ip1 = (i + 1) % nx, ip2 = (i + 2) % nx;
+    return ((((r2 * n[im2] + r1 * n[im1]) + r0 * n[i]) + r1 * n[ip1]) + r2 * n[ip2]) / rden;
+}
 
 constexpr int POIS_THREADS = 1024;
 
@@ -679,7 +695,7 @@ __device__ __forceinline__ void moments_poisson_cta(const double* __restrict__ p
         const int ip1 = (i + 1) % nx, ip2 = (i + 2) % nx;
         const double Ax =
             (p.la2 * phs[im2] + p.la1 * phs[im1] + p.la0 * pc + p.la1 * phs[ip1] + p.la2 * phs[ip2]) * p.hx2_inv / p.lden;
-        const double r = Ax + (nn[i] - nmean) * p.charge;
+        const double r = Ax + (rhs_density(nn, i, nx, p.ravg, p.ra0, p.ra1, p.ra2, p.rden) - nmean) * p.charge;
         r2 += r * r;
     }
     r2 = block_sum(r2, red);
@@ -696,15 +712,17 @@ k_moments_poisson(const double* __restrict__ part, const double* __restrict__ n_
     moments_poisson_cta(part, n_in, n, u, e, a, phi, h1, scal, p);
 }
 
-// Poisson apply (one CTA): mode 0 rhs b = -(n - mean n) charge, 1 matvec
+// Poisson apply (one CTA): mode 0 rhs b = -(n~ - mean n) charge, 1 matvec
 // (the stencil (a2, a1, a0, a1, a2) / den hx^-2 of the Laplacian), 2
-// function (matvec + (n - mean n) charge); optional ||y||^2 -> sumsq
-// (PETScPoissonSolver.pyx:58-74, PETScPoissonCFD4.pyx:64-101,
-// PETScPoissonCFD2.pyx:64-101, PETScPoissonSimpson.pyx:62-101)
+// function (matvec + (n~ - mean n) charge), n~ = rhs_density; optional
+// ||y||^2 -> sumsq (PETScPoissonSolver.pyx:58-74, PETScPoissonCFD4.pyx:64-101,
+// PETScPoissonCFD2.pyx:64-101, PETScPoissonSimpson.pyx:62-101,
+// PETScPoissonCFD2Ave.pyx, PETScPoissonSimpsonAve.pyx)
 __device__ __forceinline__ void poisson_apply_cta(const double* __restrict__ x, const double* __restrict__ n,
                                                   double* __restrict__ y, int nx, double hx2_inv, double charge,
                                                   int mode, double* __restrict__ sumsq, double a0, double a1,
-                                                  double a2, double den) {
+                                                  double a2, double den, int ravg, double ra0, double ra1,
+                                                  double ra2, double rden) {
     __shared__ double red[32];
     __shared__ double nmean_s;
     double t = 0.0;
@@ -718,12 +736,12 @@ __device__ __forceinline__ void poisson_apply_cta(const double* __restrict__ x, 
     for (int i = threadIdx.x; i < nx; i += blockDim.x) {
         double r;
         if (mode == 0) {
-            r = -(n[i] - nmean_s) * charge;
+            r = -(rhs_density(n, i, nx, ravg, ra0, ra1, ra2, rden) - nmean_s) * charge;
         } else {
             const int im2 = (i - 2 + 2 * nx) % nx, im1 = (i - 1 + nx) % nx;
             const int ip1 = (i + 1) % nx, ip2 = (i + 2) % nx;
             r = (a2 * x[im2] + a1 * x[im1] + a0 * x[i] + a1 * x[ip1] + a2 * x[ip2]) * hx2_inv / den;
-            if (mode == 2) r = r + (n[i] - nmean_s) * charge;
+            if (mode == 2) r = r + (rhs_density(n, i, nx, ravg, ra0, ra1, ra2, rden) - nmean_s) * charge;
         }
         if (y) y[i] = r;
         r2 += r * r;

@@ -367,8 +367,10 @@ class PETScVlasovSolver:
 # ---------------------------------------------------------------------------
 class PETScPoissonSolver:
     """Periodic Poisson solver of the chosen Laplacian: CFD4 (default,
-    PETScPoissonCFD4.pyx:18-183), CFD2 (PETScPoissonCFD2.pyx) or Simpson
-    (PETScPoissonSimpson.pyx)."""
+    PETScPoissonCFD4.pyx:18-183), CFD2 (PETScPoissonCFD2.pyx), Simpson
+    (PETScPoissonSimpson.pyx), or CFD2Ave / SimpsonAve (PETScPoissonCFD2Ave.pyx,
+    PETScPoissonSimpsonAve.pyx: those Laplacians with the density averaged
+    in the right-hand side)."""
 
     def __init__(self, dax, nx=None, hx=None, charge=-1.0, grid=None, laplace="cfd4"):
         grid = grid if grid is not None else dax
