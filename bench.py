@@ -60,9 +60,9 @@ def measured_peaks():
     return 6650.0, "fallback"
 
 
-def profiled_traffic():
-    """DRAM bytes per whole-table multi-dot launch from the committed ncu summary (or None)."""
-    p = os.path.join(ROOT, "profiles", "batch_mdot_traffic.json")
+def profiled_traffic(name):
+    """DRAM bytes per whole-table launch of a kernel from its committed ncu summary (or None)."""
+    p = os.path.join(ROOT, "profiles", name)
     if os.path.exists(p):
         with open(p) as fh:
             return json.load(fh).get("bytes_per_launch")
@@ -158,6 +158,7 @@ def run_gpu(args, rank, world):
     stream = torch.cuda.current_stream(dev)
     specs = specs_for(rank)
     cells = sum(s["nx"] * s["nv"] for s in specs)
+    mode_rows = sum((s["nx"] // 2 + 1) * s["nv"] for s in specs)   # complex unknowns of the tridiagonal stage
     mixed = W.sweep_runs(specs=specs, device=dev, precision="mixed")
     plain = W.sweep_runs(specs=specs, device=dev, precision="fp64")
     batch = Batch(mixed)
@@ -190,6 +191,7 @@ def run_gpu(args, rank, world):
     mdot_s = batch.time_kernel(0, it=MDOT_IT, reps=20)
     pc_s = batch.time_kernel(1, it=MDOT_IT, reps=10)
     jvp_s = batch.time_kernel(2, it=MDOT_IT, reps=20)
+    tri_s = batch.time_kernel(4, it=MDOT_IT, reps=10)
     # ---- e2e: host buffers through the public API, the same K steps again ----
     hosts = [torch.empty_like(r.fc, device="cpu").pin_memory() for r in mixed]
     for h, snap, r in zip(hosts, snapshot, mixed):
@@ -211,7 +213,8 @@ def run_gpu(args, rank, world):
     if world > 1:
         (t_value, t_plain, t_e2e), (total_cells,) = reduce_over_ranks([t_value, t_plain, t_e2e], [cells], dev)
     return dict(cells=cells, total_cells=total_cells, t_value=t_value, t_plain=t_plain, t_e2e=t_e2e, launches=launches, clocks=clocks,
-                picard=picard, gmres=gmres, fe_rel=fe_rel, mdot_s=mdot_s, pc_s=pc_s, jvp_s=jvp_s)
+                picard=picard, gmres=gmres, fe_rel=fe_rel, mdot_s=mdot_s, pc_s=pc_s, jvp_s=jvp_s, tri_s=tri_s,
+                mode_rows=mode_rows)
 
 
 def port_runs(specs):
@@ -324,12 +327,20 @@ def main():
     e2e = work / res["t_e2e"] / 1e9
     peak, peak_kind = measured_peaks()
     mdot_bytes = cells * (MDOT_IT + 2) * 4      # w and V_0..V_it read in FP32
-    achieved = mdot_bytes / res["mdot_s"] / 1e9
-    roofline = {"kernel": "k_b_gm_mdot_p<float> (Gram-Schmidt multi-dot, whole table, Arnoldi index %d)" % MDOT_IT,
+    # the tridiagonal stage: read the FP32 complex spectrum and the LU
+    # reciprocals, write the solution (3 x 8 B per mode and row)
+    tri_bytes = res["mode_rows"] * 24
+    achieved = tri_bytes / res["tri_s"] / 1e9
+    roofline = {"kernel": "tridiagonal stage of the preconditioner (the tuned batch kernel, whole table; "
+                          "the largest share of the step's launch list)",
                 "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                "peak_kind": peak_kind, "traffic": profiled_traffic(), "algorithmic_bytes_per_launch": mdot_bytes,
-                "avg_launch_us": res["mdot_s"] * 1e6,
-                "others": {"preconditioner_3_kernels_us": res["pc_s"] * 1e6,
+                "peak_kind": peak_kind, "traffic": profiled_traffic("batch_tridiag_traffic.json"),
+                "algorithmic_bytes_per_launch": tri_bytes, "avg_launch_us": res["tri_s"] * 1e6,
+                "others": {"multidot_us": res["mdot_s"] * 1e6,
+                           "multidot_achieved_GBps": mdot_bytes / res["mdot_s"] / 1e9,
+                           "multidot_frac": mdot_bytes / res["mdot_s"] / 1e9 / peak,
+                           "multidot_traffic": profiled_traffic("batch_mdot_traffic.json"),
+                           "preconditioner_3_kernels_us": res["pc_s"] * 1e6,
                            "preconditioner_achieved_GBps": cells * 24 / res["pc_s"] / 1e9,
                            "jacobian_stencil_us": res["jvp_s"] * 1e6,
                            "jacobian_achieved_GBps": cells * 8 / res["jvp_s"] / 1e9}}

@@ -2070,6 +2070,7 @@ struct vv_batch {
     int tri_kind;                // tridiagonal solves: 0 CTA per mode (tables staged), 1 warp per mode,
                                  // 2 CTA per mode (tables through L1)
     size_t smem_tri_stage, smem_tri_plain, smem_tri_warp;
+    size_t smem_tri_js;          // k_b_tridiagjs (padded warp slices)
     int nvmax;                   // largest velocity grid of the table
     int smem_limit;              // dynamic shared memory per block available to the batch kernels
     double* wpart;               // device: per-warp partial sums of every instance
@@ -2134,6 +2135,26 @@ int b_flag(vv_batch* b, int* out) {
     return VV_OK;
 }
 
+// the tridiagonal stage of P^-1 (the tuned kernel) on the spectra of the
+// instances in list L, in place
+template <typename T>
+int b_tri(vv_batch* b, const int* L) {
+    const vv::BInst* tab = b->tab;
+    if (b->pcj) {
+        if (b->tri_kind == 1)
+            return blaunch(b, vv::k_b_tridiagjs<T>, vv::F_MODES, 32 * vv::TRIW_WARPS, b->smem_tri_js, tab, L, b->n,
+                           vv::tri_ws_slots(b->nvmax));
+        return blaunch(b, vv::k_b_tridiagj<T>, vv::F_MODES, 32,
+                       (size_t)64 * vv::TJ_RING * sizeof(typename Cplx<T>::type), tab, L, b->n);
+    }
+    if (b->tri_kind == 1)
+        return blaunch(b, vv::k_b_tridiag_w<T>, vv::F_MODES, 32 * vv::TRIW_WARPS, b->smem_tri_warp, tab, L, b->n,
+                       vv::tri_ws_slots(b->nvmax));
+    if (b->tri_kind == 2)
+        return blaunch(b, vv::k_b_tridiag<T, false>, vv::F_MODES, vv::TRI_THREADS, b->smem_tri_plain, tab, L, b->n);
+    return blaunch(b, vv::k_b_tridiag<T, true>, vv::F_MODES, vv::TRI_THREADS, b->smem_tri_stage, tab, L, b->n);
+}
+
 // P^-1 of every instance in list l: input FP64 tmp (right-hand side) or the
 // GMRES-precision scratch; output b, V0 or V[it+1]
 template <typename T>
@@ -2144,12 +2165,7 @@ int b_pc(vv_batch* b, int l, bool from_tmp64, int dst) {
         const dim3 ft(vv::FJ_THREADS);
         if (from_tmp64) TRY(blaunch(b, vv::k_b_rfftj<double, T>, vv::F_ROWS, ft, b->smem_fftj, tab, L, b->n, 1));
         else TRY(blaunch(b, vv::k_b_rfftj<T, T>, vv::F_ROWS, ft, b->smem_fftj, tab, L, b->n, 0));
-        if (b->tri_kind == 1)
-            TRY(blaunch(b, vv::k_b_tridiagjs<T>, vv::F_MODES, 32 * vv::TRIW_WARPS, b->smem_tri_warp, tab, L, b->n,
-                        vv::tri_ws_slots(b->nvmax)));
-        else
-            TRY(blaunch(b, vv::k_b_tridiagj<T>, vv::F_MODES, 32,
-                        (size_t)64 * vv::TJ_RING * sizeof(typename Cplx<T>::type), tab, L, b->n));
+        TRY(b_tri<T>(b, L));
         return blaunch(b, vv::k_b_irfftj<T, T>, vv::F_ROWS, ft, b->smem_fftj, tab, L, b->n, dst);
     }
     const dim3 rt(32 * b->R);
@@ -2160,11 +2176,7 @@ int b_pc(vv_batch* b, int l, bool from_tmp64, int dst) {
         if (from_tmp64) TRY(blaunch(b, vv::k_b_rfft<double, T, false>, vv::F_ROWS, rt, b->smem_rfft, tab, L, b->n, 1));
         else TRY(blaunch(b, vv::k_b_rfft<T, T, false>, vv::F_ROWS, rt, b->smem_rfft, tab, L, b->n, 0));
     }
-    if (b->tri_kind == 1)
-        TRY(blaunch(b, vv::k_b_tridiag_w<T>, vv::F_MODES, 32 * vv::TRIW_WARPS, b->smem_tri_warp, tab, L, b->n,
-                    vv::tri_ws_slots(b->nvmax)));
-    else if (b->tri_kind == 2) TRY(blaunch(b, vv::k_b_tridiag<T, false>, vv::F_MODES, vv::TRI_THREADS, b->smem_tri_plain, tab, L, b->n));
-    else TRY(blaunch(b, vv::k_b_tridiag<T, true>, vv::F_MODES, vv::TRI_THREADS, b->smem_tri_stage, tab, L, b->n));
+    TRY(b_tri<T>(b, L));
     if (b->fft4) return blaunch(b, vv::k_b_irfft<T, T, true>, vv::F_ROWS, rt, b->smem_irfft, tab, L, b->n, dst);
     return blaunch(b, vv::k_b_irfft<T, T, false>, vv::F_ROWS, rt, b->smem_irfft, tab, L, b->n, dst);
 }
@@ -2477,7 +2489,7 @@ int b_autotune(vv_batch* b, std::vector<vv::BInst>& tab) {
     for (int pj = 0; pj <= (b->pcj_ok ? 1 : 0) && r == VV_OK; ++pj)
     for (int f4 = 0; f4 <= (pj ? 0 : 1) && r == VV_OK; ++f4)
     for (int tw = 0; tw <= (pj ? 1 : 2) && r == VV_OK; ++tw) {
-        if (tw == 1 && b->smem_tri_warp > (size_t)b->smem_limit) continue;
+        if (tw == 1 && (pj ? b->smem_tri_js : b->smem_tri_warp) > (size_t)b->smem_limit) continue;
         for (int R = 2; R <= (pj ? 2 : 8) && r == VV_OK; R *= 2) {
             b_shape(b, tab, R, tw, f4, pj);
             if ((r = b_apply_shape(b, tab)) != VV_OK) break;
@@ -2643,6 +2655,7 @@ int vv_batch_create(int n, vv_ctx* const* ctxs, const vv_state* states, vv_batch
             b->smem_tri_plain = std::max(b->smem_tri_plain, np * (b->mixed ? sizeof(float2) : sizeof(double2)));
             b->smem_tri_warp = std::max(b->smem_tri_warp, tri_ws_smem(c->nv, b->mixed ? sizeof(float2) : sizeof(double2)));
             b->nvmax = std::max(b->nvmax, c->nv);
+            b->smem_tri_js = vv::tri_js_smem(b->nvmax, b->mixed ? sizeof(float2) : sizeof(double2));
         }
         b->smem_pois = std::max(b->smem_pois, c->smem_pois);
     }
@@ -2724,7 +2737,7 @@ int vv_batch_create(int n, vv_ctx* const* ctxs, const vv_state* states, vv_batch
         const int nf = bs ? sscanf(bs, "%d,%d,%d,%d,%d", &fR, &fT, &fF, &fJ, &fM) : 0;
         const bool fixed = nf >= 3 && (fR == 2 || fR == 4 || fR == 8) && fT >= 0 && fT <= 2 && (fF == 0 || fF == 1) &&
                            (fJ == 0 || (fJ == 1 && b->pcj_ok)) &&
-                           !(fT == 1 && b->smem_tri_warp > (size_t)b->smem_limit);
+                           !(fT == 1 && (fJ ? b->smem_tri_js : b->smem_tri_warp) > (size_t)b->smem_limit);
         const char* at = getenv("VV_AUTOTUNE");
         if (fixed) {
             b->march = fM != 0;
@@ -2821,7 +2834,7 @@ int vv_batch_step(vv_batch* b, const vv_snes_opts* so, const vv_ksp_opts* ko, vv
 }
 
 int vv_batch_time_kernel(vv_batch* b, int which, int it, int reps, double* avg_ms) {
-    if (!b || !avg_ms || reps < 1 || which < 0 || which > 3 || it < 0) return VV_ERR_ARG;
+    if (!b || !avg_ms || reps < 1 || which < 0 || which > 4 || it < 0) return VV_ERR_ARG;
     for (int i = 0; i < b->n; ++i)
         if (it + 1 >= b->ctx[i]->restart + 1) return VV_ERR_ARG;   // V[it+1] must exist
     const int64_t l0 = b->launches;
@@ -2837,6 +2850,7 @@ int vv_batch_time_kernel(vv_batch* b, int which, int it, int reps, double* avg_m
                                 : blaunch(b, vv::k_b_gm_mdot_p<double>, vv::F_VEC, vv::RED_THREADS, 0, tab, L, b->n);
             case 1: return b->mixed ? b_pc<float>(b, vv::L_ALL, false, vv::BD_B) : b_pc<double>(b, vv::L_ALL, false, vv::BD_B);
             case 2: return b->mixed ? b_jvp_all<float>(b) : b_jvp_all<double>(b);   // the tuned stencil kernel
+            case 4: return b->mixed ? b_tri<float>(b, L) : b_tri<double>(b, L);     // the tuned tridiagonal stage
             default:
                 return b->mixed ? blaunch(b, vv::k_b_gm_maxpy_p<float>, vv::F_VEC, vv::RED_THREADS, 0, tab, L, b->n)
                                 : blaunch(b, vv::k_b_gm_maxpy_p<double>, vv::F_VEC, vv::RED_THREADS, 0, tab, L, b->n);

@@ -278,11 +278,21 @@ __global__ void __launch_bounds__(FJ_THREADS) k_b_irfftj(const BInst* __restrict
     });
 }
 
+// pad between the warps' slices of k_b_tridiagjs (complex slots)
+constexpr int TRIJS_PAD = 8;
+__host__ __device__ constexpr size_t tri_js_smem(int nvmax, size_t csz) {
+    return (size_t)TRIW_WARPS * (2 * tri_ws_slots(nvmax) + TRIJS_PAD) * csz + 2 * (size_t)tri_ws_slots(nvmax) * (csz / 2);
+}
+
 // LU solves on the v-major layout by the staged warp solve: TRIW_WARPS
 // consecutive modes per work item, one warp per mode; the CTA stages the
 // modes' columns together (a row's TRIW_WARPS values are one 32-byte sector
 // in FP32) into the warps' slices and writes the solutions back the same
-// way (dynamic smem as k_b_tridiag_w)
+// way.  The warps' slices are 2 ns + TRIJS_PAD complex apart: with 8-byte
+// elements a staging instruction writes 8 rows x TRIW_WARPS modes, and a
+// slice stride of 8 (mod 16) complex spreads the four modes of a row over
+// both halves of the banks (two wavefronts, the minimum) where a multiple of
+// 16 put them on one bank pair.  Dynamic smem: tri_js_smem.
 template <typename R>
 __global__ void __launch_bounds__(32 * TRIW_WARPS) k_b_tridiagjs(const BInst* __restrict__ tab, const int* __restrict__ L,
                                                                 int n, int nsmax) {
@@ -294,8 +304,9 @@ __global__ void __launch_bounds__(32 * TRIW_WARPS) k_b_tridiagjs(const BInst* __
         const int ns = tri_ws_slots(nv);
         const int w = threadIdx.x >> 5;
         const int k0 = local * TRIW_WARPS;
+        const int ws = 2 * ns + TRIJS_PAD;   // complex slots per warp slice
         C* base = reinterpret_cast<C*>(smem_raw);
-        R* sal = reinterpret_cast<R*>(base + (size_t)TRIW_WARPS * 2 * nsmax);
+        R* sal = reinterpret_cast<R*>(base + (size_t)TRIW_WARPS * (2 * nsmax + TRIJS_PAD));
         R* sga = sal + ns;
         C* spec = (C*)I.specT;
         const C* dj = (const C*)I.dinvJ;
@@ -304,7 +315,7 @@ __global__ void __launch_bounds__(32 * TRIW_WARPS) k_b_tridiagjs(const BInst* __
             const int j = t / TRIW_WARPS, m = t % TRIW_WARPS;
             const int k = k0 + m;
             if (k < nm) {
-                C* sb = base + (size_t)m * 2 * ns;
+                C* sb = base + (size_t)m * ws;
                 const int q = j + j / CH;
                 cp_async_elem(&sb[q], &spec[(size_t)j * nm + k]);
                 cp_async_elem(&sb[ns + q], &dj[(size_t)j * nm + k]);
@@ -314,14 +325,14 @@ __global__ void __launch_bounds__(32 * TRIW_WARPS) k_b_tridiagjs(const BInst* __
         cp_async_wait0();
         __syncthreads();
         if (k0 + w < nm) {
-            C* sb = base + (size_t)w * 2 * ns;
+            C* sb = base + (size_t)w * ws;
             tri_ws_solve<R>(sb, sb + ns, sal, sga, reinterpret_cast<const C*>(I.tp.lambda)[k0 + w], nv);
         }
         __syncthreads();
         for (int t = threadIdx.x; t < nv * TRIW_WARPS; t += blockDim.x) {
             const int j = t / TRIW_WARPS, m = t % TRIW_WARPS;
             const int k = k0 + m;
-            if (k < nm) spec[(size_t)j * nm + k] = base[(size_t)m * 2 * ns + j + j / CH];
+            if (k < nm) spec[(size_t)j * nm + k] = base[(size_t)m * ws + j + j / CH];
         }
     });
 }
