@@ -310,13 +310,14 @@ __global__ void __launch_bounds__(32 * TRIW_WARPS) k_b_tridiagjs(const BInst* __
         R* sga = sal + ns;
         C* spec = (C*)I.specT;
         const C* dj = (const C*)I.dinvJ;
+        const FastDiv dch((unsigned)CH);
         tri_ws_stage_tables<R>(I.tp, sal, sga);
         for (int t = threadIdx.x; t < nv * TRIW_WARPS; t += blockDim.x) {
             const int j = t / TRIW_WARPS, m = t % TRIW_WARPS;
             const int k = k0 + m;
             if (k < nm) {
                 C* sb = base + (size_t)m * ws;
-                const int q = j + j / CH;
+                const int q = j + (int)dch((unsigned)j);
                 cp_async_elem(&sb[q], &spec[(size_t)j * nm + k]);
                 cp_async_elem(&sb[ns + q], &dj[(size_t)j * nm + k]);
             }
@@ -332,7 +333,7 @@ __global__ void __launch_bounds__(32 * TRIW_WARPS) k_b_tridiagjs(const BInst* __
         for (int t = threadIdx.x; t < nv * TRIW_WARPS; t += blockDim.x) {
             const int j = t / TRIW_WARPS, m = t % TRIW_WARPS;
             const int k = k0 + m;
-            if (k < nm) spec[(size_t)j * nm + k] = base[(size_t)m * ws + j + j / CH];
+            if (k < nm) spec[(size_t)j * nm + k] = base[(size_t)m * ws + j + (int)dch((unsigned)j)];
         }
     });
 }

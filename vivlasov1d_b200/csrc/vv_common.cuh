@@ -6,6 +6,16 @@
 
 #define VV_DEV __device__ __forceinline__
 
+// n / d by one wide multiply with m = ceil(2^32 / d): floor(n m / 2^32)
+// equals floor(n / d) whenever n d < 2^32 (the excess n (m - 2^32/d) / 2^32
+// stays below 1/d).  For the pad-slot index r / CH of the staged tridiagonal
+// lines (r < nv, CH = ceil(nv / 32): exact for nv below 370,000).
+struct FastDiv {
+    unsigned long long m;
+    VV_DEV explicit FastDiv(unsigned d) : m((0xFFFFFFFFull + d) / d) {}
+    VV_DEV unsigned operator()(unsigned n) const { return (unsigned)(((unsigned long long)n * m) >> 32); }
+};
+
 VV_DEV double2 c_add(double2 a, double2 b) { return make_double2(a.x + b.x, a.y + b.y); }
 VV_DEV double2 c_sub(double2 a, double2 b) { return make_double2(a.x - b.x, a.y - b.y); }
 VV_DEV double2 c_mul(double2 a, double2 b) {

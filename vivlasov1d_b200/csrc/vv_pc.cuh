@@ -575,8 +575,9 @@ __device__ __forceinline__ void tridiag_mode(typename Cplx<R>::type* __restrict_
     const R* alpha_g = reinterpret_cast<const R*>(p.alpha);
     const R* gamma_g = reinterpret_cast<const R*>(p.gamma);
     const C lam = reinterpret_cast<const C*>(p.lambda)[k];
+    const FastDiv dch((unsigned)CH);
     for (int r = threadIdx.x; r < nv; r += TRI_THREADS) {   // every copy in flight at once
-        const int q = r + r / CH;
+        const int q = r + (int)dch((unsigned)r);
         cp_async_elem(&b[q], &line[r]);
         if (STAGE) {
             cp_async_elem(&di[q], &dinv_g[r]);
@@ -767,8 +768,9 @@ __device__ __forceinline__ void tri_ws_stage_tables(const TriParams& p, R* __res
     const int CH = (nv + 31) / 32;
     const R* al = reinterpret_cast<const R*>(p.alpha);
     const R* ga = reinterpret_cast<const R*>(p.gamma);
+    const FastDiv dch((unsigned)CH);
     for (int r = threadIdx.x; r < nv; r += blockDim.x) {
-        const int q = r + r / CH;
+        const int q = r + (int)dch((unsigned)r);
         cp_async_elem(&sal[q], &al[r]);
         cp_async_elem(&sga[q], &ga[r]);
     }
@@ -783,8 +785,9 @@ __device__ __forceinline__ void tri_ws_stage_line(const typename Cplx<R>::type* 
     const int CH = (nv + 31) / 32;
     const C* line = spec + (size_t)k * nv;
     const C* dg = reinterpret_cast<const C*>(p.dinv) + (size_t)k * nv;
+    const FastDiv dch((unsigned)CH);
     for (int r = lane; r < nv; r += 32) {   // every copy in flight at once
-        const int q = r + r / CH;
+        const int q = r + (int)dch((unsigned)r);
         cp_async_elem(&sb[q], &line[r]);
         cp_async_elem(&sd[q], &dg[r]);
     }
@@ -863,7 +866,8 @@ __device__ __forceinline__ void tridiag_warp_staged(typename Cplx<R>::type* __re
     C* line = spec + (size_t)k * nv;
     tri_ws_solve<R>(sb, sd, al, ga, reinterpret_cast<const C*>(p.lambda)[k], nv);
     __syncwarp();
-    for (int r = lane; r < nv; r += 32) line[r] = sb[r + r / CH];
+    const FastDiv dch((unsigned)CH);
+    for (int r = lane; r < nv; r += 32) line[r] = sb[r + (int)dch((unsigned)r)];
 }
 
 // dynamic smem: TRIW_WARPS x 2 x tri_ws_slots(nv) complex + 2 x tri_ws_slots(nv) real
