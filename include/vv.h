@@ -77,6 +77,12 @@ enum vv_averaging {          /* solver.averaging_operator: the time derivative
     VV_AVERAGING_ARAKAWA_J4 = 4,/* TimeDerivativeArakawaJ4 (:245-321)          */
     VV_AVERAGING_SIMPSON = 5    /* TimeDerivativeSimpson (:160-233)            */
 };
+enum vv_collision {          /* solver.collision_operator with dissipation_type
+                                = 'collisions' (CollisionOperator.pyx:44-58)  */
+    VV_COLLISION_NONE = 0,
+    VV_COLLISION_T = 1,      /* collT: CollisionOperator.pyx:68-157            */
+    VV_COLLISION_E = 2       /* collE: CollisionOperator.pyx:160-250           */
+};
 enum vv_order {              /* arithmetic of the bracket kernels             */
     VV_ORDER_FACTORED = 0,   /* separable-h coefficient form (fast, default)   */
     VV_ORDER_REFERENCE = 1   /* the reference loop's operation order, no FMA   */
@@ -119,6 +125,16 @@ typedef struct vv_grid {
                                 F times 1/(ht d); they are supported by the
                                 single-instance step, not by vv_batch_create
                                 or vv_step_adjoint (VV_ERR_UNSUPPORTED).      */
+    int32_t collision;       /* enum vv_collision (0: none); active only with
+                                coll_freq != 0, as config.py:148-154.  The
+                                residual and Jacobian then add the operator
+                                with the moments of vv_set_moments (vv_step:
+                                the state's n, u, a and their copies at
+                                make_history).  Single runs only: not in
+                                vv_batch_create or vv_step_adjoint.          */
+    double  coll_freq;       /* runspec coll_freq (collision frequency)       */
+    double  coll_diff;       /* runspec coll_diff (weight of diffusion, 1)    */
+    double  coll_drag;       /* runspec coll_drag (weight of drag, 1)         */
 } vv_grid;
 
 typedef struct vv_ctx vv_ctx;
@@ -172,6 +188,12 @@ int vv_pc_apply(vv_ctx* ctx, const double* X, double* Y);
  * The time step (vv_step) takes phi at its own make_history.  A no-op for the
  * other preconditioners. */
 int vv_pc_set_potential(vv_ctx* ctx, const double* phi);
+/* PETScVlasovSolver.set_moments (PETScVlasovSolver.pyx:123-132): the current
+ * (p) and history (h) moments the collision operator reads (device x
+ * profiles, copied; e unused by the operators).  No-op without collisions.
+ * vv_step takes the state's moments instead. */
+int vv_set_moments(vv_ctx* ctx, const double* n_p, const double* u_p, const double* e_p, const double* a_p,
+                   const double* n_h, const double* u_h, const double* e_h, const double* a_h);
 
 /* ---- Toolbox ------------------------------------------------------------ */
 /* compute_density / compute_velocity_density / compute_energy_density /

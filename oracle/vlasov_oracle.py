@@ -343,21 +343,71 @@ def time_derivative_add(x, y, grid, averaging="point"):
 
 
 # --------------------------------------------------------------------------
+# collision operators  (solvers/components/CollisionOperator.pyx)
+# --------------------------------------------------------------------------
+@dataclass
+class Collisions:
+    """``dissipation_type = 'collisions'``: operator 'collt' or 'colle'
+    (CollisionOperator.create, CollisionOperator.pyx:44-58; '' = none) and
+    the runspec's coll_freq / coll_diff / coll_drag."""
+    kind: str = ""
+    freq: float = 0.0
+    diff: float = 1.0
+    drag: float = 1.0
+
+
+def collision_add(f, y, grid, coll, n, U, a, factor):
+    """``y += factor C[f]`` in place on the rows 2 <= j < nv-2, with the
+    moments (n, U, a) frozen (CollisionOperator.pyx:72-110 collT,
+    :164-202 collE), in the loop body's operation order: u = U / n,
+
+      collT: ((v+ - u) f+ - (v- - u) f-) a drag_fac + (f+ - 2 f + f-) diff_fac
+      collE: ((v+ - u) f+ - (v- - u) f-) drag_fac + ((f+ - 2 f + f-) / a) diff_fac
+
+    drag_fac = -factor nu drag hv^-1 / 2, diff_fac = -factor nu diff hv^-2."""
+    if coll is None or coll.kind not in ("collt", "colle") or coll.freq == 0. or factor == 0.:
+        return y
+    drag_fac = - factor * coll.freq * coll.drag * grid.hv_inv * 0.5
+    diff_fac = - factor * coll.freq * coll.diff * grid.hv2_inv
+    nv = f.shape[1]
+    v = grid.v
+    u = (np.asarray(U) / np.asarray(n))[:, None]
+    a = np.asarray(a)[:, None]
+    fp, f0, fm = f[:, STENCIL + 1:nv - STENCIL + 1], f[:, STENCIL:nv - STENCIL], f[:, STENCIL - 1:nv - STENCIL - 1]
+    vp, vm = v[None, STENCIL + 1:nv - STENCIL + 1], v[None, STENCIL - 1:nv - STENCIL - 1]
+    if coll.kind == "collt":
+        drag = ((vp - u) * fp - (vm - u) * fm) * a
+        diff = (fp - 2. * f0 + fm)
+    else:
+        drag = (vp - u) * fp - (vm - u) * fm
+        diff = (fp - 2. * f0 + fm) / a
+    y[:, STENCIL:nv - STENCIL] += drag_fac * drag + diff_fac * diff
+    return y
+
+
+# --------------------------------------------------------------------------
 # residual and JVP  (solvers/vlasov/PETScNLVlasovMP.pyx:33-58)
 # --------------------------------------------------------------------------
-def residual(F, Fh, Have, grid, scheme="arakawaj4", averaging="point"):
-    """``R(F) = D_t (F - Fh) + [ (F+Fh)/2 , Have ]`` (PETScNLVlasovMP.pyx:43-58)."""
+def residual(F, Fh, Have, grid, scheme="arakawaj4", averaging="point", coll=None, mom_p=None, mom_h=None):
+    """``R(F) = D_t (F - Fh) + [ (F+Fh)/2 , Have ] + C_p[F]/2 + C_h[Fh]/2``
+    (PETScNLVlasovMP.pyx:43-58); mom_p / mom_h = (n, U, a) of the current
+    and the history moments (set_moments)."""
     Fave = 0.5 * Fh + 0.5 * F            # Fave.set(0); axpy(.5,Fh); axpy(.5,F)
     Fder = F - Fh                        # Fder.set(0); axpy(+1,F); axpy(-1,Fh)
     Y = time_derivative_add(Fder, np.zeros_like(F), grid, averaging)
     bracket_add(Fave, Have, Y, 1.0, grid, scheme)
+    if coll is not None and coll.kind:
+        collision_add(F, Y, grid, coll, *mom_p, 0.5)
+        collision_add(Fh, Y, grid, coll, *mom_h, 0.5)
     return Y
 
 
-def jvp(X, Have, grid, scheme="arakawaj4", averaging="point"):
-    """``J X = D_t X + 0.5 [X, Have]`` (PETScNLVlasovMP.pyx:33-40)."""
+def jvp(X, Have, grid, scheme="arakawaj4", averaging="point", coll=None, mom_p=None):
+    """``J X = D_t X + 0.5 [X, Have] + C_p[X]/2`` (PETScNLVlasovMP.pyx:33-40)."""
     Y = time_derivative_add(X, np.zeros_like(X), grid, averaging)
     bracket_add(X, Have, Y, 0.5, grid, scheme)
+    if coll is not None and coll.kind:
+        collision_add(X, Y, grid, coll, *mom_p, 0.5)
     return Y
 
 
@@ -729,11 +779,14 @@ def gmres(apply_A, b, rtol=1e-5, atol=1e-50, max_it=10000, restart=30,
 class VlasovSolver:
     """Restates ``PETScVlasovSolver`` for the nonlinear midpoint scheme."""
 
-    def __init__(self, grid, h0v, scheme="arakawaj4", preconditioner="tensor_kinetic", averaging="point"):
+    def __init__(self, grid, h0v, scheme="arakawaj4", preconditioner="tensor_kinetic", averaging="point",
+                 coll=None):
         self.grid = grid
         self.h0v = np.asarray(h0v, dtype=np.float64)
         self.scheme = scheme
         self.averaging = averaging_kind(averaging)   # PETScVlasovSolver.pyx:99
+        self.coll = coll                             # PETScVlasovSolver.pyx:102
+        self.mom_p = self.mom_h = None
         if preconditioner == "tensor_kinetic":
             self.pc = TensorKineticPreconditioner(grid)
         elif preconditioner == "tensor_potential":
@@ -751,11 +804,15 @@ class VlasovSolver:
     def update_previous(self, h1p, h1h, h2p=None, h2h=None):  # :142-157
         self.Have = have_field(self.h0v, h1p, h1h, h2p, h2h)
 
+    def set_moments(self, mom_p, mom_h):   # PETScVlasovSolver.pyx:123-132: (n, U, a) each
+        self.mom_p, self.mom_h = mom_p, mom_h
+
     def function_solver(self, F):          # PETScNLVlasovMP.pyx:43-58
-        return residual(F, self.Fh, self.Have, self.grid, self.scheme, self.averaging)
+        return residual(F, self.Fh, self.Have, self.grid, self.scheme, self.averaging, self.coll,
+                        self.mom_p, self.mom_h)
 
     def jacobian_solver(self, F):          # PETScNLVlasovMP.pyx:33-40
-        return jvp(F, self.Have, self.grid, self.scheme, self.averaging)
+        return jvp(F, self.Have, self.grid, self.scheme, self.averaging, self.coll, self.mom_p)
 
     def function(self, F):                 # PETScVlasovSolver.pyx:168-174
         Y = self.function_solver(F)
@@ -791,7 +848,7 @@ class Run:
     def __init__(self, grid, f0, scheme="arakawaj4", preconditioner="tensor_kinetic",
                  charge=-1.0, mass=1.0, ksp_rtol=1e-4, ksp_atol=1e-50,
                  ksp_max_it=1000, snes_atol=1e-10, snes_max_iter=20,
-                 normalise_f=True, laplace="cfd4", averaging="point"):
+                 normalise_f=True, laplace="cfd4", averaging="point", coll=None):
         self.grid = grid
         self.laplace = laplace
         self.charge = charge
@@ -800,7 +857,7 @@ class Run:
         self.snes_atol = snes_atol
         self.snes_max_iter = snes_max_iter
         self.h0v = kinetic_hamiltonian_v(grid, mass)
-        self.solver = VlasovSolver(grid, self.h0v, scheme, preconditioner, averaging)
+        self.solver = VlasovSolver(grid, self.h0v, scheme, preconditioner, averaging, coll)
         f = np.asarray(f0, dtype=np.float64)
         self.fc = normalise(f, grid) if normalise_f else f.copy()
         self.h2c = np.zeros(grid.nx)
@@ -808,12 +865,16 @@ class Run:
         self.calculate_moments()
         self.fh = self.fc.copy()
         self.h1h = self.h1c.copy()
+        self.mom_h = (self.n, self.u, self.a)
+        self.solver.set_moments((self.n, self.u, self.a), self.mom_h)
         self.reports = []
 
     def calculate_moments(self):           # run_base.py:640-655
         self.n, self.u, self.e, self.a = moments(self.fc, self.grid)
         self.phi = poisson_solve(self.n, self.grid, self.charge, self.laplace)
         self.h1c = potential_to_hamiltonian(self.phi)
+        if hasattr(self, "mom_h"):          # the solver holds the current moment vectors
+            self.solver.set_moments((self.n, self.u, self.a), self.mom_h)
 
     def calculate_residual(self):          # run_base.py:631-637
         fnorm = self.solver.function_norm(self.fc)
@@ -824,6 +885,8 @@ class Run:
         self.fh = self.fc.copy()
         self.h1h = self.h1c.copy()
         self.h2h = self.h2c.copy()
+        self.mom_h = (self.n.copy(), self.u.copy(), self.a.copy())   # nc -> nh, uc -> uh, ac -> ah
+        self.solver.set_moments((self.n, self.u, self.a), self.mom_h)
         self.solver.update_history(self.fc, self.phi)
 
     def update_previous(self):

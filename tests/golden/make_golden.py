@@ -323,9 +323,10 @@ PETSc = types.SimpleNamespace(InsertMode=InsertMode, Scatter=_Scatter,
 
 
 class Config:
-    def __init__(self, bracket, averaging="point"):
+    def __init__(self, bracket, averaging="point", collision=""):
         self.bracket = bracket
         self.averaging = averaging
+        self.collision = collision
 
     def get_averaging_operator(self):
         return self.averaging
@@ -337,7 +338,7 @@ class Config:
         return ""
 
     def get_collision_operator(self):
-        return ""
+        return self.collision
 
     def get_preconditioner(self):
         return ""
@@ -485,6 +486,36 @@ def make_case(ns, nx, nv, L, vmin, vmax, ht, seed):
             Y2 = da1.createGlobalVec()
             solver.jacobian(Fv, Y2)
             out["jvp_%s_avg_%s" % (scheme, avg)] = vec_to_2d(Y2, nx, nv)
+
+    # collision operators (CollisionOperator.pyx:72-110, :164-202) in the J4
+    # residual and Jacobian, moments frozen by set_moments (PETScVlasovSolver.pyx:123-132)
+    Fp, Fhp = np.abs(F) + 0.1, np.abs(Fh) + 0.1
+    mom = []
+    for fld in (Fp, Fhp):
+        Nv, Uv, Ev, Av = (dax.createGlobalVec() for _ in range(4))
+        fv = to_vec(fld)
+        tb.compute_density(fv, Nv)
+        tb.compute_velocity_density(fv, Uv)
+        tb.compute_energy_density(fv, Ev)
+        tb.compute_collision_factor(Nv, Uv, Ev, Av)
+        mom.append((Nv, Uv, Ev, Av))
+    out["coll_Fh_pos"] = Fhp
+    for k, (Nv, Uv, Ev, Av) in zip(("p", "h"), mom):
+        out["coll_n_" + k], out["coll_u_" + k] = Nv.a.copy(), Uv.a.copy()
+        out["coll_e_" + k], out["coll_a_" + k] = Ev.a.copy(), Av.a.copy()
+    for kind in ("collt", "colle"):
+        solver = ns["PETScVlasovSolver"](Config("arakawaj4", "point", kind), da1, dax, grid, H0, H1p, H1h, H2, H2, P,
+                                         coll_freq=0.3, coll_diff=0.7, coll_drag=1.3)
+        solver.set_moments(*mom[0], *mom[1])
+        Fv = to_vec(F)
+        solver.update_history(to_vec(Fh))
+        solver.update_previous(Fv)
+        Y = da1.createGlobalVec()
+        solver.function(Fv, Y)
+        out["residual_" + kind] = vec_to_2d(Y, nx, nv)
+        Y2 = da1.createGlobalVec()
+        solver.jacobian(Fv, Y2)
+        out["jvp_" + kind] = vec_to_2d(Y2, nx, nv)
 
     # moments (Toolbox.pyx:79-165)
     N, U, E, A = (dax.createGlobalVec() for _ in range(4))

@@ -61,7 +61,19 @@ def test_averaging_operator_names():
     for bad in ("arakawaj1", "arakawaj4", "trapezoid"):
         with pytest.raises(ValueError):
             _lib.averaging_code(bad)
-    assert [f[0] for f in _lib.vv_grid._fields_][-1] == "averaging"
+
+
+def test_grid_struct_mirrors_header():
+    """The ctypes vv_grid has the header's fields in the header's order."""
+    import re
+    from vivlasov1d_b200 import _lib
+    src = open(os.path.join(os.path.dirname(__file__), "..", "include", "vv.h")).read()
+    body = src[src.index("typedef struct vv_grid {"):src.index("} vv_grid;")]
+    body = re.sub(r"/\*.*?\*/", "", body, flags=re.S)
+    names = []
+    for decl in re.findall(r"(?:int32_t|double)\s+([^;]+);", body):
+        names += [n.strip() for n in decl.split(",")]
+    assert names == [f[0] for f in _lib.vv_grid._fields_]
 
 
 def test_product_does_not_import_oracle():

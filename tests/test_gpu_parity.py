@@ -937,3 +937,149 @@ def test_averaged_batch_and_adjoint_unsupported():
     with pytest.raises(_lib.VVError) as e:
         Adjoint(run).step(run.fc.clone(), f, torch.ones_like(f))
     assert e.value.status == _lib.VV_ERR_UNSUPPORTED
+
+
+# ---------------------------------------------------------------------------
+# collision operators (dissipation_type = 'collisions')
+# ---------------------------------------------------------------------------
+COLL = dict(coll_freq=0.3, coll_diff=0.7, coll_drag=1.3)
+
+
+def make_coll_solver(grid, kind, order, g):
+    from vivlasov1d_b200 import PETScVlasovSolver
+    cfg = {"poisson_bracket": "arakawaj4", "preconditioner": "", "collision_operator": kind}
+    s = PETScVlasovSolver(cfg, None, None, grid, None, xdev(g["h1p"][:, 0]), xdev(g["h1h"][:, 0]), None, None,
+                          None, order=order, **COLL)
+    s.set_moments(*[xdev(g["coll_%s_%s" % (m, k)]) for k in ("p", "h") for m in ("n", "u", "e", "a")])
+    return s
+
+
+@pytest.mark.parametrize("path", GOLDEN, ids=[os.path.basename(p) for p in GOLDEN])
+@pytest.mark.parametrize("kind", ["collt", "colle"])
+def test_collision_residual_jvp_golden(path, kind):
+    """The collision operator after the bracket, moments frozen by
+    set_moments, against the vectors of the reference's own classes:
+    bit-exact in the reference order, 1e-12 relative in the factored order."""
+    g = dict(np.load(path))
+    grid = ggrid(g)
+    for order in ("reference", "factored"):
+        s = make_coll_solver(grid, kind, order, g)
+        F, Fh = dev(g["F"]), dev(g["Fh"])
+        s.update_history(Fh)
+        s.update_previous(F)
+        Y = grid.field()
+        s.function_solver(F, Y)
+        r = host(Y)
+        s.jacobian_solver(F, Y)
+        j = host(Y)
+        if order == "reference":
+            assert np.array_equal(r, g["residual_" + kind])
+            assert np.array_equal(j, g["jvp_" + kind])
+        else:
+            assert rel(r, g["residual_" + kind]) < 1e-12
+            assert rel(j, g["jvp_" + kind]) < 1e-12
+        n = s.function_norm(F, Y)
+        ref = float(np.sqrt((g["residual_" + kind] ** 2).sum()))
+        assert abs(n - ref) <= 1e-12 * ref
+
+
+@pytest.mark.parametrize("kind", ["collt", "colle"])
+def test_collision_jvp_wide_tiles(monkeypatch, kind):
+    """nx a multiple of 64: the Jacobian's bracket in the wide tiles followed
+    by the collision kernel, and the residual (narrow tiles, partial sums
+    from the collision kernel), against the oracle to 1e-12."""
+    from vivlasov1d_b200 import Grid
+    monkeypatch.setenv("VV_AUTOTUNE", "0")
+    nx, nv = 128, 96
+    og = vo.Grid(nx, nv, 4 * np.pi, 8.0, -8.0, ht=0.05)
+    rng = np.random.default_rng(11)
+    F = rng.normal(size=(nx, nv))
+    Fh = F + 0.01 * rng.normal(size=(nx, nv))
+    h1p, h1h = 0.1 * rng.normal(size=nx), 0.1 * rng.normal(size=nx)
+    fp = np.abs(F) + 0.1
+    mom_p = vo.moments(fp, og)
+    mom_h = vo.moments(np.abs(Fh) + 0.1, og)
+    grid = Grid(nx, nv, 4 * np.pi, 8.0, -8.0, ht=0.05)
+    g = {"h1p": np.repeat(h1p[:, None], nv, 1), "h1h": np.repeat(h1h[:, None], nv, 1)}
+    for k, mom in (("p", mom_p), ("h", mom_h)):
+        for name, arr in zip(("n", "u", "e", "a"), mom):
+            g["coll_%s_%s" % (name, k)] = arr
+    s = make_coll_solver(grid, kind, "factored", g)
+    s.update_history(dev(Fh))
+    s.update_previous(dev(F))
+    H = vo.have_field(vo.kinetic_hamiltonian_v(og), h1p, h1h)
+    coll = vo.Collisions(kind, **{k.replace("coll_", ""): v for k, v in COLL.items()})
+    mp, mh = (mom_p[0], mom_p[1], mom_p[3]), (mom_h[0], mom_h[1], mom_h[3])
+    Y = grid.field()
+    s.jacobian_solver(dev(F), Y)
+    assert rel(host(Y), vo.jvp(F, H, og, "arakawaj4", "point", coll, mp)) < 1e-12
+    s.function_solver(dev(F), Y)
+    ref = vo.residual(F, Fh, H, og, "arakawaj4", "point", coll, mp, mh)
+    assert rel(host(Y), ref) < 1e-12
+    assert abs(s.function_norm(dev(F), Y) - np.sqrt((ref ** 2).sum())) <= 1e-12 * np.sqrt((ref ** 2).sum())
+
+
+def _coll_cfg(nx, nv, kind, freq=0.05, **solver):
+    cfg = _example_cfg(nx, nv, **solver)
+    cfg["solver"].update({"dissipation_type": "collisions", "collision_operator": kind, "coll_freq": freq,
+                          "coll_diff": 1.0, "coll_drag": 1.0})
+    return cfg
+
+
+@pytest.mark.parametrize("kind", ["collT", "collE"])
+@pytest.mark.parametrize("order", ["factored", "reference"])
+def test_collision_step_matches_oracle(kind, order):
+    """Two implicit steps with dissipation_type = 'collisions' (the state's
+    moments in the Jacobian and residual, their copies at make_history as
+    the history moments) against the oracle's steps: same Picard counts, f
+    to 1e-10."""
+    from vivlasov1d_b200.run import Run
+    nx, nv = 64, 128
+    og = vo.Grid(nx, nv, 4 * np.pi, 10.0, -10.0, ht=0.1)
+    f0 = vo.initialise_distribution_function(og, vo.f0_landau(0.2))
+    run = Run(_coll_cfg(nx, nv, kind), f0=torch.from_numpy(vo.to_flat(f0)), order=order)
+    orun = vo.Run(og, f0, ksp_rtol=1e-10, snes_atol=1e-12, coll=vo.Collisions(kind.lower(), 0.05, 1.0, 1.0))
+    for _ in range(2):
+        rep = run.step()
+        orep = orun.step()
+        assert rep["picard_its"] == orep.picard_its, (rep, orep.picard_its)
+    assert rel(host(run.fc), orun.fc) < 1e-10
+    # the collisions act: the run differs from the collisionless one
+    orun0 = vo.Run(og, f0, ksp_rtol=1e-10, snes_atol=1e-12)
+    orun0.step(); orun0.step()
+    assert rel(orun.fc, orun0.fc) > 1e-6
+
+
+def test_collision_mixed_precision_field_energy():
+    """Mixed precision with collT (FP32 collision term in the Jacobian):
+    field energy within 1e-9 of the FP64 run after three steps."""
+    from vivlasov1d_b200.run import Run
+    og = vo.Grid(128, 128, 4 * np.pi, 10.0, -10.0, ht=0.1)
+    f0 = torch.from_numpy(vo.to_flat(vo.initialise_distribution_function(og, vo.f0_landau(0.2))))
+    cfg = _coll_cfg(128, 128, "collT", petsc_ksp_rtol=1e-4)
+    r64 = Run(cfg, f0=f0)
+    r32 = Run(cfg, f0=f0, precision="mixed")
+    for _ in range(3):
+        assert r64.step()["ksp_failures"] == 0
+        assert r32.step()["ksp_failures"] == 0
+    a, b = r32.invariants()["field_energy"], r64.invariants()["field_energy"]
+    assert abs(a - b) <= 1e-9 * abs(b)
+
+
+def test_collision_batch_and_adjoint_unsupported():
+    """The batch table and the discrete adjoint refuse a collisional context."""
+    from vivlasov1d_b200 import _lib
+    from vivlasov1d_b200.run import Run
+    from vivlasov1d_b200.batch import Batch
+    from vivlasov1d_b200.adjoint import Adjoint
+    og = vo.Grid(64, 64, 4 * np.pi, 10.0, -10.0, ht=0.1)
+    f0 = torch.from_numpy(vo.to_flat(vo.initialise_distribution_function(og, vo.f0_landau(0.1))))
+    run = Run(_coll_cfg(64, 64, "collT"), f0=f0)
+    with pytest.raises(_lib.VVError) as e:
+        Batch([run])
+    assert e.value.status == _lib.VV_ERR_UNSUPPORTED
+    f = run.fc.clone()
+    run.step()
+    with pytest.raises(_lib.VVError) as e:
+        Adjoint(run).step(run.fc.clone(), f, torch.ones_like(f))
+    assert e.value.status == _lib.VV_ERR_UNSUPPORTED

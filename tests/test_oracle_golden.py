@@ -79,6 +79,22 @@ def test_averaged_time_derivative_bitexact(golden, scheme, avg):
     assert np.max(np.abs(d[:, 2:-2])) > 0
 
 
+@pytest.mark.parametrize("kind", ["collt", "colle"])
+def test_collision_operator_bitexact(golden, kind):
+    """The collision operators (CollisionOperator.pyx) in the J4 residual and
+    Jacobian with frozen current / history moments, against the vectors of
+    the reference's own classes -> identical bits."""
+    g = _grid(golden)
+    coll = vo.Collisions(kind, 0.3, 0.7, 1.3)
+    mp = (golden["coll_n_p"], golden["coll_u_p"], golden["coll_a_p"])
+    mh = (golden["coll_n_h"], golden["coll_u_h"], golden["coll_a_h"])
+    F, Fh, H = golden["F"], golden["Fh"], golden["Have"]
+    assert np.array_equal(vo.residual(F, Fh, H, g, "arakawaj4", "point", coll, mp, mh), golden["residual_" + kind])
+    assert np.array_equal(vo.jvp(F, H, g, "arakawaj4", "point", coll, mp), golden["jvp_" + kind])
+    # the terms are there: the collisional vectors differ from the plain ones
+    assert np.max(np.abs(golden["jvp_" + kind] - golden["jvp_arakawaj4"])) > 1e-3
+
+
 def test_averaging_operator_names():
     """TimeDerivative.create's names (TimeDerivative.pyx:36-53): the J1 class
     is the midpoint stencil, the J2 class the point derivative; unknown names

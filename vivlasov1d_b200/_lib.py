@@ -20,6 +20,8 @@ NOALLOC_MAX_NX = 16384      # VV_NOALLOC_MAX_NX: largest nx of vv_invariants_noa
 BRACKET = {"arakawaj1": 1, "arakawaj2": 2, "arakawaj4": 4, "simpson": 5}
 PC_NONE, PC_TENSOR_KINETIC, PC_TENSOR_POTENTIAL = 0, 1, 2
 LAPLACE = {"cfd2": 2, "cfd4": 4, "simpson": 5, "cfd2ave": 12, "simpsonave": 15}
+# the collision operator by the names CollisionOperator.create knows (CollisionOperator.pyx:44-58)
+COLLISION = {"": 0, "collt": 1, "colle": 2}
 # the time derivative by the names TimeDerivative.create knows (TimeDerivative.pyx:36-53)
 AVERAGING = {"point": 0, "midpoint": 1, "arakawa_J1": 1, "arakawa_J2": 2, "arakawa_J4": 4, "simpson": 5}
 
@@ -54,7 +56,8 @@ class vv_grid(C.Structure):
                 ("vmax", C.c_double), ("ht", C.c_double), ("charge", C.c_double), ("mass", C.c_double),
                 ("bracket", C.c_int32), ("preconditioner", C.c_int32), ("laplace", C.c_int32),
                 ("order", C.c_int32), ("gmres_restart", C.c_int32), ("precision", C.c_int32),
-                ("mixed_rtol", C.c_double), ("averaging", C.c_int32)]
+                ("mixed_rtol", C.c_double), ("averaging", C.c_int32), ("collision", C.c_int32),
+                ("coll_freq", C.c_double), ("coll_diff", C.c_double), ("coll_drag", C.c_double)]
 
 
 class vv_ksp_opts(C.Structure):
@@ -111,6 +114,7 @@ SIGNATURES = {
     "vv_bracket": (I, [P, P, P, D]),
     "vv_pc_apply": (I, [P, P, P]),
     "vv_pc_set_potential": (I, [P, P]),
+    "vv_set_moments": (I, [P, P, P, P, P, P, P, P, P]),
     "vv_moments": (I, [P, P, P, P, P, P]),
     "vv_potential_to_hamiltonian": (I, [P, P, P]),
     "vv_poisson_rhs": (I, [P, P, P]),

@@ -121,8 +121,20 @@ class Config(dict):
         d = self["solver"]["dissipation_type"]
         return d is None or self["solver"]["coll_freq"] == 0. or d.lower() == "none"
 
-    def get_collision_operator(self):
-        return ""
+    def is_dissipation_collisions(self):        # config.py:135-139
+        d = self["solver"]["dissipation_type"]
+        return not (d is None or self["solver"]["coll_freq"] == 0.) and d.lower() == "collisions"
 
-    def get_double_bracket(self):
-        return ""
+    def is_dissipation_double_bracket(self):    # config.py:141-145
+        d = self["solver"]["dissipation_type"]
+        return not (d is None or self["solver"]["coll_freq"] == 0.) and d.lower() == "double_bracket"
+
+    def get_collision_operator(self):           # config.py:148-154
+        if not self.is_dissipation_collisions():
+            return ""
+        return (self["solver"]["collision_operator"] or "").lower()
+
+    def get_double_bracket(self):               # config.py:156-162
+        if not self.is_dissipation_double_bracket():
+            return ""
+        return (self["solver"]["bracket_operator"] or "").lower()

@@ -15,6 +15,7 @@
 #include "vv_batch.cuh"
 #include "vv_adjoint.cuh"
 #include "vv_pcv.cuh"
+#include "vv_coll.cuh"
 
 #include <algorithm>
 #include <array>
@@ -39,6 +40,14 @@ struct vv_ctx {
     double ravg[4];  // the right-hand side's density average: r0, r1, r2, denominator
     int avg;         // the time derivative (vv::AvgKind; arakawa_J2 -> point)
     double tfac;     // ht_inv / divisor of the averaging stencil
+    // collisions (vv::CollKind; none unless dissipation 'collisions' with
+    // coll_freq != 0): the factors for the midpoint weight 1/2, the current
+    // moments in use (the state's inside vv_step, mom_p after vv_set_moments)
+    // and the history moments (mom_h, copied at make_history); n, U, a each
+    int coll;
+    double coll_drag_fac, coll_diff_fac;
+    vv::CollMoments coll_p, coll_h;
+    double *mom_p, *mom_h;
     // the potential preconditioner (VV_PC_TENSOR_POTENTIAL): v modes, eigenvalues
     // for n = nv, nv twiddles, transposed field, v spectrum, elimination
     // scratch (FP32 copies in the mixed mode), rows per CTA of the v FFT, phi
@@ -225,11 +234,12 @@ int drain_timing(vv_ctx* c) {
 // ---- bracket launches -------------------------------------------------------
 bool aligned16(const void* p) { return p == nullptr || ((uintptr_t)p & 15u) == 0; }
 
-// the wide tiles; with an averaged time derivative only for the Jacobian
-// (the residual, Xh != null, stages F - Fh in the narrow tiles)
+// the wide tiles; with an averaged time derivative or collisions only for
+// the Jacobian (the residual, Xh != null, stages F - Fh in the narrow tiles,
+// or takes its partial sums from the collision kernel's narrow tiling)
 bool wide_ok(const vv_ctx* c, const void* X, const void* Xh, const void* Y) {
     return !c->narrow_bracket && c->nx % vv::WX == 0 && aligned16(X) && aligned16(Xh) && aligned16(Y) &&
-           !(c->avg != vv::AVG_POINT && Xh != nullptr);
+           !((c->avg != vv::AVG_POINT || c->coll != vv::COLL_NONE) && Xh != nullptr);
 }
 
 // the marching Jacobian stencil: about two waves of CTAs, segments of whole chunks
@@ -320,8 +330,7 @@ int launch_bracket_avg(vv_ctx* c, const T* X, const T* Xh, T* Y, double factor, 
 
 // MODE_ADD (the bare bracket) has no time derivative
 template <int MODE, typename T>
-int launch_bracket(vv_ctx* c, const T* X, const T* Xh, T* Y, double factor, double* sumsq,
-                   const int* xidx = nullptr) {
+int launch_bracket_td(vv_ctx* c, const T* X, const T* Xh, T* Y, double factor, double* sumsq, const int* xidx) {
     if constexpr (MODE != vv::MODE_ADD) {
         switch (c->avg) {
             case vv::AVG_MIDPOINT:
@@ -333,6 +342,38 @@ int launch_bracket(vv_ctx* c, const T* X, const T* Xh, T* Y, double factor, doub
         }
     }
     return launch_bracket_avg<MODE, T, vv::AVG_POINT>(c, X, Xh, Y, factor, sumsq, xidx);
+}
+
+// Y += C_p[X] (+ C_h[Xh]) after the bracket, per-tile sums of squares of Y on
+// the narrow tiling (PETScNLVlasovMP.pyx:33-58 adds the collision operator
+// after the bracket; CollisionOperator.pyx:72-110, :164-202)
+template <typename T>
+int launch_collision(vv_ctx* c, const T* X, const T* Xh, T* Y, double* sumsq, const int* xidx) {
+    vv::CollParams p;
+    p.nx = c->nx;
+    p.nv = c->nv;
+    p.kind = c->coll;
+    p.drag_fac = c->coll_drag_fac;
+    p.diff_fac = c->coll_diff_fac;
+    p.v = c->v;
+    p.xidx = xidx;
+    p.xstride = xidx ? c->ncell : 0;
+    dim3 grid((c->nx + vv::BX - 1) / vv::BX, (c->nv + vv::BY - 1) / vv::BY);
+    vv::k_collision<T><<<grid, dim3(vv::BX, vv::TY), 0, c->st>>>(X, Xh, Y, p, c->coll_p, c->coll_h, sumsq);
+    CKL(c);
+    return VV_OK;
+}
+
+// the residual (MODE_RESIDUAL) or Jacobian (MODE_JVP) of the chosen
+// discretisation, or the bare bracket (MODE_ADD); with collisions the
+// residual's partial sums come from the collision kernel
+template <int MODE, typename T>
+int launch_bracket(vv_ctx* c, const T* X, const T* Xh, T* Y, double factor, double* sumsq,
+                   const int* xidx = nullptr) {
+    const bool coll = MODE != vv::MODE_ADD && c->coll != vv::COLL_NONE;
+    TRY(launch_bracket_td<MODE, T>(c, X, Xh, Y, factor, coll ? nullptr : sumsq, xidx));
+    if (coll) return launch_collision<T>(c, X, MODE == vv::MODE_RESIDUAL ? Xh : nullptr, Y, sumsq, xidx);
+    return VV_OK;
 }
 
 // number of per-CTA partials a bracket launch writes for these operands
@@ -1049,6 +1090,12 @@ int step_prologue(vv_ctx* c, vv_state* st) {
     TRY(copy_d(c, c->Fh, st->f, n));
     // update_history -> update_matrices of the potential preconditioner
     if (c->g.preconditioner == VV_PC_TENSOR_POTENTIAL) TRY(copy_d(c, c->phipc, st->phi, nx));
+    // nc -> nh, uc -> uh, ac -> ah (run_base.py:757-760) for the collision operator
+    if (c->coll != vv::COLL_NONE) {
+        TRY(copy_d(c, c->mom_h, st->n, nx));
+        TRY(copy_d(c, c->mom_h + nx, st->u, nx));
+        TRY(copy_d(c, c->mom_h + 2 * nx, st->a, nx));
+    }
     TRY(set_hxp(c, st->h1c, st->h1h, st->h2c, st->h2h));
     return step_residual(c, st, 0);
 }
@@ -1365,6 +1412,8 @@ int vv_create(const vv_grid* grid, vv_ctx** out) {
         g.averaging != VV_AVERAGING_ARAKAWA_J2 && g.averaging != VV_AVERAGING_ARAKAWA_J4 &&
         g.averaging != VV_AVERAGING_SIMPSON)
         return VV_ERR_ARG;
+    if (g.collision != VV_COLLISION_NONE && g.collision != VV_COLLISION_T && g.collision != VV_COLLISION_E)
+        return VV_ERR_ARG;
     const int restart = g.gmres_restart > 0 ? g.gmres_restart : 30;
     if (restart > vv::MAX_RESTART) return VV_ERR_ARG;
     if (g.precision != VV_PRECISION_FP64 && g.precision != VV_PRECISION_MIXED) return VV_ERR_ARG;
@@ -1400,6 +1449,13 @@ int vv_create(const vv_grid* grid, vv_ctx** out) {
              : g.averaging == VV_AVERAGING_ARAKAWA_J4 ? vv::AVG_J4
                                                       : vv::AVG_POINT;
     c->tfac = c->ht_inv / vv::avg_divisor(c->avg);
+    // collisions (CollisionOperator.create, config.py:148-154: none unless coll_freq != 0);
+    // the factors of the midpoint rule's 1/2 in CollisionOperator.pyx:80-81's order
+    c->coll = (g.collision != VV_COLLISION_NONE && g.coll_freq != 0.0)
+                  ? (g.collision == VV_COLLISION_T ? vv::COLL_T : vv::COLL_E)
+                  : vv::COLL_NONE;
+    c->coll_drag_fac = -0.5 * g.coll_freq * g.coll_drag * c->hv_inv * 0.5;
+    c->coll_diff_fac = -0.5 * g.coll_freq * g.coll_diff * (1. / (c->hv * c->hv));
     {   // the Laplacian's stencil (matrix_mult of PETScPoissonCFD2/CFD4/Simpson.pyx; the Ave classes
         // keep CFD2's / Simpson's) and the density average of their formRHS (PETScPoissonCFD2Ave.pyx:
         // 0.25 (n_{i-1} + 2 n_i + n_{i+1}); PETScPoissonSimpsonAve.pyx: (n_{i-2} + 8 n_{i-1} + 18 n_i
@@ -1621,6 +1677,20 @@ int vv_create(const vv_grid* grid, vv_ctx** out) {
             return fail_cuda(cudaGetLastError(), "vv_create upload (potential preconditioner)");
         }
     }
+    // collisions: current / history moment profiles (n, U, a)
+    if (c->coll != vv::COLL_NONE) {
+        if ((s = dalloc(&c->mom_p, (size_t)3 * nx)) || (s = dalloc(&c->mom_h, (size_t)3 * nx))) {
+            vv_destroy(c);
+            return s;
+        }
+        c->coll_p = {c->mom_p, c->mom_p + nx, c->mom_p + 2 * nx};
+        c->coll_h = {c->mom_h, c->mom_h + nx, c->mom_h + 2 * nx};
+        if (cudaMemset(c->mom_p, 0, 3 * nx * sizeof(double)) != cudaSuccess ||
+            cudaMemset(c->mom_h, 0, 3 * nx * sizeof(double)) != cudaSuccess) {
+            vv_destroy(c);
+            return fail_cuda(cudaGetLastError(), "vv_create upload (collision moments)");
+        }
+    }
     // dynamic shared memory limits (process-wide, raised once per device)
     {
         int limit = 0;
@@ -1666,7 +1736,8 @@ int vv_destroy(vv_ctx* c) {
                     c->sym_inv, c->ds, c->V32, c->tmp32, c->bvec32, c->delta32, c->alpha32, c->gamma32,
                     c->spec32, c->tw32, c->lambda32, c->dinv32, c->adj_cH, c->adj_cF, c->adj_zpart,
                     c->adj_zbuf, c->adj_q, c->adj_hprof, c->adj_h1a, c->adj_h1b, c->lamv, c->twv, c->pv_spec,
-                    c->pv_scr, c->pv_xt, c->phipc, c->twv32, c->pv_spec32, c->pv_scr32, c->pv_xt32};
+                    c->pv_scr, c->pv_xt, c->phipc, c->twv32, c->pv_spec32, c->pv_scr32, c->pv_xt32,
+                    c->mom_p, c->mom_h};
     destroy_graph(c);
     for (int k = 0; k < 4; ++k)
         if (c->cs[k]) cudaStreamDestroy(c->cs[k]);
@@ -1733,6 +1804,23 @@ int vv_pc_apply(vv_ctx* c, const double* X, double* Y) {
     if (!c || !X || !Y) return VV_ERR_ARG;
     if (c->g.preconditioner == VV_PC_NONE) return copy_d(c, Y, X, c->ncell);
     return pc_apply(c, X, Y);
+}
+
+int vv_set_moments(vv_ctx* c, const double* n_p, const double* u_p, const double* e_p, const double* a_p,
+                   const double* n_h, const double* u_h, const double* e_h, const double* a_h) {
+    (void)e_p;
+    (void)e_h;   // the collision operators read n, U and a only
+    if (!c || !n_p || !u_p || !a_p || !n_h || !u_h || !a_h) return VV_ERR_ARG;
+    if (c->coll == vv::COLL_NONE) return VV_OK;
+    const int nx = c->nx;
+    TRY(copy_d(c, c->mom_p, n_p, nx));
+    TRY(copy_d(c, c->mom_p + nx, u_p, nx));
+    TRY(copy_d(c, c->mom_p + 2 * nx, a_p, nx));
+    TRY(copy_d(c, c->mom_h, n_h, nx));
+    TRY(copy_d(c, c->mom_h + nx, u_h, nx));
+    TRY(copy_d(c, c->mom_h + 2 * nx, a_h, nx));
+    c->coll_p = {c->mom_p, c->mom_p + nx, c->mom_p + 2 * nx};
+    return VV_OK;
 }
 
 int vv_pc_set_potential(vv_ctx* c, const double* phi) {
@@ -1836,6 +1924,8 @@ int vv_step_adjoint(vv_ctx* c, const double* F, const double* f, const double* h
         return fail(VV_ERR_UNSUPPORTED, "vv_step_adjoint: the Simpson bracket has no transposed stencil here");
     if (c->avg != vv::AVG_POINT)   // the transposed operator is built for the point time derivative
         return fail(VV_ERR_UNSUPPORTED, "vv_step_adjoint: averaged time derivatives have no transposed stencil here");
+    if (c->coll != vv::COLL_NONE)
+        return fail(VV_ERR_UNSUPPORTED, "vv_step_adjoint: the collision operators have no transposed stencil here");
     const int restart = (o->restart > 0) ? o->restart : c->restart;
     if (restart > c->restart || restart < 1 || o->max_it < 0) return VV_ERR_ARG;
     TRY(adj_buffers(c));
@@ -1915,6 +2005,10 @@ int vv_step(vv_ctx* c, vv_state* st, const vv_snes_opts* so, const vv_ksp_opts* 
         return VV_ERR_ARG;
     const int restart = (ko->restart > 0) ? ko->restart : c->restart;
     if (restart > c->restart || restart < 1 || ko->max_it < 0 || so->max_iter < 1) return VV_ERR_ARG;
+    if (c->coll != vv::COLL_NONE) {   // the collision operator reads the state's moments (set_moments nc, uc, ac)
+        if (!st->u || !st->a) return VV_ERR_ARG;
+        c->coll_p = {st->n, st->u, st->a};
+    }
     std::memset(rep, 0, sizeof(*rep));
     if (c->use_graph) {
         if (!c->step_exec || !same_state(c->step_key, *st)) TRY(build_step_graph(c, st));
@@ -2591,7 +2685,7 @@ int vv_batch_create(int n, vv_ctx* const* ctxs, const vv_state* states, vv_batch
         // the point time derivative
         if (c->mixed != c0->mixed || c->g.bracket != c0->g.bracket ||
             c->g.preconditioner != VV_PC_TENSOR_KINETIC || c->g.order == VV_ORDER_REFERENCE ||
-            c->g.bracket == VV_BRACKET_SIMPSON || c->avg != vv::AVG_POINT ||
+            c->g.bracket == VV_BRACKET_SIMPSON || c->avg != vv::AVG_POINT || c->coll != vv::COLL_NONE ||
             c->nx % vv::WX != 0 || !c->pow2 || c->device != c0->device)
             return VV_ERR_UNSUPPORTED;
     }

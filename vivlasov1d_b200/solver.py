@@ -80,9 +80,11 @@ class Grid:
         return torch.zeros(self.nx, dtype=torch.float64, device=self.device)
 
     def context(self, bracket="arakawaj4", preconditioner="tensor_kinetic", charge=-1.0, mass=1.0,
-                order="factored", restart=30, precision="fp64", mixed_rtol=0.0, laplace="cfd4", averaging="point"):
+                order="factored", restart=30, precision="fp64", mixed_rtol=0.0, laplace="cfd4", averaging="point",
+                collision="", coll_freq=0.0, coll_diff=1.0, coll_drag=1.0):
         key = (bracket, preconditioner, float(charge), float(mass), order, int(restart), precision, float(mixed_rtol),
-               laplace.lower(), _lib.averaging_code(averaging))
+               laplace.lower(), _lib.averaging_code(averaging), (collision or "").lower(), float(coll_freq),
+               float(coll_diff), float(coll_drag))
         ctx = self._contexts.get(key)
         if ctx is None:
             ctx = Context(self, *key)
@@ -96,7 +98,7 @@ class Context:
 
     def __init__(self, grid, bracket="arakawaj4", preconditioner="tensor_kinetic", charge=-1.0,
                  mass=1.0, order="factored", restart=30, precision="fp64", mixed_rtol=0.0, laplace="cfd4",
-                 averaging="point"):
+                 averaging="point", collision="", coll_freq=0.0, coll_diff=1.0, coll_drag=1.0):
         lib = _lib.load()
         if not torch.cuda.is_available():
             raise RuntimeError("vivlasov1d_b200 needs a CUDA device; no CPU fallback exists")
@@ -123,6 +125,10 @@ class Context:
         self.laplace = laplace.lower()
         g.averaging = _lib.averaging_code(averaging)
         self.averaging = g.averaging
+        # CollisionOperator.create: 'collt', 'colle', anything else the no-op base class
+        g.collision = _lib.COLLISION.get((collision or "").lower(), 0)
+        g.coll_freq, g.coll_diff, g.coll_drag = float(coll_freq), float(coll_diff), float(coll_drag)
+        self.collision = g.collision if g.coll_freq != 0.0 else 0
         g.order = _lib.ORDER_REFERENCE if order == "reference" else _lib.ORDER_FACTORED
         g.gmres_restart = int(restart)
         if precision not in _lib.PRECISION:
@@ -283,8 +289,11 @@ class PETScVlasovSolver:
     def __init__(self, config, da1, daph, grid, H0, H1p, H1h, H2p, H2h, phi, charge=-1.,
                  coll_freq=0., coll_diff=1., coll_drag=1., regularisation=0., order="factored",
                  restart=30):
-        if coll_freq != 0. or regularisation != 0.:
-            raise NotImplementedError("dissipative terms (coll_freq, regularisation) are not on this path")
+        if regularisation != 0.:
+            # Regularisation.function calls call_regularisation_function, which
+            # the class does not define (Regularisation.pyx:42-44): the
+            # reference fails on the first residual with a nonzero epsilon
+            raise NotImplementedError("regularisation != 0 fails in the reference (Regularisation.pyx:42-44)")
         if grid is None:
             grid = da1
         self.grid = grid
@@ -295,8 +304,13 @@ class PETScVlasovSolver:
         # TimeDerivative.create(config.get_averaging_operator(), ...) (PETScVlasovSolver.pyx:99)
         avg = _cfg_get(cfg, "get_averaging_operator", "averaging_operator", "point")
         mass = 1.0 if H0 is None or isinstance(H0, torch.Tensor) else float(H0)
+        # CollisionOperator.create(config.get_collision_operator(), ...) (PETScVlasovSolver.pyx:102)
+        coll = _cfg_get(cfg, "get_collision_operator", "collision_operator", "")
+        if _cfg_get(cfg, "get_double_bracket", "bracket_operator", "") not in ("", None):
+            raise NotImplementedError("the double bracket (dissipation_type = 'double_bracket') is not on this path")
         self.ctx = grid.context(bracket=bracket, preconditioner=pc or None, charge=charge, mass=mass,
-                                order=order, restart=restart, averaging=avg)
+                                order=order, restart=restart, averaging=avg, collision=coll, coll_freq=coll_freq,
+                                coll_diff=coll_diff, coll_drag=coll_drag)
         self.H0, self.H1p, self.H1h, self.H2p, self.H2h = H0, H1p, H1h, H2p, H2h
         self.phi = phi
         self.preconditioner = TensorProductPreconditioner.create(pc, grid=grid, phi=phi, context=self.ctx) \
@@ -307,6 +321,11 @@ class PETScVlasovSolver:
     def set_moments(self, Np, Up, Ep, Ap, Nh, Uh, Eh, Ah):   # PETScVlasovSolver.pyx:123-132
         self.Np, self.Up, self.Ep, self.Ap = Np, Up, Ep, Ap
         self.Nh, self.Uh, self.Eh, self.Ah = Nh, Uh, Eh, Ah
+        c = self.ctx
+        if c.collision:
+            c.call("vv_set_moments", *[c.xprof(t, name) for t, name in
+                                       ((Np, "Np"), (Up, "Up"), (Ep, "Ep"), (Ap, "Ap"),
+                                        (Nh, "Nh"), (Uh, "Uh"), (Eh, "Eh"), (Ah, "Ah"))])
 
     def update_history(self, F):                               # :135-140
         self.ctx.call("vv_update_history", self.ctx.field(F, "F"))
