@@ -386,26 +386,62 @@ def collision_add(f, y, grid, coll, n, U, a, factor):
 
 
 # --------------------------------------------------------------------------
+# double bracket  (solvers/components/DoubleBracket.pyx)
+# --------------------------------------------------------------------------
+def double_bracket_function(Fave, Have, Y, grid, scheme, db, nu, factor):
+    """``dissipation_type = 'double_bracket'`` in the residual
+    (DoubleBracket.pyx:79-83 ffh: Y += -nu f [Fave, [Fave, Have]];
+    :94-97 fhh: Y += -nu f [[Fave, Have], Have]); db '' is the no-op base."""
+    if db not in ("ffh", "fhh"):
+        return Y
+    B = bracket_add(Fave, Have, np.zeros_like(Y), 1.0, grid, scheme)
+    if db == "ffh":
+        return bracket_add(Fave, B, Y, - nu * factor, grid, scheme)
+    return bracket_add(B, Have, Y, - nu * factor, grid, scheme)
+
+
+def double_bracket_jacobian(F, Fave, Have, Y, grid, scheme, db, nu, factor):
+    """The double bracket in the Jacobian (DoubleBracket.pyx:69-77 ffh:
+    Y += -nu f ([F, [Fave, Have]] + [Fave, [F, Have]]); :88-92 fhh:
+    Y += -nu f [[F, Have], Have]), Fave frozen at the last residual."""
+    if db not in ("ffh", "fhh"):
+        return Y
+    if db == "ffh":
+        B = bracket_add(Fave, Have, np.zeros_like(Y), 1.0, grid, scheme)
+        bracket_add(F, B, Y, - nu * factor, grid, scheme)
+        B = bracket_add(F, Have, np.zeros_like(Y), 1.0, grid, scheme)
+        return bracket_add(Fave, B, Y, - nu * factor, grid, scheme)
+    B = bracket_add(F, Have, np.zeros_like(Y), 1.0, grid, scheme)
+    return bracket_add(B, Have, Y, - nu * factor, grid, scheme)
+
+
+# --------------------------------------------------------------------------
 # residual and JVP  (solvers/vlasov/PETScNLVlasovMP.pyx:33-58)
 # --------------------------------------------------------------------------
-def residual(F, Fh, Have, grid, scheme="arakawaj4", averaging="point", coll=None, mom_p=None, mom_h=None):
-    """``R(F) = D_t (F - Fh) + [ (F+Fh)/2 , Have ] + C_p[F]/2 + C_h[Fh]/2``
+def residual(F, Fh, Have, grid, scheme="arakawaj4", averaging="point", coll=None, mom_p=None, mom_h=None,
+             db="", db_nu=0.0):
+    """``R(F) = D_t (F - Fh) + [ (F+Fh)/2 , Have ] + DB + C_p[F]/2 + C_h[Fh]/2``
     (PETScNLVlasovMP.pyx:43-58); mom_p / mom_h = (n, U, a) of the current
-    and the history moments (set_moments)."""
+    and the history moments (set_moments); db the double bracket ('ffh',
+    'fhh') with its nu = coll_freq."""
     Fave = 0.5 * Fh + 0.5 * F            # Fave.set(0); axpy(.5,Fh); axpy(.5,F)
     Fder = F - Fh                        # Fder.set(0); axpy(+1,F); axpy(-1,Fh)
     Y = time_derivative_add(Fder, np.zeros_like(F), grid, averaging)
     bracket_add(Fave, Have, Y, 1.0, grid, scheme)
+    double_bracket_function(Fave, Have, Y, grid, scheme, db, db_nu, 1.0)
     if coll is not None and coll.kind:
         collision_add(F, Y, grid, coll, *mom_p, 0.5)
         collision_add(Fh, Y, grid, coll, *mom_h, 0.5)
     return Y
 
 
-def jvp(X, Have, grid, scheme="arakawaj4", averaging="point", coll=None, mom_p=None):
-    """``J X = D_t X + 0.5 [X, Have] + C_p[X]/2`` (PETScNLVlasovMP.pyx:33-40)."""
+def jvp(X, Have, grid, scheme="arakawaj4", averaging="point", coll=None, mom_p=None, db="", db_nu=0.0,
+        Fave=None):
+    """``J X = D_t X + 0.5 [X, Have] + DB' + C_p[X]/2`` (PETScNLVlasovMP.pyx:33-40);
+    Fave: the average of the last residual evaluation (the double bracket's)."""
     Y = time_derivative_add(X, np.zeros_like(X), grid, averaging)
     bracket_add(X, Have, Y, 0.5, grid, scheme)
+    double_bracket_jacobian(X, Fave, Have, Y, grid, scheme, db, db_nu, 0.5)
     if coll is not None and coll.kind:
         collision_add(X, Y, grid, coll, *mom_p, 0.5)
     return Y
@@ -780,13 +816,15 @@ class VlasovSolver:
     """Restates ``PETScVlasovSolver`` for the nonlinear midpoint scheme."""
 
     def __init__(self, grid, h0v, scheme="arakawaj4", preconditioner="tensor_kinetic", averaging="point",
-                 coll=None):
+                 coll=None, db="", db_nu=0.0):
         self.grid = grid
         self.h0v = np.asarray(h0v, dtype=np.float64)
         self.scheme = scheme
         self.averaging = averaging_kind(averaging)   # PETScVlasovSolver.pyx:99
         self.coll = coll                             # PETScVlasovSolver.pyx:102
+        self.db, self.db_nu = db, db_nu              # PETScVlasovSolver.pyx:101
         self.mom_p = self.mom_h = None
+        self.Fave = None
         if preconditioner == "tensor_kinetic":
             self.pc = TensorKineticPreconditioner(grid)
         elif preconditioner == "tensor_potential":
@@ -808,11 +846,13 @@ class VlasovSolver:
         self.mom_p, self.mom_h = mom_p, mom_h
 
     def function_solver(self, F):          # PETScNLVlasovMP.pyx:43-58
+        self.Fave = 0.5 * self.Fh + 0.5 * F
         return residual(F, self.Fh, self.Have, self.grid, self.scheme, self.averaging, self.coll,
-                        self.mom_p, self.mom_h)
+                        self.mom_p, self.mom_h, self.db, self.db_nu)
 
     def jacobian_solver(self, F):          # PETScNLVlasovMP.pyx:33-40
-        return jvp(F, self.Have, self.grid, self.scheme, self.averaging, self.coll, self.mom_p)
+        return jvp(F, self.Have, self.grid, self.scheme, self.averaging, self.coll, self.mom_p, self.db,
+                   self.db_nu, self.Fave)
 
     def function(self, F):                 # PETScVlasovSolver.pyx:168-174
         Y = self.function_solver(F)
@@ -848,7 +888,7 @@ class Run:
     def __init__(self, grid, f0, scheme="arakawaj4", preconditioner="tensor_kinetic",
                  charge=-1.0, mass=1.0, ksp_rtol=1e-4, ksp_atol=1e-50,
                  ksp_max_it=1000, snes_atol=1e-10, snes_max_iter=20,
-                 normalise_f=True, laplace="cfd4", averaging="point", coll=None):
+                 normalise_f=True, laplace="cfd4", averaging="point", coll=None, db="", db_nu=0.0):
         self.grid = grid
         self.laplace = laplace
         self.charge = charge
@@ -857,7 +897,7 @@ class Run:
         self.snes_atol = snes_atol
         self.snes_max_iter = snes_max_iter
         self.h0v = kinetic_hamiltonian_v(grid, mass)
-        self.solver = VlasovSolver(grid, self.h0v, scheme, preconditioner, averaging, coll)
+        self.solver = VlasovSolver(grid, self.h0v, scheme, preconditioner, averaging, coll, db, db_nu)
         f = np.asarray(f0, dtype=np.float64)
         self.fc = normalise(f, grid) if normalise_f else f.copy()
         self.h2c = np.zeros(grid.nx)

@@ -323,10 +323,11 @@ PETSc = types.SimpleNamespace(InsertMode=InsertMode, Scatter=_Scatter,
 
 
 class Config:
-    def __init__(self, bracket, averaging="point", collision=""):
+    def __init__(self, bracket, averaging="point", collision="", double_bracket=""):
         self.bracket = bracket
         self.averaging = averaging
         self.collision = collision
+        self.double_bracket = double_bracket
 
     def get_averaging_operator(self):
         return self.averaging
@@ -335,7 +336,7 @@ class Config:
         return self.bracket
 
     def get_double_bracket(self):
-        return ""
+        return self.double_bracket
 
     def get_collision_operator(self):
         return self.collision
@@ -516,6 +517,22 @@ def make_case(ns, nx, nv, L, vmin, vmax, ht, seed):
         Y2 = da1.createGlobalVec()
         solver.jacobian(Fv, Y2)
         out["jvp_" + kind] = vec_to_2d(Y2, nx, nv)
+
+    # double bracket (DoubleBracket.pyx:67-97) in the residual and Jacobian of
+    # the J4 and Simpson brackets; the Jacobian takes Fave from the residual
+    for db in ("ffh", "fhh"):
+        for scheme in ("arakawaj4", "simpson"):
+            solver = ns["PETScVlasovSolver"](Config(scheme, "point", "", db), da1, dax, grid, H0, H1p, H1h, H2, H2,
+                                             P, coll_freq=0.3)
+            Fv = to_vec(F)
+            solver.update_history(to_vec(Fh))
+            solver.update_previous(Fv)
+            Y = da1.createGlobalVec()
+            solver.function(Fv, Y)
+            out["residual_%s_db_%s" % (scheme, db)] = vec_to_2d(Y, nx, nv)
+            Y2 = da1.createGlobalVec()
+            solver.jacobian(Fv, Y2)
+            out["jvp_%s_db_%s" % (scheme, db)] = vec_to_2d(Y2, nx, nv)
 
     # moments (Toolbox.pyx:79-165)
     N, U, E, A = (dax.createGlobalVec() for _ in range(4))

@@ -95,6 +95,22 @@ def test_collision_operator_bitexact(golden, kind):
     assert np.max(np.abs(golden["jvp_" + kind] - golden["jvp_arakawaj4"])) > 1e-3
 
 
+@pytest.mark.parametrize("db", ["ffh", "fhh"])
+@pytest.mark.parametrize("scheme", ["arakawaj4", "simpson"])
+def test_double_bracket_bitexact(golden, scheme, db):
+    """The double bracket (DoubleBracket.pyx) in the residual and in the
+    Jacobian (Fave from the residual), against the vectors of the
+    reference's own classes -> identical bits."""
+    g = _grid(golden)
+    F, Fh, H = golden["F"], golden["Fh"], golden["Have"]
+    key = "%s_db_%s" % (scheme, db)
+    assert np.array_equal(vo.residual(F, Fh, H, g, scheme, "point", None, None, None, db, 0.3),
+                          golden["residual_" + key])
+    Fave = 0.5 * Fh + 0.5 * F
+    assert np.array_equal(vo.jvp(F, H, g, scheme, "point", None, None, db, 0.3, Fave), golden["jvp_" + key])
+    assert np.max(np.abs(golden["jvp_" + key] - golden["jvp_" + scheme])) > 1e-3
+
+
 def test_averaging_operator_names():
     """TimeDerivative.create's names (TimeDerivative.pyx:36-53): the J1 class
     is the midpoint stencil, the J2 class the point derivative; unknown names
