@@ -83,6 +83,12 @@ enum vv_collision {          /* solver.collision_operator with dissipation_type
     VV_COLLISION_T = 1,      /* collT: CollisionOperator.pyx:68-157            */
     VV_COLLISION_E = 2       /* collE: CollisionOperator.pyx:160-250           */
 };
+enum vv_double_bracket {     /* solver.bracket_operator with dissipation_type
+                                = 'double_bracket' (DoubleBracket.pyx:46-55)  */
+    VV_DOUBLE_BRACKET_NONE = 0,
+    VV_DOUBLE_BRACKET_FFH = 1,  /* DoubleBracketFFH: DoubleBracket.pyx:67-83   */
+    VV_DOUBLE_BRACKET_FHH = 2   /* DoubleBracketFHH: DoubleBracket.pyx:86-97   */
+};
 enum vv_order {              /* arithmetic of the bracket kernels             */
     VV_ORDER_FACTORED = 0,   /* separable-h coefficient form (fast, default)   */
     VV_ORDER_REFERENCE = 1   /* the reference loop's operation order, no FMA   */
@@ -135,6 +141,14 @@ typedef struct vv_grid {
     double  coll_freq;       /* runspec coll_freq (collision frequency)       */
     double  coll_diff;       /* runspec coll_diff (weight of diffusion, 1)    */
     double  coll_drag;       /* runspec coll_drag (weight of drag, 1)         */
+    int32_t double_bracket;  /* enum vv_double_bracket (0: none); active only
+                                with coll_freq != 0 (nu = coll_freq), as
+                                config.py:156-162.  FP64 only (a mixed context
+                                returns VV_ERR_UNSUPPORTED); its brackets run in
+                                the reference's operation order; the Jacobian
+                                uses the Fave of the last residual evaluation
+                                (vv_function / the step's residual).  Single
+                                runs only.                                    */
 } vv_grid;
 
 typedef struct vv_ctx vv_ctx;

@@ -1083,3 +1083,102 @@ def test_collision_batch_and_adjoint_unsupported():
     with pytest.raises(_lib.VVError) as e:
         Adjoint(run).step(run.fc.clone(), f, torch.ones_like(f))
     assert e.value.status == _lib.VV_ERR_UNSUPPORTED
+
+
+# ---------------------------------------------------------------------------
+# double bracket (dissipation_type = 'double_bracket')
+# ---------------------------------------------------------------------------
+def make_db_solver(grid, scheme, db, order, g):
+    from vivlasov1d_b200 import PETScVlasovSolver
+    cfg = {"poisson_bracket": scheme, "preconditioner": "", "bracket_operator": db}
+    return PETScVlasovSolver(cfg, None, None, grid, None, xdev(g["h1p"][:, 0]), xdev(g["h1h"][:, 0]), None, None,
+                             None, order=order, coll_freq=0.3)
+
+
+@pytest.mark.parametrize("path", GOLDEN, ids=[os.path.basename(p) for p in GOLDEN])
+@pytest.mark.parametrize("scheme", ["arakawaj4", "simpson"])
+@pytest.mark.parametrize("db", ["ffh", "fhh"])
+def test_double_bracket_golden(path, scheme, db):
+    """The double bracket after the bracket (its brackets in the reference's
+    operation order; the Jacobian with the Fave of the residual) against the
+    vectors of the reference's own classes: bit-exact in the reference order,
+    1e-12 relative in the factored order."""
+    g = dict(np.load(path))
+    grid = ggrid(g)
+    key = "%s_db_%s" % (scheme, db)
+    for order in ("reference", "factored"):
+        s = make_db_solver(grid, scheme, db, order, g)
+        F, Fh = dev(g["F"]), dev(g["Fh"])
+        s.update_history(Fh)
+        s.update_previous(F)
+        Y = grid.field()
+        s.function_solver(F, Y)
+        r = host(Y)
+        s.jacobian_solver(F, Y)
+        j = host(Y)
+        if order == "reference" or scheme == "simpson":
+            assert np.array_equal(r, g["residual_" + key]), order
+            assert np.array_equal(j, g["jvp_" + key]), order
+        else:
+            assert rel(r, g["residual_" + key]) < 1e-12
+            assert rel(j, g["jvp_" + key]) < 1e-12
+        n = s.function_norm(F, Y)
+        ref = float(np.sqrt((g["residual_" + key] ** 2).sum()))
+        assert abs(n - ref) <= 1e-12 * ref
+
+
+@pytest.mark.parametrize("db", ["ffh", "fhh"])
+def test_double_bracket_wide_tiles(monkeypatch, db):
+    """nx a multiple of 64: the Jacobian's bracket in the wide tiles, then the
+    double bracket, against the oracle to 1e-12 (and the residual)."""
+    from vivlasov1d_b200 import Grid
+    monkeypatch.setenv("VV_AUTOTUNE", "0")
+    nx, nv = 128, 96
+    og = vo.Grid(nx, nv, 4 * np.pi, 8.0, -8.0, ht=0.05)
+    rng = np.random.default_rng(5)
+    F = rng.normal(size=(nx, nv))
+    Fh = F + 0.01 * rng.normal(size=(nx, nv))
+    h1p, h1h = 0.1 * rng.normal(size=nx), 0.1 * rng.normal(size=nx)
+    grid = Grid(nx, nv, 4 * np.pi, 8.0, -8.0, ht=0.05)
+    g = {"h1p": np.repeat(h1p[:, None], nv, 1), "h1h": np.repeat(h1h[:, None], nv, 1)}
+    s = make_db_solver(grid, "arakawaj4", db, "factored", g)
+    s.update_history(dev(Fh))
+    s.update_previous(dev(F))
+    H = vo.have_field(vo.kinetic_hamiltonian_v(og), h1p, h1h)
+    Y = grid.field()
+    s.function_solver(dev(F), Y)
+    assert rel(host(Y), vo.residual(F, Fh, H, og, "arakawaj4", "point", None, None, None, db, 0.3)) < 1e-12
+    s.jacobian_solver(dev(F), Y)
+    Fave = 0.5 * Fh + 0.5 * F
+    assert rel(host(Y), vo.jvp(F, H, og, "arakawaj4", "point", None, None, db, 0.3, Fave)) < 1e-12
+
+
+@pytest.mark.parametrize("db", ["ffh", "fhh"])
+def test_double_bracket_step_matches_oracle(db):
+    """Two implicit steps with dissipation_type = 'double_bracket' against the
+    oracle's steps: same Picard counts, f to 1e-10."""
+    from vivlasov1d_b200.run import Run
+    nx, nv = 64, 128
+    og = vo.Grid(nx, nv, 4 * np.pi, 10.0, -10.0, ht=0.1)
+    f0 = vo.initialise_distribution_function(og, vo.f0_landau(0.2))
+    cfg = _example_cfg(nx, nv)
+    cfg["solver"].update({"dissipation_type": "double_bracket", "bracket_operator": db, "coll_freq": 1e-3})
+    run = Run(cfg, f0=torch.from_numpy(vo.to_flat(f0)))
+    orun = vo.Run(og, f0, ksp_rtol=1e-10, snes_atol=1e-12, db=db, db_nu=1e-3)
+    for _ in range(2):
+        rep = run.step()
+        orep = orun.step()
+        assert rep["picard_its"] == orep.picard_its, (rep, orep.picard_its)
+    assert rel(host(run.fc), orun.fc) < 1e-10
+    orun0 = vo.Run(og, f0, ksp_rtol=1e-10, snes_atol=1e-12)
+    orun0.step(); orun0.step()
+    assert rel(orun.fc, orun0.fc) > 1e-8
+
+
+def test_double_bracket_mixed_unsupported():
+    """The double bracket runs in FP64 only: a mixed-precision context is refused."""
+    from vivlasov1d_b200 import _lib, Grid
+    grid = Grid(32, 64, 4 * np.pi, 8.0, -8.0, ht=0.1)
+    with pytest.raises(_lib.VVError) as e:
+        grid.context(precision="mixed", double_bracket="ffh", coll_freq=0.1)
+    assert e.value.status == _lib.VV_ERR_UNSUPPORTED

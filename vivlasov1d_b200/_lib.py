@@ -22,6 +22,8 @@ PC_NONE, PC_TENSOR_KINETIC, PC_TENSOR_POTENTIAL = 0, 1, 2
 LAPLACE = {"cfd2": 2, "cfd4": 4, "simpson": 5, "cfd2ave": 12, "simpsonave": 15}
 # the collision operator by the names CollisionOperator.create knows (CollisionOperator.pyx:44-58)
 COLLISION = {"": 0, "collt": 1, "colle": 2}
+# the double bracket by the names DoubleBracket.create knows (DoubleBracket.pyx:46-55)
+DOUBLE_BRACKET = {"": 0, "ffh": 1, "fhh": 2}
 # the time derivative by the names TimeDerivative.create knows (TimeDerivative.pyx:36-53)
 AVERAGING = {"point": 0, "midpoint": 1, "arakawa_J1": 1, "arakawa_J2": 2, "arakawa_J4": 4, "simpson": 5}
 
@@ -57,7 +59,8 @@ class vv_grid(C.Structure):
                 ("bracket", C.c_int32), ("preconditioner", C.c_int32), ("laplace", C.c_int32),
                 ("order", C.c_int32), ("gmres_restart", C.c_int32), ("precision", C.c_int32),
                 ("mixed_rtol", C.c_double), ("averaging", C.c_int32), ("collision", C.c_int32),
-                ("coll_freq", C.c_double), ("coll_diff", C.c_double), ("coll_drag", C.c_double)]
+                ("coll_freq", C.c_double), ("coll_diff", C.c_double), ("coll_drag", C.c_double),
+                ("double_bracket", C.c_int32)]
 
 
 class vv_ksp_opts(C.Structure):

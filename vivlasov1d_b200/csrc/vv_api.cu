@@ -48,6 +48,12 @@ struct vv_ctx {
     double coll_drag_fac, coll_diff_fac;
     vv::CollMoments coll_p, coll_h;
     double *mom_p, *mom_h;
+    // double bracket (dissipation_type = 'double_bracket'; 0 none, 1 ffh, 2 fhh,
+    // FP64): nu = coll_freq, the residual's Fave (kept for the Jacobian) and
+    // the inner bracket
+    int db;
+    double db_nu;
+    double *db_fave, *db_b;
     // the potential preconditioner (VV_PC_TENSOR_POTENTIAL): v modes, eigenvalues
     // for n = nv, nv twiddles, transposed field, v spectrum, elimination
     // scratch (FP32 copies in the mixed mode), rows per CTA of the v FFT, phi
@@ -191,6 +197,7 @@ vv::BracketParams bparams(const vv_ctx* c, double factor) {
     p.hxp = c->hxp;
     p.xidx = nullptr;
     p.xstride = 0;
+    p.hfield = nullptr;
     return p;
 }
 
@@ -239,7 +246,7 @@ bool aligned16(const void* p) { return p == nullptr || ((uintptr_t)p & 15u) == 0
 // or takes its partial sums from the collision kernel's narrow tiling)
 bool wide_ok(const vv_ctx* c, const void* X, const void* Xh, const void* Y) {
     return !c->narrow_bracket && c->nx % vv::WX == 0 && aligned16(X) && aligned16(Xh) && aligned16(Y) &&
-           !((c->avg != vv::AVG_POINT || c->coll != vv::COLL_NONE) && Xh != nullptr);
+           !((c->avg != vv::AVG_POINT || c->coll != vv::COLL_NONE || c->db != 0) && Xh != nullptr);
 }
 
 // the marching Jacobian stencil: about two waves of CTAs, segments of whole chunks
@@ -364,14 +371,74 @@ int launch_collision(vv_ctx* c, const T* X, const T* Xh, T* Y, double* sumsq, co
     return VV_OK;
 }
 
+// Y += factor [X, H] in the reference order (FP64, narrow tiles) with H the
+// profiles (hfield null) or a general field: the double bracket's brackets
+int launch_bracket_gen(vv_ctx* c, const double* X, const int* xidx, double* Y, const double* hfield, double factor,
+                       double* sumsq) {
+    dim3 grid((c->nx + vv::BX - 1) / vv::BX, (c->nv + vv::BY - 1) / vv::BY);
+    dim3 block(vv::BX, vv::TY);
+    vv::BracketParams p = bparams(c, factor);
+    p.xidx = xidx;
+    p.xstride = xidx ? c->ncell : 0;
+    p.hfield = hfield;
+    switch (c->g.bracket) {
+        case VV_BRACKET_SIMPSON:
+            vv::k_bracket_simpson<vv::MODE_ADD, double><<<grid, block, 0, c->st>>>(X, nullptr, Y, p, sumsq);
+            break;
+        case VV_BRACKET_J1: vv::k_bracket_ref<1, vv::MODE_ADD><<<grid, block, 0, c->st>>>(X, nullptr, Y, p, sumsq); break;
+        case VV_BRACKET_J2: vv::k_bracket_ref<2, vv::MODE_ADD><<<grid, block, 0, c->st>>>(X, nullptr, Y, p, sumsq); break;
+        default: vv::k_bracket_ref<4, vv::MODE_ADD><<<grid, block, 0, c->st>>>(X, nullptr, Y, p, sumsq); break;
+    }
+    CKL(c);
+    return VV_OK;
+}
+
+__global__ void k_fave(const double* __restrict__ F, const double* __restrict__ Fh, double* __restrict__ Fave, size_t n) {
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
+        Fave[i] = __dadd_rn(__dmul_rn(0.5, Fh[i]), __dmul_rn(0.5, F[i]));   // Fave.set(0); axpy(.5, Fh); axpy(.5, F)
+}
+
+// the double bracket after the bracket (PETScNLVlasovMP.pyx:33-58): the
+// residual stores Fave and adds DoubleBracket.function(Fave, Have, Y, 1);
+// the Jacobian adds DoubleBracket.jacobian(X, Fave, Have, Y, 1/2)
+// (DoubleBracket.pyx:69-97); sumsq from the last launch
+int db_apply(vv_ctx* c, int mode, const double* X, const double* Xh, const int* xidx, double* Y, double* sumsq) {
+    const size_t bytes = c->ncell * sizeof(double);
+    double* B = c->db_b;
+    const double* Fa = c->db_fave;
+    if (mode == vv::MODE_RESIDUAL) {
+        k_fave<<<grid1d(c->ncell, 256), 256, 0, c->st>>>(X, Xh, c->db_fave, c->ncell);
+        CKL(c);
+        CK(cudaMemsetAsync(B, 0, bytes, c->st));
+        TRY(launch_bracket_gen(c, Fa, nullptr, B, nullptr, 1.0, nullptr));                 // B = [Fave, Have]
+        if (c->db == 1) return launch_bracket_gen(c, Fa, nullptr, Y, B, -c->db_nu * 1.0, sumsq);   // [Fave, B]
+        return launch_bracket_gen(c, B, nullptr, Y, nullptr, -c->db_nu * 1.0, sumsq);             // [B, Have]
+    }
+    const double f = -c->db_nu * 0.5;
+    CK(cudaMemsetAsync(B, 0, bytes, c->st));
+    if (c->db == 1) {
+        TRY(launch_bracket_gen(c, Fa, nullptr, B, nullptr, 1.0, nullptr));    // B = [Fave, Have]
+        TRY(launch_bracket_gen(c, X, xidx, Y, B, f, nullptr));                // Y += f [X, B]
+        CK(cudaMemsetAsync(B, 0, bytes, c->st));
+        TRY(launch_bracket_gen(c, X, xidx, B, nullptr, 1.0, nullptr));        // B = [X, Have]
+        return launch_bracket_gen(c, Fa, nullptr, Y, B, f, sumsq);            // Y += f [Fave, B]
+    }
+    TRY(launch_bracket_gen(c, X, xidx, B, nullptr, 1.0, nullptr));            // B = [X, Have]
+    return launch_bracket_gen(c, B, nullptr, Y, nullptr, f, sumsq);           // Y += f [B, Have]
+}
+
 // the residual (MODE_RESIDUAL) or Jacobian (MODE_JVP) of the chosen
-// discretisation, or the bare bracket (MODE_ADD); with collisions the
-// residual's partial sums come from the collision kernel
+// discretisation, or the bare bracket (MODE_ADD); with a double bracket or
+// collisions the residual's partial sums come from the last kernel
 template <int MODE, typename T>
 int launch_bracket(vv_ctx* c, const T* X, const T* Xh, T* Y, double factor, double* sumsq,
                    const int* xidx = nullptr) {
     const bool coll = MODE != vv::MODE_ADD && c->coll != vv::COLL_NONE;
-    TRY(launch_bracket_td<MODE, T>(c, X, Xh, Y, factor, coll ? nullptr : sumsq, xidx));
+    const bool db = MODE != vv::MODE_ADD && c->db != 0 && std::is_same<T, double>::value;
+    TRY(launch_bracket_td<MODE, T>(c, X, Xh, Y, factor, (coll || db) ? nullptr : sumsq, xidx));
+    if constexpr (std::is_same<T, double>::value) {
+        if (db) TRY(db_apply(c, MODE, X, Xh, xidx, Y, coll ? nullptr : sumsq));
+    }
     if (coll) return launch_collision<T>(c, X, MODE == vv::MODE_RESIDUAL ? Xh : nullptr, Y, sumsq, xidx);
     return VV_OK;
 }
@@ -1414,6 +1481,11 @@ int vv_create(const vv_grid* grid, vv_ctx** out) {
         return VV_ERR_ARG;
     if (g.collision != VV_COLLISION_NONE && g.collision != VV_COLLISION_T && g.collision != VV_COLLISION_E)
         return VV_ERR_ARG;
+    if (g.double_bracket != VV_DOUBLE_BRACKET_NONE && g.double_bracket != VV_DOUBLE_BRACKET_FFH &&
+        g.double_bracket != VV_DOUBLE_BRACKET_FHH)
+        return VV_ERR_ARG;
+    if (g.double_bracket != VV_DOUBLE_BRACKET_NONE && g.coll_freq != 0.0 && g.precision == VV_PRECISION_MIXED)
+        return VV_ERR_UNSUPPORTED;   // the double bracket runs in FP64 only
     const int restart = g.gmres_restart > 0 ? g.gmres_restart : 30;
     if (restart > vv::MAX_RESTART) return VV_ERR_ARG;
     if (g.precision != VV_PRECISION_FP64 && g.precision != VV_PRECISION_MIXED) return VV_ERR_ARG;
@@ -1456,6 +1528,9 @@ int vv_create(const vv_grid* grid, vv_ctx** out) {
                   : vv::COLL_NONE;
     c->coll_drag_fac = -0.5 * g.coll_freq * g.coll_drag * c->hv_inv * 0.5;
     c->coll_diff_fac = -0.5 * g.coll_freq * g.coll_diff * (1. / (c->hv * c->hv));
+    // the double bracket (DoubleBracket.create, config.py:156-162: none unless coll_freq != 0)
+    c->db = (g.double_bracket != VV_DOUBLE_BRACKET_NONE && g.coll_freq != 0.0) ? g.double_bracket : 0;
+    c->db_nu = g.coll_freq;
     {   // the Laplacian's stencil (matrix_mult of PETScPoissonCFD2/CFD4/Simpson.pyx; the Ave classes
         // keep CFD2's / Simpson's) and the density average of their formRHS (PETScPoissonCFD2Ave.pyx:
         // 0.25 (n_{i-1} + 2 n_i + n_{i+1}); PETScPoissonSimpsonAve.pyx: (n_{i-2} + 8 n_{i-1} + 18 n_i
@@ -1677,6 +1752,16 @@ int vv_create(const vv_grid* grid, vv_ctx** out) {
             return fail_cuda(cudaGetLastError(), "vv_create upload (potential preconditioner)");
         }
     }
+    // double bracket: Fave and the inner bracket
+    if (c->db && ((s = dalloc(&c->db_fave, n)) || (s = dalloc(&c->db_b, n)))) {
+        vv_destroy(c);
+        return s;
+    }
+    if (c->db && (cudaMemset(c->db_fave, 0, n * sizeof(double)) != cudaSuccess ||
+                  cudaMemset(c->db_b, 0, n * sizeof(double)) != cudaSuccess)) {
+        vv_destroy(c);
+        return fail_cuda(cudaGetLastError(), "vv_create upload (double bracket)");
+    }
     // collisions: current / history moment profiles (n, U, a)
     if (c->coll != vv::COLL_NONE) {
         if ((s = dalloc(&c->mom_p, (size_t)3 * nx)) || (s = dalloc(&c->mom_h, (size_t)3 * nx))) {
@@ -1737,7 +1822,7 @@ int vv_destroy(vv_ctx* c) {
                     c->spec32, c->tw32, c->lambda32, c->dinv32, c->adj_cH, c->adj_cF, c->adj_zpart,
                     c->adj_zbuf, c->adj_q, c->adj_hprof, c->adj_h1a, c->adj_h1b, c->lamv, c->twv, c->pv_spec,
                     c->pv_scr, c->pv_xt, c->phipc, c->twv32, c->pv_spec32, c->pv_scr32, c->pv_xt32,
-                    c->mom_p, c->mom_h};
+                    c->mom_p, c->mom_h, c->db_fave, c->db_b};
     destroy_graph(c);
     for (int k = 0; k < 4; ++k)
         if (c->cs[k]) cudaStreamDestroy(c->cs[k]);
@@ -1924,8 +2009,8 @@ int vv_step_adjoint(vv_ctx* c, const double* F, const double* f, const double* h
         return fail(VV_ERR_UNSUPPORTED, "vv_step_adjoint: the Simpson bracket has no transposed stencil here");
     if (c->avg != vv::AVG_POINT)   // the transposed operator is built for the point time derivative
         return fail(VV_ERR_UNSUPPORTED, "vv_step_adjoint: averaged time derivatives have no transposed stencil here");
-    if (c->coll != vv::COLL_NONE)
-        return fail(VV_ERR_UNSUPPORTED, "vv_step_adjoint: the collision operators have no transposed stencil here");
+    if (c->coll != vv::COLL_NONE || c->db)
+        return fail(VV_ERR_UNSUPPORTED, "vv_step_adjoint: the dissipative terms have no transposed stencil here");
     const int restart = (o->restart > 0) ? o->restart : c->restart;
     if (restart > c->restart || restart < 1 || o->max_it < 0) return VV_ERR_ARG;
     TRY(adj_buffers(c));
@@ -2685,7 +2770,7 @@ int vv_batch_create(int n, vv_ctx* const* ctxs, const vv_state* states, vv_batch
         // the point time derivative
         if (c->mixed != c0->mixed || c->g.bracket != c0->g.bracket ||
             c->g.preconditioner != VV_PC_TENSOR_KINETIC || c->g.order == VV_ORDER_REFERENCE ||
-            c->g.bracket == VV_BRACKET_SIMPSON || c->avg != vv::AVG_POINT || c->coll != vv::COLL_NONE ||
+            c->g.bracket == VV_BRACKET_SIMPSON || c->avg != vv::AVG_POINT || c->coll != vv::COLL_NONE || c->db ||
             c->nx % vv::WX != 0 || !c->pow2 || c->device != c0->device)
             return VV_ERR_UNSUPPORTED;
     }

@@ -37,6 +37,8 @@ struct BracketParams {
     const double* hxp;  // 4*nx: h1p, h1h, h2p, h2h profiles
     const int* xidx;    // optional: input is X + (*xidx) * xstride (GMRES basis vector)
     size_t xstride;
+    const double* hfield;   // optional (MODE_ADD, reference-order kernels): a general h[j*nx + i]
+                            // instead of the profiles (the double bracket's inner bracket)
 };
 
 template <typename T> VV_DEV T rn_add(T a, T b);
@@ -156,7 +158,7 @@ __device__ __forceinline__ void stage_tile(const double* __restrict__ X, const d
             } else {
                 xv = X[g];
             }
-            if (STAGE_H) hv = h_ref(p, gi, gj);
+            if (STAGE_H) hv = p.hfield ? p.hfield[g] : h_ref(p, gi, gj);
         }
         sx[ly][lx] = xv;
         if (STAGE_H) sh[ly][lx] = hv;
@@ -309,7 +311,7 @@ k_bracket_simpson(const T* __restrict__ X, const T* __restrict__ Xh, T* __restri
             const size_t g = (size_t)gj * p.nx + gi;
             // Fave = 0 + .5 Fh + .5 F  (PETScNLVlasovMP.pyx:49-51)
             xv = (MODE == MODE_RESIDUAL) ? rn_add<T>(rn_mul<T>(T(0.5), Xh[g]), rn_mul<T>(T(0.5), X[g])) : X[g];
-            hv = T(h_ref(p, gi, gj));
+            hv = T(p.hfield ? p.hfield[g] : h_ref(p, gi, gj));
         }
         sx[ly][lx] = xv;
         sh[ly][lx] = hv;

@@ -40,8 +40,6 @@ class Run:
             pass
         if so["timestepping"].lower() != "mp" or so["mode"] != "split":
             raise NotImplementedError("only the split midpoint (mp) method is on this path")
-        if cfg.is_dissipation_double_bracket():
-            raise NotImplementedError("the double bracket (dissipation_type = 'double_bracket') is not on this path")
         if so.get("regularisation", 0.0) not in (0, 0.0, None):
             # Regularisation.function calls an undefined method (Regularisation.pyx:42-44)
             raise NotImplementedError("regularisation != 0 fails in the reference (Regularisation.pyx:42-44)")
@@ -55,7 +53,8 @@ class Run:
                                      precision=precision, laplace=cfg.get_laplace_operator(),
                                      averaging=cfg.get_averaging_operator(),
                                      collision=cfg.get_collision_operator(), coll_freq=so["coll_freq"],
-                                     coll_diff=so["coll_diff"], coll_drag=so["coll_drag"])
+                                     coll_diff=so["coll_diff"], coll_drag=so["coll_drag"],
+                                     double_bracket=cfg.get_double_bracket())
         g = self.grid
         fld, xv = g.field, g.xvec
         self.fc, self.fh = fld(), fld()

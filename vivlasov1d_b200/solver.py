@@ -81,10 +81,10 @@ class Grid:
 
     def context(self, bracket="arakawaj4", preconditioner="tensor_kinetic", charge=-1.0, mass=1.0,
                 order="factored", restart=30, precision="fp64", mixed_rtol=0.0, laplace="cfd4", averaging="point",
-                collision="", coll_freq=0.0, coll_diff=1.0, coll_drag=1.0):
+                collision="", coll_freq=0.0, coll_diff=1.0, coll_drag=1.0, double_bracket=""):
         key = (bracket, preconditioner, float(charge), float(mass), order, int(restart), precision, float(mixed_rtol),
                laplace.lower(), _lib.averaging_code(averaging), (collision or "").lower(), float(coll_freq),
-               float(coll_diff), float(coll_drag))
+               float(coll_diff), float(coll_drag), (double_bracket or "").lower())
         ctx = self._contexts.get(key)
         if ctx is None:
             ctx = Context(self, *key)
@@ -98,7 +98,7 @@ class Context:
 
     def __init__(self, grid, bracket="arakawaj4", preconditioner="tensor_kinetic", charge=-1.0,
                  mass=1.0, order="factored", restart=30, precision="fp64", mixed_rtol=0.0, laplace="cfd4",
-                 averaging="point", collision="", coll_freq=0.0, coll_diff=1.0, coll_drag=1.0):
+                 averaging="point", collision="", coll_freq=0.0, coll_diff=1.0, coll_drag=1.0, double_bracket=""):
         lib = _lib.load()
         if not torch.cuda.is_available():
             raise RuntimeError("vivlasov1d_b200 needs a CUDA device; no CPU fallback exists")
@@ -129,6 +129,9 @@ class Context:
         g.collision = _lib.COLLISION.get((collision or "").lower(), 0)
         g.coll_freq, g.coll_diff, g.coll_drag = float(coll_freq), float(coll_diff), float(coll_drag)
         self.collision = g.collision if g.coll_freq != 0.0 else 0
+        # DoubleBracket.create: 'ffh', 'fhh', anything else the no-op base class
+        g.double_bracket = _lib.DOUBLE_BRACKET.get((double_bracket or "").lower(), 0)
+        self.double_bracket = g.double_bracket if g.coll_freq != 0.0 else 0
         g.order = _lib.ORDER_REFERENCE if order == "reference" else _lib.ORDER_FACTORED
         g.gmres_restart = int(restart)
         if precision not in _lib.PRECISION:
@@ -306,11 +309,11 @@ class PETScVlasovSolver:
         mass = 1.0 if H0 is None or isinstance(H0, torch.Tensor) else float(H0)
         # CollisionOperator.create(config.get_collision_operator(), ...) (PETScVlasovSolver.pyx:102)
         coll = _cfg_get(cfg, "get_collision_operator", "collision_operator", "")
-        if _cfg_get(cfg, "get_double_bracket", "bracket_operator", "") not in ("", None):
-            raise NotImplementedError("the double bracket (dissipation_type = 'double_bracket') is not on this path")
+        # DoubleBracket.create(config.get_double_bracket(), ...) (PETScVlasovSolver.pyx:101)
+        db = _cfg_get(cfg, "get_double_bracket", "bracket_operator", "")
         self.ctx = grid.context(bracket=bracket, preconditioner=pc or None, charge=charge, mass=mass,
                                 order=order, restart=restart, averaging=avg, collision=coll, coll_freq=coll_freq,
-                                coll_diff=coll_diff, coll_drag=coll_drag)
+                                coll_diff=coll_diff, coll_drag=coll_drag, double_bracket=db)
         self.H0, self.H1p, self.H1h, self.H2p, self.H2h = H0, H1p, H1h, H2p, H2h
         self.phi = phi
         self.preconditioner = TensorProductPreconditioner.create(pc, grid=grid, phi=phi, context=self.ctx) \
