@@ -713,15 +713,19 @@ __device__ __forceinline__ void bracket_wide_tile(const T* __restrict__ X, const
 // Marching Jacobian-vector product: a CTA owns a strip of MW columns (one
 // thread per column) and a segment of rows, and walks down v through a ring
 // of NR rows in shared memory (a power of two) that cp.async fills three
-// chunks of CH rows ahead of the compute.  Each thread keeps its column's five-row
+// chunks of CH rows ahead of the compute.  One block barrier per chunk: the
+// ring holds the chunk being computed with its 2-row halos and the three
+// chunks after it (NR = 4 CH + 4), so the copies of chunk k+3 go out right
+// after the barrier that publishes chunk k -- every thread has passed it, so
+// chunk k-1's rows are free -- and the row coefficients are double-buffered.  Each thread keeps its column's five-row
 // window and its column's x-coefficients in registers; the v-coefficients of
 // a chunk's rows are formed once per CTA.  A row costs 5 shared loads per
 // output; the x halo is 4 of MW + 4 columns and the v halo 4 rows per segment.
 // ---------------------------------------------------------------------------
-// rows per chunk and ring rows (a power of two >= 2 chunks + 4 halo rows)
+// rows per chunk and ring rows (a power of two = 4 chunks + 4 halo rows)
 template <typename T> struct MarchShape;
-template <> struct MarchShape<double> { static constexpr int CH = 8, NR = 32; };
-template <> struct MarchShape<float> { static constexpr int CH = 16, NR = 64; };
+template <> struct MarchShape<double> { static constexpr int CH = 7, NR = 32; };
+template <> struct MarchShape<float> { static constexpr int CH = 15, NR = 64; };
 
 
 // ring row layout: [pad][2 left halo][MW columns][2 right halo][pad]; the
@@ -731,7 +735,7 @@ struct MarchRow {
     static constexpr int LP = 16 / (int)sizeof(T);
     static constexpr int RS = MW + 2 * LP;
     static constexpr size_t smem_bytes() {
-        return (size_t)MarchShape<T>::NR * RS * sizeof(T) + (size_t)MarchShape<T>::CH * 3 * sizeof(double);
+        return (size_t)MarchShape<T>::NR * RS * sizeof(T) + (size_t)2 * MarchShape<T>::CH * 3 * sizeof(double);
     }
 };
 
@@ -770,10 +774,10 @@ VV_DEV void bracket_march_item(const T* __restrict__ X, T* __restrict__ Y, const
                                int strip, int segi) {
     using RW = MarchRow<T, MW>;
     constexpr int CH = MarchShape<T>::CH, NR = MarchShape<T>::NR;
-    static_assert(NR >= 3 * CH + 4 && (NR & (NR - 1)) == 0, "ring of three chunks and the halo, a power of two");
+    static_assert(NR >= 4 * CH + 4 && (NR & (NR - 1)) == 0, "ring of four chunks and the halo, a power of two");
     extern __shared__ __align__(16) unsigned char smem_raw[];
     T* ring = reinterpret_cast<T*>(smem_raw);
-    double* rc = reinterpret_cast<double*>(smem_raw + (size_t)NR * RW::RS * sizeof(T));   // [CH][3] row coefficients
+    double* rcb = reinterpret_cast<double*>(smem_raw + (size_t)NR * RW::RS * sizeof(T));   // [2][CH][3] row coefficients
     const int nx = p.nx, nv = p.nv;
     const int tx = threadIdx.x;
     const int x0 = strip * MW;
@@ -808,9 +812,12 @@ VV_DEV void bracket_march_item(const T* __restrict__ X, T* __restrict__ Y, const
     auto rowp = [&](int r) -> const T* { return ring + ((r + NR) & (NR - 1)) * RW::RS + lx; };
     T w0, w1, w2, w3, m0, m1, q0, q1;
     bool primed = false;
-    for (int jc = j_start; jc < j_end; jc += CH) {
+    int par = 0;
+    for (int jc = j_start; jc < j_end; jc += CH, par ^= 1) {
         const int jn = min(jc + CH, j_end);
-        // the chunk's row coefficients (A1, am, ap), once per CTA
+        double* rc = rcb + par * 3 * CH;
+        // the chunk's row coefficients (A1, am, ap), once per CTA (the other
+        // buffer may still be read by threads computing the previous chunk)
         if (tx < jn - jc) {
             const int j = jc + tx;
             const double a0 = hv0(j - 2), a1 = hv0(j - 1), a2 = hv0(j), a3 = hv0(j + 1), a4 = hv0(j + 2);
@@ -822,6 +829,13 @@ VV_DEV void bracket_march_item(const T* __restrict__ X, T* __restrict__ Y, const
         }
         cp_async_wait2();
         __syncthreads();
+        // the third chunk ahead into the slots of the previous chunk, which
+        // every thread has finished (it passed this barrier after computing it)
+        {
+            const int ra = jc + 3 * CH + 2, rb = min(jc + 4 * CH + 1, j_end + 1);
+            if (ra <= rb) march_load<T, MW>(X, ring, nx, nv, x0, ra, rb);
+            cp_async_commit();
+        }
         if (!primed) {
             w0 = rowp(jc - 2)[0]; w1 = rowp(jc - 1)[0]; w2 = rowp(jc)[0]; w3 = rowp(jc + 1)[0];
             m0 = rowp(jc - 1)[-1]; m1 = rowp(jc)[-1];
@@ -871,13 +885,9 @@ VV_DEV void bracket_march_item(const T* __restrict__ X, T* __restrict__ Y, const
         } else {
             for (int j = jc; j < jn; ++j, yout += nx) row_out(j, yout);
         }
-        __syncthreads();
-        // the third chunk ahead into the slots this chunk no longer needs
-        const int ra = jc + 3 * CH + 2, rb = min(jc + 4 * CH + 1, j_end + 1);
-        if (ra <= rb) march_load<T, MW>(X, ring, nx, nv, x0, ra, rb);
-        cp_async_commit();
     }
     cp_async_wait0();
+    __syncthreads();   // the ring is idle for the next item
 }
 
 template <int SCHEME, typename T, int MW>
