@@ -116,3 +116,17 @@ hdf5_output = twostream_test.hdf5"
     assert c["solver"]["petsc_ksp_rtol"] == 1e-5
     assert c["initial_data"]["charge"] == -1.0 and c["initial_data"]["nfourier"] == 32
     assert c.get_averaging_operator() == "point"
+
+
+def test_run_refuses_reference_failure_modes():
+    """Options whose reference path fails (an initial-guess predictor, a
+    nonzero regularisation) are refused when the run is built, before any
+    device work."""
+    from vivlasov1d_b200.run import Run
+    base = {"grid": {"nx": 16, "nv": 32, "L": 12.566370614359172, "vmin": -8.0, "vmax": 8.0, "ht": 0.1, "nt": 1},
+            "solver": {"method": "matrixfree"}, "initial_data": {"charge": -1.0}}
+    for key, val in (("initial_guess", "rk4"), ("initial_guess", "rk4_16"), ("regularisation", 1e-3)):
+        cfg = {k: dict(v) for k, v in base.items()}
+        cfg["solver"][key] = val
+        with pytest.raises(NotImplementedError):
+            Run(cfg)

@@ -40,6 +40,11 @@ class Run:
             pass
         if so["timestepping"].lower() != "mp" or so["mode"] != "split":
             raise NotImplementedError("only the split midpoint (mp) method is on this path")
+        ig = so.get("initial_guess")
+        if ig not in (None, "", "None"):
+            # run_base.py:173-183: 'rk4' calls PETScArakawaRungeKutta.rk18_J4, which the class does
+            # not define; the runspec's own names ('rk4_16', 'gear2', ...) are not keys of the table
+            raise NotImplementedError("initial_guess %r fails in the reference (run_base.py:173-183, 815-828)" % ig)
         if so.get("regularisation", 0.0) not in (0, 0.0, None):
             # Regularisation.function calls an undefined method (Regularisation.pyx:42-44)
             raise NotImplementedError("regularisation != 0 fails in the reference (Regularisation.pyx:42-44)")
