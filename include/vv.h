@@ -38,7 +38,7 @@ extern "C" {
 enum vv_status {
     VV_OK = 0,
     VV_ERR_ARG = 1,          /* invalid argument or NULL pointer             */
-    VV_ERR_UNSUPPORTED = 2,  /* configuration not supported by this build    */
+    VV_ERR_UNSUPPORTED = 2,  /* configuration the library does not support  */
     VV_ERR_CUDA = 3,         /* a CUDA runtime call failed                   */
     VV_ERR_ALLOC = 4,        /* device allocation failed                     */
     VV_ERR_DIVERGED = 5,     /* Picard residual above the abort threshold    */
