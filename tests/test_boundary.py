@@ -130,3 +130,26 @@ def test_run_refuses_reference_failure_modes():
         cfg["solver"][key] = val
         with pytest.raises(NotImplementedError):
             Run(cfg)
+
+
+def test_config_dissipation_choices():
+    """config.py:129-162: the collision operator and the double bracket are
+    chosen by dissipation_type and only with coll_freq != 0; the names map
+    to the vv_grid codes the factories know (anything else is the no-op base
+    class in CollisionOperator.create / DoubleBracket.create)."""
+    from vivlasov1d_b200 import _lib
+    from vivlasov1d_b200.config import Config
+
+    def cfg(**solver):
+        return Config(overrides={"solver": solver})
+
+    c = cfg(dissipation_type="collisions", collision_operator="collT", coll_freq=0.1)
+    assert c.is_dissipation_collisions() and not c.is_dissipation_double_bracket()
+    assert c.get_collision_operator() == "collt" and c.get_double_bracket() == ""
+    assert cfg(dissipation_type="collisions", collision_operator="collE", coll_freq=0.0).get_collision_operator() == ""
+    d = cfg(dissipation_type="double_bracket", bracket_operator="FHH", coll_freq=0.2)
+    assert d.get_double_bracket() == "fhh" and d.get_collision_operator() == ""
+    assert cfg().get_collision_operator() == "" and cfg().get_double_bracket() == ""
+    assert _lib.COLLISION["collt"] == 1 and _lib.COLLISION["colle"] == 2
+    assert _lib.DOUBLE_BRACKET["ffh"] == 1 and _lib.DOUBLE_BRACKET["fhh"] == 2
+    assert _lib.LAPLACE["cfd2ave"] == 12 and _lib.LAPLACE["simpsonave"] == 15
