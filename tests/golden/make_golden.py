@@ -518,6 +518,23 @@ def make_case(ns, nx, nv, L, vmin, vmax, ht, seed):
         solver.jacobian(Fv, Y2)
         out["jvp_" + kind] = vec_to_2d(Y2, nx, nv)
 
+    # every term at once (averaged time derivative, bracket, double bracket,
+    # collision operator) in one solver: the order in which PETScNLVlasovMP
+    # adds them (the runspec makes the two dissipations exclusive; the solver
+    # class adds whatever its factories built)
+    solver = ns["PETScVlasovSolver"](Config("arakawaj4", "midpoint", "collt", "ffh"), da1, dax, grid, H0, H1p, H1h,
+                                     H2, H2, P, coll_freq=0.2, coll_diff=0.7, coll_drag=1.3)
+    solver.set_moments(*mom[0], *mom[1])
+    Fv = to_vec(F)
+    solver.update_history(to_vec(Fh))
+    solver.update_previous(Fv)
+    Y = da1.createGlobalVec()
+    solver.function(Fv, Y)
+    out["residual_all_terms"] = vec_to_2d(Y, nx, nv)
+    Y2 = da1.createGlobalVec()
+    solver.jacobian(Fv, Y2)
+    out["jvp_all_terms"] = vec_to_2d(Y2, nx, nv)
+
     # double bracket (DoubleBracket.pyx:67-97) in the residual and Jacobian of
     # the J4 and Simpson brackets; the Jacobian takes Fave from the residual
     for db in ("ffh", "fhh"):

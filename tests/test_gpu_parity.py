@@ -1182,3 +1182,34 @@ def test_double_bracket_mixed_unsupported():
     with pytest.raises(_lib.VVError) as e:
         grid.context(precision="mixed", double_bracket="ffh", coll_freq=0.1)
     assert e.value.status == _lib.VV_ERR_UNSUPPORTED
+
+
+@pytest.mark.parametrize("path", GOLDEN, ids=[os.path.basename(p) for p in GOLDEN])
+def test_all_terms_golden(path):
+    """The midpoint time derivative, the J4 bracket, the ffh double bracket
+    and the collT operator in one context, in the order PETScNLVlasovMP adds
+    them, against the reference's own vectors: bit-exact in the reference
+    order, 1e-12 relative in the factored order."""
+    from vivlasov1d_b200 import PETScVlasovSolver
+    g = dict(np.load(path))
+    grid = ggrid(g)
+    cfg = {"poisson_bracket": "arakawaj4", "preconditioner": "", "averaging_operator": "midpoint",
+           "collision_operator": "collt", "bracket_operator": "ffh"}
+    for order in ("reference", "factored"):
+        s = PETScVlasovSolver(cfg, None, None, grid, None, xdev(g["h1p"][:, 0]), xdev(g["h1h"][:, 0]), None, None,
+                              None, order=order, coll_freq=0.2, coll_diff=0.7, coll_drag=1.3)
+        s.set_moments(*[xdev(g["coll_%s_%s" % (m, k)]) for k in ("p", "h") for m in ("n", "u", "e", "a")])
+        F, Fh = dev(g["F"]), dev(g["Fh"])
+        s.update_history(Fh)
+        s.update_previous(F)
+        Y = grid.field()
+        s.function_solver(F, Y)
+        r = host(Y)
+        s.jacobian_solver(F, Y)
+        j = host(Y)
+        if order == "reference":
+            assert np.array_equal(r, g["residual_all_terms"])
+            assert np.array_equal(j, g["jvp_all_terms"])
+        else:
+            assert rel(r, g["residual_all_terms"]) < 1e-12
+            assert rel(j, g["jvp_all_terms"]) < 1e-12

@@ -111,6 +111,21 @@ def test_double_bracket_bitexact(golden, scheme, db):
     assert np.max(np.abs(golden["jvp_" + key] - golden["jvp_" + scheme])) > 1e-3
 
 
+def test_all_terms_bitexact(golden):
+    """Every term at once -- the midpoint time derivative, the J4 bracket, the
+    ffh double bracket and the collT operator -- in PETScNLVlasovMP's order,
+    against the reference's own vectors -> identical bits."""
+    g = _grid(golden)
+    coll = vo.Collisions("collt", 0.2, 0.7, 1.3)
+    mp = (golden["coll_n_p"], golden["coll_u_p"], golden["coll_a_p"])
+    mh = (golden["coll_n_h"], golden["coll_u_h"], golden["coll_a_h"])
+    F, Fh, H = golden["F"], golden["Fh"], golden["Have"]
+    assert np.array_equal(vo.residual(F, Fh, H, g, "arakawaj4", "midpoint", coll, mp, mh, "ffh", 0.2),
+                          golden["residual_all_terms"])
+    assert np.array_equal(vo.jvp(F, H, g, "arakawaj4", "midpoint", coll, mp, "ffh", 0.2, 0.5 * Fh + 0.5 * F),
+                          golden["jvp_all_terms"])
+
+
 def test_averaging_operator_names():
     """TimeDerivative.create's names (TimeDerivative.pyx:36-53): the J1 class
     is the midpoint stencil, the J2 class the point derivative; unknown names
