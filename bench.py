@@ -23,8 +23,15 @@ field_energy: after W+K steps, |E_mixed - E_fp64| / |E_fp64| per instance.
 e2e         : the batched mixed step through Batch.step with every
               instance's f copied host->device (pinned) before and
               device->host after each step.
+batched_fp64: the same table through the batch in FP64 (ksp_rtol 1e-4): the
+              gain of batching alone, apart from the FP32 inner solves.
+step_roofline: algorithmic bytes of the timed steps (from the logged
+              Picard and GMRES counts) over their device time.
 --impl reference : the CPU restatement of the reference algorithm (the C
-              port under oracle/, all host threads) on the same instances.
+              port under oracle/) on the same instances, spread over all host
+              threads (each instance single-threaded, as separate runs of a
+              sweep use a many-core host); also reported: the port stepping
+              one instance after the other with OpenMP inside each.
 Multi-GPU: independent replicas, one sweep per rank with its own seed
 (scaling "weak"); the time is the max over ranks.
 """
@@ -136,6 +143,30 @@ def reduce_over_ranks(maxes, sums, device):
     return [float(x) for x in tm], [float(x) for x in ts]
 
 
+def step_algorithmic_bytes(specs, reps, mixed, restart=30):
+    """Algorithmic HBM bytes of the timed steps from the logged iteration
+    counts: per instance and step, cells x [N_pic (24 + 16 + 8) + N_gmres
+    (16 + 48) + sum over Arnoldi steps (16 k + 40)] in FP64 (residual, its
+    norm and the moments per Picard pass; Jacobian product and the 3-pass
+    preconditioner per GMRES iteration; Gram-Schmidt against the k basis
+    vectors of the cycle).  The mixed mode runs the Jacobian product, the
+    preconditioner and Gram-Schmidt in FP32: those terms are halved."""
+    inner = 0.5 if mixed else 1.0
+    total = 0.0
+    for rep in reps:                      # one list of instance reports per step
+        for s, r in zip(specs, rep):
+            cells = s["nx"] * s["nv"]
+            npic = r["picard_its"]
+            gm = sum(r["gmres_its"])
+            gs = 0.0
+            for m in r["gmres_its"]:
+                for it in range(m):
+                    k = it % restart + 1
+                    gs += 16 * k + 40
+            total += cells * (npic * 48 + inner * (gm * 64 + gs))
+    return total
+
+
 def time_steps(fn, k, stream):
     import torch
     torch.cuda.synchronize()
@@ -161,10 +192,13 @@ def run_gpu(args, rank, world):
     mode_rows = sum((s["nx"] // 2 + 1) * s["nv"] for s in specs)   # complex unknowns of the tridiagonal stage
     mixed = W.sweep_runs(specs=specs, device=dev, precision="mixed")
     plain = W.sweep_runs(specs=specs, device=dev, precision="fp64")
+    bfp64 = W.sweep_runs(specs=specs, device=dev, precision="fp64")
     batch = Batch(mixed)
-    # ---- warm-up (both arms advance W steps from the same initial state) ----
+    batch64 = Batch(bfp64)
+    # ---- warm-up (every arm advances W steps from the same initial state) ----
     for _ in range(args.warmup):
         batch.step()
+        batch64.step()
         for r in plain:
             r.step()
     torch.cuda.synchronize()
@@ -183,10 +217,16 @@ def run_gpu(args, rank, world):
     clocks = sampler.stop() if sampler else None
     picard = sum(r["picard_its"] for rep in reps for r in rep) / (args.steps * len(specs))
     gmres = sum(sum(r["gmres_its"]) for rep in reps for r in rep) / (args.steps * len(specs))
+    # ---- batched FP64: the same table and tolerances in FP64 (separates the
+    # gain of batching from the gain of the FP32 inner solves) ----
+    t_b64, reps64 = time_steps(batch64.step, args.steps, stream)
     # ---- plain FP64, one instance after the other ----
     t_plain, _ = time_steps(lambda: [r.step() for r in plain], args.steps, stream)
-    fe_m, fe_p = W.field_energies(mixed), W.field_energies(plain)
+    fe_m, fe_p, fe_b = W.field_energies(mixed), W.field_energies(plain), W.field_energies(bfp64)
     fe_rel = np.abs(fe_m - fe_p) / np.abs(fe_p)
+    fe_rel_b64 = np.abs(fe_b - fe_p) / np.abs(fe_p)
+    step_bytes = step_algorithmic_bytes(specs, reps, mixed=True)
+    step_bytes64 = step_algorithmic_bytes(specs, reps64, mixed=False)
     # ---- roofline kernels on the whole table (between steps) ----
     mdot_s = batch.time_kernel(0, it=MDOT_IT, reps=20)
     pc_s = batch.time_kernel(1, it=MDOT_IT, reps=10)
@@ -211,10 +251,12 @@ def run_gpu(args, rank, world):
     t_e2e, _ = time_steps(e2e_step, args.steps, stream)
     total_cells = cells
     if world > 1:
-        (t_value, t_plain, t_e2e), (total_cells,) = reduce_over_ranks([t_value, t_plain, t_e2e], [cells], dev)
-    return dict(cells=cells, total_cells=total_cells, t_value=t_value, t_plain=t_plain, t_e2e=t_e2e, launches=launches, clocks=clocks,
-                picard=picard, gmres=gmres, fe_rel=fe_rel, mdot_s=mdot_s, pc_s=pc_s, jvp_s=jvp_s, tri_s=tri_s,
-                mode_rows=mode_rows)
+        (t_value, t_plain, t_e2e, t_b64), (total_cells,) = reduce_over_ranks([t_value, t_plain, t_e2e, t_b64],
+                                                                             [cells], dev)
+    return dict(cells=cells, total_cells=total_cells, t_value=t_value, t_plain=t_plain, t_e2e=t_e2e, t_b64=t_b64,
+                launches=launches, clocks=clocks, picard=picard, gmres=gmres, fe_rel=fe_rel, fe_rel_b64=fe_rel_b64,
+                mdot_s=mdot_s, pc_s=pc_s, jvp_s=jvp_s, tri_s=tri_s, mode_rows=mode_rows, step_bytes=step_bytes,
+                step_bytes64=step_bytes64, specs=specs)
 
 
 def port_runs(specs):
@@ -236,46 +278,72 @@ def port_runs(specs):
     return runs
 
 
-def cpu_baseline_sample(specs, seconds=15.0):
-    """The C port on the host: whole sweep steps (every instance once) until
-    about `seconds` have passed, at least one."""
+def _largest_first(specs):
+    return sorted(range(len(specs)), key=lambda i: -specs[i]["nx"] * specs[i]["nv"])
+
+
+def port_sweep_step(runs, order, mode):
+    """One sweep step of the C port.  mode "instances": the runs spread over
+    the host threads, each single-threaded inside (how a sweep of separate
+    runs uses a many-core host; largest instances first); mode "inside": one
+    run after the other, each parallel inside its kernels."""
+    from oracle.c import step_many
+    if mode == "instances":
+        step_many(runs, order)
+    else:
+        for p in runs:
+            p.step()
+
+
+def cpu_sample(specs, seconds, mode):
+    """The C port on the host: whole sweep steps (every instance once) from
+    t=0 until about `seconds` have passed, at least one."""
     runs = port_runs(specs)
+    order = _largest_first(specs)
     cells = sum(s["nx"] * s["nv"] for s in specs)
     t0 = time.perf_counter()
     steps = 0
     while True:
-        for p in runs:
-            p.step()
+        port_sweep_step(runs, order, mode)
         steps += 1
         if time.perf_counter() - t0 > seconds:
             break
     dt = time.perf_counter() - t0
+    what = ("instances spread over the threads, each single-threaded" if mode == "instances"
+            else "one instance after the other, OpenMP inside each")
     return {"value": cells * steps / dt / 1e9, "unit": METRIC, "cores": runs[0].threads, "kind": "port",
-            "sample": "%d step(s) of all %d sweep instances from t=0 (C port of the oracle, OpenMP)"
-                      % (steps, len(specs))}
+            "sample": "%d step(s) of all %d sweep instances from t=0 (C port of the oracle, %s)"
+                      % (steps, len(specs), what)}
+
+
+def cpu_baseline_sample(specs, seconds=15.0):
+    return cpu_sample(specs, seconds, "instances")
 
 
 def reference_arm(steps, warmup, budget=240.0):
-    """W warm-up + K timed sweep steps of the C port on all host threads;
-    stops early (and says so) if the timed steps would exceed `budget` s."""
+    """W warm-up + K timed sweep steps of the C port, the instances spread over
+    all host threads; stops early (and says so) if the timed steps would
+    exceed `budget` s.  A second figure: the port stepping one instance after
+    the other with OpenMP inside each, on a bounded sample."""
     specs = specs_for(0)
     runs = port_runs(specs)
+    order = _largest_first(specs)
     cells = sum(s["nx"] * s["nv"] for s in specs)
     for _ in range(warmup):
-        for p in runs:
-            p.step()
+        port_sweep_step(runs, order, "instances")
     t0 = time.perf_counter()
     done = 0
     for _ in range(steps):
-        for p in runs:
-            p.step()
+        port_sweep_step(runs, order, "instances")
         done += 1
         if time.perf_counter() - t0 > budget:
             break
     dt = time.perf_counter() - t0
+    inside = cpu_sample(specs, 15.0, "inside")
     return {"value": cells * done / dt / 1e9, "cores": runs[0].threads, "kind": "port",
-            "sample": "%d timed sweep steps (all %d instances) after %d warm-up steps (C port of the oracle, "
-                      "OpenMP)" % (done, len(specs), warmup)}
+            "sample": "%d timed sweep steps (all %d instances) after %d warm-up steps (C port of the oracle; "
+                      "instances spread over the host threads, each single-threaded)" % (done, len(specs), warmup),
+            "inside_parallel": inside}
 
 
 def main():
@@ -303,6 +371,7 @@ def main():
                 "data": "synthetic (seeded analytic initial data)", "config": config,
                 "cpu_baseline": {"value": cb["value"], "unit": METRIC, "cores": cb["cores"], "kind": cb["kind"],
                                  "sample": cb["sample"]},
+                "one_instance_at_a_time": cb["inside_parallel"],
                 "e2e": {"value": cb["value"], "unit": METRIC, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
         print(json.dumps(line))
         return
@@ -325,7 +394,17 @@ def main():
     value = work / res["t_value"] / 1e9
     plain = work / res["t_plain"] / 1e9
     e2e = work / res["t_e2e"] / 1e9
+    b64 = work / res["t_b64"] / 1e9
     peak, peak_kind = measured_peaks()
+    step_roofline = {
+        "what": "algorithmic bytes of the whole timed steps (per instance: cells x [N_pic x 48 + N_gmres x 64 + "
+                "sum over Arnoldi steps (16 k + 40)] B in FP64, the FP32 inner terms halved) from the logged "
+                "Picard/GMRES counts, over the device time of the steps",
+        "bytes_per_step": res["step_bytes"] / args.steps,
+        "achieved": res["step_bytes"] / res["t_value"] / 1e9, "peak": peak, "unit": "GB/s",
+        "frac": res["step_bytes"] / res["t_value"] / 1e9 / peak,
+        "batched_fp64_achieved": res["step_bytes64"] / res["t_b64"] / 1e9,
+        "batched_fp64_frac": res["step_bytes64"] / res["t_b64"] / 1e9 / peak}
     mdot_bytes = cells * (MDOT_IT + 2) * 4      # w and V_0..V_it read in FP32
     # the tridiagonal stage: read the FP32 complex spectrum and the LU
     # reciprocals, write the solution (3 x 8 B per mode and row)
@@ -351,6 +430,10 @@ def main():
             "data": "synthetic (seeded analytic initial data)", "config": config,
             "plain_fp64": {"value": plain, "unit": METRIC, "ms_per_step": res["t_plain"] * 1e3 / args.steps,
                            "ratio_batched_mixed": value / plain},
+            "batched_fp64": {"value": b64, "unit": METRIC, "ms_per_step": res["t_b64"] * 1e3 / args.steps,
+                             "ratio_vs_plain": b64 / plain, "ratio_batched_mixed_vs_this": value / b64,
+                             "ksp_rtol": 1e-4, "field_energy_rel_err_vs_plain_max": float(res["fe_rel_b64"].max())},
+            "step_roofline": step_roofline,
             "field_energy_rel_err": {"max": float(fe.max()), "median": float(np.median(fe)),
                                      "vs": "plain FP64 GPU step (pinned to the oracle by the tests)"},
             "e2e": {"value": e2e, "unit": METRIC, "h2d_bytes_per_step": cells * 8, "d2h_bytes_per_step": cells * 8},

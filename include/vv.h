@@ -368,6 +368,16 @@ int vv_timing_read(vv_ctx* ctx, int64_t* launches, double* total_ms, int reset);
 /* Number of kernels the library has launched since the last reset
  * (kernels executed inside the time-step graph included). */
 int vv_launch_count(vv_ctx* ctx, int64_t* launches, int reset);
+/* Kernel variants the context runs, as five ints: FFT kind of the
+ * preconditioner's x transforms (0 shared-memory radix-2, 1 four-step
+ * register/shuffle, 2 direct DFT), FFT rows per CTA, tridiagonal kind (0 CTA
+ * per mode, 1 warp per mode), narrow bracket tiles (1: 32 x 16 instead of
+ * 64 x 32) and the marching Jacobian stencil's strip width (0: tiles).
+ * vv_create picks them by timing the candidates on the device at hand, or
+ * takes them from the environment variable VV_SHAPE="fft,R,tri,narrow[,march]"
+ * (VV_ERR_ARG when they do not fit the grid).  No reference counterpart: the
+ * reference has one implementation per operation. */
+int vv_kernel_shape(vv_ctx* ctx, int32_t* shape);
 /* Device time of one kernel on the context's own buffers: `reps` launches
  * are captured back to back in a CUDA graph and timed with CUDA events on the
  * context's stream.  which: 0 Jacobian-vector product (input: GMRES basis
@@ -398,9 +408,11 @@ int vv_time_kernel(vv_ctx* ctx, int which, int reps, double* avg_ms);
  *   The array is shared by all callers on a device: calls whose kernels can
  *   overlap in time (two host threads, or two unordered streams) race on it
  *   and must be serialised by the caller.
- *   The first call on each device does a one-time set-up (it looks up the
- *   array's device address, which may load the library's device code); make
- *   that first call before any stream capture begins on that device.
+ *   The first call on each device (and the first after the device's CUDA
+ *   context was destroyed and re-created, e.g. by cudaDeviceReset) does a
+ *   one-time set-up: it looks up the array's device address in the current
+ *   context, which may load the library's device code.  Make that first
+ *   call before any stream capture begins on that device.
  *   Nothing in the array has to start at zero. */
 #define VV_NOALLOC_MAX_NX 16384
 int vv_invariants_noalloc(const vv_grid* grid, const double* f, const double* phi,

@@ -44,6 +44,8 @@ def load():
         lib.vvp_get_phi.argtypes = [C.c_void_p, C.c_void_p]
         lib.vvp_step.argtypes = [C.c_void_p, C.POINTER(C.c_int)]
         lib.vvp_step.restype = C.c_int
+        lib.vvp_step_many.argtypes = [C.POINTER(C.c_void_p), C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_int)]
+        lib.vvp_step_many.restype = None
         _lib = lib
     return _lib
 
@@ -87,3 +89,23 @@ class CPort:
         g = C.c_int()
         p = self.lib.vvp_step(self.h, C.byref(g))
         return p, g.value
+
+
+def step_many(ports, order=None):
+    """One time step of every run in `ports`, the runs spread over the host
+    threads (dynamic schedule in the given order, e.g. largest first; each
+    run single-threaded inside).  Returns (picard counts, GMRES totals)."""
+    if not ports:
+        return [], []
+    lib = load()
+    seq = [ports[i] for i in order] if order is not None else list(ports)
+    n = len(seq)
+    hs = (C.c_void_p * n)(*[p.h for p in seq])
+    pic = (C.c_int * n)()
+    gm = (C.c_int * n)()
+    lib.vvp_step_many(hs, n, pic, gm)
+    idx = list(order) if order is not None else list(range(n))
+    picard, gmres = [0] * n, [0] * n
+    for k, i in enumerate(idx):
+        picard[i], gmres[i] = pic[k], gm[k]
+    return picard, gmres

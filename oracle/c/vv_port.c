@@ -478,3 +478,24 @@ int vvp_step(port* p, int* gmres_total) {
     if (gmres_total) *gmres_total = tot;
     return i;
 }
+
+/* one time step of n independent runs, the runs spread over the host threads
+ * (each run single-threaded inside: the kernels' own parallel loops are nested
+ * regions, which run on one thread) -- how a sweep of separate runs uses a
+ * many-core host.  picard[i], gmres[i] get each run's counts. */
+void vvp_step_many(port** ps, int n, int* picard, int* gmres_total) {
+#ifdef _OPENMP
+    const int saved = omp_get_max_active_levels();
+    omp_set_max_active_levels(1);
+#endif
+#pragma omp parallel for schedule(dynamic, 1)
+    for (int i = 0; i < n; ++i) {
+        int g = 0;
+        const int p = vvp_step(ps[i], &g);
+        if (picard) picard[i] = p;
+        if (gmres_total) gmres_total[i] = g;
+    }
+#ifdef _OPENMP
+    omp_set_max_active_levels(saved);
+#endif
+}

@@ -23,7 +23,8 @@ petsc4py exists in this image, so its extensions cannot be compiled.  Its
 The reference tree is read only when this script runs (in the development
 container); the GPU tests use the committed .npz files.
 
-Usage:  python tests/golden/make_golden.py [/path/to/viVlasov1D]
+Usage:  python tests/golden/make_golden.py /path/to/viVlasov1D
+        (or VIVLASOV1D_REF=/path/to/viVlasov1D python tests/golden/make_golden.py)
 """
 from __future__ import annotations
 
@@ -36,7 +37,7 @@ import types
 import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-REF = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+REF = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("VIVLASOV1D_REF", "")
 
 
 # ---------------------------------------------------------------------------
@@ -654,6 +655,9 @@ CASES = [
 
 
 def main():
+    if not REF or not os.path.isdir(os.path.join(REF, "vlasov")):
+        sys.exit("usage: make_golden.py /path/to/viVlasov1D (the reference source tree; "
+                 "or set VIVLASOV1D_REF)")
     ns = reference_namespace()
     for (nx, nv, L, vmin, vmax, ht, seed) in CASES:
         out = make_case(ns, nx, nv, L, vmin, vmax, ht, seed)

@@ -3,7 +3,8 @@
 Collected last (file name) so that it runs both on its own and after every
 other GPU test in one process.  The GPU test compares it through the C ABI
 with vv_invariants (the context entry point) on the same device fields, on
-two calls in a row and across two grids, with the tolerance below.  The CPU
+calls in a row and across two grids, with the tolerance below, and checks
+that the device's free memory does not change across those calls.  The CPU
 tests check the argument and size checks, which return before any device
 work.
 """
@@ -67,12 +68,19 @@ def test_noalloc_invariants_match_context_entry_point():
             ref = _lib.vv_invariant_set()
             _lib.check(lib.vv_invariants(ctx.h, C.c_void_p(f.data_ptr()), C.c_void_p(phi.data_ptr()), hp,
                                          C.byref(ref)), "vv_invariants")
-            for call in range(2):                      # two calls in a row on the same scratch
+            free0 = None
+            for call in range(3):                      # calls in a row on the same scratch
                 got = _lib.vv_invariant_set()
                 _lib.check(lib.vv_invariants_noalloc(C.byref(gs), C.c_void_p(f.data_ptr()),
                                                      C.c_void_p(phi.data_ptr()), hp, C.c_void_p(stream),
                                                      C.byref(got)), "vv_invariants_noalloc")
                 _compare(got, ref, (nx, nv, h is not None, call))
+                # the device's free memory does not move across the calls after the first
+                # (which may load the library's device code): nothing is allocated
+                free = torch.cuda.mem_get_info()[0]
+                if free0 is None:
+                    free0 = free
+                assert free == free0, (nx, nv, call, free0 - free)
             assert ref.mass > 0 and ref.L2 > 0 and ref.field_energy != 0.0
 
 

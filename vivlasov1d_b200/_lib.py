@@ -138,6 +138,7 @@ SIGNATURES = {
     "vv_timing_read": (I, [P, C.POINTER(C.c_int64), C.POINTER(D), I]),
     "vv_launch_count": (I, [P, C.POINTER(C.c_int64), I]),
     "vv_time_kernel": (I, [P, I, I, C.POINTER(D)]),
+    "vv_kernel_shape": (I, [P, C.POINTER(C.c_int32)]),
     "vv_batch_create": (I, [I, C.POINTER(P), C.POINTER(vv_state), C.POINTER(P)]),
     "vv_batch_destroy": (I, [P]),
     "vv_batch_set_stream": (I, [P, P]),

@@ -1323,6 +1323,31 @@ int autotune(vv_ctx* c) {
     return VV_OK;
 }
 
+// A fixed kernel shape "fft,R,tri,narrow[,march]" (the fields of TuneResult),
+// checked against what the grid allows; VV_ERR_ARG when it does not fit.
+int apply_shape(vv_ctx* c, const char* spec) {
+    int v[5] = {0, 1, 0, 0, 0};
+    const int n = sscanf(spec, "%d,%d,%d,%d,%d", &v[0], &v[1], &v[2], &v[3], &v[4]);
+    if (n < 4) return fail(VV_ERR_ARG, "VV_SHAPE=\"%s\": expected fft,R,tri,narrow[,march]", spec);
+    const int kind = v[0], R = v[1], tk = v[2], nb = v[3], mw = v[4];
+    if (kind < 0 || kind > 2 || ((kind == 0 || kind == 1) && !c->pow2) || (kind == 1 && !four_step_ok(c->M)))
+        return fail(VV_ERR_ARG, "VV_SHAPE: FFT kind %d does not fit nx %d", kind, c->nx);
+    if (R != 1 && R != 2 && R != 4 && R != 8)
+        return fail(VV_ERR_ARG, "VV_SHAPE: rows per CTA %d not in {1, 2, 4, 8}", R);
+    if (kind < 2 && fft_smem(kind, c->M, R, sizeof(double2), true) > (size_t)c->smem_limit)
+        return fail(VV_ERR_ARG, "VV_SHAPE: %d FFT rows per CTA need more shared memory than the limit", R);
+    if (tk != 0 && tk != 1) return fail(VV_ERR_ARG, "VV_SHAPE: tridiagonal kind %d not in {0, 1}", tk);
+    if (nb != 0 && nb != 1) return fail(VV_ERR_ARG, "VV_SHAPE: narrow flag %d not in {0, 1}", nb);
+    if (mw != 0 && ((mw != 128 && mw != 256) || c->nx % mw != 0))
+        return fail(VV_ERR_ARG, "VV_SHAPE: marching strip width %d does not fit nx %d", mw, c->nx);
+    c->fft_kind = kind;
+    c->pcR = kind == 2 ? 1 : R;
+    c->tri_kind = tk;
+    c->narrow_bracket = nb;
+    c->march = mw;
+    return VV_OK;
+}
+
 void destroy_graph(vv_ctx* c) {
     if (c->step_exec) cudaGraphExecDestroy(c->step_exec);
     if (c->step_graph) cudaGraphDestroy(c->step_graph);
@@ -1802,6 +1827,19 @@ int vv_create(const vv_grid* grid, vv_ctx** out) {
         if (e) c->march = atoi(e);
     }
     {
+        // VV_SHAPE="fft,R,tri,narrow[,march]" fixes the kernel variants (tests run each variant
+        // explicitly; profiling); else the autotuner picks them by timing
+        const char* sh = getenv("VV_SHAPE");
+        if (sh && sh[0]) {
+            if ((s = apply_shape(c, sh)) != VV_OK) {
+                vv_destroy(c);
+                return s;
+            }
+            *out = c;
+            return VV_OK;
+        }
+    }
+    {
         const char* e = getenv("VV_AUTOTUNE");
         if (!(e && e[0] == '0')) {
             if ((s = autotune(c)) != VV_OK) {
@@ -2214,6 +2252,16 @@ int vv_time_kernel(vv_ctx* c, int which, int reps, double* avg_ms) {
     cudaGraphExecDestroy(ex);
     if (e != cudaSuccess) return fail_cuda(e, "vv_time_kernel");
     *avg_ms = (double)ms / reps;
+    return VV_OK;
+}
+
+int vv_kernel_shape(vv_ctx* c, int32_t* shape) {
+    if (!c || !shape) return VV_ERR_ARG;
+    shape[0] = c->fft_kind;
+    shape[1] = c->pcR;
+    shape[2] = c->tri_kind;
+    shape[3] = c->narrow_bracket;
+    shape[4] = c->march;
     return VV_OK;
 }
 

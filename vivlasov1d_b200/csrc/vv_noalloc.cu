@@ -25,7 +25,8 @@
 //     two host threads, or on two streams without ordering between them)
 //     overwrite each other's partial sums.  Serialise them (one stream, or a
 //     synchronisation between calls).
-//   * the first call on each device looks the array's address up
+//   * the first call on each device (and the first after that device's CUDA
+//     context was destroyed and re-created) looks the array's address up
 //     (cudaGetSymbolAddress), which may load the library's device code; make
 //     that first call before any stream capture begins on that device.
 // No part of the array has to start at zero: every word a kernel reads in a
@@ -179,22 +180,61 @@ static __device__ __align__(256) double g_scratch[NA_WORDS];
 
 namespace {
 
-// device address of g_scratch, looked up once per device
+// device address of g_scratch, looked up once per device and CUDA context:
+// a context destroyed and re-created (cudaDeviceReset, a driver-API context
+// of its own) reloads the module, so the address of the old context is not
+// reused -- the context's process-unique id (cuCtxGetId) keys the cache
 constexpr int NA_MAX_DEVICES = 64;
+struct ScratchOf {
+    unsigned long long ctx_id;
+    double* ptr;
+};
 std::mutex g_setup_mu;
-double* g_scratch_of[NA_MAX_DEVICES] = {};
+ScratchOf g_scratch_of[NA_MAX_DEVICES] = {};
+
+typedef int (*ctx_get_current_fn)(void**);
+typedef int (*ctx_get_id_fn)(void*, unsigned long long*);
+
+// id of the context current on this thread (0 if none or not available)
+unsigned long long current_ctx_id() {
+    static ctx_get_current_fn get_current = nullptr;
+    static ctx_get_id_fn get_id = nullptr;
+    static bool looked_up = false;
+    if (!looked_up) {
+        void* f1 = nullptr;
+        void* f2 = nullptr;
+        cudaDriverEntryPointQueryResult q1, q2;
+        if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &f1, cudaEnableDefault, &q1) == cudaSuccess &&
+            cudaGetDriverEntryPoint("cuCtxGetId", &f2, cudaEnableDefault, &q2) == cudaSuccess &&
+            q1 == cudaDriverEntryPointSuccess && q2 == cudaDriverEntryPointSuccess) {
+            get_current = (ctx_get_current_fn)f1;
+            get_id = (ctx_get_id_fn)f2;
+        }
+        looked_up = true;
+    }
+    void* ctx = nullptr;
+    unsigned long long id = 0;
+    if (!get_current || !get_id || get_current(&ctx) != 0 || !ctx || get_id(ctx, &id) != 0) return 0;
+    return id;
+}
 
 int scratch_for_current_device(double** out) {
     int dev = 0;
     if (cudaGetDevice(&dev) != cudaSuccess) return VV_ERR_CUDA;
     if (dev < 0 || dev >= NA_MAX_DEVICES) return VV_ERR_UNSUPPORTED;
     std::lock_guard<std::mutex> lock(g_setup_mu);
-    if (!g_scratch_of[dev]) {
+    unsigned long long id = current_ctx_id();
+    ScratchOf& e = g_scratch_of[dev];
+    if (!e.ptr || id == 0 || e.ctx_id != id) {
+        // set-up on this device and context (the lookup makes the runtime's
+        // context current if no call on this thread has done so yet)
         double* p = nullptr;
         if (cudaGetSymbolAddress((void**)&p, g_scratch) != cudaSuccess || !p) return VV_ERR_CUDA;
-        g_scratch_of[dev] = p;
+        if (id == 0) id = current_ctx_id();
+        e.ptr = p;
+        e.ctx_id = id;
     }
-    *out = g_scratch_of[dev];
+    *out = e.ptr;
     return VV_OK;
 }
 

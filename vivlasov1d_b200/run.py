@@ -35,9 +35,14 @@ class Run:
             cfg = Config(cfg) if isinstance(cfg, str) else Config(overrides=cfg)
         self.cfg = cfg
         gr, so, idata = cfg["grid"], cfg["solver"], cfg["initial_data"]
-        if so["method"] not in ("matrixfree",) and so.get("_allow_any_method") is None:
-            # the reference dispatches other methods to other runscripts (run.py:61-93)
-            pass
+        if so["method"] != "matrixfree" or so["type"] != "nonlinear":
+            # run.py:61-93 loads run_<type>_<method>_<mode>_<timestepping>: 'direct' assembles the
+            # Jacobian and factors it (run_nonlinear_direct_split_mp.py), 'explicit' runs an explicit
+            # integrator, and the runspec default 'iterative' fails at dispatch in the reference (its
+            # runscript defines viVlasov1Dgmres, not viVlasov1Drunscript; its __init__ takes no cfg)
+            raise NotImplementedError("solver.method = %r, type = %r: this path is the nonlinear matrix-free "
+                                      "runscript (method = 'matrixfree', type = 'nonlinear')"
+                                      % (so["method"], so["type"]))
         if so["timestepping"].lower() != "mp" or so["mode"] != "split":
             raise NotImplementedError("only the split midpoint (mp) method is on this path")
         ig = so.get("initial_guess")

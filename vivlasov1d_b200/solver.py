@@ -209,6 +209,13 @@ class Context:
         self.call("vv_launch_count", C.byref(n), int(reset))
         return n.value
 
+    def kernel_shape(self):
+        """The kernel variants this context runs, (fft, R, tri, narrow,
+        march): picked by the autotuner, or fixed by VV_SHAPE."""
+        out = (C.c_int32 * 5)()
+        self.call("vv_kernel_shape", out)
+        return tuple(int(x) for x in out)
+
 
 # ---------------------------------------------------------------------------
 class TensorProductPreconditioner:
