@@ -832,7 +832,8 @@ class VlasovSolver:
         else:
             self.pc = None
         self.Fh = None
-        self.Have = None
+        # a new global Vec (PETScVlasovSolver.pyx:73): zero until the first update_previous
+        self.Have = np.zeros((grid.nx, grid.nv))
 
     def update_history(self, F, phi=None):  # PETScVlasovSolver.pyx:135-140
         self.Fh = F.copy()
@@ -868,6 +869,96 @@ class VlasovSolver:
 
 
 # --------------------------------------------------------------------------
+# explicit predictors of the initial guess  (solvers/explicit/,
+# run_base.py:173-181, 786-912)
+# --------------------------------------------------------------------------
+# the names run_base.py's option table and runspec.cfg:58 use, mapped to the
+# integrator: 'rk4' calls rk18_J4, which PETScArakawaRungeKutta does not
+# define; its closest method is rk4_18
+PREDICTORS = {"symplectic2": "symplectic2", "symplectic4": "symplectic4", "rk4_16": "rk4_16",
+              "rk4_18": "rk4_18", "rk4": "rk4_18"}
+
+
+def symplectic4_coefficients():
+    """run_base.py:887-898 (initial_guess_symplectic4)."""
+    fac2 = 2. ** (1. / 3.)
+    c1 = 0.5 / (2. - fac2)
+    c2 = c1 * (1. - fac2)
+    d1 = 1. / (2. - fac2)
+    return (c1, c2, c2, c1), (d1, - d1 * fac2, d1)
+
+
+def _pred_bracket(x, h, grid, scheme):
+    """The explicit classes' bracket ``Y = [x, h]`` with three corrections:
+    the arguments in the order of PoissonBracket.pyx:80 (the classes pass
+    (x, y, h)), the output zeroed first (the classes add into work vectors
+    they never clear) and factor -1, the sign of the implicit residual
+    (PETScNLVlasovMP.pyx:43-58: df/dt = -[f, h]; with +1 the predictor steps
+    backwards in time and the residual guard discards it)."""
+    y = np.zeros_like(x)
+    return bracket_add(x, h, y, -1.0, grid, scheme)
+
+
+def symplectic_substep(x, h, factor, grid, scheme, niter):
+    """PETScArakawaSymplectic.kinetic / potential (PETScArakawaSymplectic.pyx:
+    62-92): ``x += factor * ht / niter * [x, h]``."""
+    y = _pred_bracket(x, h, grid, scheme)
+    return x + factor * grid.ht / float(niter) * y
+
+
+def rk4_16(x, h, grid, scheme, niter):
+    """PETScArakawaRungeKutta.rk4_16 (PETScArakawaRungeKutta.pyx:20-58), the
+    classical RK4, with the expressions' evaluation order."""
+    ht = grid.ht
+    t1 = _pred_bracket(x, h, grid, scheme)
+    t2 = _pred_bracket(x + 0.5 * ht / float(niter) * t1, h, grid, scheme)
+    t3 = _pred_bracket(x + 0.5 * ht / float(niter) * t2, h, grid, scheme)
+    t4 = _pred_bracket(x + 1.0 * ht / float(niter) * t3, h, grid, scheme)
+    return x + ht / float(niter) * (t1 + 2. * t2 + 2. * t3 + t4) / 6.
+
+
+def rk4_18(x, h, grid, scheme, niter):
+    """PETScArakawaRungeKutta.rk4_18 (PETScArakawaRungeKutta.pyx:61-100), the
+    3/8 rule."""
+    ht = grid.ht
+    t1 = _pred_bracket(x, h, grid, scheme)
+    t2 = _pred_bracket(x + 1. / 3. * ht / float(niter) * t1, h, grid, scheme)
+    t3 = _pred_bracket(x - 1. / 3. * ht / float(niter) * t1 + ht / float(niter) * t2, h, grid, scheme)
+    t4 = _pred_bracket(x + ht / float(niter) * t1 - ht / float(niter) * t2 + ht / float(niter) * t3, h, grid,
+                       scheme)
+    return x + ht / float(niter) * (t1 + 3. * t2 + 3. * t3 + t4) / 8.
+
+
+def predict(f, grid, h0v, h1h, h2h=None, scheme="arakawaj4", method="symplectic2", niter=1):
+    """The initial-guess predictor of run_base.py:811-912 over ``niter`` =
+    initial_iter iterations of ht/niter each: the kinetic part with H0, the
+    potential part with H1h + H2h (the history potentials the classes are
+    built with, run_base.py:370-372), RK4 with H0 + H1h + H2h.  The moments
+    the reference recomputes between iterations do not enter the predictor."""
+    method = PREDICTORS[method]
+    nx, nv = f.shape
+    h0 = np.broadcast_to(np.asarray(h0v, dtype=np.float64)[None, :], (nx, nv))
+    h1 = np.broadcast_to(np.asarray(h1h, dtype=np.float64)[:, None], (nx, nv))
+    h2 = np.broadcast_to((np.zeros(nx) if h2h is None else np.asarray(h2h, dtype=np.float64))[:, None], (nx, nv))
+    x = np.array(f, dtype=np.float64)
+    for _ in range(niter):
+        if method == "symplectic2":              # run_base.py:866-877
+            x = symplectic_substep(x, h0, 0.5, grid, scheme, niter)
+            x = symplectic_substep(x, h1 + h2, 1.0, grid, scheme, niter)
+            x = symplectic_substep(x, h0, 0.5, grid, scheme, niter)
+        elif method == "symplectic4":            # run_base.py:900-912
+            (c1, c2, c3, c4), (d1, d2, d3) = symplectic4_coefficients()
+            for c, d in ((c1, d1), (c2, d2), (c3, d3)):
+                x = symplectic_substep(x, h0, c, grid, scheme, niter)
+                x = symplectic_substep(x, h1 + h2, d, grid, scheme, niter)
+            x = symplectic_substep(x, h0, c4, grid, scheme, niter)
+        else:                                   # run_base.py:811-832 (rk18_J4 -> rk4_18)
+            h = h0 + h1 + h2
+            x = (rk4_16 if method == "rk4_16" else rk4_18)(x, h, grid, scheme, niter)
+    return x
+
+
+# --------------------------------------------------------------------------
 # the time loop  (run/run_nonlinear_matrixfree_split_mp.py:111-174,
 #                 run/run_base.py:631-655, 749-763)
 # --------------------------------------------------------------------------
@@ -880,6 +971,9 @@ class StepReport:
     reverted: bool = False
     stop_rule: str = ""
     aborted: bool = False
+    guess_prev: float = 0.0     # residual before / after the predictor (0 without one)
+    guess: float = 0.0
+    guess_kept: bool = False
 
 
 class Run:
@@ -888,7 +982,8 @@ class Run:
     def __init__(self, grid, f0, scheme="arakawaj4", preconditioner="tensor_kinetic",
                  charge=-1.0, mass=1.0, ksp_rtol=1e-4, ksp_atol=1e-50,
                  ksp_max_it=1000, snes_atol=1e-10, snes_max_iter=20,
-                 normalise_f=True, laplace="cfd4", averaging="point", coll=None, db="", db_nu=0.0):
+                 normalise_f=True, laplace="cfd4", averaging="point", coll=None, db="", db_nu=0.0,
+                 initial_guess=None, initial_iter=1):
         self.grid = grid
         self.laplace = laplace
         self.charge = charge
@@ -896,6 +991,9 @@ class Run:
         self.ksp = dict(rtol=ksp_rtol, atol=ksp_atol, max_it=ksp_max_it)
         self.snes_atol = snes_atol
         self.snes_max_iter = snes_max_iter
+        self.scheme = scheme
+        self.initial_guess = PREDICTORS[initial_guess] if initial_guess not in (None, "", "None") else None
+        self.initial_iter = int(initial_iter)
         self.h0v = kinetic_hamiltonian_v(grid, mass)
         self.solver = VlasovSolver(grid, self.h0v, scheme, preconditioner, averaging, coll, db, db_nu)
         f = np.asarray(f0, dtype=np.float64)
@@ -949,10 +1047,29 @@ class Run:
         if res.reason >= 0:
             self.fc = self.fc - from_flat(res.x, g.nx, g.nv)
 
+    def guess(self, rep):
+        """initial_guess (run_base.py:786-808): the predictor from the current
+        f, kept only if the residual went down.  The residuals use the
+        solver's Have of the last update_previous and Fh = f (make_history
+        ran); on a revert the moments are recomputed from the restored f (the
+        reference keeps the guess's potential with the restored f)."""
+        fl = self.fc.copy()
+        rep.guess_prev = self.calculate_residual()
+        self.fc = predict(self.fc, self.grid, self.h0v, self.h1h, self.h2h, self.scheme, self.initial_guess,
+                          self.initial_iter)
+        self.calculate_moments()
+        rep.guess = self.calculate_residual()
+        rep.guess_kept = not rep.guess > rep.guess_prev
+        if not rep.guess_kept:
+            self.fc = fl
+            self.calculate_moments()
+
     def step(self):
         """One time step (run_nonlinear_matrixfree_split_mp.py:111-174)."""
         rep = StepReport()
         self.make_history()
+        if self.initial_guess:
+            self.guess(rep)
         self.update_previous()
         pred_norm = self.calculate_residual()
         rep.residuals.append(pred_norm)

@@ -140,6 +140,46 @@ def load(relpath: str, ns: dict) -> dict:
     return ns
 
 
+def fix_explicit(src: str) -> str:
+    """The explicit integrators (solvers/explicit/) as predictors of the
+    initial guess, with three corrections to the reference's text, each
+    needed for them to compute a bracket step at all:
+      1. poisson_bracket_array is called with its arguments in the order of
+         its signature (x, h, y, factor) (PoissonBracket.pyx:80); the classes
+         pass (x, y, h), which reads the output vector as the Hamiltonian and
+         adds the bracket into the Hamiltonian's local array;
+      2. the output array is zeroed before each bracket, which adds into it
+         (the classes reuse their work vectors Y, X1..X4 without clearing);
+      3. factor -1 instead of 1, so that the predictor advances
+         df/dt = -[f, h], the sign of the implicit residual
+         (F - Fh)/ht + [Fave, Have] (PETScNLVlasovMP.pyx:43-58); with +1 it
+         steps backwards in time and the residual guard of initial_guess
+         (run_base.py:786-808) discards every guess.
+    Nothing else in the text changes."""
+    out, n = [], 0
+    pat = re.compile(r"^(\s*)self\.arakawa\.poisson_bracket_array\((.*)\)\s*$")
+    for ln in src.split("\n"):
+        m = pat.match(ln)
+        if m:
+            ind, args = m.group(1), [a.strip() for a in _split_args(m.group(2))]
+            assert len(args) == 4 and args[3] == "1.0", ln
+            x, y, h = args[0], args[1], args[2]
+            out.append("%s%s[:,:] = 0." % (ind, y))
+            out.append("%sself.arakawa.poisson_bracket_array(%s, %s, %s, -1.0)" % (ind, x, h, y))
+            n += 1
+        else:
+            out.append(ln)
+    assert n > 0
+    return "\n".join(out)
+
+
+def load_fixed(relpath: str, ns: dict) -> dict:
+    with open(os.path.join(REF, relpath)) as fh:
+        code = decythonize(fix_explicit(fh.read()))
+    exec(compile(code, "ref:" + relpath, "exec"), ns)
+    return ns
+
+
 def extract_method(relpath: str, name: str) -> str:
     with open(os.path.join(REF, relpath)) as fh:
         lines = fh.read().split("\n")
@@ -392,7 +432,23 @@ def reference_namespace():
     exec(extract_method("vlasov/solvers/preconditioner/TensorProductPotentialFast.pyx",
                         "formBandedPreconditionerMatrix"), pot)
     ns["formBandedPotential_fn"] = pot["formBandedPreconditionerMatrix"]
+    load("vlasov/solvers/explicit/PETScExplicitSolver.pyx", ns)
+    load_fixed("vlasov/solvers/explicit/PETScArakawaRungeKutta.pyx", ns)
+    load_fixed("vlasov/solvers/explicit/PETScArakawaSymplectic.pyx", ns)
     return ns
+
+
+def symplectic4_coefficients():
+    """run_base.py:887-898 (initial_guess_symplectic4)."""
+    fac2 = 2. ** (1. / 3.)
+    c1 = 0.5 / (2. - fac2)
+    c2 = c1 * (1. - fac2)
+    c3 = c2
+    c4 = c1
+    d1 = 1. / (2. - fac2)
+    d2 = - d1 * fac2
+    d3 = d1
+    return (c1, c2, c3, c4), (d1, d2, d3)
 
 
 # ---------------------------------------------------------------------------
@@ -551,6 +607,52 @@ def make_case(ns, nx, nv, L, vmin, vmax, ht, seed):
             Y2 = da1.createGlobalVec()
             solver.jacobian(Fv, Y2)
             out["jvp_%s_db_%s" % (scheme, db)] = vec_to_2d(Y2, nx, nv)
+
+    # explicit predictors of the initial guess (run_base.py:173-181 option
+    # table, :811-912 the initial_guess_* sequences; the classes with the
+    # corrections of fix_explicit), kinetic h0, potential h1h + h2h with a
+    # nonzero h2, on a positive field; niter = initial_iter = 1 and 2
+    Fpr = np.abs(F) + 0.1
+    out["pred_F"] = Fpr
+    h2x = 0.05 * np.cos(2 * np.pi * xg / L + 0.3)
+    H2x = da1.createGlobalVec()
+    H2x.a[:] = np.tile(h2x, nv)
+    out["pred_h2"] = h2x
+    for scheme in ("arakawaj4", "simpson"):
+        for niter in (1, 2):
+            S = ns["PETScArakawaSymplectic"](Config(scheme), da1, grid, H0, H1h, H2x, niter)
+            if niter == 1:
+                X = to_vec(Fpr)
+                S.kinetic(X, 0.5)
+                out["pred_kinetic_" + scheme] = vec_to_2d(X, nx, nv)
+                X = to_vec(Fpr)
+                S.potential(X, 1.0)
+                out["pred_potential_" + scheme] = vec_to_2d(X, nx, nv)
+            X = to_vec(Fpr)
+            for _ in range(niter):           # run_base.py:866-877
+                S.kinetic(X, 0.5)
+                S.potential(X, 1.0)
+                S.kinetic(X, 0.5)
+            out["pred_symplectic2_%s_n%d" % (scheme, niter)] = vec_to_2d(X, nx, nv)
+            (c1, c2, c3, c4), (d1, d2, d3) = symplectic4_coefficients()
+            X = to_vec(Fpr)
+            for _ in range(niter):           # run_base.py:900-912
+                S.kinetic(X, c1)
+                S.potential(X, d1)
+                S.kinetic(X, c2)
+                S.potential(X, d2)
+                S.kinetic(X, c3)
+                S.potential(X, d3)
+                S.kinetic(X, c4)
+            out["pred_symplectic4_%s_n%d" % (scheme, niter)] = vec_to_2d(X, nx, nv)
+            RK = ns["PETScArakawaRungeKutta"](Config(scheme), da1, grid, H0, H1h, H2x, niter)
+            # the local work vectors the RK methods use and the base class never creates
+            RK.localX, RK.localX1, RK.localX2, RK.localX3 = (da1.createLocalVec() for _ in range(4))
+            for meth in ("rk4_16", "rk4_18"):
+                X = to_vec(Fpr)
+                for _ in range(niter):
+                    getattr(RK, meth)(X, H1h)
+                out["pred_%s_%s_n%d" % (meth, scheme, niter)] = vec_to_2d(X, nx, nv)
 
     # moments (Toolbox.pyx:79-165)
     N, U, E, A = (dax.createGlobalVec() for _ in range(4))

@@ -295,7 +295,7 @@ def test_step_every_kernel_shape(monkeypatch, precision):
             if precision == "fp64":
                 assert rep["picard_its"] == orep.picard_its, (picked, rep, orep.picard_its)
         if precision == "fp64":
-            assert rel(host(run.fc), orun.fc) < 1e-10, picked
+            assert rel(host(run.fc), orun.fc) < STEP_TOL, picked
         fe = run.invariants()["field_energy"]
         assert abs(fe - ofe) <= 1e-9 * abs(ofe), (picked, fe, ofe)
     assert tried >= 40
@@ -439,7 +439,8 @@ BATCH_SPECS = [(64, 128, vo.f0_landau(0.1, 0.5), 4 * np.pi, 0.1),
                (64, 512, vo.f0_bump_on_tail(0.04, 0.3), 2 * np.pi / 0.3, 0.1)]
 
 
-@pytest.mark.parametrize("shape", [None, "2,1,0", "8,2,1", "4,0,1", "2,0,0,1", "2,1,0,1", "4,0,1,0,1"])
+@pytest.mark.parametrize("shape", [None, "2,1,0", "8,2,1", "4,0,1", "2,0,0,1", "2,1,0,1", "2,2,0,1", "2,3,0,1",
+                                   "4,0,1,0,1"])
 def test_batch_step_equals_single_steps(monkeypatch, shape):
     """A lockstep batch of uneven instances (every kernel launched once for
     the table, per-instance masks) follows each instance's own time step:
@@ -461,7 +462,7 @@ def test_batch_step_equals_single_steps(monkeypatch, shape):
     assert batch.launch_count() > 0
 
 
-@pytest.mark.parametrize("shape", ["4,0,0", "4,1,1", "2,0,0,1", "2,1,0,1", "2,1,0,1,1"])
+@pytest.mark.parametrize("shape", ["4,0,0", "4,1,1", "2,0,0,1", "2,1,0,1", "2,3,0,1", "2,1,0,1,1"])
 def test_batch_graph_equals_host_driven(monkeypatch, shape):
     """The batch graph (conditional loops folded over the instance masks)
     and the host-driven loop over the same kernels (one fixed shape) give
@@ -516,7 +517,7 @@ def test_batch_sweep_instances_match_single_steps():
             _assert_batch_matches(rb[i], r.step(), br[i].fc, r.fc, i, 1e-9)
 
 
-@pytest.mark.parametrize("shape", [None, "4,0,1,0", "2,0,0,1", "2,1,0,1", "2,1,0,1,1"])
+@pytest.mark.parametrize("shape", [None, "4,0,1,0", "2,0,0,1", "2,1,0,1", "2,2,0,1", "2,3,0,1", "2,1,0,1,1"])
 def test_batch_mixed_precision_field_energy(monkeypatch, shape):
     """Batched mixed precision against FP64 single steps: field energy to
     1e-9 relative after three steps for every instance (autotuned, the
@@ -925,6 +926,11 @@ def test_averaged_jvp_wide_tiles(monkeypatch, avg):
 # round-off.  The tests stop above the floor, where every solve converges; the
 # Simpson average converges to round-off and keeps a tolerance of 1e-11.
 AVG_ATOL = {"midpoint": 1e-6, "arakawa_J4": 1e-6, "Simpson": 1e-11}
+# f after steps whose Picard and ksponly decisions all equal the oracle's
+# (checked by the tests that use it): the two then differ only by the
+# kernels' summation orders, measured at <= 2e-15 relative (max norm) over
+# every kernel variant on these grids; 1e-12 leaves a factor of 500
+STEP_TOL = 1e-12
 
 
 def kernel_shapes(nx, march=False):
@@ -1002,7 +1008,7 @@ def test_averaged_step_matches_oracle(monkeypatch, avg, scheme):
             rep = run.step()
             assert rep["picard_its"] == orep.picard_its, (picked, rep, orep.picard_its)
             assert all(k > 0 for k in rep["ksp_reason"]), (picked, rep)
-        assert rel(host(run.fc), ofc) < 1e-10, picked
+        assert rel(host(run.fc), ofc) < STEP_TOL, picked
     assert tried >= 17
 
 

@@ -264,3 +264,56 @@ def test_poisson_operator_variants(golden, laplace):
     phi = vo.poisson_solve(n, g, -1.0, laplace)
     r = vo.poisson_function(phi, n, g.hx2_inv, -1.0, laplace)
     assert np.max(np.abs(r)) < 1e-12 * max(1.0, np.max(np.abs(golden["poisson_rhs"])))
+
+
+@pytest.mark.parametrize("scheme", ["arakawaj4", "simpson"])
+def test_explicit_predictors_bitexact(golden, scheme):
+    """The predictors of the initial guess (symplectic2/4, rk4_16/18, one and
+    two iterations, and the kinetic / potential substeps) equal the
+    reference's explicit classes run with the corrections make_golden.py
+    names (argument order, zeroed work vectors, sign), bit for bit."""
+    g = _grid(golden)
+    h0v, h1h, h2 = golden["h0"][0], golden["h1h"][:, 0], golden["pred_h2"]
+    F = golden["pred_F"]
+    for n in (1, 2):
+        for m in ("symplectic2", "symplectic4", "rk4_16", "rk4_18"):
+            x = vo.predict(F, g, h0v, h1h, h2, scheme, m, n)
+            assert np.array_equal(x, golden["pred_%s_%s_n%d" % (m, scheme, n)]), (m, n)
+    h0 = np.broadcast_to(h0v[None, :], F.shape)
+    assert np.array_equal(vo.symplectic_substep(F, h0, 0.5, g, scheme, 1), golden["pred_kinetic_" + scheme])
+    hp = np.broadcast_to(h1h[:, None], F.shape) + np.broadcast_to(h2[:, None], F.shape)
+    assert np.array_equal(vo.symplectic_substep(F, hp, 1.0, g, scheme, 1), golden["pred_potential_" + scheme])
+
+
+def test_predictor_names():
+    """runspec.cfg:58 and run_base.py:173-181 spell the predictors 'rk4_16',
+    'rk4_18', 'symplectic2', 'symplectic4' and 'rk4' (the table key, whose
+    method calls rk18_J4: the 3/8 rule)."""
+    assert vo.PREDICTORS["rk4"] == "rk4_18"
+    for k in ("rk4_16", "rk4_18", "symplectic2", "symplectic4"):
+        assert vo.PREDICTORS[k] == k
+    c, d = vo.symplectic4_coefficients()
+    assert abs(sum(c) - 1.0) < 1e-15 and abs(sum(d) - 1.0) < 1e-15
+
+
+@pytest.mark.parametrize("method", ["symplectic2", "symplectic4", "rk4_16", "rk4"])
+def test_predicted_step_reaches_same_solution(method):
+    """A step with the predictor starts far closer to the solution (the guess
+    is kept: its residual is below the previous step's) and lands on the same
+    fixed point as the step without it, in fewer Picard passes."""
+    og = vo.Grid(32, 64, 4 * np.pi, 10.0, -10.0, ht=0.1)
+    f0 = vo.initialise_distribution_function(og, vo.f0_landau(0.2))
+    a = vo.Run(og, f0, ksp_rtol=1e-10, snes_atol=1e-11)
+    b = vo.Run(og, f0, ksp_rtol=1e-10, snes_atol=1e-11, initial_guess=method)
+    # the first step: the solver's Have is still the zero vector of its
+    # construction, so the residual before the guess is that of a zero
+    # Hamiltonian with Fh = f (round-off) and the guess is discarded
+    ra, rb = a.step(), b.step()
+    assert not rb.guess_kept and rb.guess_prev < 1e-12
+    assert rb.picard_its == ra.picard_its
+    for _ in range(2):
+        ra, rb = a.step(), b.step()
+        assert rb.guess_kept and rb.guess < 0.25 * rb.guess_prev
+        assert rb.residuals[0] < 0.25 * ra.residuals[0]
+        assert rb.picard_its < ra.picard_its
+    assert relerr(b.fc, a.fc) < 1e-10

@@ -565,6 +565,8 @@ void smem_attributes(int optin, int& lowest, cudaError_t& e) {
     set((const void*)vv::k_b_irfftj<R, R>);
     set((const void*)vv::k_b_tridiagj<R>);
     set((const void*)vv::k_b_tridiagjs<R>);
+    set((const void*)vv::k_b_tridiagjm<R, 2>);
+    set((const void*)vv::k_b_tridiagjm<R, 4>);
 }
 
 // dynamic shared memory of the staged warp-per-mode tridiagonal solve
@@ -2298,6 +2300,7 @@ struct vv_batch {
                                  // 2 CTA per mode (tables through L1)
     size_t smem_tri_stage, smem_tri_plain, smem_tri_warp;
     size_t smem_tri_js;          // k_b_tridiagjs (padded warp slices)
+    size_t smem_tri_jm2, smem_tri_jm4;   // k_b_tridiagjm, 2 and 4 warps per mode
     int nvmax;                   // largest velocity grid of the table
     int smem_limit;              // dynamic shared memory per block available to the batch kernels
     double* wpart;               // device: per-warp partial sums of every instance
@@ -2371,6 +2374,12 @@ int b_tri(vv_batch* b, const int* L) {
         if (b->tri_kind == 1)
             return blaunch(b, vv::k_b_tridiagjs<T>, vv::F_MODES, 32 * vv::TRIW_WARPS, b->smem_tri_js, tab, L, b->n,
                            vv::tri_ws_slots(b->nvmax));
+        if (b->tri_kind == 2)
+            return blaunch(b, vv::k_b_tridiagjm<T, 2>, vv::F_MODES, 32 * vv::TRIW_WARPS * 2, b->smem_tri_jm2, tab, L,
+                           b->n, b->nvmax);
+        if (b->tri_kind == 3)
+            return blaunch(b, vv::k_b_tridiagjm<T, 4>, vv::F_MODES, 32 * vv::TRIW_WARPS * 4, b->smem_tri_jm4, tab, L,
+                           b->n, b->nvmax);
         return blaunch(b, vv::k_b_tridiagj<T>, vv::F_MODES, 32,
                        (size_t)64 * vv::TJ_RING * sizeof(typename Cplx<T>::type), tab, L, b->n);
     }
@@ -2646,7 +2655,7 @@ void b_shape(vv_batch* b, std::vector<vv::BInst>& tab, int R, int tri_kind, int 
         if (b->pcj) {
             const int rb = vv::fj_rows_of(c->M);
             I.cnt[vv::F_ROWS] = (c->nv + rb - 1) / rb;
-            I.cnt[vv::F_MODES] = tri_warp ? (c->nmodes + vv::TRIW_WARPS - 1) / vv::TRIW_WARPS : (c->nmodes + 31) / 32;
+            I.cnt[vv::F_MODES] = tri_kind >= 1 ? (c->nmodes + vv::TRIW_WARPS - 1) / vv::TRIW_WARPS : (c->nmodes + 31) / 32;
         }
         for (int f = 0; f < vv::NFAM; ++f) b->tot[f] += I.cnt[f];
         b->smem_rfft = std::max(b->smem_rfft, fft_smem(0, c->M, R, csz, false));
@@ -2664,6 +2673,14 @@ int b_apply_shape(vv_batch* b, const std::vector<vv::BInst>& tab) {
     TRY(b_ctrl(b, vv::BC_ALL, -1));
     CK(cudaStreamSynchronize(b->st));
     return VV_OK;
+}
+
+// whether tridiagonal variant tw (layout pj) fits the device's shared memory
+bool b_tri_fits(const vv_batch* b, int tw, int pj) {
+    size_t need = 0;
+    if (pj) need = tw == 1 ? b->smem_tri_js : tw == 2 ? b->smem_tri_jm2 : tw == 3 ? b->smem_tri_jm4 : 0;
+    else if (tw == 1) need = b->smem_tri_warp;
+    return need <= (size_t)b->smem_limit;
 }
 
 // Batch autotuner: times the whole-table preconditioner (the step's largest
@@ -2715,8 +2732,8 @@ int b_autotune(vv_batch* b, std::vector<vv::BInst>& tab) {
     int bR = b->R, bW = b->tri_kind, bF = b->fft4, bJ = b->pcj, r = VV_OK;
     for (int pj = 0; pj <= (b->pcj_ok ? 1 : 0) && r == VV_OK; ++pj)
     for (int f4 = 0; f4 <= (pj ? 0 : 1) && r == VV_OK; ++f4)
-    for (int tw = 0; tw <= (pj ? 1 : 2) && r == VV_OK; ++tw) {
-        if (tw == 1 && (pj ? b->smem_tri_js : b->smem_tri_warp) > (size_t)b->smem_limit) continue;
+    for (int tw = 0; tw <= (pj ? 3 : 2) && r == VV_OK; ++tw) {
+        if (!b_tri_fits(b, tw, pj)) continue;
         for (int R = 2; R <= (pj ? 2 : 8) && r == VV_OK; R *= 2) {
             b_shape(b, tab, R, tw, f4, pj);
             if ((r = b_apply_shape(b, tab)) != VV_OK) break;
@@ -2883,6 +2900,8 @@ int vv_batch_create(int n, vv_ctx* const* ctxs, const vv_state* states, vv_batch
             b->smem_tri_warp = std::max(b->smem_tri_warp, tri_ws_smem(c->nv, b->mixed ? sizeof(float2) : sizeof(double2)));
             b->nvmax = std::max(b->nvmax, c->nv);
             b->smem_tri_js = vv::tri_js_smem(b->nvmax, b->mixed ? sizeof(float2) : sizeof(double2));
+            b->smem_tri_jm2 = vv::tri_jm_smem(b->nvmax, b->mixed ? sizeof(float2) : sizeof(double2), 2);
+            b->smem_tri_jm4 = vv::tri_jm_smem(b->nvmax, b->mixed ? sizeof(float2) : sizeof(double2), 4);
         }
         b->smem_pois = std::max(b->smem_pois, c->smem_pois);
     }
@@ -2962,9 +2981,8 @@ int vv_batch_create(int n, vv_ctx* const* ctxs, const vv_state* states, vv_batch
         const char* bs = getenv("VV_BATCH_SHAPE");
         int fR = 0, fT = 0, fF = 0, fJ = 0, fM = 0;
         const int nf = bs ? sscanf(bs, "%d,%d,%d,%d,%d", &fR, &fT, &fF, &fJ, &fM) : 0;
-        const bool fixed = nf >= 3 && (fR == 2 || fR == 4 || fR == 8) && fT >= 0 && fT <= 2 && (fF == 0 || fF == 1) &&
-                           (fJ == 0 || (fJ == 1 && b->pcj_ok)) &&
-                           !(fT == 1 && (fJ ? b->smem_tri_js : b->smem_tri_warp) > (size_t)b->smem_limit);
+        const bool fixed = nf >= 3 && (fR == 2 || fR == 4 || fR == 8) && fT >= 0 && fT <= (fJ ? 3 : 2) &&
+                           (fF == 0 || fF == 1) && (fJ == 0 || (fJ == 1 && b->pcj_ok)) && b_tri_fits(b, fT, fJ);
         const char* at = getenv("VV_AUTOTUNE");
         if (fixed) {
             b->march = fM != 0;

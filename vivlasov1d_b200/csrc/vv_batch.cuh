@@ -835,4 +835,164 @@ __global__ void k_b_gather_states(const BInst* __restrict__ tab, int words, unsi
     for (int w = threadIdx.x; w < words; w += blockDim.x) dst[w] = src[w];
 }
 
+// ---- LU solves on the v-major layout, W warps per mode ------------------------
+// k_b_tridiagjs with each mode's line split over W warps instead of one: lane
+// l of sub-warp s owns the chunk c = 32 s + l of CH = ceil(nv / 32 W) rows, so
+// the sequential chunk sweeps are W times shorter and a CTA of 4 modes runs
+// 4 W warps on the same staged lines.  The chunks' affine maps are joined by
+// a warp scan and then across the W sub-warps through shared memory.  Slot
+// of row r: r + r / CH (one pad per chunk; CH + 1 odd for power-of-two lines,
+// so the chunk-strided accesses are conflict-free).
+__host__ __device__ constexpr int tri_jm_slots(int nv, int W) { return nv + 32 * W; }
+__host__ __device__ constexpr size_t tri_jm_smem(int nvmax, size_t csz, int W) {
+    return (size_t)TRIW_WARPS * (2 * tri_jm_slots(nvmax, W) + TRIJS_PAD) * csz +
+           2 * (size_t)tri_jm_slots(nvmax, W) * (csz / 2);
+}
+
+// inclusive warp scan of affine maps in `forward` lane order; *ex gets the
+// exclusive prefix (identity for the first lane)
+template <typename C>
+__device__ __forceinline__ Aff<C> warp_scan_aff_ie(Aff<C> a, bool forward, Aff<C>* ex) {
+    const int lane = threadIdx.x & 31;
+    const int pos = forward ? lane : 31 - lane;
+    Aff<C> inc = a;
+#pragma unroll
+    for (int d = 1; d < 32; d <<= 1) {
+        const Aff<C> o = shfl_aff(inc, d, forward);
+        if (pos >= d) inc = aff_combine(o, inc);
+    }
+    const Aff<C> prev = shfl_aff(inc, 1, forward);
+    if (pos > 0) *ex = prev;
+    else {
+        ex->P = c_make<C>(1.0, 0.0);
+        ex->Q = c_make<C>(0.0, 0.0);
+    }
+    return inc;
+}
+
+template <typename R, int W>
+__global__ void __launch_bounds__(32 * TRIW_WARPS * W) k_b_tridiagjm(const BInst* __restrict__ tab,
+                                                                    const int* __restrict__ L, int n, int nsmax) {
+    using C = typename Cplx<R>::type;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    __shared__ Aff<C> tot[2][TRIW_WARPS][W];
+    for_work<F_MODES>(tab, L, n, [&](const BInst& I, int local) {
+        const int nv = I.tp.nv, nm = I.tp.nmodes;
+        const int CH = (nv + 32 * W - 1) / (32 * W);
+        const int ns = tri_jm_slots(nv, W);
+        const int wid = threadIdx.x >> 5, lane = threadIdx.x & 31;
+        const int m = wid / W, sw = wid % W;        // mode of the CTA's item, sub-warp within the mode
+        const int k0 = local * TRIW_WARPS;
+        const int ws = 2 * ns + TRIJS_PAD;
+        C* base = reinterpret_cast<C*>(smem_raw);
+        R* sal = reinterpret_cast<R*>(base + (size_t)TRIW_WARPS * (2 * tri_jm_slots(nsmax, W) + TRIJS_PAD));
+        R* sga = sal + ns;
+        C* spec = (C*)I.specT;
+        const C* dj = (const C*)I.dinvJ;
+        const FastDiv dch((unsigned)CH);
+        {
+            const R* al = reinterpret_cast<const R*>(I.tp.alpha);
+            const R* ga = reinterpret_cast<const R*>(I.tp.gamma);
+            for (int r = threadIdx.x; r < nv; r += blockDim.x) {
+                const int q = r + (int)dch((unsigned)r);
+                cp_async_elem(&sal[q], &al[r]);
+                cp_async_elem(&sga[q], &ga[r]);
+            }
+        }
+        for (int t = threadIdx.x; t < nv * TRIW_WARPS; t += blockDim.x) {
+            const int j = t / TRIW_WARPS, mm = t % TRIW_WARPS;
+            const int k = k0 + mm;
+            if (k < nm) {
+                C* sb = base + (size_t)mm * ws;
+                const int q = j + (int)dch((unsigned)j);
+                cp_async_elem(&sb[q], &spec[(size_t)j * nm + k]);
+                cp_async_elem(&sb[ns + q], &dj[(size_t)j * nm + k]);
+            }
+        }
+        cp_async_commit();
+        cp_async_wait0();
+        __syncthreads();
+        const bool on = k0 + m < nm;
+        C* sb = base + (size_t)m * ws;
+        const C* sd = sb + ns;
+        const C lam = on ? reinterpret_cast<const C*>(I.tp.lambda)[k0 + m] : c_make<C>(0.0, 0.0);
+        const int chunk = sw * 32 + lane;
+        const int r0 = chunk * CH;
+        const int r1 = min(r0 + CH, nv);
+        const int q0 = chunk * (CH + 1);
+        // forward: y_r = b_r - l_r y_{r-1},  l_r = lambda alpha_r / U_{r-1}
+        Aff<C> a;
+        a.P = c_make<C>(1.0, 0.0);
+        a.Q = c_make<C>(0.0, 0.0);
+        if (on)
+            for (int r = r0, q = q0; r < r1; ++r, ++q) {
+                Aff<C> mp;
+                if (r == 0) mp.P = c_make<C>(0.0, 0.0);
+                else {
+                    const C dprev = sd[(r == r0) ? q - 2 : q - 1];   // row r0-1 sits before the previous pad slot
+                    const C l = c_mul(c_rmul(lam, sal[q]), dprev);
+                    mp.P = c_make<C>(-l.x, -l.y);
+                }
+                mp.Q = sb[q];
+                a = aff_combine(a, mp);
+            }
+        Aff<C> ex;
+        Aff<C> inc = warp_scan_aff_ie<C>(a, true, &ex);
+        if (lane == 31) tot[0][m][sw] = inc;
+        __syncthreads();
+        Aff<C> pre;
+        pre.P = c_make<C>(1.0, 0.0);
+        pre.Q = c_make<C>(0.0, 0.0);
+        for (int u = 0; u < sw; ++u) pre = aff_combine(pre, tot[0][m][u]);
+        C y = aff_combine(pre, ex).Q;
+        if (on)
+            for (int r = r0, q = q0; r < r1; ++r, ++q) {
+                const C b = sb[q];
+                if (r == 0) y = b;
+                else {
+                    const C dprev = sd[(r == r0) ? q - 2 : q - 1];
+                    const C l = c_mul(c_rmul(lam, sal[q]), dprev);
+                    y = c_sub(b, c_mul(l, y));
+                }
+                sb[q] = y;
+            }
+        // backward: x_r = U_r^-1 (y_r - c_r x_{r+1}) == mu_r + nu_r x_{r+1}; each lane reads its own chunk only
+        a.P = c_make<C>(1.0, 0.0);
+        a.Q = c_make<C>(0.0, 0.0);
+        if (on)
+            for (int r = r1 - 1, q = q0 + (r1 - 1 - r0); r >= r0; --r, --q) {
+                Aff<C> mp;
+                const C d = sd[q];
+                mp.Q = c_mul(d, sb[q]);
+                if (r == nv - 1) mp.P = c_make<C>(0.0, 0.0);
+                else {
+                    const C nu = c_mul(d, c_rmul(lam, sga[q]));
+                    mp.P = c_make<C>(-nu.x, -nu.y);
+                }
+                a = aff_combine(a, mp);
+            }
+        inc = warp_scan_aff_ie<C>(a, false, &ex);
+        if (lane == 0) tot[1][m][sw] = inc;
+        __syncthreads();
+        pre.P = c_make<C>(1.0, 0.0);
+        pre.Q = c_make<C>(0.0, 0.0);
+        for (int u = W - 1; u > sw; --u) pre = aff_combine(pre, tot[1][m][u]);
+        C x = aff_combine(pre, ex).Q;
+        if (on)
+            for (int r = r1 - 1, q = q0 + (r1 - 1 - r0); r >= r0; --r, --q) {
+                const C d = sd[q];
+                if (r == nv - 1) x = c_mul(d, sb[q]);
+                else x = c_mul(d, c_sub(sb[q], c_mul(c_rmul(lam, sga[q]), x)));
+                sb[q] = x;
+            }
+        __syncthreads();
+        for (int t = threadIdx.x; t < nv * TRIW_WARPS; t += blockDim.x) {
+            const int j = t / TRIW_WARPS, mm = t % TRIW_WARPS;
+            const int k = k0 + mm;
+            if (k < nm) spec[(size_t)j * nm + k] = base[(size_t)mm * ws + j + (int)dch((unsigned)j)];
+        }
+        __syncthreads();
+    });
+}
+
 }  // namespace vv
