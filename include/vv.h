@@ -89,6 +89,19 @@ enum vv_double_bracket {     /* solver.bracket_operator with dissipation_type
     VV_DOUBLE_BRACKET_FFH = 1,  /* DoubleBracketFFH: DoubleBracket.pyx:67-83   */
     VV_DOUBLE_BRACKET_FHH = 2   /* DoubleBracketFHH: DoubleBracket.pyx:86-97   */
 };
+enum vv_initial_guess {      /* solver.initial_guess: the explicit predictor of
+                                the step's first iterate (run_base.py:173-181,
+                                786-912; runspec.cfg:58 names)                 */
+    VV_GUESS_NONE = 0,
+    VV_GUESS_SYMPLECTIC2 = 1,   /* 'symplectic2': PETScArakawaSymplectic.pyx:62-92
+                                   kinetic 1/2, potential 1, kinetic 1/2       */
+    VV_GUESS_SYMPLECTIC4 = 2,   /* 'symplectic4': the 4th-order composition of
+                                   run_base.py:887-912                         */
+    VV_GUESS_RK4_16 = 3,        /* 'rk4_16': PETScArakawaRungeKutta.pyx:20-58   */
+    VV_GUESS_RK4_18 = 4         /* 'rk4_18' and the option key 'rk4' (whose
+                                   method calls the undefined rk18_J4):
+                                   PETScArakawaRungeKutta.pyx:61-100, 3/8 rule */
+};
 enum vv_order {              /* arithmetic of the bracket kernels             */
     VV_ORDER_FACTORED = 0,   /* separable-h coefficient form (fast, default)   */
     VV_ORDER_REFERENCE = 1   /* the reference loop's operation order, no FMA   */
@@ -149,6 +162,19 @@ typedef struct vv_grid {
                                 uses the Fave of the last residual evaluation
                                 (vv_function / the step's residual).  Single
                                 runs only.                                    */
+    int32_t initial_guess;   /* enum vv_initial_guess (0: none).  The
+                                explicit classes of the reference compute no
+                                bracket step as written; the predictor here
+                                calls the bracket with the arguments in the
+                                order of its signature (PoissonBracket.pyx:80;
+                                the classes pass (x, y, h)), on cleared work
+                                vectors, and with the sign of the implicit
+                                residual, df/dt = -[f, h] (with the classes'
+                                sign it steps backwards in time and the guard
+                                discards every guess).  Single runs only (not
+                                in vv_batch_create).                          */
+    int32_t initial_iter;    /* runspec initial_iter: predictor iterations of
+                                ht/initial_iter each (<= 0: 1)                */
 } vv_grid;
 
 typedef struct vv_ctx vv_ctx;
@@ -278,6 +304,9 @@ typedef struct vv_step_report {
     int32_t gmres_its[VV_MAX_PICARD];
     int32_t ksp_reason[VV_MAX_PICARD];
     double  residual[VV_MAX_PICARD + 1]; /* residual before/after each pass  */
+    int32_t guess_kept;      /* initial guess: 1 if the predicted f was kept  */
+    double  guess_prev;      /* residual before the predictor                 */
+    double  guess_residual;  /* residual of the predicted f                   */
 } vv_step_report;
 /* Initial set-up of a run: optionally normalise f so that sum(f)*hv/nx == 1
  * (run_base.py:623-628), then moments, Poisson and h1 (run_base.py:506). */
@@ -286,10 +315,26 @@ int vv_run_init(vv_ctx* ctx, vv_state* st, int normalise);
 int vv_calculate_moments(vv_ctx* ctx, vv_state* st);
 /* calculate_residual: ||R(f)||_2 + ||Poisson residual||_2 (run_base.py:631-637). */
 int vv_calculate_residual(vv_ctx* ctx, vv_state* st, double* residual);
-/* One implicit time step: make_history, update_previous, Picard loop with
- * one ksponly GMRES solve per pass, revert/stop/abort rules. */
+/* One implicit time step: make_history, the initial guess (when the grid
+ * names a predictor), update_previous, Picard loop with one ksponly GMRES
+ * solve per pass, revert/stop/abort rules. */
 int vv_step(vv_ctx* ctx, vv_state* st, const vv_snes_opts* snes,
             const vv_ksp_opts* ksp, vv_step_report* report);
+/* The predictor alone: Y = the grid's initial_guess method applied to F over
+ * initial_iter iterations of ht/initial_iter, with H0, the history profiles
+ * h1h and h2h (NULL: zero) and the grid's bracket in the reference's
+ * operation order (PETScArakawaSymplectic.pyx:62-92,
+ * PETScArakawaRungeKutta.pyx:20-100, run_base.py:811-912).  Y may alias F.
+ * VV_ERR_ARG if the grid names no predictor. */
+int vv_predict(vv_ctx* ctx, const double* F, const double* h1h, const double* h2h, double* Y);
+/* initial_guess (run_base.py:786-808) on a state whose history is set
+ * (after make_history): the residual of st->f (with the solver's Have of the
+ * last update_previous, zero before the first), the predictor, moments, the
+ * residual of the prediction; the prediction is kept unless its residual is
+ * larger, else st->f is restored and its moments recomputed (the reference
+ * keeps the prediction's potential there).  Host scalars: the two residuals
+ * and whether the prediction was kept. */
+int vv_initial_guess(vv_ctx* ctx, vv_state* st, double* prev, double* guess, int32_t* kept);
 
 /* ---- batched sweep: many independent runs in lockstep -------------------- */
 /* The reference runs one instance per process; a parameter sweep is many

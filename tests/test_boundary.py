@@ -119,17 +119,33 @@ hdf5_output = twostream_test.hdf5"
 
 
 def test_run_refuses_reference_failure_modes():
-    """Options whose reference path fails (an initial-guess predictor, a
-    nonzero regularisation) are refused when the run is built, before any
-    device work."""
+    """Options whose reference path fails or is not on this path (a
+    multistep initial-guess predictor, an unknown predictor name, a nonzero
+    regularisation, a method other than the nonlinear matrix-free runscript)
+    are refused when the run is built, before any device work."""
     from vivlasov1d_b200.run import Run
     base = {"grid": {"nx": 16, "nv": 32, "L": 12.566370614359172, "vmin": -8.0, "vmax": 8.0, "ht": 0.1, "nt": 1},
             "solver": {"method": "matrixfree"}, "initial_data": {"charge": -1.0}}
-    for key, val in (("initial_guess", "rk4"), ("initial_guess", "rk4_16"), ("regularisation", 1e-3)):
+    for key, val, exc in (("initial_guess", "gear2", NotImplementedError), ("initial_guess", "leapfrog",
+                                                                           NotImplementedError),
+                          ("initial_guess", "rk17", ValueError), ("regularisation", 1e-3, NotImplementedError),
+                          ("method", "iterative", NotImplementedError), ("method", "direct", NotImplementedError),
+                          ("type", "linear", NotImplementedError)):
         cfg = {k: dict(v) for k, v in base.items()}
         cfg["solver"][key] = val
-        with pytest.raises(NotImplementedError):
+        with pytest.raises(exc):
             Run(cfg)
+
+
+def test_initial_guess_names():
+    """The predictors by the names of runspec.cfg:58 and the option key 'rk4'
+    of run_base.py:173-181 (whose method, rk18_J4, is the 3/8 rule)."""
+    from vivlasov1d_b200 import _lib
+    assert _lib.initial_guess_code(None) == _lib.initial_guess_code("None") == 0
+    assert _lib.initial_guess_code("symplectic2") == 1 and _lib.initial_guess_code("symplectic4") == 2
+    assert _lib.initial_guess_code("rk4_16") == 3
+    assert _lib.initial_guess_code("rk4_18") == _lib.initial_guess_code("rk4") == 4
+    assert _lib.initial_guess_code(4) == 4
 
 
 def test_config_dissipation_choices():

@@ -44,6 +44,29 @@ def averaging_code(name):
         return AVERAGING[str(name).lower()]
     raise ValueError("unknown averaging operator %r (TimeDerivative.create knows %s)"
                      % (name, sorted(AVERAGING)))
+# the predictor of the initial guess by the names of runspec.cfg:58 and the
+# option table of run_base.py:173-181 ('rk4' calls rk18_J4: the 3/8 rule)
+INITIAL_GUESS = {"symplectic2": 1, "symplectic4": 2, "rk4_16": 3, "rk4_18": 4, "rk4": 4}
+
+
+def initial_guess_code(name):
+    """vv_initial_guess code of a runspec initial_guess value.  None/''/'None'
+    is no predictor.  The Gear and leapfrog predictors ('gear', 'gear2-4',
+    'leapfrog') step from the history of earlier time levels and are not on
+    this path; other names are not predictors of the reference."""
+    if name in (None, "", "None", "none"):
+        return 0
+    if isinstance(name, int) and name in INITIAL_GUESS.values():
+        return name
+    key = str(name).lower()
+    if key in INITIAL_GUESS:
+        return INITIAL_GUESS[key]
+    if key.startswith("gear") or key == "leapfrog":
+        raise NotImplementedError("initial_guess %r: the multistep (Gear, leapfrog) predictors are not on this "
+                                  "path" % name)
+    raise ValueError("unknown initial_guess %r (known: %s)" % (name, sorted(INITIAL_GUESS)))
+
+
 ORDER_FACTORED, ORDER_REFERENCE = 0, 1
 PRECISION = {"fp64": 0, "mixed": 1}
 MAX_PICARD = 64
@@ -60,7 +83,7 @@ class vv_grid(C.Structure):
                 ("order", C.c_int32), ("gmres_restart", C.c_int32), ("precision", C.c_int32),
                 ("mixed_rtol", C.c_double), ("averaging", C.c_int32), ("collision", C.c_int32),
                 ("coll_freq", C.c_double), ("coll_diff", C.c_double), ("coll_drag", C.c_double),
-                ("double_bracket", C.c_int32)]
+                ("double_bracket", C.c_int32), ("initial_guess", C.c_int32), ("initial_iter", C.c_int32)]
 
 
 class vv_ksp_opts(C.Structure):
@@ -86,7 +109,8 @@ class vv_step_report(C.Structure):
     _fields_ = [("picard_its", C.c_int32), ("gmres_its_total", C.c_int32), ("reverted", C.c_int32),
                 ("stop_rule", C.c_int32), ("ksp_failures", C.c_int32), ("aborted", C.c_int32),
                 ("gmres_its", C.c_int32 * MAX_PICARD), ("ksp_reason", C.c_int32 * MAX_PICARD),
-                ("residual", C.c_double * (MAX_PICARD + 1))]
+                ("residual", C.c_double * (MAX_PICARD + 1)), ("guess_kept", C.c_int32),
+                ("guess_prev", C.c_double), ("guess_residual", C.c_double)]
 
 
 INVARIANT_NAMES = ("mass", "L1", "L2", "L3", "L4", "L5", "L6", "L8", "Lmin", "Lmax", "entropy",
@@ -139,6 +163,8 @@ SIGNATURES = {
     "vv_launch_count": (I, [P, C.POINTER(C.c_int64), I]),
     "vv_time_kernel": (I, [P, I, I, C.POINTER(D)]),
     "vv_kernel_shape": (I, [P, C.POINTER(C.c_int32)]),
+    "vv_predict": (I, [P, P, P, P, P]),
+    "vv_initial_guess": (I, [P, C.POINTER(vv_state), C.POINTER(D), C.POINTER(D), C.POINTER(C.c_int32)]),
     "vv_batch_create": (I, [I, C.POINTER(P), C.POINTER(vv_state), C.POINTER(P)]),
     "vv_batch_destroy": (I, [P]),
     "vv_batch_set_stream": (I, [P, P]),

@@ -18,7 +18,7 @@ INCLUDE = os.path.join(ROOT, "include")
 LIB = os.path.join(HERE, "libvv.so")
 
 SOURCES = ["vv_api.cu", "vv_noalloc.cu"]
-HEADERS = ["vv_common.cuh", "vv_bracket.cuh", "vv_pc.cuh", "vv_pcj.cuh", "vv_pcv.cuh", "vv_coll.cuh", "vv_vec.cuh", "vv_batch.cuh", "vv_adjoint.cuh"]
+HEADERS = ["vv_common.cuh", "vv_bracket.cuh", "vv_pc.cuh", "vv_pcj.cuh", "vv_pcv.cuh", "vv_coll.cuh", "vv_vec.cuh", "vv_batch.cuh", "vv_adjoint.cuh", "vv_pred.cuh"]
 
 NVCC_FLAGS = [
     "-O3", "-std=c++17",

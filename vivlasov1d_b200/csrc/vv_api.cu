@@ -16,6 +16,7 @@
 #include "vv_adjoint.cuh"
 #include "vv_pcv.cuh"
 #include "vv_coll.cuh"
+#include "vv_pred.cuh"
 
 #include <algorithm>
 #include <array>
@@ -54,6 +55,11 @@ struct vv_ctx {
     int db;
     double db_nu;
     double *db_fave, *db_b;
+    // explicit predictor of the initial guess (vv_pred.cuh): method, iterations,
+    // h fields (kinetic, potential or RK), bracket output, RK stages, stage
+    // input, the saved iterate, collision-only residual partials
+    int pred, pred_iter;
+    double *pred_H, *pred_Hp, *pred_Y, *pred_K, *pred_S, *pred_fl, *pred_cpart;
     // the potential preconditioner (VV_PC_TENSOR_POTENTIAL): v modes, eigenvalues
     // for n = nv, nv twiddles, transposed field, v spectrum, elimination
     // scratch (FP32 copies in the mixed mode), rows per CTA of the v FFT, phi
@@ -1148,6 +1154,119 @@ int step_residual(vv_ctx* c, vv_state* st, int phase) {
     return VV_OK;
 }
 
+// ---- explicit predictors of the initial guess (vv_pred.cuh) ------------------
+// Y = -[X, H] (zeroed first) in the reference-order kernels with a general h
+int pred_bracket(vv_ctx* c, const double* X, const double* H, double* Y) {
+    CK(cudaMemsetAsync(Y, 0, c->ncell * sizeof(double), c->st));
+    return launch_bracket_gen(c, X, nullptr, Y, H, -1.0, nullptr);
+}
+
+// kinetic / potential substep: X += factor * ht / niter * (-[X, H])
+int pred_substep(vv_ctx* c, double* X, const double* H, double factor) {
+    TRY(pred_bracket(c, X, H, c->pred_Y));
+    const double s = factor * c->g.ht / (double)c->pred_iter;
+    vv::k_pred_axpy<<<grid1d(c->ncell, 256), 256, 0, c->st>>>(X, c->pred_Y, s, c->ncell);
+    CKL(c);
+    return VV_OK;
+}
+
+// Y = the predictor applied to F (Y may alias F), with H0 and the history
+// profiles h1h, h2h (run_base.py:811-912)
+int pred_run(vv_ctx* c, const double* F, const double* h1h, const double* h2h, double* Y) {
+    const size_t n = c->ncell;
+    const int nx = c->nx, nv = c->nv;
+    const unsigned gr = grid1d(n, 256);
+    const double ht = c->g.ht, niter = (double)c->pred_iter;
+    TRY(copy_d(c, Y, F, n));
+    if (c->pred == VV_GUESS_SYMPLECTIC2 || c->pred == VV_GUESS_SYMPLECTIC4) {
+        vv::k_pred_hfield<<<gr, 256, 0, c->st>>>(c->h0, h1h, h2h, c->pred_H, nx, nv, 0);
+        vv::k_pred_hfield<<<gr, 256, 0, c->st>>>(c->h0, h1h, h2h, c->pred_Hp, nx, nv, 1);
+        CKL(c);
+        // run_base.py:887-898
+        const double fac2 = std::pow(2., 1. / 3.);
+        const double c1 = 0.5 / (2. - fac2), c2 = c1 * (1. - fac2);
+        const double d1 = 1. / (2. - fac2), d2 = -d1 * fac2;
+        for (int it = 0; it < c->pred_iter; ++it) {
+            if (c->pred == VV_GUESS_SYMPLECTIC2) {   // run_base.py:866-877
+                TRY(pred_substep(c, Y, c->pred_H, 0.5));
+                TRY(pred_substep(c, Y, c->pred_Hp, 1.0));
+                TRY(pred_substep(c, Y, c->pred_H, 0.5));
+            } else {                                // run_base.py:900-912
+                TRY(pred_substep(c, Y, c->pred_H, c1));
+                TRY(pred_substep(c, Y, c->pred_Hp, d1));
+                TRY(pred_substep(c, Y, c->pred_H, c2));
+                TRY(pred_substep(c, Y, c->pred_Hp, d2));
+                TRY(pred_substep(c, Y, c->pred_H, c2));
+                TRY(pred_substep(c, Y, c->pred_Hp, d1));
+                TRY(pred_substep(c, Y, c->pred_H, c1));
+            }
+        }
+        return VV_OK;
+    }
+    vv::k_pred_hfield<<<gr, 256, 0, c->st>>>(c->h0, h1h, h2h, c->pred_H, nx, nv, 2);
+    CKL(c);
+    double* K1 = c->pred_K;
+    double* K2 = K1 + n;
+    double* K3 = K2 + n;
+    double* K4 = K3 + n;
+    double* S = c->pred_S;
+    const double b = ht / niter;
+    for (int it = 0; it < c->pred_iter; ++it) {
+        TRY(pred_bracket(c, Y, c->pred_H, K1));
+        if (c->pred == VV_GUESS_RK4_16) {           // PETScArakawaRungeKutta.pyx:20-58
+            const double a = 0.5 * ht / niter;
+            vv::k_pred_stage<<<gr, 256, 0, c->st>>>(Y, K1, nullptr, nullptr, S, a, 0.0, 0, n);
+            TRY(pred_bracket(c, S, c->pred_H, K2));
+            vv::k_pred_stage<<<gr, 256, 0, c->st>>>(Y, K2, nullptr, nullptr, S, a, 0.0, 0, n);
+            TRY(pred_bracket(c, S, c->pred_H, K3));
+            vv::k_pred_stage<<<gr, 256, 0, c->st>>>(Y, K3, nullptr, nullptr, S, 1.0 * ht / niter, 0.0, 0, n);
+            TRY(pred_bracket(c, S, c->pred_H, K4));
+            vv::k_pred_rk_final<<<gr, 256, 0, c->st>>>(Y, K1, K2, K3, K4, b, 2., 6., n);
+        } else {                                    // PETScArakawaRungeKutta.pyx:61-100
+            const double a = 1. / 3. * ht / niter;
+            vv::k_pred_stage<<<gr, 256, 0, c->st>>>(Y, K1, nullptr, nullptr, S, a, 0.0, 0, n);
+            TRY(pred_bracket(c, S, c->pred_H, K2));
+            vv::k_pred_stage<<<gr, 256, 0, c->st>>>(Y, K1, K2, nullptr, S, a, b, 1, n);
+            TRY(pred_bracket(c, S, c->pred_H, K3));
+            vv::k_pred_stage<<<gr, 256, 0, c->st>>>(Y, K1, K2, K3, S, 0.0, b, 2, n);
+            TRY(pred_bracket(c, S, c->pred_H, K4));
+            vv::k_pred_rk_final<<<gr, 256, 0, c->st>>>(Y, K1, K2, K3, K4, b, 3., 8., n);
+        }
+        CKL(c);
+    }
+    return VV_OK;
+}
+
+// the guard's residual (phase 0: of the current f, 1: of the prediction)
+int pred_residual(vv_ctx* c, vv_state* st, int phase) {
+    const int tiles = bracket_tiles(c, st->f, c->Fh, c->tmp);
+    TRY(launch_bracket<vv::MODE_RESIDUAL, double>(c, st->f, c->Fh, c->tmp, 1.0, c->part));
+    TRY(poisson_apply(c, st->phi, st->n, nullptr, 2, &c->ds->pnorm2));
+    int ncp = 0;
+    if (phase == 0 && c->coll != vv::COLL_NONE) {
+        // what a zero Have leaves of R(f) with Fh = f: the collision terms
+        CK(cudaMemsetAsync(c->pred_Y, 0, c->ncell * sizeof(double), c->st));
+        TRY(launch_collision<double>(c, st->f, c->Fh, c->pred_Y, c->pred_cpart, nullptr));
+        ncp = ((c->nx + vv::BX - 1) / vv::BX) * ((c->nv + vv::BY - 1) / vv::BY);
+    }
+    vv::k_pred_norm<<<1, 32, 0, c->st>>>(c->ds, c->part, tiles, ncp ? c->pred_cpart : nullptr, ncp, phase);
+    CKL(c);
+    return VV_OK;
+}
+
+// initial_guess (run_base.py:786-808) after make_history, before update_previous
+int pred_guess(vv_ctx* c, vv_state* st) {
+    const size_t n = c->ncell;
+    TRY(copy_d(c, c->pred_fl, st->f, n));
+    TRY(pred_residual(c, st, 0));
+    TRY(pred_run(c, st->f, st->h1h, st->h2h, st->f));
+    TRY(calc_moments(c, st));
+    TRY(pred_residual(c, st, 1));
+    vv::k_pred_guard<<<grid1d(n, 256), 256, 0, c->st>>>(c->ds, st->f, c->pred_fl, n);
+    CKL(c);
+    return calc_moments(c, st);
+}
+
 // make_history + update_previous + initial residual
 int step_prologue(vv_ctx* c, vv_state* st) {
     const size_t n = c->ncell;
@@ -1165,6 +1284,7 @@ int step_prologue(vv_ctx* c, vv_state* st) {
         TRY(copy_d(c, c->mom_h + nx, st->u, nx));
         TRY(copy_d(c, c->mom_h + 2 * nx, st->a, nx));
     }
+    if (c->pred) TRY(pred_guess(c, st));
     TRY(set_hxp(c, st->h1c, st->h1h, st->h2c, st->h2h));
     return step_residual(c, st, 0);
 }
@@ -1425,6 +1545,11 @@ int fill_report(vv_ctx* c, const vv::DevState& d, int restart, vv_step_report* r
         rep->ksp_reason[k] = d.ksp_reason[k];
     }
     for (int k = 0; k <= np; ++k) rep->residual[k] = d.residual[k];
+    if (c->pred) {
+        rep->guess_kept = d.guess_kept;
+        rep->guess_prev = d.guess_prev;
+        rep->guess_residual = d.guess_res;
+    }
     (void)restart;
     if (c->use_graph && count_launches) {
         // kernels the graph executed: top level once, the Picard body per pass,
@@ -1516,6 +1641,7 @@ int vv_create(const vv_grid* grid, vv_ctx** out) {
     const int restart = g.gmres_restart > 0 ? g.gmres_restart : 30;
     if (restart > vv::MAX_RESTART) return VV_ERR_ARG;
     if (g.precision != VV_PRECISION_FP64 && g.precision != VV_PRECISION_MIXED) return VV_ERR_ARG;
+    if (g.initial_guess < VV_GUESS_NONE || g.initial_guess > VV_GUESS_RK4_18) return VV_ERR_ARG;
 
     vv_ctx* c = new vv_ctx();
     c->g = g;
@@ -1558,6 +1684,8 @@ int vv_create(const vv_grid* grid, vv_ctx** out) {
     // the double bracket (DoubleBracket.create, config.py:156-162: none unless coll_freq != 0)
     c->db = (g.double_bracket != VV_DOUBLE_BRACKET_NONE && g.coll_freq != 0.0) ? g.double_bracket : 0;
     c->db_nu = g.coll_freq;
+    c->pred = g.initial_guess;
+    c->pred_iter = g.initial_iter > 0 ? g.initial_iter : 1;
     {   // the Laplacian's stencil (matrix_mult of PETScPoissonCFD2/CFD4/Simpson.pyx; the Ave classes
         // keep CFD2's / Simpson's) and the density average of their formRHS (PETScPoissonCFD2Ave.pyx:
         // 0.25 (n_{i-1} + 2 n_i + n_{i+1}); PETScPoissonSimpsonAve.pyx: (n_{i-2} + 8 n_{i-1} + 18 n_i
@@ -1789,6 +1917,16 @@ int vv_create(const vv_grid* grid, vv_ctx** out) {
         vv_destroy(c);
         return fail_cuda(cudaGetLastError(), "vv_create upload (double bracket)");
     }
+    // the predictor's work fields
+    if (c->pred) {
+        const size_t ntile = (size_t)((nx + vv::BX - 1) / vv::BX) * ((nv + vv::BY - 1) / vv::BY);
+        if ((s = dalloc(&c->pred_H, n)) || (s = dalloc(&c->pred_Hp, n)) || (s = dalloc(&c->pred_Y, n)) ||
+            (s = dalloc(&c->pred_K, 4 * n)) || (s = dalloc(&c->pred_S, n)) || (s = dalloc(&c->pred_fl, n)) ||
+            (s = dalloc(&c->pred_cpart, ntile))) {
+            vv_destroy(c);
+            return s;
+        }
+    }
     // collisions: current / history moment profiles (n, U, a)
     if (c->coll != vv::COLL_NONE) {
         if ((s = dalloc(&c->mom_p, (size_t)3 * nx)) || (s = dalloc(&c->mom_h, (size_t)3 * nx))) {
@@ -1862,7 +2000,8 @@ int vv_destroy(vv_ctx* c) {
                     c->spec32, c->tw32, c->lambda32, c->dinv32, c->adj_cH, c->adj_cF, c->adj_zpart,
                     c->adj_zbuf, c->adj_q, c->adj_hprof, c->adj_h1a, c->adj_h1b, c->lamv, c->twv, c->pv_spec,
                     c->pv_scr, c->pv_xt, c->phipc, c->twv32, c->pv_spec32, c->pv_scr32, c->pv_xt32,
-                    c->mom_p, c->mom_h, c->db_fave, c->db_b};
+                    c->mom_p, c->mom_h, c->db_fave, c->db_b, c->pred_H, c->pred_Hp, c->pred_Y, c->pred_K,
+                    c->pred_S, c->pred_fl, c->pred_cpart};
     destroy_graph(c);
     for (int k = 0; k < 4; ++k)
         if (c->cs[k]) cudaStreamDestroy(c->cs[k]);
@@ -1896,7 +2035,26 @@ int vv_update_history(vv_ctx* c, const double* F) {
 
 int vv_update_previous(vv_ctx* c, const double* h1p, const double* h1h, const double* h2p, const double* h2h) {
     if (!c) return VV_ERR_ARG;
-    return set_hxp(c, h1p, h1h, h2p, h2h);
+    TRY(set_hxp(c, h1p, h1h, h2p, h2h));
+    vv::k_set_have<<<1, 1, 0, c->st>>>(c->ds);
+    CKL(c);
+    return VV_OK;
+}
+
+int vv_predict(vv_ctx* c, const double* F, const double* h1h, const double* h2h, double* Y) {
+    if (!c || !F || !Y || !c->pred) return VV_ERR_ARG;
+    return pred_run(c, F, h1h, h2h, Y);
+}
+
+int vv_initial_guess(vv_ctx* c, vv_state* st, double* prev, double* guess, int32_t* kept) {
+    if (!c || !st || !st->f || !st->phi || !st->n || !st->h1c || !c->pred) return VV_ERR_ARG;
+    TRY(pred_guess(c, st));
+    CK(cudaMemcpyAsync(c->hds, c->ds, offsetof(vv::DevState, hcol), cudaMemcpyDeviceToHost, c->st));
+    CK(cudaStreamSynchronize(c->st));
+    if (prev) *prev = c->hds->guess_prev;
+    if (guess) *guess = c->hds->guess_res;
+    if (kept) *kept = c->hds->guess_kept;
+    return VV_OK;
 }
 
 int vv_function(vv_ctx* c, const double* F, double* Y, int apply_pc) {
@@ -2836,7 +2994,7 @@ int vv_batch_create(int n, vv_ctx* const* ctxs, const vv_state* states, vv_batch
         if (c->mixed != c0->mixed || c->g.bracket != c0->g.bracket ||
             c->g.preconditioner != VV_PC_TENSOR_KINETIC || c->g.order == VV_ORDER_REFERENCE ||
             c->g.bracket == VV_BRACKET_SIMPSON || c->avg != vv::AVG_POINT || c->coll != vv::COLL_NONE || c->db ||
-            c->nx % vv::WX != 0 || !c->pow2 || c->device != c0->device)
+            c->pred || c->nx % vv::WX != 0 || !c->pow2 || c->device != c0->device)
             return VV_ERR_UNSUPPORTED;
     }
     vv_batch* b = new vv_batch();   // value-initialised: pointers and counts start at zero

@@ -40,6 +40,11 @@ struct DevState {
     int gmres_its[MAX_PICARD_DEV];
     int ksp_reason[MAX_PICARD_DEV];
     double residual[MAX_PICARD_DEV + 1];
+    // initial guess (after the option header, which the host uploads before a
+    // step, and before the GMRES arrays: part of the report read-back)
+    double guess_prev, guess_res;
+    int guess_kept;
+    int have_set;   // 1 once update_previous has run (before it the solver's Have is zero)
     // GMRES arrays
     double hcol[MAX_RESTART + 2];
     double grs[MAX_RESTART + 2];
@@ -452,6 +457,7 @@ __device__ __forceinline__ void pic_residual_warp(DevState* s, const double* __r
     if (threadIdx.x != 0) return;
     const double pred = sqrt(f2) + sqrt(s->pnorm2);
     if (phase == 0) {
+        s->have_set = 1;   // the step's prologue ran update_previous
         s->pred = pred;
         s->residual[0] = pred;
         s->pic_i = 0;

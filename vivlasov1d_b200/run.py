@@ -45,11 +45,9 @@ class Run:
                                       % (so["method"], so["type"]))
         if so["timestepping"].lower() != "mp" or so["mode"] != "split":
             raise NotImplementedError("only the split midpoint (mp) method is on this path")
-        ig = so.get("initial_guess")
-        if ig not in (None, "", "None"):
-            # run_base.py:173-183: 'rk4' calls PETScArakawaRungeKutta.rk18_J4, which the class does
-            # not define; the runspec's own names ('rk4_16', 'gear2', ...) are not keys of the table
-            raise NotImplementedError("initial_guess %r fails in the reference (run_base.py:173-183, 815-828)" % ig)
+        # the predictor of the initial guess (run_base.py:173-181, 786-912): the runspec's names
+        # (runspec.cfg:58) and the option table's 'rk4'; the multistep predictors raise
+        _lib.initial_guess_code(so.get("initial_guess"))
         if so.get("regularisation", 0.0) not in (0, 0.0, None):
             # Regularisation.function calls an undefined method (Regularisation.pyx:42-44)
             raise NotImplementedError("regularisation != 0 fails in the reference (Regularisation.pyx:42-44)")
@@ -64,7 +62,8 @@ class Run:
                                      averaging=cfg.get_averaging_operator(),
                                      collision=cfg.get_collision_operator(), coll_freq=so["coll_freq"],
                                      coll_diff=so["coll_diff"], coll_drag=so["coll_drag"],
-                                     double_bracket=cfg.get_double_bracket())
+                                     double_bracket=cfg.get_double_bracket(),
+                                     initial_guess=so.get("initial_guess"), initial_iter=so.get("initial_iter", 1))
         g = self.grid
         fld, xv = g.field, g.xvec
         self.fc, self.fh = fld(), fld()
@@ -170,6 +169,9 @@ def report_dict(rep):
         "reverted": bool(rep.reverted),
         "stop_rule": {1: "rose", 2: "atol", 3: "max_iter"}.get(rep.stop_rule, ""),
         "ksp_failures": rep.ksp_failures,
+        "guess_kept": bool(rep.guess_kept),
+        "guess_prev": rep.guess_prev,
+        "guess_residual": rep.guess_residual,
     }
 
 

@@ -81,10 +81,12 @@ class Grid:
 
     def context(self, bracket="arakawaj4", preconditioner="tensor_kinetic", charge=-1.0, mass=1.0,
                 order="factored", restart=30, precision="fp64", mixed_rtol=0.0, laplace="cfd4", averaging="point",
-                collision="", coll_freq=0.0, coll_diff=1.0, coll_drag=1.0, double_bracket=""):
+                collision="", coll_freq=0.0, coll_diff=1.0, coll_drag=1.0, double_bracket="", initial_guess=None,
+                initial_iter=1):
         key = (bracket, preconditioner, float(charge), float(mass), order, int(restart), precision, float(mixed_rtol),
                laplace.lower(), _lib.averaging_code(averaging), (collision or "").lower(), float(coll_freq),
-               float(coll_diff), float(coll_drag), (double_bracket or "").lower())
+               float(coll_diff), float(coll_drag), (double_bracket or "").lower(),
+               _lib.initial_guess_code(initial_guess), max(1, int(initial_iter or 1)))
         ctx = self._contexts.get(key)
         if ctx is None:
             ctx = Context(self, *key)
@@ -98,7 +100,8 @@ class Context:
 
     def __init__(self, grid, bracket="arakawaj4", preconditioner="tensor_kinetic", charge=-1.0,
                  mass=1.0, order="factored", restart=30, precision="fp64", mixed_rtol=0.0, laplace="cfd4",
-                 averaging="point", collision="", coll_freq=0.0, coll_diff=1.0, coll_drag=1.0, double_bracket=""):
+                 averaging="point", collision="", coll_freq=0.0, coll_diff=1.0, coll_drag=1.0, double_bracket="",
+                 initial_guess=None, initial_iter=1):
         lib = _lib.load()
         if not torch.cuda.is_available():
             raise RuntimeError("vivlasov1d_b200 needs a CUDA device; no CPU fallback exists")
@@ -132,6 +135,9 @@ class Context:
         # DoubleBracket.create: 'ffh', 'fhh', anything else the no-op base class
         g.double_bracket = _lib.DOUBLE_BRACKET.get((double_bracket or "").lower(), 0)
         self.double_bracket = g.double_bracket if g.coll_freq != 0.0 else 0
+        g.initial_guess = _lib.initial_guess_code(initial_guess)
+        g.initial_iter = max(1, int(initial_iter or 1))
+        self.initial_guess = g.initial_guess
         g.order = _lib.ORDER_REFERENCE if order == "reference" else _lib.ORDER_FACTORED
         g.gmres_restart = int(restart)
         if precision not in _lib.PRECISION:
