@@ -16,6 +16,7 @@ VV_OK = 0
 VV_ERR_ARG = 1
 VV_ERR_UNSUPPORTED = 2
 VV_ERR_DIVERGED = 5
+VV_ERR_NAN = 6
 NOALLOC_MAX_NX = 16384      # VV_NOALLOC_MAX_NX: largest nx of vv_invariants_noalloc
 BRACKET = {"arakawaj1": 1, "arakawaj2": 2, "arakawaj4": 4, "simpson": 5}
 PC_NONE, PC_TENSOR_KINETIC, PC_TENSOR_POTENTIAL = 0, 1, 2

@@ -30,7 +30,8 @@ from .solver import Grid, Toolbox, STENCIL
 class Run:
     """State and driver of one run (run_base.py:35-566 + the runscript)."""
 
-    def __init__(self, cfg, f0=None, device=None, order="factored", restart=30, normalise=True, precision="fp64"):
+    def __init__(self, cfg, f0=None, device=None, order="factored", restart=30, normalise=True, precision="fp64",
+                 mixed_rtol=0.0):
         if not isinstance(cfg, Config):
             cfg = Config(cfg) if isinstance(cfg, str) else Config(overrides=cfg)
         self.cfg = cfg
@@ -58,7 +59,8 @@ class Run:
         self.ctx = self.grid.context(bracket=cfg.get_poisson_bracket(),
                                      preconditioner=cfg.get_preconditioner() or None,
                                      charge=self.charge, mass=self.mass, order=order, restart=restart,
-                                     precision=precision, laplace=cfg.get_laplace_operator(),
+                                     precision=precision, mixed_rtol=mixed_rtol,
+                                     laplace=cfg.get_laplace_operator(),
                                      averaging=cfg.get_averaging_operator(),
                                      collision=cfg.get_collision_operator(), coll_freq=so["coll_freq"],
                                      coll_diff=so["coll_diff"], coll_drag=so["coll_drag"],

@@ -51,8 +51,9 @@ def config(nx, nv, L, vmin, vmax, ht, ksp_rtol=1e-4, snes_atol=1e-10, nt=1):
             "initial_data": {"charge": -1.0}}
 
 
-def make_run(nx, nv, L, vmin, vmax, ht, fn, device=None, precision="fp64", **kw):
-    return Run(config(nx, nv, L, vmin, vmax, ht, **kw), f0=fn, device=device, precision=precision)
+def make_run(nx, nv, L, vmin, vmax, ht, fn, device=None, precision="fp64", mixed_rtol=0.0, **kw):
+    return Run(config(nx, nv, L, vmin, vmax, ht, **kw), f0=fn, device=device, precision=precision,
+               mixed_rtol=mixed_rtol)
 
 
 def landau_linear(device=None, precision="fp64"):
@@ -83,10 +84,10 @@ def sweep_specs(n=256, seed=SWEEP_SEED):
     return out
 
 
-def sweep_runs(n=256, seed=SWEEP_SEED, device=None, precision="fp64", specs=None):
+def sweep_runs(n=256, seed=SWEEP_SEED, device=None, precision="fp64", specs=None, snes_atol=1e-10, mixed_rtol=0.0):
     specs = specs if specs is not None else sweep_specs(n, seed)
     return [make_run(s["nx"], s["nv"], s["L"], -10.0, 10.0, 0.1, FAMILIES[s["family"]](s["amp"], s["k"]),
-                     device, precision) for s in specs]
+                     device, precision, mixed_rtol=mixed_rtol, snes_atol=snes_atol) for s in specs]
 
 
 def cells(runs):
