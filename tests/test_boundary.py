@@ -145,7 +145,10 @@ def test_initial_guess_names():
     assert _lib.initial_guess_code("symplectic2") == 1 and _lib.initial_guess_code("symplectic4") == 2
     assert _lib.initial_guess_code("rk4_16") == 3
     assert _lib.initial_guess_code("rk4_18") == _lib.initial_guess_code("rk4") == 4
-    assert _lib.initial_guess_code(4) == 4
+    assert _lib.initial_guess_code(4) == 4 and _lib.initial_guess_code(0) == 0
+    # the context key stores the code: every valid code maps to itself
+    for code in range(5):
+        assert _lib.initial_guess_code(code) == code
 
 
 def test_config_dissipation_choices():

@@ -57,7 +57,7 @@ def initial_guess_code(name):
     this path; other names are not predictors of the reference."""
     if name in (None, "", "None", "none"):
         return 0
-    if isinstance(name, int) and name in INITIAL_GUESS.values():
+    if isinstance(name, int) and (name == 0 or name in INITIAL_GUESS.values()):
         return name
     key = str(name).lower()
     if key in INITIAL_GUESS:

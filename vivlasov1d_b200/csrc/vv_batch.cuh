@@ -524,48 +524,61 @@ __global__ void k_b_gm_cycle_f(const BInst* __restrict__ tab, const int* __restr
 
 
 // <w, V_q>, q = 0..it, w = V[it+1], per warp item (column q of the partials)
+// basis vectors whose 16-byte loads a lane issues together before using them
+// (the loads of a chunk are independent; issuing them first keeps a chunk's
+// worth of bytes in flight per warp instead of one vector's)
+template <typename T> VV_DEV constexpr int gs_chunk() { return sizeof(T) == 4 ? 4 : 2; }
 template <typename T>
-__global__ void __launch_bounds__(RED_THREADS, 4) k_b_gm_mdot_p(const BInst* __restrict__ tab, const int* __restrict__ L, int n) {
+VV_DEV void vload_raw(const T* p, typename Vec16<T>::type& o) { o = *reinterpret_cast<const typename Vec16<T>::type*>(p); }
+VV_DEV void vexpand(const float4& v, double (&o)[4]) { o[0] = v.x; o[1] = v.y; o[2] = v.z; o[3] = v.w; }
+VV_DEV void vexpand(const double2& v, double (&o)[2]) { o[0] = v.x; o[1] = v.y; }
+
+template <typename T>
+__global__ void __launch_bounds__(RED_THREADS, 3) k_b_gm_mdot_p(const BInst* __restrict__ tab, const int* __restrict__ L, int n) {
     static_assert(RED_THREADS == 256, "eight warp items per block item");
-    constexpr int VN = vec_n<T>(), WV = WCELLS / (32 * VN);
+    constexpr int VN = vec_n<T>(), WV = WCELLS / (32 * VN), CK = gs_chunk<T>();
+    using V16 = typename Vec16<T>::type;
     for_warp_work<F_VEC>(tab, L, n, [&](const BInst& I, int wi) {
         const int lane = threadIdx.x & 31, nwi = wi_count(I);
         const int it = I.ds->it, m = it + 1;
         const size_t nc = I.ncell;
         const T* V = (const T*)I.V;
         const T* w = V + (size_t)(it + 1) * nc;
-        for (int q0 = 0; q0 < m; q0 += MDOT_CHUNK) {
-            double acc[MDOT_CHUNK];
+        for (int q0 = 0; q0 < m; q0 += CK) {
+            double acc[CK];
 #pragma unroll
-            for (int c = 0; c < MDOT_CHUNK; ++c) acc[c] = 0.0;
-            const int cnt = min(MDOT_CHUNK, m - q0);
+            for (int c = 0; c < CK; ++c) acc[c] = 0.0;
+            const int cnt = min(CK, m - q0);
             for (size_t base = (size_t)wi * WCELLS; base < nc; base += (size_t)nwi * WCELLS) {
-                double wv[WV][VN];
+                V16 wr[WV], vr[CK][WV];
 #pragma unroll
                 for (int t = 0; t < WV; ++t) {
                     const size_t i = base + (size_t)(lane + 32 * t) * VN;
-                    if (i < nc) vload(w + i, wv[t]);
-                    else for (int e = 0; e < VN; ++e) wv[t][e] = 0.0;
+                    if (i < nc) vload_raw(w + i, wr[t]);
+                    else wr[t] = V16{};
                 }
 #pragma unroll
-                for (int c = 0; c < MDOT_CHUNK; ++c) {
-                    if (c < cnt) {
-                        const T* vq = V + (size_t)(q0 + c) * nc;
+                for (int c = 0; c < CK; ++c)
 #pragma unroll
-                        for (int t = 0; t < WV; ++t) {
-                            const size_t i = base + (size_t)(lane + 32 * t) * VN;
-                            if (i < nc) {
-                                double v[VN];
-                                vload(vq + i, v);
+                    for (int t = 0; t < WV; ++t) {
+                        const size_t i = base + (size_t)(lane + 32 * t) * VN;
+                        if (c < cnt && i < nc) vload_raw(V + (size_t)(q0 + c) * nc + i, vr[c][t]);
+                        else vr[c][t] = V16{};
+                    }
 #pragma unroll
-                                for (int e = 0; e < VN; ++e) acc[c] += wv[t][e] * v[e];
-                            }
-                        }
+                for (int c = 0; c < CK; ++c) {
+#pragma unroll
+                    for (int t = 0; t < WV; ++t) {
+                        double wv[VN], v[VN];
+                        vexpand(wr[t], wv);
+                        vexpand(vr[c][t], v);
+#pragma unroll
+                        for (int e = 0; e < VN; ++e) acc[c] += wv[e] * v[e];
                     }
                 }
             }
 #pragma unroll
-            for (int c = 0; c < MDOT_CHUNK; ++c) {
+            for (int c = 0; c < CK; ++c) {
                 if (c < cnt) {
                     const double t = warp_sum(acc[c]);
                     if (lane == 0) I.wpart[(size_t)(q0 + c) * nwi + wi] = t;
