@@ -59,8 +59,13 @@ N_INSTANCES = 256
 WORKLOAD = ("sweep: 256 seeded instances (Landau/two-stream/bump-on-tail, nx 64-256, nv 128-1024), "
             "J4, dt=0.1, GMRES(30)+tensor_kinetic, batched + mixed precision vs plain FP64")
 MDOT_IT = 4   # Arnoldi index of the roofline launch of the multi-dot
-# Picard tolerance (petsc_snes_atol) of every arm, GPU and CPU
-SNES_ATOL = 1e-10
+# Picard tolerance (petsc_snes_atol) of every arm, GPU and CPU.  The runspec
+# default 1e-10 lets two FP64 runs of the same step stop at points of the
+# residual ball that differ in field energy by up to 1e-8 relative on the
+# strongly damped instances within 25 steps (measured between the FP32-inner
+# and FP64 arms; 3e-7 between 1e-10 and 1e-12 themselves at 200 steps); the
+# metric's 1e-9 field-energy bound is kept by tightening every arm alike
+SNES_ATOL = 1e-12
 
 
 def measured_peaks():

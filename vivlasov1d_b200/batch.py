@@ -75,6 +75,8 @@ class Batch:
         for i, r in enumerate(self.runs):
             r.itime += 1
             reps[i]["status"] = self._status[i]
-        if st not in (_lib.VV_OK, _lib.VV_ERR_DIVERGED):
+        # an instance whose residual is above the abort threshold or NaN fails
+        # alone: its status is in its report and the others are not touched
+        if st not in (_lib.VV_OK, _lib.VV_ERR_DIVERGED, _lib.VV_ERR_NAN):
             _lib.check(st, "vv_batch_step")
         return reps

@@ -59,7 +59,10 @@ struct vv_ctx {
     // h fields (kinetic, potential or RK), bracket output, RK stages, stage
     // input, the saved iterate, collision-only residual partials
     int pred, pred_iter;
-    double *pred_H, *pred_Hp, *pred_Y, *pred_K, *pred_S, *pred_fl, *pred_cpart;
+    double *pred_H, *pred_Hp, *pred_Y, *pred_K, *pred_S, *pred_fl, *pred_cpart, *pred_zero;
+    // non-null: the bracket kernels run in the reference order with this h
+    // field (the predictor's residual with a zero Have)
+    const double* zero_h;
     // the potential preconditioner (VV_PC_TENSOR_POTENTIAL): v modes, eigenvalues
     // for n = nv, nv twiddles, transposed field, v spectrum, elimination
     // scratch (FP32 copies in the mixed mode), rows per CTA of the v FFT, phi
@@ -292,7 +295,8 @@ int launch_bracket_a(vv_ctx* c, const T* X, const T* Xh, T* Y, double factor, do
     }
     bool done = false;
     if constexpr (std::is_same<T, double>::value) {
-        if (c->g.order == VV_ORDER_REFERENCE) {
+        if (c->g.order == VV_ORDER_REFERENCE || c->zero_h) {
+            p.hfield = c->zero_h;
             vv::k_bracket_ref<SCHEME, MODE, AVG><<<grid, block, 0, c->st>>>(X, Xh, Y, p, sumsq);
             done = true;
         }
@@ -326,6 +330,7 @@ int launch_simpson(vv_ctx* c, const T* X, const T* Xh, T* Y, double factor, doub
     vv::BracketParams p = bparams(c, factor);
     p.xidx = xidx;
     p.xstride = xidx ? c->ncell : 0;
+    if constexpr (std::is_same<T, double>::value) p.hfield = c->zero_h;
     vv::k_bracket_simpson<MODE, T, AVG><<<grid, block, 0, c->st>>>(X, Xh, Y, p, sumsq);
     CKL(c);
     return VV_OK;
@@ -573,6 +578,7 @@ void smem_attributes(int optin, int& lowest, cudaError_t& e) {
     set((const void*)vv::k_b_tridiagjs<R>);
     set((const void*)vv::k_b_tridiagjm<R, 2>);
     set((const void*)vv::k_b_tridiagjm<R, 4>);
+    set((const void*)vv::k_b_tridiagjv<R>);
 }
 
 // dynamic shared memory of the staged warp-per-mode tridiagonal solve
@@ -1237,19 +1243,24 @@ int pred_run(vv_ctx* c, const double* F, const double* h1h, const double* h2h, d
     return VV_OK;
 }
 
-// the guard's residual (phase 0: of the current f, 1: of the prediction)
+// the guard's residual (phase 0: of the current f, 1: of the prediction),
+// with the Have of the last update_previous and, for a solver whose Have is
+// still the zero vector of its construction (no update_previous yet; the
+// device flag decides), with a zero Have: the time derivative and the
+// collision terms (the brackets and the double bracket of a zero h vanish)
 int pred_residual(vv_ctx* c, vv_state* st, int phase) {
     const int tiles = bracket_tiles(c, st->f, c->Fh, c->tmp);
     TRY(launch_bracket<vv::MODE_RESIDUAL, double>(c, st->f, c->Fh, c->tmp, 1.0, c->part));
     TRY(poisson_apply(c, st->phi, st->n, nullptr, 2, &c->ds->pnorm2));
-    int ncp = 0;
-    if (phase == 0 && c->coll != vv::COLL_NONE) {
-        // what a zero Have leaves of R(f) with Fh = f: the collision terms
-        CK(cudaMemsetAsync(c->pred_Y, 0, c->ncell * sizeof(double), c->st));
-        TRY(launch_collision<double>(c, st->f, c->Fh, c->pred_Y, c->pred_cpart, nullptr));
-        ncp = ((c->nx + vv::BX - 1) / vv::BX) * ((c->nv + vv::BY - 1) / vv::BY);
-    }
-    vv::k_pred_norm<<<1, 32, 0, c->st>>>(c->ds, c->part, tiles, ncp ? c->pred_cpart : nullptr, ncp, phase);
+    const bool coll = c->coll != vv::COLL_NONE;
+    c->zero_h = c->pred_zero;
+    const int r = launch_bracket_td<vv::MODE_RESIDUAL, double>(c, st->f, c->Fh, c->pred_Y, 1.0,
+                                                                coll ? nullptr : c->pred_cpart, nullptr);
+    c->zero_h = nullptr;
+    TRY(r);
+    if (coll) TRY(launch_collision<double>(c, st->f, c->Fh, c->pred_Y, c->pred_cpart, nullptr));
+    const int ncp = ((c->nx + vv::BX - 1) / vv::BX) * ((c->nv + vv::BY - 1) / vv::BY);
+    vv::k_pred_norm<<<1, 32, 0, c->st>>>(c->ds, c->part, tiles, c->pred_cpart, ncp, phase);
     CKL(c);
     return VV_OK;
 }
@@ -1922,9 +1933,13 @@ int vv_create(const vv_grid* grid, vv_ctx** out) {
         const size_t ntile = (size_t)((nx + vv::BX - 1) / vv::BX) * ((nv + vv::BY - 1) / vv::BY);
         if ((s = dalloc(&c->pred_H, n)) || (s = dalloc(&c->pred_Hp, n)) || (s = dalloc(&c->pred_Y, n)) ||
             (s = dalloc(&c->pred_K, 4 * n)) || (s = dalloc(&c->pred_S, n)) || (s = dalloc(&c->pred_fl, n)) ||
-            (s = dalloc(&c->pred_cpart, ntile))) {
+            (s = dalloc(&c->pred_cpart, ntile)) || (s = dalloc(&c->pred_zero, n))) {
             vv_destroy(c);
             return s;
+        }
+        if (cudaMemset(c->pred_zero, 0, n * sizeof(double)) != cudaSuccess) {
+            vv_destroy(c);
+            return fail_cuda(cudaGetLastError(), "vv_create (predictor)");
         }
     }
     // collisions: current / history moment profiles (n, U, a)
@@ -2001,7 +2016,7 @@ int vv_destroy(vv_ctx* c) {
                     c->adj_zbuf, c->adj_q, c->adj_hprof, c->adj_h1a, c->adj_h1b, c->lamv, c->twv, c->pv_spec,
                     c->pv_scr, c->pv_xt, c->phipc, c->twv32, c->pv_spec32, c->pv_scr32, c->pv_xt32,
                     c->mom_p, c->mom_h, c->db_fave, c->db_b, c->pred_H, c->pred_Hp, c->pred_Y, c->pred_K,
-                    c->pred_S, c->pred_fl, c->pred_cpart};
+                    c->pred_S, c->pred_fl, c->pred_cpart, c->pred_zero};
     destroy_graph(c);
     for (int k = 0; k < 4; ++k)
         if (c->cs[k]) cudaStreamDestroy(c->cs[k]);
@@ -2459,6 +2474,7 @@ struct vv_batch {
     size_t smem_tri_stage, smem_tri_plain, smem_tri_warp;
     size_t smem_tri_js;          // k_b_tridiagjs (padded warp slices)
     size_t smem_tri_jm2, smem_tri_jm4;   // k_b_tridiagjm, 2 and 4 warps per mode
+    size_t smem_tri_jv;                  // k_b_tridiagjv (lanes per mode by line length)
     int nvmax;                   // largest velocity grid of the table
     int smem_limit;              // dynamic shared memory per block available to the batch kernels
     double* wpart;               // device: per-warp partial sums of every instance
@@ -2538,6 +2554,8 @@ int b_tri(vv_batch* b, const int* L) {
         if (b->tri_kind == 3)
             return blaunch(b, vv::k_b_tridiagjm<T, 4>, vv::F_MODES, 32 * vv::TRIW_WARPS * 4, b->smem_tri_jm4, tab, L,
                            b->n, b->nvmax);
+        if (b->tri_kind == 4)
+            return blaunch(b, vv::k_b_tridiagjv<T>, vv::F_MODES, vv::TJV_THREADS, b->smem_tri_jv, tab, L, b->n);
         return blaunch(b, vv::k_b_tridiagj<T>, vv::F_MODES, 32,
                        (size_t)64 * vv::TJ_RING * sizeof(typename Cplx<T>::type), tab, L, b->n);
     }
@@ -2813,7 +2831,10 @@ void b_shape(vv_batch* b, std::vector<vv::BInst>& tab, int R, int tri_kind, int 
         if (b->pcj) {
             const int rb = vv::fj_rows_of(c->M);
             I.cnt[vv::F_ROWS] = (c->nv + rb - 1) / rb;
-            I.cnt[vv::F_MODES] = tri_kind >= 1 ? (c->nmodes + vv::TRIW_WARPS - 1) / vv::TRIW_WARPS : (c->nmodes + 31) / 32;
+            const int items = (c->nmodes + vv::TRIW_WARPS - 1) / vv::TRIW_WARPS;
+            I.cnt[vv::F_MODES] = tri_kind == 4   ? (items + vv::tjv_group(c->nv) - 1) / vv::tjv_group(c->nv)
+                                 : tri_kind >= 1 ? items
+                                                 : (c->nmodes + 31) / 32;
         }
         for (int f = 0; f < vv::NFAM; ++f) b->tot[f] += I.cnt[f];
         b->smem_rfft = std::max(b->smem_rfft, fft_smem(0, c->M, R, csz, false));
@@ -2836,7 +2857,8 @@ int b_apply_shape(vv_batch* b, const std::vector<vv::BInst>& tab) {
 // whether tridiagonal variant tw (layout pj) fits the device's shared memory
 bool b_tri_fits(const vv_batch* b, int tw, int pj) {
     size_t need = 0;
-    if (pj) need = tw == 1 ? b->smem_tri_js : tw == 2 ? b->smem_tri_jm2 : tw == 3 ? b->smem_tri_jm4 : 0;
+    if (pj)
+        need = tw == 1 ? b->smem_tri_js : tw == 2 ? b->smem_tri_jm2 : tw == 3 ? b->smem_tri_jm4 : tw == 4 ? b->smem_tri_jv : 0;
     else if (tw == 1) need = b->smem_tri_warp;
     return need <= (size_t)b->smem_limit;
 }
@@ -2890,7 +2912,7 @@ int b_autotune(vv_batch* b, std::vector<vv::BInst>& tab) {
     int bR = b->R, bW = b->tri_kind, bF = b->fft4, bJ = b->pcj, r = VV_OK;
     for (int pj = 0; pj <= (b->pcj_ok ? 1 : 0) && r == VV_OK; ++pj)
     for (int f4 = 0; f4 <= (pj ? 0 : 1) && r == VV_OK; ++f4)
-    for (int tw = 0; tw <= (pj ? 3 : 2) && r == VV_OK; ++tw) {
+    for (int tw = 0; tw <= (pj ? 4 : 2) && r == VV_OK; ++tw) {
         if (!b_tri_fits(b, tw, pj)) continue;
         for (int R = 2; R <= (pj ? 2 : 8) && r == VV_OK; R *= 2) {
             b_shape(b, tab, R, tw, f4, pj);
@@ -3060,6 +3082,7 @@ int vv_batch_create(int n, vv_ctx* const* ctxs, const vv_state* states, vv_batch
             b->smem_tri_js = vv::tri_js_smem(b->nvmax, b->mixed ? sizeof(float2) : sizeof(double2));
             b->smem_tri_jm2 = vv::tri_jm_smem(b->nvmax, b->mixed ? sizeof(float2) : sizeof(double2), 2);
             b->smem_tri_jm4 = vv::tri_jm_smem(b->nvmax, b->mixed ? sizeof(float2) : sizeof(double2), 4);
+            b->smem_tri_jv = std::max(b->smem_tri_jv, vv::tjv_smem_of(c->nv, b->mixed ? sizeof(float2) : sizeof(double2)));
         }
         b->smem_pois = std::max(b->smem_pois, c->smem_pois);
     }
@@ -3139,7 +3162,7 @@ int vv_batch_create(int n, vv_ctx* const* ctxs, const vv_state* states, vv_batch
         const char* bs = getenv("VV_BATCH_SHAPE");
         int fR = 0, fT = 0, fF = 0, fJ = 0, fM = 0;
         const int nf = bs ? sscanf(bs, "%d,%d,%d,%d,%d", &fR, &fT, &fF, &fJ, &fM) : 0;
-        const bool fixed = nf >= 3 && (fR == 2 || fR == 4 || fR == 8) && fT >= 0 && fT <= (fJ ? 3 : 2) &&
+        const bool fixed = nf >= 3 && (fR == 2 || fR == 4 || fR == 8) && fT >= 0 && fT <= (fJ ? 4 : 2) &&
                            (fF == 0 || fF == 1) && (fJ == 0 || (fJ == 1 && b->pcj_ok)) && b_tri_fits(b, fT, fJ);
         const char* at = getenv("VV_AUTOTUNE");
         if (fixed) {

@@ -1008,4 +1008,182 @@ __global__ void __launch_bounds__(32 * TRIW_WARPS * W) k_b_tridiagjm(const BInst
     });
 }
 
+// ---- LU solves on the v-major layout, lanes per mode set by the line length ----
+// The chunked solves cost a warp scan (and a sub-warp combine) per chunk on
+// top of the per-row work, so short lines want fewer, longer chunks: each
+// mode gets LPM = 8..64 lanes, enough for chunks of about TJV_CH rows, and a
+// CTA of TJV_THREADS threads solves G = TJV_THREADS / (4 LPM) consecutive
+// 4-mode items of one instance at once (G items x 4 modes x nv rows staged:
+// about the same shared memory for every nv).  The lanes of a mode scan
+// their chunks' affine maps with width-LPM warp shuffles (LPM <= 32) or a
+// warp scan and a combine of the two sub-warps (LPM = 64).  The alpha/gamma
+// tables are read through L1 in the chunk order.
+constexpr int TJV_THREADS = 256, TJV_CH = 16;
+__host__ __device__ constexpr int tjv_lpm(int nv) {
+    return nv <= 8 * TJV_CH ? 8 : nv <= 16 * TJV_CH ? 16 : nv <= 32 * TJV_CH ? 32 : 64;
+}
+__host__ __device__ constexpr int tjv_group(int nv) { return TJV_THREADS / (TRIW_WARPS * tjv_lpm(nv)); }
+__host__ __device__ constexpr int tjv_slots(int nv) { return nv + tjv_lpm(nv); }
+// complex slots of one group's 4-mode item: 4 x (line + LU reciprocals) + pad
+__host__ __device__ constexpr int tjv_item_slots(int nv) { return TRIW_WARPS * (2 * tjv_slots(nv) + TRIJS_PAD); }
+__host__ __device__ constexpr size_t tjv_smem_of(int nv, size_t csz) {
+    return (size_t)tjv_group(nv) * tjv_item_slots(nv) * csz;
+}
+
+template <typename C>
+__device__ __forceinline__ C shfl_w(C v, int d, bool up, int width) {
+    C r;
+    r.x = up ? __shfl_up_sync(0xffffffffu, v.x, d, width) : __shfl_down_sync(0xffffffffu, v.x, d, width);
+    r.y = up ? __shfl_up_sync(0xffffffffu, v.y, d, width) : __shfl_down_sync(0xffffffffu, v.y, d, width);
+    return r;
+}
+// inclusive scan of affine maps over segments of `width` lanes in `forward`
+// order; *ex gets the exclusive prefix (identity for a segment's first lane)
+template <typename C>
+__device__ __forceinline__ Aff<C> seg_scan_aff(Aff<C> a, bool forward, int width, Aff<C>* ex) {
+    const int l = threadIdx.x & (width - 1);
+    const int pos = forward ? l : width - 1 - l;
+    Aff<C> inc = a;
+    for (int d = 1; d < width; d <<= 1) {
+        Aff<C> o;
+        o.P = shfl_w(inc.P, d, forward, width);
+        o.Q = shfl_w(inc.Q, d, forward, width);
+        if (pos >= d) inc = aff_combine(o, inc);
+    }
+    Aff<C> prev;
+    prev.P = shfl_w(inc.P, 1, forward, width);
+    prev.Q = shfl_w(inc.Q, 1, forward, width);
+    if (pos > 0) *ex = prev;
+    else {
+        ex->P = c_make<C>(1.0, 0.0);
+        ex->Q = c_make<C>(0.0, 0.0);
+    }
+    return inc;
+}
+
+template <typename R>
+__global__ void __launch_bounds__(TJV_THREADS) k_b_tridiagjv(const BInst* __restrict__ tab, const int* __restrict__ L,
+                                                             int n) {
+    using C = typename Cplx<R>::type;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    __shared__ Aff<C> tot[2][TJV_THREADS / 32];
+    for_work<F_MODES>(tab, L, n, [&](const BInst& I, int local) {
+        const int nv = I.tp.nv, nm = I.tp.nmodes;
+        const int lpm = tjv_lpm(nv), G = tjv_group(nv);
+        const int CH = (nv + lpm - 1) / lpm;
+        const int ns = tjv_slots(nv), is = tjv_item_slots(nv);
+        const int ws = 2 * ns + TRIJS_PAD;
+        const int tid = threadIdx.x;
+        const int gi = tid / (TRIW_WARPS * lpm);               // item of the group
+        const int m = (tid / lpm) % TRIW_WARPS;                 // mode within the item
+        const int l = tid % lpm;                                // lane within the mode
+        const int kbase = local * G * TRIW_WARPS;               // first mode of the CTA's group
+        C* base = reinterpret_cast<C*>(smem_raw);
+        C* spec = (C*)I.specT;
+        const C* dj = (const C*)I.dinvJ;
+        const R* al = reinterpret_cast<const R*>(I.tp.alpha);
+        const R* ga = reinterpret_cast<const R*>(I.tp.gamma);
+        const FastDiv dch((unsigned)CH);
+        // stage G items: row j of an item's 4 modes is one 32-byte sector
+        const int cols = G * TRIW_WARPS;
+        for (int t = tid; t < nv * cols; t += TJV_THREADS) {
+            const int j = t / cols, c = t % cols;
+            const int k = kbase + c;
+            if (k < nm) {
+                C* sb = base + (size_t)(c / TRIW_WARPS) * is + (size_t)(c % TRIW_WARPS) * ws;
+                const int q = j + (int)dch((unsigned)j);
+                cp_async_elem(&sb[q], &spec[(size_t)j * nm + k]);
+                cp_async_elem(&sb[ns + q], &dj[(size_t)j * nm + k]);
+            }
+        }
+        cp_async_commit();
+        cp_async_wait0();
+        __syncthreads();
+        const int k = kbase + gi * TRIW_WARPS + m;
+        const bool on = gi < G && k < nm;
+        C* sb = base + (size_t)gi * is + (size_t)m * ws;
+        const C* sd = sb + ns;
+        const C lam = on ? reinterpret_cast<const C*>(I.tp.lambda)[k] : c_make<C>(0.0, 0.0);
+        const int r0 = l * CH;
+        const int r1 = min(r0 + CH, nv);
+        const int q0 = l * (CH + 1);
+        const int width = lpm < 32 ? lpm : 32;
+        const int wid = tid >> 5;
+        const bool two = lpm > 32;                              // two sub-warps per mode
+        // forward: y_r = b_r - l_r y_{r-1},  l_r = lambda alpha_r / U_{r-1}
+        Aff<C> a;
+        a.P = c_make<C>(1.0, 0.0);
+        a.Q = c_make<C>(0.0, 0.0);
+        if (on)
+            for (int r = r0, q = q0; r < r1; ++r, ++q) {
+                Aff<C> mp;
+                if (r == 0) mp.P = c_make<C>(0.0, 0.0);
+                else {
+                    const C dprev = sd[(r == r0) ? q - 2 : q - 1];
+                    const C lr = c_mul(c_rmul(lam, __ldg(al + r)), dprev);
+                    mp.P = c_make<C>(-lr.x, -lr.y);
+                }
+                mp.Q = sb[q];
+                a = aff_combine(a, mp);
+            }
+        Aff<C> ex;
+        Aff<C> inc = seg_scan_aff<C>(a, true, width, &ex);
+        if (two) {
+            if ((tid & 31) == 31) tot[0][wid] = inc;
+            __syncthreads();
+            if (l >= 32) ex = aff_combine(tot[0][wid - 1], ex);
+        }
+        C y = ex.Q;
+        if (on)
+            for (int r = r0, q = q0; r < r1; ++r, ++q) {
+                const C b = sb[q];
+                if (r == 0) y = b;
+                else {
+                    const C dprev = sd[(r == r0) ? q - 2 : q - 1];
+                    const C lr = c_mul(c_rmul(lam, __ldg(al + r)), dprev);
+                    y = c_sub(b, c_mul(lr, y));
+                }
+                sb[q] = y;
+            }
+        // backward: x_r = U_r^-1 (y_r - c_r x_{r+1}) == mu_r + nu_r x_{r+1}
+        a.P = c_make<C>(1.0, 0.0);
+        a.Q = c_make<C>(0.0, 0.0);
+        if (on)
+            for (int r = r1 - 1, q = q0 + (r1 - 1 - r0); r >= r0; --r, --q) {
+                Aff<C> mp;
+                const C d = sd[q];
+                mp.Q = c_mul(d, sb[q]);
+                if (r == nv - 1) mp.P = c_make<C>(0.0, 0.0);
+                else {
+                    const C nu = c_mul(d, c_rmul(lam, __ldg(ga + r)));
+                    mp.P = c_make<C>(-nu.x, -nu.y);
+                }
+                a = aff_combine(a, mp);
+            }
+        inc = seg_scan_aff<C>(a, false, width, &ex);
+        if (two) {
+            if ((tid & 31) == 0) tot[1][wid] = inc;
+            __syncthreads();
+            if (l < 32) ex = aff_combine(tot[1][wid + 1], ex);
+        }
+        C x = ex.Q;
+        if (on)
+            for (int r = r1 - 1, q = q0 + (r1 - 1 - r0); r >= r0; --r, --q) {
+                const C d = sd[q];
+                if (r == nv - 1) x = c_mul(d, sb[q]);
+                else x = c_mul(d, c_sub(sb[q], c_mul(c_rmul(lam, __ldg(ga + r)), x)));
+                sb[q] = x;
+            }
+        __syncthreads();
+        for (int t = tid; t < nv * cols; t += TJV_THREADS) {
+            const int j = t / cols, c = t % cols;
+            const int kk = kbase + c;
+            if (kk < nm)
+                spec[(size_t)j * nm + kk] =
+                    base[(size_t)(c / TRIW_WARPS) * is + (size_t)(c % TRIW_WARPS) * ws + j + (int)dch((unsigned)j)];
+        }
+        __syncthreads();
+    });
+}
+
 }  // namespace vv

@@ -60,17 +60,14 @@ __global__ void k_pred_rk_final(double* __restrict__ x, const double* __restrict
 
 // Residual norms of the guard (calculate_residual, run_base.py:631-637):
 // ||R(f)|| from the residual kernel's partials plus ||Poisson residual||.
-// phase 0 (before the predictor): before the first update_previous the
-// solver's Have is the zero vector of its construction and Fh = f, so only
-// the collision part of R survives (its partials in cpart, or none).
-// phase 1 (after): the prediction's residual and the keep decision.
-__global__ void k_pred_norm(DevState* s, const double* __restrict__ part, int np, const double* __restrict__ cpart,
-                            int ncp, int phase) {
+// Before the first update_previous the solver's Have is the zero vector of
+// its construction: R then comes from the partials of the zero-Have residual
+// (zpart).  phase 0: before the predictor; phase 1: the prediction's
+// residual and the keep decision.
+__global__ void k_pred_norm(DevState* s, const double* __restrict__ part, int np, const double* __restrict__ zpart,
+                            int nzp, int phase) {
     if (threadIdx.x >= 32) return;
-    const bool zero_have = phase == 0 && !s->have_set;
-    double f2 = 0.0;
-    if (!zero_have) f2 = warp_reduce_parts(part, np);
-    else if (cpart) f2 = warp_reduce_parts(cpart, ncp);
+    const double f2 = s->have_set ? warp_reduce_parts(part, np) : warp_reduce_parts(zpart, nzp);
     if (threadIdx.x != 0) return;
     const double r = sqrt(f2) + sqrt(s->pnorm2);
     if (phase == 0) {
