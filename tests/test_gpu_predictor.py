@@ -26,6 +26,11 @@ STEP_TOL = 1e-12
 # of the oracle's runs stays a factor 3 or more away from them (checked in
 # the tests), so no stop decision is left to round-off
 PRED_ATOL = {"symplectic2": 7e-10, "symplectic4": 7e-10, "rk4_16": 1e-11, "rk4_18": 1e-11, "rk4": 1e-11}
+# the guard's residual norms: a good guess's residual is 100-1000x smaller
+# than the terms it cancels (about the previous step's residual), so the
+# summation-order differences of the GPU kernels are bounded relative to the
+# larger of the two residuals (measured: <= 1.2e-14 of it)
+GUARD_TOL = 1e-12
 
 
 @pytest.fixture(scope="module", autouse=True)
@@ -106,9 +111,10 @@ def test_step_with_predictor_matches_oracle(method):
         orep = orun.step()
         _assert_margin(orep, atol)
         assert rep["guess_kept"] == orep.guess_kept == (k > 0), (k, rep, orep)
-        assert abs(rep["guess_residual"] - orep.guess) <= 1e-12 * orep.guess
+        scale = max(orep.guess, orep.guess_prev)
+        assert abs(rep["guess_residual"] - orep.guess) <= GUARD_TOL * scale
         if k > 0:
-            assert abs(rep["guess_prev"] - orep.guess_prev) <= 1e-12 * orep.guess_prev
+            assert abs(rep["guess_prev"] - orep.guess_prev) <= GUARD_TOL * scale
         assert rep["picard_its"] == orep.picard_its, (k, rep, orep.picard_its)
     assert rel(host(run.fc), orun.fc) < STEP_TOL
 
@@ -132,8 +138,9 @@ def test_step_with_predictor_and_collisions():
         orep = orun.step()
         _assert_margin(orep, atol)
         assert rep["guess_kept"] == orep.guess_kept, (k, rep, orep)
-        assert abs(rep["guess_prev"] - orep.guess_prev) <= 1e-12 * orep.guess_prev, k
-        assert abs(rep["guess_residual"] - orep.guess) <= 1e-12 * orep.guess, k
+        scale = max(orep.guess, orep.guess_prev)
+        assert abs(rep["guess_prev"] - orep.guess_prev) <= GUARD_TOL * scale, k
+        assert abs(rep["guess_residual"] - orep.guess) <= GUARD_TOL * scale, k
         assert rep["picard_its"] == orep.picard_its, (k, rep, orep.picard_its)
     assert rel(host(run.fc), orun.fc) < STEP_TOL
 
@@ -162,8 +169,9 @@ def test_initial_guess_entry_point():
     orep = vo.StepReport()
     orun.guess(orep)
     assert bool(kept.value) == orep.guess_kept and orep.guess_kept
-    assert abs(prev.value - orep.guess_prev) <= 1e-12 * orep.guess_prev
-    assert abs(guess.value - orep.guess) <= 1e-12 * orep.guess
+    scale = max(orep.guess, orep.guess_prev)
+    assert abs(prev.value - orep.guess_prev) <= GUARD_TOL * scale
+    assert abs(guess.value - orep.guess) <= GUARD_TOL * scale
     assert rel(host(run.fc), orun.fc) < STEP_TOL
     assert rel(run.pc_int.cpu().numpy(), orun.phi) < 1e-10
 

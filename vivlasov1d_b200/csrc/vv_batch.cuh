@@ -1085,9 +1085,11 @@ __global__ void __launch_bounds__(TJV_THREADS) k_b_tridiagjv(const BInst* __rest
         const R* ga = reinterpret_cast<const R*>(I.tp.gamma);
         const FastDiv dch((unsigned)CH);
         // stage G items: row j of an item's 4 modes is one 32-byte sector
+        // (cols = 4 G is a power of two: shifts, no runtime division)
         const int cols = G * TRIW_WARPS;
+        const int lc = __ffs(cols) - 1;
         for (int t = tid; t < nv * cols; t += TJV_THREADS) {
-            const int j = t / cols, c = t % cols;
+            const int j = t >> lc, c = t & (cols - 1);
             const int k = kbase + c;
             if (k < nm) {
                 C* sb = base + (size_t)(c / TRIW_WARPS) * is + (size_t)(c % TRIW_WARPS) * ws;
@@ -1176,7 +1178,7 @@ __global__ void __launch_bounds__(TJV_THREADS) k_b_tridiagjv(const BInst* __rest
             }
         __syncthreads();
         for (int t = tid; t < nv * cols; t += TJV_THREADS) {
-            const int j = t / cols, c = t % cols;
+            const int j = t >> lc, c = t & (cols - 1);
             const int kk = kbase + c;
             if (kk < nm)
                 spec[(size_t)j * nm + kk] =

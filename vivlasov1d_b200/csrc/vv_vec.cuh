@@ -286,31 +286,40 @@ VV_DEV void gm_arnoldi(DevState* s, double tt) {
     const int ld = s->restart + 2;
     double* hh = s->hh;
 #define HH(a, b) hh[(b) * ld + (a)]
-    for (int j = 0; j <= it; ++j) HH(j, it) = s->hcol[j];
     s->scale = (tt != 0.0) ? 1.0 / tt : 1.0;
     s->vsc[it + 1] = s->scale;
     HH(it + 1, it) = tt;
     double hapbnd = fabs(tt / s->grs[it]);
     if (hapbnd > s->haptol) hapbnd = s->haptol;
     const bool hapend = tt < hapbnd;
+    // apply the previous rotations to the new column hcol (KSPGMRES's
+    // HH(j-1) <- c t + s HH(j), HH(j) <- c HH(j) - s t, t = HH(j-1)): the
+    // value carried from row to row stays in a register and the loads of
+    // hcol, cc and ss do not wait on the stores of earlier rows
+    double hj = s->hcol[0];
     for (int j = 1; j <= it; ++j) {
-        const double t = HH(j - 1, it);
-        HH(j - 1, it) = s->cc[j - 1] * t + s->ss[j - 1] * HH(j, it);
-        HH(j, it) = s->cc[j - 1] * HH(j, it) - s->ss[j - 1] * t;
+        const double hn = s->hcol[j];
+        const double c = s->cc[j - 1], sn = s->ss[j - 1];
+        HH(j - 1, it) = c * hj + sn * hn;
+        hj = c * hn - sn * hj;
     }
+    HH(it, it) = hj;
     bool null = false;
     if (!hapend) {
-        const double t = sqrt(HH(it, it) * HH(it, it) + HH(it + 1, it) * HH(it + 1, it));
+        const double h1 = tt;
+        const double t = sqrt(hj * hj + h1 * h1);
         if (t == 0.0) {
             s->reason = R_NULL;
             null = true;
         } else {
-            s->cc[it] = HH(it, it) / t;
-            s->ss[it] = HH(it + 1, it) / t;
-            s->grs[it + 1] = -(s->ss[it] * s->grs[it]);
-            s->grs[it] = s->cc[it] * s->grs[it];
-            HH(it, it) = s->cc[it] * HH(it, it) + s->ss[it] * HH(it + 1, it);
-            s->res = fabs(s->grs[it + 1]);
+            const double c = hj / t, sn = h1 / t;
+            s->cc[it] = c;
+            s->ss[it] = sn;
+            const double g = s->grs[it];
+            s->grs[it + 1] = -(sn * g);
+            s->grs[it] = c * g;
+            HH(it, it) = c * hj + sn * h1;
+            s->res = fabs(sn * g);
         }
     } else {
         s->res = 0.0;
