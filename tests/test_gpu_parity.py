@@ -440,7 +440,7 @@ BATCH_SPECS = [(64, 128, vo.f0_landau(0.1, 0.5), 4 * np.pi, 0.1),
 
 
 @pytest.mark.parametrize("shape", [None, "2,1,0", "8,2,1", "4,0,1", "2,0,0,1", "2,1,0,1", "2,2,0,1", "2,3,0,1",
-                                   "2,4,0,1", "4,0,1,0,1"])
+                                   "2,4,0,1", "2,5,0,1", "4,0,1,0,1"])
 def test_batch_step_equals_single_steps(monkeypatch, shape):
     """A lockstep batch of uneven instances (every kernel launched once for
     the table, per-instance masks) follows each instance's own time step:
@@ -462,7 +462,8 @@ def test_batch_step_equals_single_steps(monkeypatch, shape):
     assert batch.launch_count() > 0
 
 
-@pytest.mark.parametrize("shape", ["4,0,0", "4,1,1", "2,0,0,1", "2,1,0,1", "2,3,0,1", "2,4,0,1", "2,1,0,1,1"])
+@pytest.mark.parametrize("shape", ["4,0,0", "4,1,1", "2,0,0,1", "2,1,0,1", "2,3,0,1", "2,4,0,1", "2,5,0,1",
+                                   "2,1,0,1,1"])
 def test_batch_graph_equals_host_driven(monkeypatch, shape):
     """The batch graph (conditional loops folded over the instance masks)
     and the host-driven loop over the same kernels (one fixed shape) give
@@ -517,7 +518,8 @@ def test_batch_sweep_instances_match_single_steps():
             _assert_batch_matches(rb[i], r.step(), br[i].fc, r.fc, i, 1e-9)
 
 
-@pytest.mark.parametrize("shape", [None, "4,0,1,0", "2,0,0,1", "2,1,0,1", "2,2,0,1", "2,3,0,1", "2,4,0,1", "2,1,0,1,1"])
+@pytest.mark.parametrize("shape", [None, "4,0,1,0", "2,0,0,1", "2,1,0,1", "2,2,0,1", "2,3,0,1", "2,4,0,1", "2,5,0,1",
+                                   "2,1,0,1,1"])
 def test_batch_mixed_precision_field_energy(monkeypatch, shape):
     """Batched mixed precision against FP64 single steps: field energy to
     1e-9 relative after three steps for every instance (autotuned, the

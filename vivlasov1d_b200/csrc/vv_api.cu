@@ -2556,6 +2556,8 @@ int b_tri(vv_batch* b, const int* L) {
                            b->n, b->nvmax);
         if (b->tri_kind == 4)
             return blaunch(b, vv::k_b_tridiagjv<T>, vv::F_MODES, vv::TJV_THREADS, b->smem_tri_jv, tab, L, b->n);
+        if (b->tri_kind == 5)
+            return blaunch(b, vv::k_b_tridiagjc<T>, vv::F_MODES, vv::TJC_THREADS, 0, tab, L, b->n);
         return blaunch(b, vv::k_b_tridiagj<T>, vv::F_MODES, 32,
                        (size_t)64 * vv::TJ_RING * sizeof(typename Cplx<T>::type), tab, L, b->n);
     }
@@ -2832,7 +2834,8 @@ void b_shape(vv_batch* b, std::vector<vv::BInst>& tab, int R, int tri_kind, int 
             const int rb = vv::fj_rows_of(c->M);
             I.cnt[vv::F_ROWS] = (c->nv + rb - 1) / rb;
             const int items = (c->nmodes + vv::TRIW_WARPS - 1) / vv::TRIW_WARPS;
-            I.cnt[vv::F_MODES] = tri_kind == 4   ? (items + vv::tjv_group(c->nv) - 1) / vv::tjv_group(c->nv)
+            I.cnt[vv::F_MODES] = tri_kind == 5   ? (c->nmodes + vv::TJC_MG - 1) / vv::TJC_MG
+                                 : tri_kind == 4 ? (items + vv::tjv_group(c->nv) - 1) / vv::tjv_group(c->nv)
                                  : tri_kind >= 1 ? items
                                                  : (c->nmodes + 31) / 32;
         }
@@ -2912,7 +2915,7 @@ int b_autotune(vv_batch* b, std::vector<vv::BInst>& tab) {
     int bR = b->R, bW = b->tri_kind, bF = b->fft4, bJ = b->pcj, r = VV_OK;
     for (int pj = 0; pj <= (b->pcj_ok ? 1 : 0) && r == VV_OK; ++pj)
     for (int f4 = 0; f4 <= (pj ? 0 : 1) && r == VV_OK; ++f4)
-    for (int tw = 0; tw <= (pj ? 4 : 2) && r == VV_OK; ++tw) {
+    for (int tw = 0; tw <= (pj ? 5 : 2) && r == VV_OK; ++tw) {
         if (!b_tri_fits(b, tw, pj)) continue;
         for (int R = 2; R <= (pj ? 2 : 8) && r == VV_OK; R *= 2) {
             b_shape(b, tab, R, tw, f4, pj);
@@ -3162,7 +3165,7 @@ int vv_batch_create(int n, vv_ctx* const* ctxs, const vv_state* states, vv_batch
         const char* bs = getenv("VV_BATCH_SHAPE");
         int fR = 0, fT = 0, fF = 0, fJ = 0, fM = 0;
         const int nf = bs ? sscanf(bs, "%d,%d,%d,%d,%d", &fR, &fT, &fF, &fJ, &fM) : 0;
-        const bool fixed = nf >= 3 && (fR == 2 || fR == 4 || fR == 8) && fT >= 0 && fT <= (fJ ? 4 : 2) &&
+        const bool fixed = nf >= 3 && (fR == 2 || fR == 4 || fR == 8) && fT >= 0 && fT <= (fJ ? 5 : 2) &&
                            (fF == 0 || fF == 1) && (fJ == 0 || (fJ == 1 && b->pcj_ok)) && b_tri_fits(b, fT, fJ);
         const char* at = getenv("VV_AUTOTUNE");
         if (fixed) {

@@ -693,11 +693,16 @@ enum BCtrl { BC_PIC = 0, BC_GM_START = 1, BC_INNER = 2, BC_GM_FINISH = 3, BC_REV
 
 constexpr int CTRL_THREADS = 1024;
 
-// rebuild list `l` from the per-instance membership test `in(q)`: one pass
-// of warp scans over (member, work items per family) and one scan of the
-// warp totals per value (CTRL_THREADS threads)
-template <typename In>
-__device__ void ctrl_build(const BInst* __restrict__ tab, int n, int* __restrict__ lists, int l, In in) {
+// rebuild list `l` from the per-instance membership test `in(q)` over the
+// candidates src(0..cnt-1) (every instance, or the list's own members when
+// the list only shrinks: the build then compacts it in place -- a chunk reads
+// its candidates before the barrier that precedes its writes, and every
+// write lands at or before the position it was read from): one pass of warp
+// scans over (member, work items per family) and one scan of the warp totals
+// per value (CTRL_THREADS threads)
+template <typename In, typename Src>
+__device__ void ctrl_build_from(const BInst* __restrict__ tab, int n, int cnt, int* __restrict__ lists, int l, In in,
+                                Src src) {
     constexpr int NV = NFAM + 1, NW = CTRL_THREADS / 32;
     static_assert(NV <= NW, "one warp per scanned value");
     int* L = lists + (size_t)l * blist_words(n);
@@ -709,9 +714,10 @@ __device__ void ctrl_build(const BInst* __restrict__ tab, int n, int* __restrict
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
     if (threadIdx.x < NV) carry[threadIdx.x] = 0;
     __syncthreads();
-    for (int q0 = 0; q0 < n; q0 += CTRL_THREADS) {
-        const int q = q0 + threadIdx.x;
-        const bool on = q < n && in(q);
+    for (int i0 = 0; i0 < cnt; i0 += CTRL_THREADS) {
+        const int i = i0 + threadIdx.x;
+        const int q = i < cnt ? src(i) : 0;
+        const bool on = i < cnt && in(q);
         int v[NV], inc[NV];
         v[0] = on ? 1 : 0;
 #pragma unroll
@@ -758,6 +764,11 @@ __device__ void ctrl_build(const BInst* __restrict__ tab, int n, int* __restrict
         }
     }
     __syncthreads();
+}
+
+template <typename In>
+__device__ void ctrl_build(const BInst* __restrict__ tab, int n, int* __restrict__ lists, int l, In in) {
+    ctrl_build_from(tab, n, n, lists, l, in, [](int i) { return i; });
 }
 
 // the control step by one block of CTRL_THREADS threads
@@ -831,7 +842,23 @@ k_b_arnoldi_ctrl(const BInst* __restrict__ tab, const int* __restrict__ L, int n
         }
     });
     if (!last_block(done, gridDim.x)) return;
-    ctrl_run(tab, n, BC_INNER, handle, flag, counts, lists);
+    // the inner loop only drops instances: compact the current L_INNER in
+    // place instead of scanning the whole table (a tail pass with a few
+    // instances left reads a few states, not n)
+    int* LI = lists + (size_t)L_INNER * blist_words(n);
+    const int cnt = LI[0];
+    const int* ids = LI + 1 + NFAM;
+    __syncthreads();
+    ctrl_build_from(tab, n, cnt, lists, L_INNER, [&](int q) {
+        const DevState* s = tab[q].ds;
+        return s->gm_outer != 0 && s->active != 0;
+    }, [&](int i) { return ids[i]; });
+    if (threadIdx.x == 0) {
+        const int any = LI[0] > 0 ? 1 : 0;
+        set_cond(handle, any ? 1u : 0u);
+        if (flag) *flag = any;
+        if (any && counts) counts[BC_INNER] += 1u;
+    }
 }
 
 // set the Arnoldi index of every instance (kernel timing)
@@ -1185,6 +1212,120 @@ __global__ void __launch_bounds__(TJV_THREADS) k_b_tridiagjv(const BInst* __rest
                     base[(size_t)(c / TRIW_WARPS) * is + (size_t)(c % TRIW_WARPS) * ws + j + (int)dch((unsigned)j)];
         }
         __syncthreads();
+    });
+}
+
+// ---- LU solves on the v-major layout: lane per mode, threads per row chunk ----
+// A CTA takes TJC_MG consecutive x modes of one instance and splits their
+// lines into TJC_NC chunks of CH = ceil(nv / TJC_NC) rows: thread (c, m)
+// sweeps rows [c CH, (c+1) CH) of mode m.  The TJC_MG lanes of a chunk read
+// one row of TJC_MG consecutive modes (64 contiguous bytes in FP32) straight
+// from the spectrum and the LU reciprocals in global memory -- no staging, no
+// pad slots -- and the chunk's affine maps are joined per mode by one warp
+// scan over the TJC_NC chunks (a warp per mode, through shared memory).  The
+// replay sweeps re-read their rows (L1/L2) and write y, then x, in place.
+constexpr int TJC_MG = 8, TJC_NC = 32, TJC_THREADS = TJC_MG * TJC_NC;
+
+template <typename R>
+__global__ void __launch_bounds__(TJC_THREADS) k_b_tridiagjc(const BInst* __restrict__ tab, const int* __restrict__ L,
+                                                             int n) {
+    using C = typename Cplx<R>::type;
+    static_assert(TJC_NC == 32 && TJC_MG <= TJC_THREADS / 32, "one warp scans the chunks of one mode");
+    __shared__ Aff<C> tot[TJC_NC][TJC_MG];
+    for_work<F_MODES>(tab, L, n, [&](const BInst& I, int local) {
+        const int nv = I.tp.nv, nm = I.tp.nmodes;
+        const int CH = (nv + TJC_NC - 1) / TJC_NC;
+        const int tid = threadIdx.x;
+        const int m = tid % TJC_MG, c = tid / TJC_MG;
+        const int k = local * TJC_MG + m;
+        const bool on = k < nm;
+        C* col = (C*)I.specT + k;                         // row r at col[r * nm]
+        const C* dcol = (const C*)I.dinvJ + k;
+        const R* al = reinterpret_cast<const R*>(I.tp.alpha);
+        const R* ga = reinterpret_cast<const R*>(I.tp.gamma);
+        const C lam = on ? reinterpret_cast<const C*>(I.tp.lambda)[k] : c_make<C>(0.0, 0.0);
+        const int r0 = c * CH, r1 = min(r0 + CH, nv);
+        const size_t ld = (size_t)nm;
+        // forward: y_r = b_r - l_r y_{r-1},  l_r = lambda alpha_r / U_{r-1}
+        Aff<C> a;
+        a.P = c_make<C>(1.0, 0.0);
+        a.Q = c_make<C>(0.0, 0.0);
+        if (on) {
+#pragma unroll 4
+            for (int r = r0; r < r1; ++r) {
+                Aff<C> mp;
+                mp.Q = col[r * ld];
+                if (r == 0) mp.P = c_make<C>(0.0, 0.0);
+                else {
+                    const C lr = c_mul(c_rmul(lam, __ldg(al + r)), dcol[(r - 1) * ld]);
+                    mp.P = c_make<C>(-lr.x, -lr.y);
+                }
+                a = aff_combine(a, mp);
+            }
+        }
+        tot[c][m] = a;
+        __syncthreads();
+        if (tid < TJC_MG * 32) {                           // warp w scans the chunks of mode w
+            const int w = tid >> 5, lane = tid & 31;
+            Aff<C> ex;
+            warp_scan_aff_ie<C>(tot[lane][w], true, &ex);
+            __syncwarp();
+            tot[lane][w] = ex;
+        }
+        __syncthreads();
+        C y = tot[c][m].Q;
+        if (on) {
+#pragma unroll 4
+            for (int r = r0; r < r1; ++r) {
+                const C b = col[r * ld];
+                if (r == 0) y = b;
+                else {
+                    const C lr = c_mul(c_rmul(lam, __ldg(al + r)), dcol[(r - 1) * ld]);
+                    y = c_sub(b, c_mul(lr, y));
+                }
+                col[r * ld] = y;
+            }
+        }
+        __syncthreads();   // every chunk's exclusive prefix read before the maps are overwritten
+        // backward: x_r = U_r^-1 (y_r - c_r x_{r+1}) == mu_r + nu_r x_{r+1}
+        a.P = c_make<C>(1.0, 0.0);
+        a.Q = c_make<C>(0.0, 0.0);
+        if (on) {
+#pragma unroll 4
+            for (int r = r1 - 1; r >= r0; --r) {
+                Aff<C> mp;
+                const C d = dcol[r * ld];
+                mp.Q = c_mul(d, col[r * ld]);
+                if (r == nv - 1) mp.P = c_make<C>(0.0, 0.0);
+                else {
+                    const C nu = c_mul(d, c_rmul(lam, __ldg(ga + r)));
+                    mp.P = c_make<C>(-nu.x, -nu.y);
+                }
+                a = aff_combine(a, mp);
+            }
+        }
+        tot[c][m] = a;
+        __syncthreads();
+        if (tid < TJC_MG * 32) {                           // chunks in descending order
+            const int w = tid >> 5, lane = tid & 31;
+            Aff<C> ex;
+            warp_scan_aff_ie<C>(tot[lane][w], false, &ex);
+            __syncwarp();
+            tot[lane][w] = ex;
+        }
+        __syncthreads();
+        C x = tot[c][m].Q;
+        if (on) {
+#pragma unroll 4
+            for (int r = r1 - 1; r >= r0; --r) {
+                const C d = dcol[r * ld];
+                const C yv = col[r * ld];
+                if (r == nv - 1) x = c_mul(d, yv);
+                else x = c_mul(d, c_sub(yv, c_mul(c_rmul(lam, __ldg(ga + r)), x)));
+                col[r * ld] = x;
+            }
+        }
+        __syncthreads();   // the prefixes read before the next item reuses the array
     });
 }
 
