@@ -2475,7 +2475,6 @@ struct vv_batch {
     size_t smem_tri_js;          // k_b_tridiagjs (padded warp slices)
     size_t smem_tri_jm2, smem_tri_jm4;   // k_b_tridiagjm, 2 and 4 warps per mode
     size_t smem_tri_jv;                  // k_b_tridiagjv (lanes per mode by line length)
-    bool pdl;                            // batch kernels with programmatic dependent launch (VV_PDL=0: off)
     int nvmax;                   // largest velocity grid of the table
     int smem_limit;              // dynamic shared memory per block available to the batch kernels
     double* wpart;               // device: per-warp partial sums of every instance
@@ -2517,24 +2516,9 @@ int blaunch(vv_batch* b, void (*k)(KA...), int fam, dim3 threads, size_t smem, A
     if (e != cudaSuccess) return fail_cuda(e, "batch occupancy");
     const long cap = (long)std::max(1, per_sm) * b->nsm;
     const unsigned grid = (unsigned)std::max<long>(1, std::min<long>(cap, b->tot[fam]));
-    if (b->pdl) {
-        // programmatic dependent launch (the kernels wait for their predecessor in for_work)
-        cudaLaunchConfig_t cfg = {};
-        cfg.gridDim = dim3(grid);
-        cfg.blockDim = threads;
-        cfg.dynamicSmemBytes = smem;
-        cfg.stream = b->st;
-        cudaLaunchAttribute attr[1];
-        attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
-        attr[0].val.programmaticStreamSerializationAllowed = 1;
-        cfg.attrs = attr;
-        cfg.numAttrs = 1;
-        e = cudaLaunchKernelEx(&cfg, k, args...);
-    } else {
-        k<<<grid, threads, smem, b->st>>>(args...);
-        e = cudaGetLastError();
-    }
+    k<<<grid, threads, smem, b->st>>>(args...);
     b->launches++;
+    e = cudaGetLastError();
     return e == cudaSuccess ? VV_OK : fail_cuda(e, "batch kernel launch");
 }
 
@@ -3046,10 +3030,6 @@ int vv_batch_create(int n, vv_ctx* const* ctxs, const vv_state* states, vv_batch
     b->scheme = c0->g.bracket;
     b->R = 4;
     b->use_graph = c0->use_graph;
-    {
-        const char* e = getenv("VV_PDL");
-        b->pdl = !(e && e[0] == '0');
-    }
     auto fail_b = [&](int code) { vv_batch_destroy(b); return code; };
     if (cudaDeviceGetAttribute(&b->nsm, cudaDevAttrMultiProcessorCount, c0->device) != cudaSuccess)
         return fail_b(fail_cuda(cudaGetLastError(), "multiprocessor count"));

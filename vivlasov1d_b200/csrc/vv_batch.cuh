@@ -59,15 +59,6 @@ __host__ __device__ constexpr size_t blist_words(int n) { return 1 + NFAM + (siz
 // active instances whose list a block stages in shared memory for the search
 constexpr int BLIST_SMEM = 512;
 
-// Programmatic dependent launch: the batch kernels are launched so that the
-// next kernel of the stream can be scheduled before this one has finished
-// (its launch latency hidden behind this kernel's tail); every batch kernel
-// first waits until the kernel before it has completed and its memory is
-// visible, then lets its own successor start launching.  Without the launch
-// attribute both are no-ops.
-VV_DEV void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
-VV_DEV void pdl_trigger() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
-
 // Loop of a persistent block over the work items of family F in list L:
 // body(instance, local block).  Block-uniform; a barrier separates items.
 // Lists of up to BLIST_SMEM instances are searched in shared memory.
@@ -75,8 +66,6 @@ template <int F, typename Body>
 VV_DEV void for_work(const BInst* __restrict__ tab, const int* __restrict__ L, int n, Body body) {
     __shared__ int s_pre[BLIST_SMEM + 1];
     __shared__ int s_ids[BLIST_SMEM];
-    pdl_wait();
-    pdl_trigger();
     const int nact = L[0];
     const int total = L[1 + F];
     if ((int)blockIdx.x >= total) return;
@@ -112,8 +101,6 @@ template <int F, typename Body>
 VV_DEV void for_warp_work(const BInst* __restrict__ tab, const int* __restrict__ L, int n, Body body) {
     __shared__ int s_pre[BLIST_SMEM + 1];
     __shared__ int s_ids[BLIST_SMEM];
-    pdl_wait();
-    pdl_trigger();
     const int nact = L[0];
     const int total = L[1 + F];
     if ((int)blockIdx.x >= total) return;
