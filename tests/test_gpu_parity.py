@@ -440,7 +440,7 @@ BATCH_SPECS = [(64, 128, vo.f0_landau(0.1, 0.5), 4 * np.pi, 0.1),
 
 
 @pytest.mark.parametrize("shape", [None, "2,1,0", "8,2,1", "4,0,1", "2,0,0,1", "2,1,0,1", "2,2,0,1", "2,3,0,1",
-                                   "2,4,0,1", "2,5,0,1", "4,0,1,0,1"])
+                                   "2,4,0,1", "2,5,0,1", "2,6,0,1", "4,0,1,0,1"])
 def test_batch_step_equals_single_steps(monkeypatch, shape):
     """A lockstep batch of uneven instances (every kernel launched once for
     the table, per-instance masks) follows each instance's own time step:
@@ -462,7 +462,30 @@ def test_batch_step_equals_single_steps(monkeypatch, shape):
     assert batch.launch_count() > 0
 
 
-@pytest.mark.parametrize("shape", ["4,0,0", "4,1,1", "2,0,0,1", "2,1,0,1", "2,3,0,1", "2,4,0,1", "2,5,0,1",
+RAGGED_SPECS = [(64, 100, vo.f0_landau(0.1, 0.5), 4 * np.pi, 0.1),
+                (128, 72, vo.f0_twostream(0.05, 0.5), 4 * np.pi, 0.1),
+                (64, 330, vo.f0_bump_on_tail(0.04, 0.3), 2 * np.pi / 0.3, 0.1)]
+
+
+@pytest.mark.parametrize("tri", [0, 1, 2, 3, 4, 5, 6])
+def test_batch_ragged_lines_equal_single_steps(monkeypatch, tri):
+    """Velocity grids that no chunk or warp split divides (nv 100, 72, 330):
+    every tridiagonal variant of the v-major preconditioner, batch against
+    each instance's own step."""
+    from vivlasov1d_b200.batch import Batch
+    batch_runs = [_small_run(*s) for s in RAGGED_SPECS]
+    single_runs = [_small_run(*s) for s in RAGGED_SPECS]
+    monkeypatch.setenv("VV_BATCH_SHAPE", "2,%d,0,1" % tri)
+    batch = Batch(batch_runs)
+    for _ in range(2):
+        rb = batch.step()
+        for i, r in enumerate(single_runs):
+            rs = r.step()
+            assert rb[i]["status"] == 0
+            _assert_batch_matches(rb[i], rs, batch_runs[i].fc, r.fc, i, 1e-10)
+
+
+@pytest.mark.parametrize("shape", ["4,0,0", "4,1,1", "2,0,0,1", "2,1,0,1", "2,3,0,1", "2,4,0,1", "2,5,0,1", "2,6,0,1",
                                    "2,1,0,1,1"])
 def test_batch_graph_equals_host_driven(monkeypatch, shape):
     """The batch graph (conditional loops folded over the instance masks)
@@ -519,7 +542,7 @@ def test_batch_sweep_instances_match_single_steps():
 
 
 @pytest.mark.parametrize("shape", [None, "4,0,1,0", "2,0,0,1", "2,1,0,1", "2,2,0,1", "2,3,0,1", "2,4,0,1", "2,5,0,1",
-                                   "2,1,0,1,1"])
+                                   "2,6,0,1", "2,1,0,1,1"])
 def test_batch_mixed_precision_field_energy(monkeypatch, shape):
     """Batched mixed precision against FP64 single steps: field energy to
     1e-9 relative after three steps for every instance (autotuned, the

@@ -2464,13 +2464,15 @@ struct vv_batch {
     int scheme;
     int R;                       // FFT rows per CTA
     int fft4;                    // x-FFTs: 1 four-step register/shuffle, 0 radix-2
-    int pcj;                     // 1: preconditioner in the v-major layout (vv_pcj.cuh); fft4/R/tri_kind unused
+    int pcj;                     // 1: preconditioner in the v-major layout (vv_pcj.cuh); fft4/R unused
     int march;                   // 1: Jacobian stencil by the marching kernel, 0: 64 x 32 tiles
     bool pcj_ok;                 // every instance has M in 32..256 (the v-major kernels' lengths)
     void* dinvJ;                 // device: v-major LU reciprocals of every instance (GMRES precision)
     size_t smem_fftj;            // dynamic shared memory of the v-major FFT blocks
     int tri_kind;                // tridiagonal solves: 0 CTA per mode (tables staged), 1 warp per mode,
-                                 // 2 CTA per mode (tables through L1)
+                                 // 2 CTA per mode (tables through L1); v-major: 0 lane per mode, 1 warp
+                                 // per mode, 2/3 two/four warps per mode, 4 lanes by line length, 5 lane
+                                 // per mode with chunk scans, 6 register-resident chunks
     size_t smem_tri_stage, smem_tri_plain, smem_tri_warp;
     size_t smem_tri_js;          // k_b_tridiagjs (padded warp slices)
     size_t smem_tri_jm2, smem_tri_jm4;   // k_b_tridiagjm, 2 and 4 warps per mode
@@ -2558,6 +2560,8 @@ int b_tri(vv_batch* b, const int* L) {
             return blaunch(b, vv::k_b_tridiagjv<T>, vv::F_MODES, vv::TJV_THREADS, b->smem_tri_jv, tab, L, b->n);
         if (b->tri_kind == 5)
             return blaunch(b, vv::k_b_tridiagjc<T>, vv::F_MODES, vv::TJC_THREADS, 0, tab, L, b->n);
+        if (b->tri_kind == 6)
+            return blaunch(b, vv::k_b_tridiagjr<T>, vv::F_MODES, vv::TJR_THREADS, 0, tab, L, b->n);
         return blaunch(b, vv::k_b_tridiagj<T>, vv::F_MODES, 32,
                        (size_t)64 * vv::TJ_RING * sizeof(typename Cplx<T>::type), tab, L, b->n);
     }
@@ -2834,7 +2838,9 @@ void b_shape(vv_batch* b, std::vector<vv::BInst>& tab, int R, int tri_kind, int 
             const int rb = vv::fj_rows_of(c->M);
             I.cnt[vv::F_ROWS] = (c->nv + rb - 1) / rb;
             const int items = (c->nmodes + vv::TRIW_WARPS - 1) / vv::TRIW_WARPS;
-            I.cnt[vv::F_MODES] = tri_kind == 5   ? (c->nmodes + vv::TJC_MG - 1) / vv::TJC_MG
+            const int tch = vv::tjr_ch(b->mixed ? 4 : 8);
+            I.cnt[vv::F_MODES] = tri_kind == 6   ? (c->nmodes + vv::tjr_modes(c->nv, tch) - 1) / vv::tjr_modes(c->nv, tch)
+                                 : tri_kind == 5 ? (c->nmodes + vv::TJC_MG - 1) / vv::TJC_MG
                                  : tri_kind == 4 ? (items + vv::tjv_group(c->nv) - 1) / vv::tjv_group(c->nv)
                                  : tri_kind >= 1 ? items
                                                  : (c->nmodes + 31) / 32;
@@ -2860,6 +2866,7 @@ int b_apply_shape(vv_batch* b, const std::vector<vv::BInst>& tab) {
 // whether tridiagonal variant tw (layout pj) fits the device's shared memory
 bool b_tri_fits(const vv_batch* b, int tw, int pj) {
     size_t need = 0;
+    if (pj && tw == 6) return b->nvmax <= vv::tjr_nvmax(b->mixed ? 4 : 8);   // chunks held in registers
     if (pj)
         need = tw == 1 ? b->smem_tri_js : tw == 2 ? b->smem_tri_jm2 : tw == 3 ? b->smem_tri_jm4 : tw == 4 ? b->smem_tri_jv : 0;
     else if (tw == 1) need = b->smem_tri_warp;
@@ -2915,7 +2922,7 @@ int b_autotune(vv_batch* b, std::vector<vv::BInst>& tab) {
     int bR = b->R, bW = b->tri_kind, bF = b->fft4, bJ = b->pcj, r = VV_OK;
     for (int pj = 0; pj <= (b->pcj_ok ? 1 : 0) && r == VV_OK; ++pj)
     for (int f4 = 0; f4 <= (pj ? 0 : 1) && r == VV_OK; ++f4)
-    for (int tw = 0; tw <= (pj ? 5 : 2) && r == VV_OK; ++tw) {
+    for (int tw = 0; tw <= (pj ? 6 : 2) && r == VV_OK; ++tw) {
         if (!b_tri_fits(b, tw, pj)) continue;
         for (int R = 2; R <= (pj ? 2 : 8) && r == VV_OK; R *= 2) {
             b_shape(b, tab, R, tw, f4, pj);
@@ -3165,7 +3172,7 @@ int vv_batch_create(int n, vv_ctx* const* ctxs, const vv_state* states, vv_batch
         const char* bs = getenv("VV_BATCH_SHAPE");
         int fR = 0, fT = 0, fF = 0, fJ = 0, fM = 0;
         const int nf = bs ? sscanf(bs, "%d,%d,%d,%d,%d", &fR, &fT, &fF, &fJ, &fM) : 0;
-        const bool fixed = nf >= 3 && (fR == 2 || fR == 4 || fR == 8) && fT >= 0 && fT <= (fJ ? 5 : 2) &&
+        const bool fixed = nf >= 3 && (fR == 2 || fR == 4 || fR == 8) && fT >= 0 && fT <= (fJ ? 6 : 2) &&
                            (fF == 0 || fF == 1) && (fJ == 0 || (fJ == 1 && b->pcj_ok)) && b_tri_fits(b, fT, fJ);
         const char* at = getenv("VV_AUTOTUNE");
         if (fixed) {

@@ -1329,4 +1329,196 @@ __global__ void __launch_bounds__(TJC_THREADS) k_b_tridiagjc(const BInst* __rest
     });
 }
 
+// ---- LU solves on the v-major layout, chunks held in registers ---------------
+// Every lane owns a chunk of CH <= tjr_ch rows of one mode and keeps its right
+// hand side and LU reciprocals in registers from one load to the store of the
+// solution: the four sweeps (compose and replay, forward and backward) read
+// no memory, so a row costs its arithmetic and one global load or store per
+// value.  A warp holds 4 consecutive modes x 8 chunks (lane = 4 c + m: the 8
+// rows a warp loads at once are 32-byte runs of the v-major spectrum); G
+// warps, a power of two up to TJR_G with 8 G CH >= nv, cover a mode group's
+// lines, and a CTA of TJR_G warps solves TJR_G / G groups (64 / G modes).
+// The chunks' affine maps are scanned with shuffles inside the warp and
+// joined across the G warps by a shuffle tree over their totals in shared
+// memory.  Chunks of 8 rows in FP32 and 4 in FP64 (registers).
+constexpr int TJR_G = 16, TJR_THREADS = 32 * TJR_G;
+__host__ __device__ constexpr int tjr_ch(size_t rsz) { return rsz == 4 ? 8 : 4; }
+__host__ __device__ constexpr int tjr_nvmax(size_t rsz) { return 8 * TJR_G * tjr_ch(rsz); }
+__host__ __device__ constexpr int tjr_g(int nv, int ch) {
+    return nv <= 8 * ch ? 1 : nv <= 16 * ch ? 2 : nv <= 32 * ch ? 4 : nv <= 64 * ch ? 8 : 16;
+}
+__host__ __device__ constexpr int tjr_modes(int nv, int ch) { return 4 * (TJR_G / tjr_g(nv, ch)); }   // modes per CTA item
+
+// shfl of an affine map from lane src (full warp)
+template <typename C>
+VV_DEV Aff<C> shfl_aff_idx(const Aff<C>& a, int src) {
+    Aff<C> r;
+    r.P.x = __shfl_sync(0xffffffffu, a.P.x, src);
+    r.P.y = __shfl_sync(0xffffffffu, a.P.y, src);
+    r.Q.x = __shfl_sync(0xffffffffu, a.Q.x, src);
+    r.Q.y = __shfl_sync(0xffffffffu, a.Q.y, src);
+    return r;
+}
+
+// the composition, in order, of the maps t[0..cnt) of a lane's mode (cnt <=
+// 16; one value per 8 chunk lanes of stride 4): lane c composes t[2c], t[2c+1]
+// and a tree over the 8 chunk lanes joins them; every lane gets the result
+template <typename C>
+VV_DEV Aff<C> tjr_join(const Aff<C>* t, int stride, int cnt, int c, int m) {
+    Aff<C> id;
+    id.P = c_make<C>(1.0, 0.0);
+    id.Q = c_make<C>(0.0, 0.0);
+    Aff<C> a = 2 * c < cnt ? t[(2 * c) * stride] : id;
+    if (2 * c + 1 < cnt) a = aff_combine(a, t[(2 * c + 1) * stride]);
+#pragma unroll
+    for (int d = 1; d < 8; d <<= 1) {
+        const Aff<C> o = shfl_aff(a, 4 * d, false);
+        if ((c & (2 * d - 1)) == 0 && c + d < 8) a = aff_combine(a, o);
+    }
+    return shfl_aff_idx(a, m);
+}
+
+// ordered composition of the maps mp(0) .. mp(CH - 1) (mp(0) first) as two
+// independent chains over the halves joined at the end: half the dependent
+// depth of one chain for two more registers of live state
+template <typename C, int CH, typename Map>
+VV_DEV Aff<C> aff_two_chains(Map mp) {
+    Aff<C> a = mp(0), b = mp(CH / 2);
+#pragma unroll
+    for (int j = 1; j < CH / 2; ++j) {
+        a = aff_combine(a, mp(j));
+        b = aff_combine(b, mp(CH / 2 + j));
+    }
+    return aff_combine(a, b);
+}
+
+// One lane's chunk: rows r0 .. r0 + n of mode k (FULL: n == CH for every lane
+// of the CTA, no guards).  The forward multipliers l_r and then the backward
+// products lambda gamma_r stay in registers between a sweep's compose and its
+// replay.  Lanes without a mode run the same instructions on zeros (a
+// branch around the work of idle warps keeps more state live across the
+// barriers and spills).
+template <typename R, bool FULL>
+VV_DEV void tjr_chunk(const BInst& I, int k, bool on, int r0, int n, int G, int grp, int sw, int c, int m,
+                      Aff<typename Cplx<R>::type> (*tot)[TJR_G][4]) {
+    using C = typename Cplx<R>::type;
+    constexpr int CH = tjr_ch(sizeof(R));
+    const int nv = I.tp.nv;
+    const size_t ld = (size_t)I.tp.nmodes;
+    C* col = (C*)I.specT + k + (size_t)r0 * ld;       // row r0 + j at col[j * ld]
+    const C* dcol = (const C*)I.dinvJ + k + (size_t)r0 * ld;
+    const C zero = c_make<C>(0.0, 0.0);
+    const bool first = r0 == 0, last = r0 + n == nv;   // the chunk holds row 0 / row nv - 1
+    Aff<C> id;
+    id.P = c_make<C>(1.0, 0.0);
+    id.Q = zero;
+    C lam = zero;
+    C bb[CH], dd[CH], ll[CH];
+    R gg[CH];
+    Aff<C> ex = id;
+    {
+        const R* al = reinterpret_cast<const R*>(I.tp.alpha) + r0;
+        const R* ga = reinterpret_cast<const R*>(I.tp.gamma) + r0;
+        if (on) lam = reinterpret_cast<const C*>(I.tp.lambda)[k];
+#pragma unroll
+        for (int j = 0; j < CH; ++j) {
+            const bool in = FULL || j < n;
+            bb[j] = in ? col[j * ld] : zero;
+            dd[j] = in ? dcol[j * ld] : zero;
+            const R a = in ? __ldg(al + j) : (R)0;
+            gg[j] = in ? __ldg(ga + j) : (R)0;
+            ll[j] = c_rmul(lam, a);
+        }
+        const C dp0 = (n > 0 && !first) ? dcol[-(ptrdiff_t)ld] : zero;   // U^-1 of the row before the chunk
+        // forward: y_r = b_r - l_r y_{r-1},  l_r = lambda alpha_r / U_{r-1}
+#pragma unroll
+        for (int j = 0; j < CH; ++j) ll[j] = c_mul(ll[j], j == 0 ? dp0 : dd[j > 0 ? j - 1 : 0]);
+        Aff<C> inc = aff_two_chains<C, CH>([&](int j) {
+            Aff<C> mp;
+            mp.Q = bb[j];
+            mp.P = (j == 0 && first) ? zero : c_make<C>(-ll[j].x, -ll[j].y);
+            return (FULL || j < n) ? mp : id;
+        });
+#pragma unroll
+        for (int d = 1; d < 8; d <<= 1) {
+            const Aff<C> o = shfl_aff(inc, 4 * d, true);
+            if (c >= d) inc = aff_combine(o, inc);
+        }
+        ex = shfl_aff(inc, 4, true);
+        if (c == 0) ex = id;
+        if (c == 7) tot[0][grp * G + sw][m] = inc;
+    }
+    __syncthreads();
+    {
+        const Aff<C> pre = tjr_join<C>(&tot[0][grp * G][m], 4, sw, c, m);
+        C y = aff_combine(pre, ex).Q;
+#pragma unroll
+        for (int j = 0; j < CH; ++j) {
+            if (FULL || j < n) {
+                y = (j == 0 && first) ? bb[j] : c_sub(bb[j], c_mul(ll[j], y));
+                bb[j] = y;
+            }
+        }
+        // backward: x_r = U_r^-1 (y_r - c_r x_{r+1}) == mu_r + nu_r x_{r+1}; map i is row CH - 1 - i
+#pragma unroll
+        for (int j = 0; j < CH; ++j) ll[j] = c_rmul(lam, gg[j]);
+        Aff<C> inc = aff_two_chains<C, CH>([&](int i) {
+            const int j = CH - 1 - i;
+            const C nu = c_mul(dd[j], ll[j]);
+            Aff<C> mp;
+            mp.Q = c_mul(dd[j], bb[j]);
+            mp.P = (j == n - 1 && last) ? zero : c_make<C>(-nu.x, -nu.y);
+            return (FULL || j < n) ? mp : id;
+        });
+#pragma unroll
+        for (int d = 1; d < 8; d <<= 1) {
+            const Aff<C> o = shfl_aff(inc, 4 * d, false);
+            if (c + d < 8) inc = aff_combine(o, inc);
+        }
+        ex = shfl_aff(inc, 4, false);
+        if (c == 7) ex = id;
+        if (c == 0) tot[1][grp * G + sw][m] = inc;
+    }
+    __syncthreads();
+    {
+        // the warps above this one, highest first: tot[1][grp G + G - 1 - u], u < G - 1 - sw
+        const Aff<C> post = tjr_join<C>(&tot[1][grp * G + G - 1][m], -4, G - 1 - sw, c, m);
+        C x = aff_combine(post, ex).Q;
+#pragma unroll
+        for (int j = CH - 1; j >= 0; --j) {
+            if (FULL || j < n) {
+                x = (j == n - 1 && last) ? c_mul(dd[j], bb[j]) : c_mul(dd[j], c_sub(bb[j], c_mul(ll[j], x)));
+                col[j * ld] = x;
+            }
+        }
+    }
+}
+
+template <typename R>
+__global__ void __launch_bounds__(TJR_THREADS, 1)
+    k_b_tridiagjr(const BInst* __restrict__ tab, const int* __restrict__ L, int n) {
+    using C = typename Cplx<R>::type;
+    constexpr int CHM = tjr_ch(sizeof(R));
+    __shared__ Aff<C> tot[2][TJR_G][4];
+    for_work<F_MODES>(tab, L, n, [&](const BInst& I, int local) {
+        const int nv = I.tp.nv, nm = I.tp.nmodes;
+        const int G = tjr_g(nv, CHM), MPB = tjr_modes(nv, CHM);
+        const int CH = (nv + 8 * G - 1) / (8 * G);
+        const int wid = threadIdx.x >> 5, lane = threadIdx.x & 31;
+        const int m = lane & 3, c = lane >> 2;
+        const int grp = wid / G, sw = wid % G;
+        const int k = local * MPB + 4 * grp + m;
+        const bool on = k < nm;
+        const int r0 = min((8 * sw + c) * CH, nv);
+        const int cnt = on ? min(CH, nv - r0) : 0;
+        // block-uniform choice (both paths hold barriers): every mode of the
+        // item present and every chunk CHM rows long
+        if ((local + 1) * MPB <= nm && nv == 8 * G * CHM)
+            tjr_chunk<R, true>(I, k, true, r0, CHM, G, grp, sw, c, m, tot);
+        else
+            tjr_chunk<R, false>(I, on ? k : 0, on, r0, cnt, G, grp, sw, c, m, tot);
+        __syncthreads();   // the totals read before the next item overwrites them
+    });
+}
+
 }  // namespace vv
