@@ -2649,7 +2649,7 @@ int b_cycle_head(vv_batch* b) {
     TRY(b_pc<T>(b, vv::L_GMR, false, vv::BD_V0));
     TRY(blaunch(b, vv::k_b_gm_head<T>, vv::F_VEC, vv::RED_THREADS, 0, tab, G, b->n));
     TRY(blaunch(b, vv::k_b_gm_cycle_p<T>, vv::F_VEC, vv::RED_THREADS, 0, tab, G, b->n));
-    TRY(blaunch(b, vv::k_b_gm_cycle_f, vv::F_INST, 32, 0, tab, G, b->n));
+    TRY(blaunch(b, vv::k_b_gm_cycle_f, vv::F_INST, vv::CTRL_THREADS, 0, tab, G, b->n));
     return b_ctrl(b, vv::BC_INNER, BH_INNER);
 }
 
@@ -2660,7 +2660,7 @@ int b_arnoldi(vv_batch* b) {
     TRY(b_jvp<S, vv::BS_VIT, T>(b, A));
     TRY(b_pc<T>(b, vv::L_INNER, false, vv::BD_VNEXT));
     TRY(blaunch(b, vv::k_b_gm_mdot_p<T>, vv::F_VEC, vv::RED_THREADS, 0, tab, A, b->n));
-    TRY(blaunch(b, vv::k_b_gm_mdot_f, vv::F_INST, vv::RED_THREADS, 0, tab, A, b->n));
+    TRY(blaunch(b, vv::k_b_gm_mdot_f, vv::F_INST, vv::CTRL_THREADS, 0, tab, A, b->n));
     TRY(blaunch(b, vv::k_b_gm_maxpy_p<T>, vv::F_VEC, vv::RED_THREADS, 0, tab, A, b->n));
     // ||w||, Arnoldi bookkeeping and the BC_INNER control step in one launch
     return blaunch(b, vv::k_b_arnoldi_ctrl, vv::F_INST, vv::CTRL_THREADS, 0, tab, A, b->n,

@@ -58,6 +58,7 @@ __host__ __device__ constexpr size_t blist_words(int n) { return 1 + NFAM + (siz
 
 // active instances whose list a block stages in shared memory for the search
 constexpr int BLIST_SMEM = 512;
+constexpr int CTRL_THREADS = 1024;   // control blocks and the per-instance finalize kernels
 
 // Loop of a persistent block over the work items of family F in list L:
 // body(instance, local block).  Block-uniform; a barrier separates items.
@@ -93,17 +94,25 @@ VV_DEV void for_work(const BInst* __restrict__ tab, const int* __restrict__ L, i
 
 // Warp-granular loop over the same work: block item b of an instance is the
 // eight warp items 8 b .. 8 b + 7, and every warp walks the list's warp items
-// on its own (body(instance, local warp item), warp-uniform), with no barrier
-// between items, so the warps of an SM overlap one item's header loads with
-// another's data.  For bodies that use no shared memory per item; the block
-// must have 8 warps.
-template <int F, typename Body>
+// on its own (body(instance, local warp item, part, split), warp-uniform),
+// with no barrier between items, so the warps of an SM overlap one item's
+// header loads with another's data.  With Split, a list with fewer warp items
+// than the grid has warps gives each item to `split` warps (part 0 .. split
+// - 1) to divide among them.  For bodies that use no shared memory per item;
+// the block must have 8 warps.
+constexpr int MAX_SPLIT = 8;
+template <int F, bool Split = false, typename Body>
 VV_DEV void for_warp_work(const BInst* __restrict__ tab, const int* __restrict__ L, int n, Body body) {
     __shared__ int s_pre[BLIST_SMEM + 1];
     __shared__ int s_ids[BLIST_SMEM];
     const int nact = L[0];
     const int total = L[1 + F];
-    if ((int)blockIdx.x >= total) return;
+    const int nw = gridDim.x * 8, wtotal = 8 * total;
+    // split factor: when the list holds fewer warp items than the grid has
+    // warps (a few instances left), every item is taken by `split` warps,
+    // which the body divides its work among (body(instance, item, part))
+    const int split = Split ? max(1, min(MAX_SPLIT, nw / max(1, wtotal))) : 1;
+    if ((int)blockIdx.x * 8 >= wtotal * split) return;
     const int* ids = L + 1 + NFAM;
     const int* pre = ids + n + (size_t)F * (n + 1);
     if (nact <= BLIST_SMEM) {
@@ -113,8 +122,8 @@ VV_DEV void for_warp_work(const BInst* __restrict__ tab, const int* __restrict__
         pre = s_pre;
         ids = s_ids;
     }
-    const int nw = gridDim.x * 8, wtotal = 8 * total;
-    for (int w = blockIdx.x * 8 + (threadIdx.x >> 5); w < wtotal; w += nw) {
+    for (int e = blockIdx.x * 8 + (threadIdx.x >> 5); e < wtotal * split; e += nw) {
+        const int w = e / split, part = e - w * split;
         const int bw = w >> 3;
         int lo = 0, hi = nact - 1;   // the last p with pre[p] <= bw
         while (lo < hi) {
@@ -122,7 +131,7 @@ VV_DEV void for_warp_work(const BInst* __restrict__ tab, const int* __restrict__
             if (pre[mid] <= bw) lo = mid;
             else hi = mid - 1;
         }
-        body(tab[ids[lo]], w - 8 * pre[lo]);
+        body(tab[ids[lo]], w - 8 * pre[lo], part, split);
     }
 }
 
@@ -476,6 +485,44 @@ VV_DEV void vstore(float* p, const double (&o)[4]) {
 }
 VV_DEV void vstore(double* p, const double (&o)[2]) { *reinterpret_cast<double2*>(p) = make_double2(o[0], o[1]); }
 
+// deterministic sum of part[0..np) by one warp with eight loads in flight per
+// lane (lane l adds part[l + 32 j] into accumulator j mod 8; fixed tree after)
+VV_DEV double warp_reduce_parts8(const double* __restrict__ part, int np) {
+    const int lane = threadIdx.x & 31;
+    double a[8];
+#pragma unroll
+    for (int u = 0; u < 8; ++u) a[u] = 0.0;
+    int b = lane;
+    for (; b + 7 * 32 < np; b += 8 * 32)
+#pragma unroll
+        for (int u = 0; u < 8; ++u) a[u] += __ldcg(part + b + 32 * u);
+#pragma unroll
+    for (int u = 0; u < 8; ++u)
+        if (b + 32 * u < np) a[u] += __ldcg(part + b + 32 * u);
+    return warp_sum(((a[0] + a[1]) + (a[2] + a[3])) + ((a[4] + a[5]) + (a[6] + a[7])));
+}
+
+// deterministic sum of part[0..np) by the whole block: warp w sums the w-th
+// of blockDim/32 consecutive ranges, warp 0 the warp sums in order; every
+// thread returns the sum (block-uniform call)
+VV_DEV double block_reduce_parts(const double* __restrict__ part, int np) {
+    __shared__ double ws[32];
+    const int nwarp = blockDim.x >> 5, wid = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int per = (np + nwarp - 1) / nwarp;
+    const int lo = min(np, wid * per), hi = min(np, lo + per);
+    const double t = warp_reduce_parts8(part + lo, hi - lo);
+    if (lane == 0) ws[wid] = t;
+    __syncthreads();
+    if (wid == 0) {
+        const double r = warp_sum(lane < nwarp ? ws[lane] : 0.0);
+        if (lane == 0) ws[0] = r;
+    }
+    __syncthreads();
+    const double r = ws[0];
+    __syncthreads();   // ws read by every thread before a next call writes it
+    return r;
+}
+
 // cycle head: V0 = b (first cycle) or b - P^-1 J x (restart, P^-1 J x in V0)
 template <typename T>
 __global__ void k_b_gm_head(const BInst* __restrict__ tab, const int* __restrict__ L, int n) {
@@ -513,11 +560,11 @@ __global__ void __launch_bounds__(RED_THREADS) k_b_gm_cycle_p(const BInst* __res
     });
 }
 
-// cycle start: res, convergence test, scale, `active`
-__global__ void k_b_gm_cycle_f(const BInst* __restrict__ tab, const int* __restrict__ L, int n) {
+// cycle start: res, convergence test, scale, `active` (CTRL_THREADS per instance)
+__global__ void __launch_bounds__(CTRL_THREADS, 1) k_b_gm_cycle_f(const BInst* __restrict__ tab, const int* __restrict__ L,
+                                                              int n) {
     for_work<F_INST>(tab, L, n, [&](const BInst& I, int) {
-        if (threadIdx.x >= 32) return;
-        const double ss2 = warp_reduce_parts(I.wpart, wi_count(I));
+        const double ss2 = block_reduce_parts(I.wpart, wi_count(I));
         if (threadIdx.x == 0) gm_cycle_state(I.ds, ss2);
     });
 }
@@ -538,13 +585,15 @@ __global__ void __launch_bounds__(RED_THREADS, 3) k_b_gm_mdot_p(const BInst* __r
     static_assert(RED_THREADS == 256, "eight warp items per block item");
     constexpr int VN = vec_n<T>(), WV = WCELLS / (32 * VN), CK = gs_chunk<T>();
     using V16 = typename Vec16<T>::type;
-    for_warp_work<F_VEC>(tab, L, n, [&](const BInst& I, int wi) {
+    for_warp_work<F_VEC, true>(tab, L, n, [&](const BInst& I, int wi, int part, int split) {
         const int lane = threadIdx.x & 31, nwi = wi_count(I);
         const int it = I.ds->it, m = it + 1;
         const size_t nc = I.ncell;
         const T* V = (const T*)I.V;
         const T* w = V + (size_t)(it + 1) * nc;
-        for (int q0 = 0; q0 < m; q0 += CK) {
+        // chunks of CK columns, dealt round-robin to the item's `split` warps;
+        // every partial is one warp's fixed-order sum whatever the split
+        for (int q0 = part * CK; q0 < m; q0 += split * CK) {
             double acc[CK];
 #pragma unroll
             for (int c = 0; c < CK; ++c) acc[c] = 0.0;
@@ -588,15 +637,16 @@ __global__ void __launch_bounds__(RED_THREADS, 3) k_b_gm_mdot_p(const BInst* __r
     });
 }
 
-// hcol_q = vsc_q <w, V_q> = <w, v_q> from the partials (one warp per column).
+// hcol_q = vsc_q <w, V_q> = <w, v_q> from the partials (one warp per column,
+// CTRL_THREADS per instance: every column at once for restarts up to 31).
 // A separate kernel: a last-block reduction inside the multi-dot needs a
 // device-scope fence per work item, which waits for the item's stores.
-__global__ void __launch_bounds__(RED_THREADS) k_b_gm_mdot_f(const BInst* __restrict__ tab, const int* __restrict__ L, int n) {
+__global__ void __launch_bounds__(CTRL_THREADS, 1) k_b_gm_mdot_f(const BInst* __restrict__ tab, const int* __restrict__ L, int n) {
     for_work<F_INST>(tab, L, n, [&](const BInst& I, int) {
         DevState* s = I.ds;
         const int m = s->it + 1, nwi = wi_count(I);
-        for (int q = threadIdx.x >> 5; q < m; q += RED_THREADS / 32) {
-            const double t = warp_reduce_parts(I.wpart + (size_t)q * nwi, nwi);
+        for (int q = threadIdx.x >> 5; q < m; q += blockDim.x >> 5) {
+            const double t = warp_reduce_parts8(I.wpart + (size_t)q * nwi, nwi);
             if ((threadIdx.x & 31) == 0) s->hcol[q] = t * s->vsc[q];
         }
     });
@@ -604,8 +654,9 @@ __global__ void __launch_bounds__(RED_THREADS) k_b_gm_mdot_f(const BInst* __rest
 
 // w += sum_q (-hcol_q vsc_q) V_q and ||w||^2 per warp item
 template <typename T>
-__global__ void __launch_bounds__(RED_THREADS, 4) k_b_gm_maxpy_p(const BInst* __restrict__ tab, const int* __restrict__ L, int n) {
-    constexpr int VN = vec_n<T>(), WV = WCELLS / (32 * VN);
+__global__ void __launch_bounds__(RED_THREADS, 3) k_b_gm_maxpy_p(const BInst* __restrict__ tab, const int* __restrict__ L, int n) {
+    constexpr int VN = vec_n<T>(), WV = WCELLS / (32 * VN), CK = gs_chunk<T>();
+    using V16 = typename Vec16<T>::type;
     __shared__ double cf[MAX_RESTART + 2];
     for_work<F_VEC>(tab, L, n, [&](const BInst& I, int bid) {
         const DevState* s = I.ds;
@@ -624,7 +675,32 @@ __global__ void __launch_bounds__(RED_THREADS, 4) k_b_gm_maxpy_p(const BInst* __
                 const size_t i = base + (size_t)(lane + 32 * t) * VN;
                 if (i < nc) vload(w + i, wv[t]);
             }
-            for (int q = 0; q < m; ++q) {
+            // the loads of CK basis vectors issued together, the updates in
+            // the order q = 0, 1, .. (the same sums as one vector at a time)
+            int q = 0;
+            for (; q + CK <= m; q += CK) {
+                V16 vr[CK][WV];
+#pragma unroll
+                for (int c = 0; c < CK; ++c)
+#pragma unroll
+                    for (int t = 0; t < WV; ++t) {
+                        const size_t i = base + (size_t)(lane + 32 * t) * VN;
+                        if (i < nc) vload_raw(V + (size_t)(q + c) * nc + i, vr[c][t]);
+                        else vr[c][t] = V16{};
+                    }
+#pragma unroll
+                for (int c = 0; c < CK; ++c) {
+                    const double cc = cf[q + c];
+#pragma unroll
+                    for (int t = 0; t < WV; ++t) {
+                        double v[VN];
+                        vexpand(vr[c][t], v);
+#pragma unroll
+                        for (int e = 0; e < VN; ++e) wv[t][e] += cc * v[e];
+                    }
+                }
+            }
+            for (; q < m; ++q) {
                 const T* vq = V + (size_t)q * nc;
                 const double c = cf[q];
 #pragma unroll
@@ -691,7 +767,6 @@ __global__ void __launch_bounds__(RED_THREADS) k_b_gm_update(const BInst* __rest
 // the host-driven loop).  counts[op] counts the passes.
 enum BCtrl { BC_PIC = 0, BC_GM_START = 1, BC_INNER = 2, BC_GM_FINISH = 3, BC_REVERT = 4, BC_ALL = 5 };
 
-constexpr int CTRL_THREADS = 1024;
 
 // rebuild list `l` from the per-instance membership test `in(q)` over the
 // candidates src(0..cnt-1) (every instance, or the list's own members when
@@ -827,7 +902,7 @@ k_b_build_subset(const BInst* __restrict__ tab, int n, int* __restrict__ lists, 
 }
 
 // End of an Arnoldi step: ||w|| and the Arnoldi bookkeeping of every
-// instance of list L (one warp per instance; vsc of the new vector), then the
+// instance of list L (one block per instance; vsc of the new vector), then the
 // BC_INNER control step by the block that finishes last (`done`: a grid
 // counter, zero on entry and on exit).  The blocks only write instance
 // state before the counter, so the device-scope fence is short.
@@ -836,10 +911,8 @@ k_b_arnoldi_ctrl(const BInst* __restrict__ tab, const int* __restrict__ L, int n
                  int* __restrict__ flag, unsigned int* __restrict__ counts, int* __restrict__ lists,
                  unsigned int* __restrict__ done) {
     for_work<F_INST>(tab, L, n, [&](const BInst& I, int) {
-        if (threadIdx.x < 32) {
-            const double ss2 = warp_reduce_parts(I.wpart, wi_count(I));
-            if (threadIdx.x == 0) gm_arnoldi(I.ds, sqrt(ss2));
-        }
+        const double ss2 = block_reduce_parts(I.wpart, wi_count(I));
+        if (threadIdx.x == 0) gm_arnoldi(I.ds, sqrt(ss2));
     });
     if (!last_block(done, gridDim.x)) return;
     // the inner loop only drops instances: compact the current L_INNER in

@@ -54,6 +54,7 @@ def main(argv=None):
     ap.add_argument("--it", type=int, default=4, help="Arnoldi index of the sweep multi-dot/multi-axpy launches")
     ap.add_argument("--sweep-steps", type=int, default=0,
                     help="with --sweep: run this many batched time steps (after one warm-up step) instead")
+    ap.add_argument("--snes-atol", type=float, default=1e-10, help="with --sweep-steps: the Picard tolerance")
     args = ap.parse_args(argv)
     if args.sweep:
         return sweep_main(args)
@@ -104,7 +105,7 @@ def sweep_main(args):
     from .batch import Batch
     specs = W.sweep_specs(args.sweep)
     cells = sum(s["nx"] * s["nv"] for s in specs)
-    batch = Batch(W.sweep_runs(specs=specs, precision=args.precision))
+    batch = Batch(W.sweep_runs(specs=specs, precision=args.precision, snes_atol=args.snes_atol))
     if args.sweep_steps:
         batch.step()
         for k in range(args.sweep_steps):
