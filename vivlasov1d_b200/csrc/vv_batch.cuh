@@ -910,11 +910,25 @@ __global__ void __launch_bounds__(CTRL_THREADS)
 k_b_arnoldi_ctrl(const BInst* __restrict__ tab, const int* __restrict__ L, int n, unsigned long long handle,
                  int* __restrict__ flag, unsigned int* __restrict__ counts, int* __restrict__ lists,
                  unsigned int* __restrict__ done) {
+    __shared__ double s_h[MAX_RESTART + 2], s_c[MAX_RESTART + 1], s_s[MAX_RESTART + 1];
+    // the blocks that get an item take part in the grid counter (block 0
+    // always, for an empty list); read before any block arrives, so before
+    // the last one compacts the list in place
+    const int nb = max(1, min((int)gridDim.x, L[1 + F_INST]));
     for_work<F_INST>(tab, L, n, [&](const BInst& I, int) {
-        const double ss2 = block_reduce_parts(I.wpart, wi_count(I));
-        if (threadIdx.x == 0) gm_arnoldi(I.ds, sqrt(ss2));
+        DevState* s = I.ds;
+        const int it = s->it;
+        for (int j = threadIdx.x; j <= it; j += blockDim.x) {
+            s_h[j] = s->hcol[j];
+            if (j < it) {
+                s_c[j] = s->cc[j];
+                s_s[j] = s->ss[j];
+            }
+        }
+        const double ss2 = block_reduce_parts(I.wpart, wi_count(I));   // its barriers publish the copies
+        if (threadIdx.x == 0) gm_arnoldi(s, sqrt(ss2), s_h, s_c, s_s);
     });
-    if (!last_block(done, gridDim.x)) return;
+    if ((int)blockIdx.x >= nb || !last_block(done, nb)) return;
     // the inner loop only drops instances: compact the current L_INNER in
     // place instead of scanning the whole table (a tail pass with a few
     // instances left reads a few states, not n)

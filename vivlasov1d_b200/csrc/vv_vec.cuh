@@ -281,7 +281,10 @@ k_gm_mdot(DevState* s, const T* __restrict__ V, size_t ldv, size_t n, double* __
 }
 
 // Arnoldi bookkeeping after tt = ||w|| (KSPGMRESCycle + UpdateHessenberg)
-VV_DEV void gm_arnoldi(DevState* s, double tt) {
+// hcol, cc, ss: the state's arrays or copies of them (the lockstep batch
+// stages them in shared memory so that the rotation chain does not wait on
+// global loads ordered after its own stores)
+VV_DEV void gm_arnoldi(DevState* s, double tt, const double* hcol, const double* cc, const double* ss) {
     const int it = s->it;
     const int ld = s->restart + 2;
     double* hh = s->hh;
@@ -296,10 +299,10 @@ VV_DEV void gm_arnoldi(DevState* s, double tt) {
     // HH(j-1) <- c t + s HH(j), HH(j) <- c HH(j) - s t, t = HH(j-1)): the
     // value carried from row to row stays in a register and the loads of
     // hcol, cc and ss do not wait on the stores of earlier rows
-    double hj = s->hcol[0];
+    double hj = hcol[0];
     for (int j = 1; j <= it; ++j) {
-        const double hn = s->hcol[j];
-        const double c = s->cc[j - 1], sn = s->ss[j - 1];
+        const double hn = hcol[j];
+        const double c = cc[j - 1], sn = ss[j - 1];
         HH(j - 1, it) = c * hj + sn * hn;
         hj = c * hn - sn * hj;
     }
@@ -334,6 +337,7 @@ VV_DEV void gm_arnoldi(DevState* s, double tt) {
     s->active = (s->reason == R_ITERATING && s->it < s->restart && s->its < s->max_it) ? 1 : 0;
     set_cond(s->h_gm_inner, (unsigned)s->active);
 }
+VV_DEV void gm_arnoldi(DevState* s, double tt) { gm_arnoldi(s, tt, s->hcol, s->cc, s->ss); }
 
 // w += sum_q (-hcol_q) V_q and ||w||^2 (classical Gram-Schmidt update,
 // VecMAXPY with lhh = -<w,v>); the last CTA finishes the Arnoldi step.
