@@ -367,10 +367,11 @@ int vv_batch_launch_count(vv_batch* batch, int64_t* launches, int reset);
  * events.  which: 0 Gram-Schmidt multi-dot (w and V_0..V_it read), 1
  * preconditioner (its three kernels), 2 Jacobian-vector-product stencil,
  * 3 Gram-Schmidt multi-axpy (w updated), 4 the preconditioner's tridiagonal
- * stage alone (in place on the spectra the last application left).  it: the
- * Arnoldi index set in every
- * instance first (it + 1 <= each context's restart).  Between steps only:
- * the GMRES scratch of every instance is overwritten. */
+ * stage alone (in place on the spectra the last application left), 5 the
+ * GMRES operator P^-1 J as the step applies it (the stencil fused into the
+ * preconditioner's x-FFT when the batch runs fused).  it: the Arnoldi index
+ * set in every instance first (it + 1 <= each context's restart).  Between
+ * steps only: the GMRES scratch of every instance is overwritten. */
 int vv_batch_time_kernel(vv_batch* batch, int which, int it, int reps, double* avg_ms);
 
 /* ---- discrete adjoint of the converged step (no counterpart in the

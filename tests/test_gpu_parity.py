@@ -440,7 +440,8 @@ BATCH_SPECS = [(64, 128, vo.f0_landau(0.1, 0.5), 4 * np.pi, 0.1),
 
 
 @pytest.mark.parametrize("shape", [None, "2,1,0", "8,2,1", "4,0,1", "2,0,0,1", "2,1,0,1", "2,2,0,1", "2,3,0,1",
-                                   "2,4,0,1", "2,5,0,1", "2,6,0,1", "4,0,1,0,1"])
+                                   "2,4,0,1", "2,5,0,1", "2,6,0,1", "2,6,0,1,0,0", "2,2,0,1,1,0",
+                                   "4,0,1,0,1"])
 def test_batch_step_equals_single_steps(monkeypatch, shape):
     """A lockstep batch of uneven instances (every kernel launched once for
     the table, per-instance masks) follows each instance's own time step:
@@ -467,15 +468,16 @@ RAGGED_SPECS = [(64, 100, vo.f0_landau(0.1, 0.5), 4 * np.pi, 0.1),
                 (64, 330, vo.f0_bump_on_tail(0.04, 0.3), 2 * np.pi / 0.3, 0.1)]
 
 
-@pytest.mark.parametrize("tri", [0, 1, 2, 3, 4, 5, 6])
-def test_batch_ragged_lines_equal_single_steps(monkeypatch, tri):
+@pytest.mark.parametrize("shape", ["2,%d,0,1" % t for t in range(7)] + ["2,6,0,1,0,0"])
+def test_batch_ragged_lines_equal_single_steps(monkeypatch, shape):
     """Velocity grids that no chunk or warp split divides (nv 100, 72, 330):
-    every tridiagonal variant of the v-major preconditioner, batch against
-    each instance's own step."""
+    every tridiagonal variant of the v-major preconditioner (the Jacobian
+    stencil fused into its x-FFT, and once not), batch against each
+    instance's own step."""
     from vivlasov1d_b200.batch import Batch
     batch_runs = [_small_run(*s) for s in RAGGED_SPECS]
     single_runs = [_small_run(*s) for s in RAGGED_SPECS]
-    monkeypatch.setenv("VV_BATCH_SHAPE", "2,%d,0,1" % tri)
+    monkeypatch.setenv("VV_BATCH_SHAPE", shape)
     batch = Batch(batch_runs)
     for _ in range(2):
         rb = batch.step()
@@ -486,7 +488,7 @@ def test_batch_ragged_lines_equal_single_steps(monkeypatch, tri):
 
 
 @pytest.mark.parametrize("shape", ["4,0,0", "4,1,1", "2,0,0,1", "2,1,0,1", "2,3,0,1", "2,4,0,1", "2,5,0,1", "2,6,0,1",
-                                   "2,1,0,1,1"])
+                                   "2,6,0,1,0,0", "2,1,0,1,1"])
 def test_batch_graph_equals_host_driven(monkeypatch, shape):
     """The batch graph (conditional loops folded over the instance masks)
     and the host-driven loop over the same kernels (one fixed shape) give
@@ -525,6 +527,26 @@ def test_batch_marching_stencil_equals_tiles(monkeypatch):
             _assert_batch_matches(x, y, out[0][0][i], out[1][0][i], i, 1e-12)
 
 
+def test_batch_fused_stencil_equals_tiles(monkeypatch):
+    """The Jacobian stencil fused into the preconditioner's x-FFT evaluates
+    the 64 x 32 tiles' expression: two v-major batches of the same
+    instances (fused and not), two steps each, same Picard passes, GMRES
+    counts within one, f to 1e-12."""
+    from vivlasov1d_b200.batch import Batch
+    out = []
+    for fu in ("0", "1"):
+        monkeypatch.setenv("VV_BATCH_SHAPE", "2,6,0,1,0," + fu)
+        runs = [_small_run(*s) for s in BATCH_SPECS]
+        batch = Batch(runs)
+        reps = [batch.step(), batch.step()]
+        out.append(([r.fc.clone() for r in runs], reps))
+    for a, b in zip(out[0][0], out[1][0]):
+        assert (a - b).abs().max().item() <= 1e-12 * b.abs().max().item()
+    for ra, rb in zip(out[0][1], out[1][1]):
+        for i, (x, y) in enumerate(zip(ra, rb)):
+            _assert_batch_matches(x, y, out[0][0][i], out[1][0][i], i, 1e-12)
+
+
 def test_batch_sweep_instances_match_single_steps():
     """Twelve instances of the seeded sweep (Landau, two-stream and
     bump-on-tail; nx 64..256, nv 128..1024) in one batch, FP64, against
@@ -542,7 +564,7 @@ def test_batch_sweep_instances_match_single_steps():
 
 
 @pytest.mark.parametrize("shape", [None, "4,0,1,0", "2,0,0,1", "2,1,0,1", "2,2,0,1", "2,3,0,1", "2,4,0,1", "2,5,0,1",
-                                   "2,6,0,1", "2,1,0,1,1"])
+                                   "2,6,0,1", "2,6,0,1,0,0", "2,1,0,1,1"])
 def test_batch_mixed_precision_field_energy(monkeypatch, shape):
     """Batched mixed precision against FP64 single steps: field energy to
     1e-9 relative after three steps for every instance (autotuned, the

@@ -58,7 +58,8 @@ class Batch:
     def time_kernel(self, which, it=4, reps=20):
         """Seconds per whole-table launch of one batch kernel (0 multi-dot,
         1 preconditioner, 2 Jacobian stencil, 3 multi-axpy, 4 the
-        preconditioner's tridiagonal stage); between steps."""
+        preconditioner's tridiagonal stage, 5 the GMRES operator P^-1 J as
+        the step applies it); between steps."""
         ms = C.c_double()
         _lib.check(self.lib.vv_batch_time_kernel(self.h, int(which), int(it), int(reps), C.byref(ms)),
                    "vv_batch_time_kernel")

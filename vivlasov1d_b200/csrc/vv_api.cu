@@ -579,6 +579,11 @@ void smem_attributes(int optin, int& lowest, cudaError_t& e) {
     set((const void*)vv::k_b_tridiagjm<R, 2>);
     set((const void*)vv::k_b_tridiagjm<R, 4>);
     set((const void*)vv::k_b_tridiagjv<R>);
+#define VV_SETJ(S)                                                  \
+    set((const void*)vv::k_b_jvp_rfftj<S, vv::BS_X, R>);           \
+    set((const void*)vv::k_b_jvp_rfftj<S, vv::BS_VIT, R>);
+    VV_SETJ(1) VV_SETJ(2) VV_SETJ(4)
+#undef VV_SETJ
 }
 
 // dynamic shared memory of the staged warp-per-mode tridiagonal solve
@@ -2469,6 +2474,8 @@ struct vv_batch {
     bool pcj_ok;                 // every instance has M in 32..256 (the v-major kernels' lengths)
     void* dinvJ;                 // device: v-major LU reciprocals of every instance (GMRES precision)
     size_t smem_fftj;            // dynamic shared memory of the v-major FFT blocks
+    size_t smem_fjv;             // ... of the Jacobian stencil fused with the x-FFT (k_b_jvp_rfftj)
+    int fuse;                    // 1: the GMRES operator's stencil runs inside the preconditioner's x-FFT
     int tri_kind;                // tridiagonal solves: 0 CTA per mode (tables staged), 1 warp per mode,
                                  // 2 CTA per mode (tables through L1); v-major: 0 lane per mode, 1 warp
                                  // per mode, 2/3 two/four warps per mode, 4 lanes by line length, 5 lane
@@ -2608,6 +2615,23 @@ int b_jvp(vv_batch* b, const int* L) {
     return blaunch(b, vv::k_b_bracket<S, SRC, T>, vv::F_TILE, vv::WTHREADS, 0, (const vv::BInst*)b->tab, L, b->n);
 }
 
+// P^-1 J x (SRC BS_X, into V0) or P^-1 J v_it (BS_VIT, into V[it+1]) of the
+// instances of list l: the stencil fused into the x-FFT when the v-major
+// layout runs with `fuse`, else the stencil kernel then P^-1
+template <int S, int SRC, typename T>
+int b_jvp_pc(vv_batch* b, int l, int dst) {
+    const int* L = blist(b, l);
+    if (b->pcj && b->fuse) {
+        const vv::BInst* tab = b->tab;
+        const dim3 ft(vv::FJ_THREADS);
+        TRY(blaunch(b, vv::k_b_jvp_rfftj<S, SRC, T>, vv::F_ROWS, ft, b->smem_fjv, tab, L, b->n));
+        TRY(b_tri<T>(b, L));
+        return blaunch(b, vv::k_b_irfftj<T, T>, vv::F_ROWS, ft, b->smem_fftj, tab, L, b->n, dst);
+    }
+    TRY(b_jvp<S, SRC, T>(b, L));
+    return b_pc<T>(b, l, false, dst);
+}
+
 template <typename T>
 int b_jvp_all(vv_batch* b) {
     const int* L = blist(b, vv::L_ALL);
@@ -2645,8 +2669,7 @@ template <int S, typename T>
 int b_cycle_head(vv_batch* b) {
     const vv::BInst* tab = b->tab;
     const int* G = blist(b, vv::L_GM);
-    TRY(b_jvp<S, vv::BS_X, T>(b, blist(b, vv::L_GMR)));
-    TRY(b_pc<T>(b, vv::L_GMR, false, vv::BD_V0));
+    TRY(b_jvp_pc<S, vv::BS_X, T>(b, vv::L_GMR, vv::BD_V0));
     TRY(blaunch(b, vv::k_b_gm_head<T>, vv::F_VEC, vv::RED_THREADS, 0, tab, G, b->n));
     TRY(blaunch(b, vv::k_b_gm_cycle_p<T>, vv::F_VEC, vv::RED_THREADS, 0, tab, G, b->n));
     TRY(blaunch(b, vv::k_b_gm_cycle_f, vv::F_INST, vv::CTRL_THREADS, 0, tab, G, b->n));
@@ -2657,8 +2680,7 @@ template <int S, typename T>
 int b_arnoldi(vv_batch* b) {
     const vv::BInst* tab = b->tab;
     const int* A = blist(b, vv::L_INNER);
-    TRY(b_jvp<S, vv::BS_VIT, T>(b, A));
-    TRY(b_pc<T>(b, vv::L_INNER, false, vv::BD_VNEXT));
+    TRY(b_jvp_pc<S, vv::BS_VIT, T>(b, vv::L_INNER, vv::BD_VNEXT));
     TRY(blaunch(b, vv::k_b_gm_mdot_p<T>, vv::F_VEC, vv::RED_THREADS, 0, tab, A, b->n));
     TRY(blaunch(b, vv::k_b_gm_mdot_f, vv::F_INST, vv::CTRL_THREADS, 0, tab, A, b->n));
     TRY(blaunch(b, vv::k_b_gm_maxpy_p<T>, vv::F_VEC, vv::RED_THREADS, 0, tab, A, b->n));
@@ -2873,6 +2895,9 @@ bool b_tri_fits(const vv_batch* b, int tw, int pj) {
     return need <= (size_t)b->smem_limit;
 }
 
+// whether the fused stencil + x-FFT kernel fits the device's shared memory
+bool b_fuse_fits(const vv_batch* b) { return b->pcj_ok && b->smem_fjv <= (size_t)b->smem_limit; }
+
 // Batch autotuner: times the whole-table preconditioner (the step's largest
 // share) for FFT kind x FFT rows per CTA x tridiagonal variant and keeps the
 // fastest.
@@ -2948,27 +2973,40 @@ int b_autotune(vv_batch* b, std::vector<vv::BInst>& tab) {
         r = b_apply_shape(b, tab);
     }
     if (r == VV_OK) r = tail_list();
-    // Jacobian stencil: 64 x 32 tiles or marching strips, by the same weights
-    float sj[2] = {1e30f, 1e30f};
-    for (int m = 0; m <= 1 && r == VV_OK; ++m) {
-        b->march = m;
-        const int* LT = blist(b, vv::L_TAIL);
-        const float tf = timed([&]() { return b_jvp_all<T>(b); }, 5, r);
-        const float tt = timed([&]() {
-            switch (b->scheme) {
-                case VV_BRACKET_J1: return b_jvp<1, vv::BS_X, T>(b, LT);
-                case VV_BRACKET_J2: return b_jvp<2, vv::BS_X, T>(b, LT);
-                default: return b_jvp<4, vv::BS_X, T>(b, LT);
+    // Jacobian stencil: 64 x 32 tiles or marching strips before P^-1, or (v-major
+    // layout) the stencil fused into the x-FFT; timed as the whole GMRES
+    // operator P^-1 J on the table and on the tail, by the same weights
+    float bestj = 1e30f;
+    int bM = 0, bFu = 0;
+    auto op = [&](int l) -> int {
+        switch (b->scheme) {
+            case VV_BRACKET_J1: return b_jvp_pc<1, vv::BS_X, T>(b, l, vv::BD_B);
+            case VV_BRACKET_J2: return b_jvp_pc<2, vv::BS_X, T>(b, l, vv::BD_B);
+            default: return b_jvp_pc<4, vv::BS_X, T>(b, l, vv::BD_B);
+        }
+    };
+    for (int fu = 0; fu <= (b->pcj && b_fuse_fits(b) ? 1 : 0) && r == VV_OK; ++fu)
+        for (int m = 0; m <= (fu ? 0 : 1) && r == VV_OK; ++m) {
+            b->march = m;
+            b->fuse = fu;
+            const float tf = timed([&]() { return op(vv::L_ALL); }, 5, r);
+            const float tt = timed([&]() { return op(vv::L_TAIL); }, 5, r);
+            const float score = W_FULL * tf + W_TAIL * tt;
+            if (getenv("VV_DEBUG"))
+                fprintf(stderr, "[vv_batch] tune fuse=%d march=%d: full %.1f us, tail %.1f us\n", fu, m, tf * 1e3f,
+                        tt * 1e3f);
+            if (score < bestj) {
+                bestj = score;
+                bM = m;
+                bFu = fu;
             }
-        }, 5, r);
-        sj[m] = W_FULL * tf + W_TAIL * tt;
-        if (getenv("VV_DEBUG")) fprintf(stderr, "[vv_batch] tune march=%d: full %.1f us, tail %.1f us\n", m, tf * 1e3f, tt * 1e3f);
-    }
+        }
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
     cudaFree(dmember);
     TRY(r);
-    b->march = sj[1] < sj[0] ? 1 : 0;
+    b->march = bM;
+    b->fuse = bFu;
     return VV_OK;
 }
 
@@ -3113,7 +3151,10 @@ int vv_batch_create(int n, vv_ctx* const* ctxs, const vv_state* states, vv_batch
         for (int i = 0; i < n; ++i) {
             const int slots = vv::fj_slots_of(ctxs[i]->M);
             if (slots < 0) b->pcj_ok = false;
-            else b->smem_fftj = std::max(b->smem_fftj, (size_t)slots * csz);
+            else {
+                b->smem_fftj = std::max(b->smem_fftj, (size_t)slots * csz);
+                b->smem_fjv = std::max(b->smem_fjv, vv::fjv_smem_of(ctxs[i]->M, csz / 2));
+            }
             words += (size_t)ctxs[i]->nmodes * ctxs[i]->nv;
         }
         if (b->smem_fftj > (size_t)b->smem_limit) b->pcj_ok = false;
@@ -3168,16 +3209,18 @@ int vv_batch_create(int n, vv_ctx* const* ctxs, const vv_state* states, vv_batch
     b_shape(b, tab, 4, 0, 0);
     if ((r = b_apply_shape(b, tab)) != VV_OK) return fail_b(r);
     {
-        // VV_BATCH_SHAPE="R,tri,fft4[,vmajor[,march]]" fixes the shape (tests, profiling); else the autotuner picks it
+        // VV_BATCH_SHAPE="R,tri,fft4[,vmajor[,march[,fuse]]]" fixes the shape (tests, profiling; fuse
+        // defaults to 1 with the v-major layout); else the autotuner picks it
         const char* bs = getenv("VV_BATCH_SHAPE");
-        int fR = 0, fT = 0, fF = 0, fJ = 0, fM = 0;
-        const int nf = bs ? sscanf(bs, "%d,%d,%d,%d,%d", &fR, &fT, &fF, &fJ, &fM) : 0;
+        int fR = 0, fT = 0, fF = 0, fJ = 0, fM = 0, fU = 1;
+        const int nf = bs ? sscanf(bs, "%d,%d,%d,%d,%d,%d", &fR, &fT, &fF, &fJ, &fM, &fU) : 0;
         const bool fixed = nf >= 3 && (fR == 2 || fR == 4 || fR == 8) && fT >= 0 && fT <= (fJ ? 6 : 2) &&
                            (fF == 0 || fF == 1) && (fJ == 0 || (fJ == 1 && b->pcj_ok)) && b_tri_fits(b, fT, fJ);
         const char* at = getenv("VV_AUTOTUNE");
         if (fixed) {
             b->march = fM != 0;
             b_shape(b, tab, fR, fT, fF, fJ);
+            b->fuse = (fU != 0 && b->pcj && b_fuse_fits(b)) ? 1 : 0;
             if ((r = b_apply_shape(b, tab)) != VV_OK) return fail_b(r);
         } else if (!(at && at[0] == '0')) {
             r = b->mixed ? b_autotune<float>(b, tab) : b_autotune<double>(b, tab);
@@ -3270,7 +3313,7 @@ int vv_batch_step(vv_batch* b, const vv_snes_opts* so, const vv_ksp_opts* ko, vv
 }
 
 int vv_batch_time_kernel(vv_batch* b, int which, int it, int reps, double* avg_ms) {
-    if (!b || !avg_ms || reps < 1 || which < 0 || which > 4 || it < 0) return VV_ERR_ARG;
+    if (!b || !avg_ms || reps < 1 || which < 0 || which > 5 || it < 0) return VV_ERR_ARG;
     for (int i = 0; i < b->n; ++i)
         if (it + 1 >= b->ctx[i]->restart + 1) return VV_ERR_ARG;   // V[it+1] must exist
     const int64_t l0 = b->launches;
@@ -3287,6 +3330,17 @@ int vv_batch_time_kernel(vv_batch* b, int which, int it, int reps, double* avg_m
             case 1: return b->mixed ? b_pc<float>(b, vv::L_ALL, false, vv::BD_B) : b_pc<double>(b, vv::L_ALL, false, vv::BD_B);
             case 2: return b->mixed ? b_jvp_all<float>(b) : b_jvp_all<double>(b);   // the tuned stencil kernel
             case 4: return b->mixed ? b_tri<float>(b, L) : b_tri<double>(b, L);     // the tuned tridiagonal stage
+            case 5: {   // the GMRES operator P^-1 J as the step applies it (fused or not)
+                auto op = [&](auto tag) -> int {
+                    using TT = decltype(tag);
+                    switch (b->scheme) {
+                        case VV_BRACKET_J1: return b_jvp_pc<1, vv::BS_X, TT>(b, vv::L_ALL, vv::BD_B);
+                        case VV_BRACKET_J2: return b_jvp_pc<2, vv::BS_X, TT>(b, vv::L_ALL, vv::BD_B);
+                        default: return b_jvp_pc<4, vv::BS_X, TT>(b, vv::L_ALL, vv::BD_B);
+                    }
+                };
+                return b->mixed ? op(0.0f) : op(0.0);
+            }
             default:
                 return b->mixed ? blaunch(b, vv::k_b_gm_maxpy_p<float>, vv::F_VEC, vv::RED_THREADS, 0, tab, L, b->n)
                                 : blaunch(b, vv::k_b_gm_maxpy_p<double>, vv::F_VEC, vv::RED_THREADS, 0, tab, L, b->n);

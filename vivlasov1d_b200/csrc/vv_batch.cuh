@@ -57,6 +57,11 @@ struct BInst {
 __host__ __device__ constexpr size_t blist_words(int n) { return 1 + NFAM + (size_t)n + (size_t)NFAM * (n + 1); }
 
 // active instances whose list a block stages in shared memory for the search
+// 16-byte vector of T (the batch kernels' vector loads)
+template <typename T> struct Vec16;
+template <> struct Vec16<float> { using type = float4; static constexpr int n = 4; };
+template <> struct Vec16<double> { using type = double2; static constexpr int n = 2; };
+
 constexpr int BLIST_SMEM = 512;
 constexpr int CTRL_THREADS = 1024;   // control blocks and the per-instance finalize kernels
 
@@ -270,6 +275,194 @@ __global__ void __launch_bounds__(32) k_b_tridiagj(const BInst* __restrict__ tab
     });
 }
 
+// ---- Jacobian stencil fused with the x-FFT of the preconditioner -------------
+// The GMRES operator applies the Jacobian stencil and then P^-1, whose first
+// stage is the real FFT of every v row: one kernel computes the stencil of
+// its RB rows from a band of RB + 4 input rows staged in shared memory
+// (periodic halo of 2 in x) and transforms them in place of the row loads,
+// so the stencil's output never goes through HBM and one launch per Arnoldi
+// step is saved.  The stencil is the wide-tile kernel's expression (the
+// coefficient form of the J1/J2/J4 bracket with the point time derivative,
+// coefficients from the x and v profiles of h in FP64, cast to T).
+//
+// Shared memory past the FFT's twiddles and pass-1 buffer (it aliases the
+// pass-2 buffer, which is first written after the last band read):
+//   b values (nx + 4 doubles), h0 values (RB + 4 doubles), column
+//   coefficients (nx x 3 T), row coefficients (RB x 3 T), band
+//   ((RB + 4) x (nx + 8) T, row r at band[r * (nx + 8) + 4 + i]), and the
+//   stencil's output (RB rows of nx + 16 T: the first pass's 8-byte reads of
+//   two rows per half-warp fall on distinct banks), which the FFT reads.
+// The stencil runs one column per thread down the RB rows with a rolling
+// register window (6 shared loads per output, as the wide tiles).
+__host__ __device__ constexpr size_t fjv_align(size_t b) { return (b + 15) & ~(size_t)15; }
+__host__ __device__ constexpr size_t fjv_extra(int M, int rb, size_t tsz) {
+    return fjv_align((size_t)(2 * M + 4) * 8) + fjv_align((size_t)(rb + 4) * 8) + fjv_align((size_t)2 * M * 3 * tsz) +
+           fjv_align((size_t)rb * 3 * tsz) + fjv_align((size_t)(rb + 4) * (2 * M + 8) * tsz) +
+           (size_t)rb * (2 * M + 16) * tsz;
+}
+template <int M> __host__ __device__ constexpr size_t fjv_smem_t(size_t tsz) {
+    constexpr int P1 = FftJ<M>::P1, P2 = FftJ<M>::P2, RB = fj_rows(P2);
+    const size_t csz = 2 * tsz;
+    const size_t head = (size_t)(M + RB * fj_sa(P1, P2)) * csz;
+    const size_t b2 = (size_t)RB * fj_sb(M, P2) * csz;
+    const size_t ex = fjv_extra(M, RB, tsz);
+    return head + (b2 > ex ? b2 : ex);
+}
+inline size_t fjv_smem_of(int M, size_t tsz) {
+    switch (M) {
+        case 32: return fjv_smem_t<32>(tsz);
+        case 64: return fjv_smem_t<64>(tsz);
+        case 128: return fjv_smem_t<128>(tsz);
+        case 256: return fjv_smem_t<256>(tsz);
+        default: return 0;
+    }
+}
+
+template <int SCHEME, typename T, int M>
+VV_DEV void jvp_rfftj_block(const T* __restrict__ X, typename Cplx<T>::type* __restrict__ spec, const PcParams& pp,
+                            const BracketParams& bp, int item) {
+    using C = typename Cplx<T>::type;
+    constexpr int P1 = FftJ<M>::P1, P2 = FftJ<M>::P2, RB = fj_rows(P2);
+    constexpr int NX = 2 * M, BS = NX + 8, YS = NX + 16, VN = 16 / (int)sizeof(T);
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    C* stw = reinterpret_cast<C*>(smem_raw);
+    C* A = stw + M;
+    C* B = A + RB * fj_sa(P1, P2);
+    unsigned char* ex = reinterpret_cast<unsigned char*>(B);
+    double* bv = reinterpret_cast<double*>(ex);
+    ex += fjv_align((size_t)(NX + 4) * 8);
+    double* hv = reinterpret_cast<double*>(ex);
+    ex += fjv_align((size_t)(RB + 4) * 8);
+    T* scol = reinterpret_cast<T*>(ex);
+    ex += fjv_align((size_t)NX * 3 * sizeof(T));
+    T* srow = reinterpret_cast<T*>(ex);
+    ex += fjv_align((size_t)RB * 3 * sizeof(T));
+    T* band = reinterpret_cast<T*>(ex);
+    ex += fjv_align((size_t)(RB + 4) * BS * sizeof(T));
+    T* sy = reinterpret_cast<T*>(ex);
+    const int nv = pp.nv, j0 = item * RB;
+    const C* tw = reinterpret_cast<const C*>(pp.tw);
+    for (int k = threadIdx.x; k < M; k += FJ_THREADS) stw[k] = tw[k];
+    // band rows j0 - 2 .. j0 + RB + 1 (zeros outside the grid): 16-byte interior loads, then the halo
+    using V = typename Vec16<T>::type;
+    for (int q = threadIdx.x; q < (RB + 4) * (NX / VN); q += FJ_THREADS) {
+        const int rr = q / (NX / VN), v = q - rr * (NX / VN);
+        const int jj = j0 - 2 + rr;
+        V val{};
+        if (jj >= 0 && jj < nv) val = *reinterpret_cast<const V*>(X + (size_t)jj * NX + v * VN);
+        *reinterpret_cast<V*>(band + rr * BS + 4 + v * VN) = val;
+    }
+    for (int q = threadIdx.x; q < (RB + 4) * 4; q += FJ_THREADS) {
+        const int rr = q >> 2, h = q & 3;
+        const int jj = j0 - 2 + rr;
+        const int c = h < 2 ? 2 + h : NX + 2 + h;     // band columns of x = NX - 2, NX - 1, 0, 1
+        const int xi = h < 2 ? NX - 2 + h : h - 2;
+        band[rr * BS + c] = (jj >= 0 && jj < nv) ? X[(size_t)jj * NX + xi] : T(0);
+    }
+    for (int c = threadIdx.x; c < NX + 4; c += FJ_THREADS) {
+        int xi = c - 2;
+        if (xi < 0) xi += NX;
+        else if (xi >= NX) xi -= NX;
+        bv[c] = b_fac(bp, xi);
+    }
+    for (int rr = threadIdx.x; rr < RB + 4; rr += FJ_THREADS) {
+        const int jj = j0 - 2 + rr;
+        hv[rr] = (jj >= 0 && jj < nv) ? bp.h0[jj] : 0.0;
+    }
+    __syncthreads();
+    for (int i = threadIdx.x; i < NX; i += FJ_THREADS) {
+        const int l = i + 2;
+        double bm, bq;
+        Coef<SCHEME>::col(bv[l] - bv[l - 1], bv[l + 1] - bv[l], bv[l + 1] - bv[l - 1], bv[l] - bv[l - 2],
+                          bv[l + 2] - bv[l], bm, bq);
+        scol[3 * i] = T(bv[l + 1] - bv[l - 1]);
+        scol[3 * i + 1] = T(bm);
+        scol[3 * i + 2] = T(bq);
+    }
+    if (threadIdx.x < RB) {
+        const int l = threadIdx.x + 2;
+        double am, aq;
+        Coef<SCHEME>::row(hv[l] - hv[l - 1], hv[l + 1] - hv[l], hv[l + 1] - hv[l - 1], hv[l] - hv[l - 2],
+                          hv[l + 2] - hv[l], am, aq);
+        srow[3 * threadIdx.x] = T(hv[l + 1] - hv[l - 1]);
+        srow[3 * threadIdx.x + 1] = T(am);
+        srow[3 * threadIdx.x + 2] = T(aq);
+    }
+    __syncthreads();
+    const T tscale = T(((SCHEME == 2) ? bp.f2 : bp.f1) * bp.factor);
+    const T htinv = T(bp.ht_inv);
+    // the wide tile's expression, column i per thread, rows r = 0..RB-1 through
+    // a register window: column i rows r-2..r+2, columns i+-1 rows r-1..r+1
+    for (int i = threadIdx.x; i < NX; i += FJ_THREADS) {
+        const T* bc = band + 4 + i;    // row rr of the band at bc[rr * BS]
+        const T B1 = scol[3 * i], bm = scol[3 * i + 1], bq = scol[3 * i + 2];
+        T w0 = bc[0], w1 = bc[BS], w2 = bc[2 * BS], w3 = bc[3 * BS];
+        T m0 = bc[BS - 1], m1 = bc[2 * BS - 1], q0 = bc[BS + 1], q1 = bc[2 * BS + 1];
+#pragma unroll 4
+        for (int r = 0; r < RB; ++r) {
+            const T w4 = bc[(r + 4) * BS];
+            const T m2 = bc[(r + 3) * BS - 1], q2 = bc[(r + 3) * BS + 1];
+            const int j = j0 + r;
+            T y = htinv * w2;
+            if (j >= 2 && j < nv - 2) {
+                const T A1 = srow[3 * r], am = srow[3 * r + 1], ap = srow[3 * r + 2];
+                T s = T(0);
+                if (Coef<SCHEME>::cA1 != 0.0 || Coef<SCHEME>::cA2 != 0.0) {
+                    T ax = T(0), bx = T(0);
+                    if (Coef<SCHEME>::cA1 != 0.0) {
+                        ax = T(Coef<SCHEME>::cA1) * (q1 - m1);
+                        bx = T(Coef<SCHEME>::cB1) * (w3 - w1);
+                    }
+                    if (Coef<SCHEME>::cA2 != 0.0) {
+                        ax += T(Coef<SCHEME>::cA2) * (bc[(r + 2) * BS + 2] - bc[(r + 2) * BS - 2]);
+                        bx += T(Coef<SCHEME>::cB2) * (w4 - w0);
+                    }
+                    s = A1 * ax - B1 * bx;
+                }
+                s += am * (m0 - q0);
+                s += ap * (m2 - q2);
+                s += bm * (m0 - m2);
+                s += bq * (q0 - q2);
+                y += tscale * s;
+            }
+            sy[r * YS + i] = y;
+            w0 = w1; w1 = w2; w2 = w3; w3 = w4;
+            m0 = m1; m1 = m2; q0 = q1; q1 = q2;
+        }
+    }
+    __syncthreads();
+    using T2 = typename Pair<T>::type;
+    rfftj_rows<T, M>(spec, pp, item, stw, A, B, [&](int r, int, int nn) {
+        const T2 v = *reinterpret_cast<const T2*>(sy + r * YS + 2 * nn);
+        return c_make<C>(v.x, v.y);
+    });
+}
+
+// Jacobian stencil + x-FFT of every active instance's RB-row items:
+// BS_X: J x; BS_VIT: J v_it, v_it = vsc[it] V[it] (as k_b_bracket)
+template <int SCHEME, int SRC, typename T>
+__global__ void __launch_bounds__(FJ_THREADS) k_b_jvp_rfftj(const BInst* __restrict__ tab, const int* __restrict__ L,
+                                                            int n) {
+    for_work<F_ROWS>(tab, L, n, [&](const BInst& I, int local) {
+        BracketParams p = I.bp;
+        p.xidx = nullptr;
+        p.factor = 0.5;
+        if (SRC == BS_VIT) {
+            const double sc = I.ds->vsc[I.ds->it];
+            p.factor *= sc;
+            p.ht_inv *= sc;
+        }
+        const T* X = (SRC == BS_X) ? (const T*)I.xT : (const T*)I.V + (size_t)I.ds->it * I.ncell;
+        auto* spec = (typename Cplx<T>::type*)I.specT;
+        switch (I.pp.M) {
+            case 32: jvp_rfftj_block<SCHEME, T, 32>(X, spec, I.pp, p, local); break;
+            case 64: jvp_rfftj_block<SCHEME, T, 64>(X, spec, I.pp, p, local); break;
+            case 128: jvp_rfftj_block<SCHEME, T, 128>(X, spec, I.pp, p, local); break;
+            default: jvp_rfftj_block<SCHEME, T, 256>(X, spec, I.pp, p, local); break;
+        }
+    });
+}
+
 template <typename R, typename TO>
 __global__ void __launch_bounds__(FJ_THREADS) k_b_irfftj(const BInst* __restrict__ tab, const int* __restrict__ L, int n,
                                                          int dst) {
@@ -467,9 +660,6 @@ __global__ void k_b_revert(const BInst* __restrict__ tab, const int* __restrict_
 VV_DEV int wi_count(const BInst& I) { return 8 * I.vblk; }
 
 constexpr int WCELLS = 256;   // cells of a warp item
-template <typename T> struct Vec16;
-template <> struct Vec16<float> { using type = float4; static constexpr int n = 4; };
-template <> struct Vec16<double> { using type = double2; static constexpr int n = 2; };
 template <typename T> VV_DEV constexpr int vec_n() { return Vec16<T>::n; }
 // elements of a 16-byte vector as double
 VV_DEV void vload(const float* p, double (&o)[4]) {

@@ -126,33 +126,26 @@ template <typename T> struct Pair;
 template <> struct Pair<float> { using type = float2; };
 template <> struct Pair<double> { using type = double2; };
 
-// Real FFT along x of rows [item*RB, item*RB + RB) of X (nv x nx, nx = 2M),
-// half spectra written v-major: spec[j*(M+1) + k], k = 0..M.
-template <typename TI, typename R, int M>
-VV_DEV void rfftj_block(const TI* __restrict__ X, typename Cplx<R>::type* __restrict__ spec, const PcParams& p,
-                        int item) {
+// Real FFT along x of rows [item*RB, item*RB + RB), half spectra written
+// v-major: spec[j*(M+1) + k], k = 0..M.  load(r, j, n) returns the packed
+// complex sample z_n = x_{2n} + i x_{2n+1} of row j = item*RB + r (j < nv);
+// stw / A / B: the block's twiddle, pass-1 and pass-2 buffers, the twiddles
+// staged and a barrier taken by the caller.
+template <typename R, int M, typename Load>
+VV_DEV void rfftj_rows(typename Cplx<R>::type* __restrict__ spec, const PcParams& p, int item,
+                       const typename Cplx<R>::type* stw, typename Cplx<R>::type* A, typename Cplx<R>::type* B,
+                       Load load) {
     using C = typename Cplx<R>::type;
     constexpr int P1 = FftJ<M>::P1, P2 = FftJ<M>::P2, RB = fj_rows(P2);
     constexpr int SA = fj_sa(P1, P2), SB = fj_sb(M, P2), H = M / 2 + 1;
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    C* stw = reinterpret_cast<C*>(smem_raw);
-    C* A = stw + M;
-    C* B = A + RB * SA;
-    const C* tw = reinterpret_cast<const C*>(p.tw);
-    for (int k = threadIdx.x; k < M; k += FJ_THREADS) stw[k] = tw[k];
     const int j0 = item * RB;
-    __syncthreads();
     {   // pass 1: thread = (row r, m2); z_n = x_{2n} + i x_{2n+1}, n = P2 m1 + m2
         const int r = threadIdx.x / P2, m2 = threadIdx.x % P2;
         const int j = j0 + r;
         C a[P1];
         if (j < p.nv) {
-            const TI* row = X + (size_t)j * p.nx;
 #pragma unroll
-            for (int m1 = 0; m1 < P1; ++m1) {
-                const auto v = *reinterpret_cast<const typename Pair<TI>::type*>(row + 2 * (P2 * m1 + m2));
-                a[m1] = c_make<C>((double)v.x, (double)v.y);
-            }
+            for (int m1 = 0; m1 < P1; ++m1) a[m1] = load(r, j, P2 * m1 + m2);
         } else {
 #pragma unroll
             for (int m1 = 0; m1 < P1; ++m1) a[m1] = c_make<C>(0.0, 0.0);
@@ -201,6 +194,26 @@ VV_DEV void rfftj_block(const TI* __restrict__ X, typename Cplx<R>::type* __rest
             out[kc] = c_add(E1, c_mul(w, c_make<C>(0.5 * D.y, -0.5 * D.x)));
         }
     }
+}
+
+// Real FFT along x of rows [item*RB, item*RB + RB) of X (nv x nx, nx = 2M).
+template <typename TI, typename R, int M>
+VV_DEV void rfftj_block(const TI* __restrict__ X, typename Cplx<R>::type* __restrict__ spec, const PcParams& p,
+                        int item) {
+    using C = typename Cplx<R>::type;
+    constexpr int P1 = FftJ<M>::P1, P2 = FftJ<M>::P2, RB = fj_rows(P2);
+    constexpr int SA = fj_sa(P1, P2);
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    C* stw = reinterpret_cast<C*>(smem_raw);
+    C* A = stw + M;
+    C* B = A + RB * SA;
+    const C* tw = reinterpret_cast<const C*>(p.tw);
+    for (int k = threadIdx.x; k < M; k += FJ_THREADS) stw[k] = tw[k];
+    __syncthreads();
+    rfftj_rows<R, M>(spec, p, item, stw, A, B, [&](int, int j, int nn) {
+        const auto v = *reinterpret_cast<const typename Pair<TI>::type*>(X + (size_t)j * p.nx + 2 * nn);
+        return c_make<C>((double)v.x, (double)v.y);
+    });
 }
 
 // Inverse: half spectra spec[j*(M+1) + k] of rows [item*RB, item*RB + RB)

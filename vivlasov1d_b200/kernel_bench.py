@@ -124,8 +124,11 @@ def sweep_main(args):
     # tri: the tridiagonal stage reads the complex spectrum and LU reciprocals
     # and writes the solution, 3 complex words per mode and row
     mode_rows = sum((s["nx"] // 2 + 1) * s["nv"] for s in specs)
+    # op: the GMRES operator P^-1 J (x read, the half spectrum written and
+    # read back around the tridiagonal stage, the result written)
     kinds = {"mdot": (0, (args.it + 2) * word), "pc": (1, 6 * word), "jvp": (2, 2 * word),
-             "maxpy": (3, (args.it + 3) * word), "tri": (4, 6 * word * mode_rows / cells)}
+             "maxpy": (3, (args.it + 3) * word), "tri": (4, 6 * word * mode_rows / cells),
+             "op": (5, 4 * word + 6 * word * mode_rows / cells)}
     for name in args.kernels.split(","):
         if name not in kinds:
             continue
