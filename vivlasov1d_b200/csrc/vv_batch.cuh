@@ -285,28 +285,31 @@ __global__ void __launch_bounds__(32) k_b_tridiagj(const BInst* __restrict__ tab
 // coefficient form of the J1/J2/J4 bracket with the point time derivative,
 // coefficients from the x and v profiles of h in FP64, cast to T).
 //
-// Shared memory past the FFT's twiddles and pass-1 buffer (it aliases the
-// pass-2 buffer, which is first written after the last band read):
-//   b values (nx + 4 doubles), h0 values (RB + 4 doubles), column
-//   coefficients (nx x 3 T), row coefficients (RB x 3 T), band
-//   ((RB + 4) x (nx + 8) T, row r at band[r * (nx + 8) + 4 + i]), and the
-//   stencil's output (RB rows of nx + 16 T: the first pass's 8-byte reads of
-//   two rows per half-warp fall on distinct banks), which the FFT reads.
+// Shared memory: the FFT's twiddles, then two regions that the stencil and
+// the FFT use in turn (each region's next user starts after a barrier that
+// follows its last read):
+//   region 1, the pass-1 buffer A or: b values (nx + 4 doubles), h0 values
+//     (RB + 4 doubles), column coefficients (nx x 3 T), row coefficients
+//     (RB x 3 T) and the band ((RB + 4) x (nx + 8) T, row r at
+//     band[r * (nx + 8) + 4 + i]);
+//   region 2, the pass-2 buffer B or the stencil's output (RB rows of
+//     2 SB >= nx T: the row stride of B, which keeps the first pass's 8-byte
+//     reads of two rows per half-warp on distinct banks where SB is padded).
 // The stencil runs one column per thread down the RB rows with a rolling
 // register window (6 shared loads per output, as the wide tiles).
 __host__ __device__ constexpr size_t fjv_align(size_t b) { return (b + 15) & ~(size_t)15; }
-__host__ __device__ constexpr size_t fjv_extra(int M, int rb, size_t tsz) {
+__host__ __device__ constexpr size_t fjv_band(int M, int rb, size_t tsz) {
     return fjv_align((size_t)(2 * M + 4) * 8) + fjv_align((size_t)(rb + 4) * 8) + fjv_align((size_t)2 * M * 3 * tsz) +
-           fjv_align((size_t)rb * 3 * tsz) + fjv_align((size_t)(rb + 4) * (2 * M + 8) * tsz) +
-           (size_t)rb * (2 * M + 16) * tsz;
+           fjv_align((size_t)rb * 3 * tsz) + fjv_align((size_t)(rb + 4) * (2 * M + 8) * tsz);
+}
+template <int M> __host__ __device__ constexpr size_t fjv_region1(size_t tsz) {
+    constexpr int P1 = FftJ<M>::P1, P2 = FftJ<M>::P2, RB = fj_rows(P2);
+    const size_t a = fjv_align((size_t)RB * fj_sa(P1, P2) * 2 * tsz), band = fjv_band(M, RB, tsz);
+    return a > band ? a : band;
 }
 template <int M> __host__ __device__ constexpr size_t fjv_smem_t(size_t tsz) {
-    constexpr int P1 = FftJ<M>::P1, P2 = FftJ<M>::P2, RB = fj_rows(P2);
-    const size_t csz = 2 * tsz;
-    const size_t head = (size_t)(M + RB * fj_sa(P1, P2)) * csz;
-    const size_t b2 = (size_t)RB * fj_sb(M, P2) * csz;
-    const size_t ex = fjv_extra(M, RB, tsz);
-    return head + (b2 > ex ? b2 : ex);
+    constexpr int P2 = FftJ<M>::P2, RB = fj_rows(P2);
+    return fjv_align((size_t)M * 2 * tsz) + fjv_region1<M>(tsz) + (size_t)RB * fj_sb(M, P2) * 2 * tsz;
 }
 inline size_t fjv_smem_of(int M, size_t tsz) {
     switch (M) {
@@ -323,12 +326,15 @@ VV_DEV void jvp_rfftj_block(const T* __restrict__ X, typename Cplx<T>::type* __r
                             const BracketParams& bp, int item) {
     using C = typename Cplx<T>::type;
     constexpr int P1 = FftJ<M>::P1, P2 = FftJ<M>::P2, RB = fj_rows(P2);
-    constexpr int NX = 2 * M, BS = NX + 8, YS = NX + 16, VN = 16 / (int)sizeof(T);
+    constexpr int NX = 2 * M, BS = NX + 8, YS = 2 * fj_sb(M, P2), VN = 16 / (int)sizeof(T);
+    static_assert(YS >= NX, "a stencil output row fits a pass-2 row");
     extern __shared__ __align__(16) unsigned char smem_raw[];
     C* stw = reinterpret_cast<C*>(smem_raw);
-    C* A = stw + M;
-    C* B = A + RB * fj_sa(P1, P2);
-    unsigned char* ex = reinterpret_cast<unsigned char*>(B);
+    unsigned char* r1 = smem_raw + fjv_align((size_t)M * sizeof(C));
+    C* A = reinterpret_cast<C*>(r1);
+    C* B = reinterpret_cast<C*>(r1 + fjv_region1<M>(sizeof(T)));
+    T* sy = reinterpret_cast<T*>(B);
+    unsigned char* ex = r1;
     double* bv = reinterpret_cast<double*>(ex);
     ex += fjv_align((size_t)(NX + 4) * 8);
     double* hv = reinterpret_cast<double*>(ex);
@@ -338,8 +344,6 @@ VV_DEV void jvp_rfftj_block(const T* __restrict__ X, typename Cplx<T>::type* __r
     T* srow = reinterpret_cast<T*>(ex);
     ex += fjv_align((size_t)RB * 3 * sizeof(T));
     T* band = reinterpret_cast<T*>(ex);
-    ex += fjv_align((size_t)(RB + 4) * BS * sizeof(T));
-    T* sy = reinterpret_cast<T*>(ex);
     const int nv = pp.nv, j0 = item * RB;
     const C* tw = reinterpret_cast<const C*>(pp.tw);
     for (int k = threadIdx.x; k < M; k += FJ_THREADS) stw[k] = tw[k];
