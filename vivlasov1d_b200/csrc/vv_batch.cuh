@@ -445,7 +445,7 @@ VV_DEV void jvp_rfftj_block(const T* __restrict__ X, typename Cplx<T>::type* __r
 // Jacobian stencil + x-FFT of every active instance's RB-row items:
 // BS_X: J x; BS_VIT: J v_it, v_it = vsc[it] V[it] (as k_b_bracket)
 template <int SCHEME, int SRC, typename T>
-__global__ void __launch_bounds__(FJ_THREADS) k_b_jvp_rfftj(const BInst* __restrict__ tab, const int* __restrict__ L,
+__global__ void __launch_bounds__(FJ_THREADS, 5) k_b_jvp_rfftj(const BInst* __restrict__ tab, const int* __restrict__ L,
                                                             int n) {
     for_work<F_ROWS>(tab, L, n, [&](const BInst& I, int local) {
         BracketParams p = I.bp;
