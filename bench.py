@@ -243,6 +243,7 @@ def run_gpu(args, rank, world):
     pc_s = batch.time_kernel(1, it=MDOT_IT, reps=10)
     jvp_s = batch.time_kernel(2, it=MDOT_IT, reps=20)
     tri_s = batch.time_kernel(4, it=MDOT_IT, reps=10)
+    op_s = batch.time_kernel(5, it=MDOT_IT, reps=10)
     # ---- e2e: host buffers through the public API, the same K steps again ----
     hosts = [torch.empty_like(r.fc, device="cpu").pin_memory() for r in mixed]
     for h, snap, r in zip(hosts, snapshot, mixed):
@@ -267,7 +268,7 @@ def run_gpu(args, rank, world):
     return dict(cells=cells, total_cells=total_cells, t_value=t_value, t_plain=t_plain, t_e2e=t_e2e, t_b64=t_b64,
                 launches=launches, clocks=clocks, picard=picard, gmres=gmres, fe_rel=fe_rel, fe_rel_b64=fe_rel_b64,
                 fe_m=fe_m, fe_p=fe_p, fe_b=fe_b,
-                mdot_s=mdot_s, maxpy_s=maxpy_s, pc_s=pc_s, jvp_s=jvp_s, tri_s=tri_s, mode_rows=mode_rows,
+                mdot_s=mdot_s, maxpy_s=maxpy_s, pc_s=pc_s, jvp_s=jvp_s, tri_s=tri_s, op_s=op_s, mode_rows=mode_rows,
                 step_bytes=step_bytes, step_bytes64=step_bytes64, specs=specs)
 
 
@@ -458,7 +459,12 @@ def main():
                            "preconditioner_3_kernels_us": res["pc_s"] * 1e6,
                            "preconditioner_achieved_GBps": cells * 24 / res["pc_s"] / 1e9,
                            "jacobian_stencil_us": res["jvp_s"] * 1e6,
-                           "jacobian_achieved_GBps": cells * 8 / res["jvp_s"] / 1e9}}
+                           "jacobian_achieved_GBps": cells * 8 / res["jvp_s"] / 1e9,
+                           # P^-1 J as the step applies it (the stencil fused into the x-FFT when tuned so):
+                           # x read and the result written (4 B each per cell), the half spectrum
+                           # written and read around the tridiagonal stage (24 B per complex unknown)
+                           "gmres_operator_us": res["op_s"] * 1e6,
+                           "gmres_operator_achieved_GBps": (cells * 8 + res["mode_rows"] * 24) / res["op_s"] / 1e9}}
     fe = res["fe_rel"]
     cpu = None
     fe_err = {"steps": args.warmup + args.steps, "max": float(fe.max()), "median": float(np.median(fe)),
