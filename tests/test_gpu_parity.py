@@ -547,17 +547,19 @@ def test_batch_fused_stencil_equals_tiles(monkeypatch):
             _assert_batch_matches(x, y, out[0][0][i], out[1][0][i], i, 1e-12)
 
 
-def test_batch_sweep_instances_match_single_steps():
-    """Twelve instances of the seeded sweep (Landau, two-stream and
-    bump-on-tail; nx 64..256, nv 128..1024) in one batch, FP64, against
-    each instance stepped alone."""
+@pytest.mark.parametrize("count,steps", [(12, 2), (40, 1)])
+def test_batch_sweep_instances_match_single_steps(count, steps):
+    """Instances of the seeded sweep (Landau, two-stream and bump-on-tail;
+    nx 64..256, nv 128..1024) in one batch, FP64, against each instance
+    stepped alone; 40 instances: work lists longer than the entries a
+    block's list header brings in (and than a 32-thread block)."""
     from vivlasov1d_b200 import workloads as W
     from vivlasov1d_b200.batch import Batch
-    specs = W.sweep_specs(12)
+    specs = W.sweep_specs(count)
     br = W.sweep_runs(specs=specs)
     sr = W.sweep_runs(specs=specs)
     batch = Batch(br)
-    for _ in range(2):
+    for _ in range(steps):
         rb = batch.step()
         for i, r in enumerate(sr):
             _assert_batch_matches(rb[i], r.step(), br[i].fc, r.fc, i, 1e-9)

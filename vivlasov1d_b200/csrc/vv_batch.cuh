@@ -56,14 +56,51 @@ struct BInst {
 // layout of one work list: [nact][total per family][ids: n][prefix per family: n+1]
 __host__ __device__ constexpr size_t blist_words(int n) { return 1 + NFAM + (size_t)n + (size_t)NFAM * (n + 1); }
 
-// active instances whose list a block stages in shared memory for the search
 // 16-byte vector of T (the batch kernels' vector loads)
 template <typename T> struct Vec16;
 template <> struct Vec16<float> { using type = float4; static constexpr int n = 4; };
 template <> struct Vec16<double> { using type = double2; static constexpr int n = 2; };
 
+// active instances whose list a block stages in shared memory for the search
 constexpr int BLIST_SMEM = 512;
 constexpr int CTRL_THREADS = 1024;   // control blocks and the per-instance finalize kernels
+
+// The list header of family F: the number of instances and of work items,
+// and the first entries of the list's prefix and id arrays, loaded together
+// in one round trip (the arrays' addresses do not depend on the header; a
+// tail pass of a few instances needs nothing more).  Thread t holds pre[t]
+// for t < list_npre() and ids[t] for t < list_nids() (within the arrays).
+constexpr int LIST_SPEC = 32;
+VV_DEV int list_npre() { return min(LIST_SPEC + 1, (int)blockDim.x); }
+VV_DEV int list_nids() { return min(LIST_SPEC, (int)blockDim.x); }
+struct ListHead {
+    int nact, total, pre, id;
+};
+template <int F>
+VV_DEV ListHead list_head(const int* __restrict__ L, int n) {
+    const int* ids = L + 1 + NFAM;
+    const int* pre = ids + n + (size_t)F * (n + 1);
+    const int t = threadIdx.x;
+    ListHead h;
+    h.pre = (t < list_npre() && t <= n) ? pre[t] : 0;   // pre holds n + 1 entries
+    h.id = (t < list_nids() && t < n) ? ids[t] : 0;
+    h.nact = L[0];
+    h.total = L[1 + F];
+    return h;
+}
+// stage pre[0..nact] and ids[0..nact) in shared memory (nact <= BLIST_SMEM;
+// the caller takes a barrier before reading them): the entries the header
+// brought, then the rest
+template <int F>
+VV_DEV void list_stage(const int* __restrict__ L, int n, const ListHead& h, int* s_pre, int* s_ids) {
+    const int* ids = L + 1 + NFAM;
+    const int* pre = ids + n + (size_t)F * (n + 1);
+    const int t = threadIdx.x, np = list_npre(), ni = list_nids();
+    if (t < np && t <= h.nact) s_pre[t] = h.pre;
+    if (t < ni && t < h.nact) s_ids[t] = h.id;
+    for (int i = np + t; i <= h.nact; i += blockDim.x) s_pre[i] = pre[i];
+    for (int i = ni + t; i < h.nact; i += blockDim.x) s_ids[i] = ids[i];
+}
 
 // Loop of a persistent block over the work items of family F in list L:
 // body(instance, local block).  Block-uniform; a barrier separates items.
@@ -72,15 +109,15 @@ template <int F, typename Body>
 VV_DEV void for_work(const BInst* __restrict__ tab, const int* __restrict__ L, int n, Body body) {
     __shared__ int s_pre[BLIST_SMEM + 1];
     __shared__ int s_ids[BLIST_SMEM];
-    const int nact = L[0];
-    const int total = L[1 + F];
+    const ListHead h = list_head<F>(L, n);
+    const int nact = h.nact;
+    const int total = h.total;
     if ((int)blockIdx.x >= total) return;
     const int* ids = L + 1 + NFAM;
     const int* pre = ids + n + (size_t)F * (n + 1);
     const bool staged = nact <= BLIST_SMEM;
     if (staged) {
-        for (int i = threadIdx.x; i <= nact; i += blockDim.x) s_pre[i] = pre[i];
-        for (int i = threadIdx.x; i < nact; i += blockDim.x) s_ids[i] = ids[i];
+        list_stage<F>(L, n, h, s_pre, s_ids);
         __syncthreads();
         pre = s_pre;
         ids = s_ids;
@@ -110,8 +147,9 @@ template <int F, bool Split = false, typename Body>
 VV_DEV void for_warp_work(const BInst* __restrict__ tab, const int* __restrict__ L, int n, Body body) {
     __shared__ int s_pre[BLIST_SMEM + 1];
     __shared__ int s_ids[BLIST_SMEM];
-    const int nact = L[0];
-    const int total = L[1 + F];
+    const ListHead h = list_head<F>(L, n);
+    const int nact = h.nact;
+    const int total = h.total;
     const int nw = gridDim.x * 8, wtotal = 8 * total;
     // split factor: when the list holds fewer warp items than the grid has
     // warps (a few instances left), every item is taken by `split` warps,
@@ -121,8 +159,7 @@ VV_DEV void for_warp_work(const BInst* __restrict__ tab, const int* __restrict__
     const int* ids = L + 1 + NFAM;
     const int* pre = ids + n + (size_t)F * (n + 1);
     if (nact <= BLIST_SMEM) {
-        for (int i = threadIdx.x; i <= nact; i += blockDim.x) s_pre[i] = pre[i];
-        for (int i = threadIdx.x; i < nact; i += blockDim.x) s_ids[i] = ids[i];
+        list_stage<F>(L, n, h, s_pre, s_ids);
         __syncthreads();
         pre = s_pre;
         ids = s_ids;
