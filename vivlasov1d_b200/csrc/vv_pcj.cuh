@@ -229,9 +229,23 @@ VV_DEV void irfftj_block(const typename Cplx<R>::type* __restrict__ spec, TO* __
     C* stw = reinterpret_cast<C*>(smem_raw);
     C* A = stw + M;
     C* B = A + RB * SA;
+    static_assert(SA >= M + 1 && RB % 2 == 0, "a row's half spectrum fits a pass-1 row; items start on even rows");
     const C* tw = reinterpret_cast<const C*>(p.tw);
-    for (int k = threadIdx.x; k < M; k += FJ_THREADS) stw[k] = tw[k];
     const int j0 = item * RB;
+    {   // the item's half spectra are consecutive in the v-major layout: copy
+        // them into A (free until pass 1; SA >= M + 1) with 16-byte cp.async,
+        // every load in flight at once (j0 is even, so the source is 16-byte
+        // aligned; an odd count of FP32 complex values leaves 8 bytes)
+        const int rows = min(RB, p.nv - j0);
+        const char* src = reinterpret_cast<const char*>(spec + (size_t)j0 * (M + 1));
+        char* dst = reinterpret_cast<char*>(A);
+        const int nb = rows * (M + 1) * (int)sizeof(C), n16 = nb / 16;
+        for (int q = threadIdx.x; q < n16; q += FJ_THREADS) cp_async_16(dst + 16 * q, src + 16 * q, 16);
+        if (threadIdx.x == 0 && (nb & 15)) cp_async_8(dst + 16 * n16, src + 16 * n16, 8);
+        cp_async_commit();
+    }
+    for (int k = threadIdx.x; k < M; k += FJ_THREADS) stw[k] = tw[k];
+    cp_async_wait0();
     __syncthreads();
     // unpack: Z_k = E + i O, E = (X_k + conj X_{M-k})/2, O = W_N^-k (X_k - conj X_{M-k})/2
     for (int u = threadIdx.x; u < RB * H; u += FJ_THREADS) {
@@ -240,7 +254,7 @@ VV_DEV void irfftj_block(const typename Cplx<R>::type* __restrict__ spec, TO* __
         const int kc = M - k;
         C xk = c_make<C>(0.0, 0.0), xc = xk;
         if (j < p.nv) {
-            const C* in = spec + (size_t)j * (M + 1);
+            const C* in = A + r * (M + 1);
             xk = in[k];
             xc = in[kc];
         }
