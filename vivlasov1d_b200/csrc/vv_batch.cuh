@@ -384,15 +384,16 @@ VV_DEV void jvp_rfftj_block(const T* __restrict__ X, typename Cplx<T>::type* __r
     const int nv = pp.nv, j0 = item * RB;
     const C* tw = reinterpret_cast<const C*>(pp.tw);
     for (int k = threadIdx.x; k < M; k += FJ_THREADS) stw[k] = tw[k];
-    // band rows j0 - 2 .. j0 + RB + 1 (zeros outside the grid): 16-byte interior loads, then the halo
-    using V = typename Vec16<T>::type;
+    // band rows j0 - 2 .. j0 + RB + 1 (zeros outside the grid): the interior by
+    // 16-byte cp.async, every copy in flight at once (rows outside the grid
+    // copy 0 bytes from the base and zero-fill), then the halo
     for (int q = threadIdx.x; q < (RB + 4) * (NX / VN); q += FJ_THREADS) {
         const int rr = q / (NX / VN), v = q - rr * (NX / VN);
         const int jj = j0 - 2 + rr;
-        V val{};
-        if (jj >= 0 && jj < nv) val = *reinterpret_cast<const V*>(X + (size_t)jj * NX + v * VN);
-        *reinterpret_cast<V*>(band + rr * BS + 4 + v * VN) = val;
+        const bool in = jj >= 0 && jj < nv;
+        cp_async_16(band + rr * BS + 4 + v * VN, in ? X + (size_t)jj * NX + v * VN : X, in ? 16 : 0);
     }
+    cp_async_commit();
     for (int q = threadIdx.x; q < (RB + 4) * 4; q += FJ_THREADS) {
         const int rr = q >> 2, h = q & 3;
         const int jj = j0 - 2 + rr;
@@ -410,6 +411,7 @@ VV_DEV void jvp_rfftj_block(const T* __restrict__ X, typename Cplx<T>::type* __r
         const int jj = j0 - 2 + rr;
         hv[rr] = (jj >= 0 && jj < nv) ? bp.h0[jj] : 0.0;
     }
+    cp_async_wait0();
     __syncthreads();
     for (int i = threadIdx.x; i < NX; i += FJ_THREADS) {
         const int l = i + 2;
