@@ -975,7 +975,7 @@ __global__ void k_b_gm_solve(const BInst* __restrict__ tab, const int* __restric
 }
 
 template <typename T>
-__global__ void __launch_bounds__(RED_THREADS) k_b_gm_update(const BInst* __restrict__ tab, const int* __restrict__ L, int n) {
+__global__ void __launch_bounds__(RED_THREADS, 3) k_b_gm_update(const BInst* __restrict__ tab, const int* __restrict__ L, int n) {
     __shared__ double nrs[MAX_RESTART + 1];
     for_work<F_VEC>(tab, L, n, [&](const BInst& I, int bid) {
         const DevState* s = I.ds;
@@ -985,10 +985,60 @@ __global__ void __launch_bounds__(RED_THREADS) k_b_gm_update(const BInst* __rest
         if (m <= 0) return;
         const T* V = (const T*)I.V;
         T* x = (T*)I.xT;
-        for (size_t i = bid * (size_t)RED_THREADS + threadIdx.x; i < I.ncell; i += (size_t)I.vblk * RED_THREADS) {
-            double xi = (double)x[i];
-            for (int q = 0; q < m; ++q) xi += nrs[q] * (double)V[(size_t)q * I.ncell + i];
-            x[i] = (T)xi;
+        // warp items of WCELLS cells with 16-byte loads; the loads of CK basis
+        // vectors issued together, the sums in the order q = 0, 1, ..
+        constexpr int VN = vec_n<T>(), WV = WCELLS / (32 * VN), CK = gs_chunk<T>();
+        using V16 = typename Vec16<T>::type;
+        const int lane = threadIdx.x & 31, nwi = wi_count(I), wi = bid * 8 + (threadIdx.x >> 5);
+        const size_t nc = I.ncell;
+        for (size_t base = (size_t)wi * WCELLS; base < nc; base += (size_t)nwi * WCELLS) {
+            double xv[WV][VN];
+#pragma unroll
+            for (int t = 0; t < WV; ++t) {
+                const size_t i = base + (size_t)(lane + 32 * t) * VN;
+                if (i < nc) vload(x + i, xv[t]);
+            }
+            int q = 0;
+            for (; q + CK <= m; q += CK) {
+                V16 vr[CK][WV];
+#pragma unroll
+                for (int c = 0; c < CK; ++c)
+#pragma unroll
+                    for (int t = 0; t < WV; ++t) {
+                        const size_t i = base + (size_t)(lane + 32 * t) * VN;
+                        if (i < nc) vload_raw(V + (size_t)(q + c) * nc + i, vr[c][t]);
+                        else vr[c][t] = V16{};
+                    }
+#pragma unroll
+                for (int c = 0; c < CK; ++c) {
+                    const double cc = nrs[q + c];
+#pragma unroll
+                    for (int t = 0; t < WV; ++t) {
+                        double v[VN];
+                        vexpand(vr[c][t], v);
+#pragma unroll
+                        for (int e = 0; e < VN; ++e) xv[t][e] += cc * v[e];
+                    }
+                }
+            }
+            for (; q < m; ++q) {
+                const double cc = nrs[q];
+#pragma unroll
+                for (int t = 0; t < WV; ++t) {
+                    const size_t i = base + (size_t)(lane + 32 * t) * VN;
+                    if (i < nc) {
+                        double v[VN];
+                        vload(V + (size_t)q * nc + i, v);
+#pragma unroll
+                        for (int e = 0; e < VN; ++e) xv[t][e] += cc * v[e];
+                    }
+                }
+            }
+#pragma unroll
+            for (int t = 0; t < WV; ++t) {
+                const size_t i = base + (size_t)(lane + 32 * t) * VN;
+                if (i < nc) vstore(x + i, xv[t]);
+            }
         }
     });
 }
