@@ -579,6 +579,7 @@ void smem_attributes(int optin, int& lowest, cudaError_t& e) {
     set((const void*)vv::k_b_tridiagjm<R, 2>);
     set((const void*)vv::k_b_tridiagjm<R, 4>);
     set((const void*)vv::k_b_tridiagjv<R>);
+    set((const void*)vv::k_b_gm_mdot_p<R>);
 #define VV_SETJ(S)                                                  \
     set((const void*)vv::k_b_jvp_rfftj<S, vv::BS_X, R>);           \
     set((const void*)vv::k_b_jvp_rfftj<S, vv::BS_VIT, R>);
@@ -2681,7 +2682,7 @@ int b_arnoldi(vv_batch* b) {
     const vv::BInst* tab = b->tab;
     const int* A = blist(b, vv::L_INNER);
     TRY(b_jvp_pc<S, vv::BS_VIT, T>(b, vv::L_INNER, vv::BD_VNEXT));
-    TRY(blaunch(b, vv::k_b_gm_mdot_p<T>, vv::F_VEC, vv::RED_THREADS, 0, tab, A, b->n));
+    TRY(blaunch(b, vv::k_b_gm_mdot_p<T>, vv::F_VEC, vv::RED_THREADS, vv::mdot_smem<T>(), tab, A, b->n));
     TRY(blaunch(b, vv::k_b_gm_mdot_f, vv::F_INST, vv::CTRL_THREADS, 0, tab, A, b->n));
     TRY(blaunch(b, vv::k_b_gm_maxpy_p<T>, vv::F_VEC, vv::RED_THREADS, 0, tab, A, b->n));
     // ||w||, Arnoldi bookkeeping and the BC_INNER control step in one launch
@@ -3325,8 +3326,10 @@ int vv_batch_time_kernel(vv_batch* b, int which, int it, int reps, double* avg_m
     auto one = [&]() -> int {
         switch (which) {
             case 0:
-                return b->mixed ? blaunch(b, vv::k_b_gm_mdot_p<float>, vv::F_VEC, vv::RED_THREADS, 0, tab, L, b->n)
-                                : blaunch(b, vv::k_b_gm_mdot_p<double>, vv::F_VEC, vv::RED_THREADS, 0, tab, L, b->n);
+                return b->mixed ? blaunch(b, vv::k_b_gm_mdot_p<float>, vv::F_VEC, vv::RED_THREADS,
+                                          vv::mdot_smem<float>(), tab, L, b->n)
+                                : blaunch(b, vv::k_b_gm_mdot_p<double>, vv::F_VEC, vv::RED_THREADS,
+                                          vv::mdot_smem<double>(), tab, L, b->n);
             case 1: return b->mixed ? b_pc<float>(b, vv::L_ALL, false, vv::BD_B) : b_pc<double>(b, vv::L_ALL, false, vv::BD_B);
             case 2: return b->mixed ? b_jvp_all<float>(b) : b_jvp_all<double>(b);   // the tuned stencil kernel
             case 4: return b->mixed ? b_tri<float>(b, L) : b_tri<double>(b, L);     // the tuned tridiagonal stage

@@ -813,17 +813,83 @@ VV_DEV void vload_raw(const T* p, typename Vec16<T>::type& o) { o = *reinterpret
 VV_DEV void vexpand(const float4& v, double (&o)[4]) { o[0] = v.x; o[1] = v.y; o[2] = v.z; o[3] = v.w; }
 VV_DEV void vexpand(const double2& v, double (&o)[2]) { o[0] = v.x; o[1] = v.y; }
 
+// dynamic shared memory of the multi-dot: two stages of a thread's CK basis
+// chunks (16-byte pieces, thread-interleaved)
+template <typename T> __host__ __device__ constexpr size_t mdot_smem() {
+    return (size_t)2 * gs_chunk<T>() * (WCELLS / (32 * (16 / sizeof(T)))) * 16 * RED_THREADS;
+}
+
 template <typename T>
 __global__ void __launch_bounds__(RED_THREADS, 3) k_b_gm_mdot_p(const BInst* __restrict__ tab, const int* __restrict__ L, int n) {
     static_assert(RED_THREADS == 256, "eight warp items per block item");
     constexpr int VN = vec_n<T>(), WV = WCELLS / (32 * VN), CK = gs_chunk<T>();
     using V16 = typename Vec16<T>::type;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    V16* sbuf = reinterpret_cast<V16*>(smem_raw);   // piece (stage, c, t) of this thread at [((stage CK + c) WV + t) RED_THREADS + tid]
     for_warp_work<F_VEC, true>(tab, L, n, [&](const BInst& I, int wi, int part, int split) {
         const int lane = threadIdx.x & 31, nwi = wi_count(I);
         const int it = I.ds->it, m = it + 1;
         const size_t nc = I.ncell;
         const T* V = (const T*)I.V;
         const T* w = V + (size_t)(it + 1) * nc;
+        if ((size_t)nwi * WCELLS >= nc) {
+            // one cell range per item: w in registers, the item's basis chunks
+            // streamed through two shared-memory stages by cp.async (a chunk's
+            // copies in flight while the previous one is summed); each thread
+            // reads back only its own pieces
+            const size_t base = (size_t)wi * WCELLS;
+            V16 wr[WV];
+#pragma unroll
+            for (int t = 0; t < WV; ++t) {
+                const size_t i = base + (size_t)(lane + 32 * t) * VN;
+                if (i < nc) vload_raw(w + i, wr[t]);
+                else wr[t] = V16{};
+            }
+            auto issue = [&](int q0, int stage) {
+#pragma unroll
+                for (int c = 0; c < CK; ++c)
+#pragma unroll
+                    for (int t = 0; t < WV; ++t) {
+                        const size_t i = base + (size_t)(lane + 32 * t) * VN;
+                        const bool in = q0 + c < m && i < nc;
+                        cp_async_16(&sbuf[((stage * CK + c) * WV + t) * RED_THREADS + threadIdx.x],
+                                    in ? (const void*)(V + (size_t)(q0 + c) * nc + i) : (const void*)V, in ? 16 : 0);
+                    }
+                cp_async_commit();
+            };
+            const int step = split * CK;
+            int q0 = part * CK;
+            if (q0 < m) issue(q0, 0);
+            if (q0 + step < m) issue(q0 + step, 1);
+            for (int k = 0; q0 < m; q0 += step, ++k) {
+                if (q0 + step < m) cp_async_wait1();   // the next chunk's group may still be in flight
+                else cp_async_wait0();
+                const int stage = k & 1;
+                double acc[CK];
+#pragma unroll
+                for (int c = 0; c < CK; ++c) {
+                    acc[c] = 0.0;
+#pragma unroll
+                    for (int t = 0; t < WV; ++t) {
+                        double wv[VN], v[VN];
+                        vexpand(wr[t], wv);
+                        vexpand(sbuf[((stage * CK + c) * WV + t) * RED_THREADS + threadIdx.x], v);
+#pragma unroll
+                        for (int e = 0; e < VN; ++e) acc[c] += wv[e] * v[e];
+                    }
+                }
+                if (q0 + 2 * step < m) issue(q0 + 2 * step, stage);   // after this stage's reads
+                const int cnt = min(CK, m - q0);
+#pragma unroll
+                for (int c = 0; c < CK; ++c) {
+                    if (c < cnt) {
+                        const double t = warp_sum(acc[c]);
+                        if (lane == 0) I.wpart[(size_t)(q0 + c) * nwi + wi] = t;
+                    }
+                }
+            }
+            return;
+        }
         // chunks of CK columns, dealt round-robin to the item's `split` warps;
         // every partial is one warp's fixed-order sum whatever the split
         for (int q0 = part * CK; q0 < m; q0 += split * CK) {

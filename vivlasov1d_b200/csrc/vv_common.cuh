@@ -116,4 +116,5 @@ VV_DEV void cp_async_elem(E* smem, const E* gmem) {
 // the waits clobber memory so that no shared-memory read moves above them
 VV_DEV void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
 VV_DEV void cp_async_wait2() { asm volatile("cp.async.wait_group 2;\n" ::: "memory"); }
+VV_DEV void cp_async_wait1() { asm volatile("cp.async.wait_group 1;\n" ::: "memory"); }
 VV_DEV void cp_async_wait0() { asm volatile("cp.async.wait_group 0;\n" ::: "memory"); }
