@@ -357,9 +357,21 @@ int vv_batch_create(int n, vv_ctx* const* ctxs, const vv_state* states, vv_batch
 int vv_batch_destroy(vv_batch* batch);
 int vv_batch_set_stream(vv_batch* batch, void* cuda_stream);
 /* reports and statuses: arrays of n (statuses may be NULL); returns the
- * first non-OK instance status, VV_OK if all instances stepped. */
+ * first non-OK instance status, VV_OK if all instances stepped.  Equals
+ * vv_batch_launch followed by vv_batch_collect. */
 int vv_batch_step(vv_batch* batch, const vv_snes_opts* snes, const vv_ksp_opts* ksp,
                   vv_step_report* reports, int* statuses);
+/* The step in two halves, so that a caller can run several batches at once
+ * on their own streams (a batch of the slowest instances beside one of the
+ * rest: their lockstep loops then overlap instead of the slow instances
+ * running alone at the end of every pass).  vv_batch_launch enqueues the
+ * step and the read-back of the instance states on the batch's stream and
+ * returns without waiting; vv_batch_collect waits for that stream and fills
+ * the reports (the same arguments as vv_batch_step; snes and ksp as given
+ * to the launch).  A launch must be collected before the next launch. */
+int vv_batch_launch(vv_batch* batch, const vv_snes_opts* snes, const vv_ksp_opts* ksp);
+int vv_batch_collect(vv_batch* batch, const vv_snes_opts* snes, const vv_ksp_opts* ksp,
+                     vv_step_report* reports, int* statuses);
 /* Number of kernels the batch has launched (graph nodes executed included). */
 int vv_batch_launch_count(vv_batch* batch, int64_t* launches, int reset);
 /* Device time of one whole-table launch of a batch kernel with every instance

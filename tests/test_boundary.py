@@ -33,6 +33,16 @@ def test_library_exports_every_declared_symbol():
     assert _lib.status_string(0) == "ok"
 
 
+def test_batch_launch_and_collect_reject_null_handles_without_gpu():
+    """The two halves of a batch step check their arguments before any device call."""
+    from vivlasov1d_b200 import _lib
+    lib = _lib.load()
+    so, ko = _lib.vv_snes_opts(), _lib.vv_ksp_opts()
+    reps = (_lib.vv_step_report * 1)()
+    assert lib.vv_batch_launch(None, C.byref(so), C.byref(ko)) == 1          # VV_ERR_ARG
+    assert lib.vv_batch_collect(None, C.byref(so), C.byref(ko), reps, None) == 1
+
+
 def test_create_rejects_bad_grid_without_gpu():
     """Argument checks happen before any device call."""
     from vivlasov1d_b200 import _lib

@@ -547,6 +547,45 @@ def test_batch_fused_stencil_equals_tiles(monkeypatch):
             _assert_batch_matches(x, y, out[0][0][i], out[1][0][i], i, 1e-12)
 
 
+def test_batch_split_tables_follow_one_table():
+    """Two lockstep tables stepped at once on two streams (an explicit split,
+    and "auto": the first step whole, then the slowest eighth beside the
+    rest) follow the one-table batch of the same 24 sweep instances: same
+    Picard passes, GMRES counts within one, f to 1e-10 (FP64)."""
+    from vivlasov1d_b200 import workloads as W
+    from vivlasov1d_b200.batch import Batch
+    specs = W.sweep_specs(24)
+    one, two, auto = (W.sweep_runs(specs=specs) for _ in range(3))
+    b1 = Batch(one)
+    b2 = Batch(two, split=[list(range(0, 24, 3)), [i for i in range(24) if i % 3]])
+    b3 = Batch(auto, split="auto")
+    for _ in range(3):
+        r1, r2, r3 = b1.step(), b2.step(), b3.step()
+        for i in range(24):
+            _assert_batch_matches(r2[i], r1[i], two[i].fc, one[i].fc, i, 1e-10)
+            _assert_batch_matches(r3[i], r1[i], auto[i].fc, one[i].fc, i, 1e-10)
+    assert [len(g) for g in b3.groups] == [21, 3]
+    assert b3.launch_count() > 0
+
+
+def test_batch_launch_collect_order(monkeypatch):
+    """vv_batch_collect without a launch, and a second launch before the
+    collect, are refused (VV_ERR_ARG) and leave the batch usable."""
+    import ctypes as C
+    from vivlasov1d_b200 import _lib
+    from vivlasov1d_b200.batch import Batch
+    runs = [_small_run(*s) for s in BATCH_SPECS]
+    batch = Batch(runs)
+    t = batch._tables[0]
+    reps = (_lib.vv_step_report * len(runs))()
+    assert t.lib.vv_batch_collect(t.h, C.byref(t.snes), C.byref(t.ksp), reps, None) == _lib.VV_ERR_ARG
+    t.launch(torch.cuda.current_stream())
+    assert t.lib.vv_batch_launch(t.h, C.byref(t.snes), C.byref(t.ksp)) == _lib.VV_ERR_ARG
+    st, rep = t.collect()
+    assert st == _lib.VV_OK and all(r["status"] == 0 for r in rep)
+    assert all(r["status"] == 0 for r in batch.step())
+
+
 @pytest.mark.parametrize("count,steps", [(12, 2), (40, 1)])
 def test_batch_sweep_instances_match_single_steps(count, steps):
     """Instances of the seeded sweep (Landau, two-stream and bump-on-tail;

@@ -171,6 +171,9 @@ SIGNATURES = {
     "vv_batch_set_stream": (I, [P, P]),
     "vv_batch_step": (I, [P, C.POINTER(vv_snes_opts), C.POINTER(vv_ksp_opts), C.POINTER(vv_step_report),
                           C.POINTER(C.c_int)]),
+    "vv_batch_launch": (I, [P, C.POINTER(vv_snes_opts), C.POINTER(vv_ksp_opts)]),
+    "vv_batch_collect": (I, [P, C.POINTER(vv_snes_opts), C.POINTER(vv_ksp_opts), C.POINTER(vv_step_report),
+                             C.POINTER(C.c_int)]),
     "vv_batch_launch_count": (I, [P, C.POINTER(C.c_int64), I]),
     "vv_batch_time_kernel": (I, [P, I, I, I, C.POINTER(D)]),
 }

@@ -4,10 +4,23 @@ The reference runs one instance per process (a parameter sweep is many
 ``run.py`` invocations).  ``Batch`` takes several ``Run`` objects -- any mix
 of grid sizes, initial conditions and parameters, each with its own libvv
 context -- and advances all of them by one implicit time step per
-``step()`` call (``vv_batch_step``): one CUDA graph in which every kernel
-serves the whole instance table.  Each instance keeps its own Picard and
+``step()`` call: one CUDA graph in which every kernel serves the whole
+instance table (``vv_batch_step``).  Each instance keeps its own Picard and
 GMRES state and convergence tests; converged instances are masked out of
 later passes while the others continue.
+
+A lockstep pass lasts as long as its slowest instance: in a sweep a few
+instances need ten times the median's GMRES iterations, and they run with
+few others at the end of every pass.  ``split="auto"`` steps the first call
+as one table and then, for tables of at least ``SPLIT_MIN`` instances,
+re-forms it as two tables -- the eighth of the instances that needed the
+most GMRES iterations, and the rest -- which every later step launches at
+once on two streams (``vv_batch_launch``) and collects together
+(``vv_batch_collect``), so that the two tables' passes interleave.  On the
+256-instance sweep this saves 2-3% of a step: the slow table's instances
+are the largest, and both tables' kernels need the whole GPU.  Each
+instance computes the same operations in either form (the tables' tuned
+kernel shapes may differ, so results agree to rounding).
 """
 from __future__ import annotations
 
@@ -18,30 +31,30 @@ import torch
 from . import _lib
 from .run import report_dict
 
+SPLIT_MIN = 16        # smallest table that "auto" splits
+SPLIT_FRACTION = 8    # the slow table holds 1/SPLIT_FRACTION of the instances
+SLOW_PRIORITY = 0     # stream priority of the slow table (lower is higher)
 
-class Batch:
-    def __init__(self, runs, ksp=None, snes=None):
-        if not runs:
-            raise ValueError("empty batch")
+
+class _Lockstep:
+    """One libvv batch over a list of runs (and its reports)."""
+
+    def __init__(self, runs, ksp, snes):
         ctxs = [r.ctx for r in runs]
-        if len({id(c) for c in ctxs}) != len(ctxs):
-            raise ValueError("every run of a batch needs its own context (its own Grid)")
-        self.runs = list(runs)
         self.lib = _lib.load()
-        n = len(runs)
+        self.runs = runs
+        self.n = n = len(runs)
         arr_ctx = (C.c_void_p * n)(*[c.sync_stream().value for c in ctxs])
         arr_st = (_lib.vv_state * n)(*[r._st for r in runs])
         h = C.c_void_p()
         _lib.check(self.lib.vv_batch_create(n, arr_ctx, arr_st, C.byref(h)), "vv_batch_create")
         self.h = h
-        self.n = n
-        self.ksp = ksp if ksp is not None else runs[0].ksp
-        self.snes = snes if snes is not None else runs[0].snes
+        self.ksp, self.snes = ksp, snes
         self._reports = (_lib.vv_step_report * n)()
         self._status = (C.c_int * n)()
         self._stream = None
 
-    def __del__(self):
+    def destroy(self):
         if getattr(self, "h", None) is not None and self.h.value:
             try:
                 self.lib.vv_batch_destroy(self.h)
@@ -49,35 +62,127 @@ class Batch:
                 pass
             self.h = None
 
+    def __del__(self):
+        self.destroy()
+
+    def launch(self, stream):
+        s = stream.cuda_stream
+        if s != self._stream:
+            _lib.check(self.lib.vv_batch_set_stream(self.h, C.c_void_p(s)), "vv_batch_set_stream")
+            self._stream = s
+        _lib.check(self.lib.vv_batch_launch(self.h, C.byref(self.snes), C.byref(self.ksp)), "vv_batch_launch")
+
+    def collect(self):
+        """(status, reports) of the launched step; status is the first non-OK instance status."""
+        st = self.lib.vv_batch_collect(self.h, C.byref(self.snes), C.byref(self.ksp), self._reports, self._status)
+        reps = [report_dict(self._reports[i]) for i in range(self.n)]
+        for i in range(self.n):
+            reps[i]["status"] = self._status[i]
+        return st, reps
+
     def launch_count(self, reset=False):
-        """Kernels the batch has launched so far (graph nodes executed included)."""
         n = C.c_int64()
         _lib.check(self.lib.vv_batch_launch_count(self.h, C.byref(n), int(bool(reset))), "vv_batch_launch_count")
         return n.value
+
+
+class Batch:
+    """Runs advanced together; ``split``: None (one lockstep table), "auto"
+    (the first step as one table, then the slowest eighth of the instances
+    and the rest as two concurrent tables, for tables of at least
+    SPLIT_MIN instances) or a list of index lists (those tables, each run
+    in exactly one)."""
+
+    def __init__(self, runs, ksp=None, snes=None, split=None):
+        if not runs:
+            raise ValueError("empty batch")
+        ctxs = [r.ctx for r in runs]
+        if len({id(c) for c in ctxs}) != len(ctxs):
+            raise ValueError("every run of a batch needs its own context (its own Grid)")
+        self.runs = list(runs)
+        self.n = len(runs)
+        self.ksp = ksp if ksp is not None else runs[0].ksp
+        self.snes = snes if snes is not None else runs[0].snes
+        if split is None or split == "auto":
+            groups = [list(range(self.n))]
+        else:
+            groups = [sorted(int(i) for i in g) for g in split if len(g)]
+            if sorted(i for g in groups for i in g) != list(range(self.n)):
+                raise ValueError("split: every run in exactly one table")
+        self._auto = split == "auto" and self.n >= SPLIT_MIN
+        self._form(groups)
+
+    def _form(self, groups):
+        self.groups = groups
+        self._tables = [_Lockstep([self.runs[i] for i in g], self.ksp, self.snes) for g in groups]
+        self._streams = [torch.cuda.Stream(priority=SLOW_PRIORITY if k else 0) for k in range(len(groups))]
+        self._launches = 0
+
+    def __del__(self):
+        for t in getattr(self, "_tables", []):
+            t.destroy()
+
+    def launch_count(self, reset=False):
+        """Kernels the batch has launched so far (graph nodes executed included)."""
+        n = self._launches + sum(t.launch_count(reset) for t in self._tables)
+        if reset:
+            self._launches = 0
+        return n
 
     def time_kernel(self, which, it=4, reps=20):
         """Seconds per whole-table launch of one batch kernel (0 multi-dot,
         1 preconditioner, 2 Jacobian stencil, 3 multi-axpy, 4 the
         preconditioner's tridiagonal stage, 5 the GMRES operator P^-1 J as
-        the step applies it); between steps."""
+        the step applies it); between steps, on a batch of one table."""
+        if len(self._tables) != 1:
+            raise RuntimeError("time_kernel needs a batch of one lockstep table (split=None)")
+        t = self._tables[0]
         ms = C.c_double()
-        _lib.check(self.lib.vv_batch_time_kernel(self.h, int(which), int(it), int(reps), C.byref(ms)),
-                   "vv_batch_time_kernel")
+        _lib.check(t.lib.vv_batch_time_kernel(t.h, int(which), int(it), int(reps), C.byref(ms)), "vv_batch_time_kernel")
         return ms.value / 1e3
+
+    def _resplit(self, reps):
+        """Two tables: the instances that needed the most GMRES iterations in
+        the step just taken, and the rest."""
+        gm = [sum(r["gmres_its"]) for r in reps]
+        k = max(1, self.n // SPLIT_FRACTION)
+        slow = sorted(sorted(range(self.n), key=lambda i: -gm[i])[:k])
+        fast = [i for i in range(self.n) if i not in set(slow)]
+        self._launches += sum(t.launch_count() for t in self._tables)
+        for t in self._tables:
+            t.destroy()
+        self._tables = []
+        self._form([fast, slow])
 
     def step(self):
         """Advance every instance by one time step; returns per-instance reports."""
-        s = torch.cuda.current_stream().cuda_stream
-        if s != self._stream:
-            _lib.check(self.lib.vv_batch_set_stream(self.h, C.c_void_p(s)), "vv_batch_set_stream")
-            self._stream = s
-        st = self.lib.vv_batch_step(self.h, C.byref(self.snes), C.byref(self.ksp), self._reports, self._status)
-        reps = [report_dict(self._reports[i]) for i in range(self.n)]
-        for i, r in enumerate(self.runs):
+        caller = torch.cuda.current_stream()
+        if len(self._tables) == 1:
+            t = self._tables[0]
+            t.launch(caller)
+            results = [t.collect()]
+        else:
+            ev = caller.record_event()
+            for t, s in zip(self._tables, self._streams):
+                s.wait_event(ev)
+                t.launch(s)
+            results = [t.collect() for t in self._tables]
+            for s in self._streams:
+                caller.wait_stream(s)
+        reps = [None] * self.n
+        worst = _lib.VV_OK
+        for g, (st, rg) in zip(self.groups, results):
+            for i, r in zip(g, rg):
+                reps[i] = r
+            if st != _lib.VV_OK and worst == _lib.VV_OK:
+                worst = st
+        for r in self.runs:
             r.itime += 1
-            reps[i]["status"] = self._status[i]
         # an instance whose residual is above the abort threshold or NaN fails
         # alone: its status is in its report and the others are not touched
-        if st not in (_lib.VV_OK, _lib.VV_ERR_DIVERGED, _lib.VV_ERR_NAN):
-            _lib.check(st, "vv_batch_step")
+        if worst not in (_lib.VV_OK, _lib.VV_ERR_DIVERGED, _lib.VV_ERR_NAN):
+            _lib.check(worst, "vv_batch_step")
+        if self._auto:
+            self._auto = False
+            self._resplit(reps)
         return reps

@@ -2509,6 +2509,8 @@ struct vv_batch {
     unsigned long long hnd[4];   // batch handles: pic, outer, inner, revert (index = BH_*)
     bool use_graph;
     int64_t launches;
+    int64_t pending_l0 = 0;      // launch count before the uncollected launch
+    int pending = 0;             // 1: a vv_batch_launch awaits its vv_batch_collect
     int nk_prologue, nk_pic_head, nk_cycle_head, nk_arnoldi, nk_cycle_tail, nk_pic_tail, nk_revert_ctrl, nk_revert;
 };
 
@@ -3025,6 +3027,7 @@ extern "C" {
 
 int vv_batch_destroy(vv_batch* b) {
     if (!b) return VV_OK;
+    if (b->pending && b->user) cudaStreamSynchronize(b->user);   // a launch never collected: let it finish
     for (auto s : b->cs) {
         cudaStreamCaptureStatus cst = cudaStreamCaptureStatusNone;
         if (s && cudaStreamIsCapturing(s, &cst) == cudaSuccess && cst != cudaStreamCaptureStatusNone) {
@@ -3259,9 +3262,9 @@ int vv_batch_set_stream(vv_batch* b, void* stream) {
     return VV_OK;
 }
 
-int vv_batch_step(vv_batch* b, const vv_snes_opts* so, const vv_ksp_opts* ko, vv_step_report* reports,
-                  int* statuses) {
-    if (!b || !so || !ko || !reports) return VV_ERR_ARG;
+int vv_batch_launch(vv_batch* b, const vv_snes_opts* so, const vv_ksp_opts* ko) {
+    if (!b || !so || !ko) return VV_ERR_ARG;
+    if (b->pending) return fail(VV_ERR_ARG, "vv_batch_launch: the previous launch was not collected");
     for (int i = 0; i < b->n; ++i) {
         vv_ctx* c = b->ctx[i];
         const int restart = (ko->restart > 0) ? ko->restart : c->restart;
@@ -3275,7 +3278,7 @@ int vv_batch_step(vv_batch* b, const vv_snes_opts* so, const vv_ksp_opts* ko, vv
         TRY(r);
     }
     b->st = b->user;
-    const int64_t l0 = b->launches;
+    b->pending_l0 = b->launches;
     CK(cudaMemsetAsync(b->counts, 0, 8 * sizeof(unsigned int), b->user));
     if (b->use_graph) {
         CK(cudaGraphLaunch(b->ex, b->user));
@@ -3291,11 +3294,20 @@ int vv_batch_step(vv_batch* b, const vv_snes_opts* so, const vv_ksp_opts* ko, vv
     CK(cudaMemcpyAsync(b->hgather, b->gather, (size_t)b->n * b->words * sizeof(unsigned int), cudaMemcpyDeviceToHost,
                        b->user));
     CK(cudaMemcpyAsync(b->hcounts, b->counts, 8 * sizeof(unsigned int), cudaMemcpyDeviceToHost, b->user));
-    CK(cudaStreamSynchronize(b->user));
     b->st = b->cs[0];
+    b->pending = 1;
+    return VV_OK;
+}
+
+int vv_batch_collect(vv_batch* b, const vv_snes_opts* so, const vv_ksp_opts* ko, vv_step_report* reports,
+                     int* statuses) {
+    if (!b || !so || !ko || !reports) return VV_ERR_ARG;
+    if (!b->pending) return fail(VV_ERR_ARG, "vv_batch_collect: nothing launched");
+    b->pending = 0;
+    CK(cudaStreamSynchronize(b->user));
     if (b->use_graph) {
         const unsigned* k = b->hcounts;
-        b->launches = l0 + 1 + b->nk_prologue + b->nk_revert_ctrl +
+        b->launches = b->pending_l0 + 1 + b->nk_prologue + b->nk_revert_ctrl +
                       (int64_t)k[vv::BC_PIC] * (b->nk_pic_head + b->nk_pic_tail) +
                       (int64_t)(k[vv::BC_GM_START] + k[vv::BC_GM_FINISH]) * (b->nk_cycle_head + b->nk_cycle_tail) +
                       (int64_t)k[vv::BC_INNER] * b->nk_arnoldi + (int64_t)k[vv::BC_REVERT] * b->nk_revert;
@@ -3311,6 +3323,13 @@ int vv_batch_step(vv_batch* b, const vv_snes_opts* so, const vv_ksp_opts* ko, vv
         if (s != VV_OK && first_bad == VV_OK) first_bad = s;
     }
     return first_bad;
+}
+
+int vv_batch_step(vv_batch* b, const vv_snes_opts* so, const vv_ksp_opts* ko, vv_step_report* reports,
+                  int* statuses) {
+    if (!b || !so || !ko || !reports) return VV_ERR_ARG;
+    TRY(vv_batch_launch(b, so, ko));
+    return vv_batch_collect(b, so, ko, reports, statuses);
 }
 
 int vv_batch_time_kernel(vv_batch* b, int which, int it, int reps, double* avg_ms) {

@@ -55,6 +55,8 @@ def main(argv=None):
     ap.add_argument("--sweep-steps", type=int, default=0,
                     help="with --sweep: run this many batched time steps (after one warm-up step) instead")
     ap.add_argument("--snes-atol", type=float, default=1e-10, help="with --sweep-steps: the Picard tolerance")
+    ap.add_argument("--split", default=None, choices=["auto"],
+                    help="with --sweep-steps: step the slowest instances as a second concurrent table")
     args = ap.parse_args(argv)
     if args.sweep:
         return sweep_main(args)
@@ -105,7 +107,8 @@ def sweep_main(args):
     from .batch import Batch
     specs = W.sweep_specs(args.sweep)
     cells = sum(s["nx"] * s["nv"] for s in specs)
-    batch = Batch(W.sweep_runs(specs=specs, precision=args.precision, snes_atol=args.snes_atol))
+    batch = Batch(W.sweep_runs(specs=specs, precision=args.precision, snes_atol=args.snes_atol),
+                  split=args.split if args.sweep_steps else None)
     if args.sweep_steps:
         batch.step()
         for k in range(args.sweep_steps):
