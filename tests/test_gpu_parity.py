@@ -405,16 +405,16 @@ def test_graph_step_equals_host_driven_step():
     assert run_g.ctx.launch_count() > 0
 
 
-def _small_run(nx, nv, f0fn, L, ht, vmax=10.0):
+def _small_run(nx, nv, f0fn, L, ht, vmax=10.0, snes_atol=1e-11, precision="fp64"):
     from vivlasov1d_b200.run import Run
     cfg = {"grid": {"nx": nx, "nv": nv, "L": L, "vmin": -vmax, "vmax": vmax, "ht": ht, "nt": 1},
            "solver": {"method": "matrixfree", "poisson_bracket": "ArakawaJ4", "preconditioner_type": "tensor",
                       "preconditioner_scheme": "tensor_kinetic", "petsc_ksp_rtol": 1e-6,
-                      "petsc_snes_atol": 1e-11},
+                      "petsc_snes_atol": snes_atol},
            "initial_data": {"charge": -1.0}}
     og = vo.Grid(nx, nv, L, vmax, -vmax, ht=ht)
     f0 = vo.initialise_distribution_function(og, f0fn)
-    return Run(cfg, f0=torch.from_numpy(vo.to_flat(f0)))
+    return Run(cfg, f0=torch.from_numpy(vo.to_flat(f0)), precision=precision)
 
 
 def _assert_batch_matches(rb, rs, fb, fs, i, ftol):
@@ -545,6 +545,37 @@ def test_batch_fused_stencil_equals_tiles(monkeypatch):
     for ra, rb in zip(out[0][1], out[1][1]):
         for i, (x, y) in enumerate(zip(ra, rb)):
             _assert_batch_matches(x, y, out[0][0][i], out[1][0][i], i, 1e-12)
+
+
+WIDE_SPECS = [(512, 64, vo.f0_landau(0.1, 0.5), 4 * np.pi, 0.1),
+              (256, 96, vo.f0_twostream(0.05, 0.5), 4 * np.pi, 0.1)]
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_batch_wide_rows_equal_single_steps(monkeypatch, precision):
+    """The longest rows of the v-major layout (nx 512: 256-point complex
+    x-FFTs, 8 rows per item) beside nx 256, in FP64 and mixed precision:
+    the fused stencil + x-FFT and the staged inverse x-FFT against each
+    instance's own step."""
+    from vivlasov1d_b200.batch import Batch
+
+    def runs():
+        # Picard tolerance 1e-9: these grids' residual floor is near 1e-11,
+        # where the stop rule would be decided by rounding
+        return [_small_run(*s, snes_atol=1e-9, precision=precision) for s in WIDE_SPECS]
+    batch_runs, single_runs = runs(), runs()
+    monkeypatch.setenv("VV_BATCH_SHAPE", "2,6,0,1,0,1")
+    batch = Batch(batch_runs)
+    for _ in range(2):
+        rb = batch.step()
+        for i, r in enumerate(single_runs):
+            rs = r.step()
+            assert rb[i]["status"] == 0
+            if precision == "fp64":
+                _assert_batch_matches(rb[i], rs, batch_runs[i].fc, r.fc, i, 1e-10)
+            else:   # FP32 inner solves: the same fixed point, not the same iterates
+                fb, fs = batch_runs[i].fc, r.fc
+                assert (fb - fs).abs().max().item() <= 1e-8 * fs.abs().max().item(), i
 
 
 def test_batch_split_tables_follow_one_table():
