@@ -2689,7 +2689,8 @@ int b_arnoldi(vv_batch* b) {
     TRY(blaunch(b, vv::k_b_gm_maxpy_p<T>, vv::F_VEC, vv::RED_THREADS, 0, tab, A, b->n));
     // ||w||, Arnoldi bookkeeping and the BC_INNER control step in one launch
     return blaunch(b, vv::k_b_arnoldi_ctrl, vv::F_INST, vv::CTRL_THREADS, 0, tab, A, b->n,
-                   (b->use_graph ? b->hnd[BH_INNER] : 0ull), b->flag, b->counts, b->lists, b->counts + 7);
+                   (b->use_graph ? b->hnd[BH_INNER] : 0ull), b->flag, b->counts, b->lists, b->counts + 7,
+                   b->counts + 6);
 }
 
 template <int S, typename T>

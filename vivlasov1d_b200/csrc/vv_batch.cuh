@@ -1253,13 +1253,15 @@ k_b_build_subset(const BInst* __restrict__ tab, int n, int* __restrict__ lists, 
 // End of an Arnoldi step: ||w|| and the Arnoldi bookkeeping of every
 // instance of list L (one block per instance; vsc of the new vector), then the
 // BC_INNER control step by the block that finishes last (`done`: a grid
-// counter, zero on entry and on exit).  The blocks only write instance
+// counter, zero on entry and on exit; `dropped`: the instances that left the
+// inner loop in this step, zero on entry and on exit).  The blocks only write instance
 // state before the counter, so the device-scope fence is short.
 __global__ void __launch_bounds__(CTRL_THREADS)
 k_b_arnoldi_ctrl(const BInst* __restrict__ tab, const int* __restrict__ L, int n, unsigned long long handle,
                  int* __restrict__ flag, unsigned int* __restrict__ counts, int* __restrict__ lists,
-                 unsigned int* __restrict__ done) {
+                 unsigned int* __restrict__ done, unsigned int* __restrict__ dropped) {
     __shared__ double s_h[MAX_RESTART + 2], s_c[MAX_RESTART + 1], s_s[MAX_RESTART + 1];
+    __shared__ unsigned int s_dropped;
     // the blocks that get an item take part in the grid counter (block 0
     // always, for an empty list); read before any block arrives, so before
     // the last one compacts the list in place
@@ -1275,20 +1277,26 @@ k_b_arnoldi_ctrl(const BInst* __restrict__ tab, const int* __restrict__ L, int n
             }
         }
         const double ss2 = block_reduce_parts(I.wpart, wi_count(I));   // its barriers publish the copies
-        if (threadIdx.x == 0) gm_arnoldi(s, sqrt(ss2), s_h, s_c, s_s);
+        if (threadIdx.x == 0) {
+            gm_arnoldi(s, sqrt(ss2), s_h, s_c, s_s);
+            if (!s->active) atomicAdd(dropped, 1u);   // before this block's arrival at the counter
+        }
     });
     if ((int)blockIdx.x >= nb || !last_block(done, nb)) return;
     // the inner loop only drops instances: compact the current L_INNER in
     // place instead of scanning the whole table (a tail pass with a few
-    // instances left reads a few states, not n)
+    // instances left reads a few states, not n), and only when an instance
+    // left it in this step
     int* LI = lists + (size_t)L_INNER * blist_words(n);
     const int cnt = LI[0];
     const int* ids = LI + 1 + NFAM;
+    if (threadIdx.x == 0) s_dropped = atomicExch(dropped, 0u);
     __syncthreads();
-    ctrl_build_from(tab, n, cnt, lists, L_INNER, [&](int q) {
-        const DevState* s = tab[q].ds;
-        return s->gm_outer != 0 && s->active != 0;
-    }, [&](int i) { return ids[i]; });
+    if (s_dropped)
+        ctrl_build_from(tab, n, cnt, lists, L_INNER, [&](int q) {
+            const DevState* s = tab[q].ds;
+            return s->gm_outer != 0 && s->active != 0;
+        }, [&](int i) { return ids[i]; });
     if (threadIdx.x == 0) {
         const int any = LI[0] > 0 ? 1 : 0;
         set_cond(handle, any ? 1u : 0u);
