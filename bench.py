@@ -26,9 +26,10 @@ field_energy: after W+K steps, |E - E_oracle| / |E_oracle| per instance for
               every GPU arm against the FP64 oracle (the C port run for the
               same W+K steps, which is also the timed cpu_baseline), and
               the batched mixed arm against the plain FP64 GPU arm.
-e2e         : the batched mixed step through Batch.step with every
-              instance's f copied host->device (pinned) before and
-              device->host after each step.
+e2e         : the batched mixed step through Batch.step(host=...), which
+              copies every instance's f host->device (pinned) before and
+              device->host after each step, table by table on the tables'
+              streams.
 batched_fp64: the same table through the batch in FP64 (ksp_rtol 1e-4): the
               gain of batching alone, apart from the FP32 inner solves.
 step_roofline: algorithmic bytes of the timed steps (from the logged
@@ -260,15 +261,9 @@ def run_gpu(args, rank, world):
         r.calculate_moments()
     del snapshot
 
-    def e2e_step():
-        for h, r in zip(hosts, mixed):
-            r.fc.copy_(h, non_blocking=True)
-        out = batch.step()
-        for h, r in zip(hosts, mixed):
-            h.copy_(r.fc, non_blocking=True)
-        return out
-
-    t_e2e, _ = time_steps(e2e_step, args.steps, stream)
+    # every instance's f copied in from its pinned host buffer before the step
+    # and back out after it, by the batch on each table's stream
+    t_e2e, _ = time_steps(lambda: batch.step(host=hosts), args.steps, stream)
     total_cells = cells
     if world > 1:
         (t_value, t_plain, t_e2e, t_b64), (total_cells,) = reduce_over_ranks([t_value, t_plain, t_e2e, t_b64],

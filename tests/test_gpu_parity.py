@@ -599,6 +599,27 @@ def test_batch_split_tables_follow_one_table():
     assert b3.launch_count() > 0
 
 
+@pytest.mark.parametrize("split", [None, [[0, 2], [1]]])
+def test_batch_step_host_buffers(monkeypatch, split):
+    """Batch.step(host=...) copies every instance's f in from its pinned host
+    buffer and back out after the step: the same bits as a step of the
+    resident state (one fixed kernel shape for both batches), and the
+    buffers hold the result."""
+    from vivlasov1d_b200.batch import Batch
+    monkeypatch.setenv("VV_BATCH_SHAPE", "2,6,0,1,0,1")
+    dev = [_small_run(*s) for s in BATCH_SPECS]
+    via = [_small_run(*s) for s in BATCH_SPECS]
+    hosts = [r.fc.detach().cpu().pin_memory() for r in via]
+    bd, bh = Batch(dev, split=split), Batch(via, split=split)
+    for _ in range(2):
+        rd, rh = bd.step(), bh.step(host=hosts)
+        torch.cuda.synchronize()
+        for i in range(len(BATCH_SPECS)):
+            assert rd[i] == rh[i], i
+            assert torch.equal(dev[i].fc, via[i].fc), i
+            assert torch.equal(hosts[i], via[i].fc.cpu()), i
+
+
 def test_batch_launch_collect_order(monkeypatch):
     """vv_batch_collect without a launch, and a second launch before the
     collect, are refused (VV_ERR_ARG) and leave the batch usable."""

@@ -154,18 +154,36 @@ class Batch:
         self._tables = []
         self._form([fast, slow])
 
-    def step(self):
-        """Advance every instance by one time step; returns per-instance reports."""
+    def step(self, host=None):
+        """Advance every instance by one time step; returns per-instance reports.
+
+        host: optional list of n host tensors (pinned, shaped like each run's
+        f): every instance's f is copied in from its buffer before its table's
+        step and back out after it, on the table's stream (with two tables the
+        copies of one overlap the other's step)."""
         caller = torch.cuda.current_stream()
+        if host is not None and len(host) != self.n:
+            raise ValueError("host: one buffer per run")
+
+        def run_table(k, t, s):
+            g = self.groups[k]
+            if host is not None:
+                for i in g:
+                    self.runs[i].fc.copy_(host[i], non_blocking=True)
+            t.launch(s)
+            if host is not None:
+                for i in g:
+                    host[i].copy_(self.runs[i].fc, non_blocking=True)
+
         if len(self._tables) == 1:
-            t = self._tables[0]
-            t.launch(caller)
-            results = [t.collect()]
+            run_table(0, self._tables[0], caller)
+            results = [self._tables[0].collect()]
         else:
             ev = caller.record_event()
-            for t, s in zip(self._tables, self._streams):
+            for k, (t, s) in enumerate(zip(self._tables, self._streams)):
                 s.wait_event(ev)
-                t.launch(s)
+                with torch.cuda.stream(s):
+                    run_table(k, t, s)
             results = [t.collect() for t in self._tables]
             for s in self._streams:
                 caller.wait_stream(s)
