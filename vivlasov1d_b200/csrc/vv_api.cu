@@ -2474,6 +2474,7 @@ struct vv_batch {
     int march;                   // 1: Jacobian stencil by the marching kernel, 0: 64 x 32 tiles
     bool pcj_ok;                 // every instance has M in 32..256 (the v-major kernels' lengths)
     void* dinvJ;                 // device: v-major LU reciprocals of every instance (GMRES precision)
+    void* jtab;                  // device: every instance's Jacobian stencil coefficient tables (k_b_jcoef)
     size_t smem_fftj;            // dynamic shared memory of the v-major FFT blocks
     size_t smem_fjv;             // ... of the Jacobian stencil fused with the x-FFT (k_b_jvp_rfftj)
     int fuse;                    // 1: the GMRES operator's stencil runs inside the preconditioner's x-FFT
@@ -3042,7 +3043,7 @@ int vv_batch_destroy(vv_batch* b) {
     if (b->ex) cudaGraphExecDestroy(b->ex);
     if (b->g) cudaGraphDestroy(b->g);
     for (void* p : {(void*)b->tab, (void*)b->lists, (void*)b->counts, (void*)b->flag, (void*)b->gather, (void*)b->wpart,
-                    b->dinvJ})
+                    b->dinvJ, b->jtab})
         if (p) cudaFree(p);
     if (b->hflag) cudaFreeHost(b->hflag);
     if (b->hcounts) cudaFreeHost(b->hcounts);
@@ -3178,6 +3179,24 @@ int vv_batch_create(int n, vv_ctx* const* ctxs, const vv_state* states, vv_batch
             }
             const cudaError_t e = cudaDeviceSynchronize();
             if (e != cudaSuccess) return fail_b(fail_cuda(e, "v-major LU tables"));
+            // the fused stencil's coefficient tables: (nx + nv) x 3 of the GMRES precision per
+            // instance, 16-byte aligned; filled by k_b_jcoef once the table is on the device
+            const size_t tsz = csz / 2;
+            std::vector<size_t> jo(n);
+            size_t jbytes = 0;
+            for (int i = 0; i < n; ++i) {
+                jo[i] = jbytes;
+                jbytes += (3 * (size_t)(ctxs[i]->nx + ctxs[i]->nv) * tsz + 15) & ~(size_t)15;
+            }
+            if (cudaMalloc(&b->jtab, jbytes) != cudaSuccess) return fail_b(VV_ERR_ALLOC);
+            const int js = b->scheme == VV_BRACKET_J1 ? 1 : b->scheme == VV_BRACKET_J2 ? 2 : 4;
+            for (int i = 0; i < n; ++i) {
+                char* base = (char*)b->jtab + jo[i];
+                tab[i].jcol = base;
+                tab[i].jrow = base + 3 * (size_t)ctxs[i]->nx * tsz;
+                tab[i].jfp32 = b->mixed ? 1 : 0;
+                tab[i].jscheme = js;
+            }
         }
     }
     // per-warp partials: (restart + 2) columns of 8 vblk per instance
@@ -3211,6 +3230,10 @@ int vv_batch_create(int n, vv_ctx* const* ctxs, const vv_state* states, vv_batch
     // empty lists, then the list of every instance
     if (cudaMemsetAsync(b->lists, 0, (size_t)vv::NLIST * b->list_words * sizeof(int), b->st) != cudaSuccess)
         return fail_b(fail_cuda(cudaGetLastError(), "batch lists"));
+    if (b->jtab) {
+        vv::k_b_jcoef<<<n, 1024, 0, b->st>>>(b->tab, n);
+        if (cudaGetLastError() != cudaSuccess) return fail_b(VV_ERR_CUDA);
+    }
     b_shape(b, tab, 4, 0, 0);
     if ((r = b_apply_shape(b, tab)) != VV_OK) return fail_b(r);
     {

@@ -51,6 +51,11 @@ struct BInst {
     const void* dinvJ;
     // per-warp partial sums of the GMRES reductions: (restart + 2) columns of 8 * vblk
     double* wpart;
+    // the Jacobian stencil's coefficients in the GMRES precision (jfp32: FP32):
+    // per column (B1, bm, bp) from the x profile of h (rewritten by k_b_poisson
+    // every Picard pass), per row (A1, am, ap) from h0; jscheme: 1, 2 or 4
+    void *jcol, *jrow;
+    int jfp32, jscheme;
 };
 
 // layout of one work list: [nact][total per family][ids: n][prefix per family: n+1]
@@ -104,18 +109,18 @@ VV_DEV void list_stage(const int* __restrict__ L, int n, const ListHead& h, int*
 
 // Loop of a persistent block over the work items of family F in list L:
 // body(instance, local block).  Block-uniform; a barrier separates items.
-// Lists of up to BLIST_SMEM instances are searched in shared memory.
-template <int F, typename Body>
+// Lists of up to STAGE_MAX instances are searched in shared memory.
+template <int F, int STAGE_MAX = BLIST_SMEM, typename Body>
 VV_DEV void for_work(const BInst* __restrict__ tab, const int* __restrict__ L, int n, Body body) {
-    __shared__ int s_pre[BLIST_SMEM + 1];
-    __shared__ int s_ids[BLIST_SMEM];
+    __shared__ int s_pre[STAGE_MAX + 1];
+    __shared__ int s_ids[STAGE_MAX];
     const ListHead h = list_head<F>(L, n);
     const int nact = h.nact;
     const int total = h.total;
     if ((int)blockIdx.x >= total) return;
     const int* ids = L + 1 + NFAM;
     const int* pre = ids + n + (size_t)F * (n + 1);
-    const bool staged = nact <= BLIST_SMEM;
+    const bool staged = nact <= STAGE_MAX;
     if (staged) {
         list_stage<F>(L, n, h, s_pre, s_ids);
         __syncthreads();
@@ -312,6 +317,76 @@ __global__ void __launch_bounds__(32) k_b_tridiagj(const BInst* __restrict__ tab
     });
 }
 
+// ---- the Jacobian stencil's coefficient tables --------------------------------
+// The coefficient form of the J1/J2/J4 bracket (the wide tiles' srow / scol):
+// per column i (B1, bm, bp) from b = the x profile of h at i-2..i+2
+// (periodic), per row j (A1, am, ap) from h0 at j-2..j+2 (zero outside the
+// grid), computed in FP64 and stored in the GMRES precision as three arrays
+// each (jcol = B1[nx] bm[nx] bp[nx], jrow = A1[nv] am[nv] ap[nv]).  The row
+// table is fixed; the column table follows the x profile, which changes only
+// in k_b_prologue and k_b_poisson, and k_b_poisson (which follows every
+// prologue) rewrites it.
+template <int SCHEME, typename T>
+VV_DEV void jcoef_cols_s(const BInst& I, const double* sb) {
+    T* jc = reinterpret_cast<T*>(I.jcol);
+    for (int i = threadIdx.x; i < I.nx; i += blockDim.x) {
+        const int l = i + 2;
+        double bm, bq;
+        Coef<SCHEME>::col(sb[l] - sb[l - 1], sb[l + 1] - sb[l], sb[l + 1] - sb[l - 1], sb[l] - sb[l - 2],
+                          sb[l + 2] - sb[l], bm, bq);
+        jc[i] = T(sb[l + 1] - sb[l - 1]);
+        jc[I.nx + i] = T(bm);
+        jc[2 * I.nx + i] = T(bq);
+    }
+}
+template <int SCHEME, typename T>
+VV_DEV void jcoef_rows_s(const BInst& I) {
+    T* jr = reinterpret_cast<T*>(I.jrow);
+    const double* h0 = I.bp.h0;
+    const int nv = I.nv;
+    for (int j = threadIdx.x; j < nv; j += blockDim.x) {
+        double a[5];
+#pragma unroll
+        for (int d = 0; d < 5; ++d) {
+            const int jj = j - 2 + d;
+            a[d] = (jj >= 0 && jj < nv) ? h0[jj] : 0.0;
+        }
+        double am, aq;
+        Coef<SCHEME>::row(a[2] - a[1], a[3] - a[2], a[3] - a[1], a[2] - a[0], a[4] - a[2], am, aq);
+        jr[j] = T(a[3] - a[1]);
+        jr[nv + j] = T(am);
+        jr[2 * nv + j] = T(aq);
+    }
+}
+constexpr int JCOEF_NXMAX = 512;   // the longest rows of the v-major layout (M <= 256)
+// block-uniform: the column table from the current x profile of h (and the
+// row table when `rows`), for the instance's scheme and precision
+VV_DEV void jcoef_block(const BInst& I, bool rows) {
+    if (!I.jcol || I.nx > JCOEF_NXMAX) return;
+    __shared__ double sb[JCOEF_NXMAX + 4];
+    for (int c = threadIdx.x; c < I.nx + 4; c += blockDim.x) {
+        int xi = c - 2;
+        if (xi < 0) xi += I.nx;
+        else if (xi >= I.nx) xi -= I.nx;
+        sb[c] = b_fac(I.bp, xi);
+    }
+    __syncthreads();
+    switch (I.jscheme * 2 + I.jfp32) {
+        case 2: jcoef_cols_s<1, double>(I, sb); if (rows) jcoef_rows_s<1, double>(I); break;
+        case 3: jcoef_cols_s<1, float>(I, sb); if (rows) jcoef_rows_s<1, float>(I); break;
+        case 4: jcoef_cols_s<2, double>(I, sb); if (rows) jcoef_rows_s<2, double>(I); break;
+        case 5: jcoef_cols_s<2, float>(I, sb); if (rows) jcoef_rows_s<2, float>(I); break;
+        case 8: jcoef_cols_s<4, double>(I, sb); if (rows) jcoef_rows_s<4, double>(I); break;
+        default: jcoef_cols_s<4, float>(I, sb); if (rows) jcoef_rows_s<4, float>(I); break;
+    }
+    __syncthreads();
+}
+
+// both tables of every instance (one block per instance; at batch creation)
+__global__ void __launch_bounds__(1024) k_b_jcoef(const BInst* __restrict__ tab, int n) {
+    if ((int)blockIdx.x < n) jcoef_block(tab[blockIdx.x], true);
+}
+
 // ---- Jacobian stencil fused with the x-FFT of the preconditioner -------------
 // The GMRES operator applies the Jacobian stencil and then P^-1, whose first
 // stage is the real FFT of every v row: one kernel computes the stencil of
@@ -319,16 +394,14 @@ __global__ void __launch_bounds__(32) k_b_tridiagj(const BInst* __restrict__ tab
 // (periodic halo of 2 in x) and transforms them in place of the row loads,
 // so the stencil's output never goes through HBM and one launch per Arnoldi
 // step is saved.  The stencil is the wide-tile kernel's expression (the
-// coefficient form of the J1/J2/J4 bracket with the point time derivative,
-// coefficients from the x and v profiles of h in FP64, cast to T).
+// coefficient form of the J1/J2/J4 bracket with the point time derivative),
+// its coefficients read from the instance's tables (jcoef_block).
 //
 // Shared memory: the FFT's twiddles, then two regions that the stencil and
 // the FFT use in turn (each region's next user starts after a barrier that
 // follows its last read):
-//   region 1, the pass-1 buffer A or: b values (nx + 4 doubles), h0 values
-//     (RB + 4 doubles), column coefficients (nx x 3 T), row coefficients
-//     (RB x 3 T) and the band ((RB + 4) x (nx + 8) T, row r at
-//     band[r * (nx + 8) + 4 + i]);
+//   region 1, the pass-1 buffer A or: the RB rows' coefficients (3 x RB T)
+//     and the band ((RB + 4) x (nx + 8) T, row r at band[r * (nx + 8) + 4 + i]);
 //   region 2, the pass-2 buffer B or the stencil's output (RB rows of
 //     2 SB >= nx T: the row stride of B, which keeps the first pass's 8-byte
 //     reads of two rows per half-warp on distinct banks where SB is padded).
@@ -336,8 +409,7 @@ __global__ void __launch_bounds__(32) k_b_tridiagj(const BInst* __restrict__ tab
 // register window (6 shared loads per output, as the wide tiles).
 __host__ __device__ constexpr size_t fjv_align(size_t b) { return (b + 15) & ~(size_t)15; }
 __host__ __device__ constexpr size_t fjv_band(int M, int rb, size_t tsz) {
-    return fjv_align((size_t)(2 * M + 4) * 8) + fjv_align((size_t)(rb + 4) * 8) + fjv_align((size_t)2 * M * 3 * tsz) +
-           fjv_align((size_t)rb * 3 * tsz) + fjv_align((size_t)(rb + 4) * (2 * M + 8) * tsz);
+    return fjv_align((size_t)rb * 3 * tsz) + fjv_align((size_t)(rb + 4) * (2 * M + 8) * tsz);
 }
 template <int M> __host__ __device__ constexpr size_t fjv_region1(size_t tsz) {
     constexpr int P1 = FftJ<M>::P1, P2 = FftJ<M>::P2, RB = fj_rows(P2);
@@ -360,7 +432,8 @@ inline size_t fjv_smem_of(int M, size_t tsz) {
 
 template <int SCHEME, typename T, int M>
 VV_DEV void jvp_rfftj_block(const T* __restrict__ X, typename Cplx<T>::type* __restrict__ spec, const PcParams& pp,
-                            const BracketParams& bp, int item) {
+                            const BracketParams& bp, const T* __restrict__ jcol, const T* __restrict__ jrow,
+                            int item) {
     using C = typename Cplx<T>::type;
     constexpr int P1 = FftJ<M>::P1, P2 = FftJ<M>::P2, RB = fj_rows(P2);
     constexpr int NX = 2 * M, BS = NX + 8, YS = 2 * fj_sb(M, P2), VN = 16 / (int)sizeof(T);
@@ -371,16 +444,8 @@ VV_DEV void jvp_rfftj_block(const T* __restrict__ X, typename Cplx<T>::type* __r
     C* A = reinterpret_cast<C*>(r1);
     C* B = reinterpret_cast<C*>(r1 + fjv_region1<M>(sizeof(T)));
     T* sy = reinterpret_cast<T*>(B);
-    unsigned char* ex = r1;
-    double* bv = reinterpret_cast<double*>(ex);
-    ex += fjv_align((size_t)(NX + 4) * 8);
-    double* hv = reinterpret_cast<double*>(ex);
-    ex += fjv_align((size_t)(RB + 4) * 8);
-    T* scol = reinterpret_cast<T*>(ex);
-    ex += fjv_align((size_t)NX * 3 * sizeof(T));
-    T* srow = reinterpret_cast<T*>(ex);
-    ex += fjv_align((size_t)RB * 3 * sizeof(T));
-    T* band = reinterpret_cast<T*>(ex);
+    T* srow = reinterpret_cast<T*>(r1);   // A1, am, ap of the RB rows: srow[k * RB + r]
+    T* band = reinterpret_cast<T*>(r1 + fjv_align((size_t)RB * 3 * sizeof(T)));
     const int nv = pp.nv, j0 = item * RB;
     const C* tw = reinterpret_cast<const C*>(pp.tw);
     for (int k = threadIdx.x; k < M; k += FJ_THREADS) stw[k] = tw[k];
@@ -401,36 +466,11 @@ VV_DEV void jvp_rfftj_block(const T* __restrict__ X, typename Cplx<T>::type* __r
         const int xi = h < 2 ? NX - 2 + h : h - 2;
         band[rr * BS + c] = (jj >= 0 && jj < nv) ? X[(size_t)jj * NX + xi] : T(0);
     }
-    for (int c = threadIdx.x; c < NX + 4; c += FJ_THREADS) {
-        int xi = c - 2;
-        if (xi < 0) xi += NX;
-        else if (xi >= NX) xi -= NX;
-        bv[c] = b_fac(bp, xi);
-    }
-    for (int rr = threadIdx.x; rr < RB + 4; rr += FJ_THREADS) {
-        const int jj = j0 - 2 + rr;
-        hv[rr] = (jj >= 0 && jj < nv) ? bp.h0[jj] : 0.0;
+    for (int q = threadIdx.x; q < 3 * RB; q += FJ_THREADS) {
+        const int k = q / RB, j = j0 + q - k * RB;
+        srow[q] = j < nv ? jrow[k * nv + j] : T(0);
     }
     cp_async_wait0();
-    __syncthreads();
-    for (int i = threadIdx.x; i < NX; i += FJ_THREADS) {
-        const int l = i + 2;
-        double bm, bq;
-        Coef<SCHEME>::col(bv[l] - bv[l - 1], bv[l + 1] - bv[l], bv[l + 1] - bv[l - 1], bv[l] - bv[l - 2],
-                          bv[l + 2] - bv[l], bm, bq);
-        scol[3 * i] = T(bv[l + 1] - bv[l - 1]);
-        scol[3 * i + 1] = T(bm);
-        scol[3 * i + 2] = T(bq);
-    }
-    if (threadIdx.x < RB) {
-        const int l = threadIdx.x + 2;
-        double am, aq;
-        Coef<SCHEME>::row(hv[l] - hv[l - 1], hv[l + 1] - hv[l], hv[l + 1] - hv[l - 1], hv[l] - hv[l - 2],
-                          hv[l + 2] - hv[l], am, aq);
-        srow[3 * threadIdx.x] = T(hv[l + 1] - hv[l - 1]);
-        srow[3 * threadIdx.x + 1] = T(am);
-        srow[3 * threadIdx.x + 2] = T(aq);
-    }
     __syncthreads();
     const T tscale = T(((SCHEME == 2) ? bp.f2 : bp.f1) * bp.factor);
     const T htinv = T(bp.ht_inv);
@@ -438,7 +478,7 @@ VV_DEV void jvp_rfftj_block(const T* __restrict__ X, typename Cplx<T>::type* __r
     // a register window: column i rows r-2..r+2, columns i+-1 rows r-1..r+1
     for (int i = threadIdx.x; i < NX; i += FJ_THREADS) {
         const T* bc = band + 4 + i;    // row rr of the band at bc[rr * BS]
-        const T B1 = scol[3 * i], bm = scol[3 * i + 1], bq = scol[3 * i + 2];
+        const T B1 = jcol[i], bm = jcol[NX + i], bq = jcol[2 * NX + i];
         T w0 = bc[0], w1 = bc[BS], w2 = bc[2 * BS], w3 = bc[3 * BS];
         T m0 = bc[BS - 1], m1 = bc[2 * BS - 1], q0 = bc[BS + 1], q1 = bc[2 * BS + 1];
 #pragma unroll 4
@@ -448,7 +488,7 @@ VV_DEV void jvp_rfftj_block(const T* __restrict__ X, typename Cplx<T>::type* __r
             const int j = j0 + r;
             T y = htinv * w2;
             if (j >= 2 && j < nv - 2) {
-                const T A1 = srow[3 * r], am = srow[3 * r + 1], ap = srow[3 * r + 2];
+                const T A1 = srow[r], am = srow[RB + r], ap = srow[2 * RB + r];
                 T s = T(0);
                 if (Coef<SCHEME>::cA1 != 0.0 || Coef<SCHEME>::cA2 != 0.0) {
                     T ax = T(0), bx = T(0);
@@ -482,11 +522,15 @@ VV_DEV void jvp_rfftj_block(const T* __restrict__ X, typename Cplx<T>::type* __r
 }
 
 // Jacobian stencil + x-FFT of every active instance's RB-row items:
-// BS_X: J x; BS_VIT: J v_it, v_it = vsc[it] V[it] (as k_b_bracket)
+// BS_X: J x; BS_VIT: J v_it, v_it = vsc[it] V[it] (as k_b_bracket).  The
+// list is staged for up to FJV_STAGE instances (larger lists are searched in
+// global memory), which keeps the static shared memory small enough for
+// five blocks per SM beside the largest stencil band.
+constexpr int FJV_STAGE = 256;
 template <int SCHEME, int SRC, typename T>
 __global__ void __launch_bounds__(FJ_THREADS, 5) k_b_jvp_rfftj(const BInst* __restrict__ tab, const int* __restrict__ L,
                                                             int n) {
-    for_work<F_ROWS>(tab, L, n, [&](const BInst& I, int local) {
+    for_work<F_ROWS, FJV_STAGE>(tab, L, n, [&](const BInst& I, int local) {
         BracketParams p = I.bp;
         p.xidx = nullptr;
         p.factor = 0.5;
@@ -497,11 +541,13 @@ __global__ void __launch_bounds__(FJ_THREADS, 5) k_b_jvp_rfftj(const BInst* __re
         }
         const T* X = (SRC == BS_X) ? (const T*)I.xT : (const T*)I.V + (size_t)I.ds->it * I.ncell;
         auto* spec = (typename Cplx<T>::type*)I.specT;
+        const T* jc = (const T*)I.jcol;
+        const T* jr = (const T*)I.jrow;
         switch (I.pp.M) {
-            case 32: jvp_rfftj_block<SCHEME, T, 32>(X, spec, I.pp, p, local); break;
-            case 64: jvp_rfftj_block<SCHEME, T, 64>(X, spec, I.pp, p, local); break;
-            case 128: jvp_rfftj_block<SCHEME, T, 128>(X, spec, I.pp, p, local); break;
-            default: jvp_rfftj_block<SCHEME, T, 256>(X, spec, I.pp, p, local); break;
+            case 32: jvp_rfftj_block<SCHEME, T, 32>(X, spec, I.pp, p, jc, jr, local); break;
+            case 64: jvp_rfftj_block<SCHEME, T, 64>(X, spec, I.pp, p, jc, jr, local); break;
+            case 128: jvp_rfftj_block<SCHEME, T, 128>(X, spec, I.pp, p, jc, jr, local); break;
+            default: jvp_rfftj_block<SCHEME, T, 256>(X, spec, I.pp, p, jc, jr, local); break;
         }
     });
 }
@@ -639,6 +685,8 @@ __global__ void k_b_prologue(const BInst* __restrict__ tab, const int* __restric
 __global__ void __launch_bounds__(1024) k_b_poisson(const BInst* __restrict__ tab, const int* __restrict__ L, int n) {
     for_work<F_INST>(tab, L, n, [&](const BInst& I, int) {
         for (int i = threadIdx.x; i < I.nx; i += blockDim.x) I.hxp[i] = I.h1c[i];
+        __syncthreads();
+        jcoef_block(I, false);   // the pass's Jacobian column coefficients from the new profile
         poisson_apply_cta(I.phi, I.n, nullptr, I.nx, I.po.hx2_inv, I.po.charge, 2, &I.ds->pnorm2, I.po.la0, I.po.la1,
                           I.po.la2, I.po.lden, I.po.ravg, I.po.ra0, I.po.ra1, I.po.ra2, I.po.rden);
     });
