@@ -2690,8 +2690,8 @@ int b_arnoldi(vv_batch* b) {
     TRY(blaunch(b, vv::k_b_gm_maxpy_p<T>, vv::F_VEC, vv::RED_THREADS, 0, tab, A, b->n));
     // ||w||, Arnoldi bookkeeping and the BC_INNER control step in one launch
     return blaunch(b, vv::k_b_arnoldi_ctrl, vv::F_INST, vv::CTRL_THREADS, 0, tab, A, b->n,
-                   (b->use_graph ? b->hnd[BH_INNER] : 0ull), b->flag, b->counts, b->lists, b->counts + 7,
-                   b->counts + 6);
+                   (b->use_graph ? b->hnd[BH_INNER] : 0ull), b->flag, b->counts, b->lists, b->counts + vv::BN_DONE,
+                   b->counts + vv::BN_DROPPED);
 }
 
 template <int S, typename T>
@@ -2768,6 +2768,14 @@ int b_body(vv_batch* b, int level, cudaGraph_t body, F fn) {
     return VV_OK;
 }
 
+// Arnoldi steps per iteration of the batch graph's inner loop (VV_BATCH_UNROLL=1..4 overrides)
+constexpr int INNER_UNROLL = 2;
+int inner_unroll() {
+    const char* e = getenv("VV_BATCH_UNROLL");
+    const int u = e ? atoi(e) : INNER_UNROLL;
+    return (u >= 1 && u <= 4) ? u : INNER_UNROLL;
+}
+
 template <int S, typename T>
 int b_capture(vv_batch* b) {
     // the loop handles exist before the control kernels that set them are captured
@@ -2794,10 +2802,15 @@ int b_capture(vv_batch* b) {
             b->nk_cycle_head = (int)(b->launches - q);
             cudaGraph_t inner[1];
             TRY(add_conditional(b->g, b->st, cudaGraphCondTypeWhile, 1, 0, &b->hnd[BH_INNER], inner));
+            // INNER_UNROLL Arnoldi steps per iteration of the conditional loop
+            // (each iteration costs about five kernel launches of its own); a
+            // step after the one that emptied the inner list finds it empty and
+            // does nothing (every kernel walks an empty list)
             TRY(b_body(b, 3, inner[0], [&]() -> int {
                 const int64_t w = b->launches;
-                TRY(b_arnoldi<S, T>(b));
-                b->nk_arnoldi = (int)(b->launches - w);
+                const int unroll = inner_unroll();
+                for (int u = 0; u < unroll; ++u) TRY(b_arnoldi<S, T>(b));
+                b->nk_arnoldi = (int)(b->launches - w) / unroll;
                 return VV_OK;
             }));
             q = b->launches;
@@ -3215,12 +3228,12 @@ int vv_batch_create(int n, vv_ctx* const* ctxs, const vv_state* states, vv_batch
     b->list_words = vv::blist_words(n);
     b->words = (int)(offsetof(vv::DevState, hcol) / sizeof(unsigned int));
     if (cudaMalloc((void**)&b->lists, (size_t)vv::NLIST * b->list_words * sizeof(int)) != cudaSuccess ||
-        cudaMalloc((void**)&b->counts, 8 * sizeof(unsigned int)) != cudaSuccess ||
+        cudaMalloc((void**)&b->counts, vv::BN_WORDS * sizeof(unsigned int)) != cudaSuccess ||
         cudaMalloc((void**)&b->flag, sizeof(int)) != cudaSuccess ||
         cudaMalloc((void**)&b->gather, (size_t)n * b->words * sizeof(unsigned int)) != cudaSuccess)
         return fail_b(VV_ERR_ALLOC);
     if (cudaMallocHost((void**)&b->hflag, sizeof(int)) != cudaSuccess ||
-        cudaMallocHost((void**)&b->hcounts, 8 * sizeof(unsigned int)) != cudaSuccess ||
+        cudaMallocHost((void**)&b->hcounts, vv::BN_WORDS * sizeof(unsigned int)) != cudaSuccess ||
         cudaMallocHost((void**)&b->hgather, (size_t)n * b->words * sizeof(unsigned int)) != cudaSuccess)
         return fail_b(VV_ERR_ALLOC);
     for (auto& s : b->cs)
@@ -3303,7 +3316,7 @@ int vv_batch_launch(vv_batch* b, const vv_snes_opts* so, const vv_ksp_opts* ko) 
     }
     b->st = b->user;
     b->pending_l0 = b->launches;
-    CK(cudaMemsetAsync(b->counts, 0, 8 * sizeof(unsigned int), b->user));
+    CK(cudaMemsetAsync(b->counts, 0, vv::BN_WORDS * sizeof(unsigned int), b->user));
     if (b->use_graph) {
         CK(cudaGraphLaunch(b->ex, b->user));
     } else {
@@ -3317,7 +3330,7 @@ int vv_batch_launch(vv_batch* b, const vv_snes_opts* so, const vv_ksp_opts* ko) 
     CK(cudaGetLastError());
     CK(cudaMemcpyAsync(b->hgather, b->gather, (size_t)b->n * b->words * sizeof(unsigned int), cudaMemcpyDeviceToHost,
                        b->user));
-    CK(cudaMemcpyAsync(b->hcounts, b->counts, 8 * sizeof(unsigned int), cudaMemcpyDeviceToHost, b->user));
+    CK(cudaMemcpyAsync(b->hcounts, b->counts, vv::BN_WORDS * sizeof(unsigned int), cudaMemcpyDeviceToHost, b->user));
     b->st = b->cs[0];
     b->pending = 1;
     return VV_OK;
@@ -3334,7 +3347,8 @@ int vv_batch_collect(vv_batch* b, const vv_snes_opts* so, const vv_ksp_opts* ko,
         b->launches = b->pending_l0 + 1 + b->nk_prologue + b->nk_revert_ctrl +
                       (int64_t)k[vv::BC_PIC] * (b->nk_pic_head + b->nk_pic_tail) +
                       (int64_t)(k[vv::BC_GM_START] + k[vv::BC_GM_FINISH]) * (b->nk_cycle_head + b->nk_cycle_tail) +
-                      (int64_t)k[vv::BC_INNER] * b->nk_arnoldi + (int64_t)k[vv::BC_REVERT] * b->nk_revert;
+                      (int64_t)(k[vv::BC_INNER] + k[vv::BN_IDLE]) * b->nk_arnoldi +
+                      (int64_t)k[vv::BC_REVERT] * b->nk_revert;
     }
     int first_bad = VV_OK;
     vv::DevState d;

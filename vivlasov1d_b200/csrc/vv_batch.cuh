@@ -1163,6 +1163,11 @@ __global__ void __launch_bounds__(RED_THREADS, 3) k_b_gm_update(const BInst* __r
 // the batch loop condition: handle (0 outside a graph) and *flag (read by
 // the host-driven loop).  counts[op] counts the passes.
 enum BCtrl { BC_PIC = 0, BC_GM_START = 1, BC_INNER = 2, BC_GM_FINISH = 3, BC_REVERT = 4, BC_ALL = 5 };
+// words of the batch's counter array after the passes per BCtrl op: the
+// Arnoldi control's dropped-instance count and grid counter, and the Arnoldi
+// steps that found the inner list empty (the unrolled loop body's idle
+// copies, for the launch count)
+enum BCount { BN_DROPPED = 6, BN_DONE = 7, BN_IDLE = 8, BN_WORDS = 9 };
 
 
 // rebuild list `l` from the per-instance membership test `in(q)` over the
@@ -1338,7 +1343,10 @@ k_b_arnoldi_ctrl(const BInst* __restrict__ tab, const int* __restrict__ L, int n
     int* LI = lists + (size_t)L_INNER * blist_words(n);
     const int cnt = LI[0];
     const int* ids = LI + 1 + NFAM;
-    if (threadIdx.x == 0) s_dropped = atomicExch(dropped, 0u);
+    if (threadIdx.x == 0) {
+        s_dropped = atomicExch(dropped, 0u);
+        if (cnt == 0 && counts) counts[BN_IDLE] += 1u;   // an idle copy of the step
+    }
     __syncthreads();
     if (s_dropped)
         ctrl_build_from(tab, n, cnt, lists, L_INNER, [&](int q) {
