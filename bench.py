@@ -25,8 +25,10 @@ field_energy: after W+K steps, |E - E_oracle| / |E_oracle| per instance for
               same W+K steps, which is also the timed cpu_baseline), and
               the batched mixed arm against the plain FP64 GPU arm.
 e2e         : the batched mixed step through Batch.step(host=...), which
-              copies every instance's f host->device (pinned) before and
-              device->host after each step.
+              copies every instance's f host->device (one pinned buffer)
+              before and device->host after each step, in four pieces each
+              way, a step's pieces in waiting only for the previous step's
+              same piece out (the two directions overlap).
 batched_fp64: the same table through the batch in FP64 (ksp_rtol 1e-4): the
               gain of batching alone, apart from the FP32 inner solves.  After
               the first warm-up step it runs as two tables at once on two
@@ -255,15 +257,20 @@ def run_gpu(args, rank, world):
     tri_s = batch.time_kernel(4, it=MDOT_IT, reps=10)
     op_s = batch.time_kernel(5, it=MDOT_IT, reps=10)
     # ---- e2e: host buffers through the public API, the same K steps again ----
-    hosts = [torch.empty_like(r.fc, device="cpu").pin_memory() for r in mixed]
-    for h, snap, r in zip(hosts, snapshot, mixed):
-        h.copy_(snap)
+    # one pinned host buffer with every instance's f back to back
+    hosts = torch.empty(sum(r.fc.numel() for r in mixed), dtype=mixed[0].fc.dtype).pin_memory()
+    off = 0
+    for snap, r in zip(snapshot, mixed):
+        k = snap.numel()
+        hosts[off:off + k].copy_(snap.reshape(-1))
+        off += k
         r.fc.copy_(snap)
         r.calculate_moments()
     del snapshot
 
-    # every instance's f copied in from its pinned host buffer before the step
-    # and back out after it, by the batch on each table's stream
+    # every instance's f copied in from the host buffer before the step and
+    # back out after it (Batch.step(host=...): one copy each way in pieces,
+    # the next step's pieces in overlapping this step's pieces out)
     t_e2e, _ = time_steps(lambda: batch.step(host=hosts), args.steps, stream)
     total_cells = cells
     if world > 1:

@@ -620,6 +620,37 @@ def test_batch_step_host_buffers(monkeypatch, split):
             assert torch.equal(hosts[i], via[i].fc.cpu()), i
 
 
+@pytest.mark.parametrize("split", [None, [[0, 2], [1]]])
+def test_batch_step_one_host_buffer(monkeypatch, split):
+    """Batch.step(host=<one pinned buffer>) moves every instance's f through
+    a staging buffer in pieces, the pieces of a step's copy-in waiting for
+    the previous step's pieces out: the same bits as steps of the resident
+    state, the buffer holds each step's result once the caller's stream is
+    synchronized, and a change the host makes to the buffer between steps
+    reaches the next step."""
+    from vivlasov1d_b200.batch import Batch
+    monkeypatch.setenv("VV_BATCH_SHAPE", "2,6,0,1,0,1")
+    dev = [_small_run(*s) for s in BATCH_SPECS]
+    via = [_small_run(*s) for s in BATCH_SPECS]
+    host = torch.cat([r.fc.detach().reshape(-1).cpu() for r in via]).pin_memory()
+    bd, bh = Batch(dev, split=split), Batch(via, split=split)
+    offs = [0]
+    for r in via:
+        offs.append(offs[-1] + r.fc.numel())
+    for k in range(3):
+        if k == 2:   # the host edits instance 1's f between steps; the resident arm gets the same edit
+            host[offs[1]:offs[2]] *= 1.0 + 2.0 ** -20
+            dev[1].fc.mul_(1.0 + 2.0 ** -20)
+        rd, rh = bd.step(), bh.step(host=host)
+        torch.cuda.current_stream().synchronize()
+        for i in range(len(BATCH_SPECS)):
+            assert rd[i] == rh[i], (k, i)
+            assert torch.equal(dev[i].fc, via[i].fc), (k, i)
+            assert torch.equal(host[offs[i]:offs[i + 1]], via[i].fc.reshape(-1).cpu()), (k, i)
+    with pytest.raises(ValueError):
+        bh.step(host=host[:-1])
+
+
 def test_batch_launch_collect_order(monkeypatch):
     """vv_batch_collect without a launch, and a second launch before the
     collect, are refused (VV_ERR_ARG) and leave the batch usable."""

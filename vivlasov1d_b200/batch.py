@@ -34,6 +34,7 @@ from .run import report_dict
 SPLIT_MIN = 16        # smallest table that "auto" splits
 SPLIT_FRACTION = 8    # the slow table holds 1/SPLIT_FRACTION of the instances
 SLOW_PRIORITY = 0     # stream priority of the slow table (lower is higher)
+HOST_CHUNKS = 4       # pieces of the one-buffer host copies (step(host=tensor))
 
 
 class _Lockstep:
@@ -154,14 +155,71 @@ class Batch:
         self._tables = []
         self._form([fast, slow])
 
+    def _flat_setup(self, host):
+        """The staging buffer, its views shaped like each run's f and the
+        copy streams of the one-buffer form of step(host=...)."""
+        total = sum(r.fc.numel() for r in self.runs)
+        if host.dim() != 1 or host.numel() != total or host.dtype != self.runs[0].fc.dtype:
+            raise ValueError("host: one 1-D tensor of every run's f back to back (%d values)" % total)
+        if host.device.type != "cpu" or not host.is_pinned():
+            raise ValueError("host: pinned host memory")
+        st = getattr(self, "_flat", None)
+        if st is None or st["n"] != total:
+            stage = torch.empty(total, dtype=host.dtype, device=self.runs[0].fc.device)
+            views, off = [], 0
+            for r in self.runs:
+                k = r.fc.numel()
+                views.append(stage[off:off + k].view(r.fc.shape))
+                off += k
+            bounds = [total * c // HOST_CHUNKS for c in range(HOST_CHUNKS + 1)]
+            st = {"n": total, "stage": stage, "views": views, "bounds": bounds,
+                  "cin": torch.cuda.Stream(), "cout": torch.cuda.Stream(), "out": None}
+            self._flat = st
+        return st
+
+    def _step_flat(self, host, caller):
+        st = self._flat_setup(host)
+        stage, b = st["stage"], st["bounds"]
+        fcs = [r.fc for r in self.runs]
+        # in: piece c after the previous step's piece c went out
+        with torch.cuda.stream(st["cin"]):
+            for c in range(HOST_CHUNKS):
+                if st["out"] is not None:
+                    st["cin"].wait_event(st["out"][c])
+                stage[b[c]:b[c + 1]].copy_(host[b[c]:b[c + 1]], non_blocking=True)
+        caller.wait_stream(st["cin"])
+        torch._foreach_copy_(fcs, st["views"])
+        reps = self.step()
+        # out: gather on the caller's stream, the pieces on the copy stream
+        torch._foreach_copy_(st["views"], fcs)
+        st["cout"].wait_stream(caller)
+        out = []
+        with torch.cuda.stream(st["cout"]):
+            for c in range(HOST_CHUNKS):
+                host[b[c]:b[c + 1]].copy_(stage[b[c]:b[c + 1]], non_blocking=True)
+                out.append(st["cout"].record_event())
+        st["out"] = out
+        caller.wait_stream(st["cout"])
+        return reps
+
     def step(self, host=None):
         """Advance every instance by one time step; returns per-instance reports.
 
-        host: optional list of n host tensors (pinned, shaped like each run's
-        f): every instance's f is copied in from its buffer before its table's
-        step and back out after it, on the table's stream (with two tables the
-        copies of one overlap the other's step)."""
+        host: optional host memory that every instance's f is copied in from
+        before the step and back out to after it:
+          - a list of n host tensors (pinned, shaped like each run's f): the
+            copies run on each table's stream (with two tables the copies of
+            one overlap the other's step), complete when step() returns;
+          - one pinned 1-D tensor holding every run's f back to back (run
+            order, row-major): one copy each way through a device staging
+            buffer, in HOST_CHUNKS pieces, the pieces out on a copy stream
+            that the next step's pieces in wait for piece by piece (so the
+            two directions overlap); the copies out are ordered before any
+            later work on the caller's stream -- synchronize it before
+            reading the buffer."""
         caller = torch.cuda.current_stream()
+        if isinstance(host, torch.Tensor):
+            return self._step_flat(host, caller)
         if host is not None and len(host) != self.n:
             raise ValueError("host: one buffer per run")
 
