@@ -182,3 +182,27 @@ def test_config_dissipation_choices():
     assert _lib.COLLISION["collt"] == 1 and _lib.COLLISION["colle"] == 2
     assert _lib.DOUBLE_BRACKET["ffh"] == 1 and _lib.DOUBLE_BRACKET["fhh"] == 2
     assert _lib.LAPLACE["cfd2ave"] == 12 and _lib.LAPLACE["simpsonave"] == 15
+
+
+def test_batch_reports_are_built_on_access():
+    """Batch.step's reports: snapshots of the report structs of every table,
+    mapped back to instance order, each dictionary built on first access
+    (and then kept), with the instance's status; the same contents as the
+    eager report_dict."""
+    from vivlasov1d_b200 import _lib
+    from vivlasov1d_b200.batch import Reports
+    from vivlasov1d_b200.run import report_dict
+    a = (_lib.vv_step_report * 3)()
+    a[1].picard_its = 2
+    a[1].gmres_its[0], a[1].gmres_its[1] = 5, 7
+    b = (_lib.vv_step_report * 2)()
+    b[0].picard_its = 1
+    reps = Reports([(a, [0, 0, 3]), (b, [1, 0])], [(0, 0), (1, 0), (0, 1), (1, 1), (0, 2)])
+    assert len(reps) == 5
+    assert reps[2]["gmres_its"] == [5, 7] and reps[2] is reps[2]
+    assert [r["status"] for r in reps] == [0, 1, 0, 0, 3]
+    assert reps[-1]["status"] == 3 and reps[1:3][1]["picard_its"] == 2
+    expect = dict(report_dict(a[1]), status=0)
+    assert reps[2] == expect and reps == list(reps)
+    a[1].picard_its = 9   # the snapshot is the caller's: later steps do not reach built entries
+    assert reps[2]["picard_its"] == 2

@@ -17,13 +17,22 @@ re-forms it as two tables -- the eighth of the instances that needed the
 most GMRES iterations, and the rest -- which every later step launches at
 once on two streams (``vv_batch_launch``) and collects together
 (``vv_batch_collect``), so that the two tables' passes interleave.  On the
-256-instance sweep this saves 2-3% of a step: the slow table's instances
-are the largest, and both tables' kernels need the whole GPU.  Each
-instance computes the same operations in either form (the tables' tuned
-kernel shapes may differ, so results agree to rounding).
+256-instance sweep this saves 8% of an FP64 step and costs 1-3% of a
+mixed-precision one: the slow table's instances are the largest, and both
+tables' kernels need the whole GPU.  Each instance computes the same
+operations in either form (the tables' tuned kernel shapes may differ, so
+results agree to rounding).
+
+The host stands between two steps: ``step()`` waits for the step's
+reports before it returns, and the next step's graph starts when the host
+launches it.  The reports are therefore built on access, and a process
+holding many Python objects should keep the cyclic collector's full passes
+out of its step loop (``gc.freeze()`` after set-up): on the sweep a full
+pass over 200k objects stalled the host by about 2 ms per 25.5 ms step.
 """
 from __future__ import annotations
 
+import collections.abc
 import ctypes as C
 
 import torch
@@ -35,6 +44,39 @@ SPLIT_MIN = 16        # smallest table that "auto" splits
 SPLIT_FRACTION = 8    # the slow table holds 1/SPLIT_FRACTION of the instances
 SLOW_PRIORITY = 0     # stream priority of the slow table (lower is higher)
 HOST_CHUNKS = 4       # pieces of the one-buffer host copies (step(host=tensor))
+
+
+class Reports(collections.abc.Sequence):
+    """The per-instance reports of one batch step (``report_dict`` plus
+    "status"), each built from a snapshot of the library's report structs
+    on first access: the dictionaries of a 256-instance step take 1-2 ms of
+    Python, which the host would otherwise spend between two step launches
+    while the GPU waits."""
+
+    def __init__(self, sources, where):
+        self._sources = sources   # [(report struct array snapshot, statuses)]
+        self._where = where       # instance -> (source, index in it)
+        self._built = [None] * len(where)
+
+    def __len__(self):
+        return len(self._where)
+
+    def __getitem__(self, i):
+        if isinstance(i, slice):
+            return [self[k] for k in range(*i.indices(len(self)))]
+        if i < 0:
+            i += len(self)
+        d = self._built[i]
+        if d is None:
+            k, j = self._where[i]
+            raw, status = self._sources[k]
+            d = report_dict(raw[j])
+            d["status"] = status[j]
+            self._built[i] = d
+        return d
+
+    def __eq__(self, other):
+        return list(self) == list(other)
 
 
 class _Lockstep:
@@ -74,12 +116,13 @@ class _Lockstep:
         _lib.check(self.lib.vv_batch_launch(self.h, C.byref(self.snes), C.byref(self.ksp)), "vv_batch_launch")
 
     def collect(self):
-        """(status, reports) of the launched step; status is the first non-OK instance status."""
+        """(status, (report structs, statuses)) of the launched step: snapshots
+        that the next step does not overwrite; status is the first non-OK
+        instance status."""
         st = self.lib.vv_batch_collect(self.h, C.byref(self.snes), C.byref(self.ksp), self._reports, self._status)
-        reps = [report_dict(self._reports[i]) for i in range(self.n)]
-        for i in range(self.n):
-            reps[i]["status"] = self._status[i]
-        return st, reps
+        raw = (_lib.vv_step_report * self.n)()
+        C.memmove(raw, self._reports, C.sizeof(raw))
+        return st, (raw, list(self._status))
 
     def launch_count(self, reset=False):
         n = C.c_int64()
@@ -203,7 +246,8 @@ class Batch:
         return reps
 
     def step(self, host=None):
-        """Advance every instance by one time step; returns per-instance reports.
+        """Advance every instance by one time step; returns the per-instance
+        reports (a ``Reports`` sequence of dictionaries, built on access).
 
         host: optional host memory that every instance's f is copied in from
         before the step and back out to after it:
@@ -245,13 +289,14 @@ class Batch:
             results = [t.collect() for t in self._tables]
             for s in self._streams:
                 caller.wait_stream(s)
-        reps = [None] * self.n
+        where = [None] * self.n
         worst = _lib.VV_OK
-        for g, (st, rg) in zip(self.groups, results):
-            for i, r in zip(g, rg):
-                reps[i] = r
+        for k, (g, (st, _)) in enumerate(zip(self.groups, results)):
+            for j, i in enumerate(g):
+                where[i] = (k, j)
             if st != _lib.VV_OK and worst == _lib.VV_OK:
                 worst = st
+        reps = Reports([src for _, src in results], where)
         for r in self.runs:
             r.itime += 1
         # an instance whose residual is above the abort threshold or NaN fails
