@@ -1335,7 +1335,10 @@ k_b_arnoldi_ctrl(const BInst* __restrict__ tab, const int* __restrict__ L, int n
             if (!s->active) atomicAdd(dropped, 1u);   // before this block's arrival at the counter
         }
     });
-    if ((int)blockIdx.x >= nb || !last_block(done, nb)) return;
+    // one participating block (an instance or none left: the lockstep tail)
+    // is the last by itself and skips the grid counter's fence and atomic;
+    // its own state writes are ordered by the barrier that ended its item
+    if ((int)blockIdx.x >= nb || (nb > 1 && !last_block(done, nb))) return;
     // the inner loop only drops instances: compact the current L_INNER in
     // place instead of scanning the whole table (a tail pass with a few
     // instances left reads a few states, not n), and only when an instance
